@@ -1,0 +1,330 @@
+"""Benchmark of the nonbonded force path (cutoff + PME) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload: the 14,281-atom chain-in-water box (4,463 TIP3P waters + an
+892-atom random-walk chain, 52.3 A cube), LJ C2 10 -> 12 A + Ewald real space
+(Cutoff 12 A, alpha 0.32) as one NonbondedCutoff force, plus PME 64^3, order
+4, reciprocal + correction.  One step = one full force evaluation (binning,
+pair force, PME, energy and virial).  Synthetic seeded data.
+
+`value`: mixed-precision force evaluations/s with positions already in HBM
+(device API), timed per step with CUDA events on the library's stream; the
+L2 is flushed (256 MB write) between timed steps, outside the events.
+`e2e`: the same through pmgpu_evaluate with pinned host buffers (positions
+H2D, forces + energies D2H inside the timed region), wall clock per call.
+Under torchrun each rank evaluates its own replica (the path does not
+shard); value = total evaluations/s over ranks from the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "force evals/s (cutoff+PME) mixed vs FP64 on one B200 at ≤1e-5 force error"
+UNIT = "evals/s"
+FP32_LANES_PER_SM = 128
+N_SMS = 148
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=None)
+        pg = dist
+    return rank, world, local, pg
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(system, defs, evals):
+    """The reference's own CPU force path (oracle/_ref/pmref_fast, built from
+    the ProtoMol sources with its gcc preset), 1 core."""
+    from oracle import oracle
+    from protomol_b200 import forces as F
+    specs = [F.parse_definition(d) for d in defs]
+    fast = oracle.reference_available(fast=True)
+    if fast or oracle.reference_available():
+        r = oracle.run_reference(system, specs, repeat=evals, fast=fast, timeout=600)
+        sec = r["seconds_per_eval"]
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        for _ in range(evals):
+            oracle.evaluate(system, specs)
+        sec = (time.perf_counter() - t0) / evals
+        kind = "port"
+    return {"value": 1.0 / sec, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{evals} full evaluations (after 1 warm-up) of the 14,281-atom cutoff+PME force, "
+                      f"{'pmref_fast (reference sources, -O3 -ffast-math preset)' if kind == 'reference' else 'CPU port'}"}
+
+
+def run_reference_arm(args, rank, world, pg):
+    from protomol_b200 import workloads
+    w = workloads.chain14281()
+    if rank != 0:
+        if pg:
+            pg.barrier()
+        return
+    evals = max(1, args.steps)
+    evals = min(evals, 40)
+    base = cpu_baseline(w.system, w.forces, evals)
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
+            "steps": evals, "warmup": 1, "ms_per_step": 1000.0 / base["value"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "chain14281 cutoff12 C2 + EwaldReal + PME 64^3 order 4",
+                       "atoms": w.system.n_atoms, "parallelism": "replicas"},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+
+
+def main():
+    args = parse()
+    rank, world, local, pg = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world, pg)
+        if pg:
+            pg.destroy_process_group()
+        return
+
+    import torch
+    from protomol_b200 import _lib
+    from protomol_b200 import forces as F
+    from protomol_b200 import workloads
+
+    torch.cuda.set_device(local)
+    lib = _lib.load()
+    w = workloads.chain14281()
+    s = w.system
+    n = s.n_atoms
+    topo = F.Topology(s, device=local)
+    mixed = [F.ForceFactory.make(topo, d, "mixed") for d in w.forces]
+    fp64 = [F.ForceFactory.make(topo, d, "fp64") for d in w.forces]
+    stream = torch.cuda.ExternalStream(topo.stream)
+    dpos = torch.tensor(s.positions, dtype=torch.float64, device=f"cuda:{local}")
+    dfor = torch.zeros((n, 3), dtype=torch.float64, device=f"cuda:{local}")
+    den = torch.zeros(11, dtype=torch.float64, device=f"cuda:{local}")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    VP = C.c_void_p
+
+    def step(forces):
+        arr = (VP * len(forces))(*[f.handle for f in forces])
+        _lib.check(lib.pmgpu_evaluate_device(topo.handle, len(forces), arr, VP(dpos.data_ptr()),
+                                             VP(dfor.data_ptr()), VP(den.data_ptr()), _lib.FLAG_VIRIAL), topo.handle)
+
+    def timed(forces, steps, warmup, sampler=None):
+        torch.cuda.synchronize()
+        for _ in range(warmup):
+            step(forces)
+        _lib.check(lib.pmgpu_synchronize(topo.handle), topo.handle)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        launches0 = topo.launch_count()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for k in range(steps):
+                flush.zero_()                      # L2 flush, outside the timed events
+                evs[k][0].record(stream)
+                step(forces)
+                evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        _lib.check(lib.pmgpu_synchronize(topo.handle), topo.handle)
+        if pg:
+            pg.barrier()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        return ms, topo.launch_count() - launches0
+
+    # accuracy of the mixed path against the FP64 kernels on this input
+    fm = np.zeros((n, 3)); em = F.ScalarStructure()
+    F.evaluate_group(topo, mixed, s.positions, fm, em)
+    fd = np.zeros((n, 3)); ed = F.ScalarStructure()
+    F.evaluate_group(topo, fp64, s.positions, fd, ed)
+    force_err = float(np.sqrt(((fm - fd) ** 2).sum() / (fd ** 2).sum()))
+    e_err = abs((em.lennard_jones + em.coulomb) - (ed.lennard_jones + ed.coulomb)) / (
+        abs(ed.lennard_jones) + abs(ed.coulomb))
+
+    # FP64 kernels (the comparison point of the metric)
+    ms64, _ = timed(fp64, max(20, args.steps // 10), args.warmup)
+    # mixed precision (the value)
+    with ClockSampler(local) as clk:
+        ms_mixed, launches = timed(mixed, args.steps, args.warmup)
+    # per-kernel profile of the dominant kernel: pair kernel timed alone
+    t_local = float(np.mean(ms_mixed))
+    t_fp64 = float(np.mean(ms64))
+    if pg:
+        t = torch.tensor([t_local, t_fp64], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_local, t_fp64 = float(t[0]), float(t[1])
+
+    # end to end through the host API with pinned buffers
+    hpos = torch.tensor(s.positions, dtype=torch.float64).pin_memory()
+    hfor = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
+    e = _lib.Energies()
+    arr = (VP * len(mixed))(*[f.handle for f in mixed])
+    for _ in range(args.warmup):
+        _lib.check(lib.pmgpu_evaluate(topo.handle, len(mixed), arr, VP(hpos.data_ptr()), VP(hfor.data_ptr()),
+                                      C.byref(e), _lib.FLAG_VIRIAL), topo.handle)
+    e2e_steps = max(10, args.steps // 4)
+    walls = []
+    for _ in range(e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _lib.check(lib.pmgpu_evaluate(topo.handle, len(mixed), arr, VP(hpos.data_ptr()), VP(hfor.data_ptr()),
+                                      C.byref(e), _lib.FLAG_VIRIAL), topo.handle)
+        walls.append(time.perf_counter() - t0)
+    t_e2e = float(np.mean(walls)) * 1000.0
+    if pg:
+        t = torch.tensor([t_e2e], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_e2e = float(t[0])
+
+    # roofline of the dominant kernel (pair kernel) from a separate timing
+    pair_ms = pair_kernel_ms(lib, topo, mixed[0], dpos, dfor, den, stream, flush, torch)
+    peaks, peak_src = measured_peaks()
+    n_pairs = 5212013   # within-cutoff pairs of this input (oracle pair set)
+    flops_per_pair = 95
+    fp32_peak = N_SMS * FP32_LANES_PER_SM * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    achieved = n_pairs * flops_per_pair / (pair_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "kernel": "k_pair_mixed<LJ C2 + EwaldReal Cutoff>",
+                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                "traffic": None, "launch_ms": pair_ms,
+                "peak_source": f"nominal FP32 CUDA-core rate at sm_max_mhz of MEASURED_PEAKS.json ({peak_src}): "
+                               "148 SMs x 128 lanes x 2 flop",
+                "algorithmic": f"{n_pairs} pairs x {flops_per_pair} flop"}
+
+    if rank == 0:
+        value = world * 1000.0 / t_local
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_local, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+i64 fixed-point forces, f64 sums", "data": "synthetic",
+            "config": {"workload": "chain14281 cutoff12 C2 + EwaldReal + PME 64^3 order 4", "atoms": n,
+                       "parallelism": "replicas" if world > 1 else "single", "l2": "flushed between steps (256 MB)"},
+            "fp64": {"value": world * 1000.0 / t_fp64, "ms_per_step": t_fp64},
+            "speedup_vs_fp64": t_fp64 / t_local,
+            "accuracy_vs_fp64": {"force_rel_rms": force_err, "energy_rel": e_err},
+            "e2e": {"value": world * 1000.0 / t_e2e, "unit": UNIT, "ms_per_step": t_e2e,
+                    "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 88},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(s, w.forces, 12)
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def pair_kernel_ms(lib, topo, force, dpos, dfor, den, stream, flush, torch, reps=50):
+    """Average duration of one cutoff-force evaluation (binning + pair kernel
+    + finalize) minus binning alone is not separable from outside; time the
+    cutoff force alone as the pair-kernel bound."""
+    VP = C.c_void_p
+    arr = (VP * 1)(force.handle)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for _ in range(5):
+        lib.pmgpu_evaluate_device(topo.handle, 1, arr, VP(dpos.data_ptr()), VP(dfor.data_ptr()),
+                                  VP(den.data_ptr()), 1)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(reps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            lib.pmgpu_evaluate_device(topo.handle, 1, arr, VP(dpos.data_ptr()), VP(dfor.data_ptr()),
+                                      VP(den.data_ptr()), 1)
+            evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    return float(np.mean([a.elapsed_time(b) for a, b in evs]))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,208 @@
+/*
+ * pmgpu.h -- C ABI of the B200 nonbonded force path (libpmgpu.so).
+ *
+ * The library evaluates ProtoMol's nonbonded system forces on one GPU:
+ *   - the cell-list cutoff force NonbondedCutoffSystemForce with
+ *     OneAtomPair / OneAtomPairTwo of LennardJones, Coulomb and
+ *     CoulombEwaldReal under C1, C2, Cutoff and Shift switching
+ *     (forces/NonbondedCutoffSystemForce.h:63-74, forces/OneAtomPair.h:127-188,
+ *     forces/OneAtomPairTwo.h:131-199);
+ *   - the particle-mesh Ewald force NonbondedPMEwaldSystemForce with
+ *     -real / -reciprocal / -correction and B-spline interpolation
+ *     (forces/NonbondedPMEwaldSystemForce.h:271-349).
+ *
+ * One pmgpu_system mirrors a ProtoMol Topology<PeriodicBoundaryConditions,
+ * CubicCellManager> (atoms, exclusion table, Lennard-Jones table, box, cell
+ * size).  One pmgpu_force mirrors one force object made by ForceFactory from
+ * its keyword string.  pmgpu_evaluate mirrors SystemForce::evaluate
+ * (forces/SystemForce.h:18-76) for one or several forces of a ForceGroup:
+ * forces and energies are ACCUMULATED into the caller's arrays (+=), never
+ * overwritten, exactly as the reference accumulates into its Vector3DBlock and
+ * ScalarStructure.
+ *
+ * Plain C types only; every call returns a status code (PMGPU_OK = 0) and
+ * pmgpu_last_error() returns the message of the last failure.  A context is
+ * not thread-safe; it owns one CUDA stream.  There is no CPU fallback: without
+ * a usable GPU every call that needs one fails with PMGPU_ERR_CUDA.
+ */
+#ifndef PMGPU_H
+#define PMGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMGPU_ABI_VERSION 1
+
+/* status codes */
+#define PMGPU_OK 0
+#define PMGPU_ERR_ARG 1           /* invalid argument (reference: doMake errMsg / report << error) */
+#define PMGPU_ERR_CUDA 2          /* CUDA runtime error or no device */
+#define PMGPU_ERR_OVERFLOW 3      /* non-finite or out-of-range force (fixed-point range) */
+#define PMGPU_ERR_STATE 4         /* call order: topology / box not set, size mismatch */
+#define PMGPU_ERR_UNSUPPORTED 5   /* combination the reference does not register */
+#define PMGPU_ERR_NOMEM 6         /* device allocation failed */
+#define PMGPU_ERR_CAPACITY 7      /* a caller-provided capacity was too small */
+
+/* ExclusionClass (topology/ExclusionTable.h) */
+#define PMGPU_EXCL_NONE 0
+#define PMGPU_EXCL_MODIFIED 1
+#define PMGPU_EXCL_FULL 2
+
+/* pair potentials */
+#define PMGPU_POT_NONE 0
+#define PMGPU_POT_LENNARD_JONES 1     /* forces/LennardJonesForce.h:37-74 */
+#define PMGPU_POT_COULOMB 2           /* forces/CoulombForce.h:41-57 */
+#define PMGPU_POT_EWALD_REAL 3        /* forces/CoulombEwaldRealForce.h:45-73 */
+
+/* switching functions */
+#define PMGPU_SW_UNIVERSAL 0          /* topology/UniversalSwitchingFunction.h */
+#define PMGPU_SW_CUTOFF 1             /* topology/CutoffSwitchingFunction.h:64-68 */
+#define PMGPU_SW_C1 2                 /* topology/C1SwitchingFunction.h:64-75 */
+#define PMGPU_SW_C2 3                 /* topology/C2SwitchingFunction.h:64-82 */
+#define PMGPU_SW_SHIFT 4              /* topology/ShiftSwitchingFunction.h */
+
+/* arithmetic of a force */
+#define PMGPU_PRECISION_MIXED 0       /* FP32 pair/spread/FFT/gather, int64 fixed-point forces, FP64 sums */
+#define PMGPU_PRECISION_FP64 1        /* plain FP64 kernels, reference operation order */
+
+/* evaluate flags */
+#define PMGPU_FLAG_VIRIAL 1u          /* ScalarStructure::virial() (base/ScalarStructure.h:135) */
+
+typedef struct pmgpu_system pmgpu_system;
+typedef struct pmgpu_force pmgpu_force;
+
+/* ScalarStructure slots this path writes (base/ScalarStructure.h:25-54):
+ * LENNARDJONES, COULOMB and VIRIALXX..VIRIALZZ (row major). */
+typedef struct {
+    double lennard_jones;
+    double coulomb;
+    double virial[9];
+} pmgpu_energies;
+
+/* One NonbondedCutoffSystemForce.  n_terms = 1: OneAtomPair<Periodic, sw[0],
+ * pot[0]>; n_terms = 2: OneAtomPairTwo<Periodic, sw[0], pot[0], sw[1],
+ * pot[1]> with pot[0] = LENNARD_JONES.  cutoff[k] is the switching
+ * function's -cutoff, switchon[k] the C2 -switchon, alpha[k] the
+ * CoulombEwaldReal -alpha; algorithm_cutoff is the NonbondedCutoff -cutoff
+ * that sizes the neighbour-cell deltas
+ * (forces/NonbondedCutoffForce.h:111-129). */
+typedef struct {
+    int n_terms;
+    int pot[2];
+    int sw[2];
+    double switchon[2];
+    double cutoff[2];
+    double alpha[2];
+    double algorithm_cutoff;
+    int precision;
+} pmgpu_cutoff_params;
+
+/* NonbondedPMEwaldSystemForce<Periodic, Cubic, real, reciprocal, correction,
+ * BSpline, CutoffSwitchingFunction>; parameters in getParameters() order
+ * (forces/NonbondedPMEwaldSystemForce.h:1078-1090): -gridsize nx ny nz,
+ * -cutoff, -order (default 4), -accuracy (default 1e-6), -alpha (default -1:
+ * bisection of erfc(alpha Rc)/Rc = accuracy). */
+typedef struct {
+    int real;
+    int reciprocal;
+    int correction;
+    int grid[3];
+    int order;
+    double cutoff;
+    double accuracy;
+    double alpha;
+    int precision;
+} pmgpu_pme_params;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Replaces: constructing Topology<PeriodicBoundaryConditions, CubicCellManager>
+ * (topology/Topology.h:19-72). Selects the CUDA device and creates a stream. */
+int pmgpu_system_create(int device, pmgpu_system** out);
+int pmgpu_system_destroy(pmgpu_system* sys);
+
+/* Replaces the GenericTopology members the nonbonded forces read
+ * (topology/GenericTopology.h:129-144, filled by frontend/buildTopology.cpp):
+ * atoms[i].scaledCharge / .type / .molecule, lennardJonesParameters (T*T
+ * entries of {A, B, A14, B14}), exclusions.getTable() (pairs a1 < a2 with the
+ * table class) and coulombScalingFactor.  excl_check_class (may be NULL) is
+ * the class ExclusionTable::check() returns for each table pair; it differs
+ * from the table class only when the same pair was added twice with different
+ * classes (topology/ExclusionTable.cpp:122-141). */
+int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* scaled_charge,
+                       const int* type, const int* molecule, int n_types,
+                       const double* lj_table, int n_excl, const int* excl_pairs,
+                       const int* excl_class, const int* excl_check_class,
+                       double coulomb_scaling_factor);
+
+/* Replaces PeriodicBoundaryConditions::set (topology/PeriodicBoundaryConditions.cpp:40-77)
+ * and CubicCellManager(cellsize) (topology/CubicCellManager.cpp:11-16).
+ * Each vector has 3 doubles.  Orthogonal boxes only. */
+int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* e2, const double* e3,
+                  const double* origin, double cell_size);
+
+/* ---- forces ------------------------------------------------------------- */
+
+/* Replaces NonbondedCutoffForce::doMake (forces/NonbondedCutoffForce.h:119-123). */
+int pmgpu_cutoff_create(pmgpu_system* sys, const pmgpu_cutoff_params* params, pmgpu_force** out);
+
+/* Replaces NonbondedPMEwaldSystemForce::doMake (forces/NonbondedPMEwaldSystemForce.h:1099-1139);
+ * rejects the same parameter sets with PMGPU_ERR_ARG (order < 2 or odd,
+ * grid < order, cutoff <= 0, accuracy <= 0). */
+int pmgpu_pme_create(pmgpu_system* sys, const pmgpu_pme_params* params, pmgpu_force** out);
+
+int pmgpu_force_destroy(pmgpu_force* force);
+
+/* Splitting parameter a PME force uses (after the bisection, if any). */
+int pmgpu_pme_alpha(pmgpu_force* force, double* alpha);
+
+/* ---- evaluation ----------------------------------------------------------- */
+
+/* Replaces SystemForce::evaluate for each force in turn (ForceGroup::
+ * evaluateSystemForces, forces/ForceGroup.cpp:43-96).  positions: 3N
+ * doubles (host), forces_accum: 3N doubles (host, +=), energies (host, +=).
+ * Blocks until the results are on the host. */
+int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces,
+                   const double* positions, double* forces_accum,
+                   pmgpu_energies* energies, unsigned flags);
+
+/* Same with DEVICE pointers: d_positions (3N doubles), d_forces_accum (3N
+ * doubles, +=), d_energies (11 doubles laid out as pmgpu_energies, +=).
+ * Asynchronous on the system's stream; errors detected on the device are
+ * reported by the next pmgpu_synchronize(). */
+int pmgpu_evaluate_device(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces,
+                          const double* d_positions, double* d_forces_accum,
+                          double* d_energies, unsigned flags);
+
+int pmgpu_synchronize(pmgpu_system* sys);
+
+/* The system's CUDA stream (a cudaStream_t). */
+void* pmgpu_stream(pmgpu_system* sys);
+
+/* Number of kernels the library launched since the system was created. */
+long long pmgpu_launch_count(pmgpu_system* sys);
+
+/* Copies the last error message (NUL-terminated) into buf. */
+int pmgpu_last_error(pmgpu_system* sys, char* buf, int len);
+
+/* ---- diagnostics (parity tests) ----------------------------------------- */
+
+/* Cell of every atom from the GPU binning of the last evaluation, as
+ * buildCellLists computes it (topology/buildCellLists.cpp:11-38): 3N ints
+ * (x, y, z) and the grid dims. */
+int pmgpu_get_cells(pmgpu_system* sys, int* cells, int* dims);
+
+/* Evaluates one cutoff force (or a PME force with -real) in pair-recording
+ * mode and returns the within-cutoff pair set: every (min, max) atom index
+ * pair the force interacted, in no particular order.  *count receives the
+ * number of pairs; PMGPU_ERR_CAPACITY if it exceeds cap. */
+int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* force, const double* positions,
+                    long long* count, int* pairs, long long cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMGPU_H */

@@ -1,0 +1,281 @@
+"""Python access to the parity oracle.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke``
+and by ``bench.py``'s CPU-baseline leg, never by the product package.
+
+Two oracles live here:
+
+* ``liboracle`` -- the C restatement in ``oracle/pmoracle.c`` (built into
+  ``oracle/_build/libpmoracle.so`` by :func:`build`), called through ctypes;
+* ``run_reference`` -- the reference's own force classes compiled from the
+  ProtoMol sources (``oracle/ref/Makefile`` -> ``oracle/_ref/pmref``), run as a
+  subprocess on a system file.  It exists only where it was built.
+
+Force specifications are plain dicts shared by both:
+
+``{"kind": "cut", "terms": [(sw, pot, switchon, cutoff, alpha), ...],
+"algo_cutoff": rc}``, ``{"kind": "pme", "real": 0, "reciprocal": 1,
+"correction": 1, "grid": (nx, ny, nz), "order": 4, "cutoff": rc,
+"accuracy": 1e-6, "alpha": a}`` and ``{"kind": "full", "terms": [...]}``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REF_DIR = os.path.join(HERE, "_ref")
+LIB = os.path.join(BUILD, "libpmoracle.so")
+
+SW = {"Universal": 0, "Cutoff": 1, "C1": 2, "C2": 3, "Shift": 4}
+POT = {"LennardJones": 1, "Coulomb": 2, "CoulombEwaldReal": 3}
+
+
+def build(force: bool = False) -> str:
+    """Compile the C restatement (plain gcc, no FMA contraction)."""
+    src = os.path.join(HERE, "pmoracle.c")
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
+            os.path.getmtime(src), os.path.getmtime(os.path.join(HERE, "pmoracle.h"))):
+        os.makedirs(BUILD, exist_ok=True)
+        subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared",
+                               "-o", LIB, src, "-lm"])
+    return LIB
+
+
+class _System(C.Structure):
+    _fields_ = [
+        ("n_atoms", C.c_int), ("pos", C.c_void_p), ("q", C.c_void_p),
+        ("type", C.c_void_p), ("mol", C.c_void_p), ("n_types", C.c_int),
+        ("lj", C.c_void_p), ("n_excl", C.c_int), ("excl", C.c_void_p),
+        ("excl_check", C.c_void_p), ("box", C.c_double * 12), ("csf", C.c_double),
+        ("cell_size", C.c_double),
+    ]
+
+
+class _Cut(C.Structure):
+    _fields_ = [
+        ("n_terms", C.c_int), ("pot", C.c_int * 2), ("sw", C.c_int * 2),
+        ("switchon", C.c_double * 2), ("sw_cutoff", C.c_double * 2),
+        ("alpha", C.c_double * 2), ("algo_cutoff", C.c_double),
+    ]
+
+
+class _Pme(C.Structure):
+    _fields_ = [
+        ("real", C.c_int), ("reciprocal", C.c_int), ("correction", C.c_int),
+        ("grid", C.c_int * 3), ("order", C.c_int), ("cutoff", C.c_double),
+        ("accuracy", C.c_double), ("alpha", C.c_double),
+    ]
+
+
+class _Result(C.Structure):
+    _fields_ = [
+        ("lennard_jones", C.c_double), ("coulomb", C.c_double),
+        ("virial", C.c_double * 9), ("n_pairs", C.c_longlong), ("alpha", C.c_double),
+        ("e_real", C.c_double), ("e_recip", C.c_double), ("e_intra", C.c_double),
+        ("e_self", C.c_double), ("e_charged", C.c_double), ("out_of_grid", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        _lib.pmo_poly5.restype = C.c_double
+        _lib.pmo_poly5.argtypes = [C.c_double]
+    return _lib
+
+
+class _Keep:
+    """Holds the numpy arrays a _System points into."""
+
+    def __init__(self, system, positions=None):
+        pos = system.positions if positions is None else positions
+        self.pos = np.ascontiguousarray(pos, np.float64)
+        self.q = np.ascontiguousarray(system.scaled_charge, np.float64)
+        self.type = np.ascontiguousarray(system.atom_type, np.int32)
+        self.mol = np.ascontiguousarray(system.molecule, np.int32)
+        self.lj = np.ascontiguousarray(system.lj_table, np.float64)
+        self.excl = np.ascontiguousarray(system.exclusions, np.int32)
+        self.chk = np.ascontiguousarray(system.exclusion_check, np.int32)
+        s = _System()
+        s.n_atoms = self.pos.shape[0]
+        s.pos = self.pos.ctypes.data
+        s.q = self.q.ctypes.data
+        s.type = self.type.ctypes.data
+        s.mol = self.mol.ctypes.data
+        s.n_types = self.lj.shape[0]
+        s.lj = self.lj.ctypes.data
+        s.n_excl = self.excl.shape[0]
+        s.excl = self.excl.ctypes.data if self.excl.size else None
+        s.excl_check = self.chk.ctypes.data if self.chk.size else None
+        for k, v in enumerate(np.asarray(system.box, np.float64).ravel()):
+            s.box[k] = v
+        s.csf = system.csf
+        s.cell_size = system.cell_size
+        self.s = s
+
+
+def _cut_params(spec) -> _Cut:
+    p = _Cut()
+    terms = spec["terms"]
+    p.n_terms = len(terms)
+    for k, (sw, pot, on, rc, alpha) in enumerate(terms):
+        p.sw[k] = SW[sw] if isinstance(sw, str) else sw
+        p.pot[k] = POT[pot] if isinstance(pot, str) else pot
+        p.switchon[k] = on
+        p.sw_cutoff[k] = rc
+        p.alpha[k] = alpha
+    p.algo_cutoff = spec.get("algo_cutoff", max(t[3] for t in terms))
+    return p
+
+
+def _pme_params(spec) -> _Pme:
+    p = _Pme()
+    p.real = int(spec.get("real", 0))
+    p.reciprocal = int(spec.get("reciprocal", 1))
+    p.correction = int(spec.get("correction", 1))
+    for k, g in enumerate(spec["grid"]):
+        p.grid[k] = int(g)
+    p.order = int(spec.get("order", 4))
+    p.cutoff = float(spec["cutoff"])
+    p.accuracy = float(spec.get("accuracy", 1e-6))
+    p.alpha = float(spec.get("alpha", -1.0))
+    return p
+
+
+def _result_dict(r: _Result, forces):
+    return {
+        "forces": forces, "lennard_jones": r.lennard_jones, "coulomb": r.coulomb,
+        "virial": np.array(list(r.virial)), "n_pairs": int(r.n_pairs), "alpha": r.alpha,
+        "e_real": r.e_real, "e_recip": r.e_recip, "e_intra": r.e_intra,
+        "e_self": r.e_self, "e_charged": r.e_charged, "out_of_grid": r.out_of_grid,
+    }
+
+
+def evaluate(system, specs, positions=None, want_pairs=False, pair_cap=None):
+    """Evaluates the force specs in order into one force block (like
+    ForceGroup::evaluateSystemForces).  Returns a dict."""
+    keep = _Keep(system, positions)
+    n = keep.pos.shape[0]
+    forces = np.zeros((n, 3), np.float64)
+    r = _Result()
+    pairs = None
+    L = lib()
+    for spec in specs:
+        if spec["kind"] == "cut":
+            p = _cut_params(spec)
+            if want_pairs:
+                cap = pair_cap or n * 1200
+                pairs = np.zeros((cap, 2), np.int32)
+                L.pmo_cutoff_force(C.byref(keep.s), C.byref(p), forces.ctypes.data_as(C.c_void_p),
+                                   C.byref(r), pairs.ctypes.data_as(C.c_void_p), C.c_longlong(cap))
+                if r.n_pairs > cap:
+                    raise RuntimeError("pair capacity too small")
+                pairs = pairs[: r.n_pairs]
+            else:
+                L.pmo_cutoff_force(C.byref(keep.s), C.byref(p), forces.ctypes.data_as(C.c_void_p),
+                                   C.byref(r), None, C.c_longlong(0))
+        elif spec["kind"] == "pme":
+            p = _pme_params(spec)
+            rc = L.pmo_pme_force(C.byref(keep.s), C.byref(p), forces.ctypes.data_as(C.c_void_p), C.byref(r))
+            if rc != 0:
+                raise RuntimeError("PME oracle needs an orthogonal box")
+        elif spec["kind"] == "full":
+            p = _cut_params(spec)
+            L.pmo_simple_full_force(C.byref(keep.s), C.byref(p), forces.ctypes.data_as(C.c_void_p), C.byref(r))
+        else:
+            raise ValueError(spec["kind"])
+    out = _result_dict(r, forces)
+    if want_pairs:
+        out["pairs"] = pairs
+    return out
+
+
+def cell_assign(system, positions=None):
+    keep = _Keep(system, positions)
+    cells = np.zeros((keep.pos.shape[0], 3), np.int32)
+    dims = np.zeros(3, np.int32)
+    oog = lib().pmo_cell_assign(C.byref(keep.s), cells.ctypes.data_as(C.c_void_p),
+                                dims.ctypes.data_as(C.c_void_p))
+    return cells, tuple(int(d) for d in dims), oog
+
+
+def fft3d(data: np.ndarray, sign: int) -> np.ndarray:
+    a = np.ascontiguousarray(data, np.complex128).copy()
+    nx, ny, nz = a.shape
+    lib().pmo_fft3d(a.ctypes.data_as(C.c_void_p), nx, ny, nz, sign)
+    return a
+
+
+def poly5(x: float) -> float:
+    return lib().pmo_poly5(float(x))
+
+
+# --------------------------------------------------------------- reference
+def reference_available(fast: bool = False) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "pmref_fast" if fast else "pmref"))
+
+
+def build_reference(ref_root: str = "/root/reference") -> bool:
+    """Compile the reference's own sources (only where they are present)."""
+    if not os.path.isdir(os.path.join(ref_root, "framework")):
+        return reference_available()
+    subprocess.check_call(["make", "-C", os.path.join(HERE, "ref"), f"REF={ref_root}",
+                           "-j", str(os.cpu_count() or 4), "-s"])
+    return True
+
+
+def _spec_args(spec):
+    if spec["kind"] in ("cut", "full"):
+        args = [spec["kind"], str(len(spec["terms"]))]
+        for sw, pot, on, rc, alpha in spec["terms"]:
+            args += [str(SW[sw] if isinstance(sw, str) else sw),
+                     str(POT[pot] if isinstance(pot, str) else pot),
+                     repr(float(on)), repr(float(rc)), repr(float(alpha))]
+        if spec["kind"] == "cut":
+            args.append(repr(float(spec.get("algo_cutoff", max(t[3] for t in spec["terms"])))))
+        return args
+    g = spec["grid"]
+    return ["pme", str(int(spec.get("real", 0))), str(int(spec.get("reciprocal", 1))),
+            str(int(spec.get("correction", 1))), str(g[0]), str(g[1]), str(g[2]),
+            str(int(spec.get("order", 4))), repr(float(spec["cutoff"])),
+            repr(float(spec.get("accuracy", 1e-6))), repr(float(spec.get("alpha", -1.0)))]
+
+
+def run_reference(system, specs, repeat: int = 1, fast: bool = False, timeout=None):
+    """Runs the compiled reference; returns the same dict as :func:`evaluate`
+    plus ``cells``/``dims`` and ``seconds_per_eval`` (when repeat > 1)."""
+    exe = os.path.join(REF_DIR, "pmref_fast" if fast else "pmref")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    with tempfile.TemporaryDirectory() as td:
+        sp = os.path.join(td, "sys.bin")
+        op = os.path.join(td, "out.bin")
+        system.save(sp)
+        args = [exe, sp, op, str(int(repeat))]
+        for spec in specs:
+            args += _spec_args(spec)
+        subprocess.run(args, check=True, timeout=timeout, stdout=subprocess.DEVNULL)
+        raw = open(op, "rb").read()
+    n = system.n_atoms
+    hdr = np.frombuffer(raw[: 13 * 8], np.float64)
+    off = 13 * 8
+    forces = np.frombuffer(raw[off: off + 24 * n], np.float64).reshape(n, 3).copy()
+    off += 24 * n
+    dims = tuple(int(x) for x in np.frombuffer(raw[off: off + 12], np.int32))
+    off += 12
+    cells = np.frombuffer(raw[off: off + 12 * n], np.int32).reshape(n, 3).copy()
+    return {
+        "forces": forces, "lennard_jones": float(hdr[0]), "coulomb": float(hdr[1]),
+        "virial": hdr[2:11].copy(), "seconds_per_eval": float(hdr[11]),
+        "cells": cells, "dims": dims,
+    }

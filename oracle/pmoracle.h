@@ -1,0 +1,112 @@
+/*
+ * pmoracle.h -- CPU restatement of ProtoMol's nonbonded force path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the parity checker for the GPU kernels
+ * in protomol_b200/csrc; nothing in the product links or calls it.  Only the
+ * tests, the smoke check and the benchmark's CPU-baseline leg may load it.
+ *
+ * Every function restates a reference function and cites it (paths relative
+ * to the ProtoMol source tree).  The arithmetic is plain IEEE double in the
+ * reference's operation order, compiled with -ffp-contract=off, so that on the
+ * same inputs it reproduces the compiled reference bit for bit (checked by
+ * tests/test_oracle_vs_reference.py against oracle/_ref).
+ */
+#ifndef PMORACLE_H
+#define PMORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ExclusionClass (topology/ExclusionTable.h) */
+enum { PMO_EXCL_NONE = 0, PMO_EXCL_MODIFIED = 1, PMO_EXCL_FULL = 2 };
+
+/* pair potentials (forces/LennardJonesForce.h, CoulombForce.h,
+ * CoulombEwaldRealForce.h) */
+enum { PMO_POT_NONE = 0, PMO_POT_LJ = 1, PMO_POT_COULOMB = 2, PMO_POT_EWALD_REAL = 3 };
+
+/* switching functions (topology/C1SwitchingFunction.h, C2..., Cutoff...,
+ * Shift...); UNIVERSAL = no
+ * switching and no cutoff test */
+enum { PMO_SW_UNIVERSAL = 0, PMO_SW_CUTOFF = 1, PMO_SW_C1 = 2, PMO_SW_C2 = 3, PMO_SW_SHIFT = 4 };
+
+typedef struct {
+    int n_atoms;
+    const double* pos;          /* 3N, x y z */
+    const double* q;            /* N scaled charges */
+    const int* type;            /* N */
+    const int* mol;             /* N */
+    int n_types;
+    const double* lj;           /* T*T*4: A, B, A14, B14 */
+    int n_excl;
+    const int* excl;            /* 3E: a1, a2, table class */
+    const int* excl_check;      /* E: class returned by check(); NULL = same */
+    double box[12];             /* e1, e2, e3, origin */
+    double csf;                 /* coulombScalingFactor */
+    double cell_size;           /* CubicCellManager cellsize */
+} pmo_system;
+
+/* One NonbondedCutoffSystemForce: OneAtomPair (n_terms = 1) or
+ * OneAtomPairTwo (n_terms = 2). */
+typedef struct {
+    int n_terms;
+    int pot[2];
+    int sw[2];
+    double switchon[2];         /* C2 only */
+    double sw_cutoff[2];
+    double alpha[2];            /* EwaldReal only */
+    double algo_cutoff;         /* NonbondedCutoff -cutoff (cell deltas) */
+} pmo_cutoff_params;
+
+/* NonbondedPMEwaldSystemForce<Periodic, Cubic, real, reciprocal, correction,
+ * BSpline, Cutoff> */
+typedef struct {
+    int real, reciprocal, correction;
+    int grid[3];
+    int order;
+    double cutoff;
+    double accuracy;
+    double alpha;               /* <= 0: bisection default */
+} pmo_pme_params;
+
+typedef struct {
+    double lennard_jones;
+    double coulomb;
+    double virial[9];
+    long long n_pairs;          /* interactions computed (pair set size) */
+    double alpha;               /* PME: splitting parameter used */
+    double e_real, e_recip, e_intra, e_self, e_charged;   /* PME parts */
+    int out_of_grid;            /* atoms whose cell fell outside the grid */
+} pmo_result;
+
+/* Cell of every atom as buildCellLists computes it, and the grid dims.
+ * cells: 3N ints. Returns 0. */
+int pmo_cell_assign(const pmo_system* s, int* cells, int* dims);
+
+/* Cutoff force: forces += (3N), result accumulates energies/virial.
+ * pairs (optional, capacity cap pairs) receives the (min, max) index pair of
+ * every interaction evaluated, in enumeration order. */
+int pmo_cutoff_force(const pmo_system* s, const pmo_cutoff_params* p,
+                     double* forces, pmo_result* r,
+                     int* pairs, long long cap);
+
+/* PME force: forces += (3N). */
+int pmo_pme_force(const pmo_system* s, const pmo_pme_params* p,
+                  double* forces, pmo_result* r);
+
+/* All-pairs force with vacuum boundary conditions
+ * (NonbondedSimpleFullSystemForce<OneAtomPair[Two]<Vacuum, ...>>). */
+int pmo_simple_full_force(const pmo_system* s, const pmo_cutoff_params* p,
+                          double* forces, pmo_result* r);
+
+/* The poly5 erfc approximation (base/mathutilities.cpp:29-40). */
+double pmo_poly5(double ar);
+
+/* Unnormalised 3-D complex FFT on an nx*ny*nz row-major array of
+ * (re, im) pairs; sign -1 or +1.  Exposed for tests. */
+int pmo_fft3d(double* data, int nx, int ny, int nz, int sign);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,3 @@
+/* base/fft.c calls min()/max() without declaring them (oracle build only). */
+int min(int a, int b) { return a < b ? a : b; }
+int max(int a, int b) { return a > b ? a : b; }

@@ -1,0 +1,100 @@
+"""ctypes binding of libpmgpu.so (include/pmgpu.h).
+
+Loading fails loudly: there is no CPU fallback for any force.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpmgpu.so")
+
+PMGPU_OK = 0
+ERRORS = {1: "PMGPU_ERR_ARG", 2: "PMGPU_ERR_CUDA", 3: "PMGPU_ERR_OVERFLOW", 4: "PMGPU_ERR_STATE",
+          5: "PMGPU_ERR_UNSUPPORTED", 6: "PMGPU_ERR_NOMEM", 7: "PMGPU_ERR_CAPACITY"}
+
+POT = {"LennardJones": 1, "Coulomb": 2, "CoulombEwaldReal": 3}
+SW = {"Universal": 0, "Cutoff": 1, "C1": 2, "C2": 3, "Shift": 4}
+PRECISION = {"mixed": 0, "fp64": 1}
+FLAG_VIRIAL = 1
+
+# every symbol include/pmgpu.h declares
+EXPORTS = [
+    "pmgpu_system_create", "pmgpu_system_destroy", "pmgpu_set_topology", "pmgpu_set_box",
+    "pmgpu_cutoff_create", "pmgpu_pme_create", "pmgpu_force_destroy", "pmgpu_pme_alpha",
+    "pmgpu_evaluate", "pmgpu_evaluate_device", "pmgpu_synchronize", "pmgpu_stream",
+    "pmgpu_launch_count", "pmgpu_last_error", "pmgpu_get_cells", "pmgpu_get_pairs",
+]
+
+
+class CutoffParams(C.Structure):
+    _fields_ = [
+        ("n_terms", C.c_int), ("pot", C.c_int * 2), ("sw", C.c_int * 2),
+        ("switchon", C.c_double * 2), ("cutoff", C.c_double * 2), ("alpha", C.c_double * 2),
+        ("algorithm_cutoff", C.c_double), ("precision", C.c_int),
+    ]
+
+
+class PmeParams(C.Structure):
+    _fields_ = [
+        ("real", C.c_int), ("reciprocal", C.c_int), ("correction", C.c_int),
+        ("grid", C.c_int * 3), ("order", C.c_int), ("cutoff", C.c_double),
+        ("accuracy", C.c_double), ("alpha", C.c_double), ("precision", C.c_int),
+    ]
+
+
+class Energies(C.Structure):
+    _fields_ = [("lennard_jones", C.c_double), ("coulomb", C.c_double), ("virial", C.c_double * 9)]
+
+
+class PmgpuError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def load():
+    """Loads the in-tree libpmgpu.so; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m protomol_b200.build` "
+                          "(there is no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+    lib.pmgpu_system_create.argtypes = [C.c_int, C.POINTER(vp)]
+    lib.pmgpu_system_destroy.argtypes = [vp]
+    lib.pmgpu_set_topology.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, C.c_double]
+    lib.pmgpu_set_box.argtypes = [vp, dp, dp, dp, dp, C.c_double]
+    lib.pmgpu_cutoff_create.argtypes = [vp, C.POINTER(CutoffParams), C.POINTER(vp)]
+    lib.pmgpu_pme_create.argtypes = [vp, C.POINTER(PmeParams), C.POINTER(vp)]
+    lib.pmgpu_force_destroy.argtypes = [vp]
+    lib.pmgpu_pme_alpha.argtypes = [vp, dp]
+    lib.pmgpu_evaluate.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp, C.POINTER(Energies), C.c_uint]
+    lib.pmgpu_evaluate_device.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp, vp, C.c_uint]
+    lib.pmgpu_synchronize.argtypes = [vp]
+    lib.pmgpu_stream.argtypes = [vp]
+    lib.pmgpu_stream.restype = vp
+    lib.pmgpu_launch_count.argtypes = [vp]
+    lib.pmgpu_launch_count.restype = C.c_longlong
+    lib.pmgpu_last_error.argtypes = [vp, C.c_char_p, C.c_int]
+    lib.pmgpu_get_cells.argtypes = [vp, vp, vp]
+    lib.pmgpu_get_pairs.argtypes = [vp, vp, vp, C.POINTER(C.c_longlong), vp, C.c_longlong]
+    _lib = lib
+    return lib
+
+
+def last_error(sys_handle) -> str:
+    buf = C.create_string_buffer(1024)
+    load().pmgpu_last_error(sys_handle, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(code, sys_handle=None):
+    if code != PMGPU_OK:
+        raise PmgpuError(code, last_error(sys_handle) if sys_handle else "")

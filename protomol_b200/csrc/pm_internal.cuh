@@ -1,0 +1,146 @@
+// pm_internal.cuh -- shared device structures and helpers of libpmgpu.
+//
+// Layout in HBM (per system):
+//   positions      FP64 AoS, 3N (caller's order)            24 B/atom
+//   spos           float4 per cell-sorted atom: x, y, z relative to the
+//                  atom's cell corner, scaled charge        16 B/atom
+//   smeta          int4 per cell-sorted atom: original index, LJ type,
+//                  molecule, 0                              16 B/atom
+//   facc           int64 fixed-point forces, 3 per sorted atom (scale 2^32
+//                  for mixed precision, 2^40 for FP64)      24 B/atom
+//   cell_start     CSR offsets of the cell-sorted order, ncell + 1 ints
+//   PME grid       int64 fixed-point charge grid (spread), complex
+//                  half-spectrum K_x*K_y*(K_z/2+1) (FFT), real grid (gather)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pm {
+
+constexpr int kMaxDeltas = 1024;
+constexpr int kExclWindow = 32;        // exclusion bitmask window (index delta 1..32)
+constexpr double kScaleMixed = 4294967296.0;        // 2^32
+constexpr double kScaleFp64 = 1099511627776.0;      // 2^40
+constexpr double kFixedLimit = 4.0e18;               // |value * scale| bound before int64 overflow
+
+// status bits written by kernels
+constexpr int kStatusOverflow = 1;
+constexpr int kStatusOutOfGrid = 2;
+
+// FP64 constants of PeriodicBoundaryConditions::set
+// (topology/PeriodicBoundaryConditions.cpp:40-77), orthogonal box.
+struct Pbc {
+    double e1x, e2y, e3z;       // box edge lengths (e1.x, e2.y, e3.z)
+    double e1rx, e2ry, e3rz;    // inverse basis components used by rint()
+    double hx, hy, hz;          // myH = max - min
+    double h2x, h2y, h2z;       // myH2 = myH * 0.5
+    double d;                   // myD = min(Li/2)^2
+    double ox, oy, oz;          // origin
+    double dx, dy, dz;          // origin - min (buildCellLists delta)
+};
+
+// Cell grid of CubicCellManager::initialize + ArrayCellListStructure
+// (topology/CubicCellManager.cpp:25-42, ArrayCellListStructure.cpp:24-93).
+struct CellGrid {
+    int nx, ny, nz, ncell;
+    double csx, csy, csz;       // myRealCellSize
+    double rcsx, rcsy, rcsz;    // myRealRCellSize
+};
+
+// ---- exact FP64 arithmetic in the reference's operation order ------------
+// (no FMA contraction: every product and sum rounded on its own)
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dnorm2(double x, double y, double z)
+{
+    return dadd(dadd(dmul(x, x), dmul(y, y)), dmul(z, z));
+}
+
+// PeriodicBoundaryConditions::minimalDifference(c1, c2, distSquared)
+// (topology/PeriodicBoundaryConditions.h:76-118), orthogonal branch.
+__device__ __forceinline__ double pbc_min_diff(const Pbc& b, double x1, double y1, double z1,
+                                               double x2, double y2, double z2,
+                                               double& dx, double& dy, double& dz)
+{
+    dx = dsub(x2, x1); dy = dsub(y2, y1); dz = dsub(z2, z1);
+    double d2 = dnorm2(dx, dy, dz);
+    if (d2 > b.d) {
+        if (dx < -b.h2x) dx = dadd(dx, b.hx); else if (dx > b.h2x) dx = dsub(dx, b.hx);
+        if (dy < -b.h2y) dy = dadd(dy, b.hy); else if (dy > b.h2y) dy = dsub(dy, b.hy);
+        if (dz < -b.h2z) dz = dadd(dz, b.hz); else if (dz > b.h2z) dz = dsub(dz, b.hz);
+        d2 = dnorm2(dx, dy, dz);
+        if (d2 > b.d) {
+            dx = dsub(dx, dmul(b.e1x, rint(dmul(b.e1rx, dx))));
+            dy = dsub(dy, dmul(b.e2y, rint(dmul(b.e2ry, dy))));
+            dz = dsub(dz, dmul(b.e3z, rint(dmul(b.e3rz, dz))));
+            d2 = dnorm2(dx, dy, dz);
+        }
+    }
+    return d2;
+}
+
+// PeriodicBoundaryConditions::minimalPosition (PeriodicBoundaryConditions.h:120-150)
+__device__ __forceinline__ void pbc_min_pos(const Pbc& b, double x, double y, double z,
+                                            double& rx, double& ry, double& rz)
+{
+    double dx = dsub(x, b.ox), dy = dsub(y, b.oy), dz = dsub(z, b.oz);
+    if (!(dnorm2(dx, dy, dz) <= b.d)) {
+        if (dx < -b.h2x) dx = dadd(dx, b.hx); else if (dx > b.h2x) dx = dsub(dx, b.hx);
+        if (dy < -b.h2y) dy = dadd(dy, b.hy); else if (dy > b.h2y) dy = dsub(dy, b.hy);
+        if (dz < -b.h2z) dz = dadd(dz, b.hz); else if (dz > b.h2z) dz = dsub(dz, b.hz);
+        if (!(dnorm2(dx, dy, dz) <= b.d)) {
+            dx = dsub(dx, dmul(b.e1x, rint(dmul(b.e1rx, dx))));
+            dy = dsub(dy, dmul(b.e2y, rint(dmul(b.e2ry, dy))));
+            dz = dsub(dz, dmul(b.e3z, rint(dmul(b.e3rz, dz))));
+        }
+    }
+    rx = dx; ry = dy; rz = dz;
+}
+
+// ---- fixed-point force accumulation ---------------------------------------
+// Each contribution is rounded to an int64 multiple of 1/scale and added with
+// an integer atomic, so the total is independent of summation order.
+__device__ __forceinline__ void fixed_add(unsigned long long* slot, double v, double scale, int* status)
+{
+    double s = v * scale;
+    if (!(fabs(s) < kFixedLimit)) {   // also catches NaN
+        atomicOr(status, kStatusOverflow);
+        return;
+    }
+    long long q = __double2ll_rn(s);
+    if (q != 0) atomicAdd(slot, (unsigned long long)q);
+}
+
+__device__ __forceinline__ void fixed_add3(unsigned long long* base, double x, double y, double z,
+                                           double scale, int* status)
+{
+    fixed_add(base + 0, x, scale, status);
+    fixed_add(base + 1, y, scale, status);
+    fixed_add(base + 2, z, scale, status);
+}
+
+// ---- energy / virial partial records ---------------------------------------
+// 11 doubles: LENNARDJONES, COULOMB, VIRIALXX..VIRIALZZ.
+constexpr int kERec = 11;
+
+template <int NW>
+__device__ __forceinline__ void block_reduce_store(double (&v)[kERec], double* out_rec)
+{
+    // warp reduce
+    for (int k = 0; k < kERec; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    __shared__ double red[NW][kERec];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < kERec; ++k) red[w][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < kERec) {
+        double s = 0.0;
+        for (int q = 0; q < NW; ++q) s += red[q][threadIdx.x];
+        out_rec[threadIdx.x] = s;
+    }
+}
+
+}  // namespace pm

@@ -1,0 +1,564 @@
+// pm_pair.cu -- K2 (mixed precision) and K9 (FP64) cell-pair force kernels.
+//
+// Enumeration (both kernels): one warp per work item (cell A, neighbour delta
+// k), k = 0 being A with itself.  The delta list is the reference's
+// (CellListEnumerator<Periodic, Cubic>::initialize,
+// topology/CellListEnumerator_periodicBoundaries.h:37-108), and a pair of
+// cells (A, B = A + delta mod grid) is visited only when B >= A in linear
+// order, exactly as the enumerator's next() (:157-179) does.  Inside the same
+// cell, pairs i < j (slot order = ascending original index).  So every
+// unordered atom pair is tested exactly once, like NonbondedCutoffForce::
+// doEvaluate (forces/NonbondedCutoffForce.h:85-109).
+//
+// Inside an item, lane l holds i-atom l of A in registers; the j-atoms of B
+// are staged in shared memory (float4 position + charge, int4 meta) and
+// rotated: at step t lane l pairs with j = (l + t) mod 32, so every lane
+// touches a different j and the j-force accumulator of that j in shared
+// memory without atomics.  i-forces stay in registers.  At the end of a
+// chunk each atom's partial force is rounded once to int64 fixed point and
+// added with an integer atomic -- the total force is independent of order.
+//
+// Per pair (OneAtomPair::doOneAtomPair / OneAtomPairTwo::doOneAtomPair,
+// forces/OneAtomPair.h:127-188, forces/OneAtomPairTwo.h:131-199):
+//   cutoff test r^2 > rc^2 -> skip (rc = largest switching cutoff);
+//   exclusion check only for atoms of the same molecule (FULL -> skip,
+//   MODIFIED -> A14/B14 and coulombScalingFactor);
+//   potentials, switching F = F S - E dS, E = E S when any switch modifies;
+//   f_i -= d F, f_j += d F (d = x_j - x_i), energies into the LJ / Coulomb
+//   slots, virial addVirial(d F, d) (base/ScalarStructure.cpp:41-62).
+//
+// Mixed precision: distances from FP32 cell-relative coordinates plus a
+// per-delta FP32 cell offset; a pair whose FP32 r^2 lies within a relative
+// guard band of a cutoff is re-decided in FP64 with the reference's own
+// minimalDifference arithmetic on the original positions, so the pair set is
+// the reference's bit for bit.  Potentials and switching in FP32; energies
+// and virial summed in FP64 per lane.
+//
+// FP64 kernel: every pair through the reference's minimalDifference on the
+// FP64 positions, reference operation order throughout.
+#include "pm_kernels.h"
+#include "../../include/pmgpu.h"
+
+namespace pm {
+
+// ------------------------------------------------------------------ combos
+struct Combo { int n, p0, s0, p1, s1; };
+#define LJ PMGPU_POT_LENNARD_JONES
+#define CO PMGPU_POT_COULOMB
+#define EW PMGPU_POT_EWALD_REAL
+#define NP PMGPU_POT_NONE
+#define SCUT PMGPU_SW_CUTOFF
+#define SC1 PMGPU_SW_C1
+#define SC2 PMGPU_SW_C2
+#define SSH PMGPU_SW_SHIFT
+#define SUN PMGPU_SW_UNIVERSAL
+// The registered periodic OneAtomPair[Two] templates
+// (factories/registerForceExemplarsCutoff.cpp:36-131) plus the fused
+// LennardJones Coulomb -switchingFunction C2 -switchingFunction C2.
+static const Combo kCombos[] = {
+    {1, CO, SC1, NP, SUN}, {1, CO, SC2, NP, SUN}, {1, CO, SCUT, NP, SUN}, {1, CO, SSH, NP, SUN},
+    {1, EW, SCUT, NP, SUN}, {1, LJ, SC1, NP, SUN}, {1, LJ, SC2, NP, SUN}, {1, LJ, SCUT, NP, SUN},
+    {1, LJ, SSH, NP, SUN},
+    {2, LJ, SC1, EW, SCUT}, {2, LJ, SC1, CO, SSH}, {2, LJ, SC2, CO, SC1}, {2, LJ, SC2, EW, SCUT},
+    {2, LJ, SC2, CO, SCUT}, {2, LJ, SC2, CO, SSH}, {2, LJ, SCUT, EW, SCUT}, {2, LJ, SC2, CO, SC2},
+};
+constexpr int kNumCombos = sizeof(kCombos) / sizeof(kCombos[0]);
+
+int pair_combo_id(int n_terms, const int* pot, const int* sw)
+{
+    for (int k = 0; k < kNumCombos; ++k) {
+        const Combo& c = kCombos[k];
+        if (c.n != n_terms) continue;
+        if (c.p0 == pot[0] && c.s0 == sw[0] && (n_terms == 1 || (c.p1 == pot[1] && c.s1 == sw[1])))
+            return k;
+    }
+    return -1;
+}
+
+__host__ __device__ constexpr bool sw_modifies(int s) { return s == SC1 || s == SC2 || s == SSH; }
+__host__ __device__ constexpr bool pot_r2(int p) { return p == LJ || p == CO; }
+
+// ---------------------------------------------------------------- shared
+struct ItemGeom {
+    int a, b;           // cell indices
+    int same;
+    float ox, oy, oz;   // FP32 offset of cell B's image relative to A
+    int valid;
+};
+
+__device__ __forceinline__ ItemGeom decode_item(const PairArgs& p, int item)
+{
+    ItemGeom g;
+    const CellGrid& cg = p.grid;
+    int nd1 = p.nd + 1;
+    g.a = item / nd1;
+    int k = item - g.a * nd1;
+    g.valid = 0;
+    if (k == 0) {
+        g.b = g.a; g.same = 1; g.ox = g.oy = g.oz = 0.f;
+    } else {
+        int4 d = p.deltas[k - 1];
+        int ax = g.a / (cg.ny * cg.nz), ay = (g.a / cg.nz) % cg.ny, az = g.a % cg.nz;
+        int bx = ((ax + d.x) % cg.nx + cg.nx) % cg.nx;
+        int by = ((ay + d.y) % cg.ny + cg.ny) % cg.ny;
+        int bz = ((az + d.z) % cg.nz + cg.nz) % cg.nz;
+        g.b = (bx * cg.ny + by) * cg.nz + bz;
+        g.same = 0;
+        float4 o = p.doff[k - 1];
+        g.ox = o.x; g.oy = o.y; g.oz = o.z;
+        if (g.b < g.a) return g;
+    }
+    g.valid = 1;
+    return g;
+}
+
+// ExclusionTable::check (topology/ExclusionTable.h:130-146) for a pair of the
+// same molecule; returns the class.
+__device__ __forceinline__ int excl_class(const PairArgs& p, int oi, int oj)
+{
+    int lo = min(oi, oj), hi = max(oi, oj);
+    int dl = hi - lo;
+    if (dl <= 0) return PMGPU_EXCL_NONE;
+    if (dl <= kExclWindow) {
+        uint32_t bit = 1u << (dl - 1);
+        if (__ldg(p.xfull + lo) & bit) return PMGPU_EXCL_FULL;
+        if (__ldg(p.xmod + lo) & bit) return PMGPU_EXCL_MODIFIED;
+        return PMGPU_EXCL_NONE;
+    }
+    int b = __ldg(p.xrow + lo), e = __ldg(p.xrow + lo + 1);
+    while (b < e) {   // binary search on partner index
+        int m = (b + e) >> 1;
+        int2 v = p.xent[m];
+        if (v.x == hi) return v.y;
+        if (v.x < hi) b = m + 1; else e = m;
+    }
+    return PMGPU_EXCL_NONE;
+}
+
+// ---------------------------------------------------------------- FP32 math
+__device__ __forceinline__ float poly5f(float ar)
+{
+    // poly5 (base/mathutilities.cpp:29-40), Abramowitz & Stegun 7.1.26
+    const float E1 = 0.254829592f, E2 = -0.284496736f, E3 = 1.421413741f,
+                E4 = -1.453152027f, E5 = 1.061405429f, PP = 0.3275911f;
+    float t = __frcp_rn(fmaf(PP, ar, 1.0f));
+    return t * (E1 + t * (E2 + t * (E3 + t * (E4 + t * E5))));
+}
+
+template <int POT>
+__device__ __forceinline__ void pot_f32(const PairArgs& p, const TermF& t, float r2, float rd2, float rinv,
+                                        float qi, float qj, int ti, int tj, int excl, float& e, float& f)
+{
+    if (POT == LJ) {
+        float4 par = __ldg(p.ljf + (size_t)ti * p.n_types + tj);
+        float A = excl == PMGPU_EXCL_MODIFIED ? par.z : par.x;
+        float B = excl == PMGPU_EXCL_MODIFIED ? par.w : par.y;
+        float r6 = rd2 * rd2 * rd2;
+        float r12 = r6 * r6;
+        float r6B = B * r6;
+        float r12A = A * r12;
+        e = r12A - r6B;
+        f = (12.0f * r12A - 6.0f * r6B) * rd2;
+    } else if (POT == CO) {
+        e = qi * qj * rinv;
+        if (excl == PMGPU_EXCL_MODIFIED) e *= p.csf;
+        f = e * rd2;
+    } else if (POT == EW) {
+        float qq = qi * qj;
+        if (p.csfd != 1.0 && excl == PMGPU_EXCL_MODIFIED) qq *= p.csf;
+        float r = r2 * rinv;
+        float ar = t.alpha * r;
+        float ex = qq * expf(-ar * ar);
+        e = poly5f(ar) * ex * rinv;
+        f = (e + t.two_alpha_pi * ex) * rinv * rinv;
+    } else {
+        e = 0.f; f = 0.f;
+    }
+}
+
+template <int SW>
+__device__ __forceinline__ void sw_f32(const TermF& t, float r2, float rinv, bool inside, float& v, float& d)
+{
+    if (SW == SC2) {
+        d = 0.f;
+        if (r2 > t.cut2) v = 0.f;
+        else if (r2 >= t.on2) {
+            float c2 = t.cut2 - r2;
+            float c4 = c2 * (t.s2 + 2.0f * r2);
+            v = t.s1 * (c2 * c4);
+            d = t.s3 * (c2 * c2 - c4);
+        } else v = 1.f;
+    } else if (SW == SC1) {
+        if (r2 > t.cut2) { v = 0.f; d = 0.f; return; }
+        float dist = r2 * rinv;
+        v = 1.0f - dist * (t.c1_15_1 - r2 * t.c1_05_3);
+        d = -t.c1_15_1 * rinv + dist * t.c1_15_3;
+    } else if (SW == SSH) {
+        if (r2 > t.cut2) { v = 0.f; d = 0.f; return; }
+        float x = 1.0f - r2 * t.sh_a;
+        v = x * x;
+        d = t.sh_b * x;
+    } else if (SW == SCUT) {
+        d = 0.f;
+        v = inside ? 1.f : 0.f;
+    } else {
+        v = 1.f; d = 0.f;
+    }
+}
+
+// exact FP64 squared distance of two atoms (reference minimalDifference)
+__device__ __forceinline__ double exact_d2(const PairArgs& p, int oi, int oj)
+{
+    const double* pi = p.pos + 3 * (size_t)oi;
+    const double* pj = p.pos + 3 * (size_t)oj;
+    double dx, dy, dz;
+    return pbc_min_diff(p.pbc, pi[0], pi[1], pi[2], pj[0], pj[1], pj[2], dx, dy, dz);
+}
+
+template <int NT, int P0, int S0, int P1, int S1>
+__global__ void __launch_bounds__(128) k_pair_mixed(PairArgs p)
+{
+    constexpr bool kMod = sw_modifies(S0) || (NT > 1 && sw_modifies(S1));
+    constexpr bool kUse0 = S0 != SUN;
+    __shared__ float4 sjp[4][32];
+    __shared__ int4 sjm[4][32];
+    __shared__ float4 sjf[4][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int warps_total = gridDim.x * 4;
+    const int n_items = p.grid.ncell * (p.nd + 1);
+    const float g_lo = 1.0f - p.guard, g_hi = 1.0f + p.guard;
+    const float t0c2 = p.tf[0].cut2, t1c2 = NT > 1 ? p.tf[1].cut2 : 0.f;
+    double acc[kERec];
+    for (int k = 0; k < kERec; ++k) acc[k] = 0.0;
+
+    for (int item = blockIdx.x * 4 + w; item < n_items; item += warps_total) {
+        ItemGeom g = decode_item(p, item);
+        if (!g.valid) continue;
+        int sa = p.start[g.a], ea = p.start[g.a + 1];
+        int sb = p.start[g.b], eb = p.start[g.b + 1];
+        if (sa == ea || sb == eb) continue;
+        for (int ia = sa; ia < ea; ia += 32) {
+            int i = ia + lane;
+            bool vi = i < ea;
+            float4 pi = vi ? p.spos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            int4 mi = vi ? p.smeta[i] : make_int4(-1, 0, -2, 0);
+            float fix = 0.f, fiy = 0.f, fiz = 0.f;
+            for (int jb = g.same ? ia : sb; jb < eb; jb += 32) {
+                int j = jb + lane;
+                bool vj = j < eb;
+                sjp[w][lane] = vj ? p.spos[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                sjm[w][lane] = vj ? p.smeta[j] : make_int4(-1, 0, -3, 0);
+                sjf[w][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+                __syncwarp();
+                int nj = min(32, eb - jb);
+                bool diag = g.same && jb == ia;
+                float el = 0.f, ec = 0.f, vxx = 0.f, vxy = 0.f, vxz = 0.f, vyy = 0.f, vyz = 0.f, vzz = 0.f;
+                for (int t = 0; t < 32; ++t) {
+                    int jl = (lane + t) & 31;
+                    bool ok = vi && jl < nj && (!diag || jb + jl > i);
+                    if (!ok) continue;
+                    float4 pj = sjp[w][jl];
+                    float dx = (pj.x + g.ox) - pi.x;
+                    float dy = (pj.y + g.oy) - pi.y;
+                    float dz = (pj.z + g.oz) - pi.z;
+                    if (p.wrap) {
+                        dx -= p.lx * rintf(dx * p.ilx);
+                        dy -= p.ly * rintf(dy * p.ily);
+                        dz -= p.lz * rintf(dz * p.ilz);
+                    }
+                    float r2 = dx * dx + dy * dy + dz * dz;
+                    // pair test (with exact FP64 re-decision in the guard band)
+                    bool near = (r2 >= p.cut2f * g_lo && r2 <= p.cut2f * g_hi);
+                    if (S0 == SCUT && t0c2 != p.cut2f) near |= (r2 >= t0c2 * g_lo && r2 <= t0c2 * g_hi);
+                    if (NT > 1 && S1 == SCUT && t1c2 != p.cut2f) near |= (r2 >= t1c2 * g_lo && r2 <= t1c2 * g_hi);
+                    int4 mj = sjm[w][jl];
+                    bool in_pair, in0, in1;
+                    if (near) {
+                        double d2 = exact_d2(p, mi.x, mj.x);
+                        in_pair = !(d2 > p.cut2d);
+                        in0 = !(d2 > p.td[0].cut2);
+                        in1 = NT > 1 ? !(d2 > p.td[1].cut2) : false;
+                    } else {
+                        in_pair = !(r2 > p.cut2f);
+                        in0 = !(r2 > t0c2);
+                        in1 = NT > 1 ? !(r2 > t1c2) : false;
+                    }
+                    if ((kUse0 || (NT > 1 && S1 != SUN)) && !in_pair) continue;
+                    int excl = PMGPU_EXCL_NONE;
+                    if (mi.z == mj.z) {
+                        excl = excl_class(p, mi.x, mj.x);
+                        if (excl == PMGPU_EXCL_FULL) continue;
+                    }
+                    float rinv = rsqrtf(r2);
+                    rinv = rinv * fmaf(-0.5f * r2, rinv * rinv, 1.5f);
+                    float rd2 = rinv * rinv;
+                    float e0, f0, e1 = 0.f, f1 = 0.f;
+                    pot_f32<P0>(p, p.tf[0], r2, rd2, rinv, pi.w, pj.w, mi.y, mj.y, excl, e0, f0);
+                    if (NT > 1) pot_f32<P1>(p, p.tf[1], r2, rd2, rinv, pi.w, pj.w, mi.y, mj.y, excl, e1, f1);
+                    if (kMod) {
+                        float sv, sd;
+                        sw_f32<S0>(p.tf[0], r2, rinv, in0, sv, sd);
+                        f0 = f0 * sv - e0 * sd;
+                        e0 = e0 * sv;
+                        if (NT > 1) {
+                            sw_f32<S1>(p.tf[1], r2, rinv, in1, sv, sd);
+                            f1 = f1 * sv - e1 * sd;
+                            e1 = e1 * sv;
+                        }
+                    }
+                    if (P0 == LJ) el += e0; else ec += e0;
+                    if (NT > 1) { if (P1 == LJ) el += e1; else ec += e1; }
+                    float ft = NT > 1 ? f0 + f1 : f0;
+                    float fx = dx * ft, fy = dy * ft, fz = dz * ft;
+                    fix -= fx; fiy -= fy; fiz -= fz;
+                    float4 acc_j = sjf[w][jl];
+                    acc_j.x += fx; acc_j.y += fy; acc_j.z += fz;
+                    sjf[w][jl] = acc_j;
+                    if (p.virial) {
+                        vxx += fx * dx; vxy += fx * dy; vxz += fx * dz;
+                        vyy += fy * dy; vyz += fy * dz; vzz += fz * dz;
+                    }
+                    if (p.rec_pairs) {
+                        unsigned long long k = atomicAdd(p.rec_count, 1ull);
+                        if ((long long)k < p.rec_cap) {
+                            p.rec_pairs[2 * k] = min(mi.x, mj.x);
+                            p.rec_pairs[2 * k + 1] = max(mi.x, mj.x);
+                        }
+                    }
+                }
+                __syncwarp();
+                if (vj) {
+                    float4 fj = sjf[w][lane];
+                    fixed_add3(p.facc + 3 * (size_t)j, fj.x, fj.y, fj.z, p.scale, p.status);
+                }
+                acc[0] += el; acc[1] += ec;
+                acc[2] += vxx; acc[3] += vxy; acc[4] += vxz;
+                acc[5] += vxy; acc[6] += vyy; acc[7] += vyz;
+                acc[8] += vxz; acc[9] += vyz; acc[10] += vzz;
+                __syncwarp();
+            }
+            if (vi) fixed_add3(p.facc + 3 * (size_t)i, fix, fiy, fiz, p.scale, p.status);
+        }
+    }
+    block_reduce_store<4>(acc, p.erec + (size_t)blockIdx.x * kERec);
+}
+
+// ---------------------------------------------------------------- FP64 math
+template <int POT>
+__device__ __forceinline__ void pot_f64(const PairArgs& p, const TermD& t, double d2, double rd2,
+                                        double qi, double qj, int ti, int tj, int excl, double& e, double& f)
+{
+    if (POT == LJ) {
+        // LennardJonesForce::operator() (forces/LennardJonesForce.h:37-74)
+        double4 par = p.ljd[(size_t)ti * p.n_types + tj];
+        double A = excl == PMGPU_EXCL_MODIFIED ? par.z : par.x;
+        double B = excl == PMGPU_EXCL_MODIFIED ? par.w : par.y;
+        double r6 = rd2 * rd2 * rd2;
+        double r12 = r6 * r6;
+        double r6B = B * r6;
+        double r12A = A * r12;
+        e = r12A - r6B;
+        f = 12.0 * r12A * rd2 - 6.0 * r6B * rd2;
+    } else if (POT == CO) {
+        // CoulombForce::operator() (forces/CoulombForce.h:41-57)
+        e = qi * qj * sqrt(rd2);
+        if (excl == PMGPU_EXCL_MODIFIED) e *= p.csfd;
+        f = e * rd2;
+    } else if (POT == EW) {
+        // CoulombEwaldRealForce::operator() (forces/CoulombEwaldRealForce.h:45-73)
+        double qq = qi * qj;
+        if (p.csfd != 1.0 && excl == PMGPU_EXCL_MODIFIED) qq *= p.csfd;
+        double r = sqrt(d2);
+        double rr = 1.0 / r;
+        double ar = t.alpha * r;
+        double ex = qq * exp(-ar * ar);
+        const double E1 = 0.254829592, E2 = -0.284496736, E3 = 1.421413741,
+                     E4 = -1.453152027, E5 = 1.061405429, PP = 0.3275911;
+        double tt = 1.0 / (1.0 + PP * ar);
+        double poly = tt * (E1 + tt * (E2 + tt * (E3 + tt * (E4 + tt * E5))));
+        e = poly * ex * rr;
+        f = ((e + t.two_alpha_pi * ex) * rr * rr);
+    } else {
+        e = 0.0; f = 0.0;
+    }
+}
+
+template <int SW>
+__device__ __forceinline__ void sw_f64(const TermD& t, double d2, double& v, double& d)
+{
+    if (SW == SC2) {           // C2SwitchingFunction.h:64-82
+        d = 0.0;
+        if (d2 > t.cut2) v = 0.0;
+        else if (d2 >= t.on2) {
+            double c2 = t.cut2 - d2;
+            double c4 = c2 * (t.s2 + 2.0 * d2);
+            v = t.s1 * (c2 * c4);
+            d = t.s3 * (c2 * c2 - c4);
+        } else v = 1.0;
+    } else if (SW == SC1) {    // C1SwitchingFunction.h:64-75
+        if (d2 > t.cut2) { v = 0.0; d = 0.0; return; }
+        double dist = sqrt(d2);
+        v = 1.0 - dist * (t.c1_15_1 - d2 * t.c1_05_3);
+        d = -t.c1_15_1 / dist + dist * t.c1_15_3;
+    } else if (SW == SSH) {    // ShiftSwitchingFunction.h
+        if (d2 > t.cut2) { v = 0.0; d = 0.0; return; }
+        double x = (1.0 - d2 * t.sh_a);
+        v = x * x;
+        d = t.sh_b * x;
+    } else if (SW == SCUT) {   // CutoffSwitchingFunction.h:64-68
+        d = 0.0;
+        v = (d2 > t.cut2 ? 0.0 : 1.0);
+    } else {
+        v = 1.0; d = 0.0;
+    }
+}
+
+template <int NT, int P0, int S0, int P1, int S1>
+__global__ void __launch_bounds__(128) k_pair_fp64(PairArgs p)
+{
+    constexpr bool kMod = sw_modifies(S0) || (NT > 1 && sw_modifies(S1));
+    constexpr bool kUse = S0 != SUN || (NT > 1 && S1 != SUN);
+    constexpr bool kR2 = pot_r2(P0) || (NT > 1 && pot_r2(P1));
+    __shared__ double4 sjp[4][32];
+    __shared__ int4 sjm[4][32];
+    __shared__ double4 sjf[4][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int warps_total = gridDim.x * 4;
+    const int n_items = p.grid.ncell * (p.nd + 1);
+    double acc[kERec];
+    for (int k = 0; k < kERec; ++k) acc[k] = 0.0;
+
+    for (int item = blockIdx.x * 4 + w; item < n_items; item += warps_total) {
+        ItemGeom g = decode_item(p, item);
+        if (!g.valid) continue;
+        int sa = p.start[g.a], ea = p.start[g.a + 1];
+        int sb = p.start[g.b], eb = p.start[g.b + 1];
+        if (sa == ea || sb == eb) continue;
+        for (int ia = sa; ia < ea; ia += 32) {
+            int i = ia + lane;
+            bool vi = i < ea;
+            double4 pi = vi ? p.spos64[i] : make_double4(0, 0, 0, 0);
+            int4 mi = vi ? p.smeta[i] : make_int4(-1, 0, -2, 0);
+            double fix = 0.0, fiy = 0.0, fiz = 0.0;
+            for (int jb = g.same ? ia : sb; jb < eb; jb += 32) {
+                int j = jb + lane;
+                bool vj = j < eb;
+                sjp[w][lane] = vj ? p.spos64[j] : make_double4(0, 0, 0, 0);
+                sjm[w][lane] = vj ? p.smeta[j] : make_int4(-1, 0, -3, 0);
+                sjf[w][lane] = make_double4(0, 0, 0, 0);
+                __syncwarp();
+                int nj = min(32, eb - jb);
+                bool diag = g.same && jb == ia;
+                for (int t = 0; t < 32; ++t) {
+                    int jl = (lane + t) & 31;
+                    bool ok = vi && jl < nj && (!diag || jb + jl > i);
+                    if (!ok) continue;
+                    double4 pj = sjp[w][jl];
+                    double dx, dy, dz;
+                    double d2 = pbc_min_diff(p.pbc, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+                    if (kUse && d2 > p.cut2d) continue;
+                    int4 mj = sjm[w][jl];
+                    int excl = PMGPU_EXCL_NONE;
+                    if (mi.z == mj.z) {
+                        excl = excl_class(p, mi.x, mj.x);
+                        if (excl == PMGPU_EXCL_FULL) continue;
+                    }
+                    double rd2 = kR2 ? 1.0 / d2 : 1.0;
+                    double e0, f0, e1 = 0.0, f1 = 0.0;
+                    pot_f64<P0>(p, p.td[0], d2, rd2, pi.w, pj.w, mi.y, mj.y, excl, e0, f0);
+                    if (NT > 1) pot_f64<P1>(p, p.td[1], d2, rd2, pi.w, pj.w, mi.y, mj.y, excl, e1, f1);
+                    if (kMod) {
+                        double sv, sd;
+                        sw_f64<S0>(p.td[0], d2, sv, sd);
+                        f0 = f0 * sv - e0 * sd;
+                        e0 = e0 * sv;
+                        if (NT > 1) {
+                            sw_f64<S1>(p.td[1], d2, sv, sd);
+                            f1 = f1 * sv - e1 * sd;
+                            e1 = e1 * sv;
+                        }
+                    }
+                    if (P0 == LJ) acc[0] += e0; else acc[1] += e0;
+                    if (NT > 1) { if (P1 == LJ) acc[0] += e1; else acc[1] += e1; }
+                    double ft = NT > 1 ? (f0 + f1) : f0;
+                    double fx = dx * ft, fy = dy * ft, fz = dz * ft;
+                    fix -= fx; fiy -= fy; fiz -= fz;
+                    double4 aj = sjf[w][jl];
+                    aj.x += fx; aj.y += fy; aj.z += fz;
+                    sjf[w][jl] = aj;
+                    if (p.virial) {
+                        double xy = fx * dy, xz = fx * dz, yz = fy * dz;
+                        acc[2] += fx * dx; acc[3] += xy; acc[4] += xz;
+                        acc[5] += xy; acc[6] += fy * dy; acc[7] += yz;
+                        acc[8] += xz; acc[9] += yz; acc[10] += fz * dz;
+                    }
+                    if (p.rec_pairs) {
+                        unsigned long long k = atomicAdd(p.rec_count, 1ull);
+                        if ((long long)k < p.rec_cap) {
+                            p.rec_pairs[2 * k] = min(mi.x, mj.x);
+                            p.rec_pairs[2 * k + 1] = max(mi.x, mj.x);
+                        }
+                    }
+                }
+                __syncwarp();
+                if (vj) {
+                    double4 fj = sjf[w][lane];
+                    fixed_add3(p.facc + 3 * (size_t)j, fj.x, fj.y, fj.z, p.scale, p.status);
+                }
+                __syncwarp();
+            }
+            if (vi) fixed_add3(p.facc + 3 * (size_t)i, fix, fiy, fiz, p.scale, p.status);
+        }
+    }
+    block_reduce_store<4>(acc, p.erec + (size_t)blockIdx.x * kERec);
+}
+
+// ---------------------------------------------------------------- launch
+int pair_blocks(const CellGrid& g, int nd)
+{
+    long long items = (long long)g.ncell * (nd + 1);
+    long long b = (items + 3) / 4;
+    long long cap = 148 * 16;
+    return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+template <template <int, int, int, int, int> class K>
+struct Dispatch;
+
+#define PM_COMBO_SWITCH(KERNEL)                                                                        \
+    switch (combo) {                                                                                   \
+    case 0: KERNEL<1, CO, SC1, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                               \
+    case 1: KERNEL<1, CO, SC2, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                               \
+    case 2: KERNEL<1, CO, SCUT, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                              \
+    case 3: KERNEL<1, CO, SSH, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                               \
+    case 4: KERNEL<1, EW, SCUT, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                              \
+    case 5: KERNEL<1, LJ, SC1, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                               \
+    case 6: KERNEL<1, LJ, SC2, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                               \
+    case 7: KERNEL<1, LJ, SCUT, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                              \
+    case 8: KERNEL<1, LJ, SSH, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                               \
+    case 9: KERNEL<2, LJ, SC1, EW, SCUT><<<blocks, 128, 0, s>>>(a); break;                              \
+    case 10: KERNEL<2, LJ, SC1, CO, SSH><<<blocks, 128, 0, s>>>(a); break;                              \
+    case 11: KERNEL<2, LJ, SC2, CO, SC1><<<blocks, 128, 0, s>>>(a); break;                              \
+    case 12: KERNEL<2, LJ, SC2, EW, SCUT><<<blocks, 128, 0, s>>>(a); break;                             \
+    case 13: KERNEL<2, LJ, SC2, CO, SCUT><<<blocks, 128, 0, s>>>(a); break;                             \
+    case 14: KERNEL<2, LJ, SC2, CO, SSH><<<blocks, 128, 0, s>>>(a); break;                              \
+    case 15: KERNEL<2, LJ, SCUT, EW, SCUT><<<blocks, 128, 0, s>>>(a); break;                            \
+    case 16: KERNEL<2, LJ, SC2, CO, SC2><<<blocks, 128, 0, s>>>(a); break;                              \
+    default: return (int)cudaErrorInvalidValue;                                                        \
+    }
+
+int launch_pair_mixed(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches)
+{
+    PM_COMBO_SWITCH(k_pair_mixed)
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+int launch_pair_fp64(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches)
+{
+    PM_COMBO_SWITCH(k_pair_fp64)
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+}  // namespace pm

@@ -1,0 +1,555 @@
+// pm_pme.cu -- K3 spread, K4/K5 3-D FFT with the fused reciprocal
+// convolution, K6 gather and K7 Ewald correction of the particle-mesh Ewald
+// force (NonbondedPMEwaldSystemForce, forces/NonbondedPMEwaldSystemForce.h).
+//
+// Grid conventions follow Grid<BSpline> (base/Grid.h): grid coordinate
+// u = x K / L (no origin shift) wrapped into [0, K) by repeated +-K, base
+// index floor(u) - (P-1)/2 + K, weights BSpline::set(u - floor(u))
+// (base/BSpline.cpp:64-117); reciprocal energy and virial as
+// Grid::scalarSum (base/Grid.h:276-389) summed over the full spectrum; the
+// convolved grid is the real part of the unnormalised inverse transform;
+// forces as Grid::interpolateForce (base/Grid.h:193-228).
+//
+// The complex-to-complex ZFFT of the reference (base/fft.c, FFTComplex.cpp)
+// is replaced by a real-to-complex transform: z lines r2c into the half
+// spectrum K_x * K_y * (K_z/2 + 1), then complex passes along y and x.  The
+// x pass is fused with the convolution: a CTA transforms a tile of x-lines
+// forward, multiplies by theta(m) while summing energy and virial in FP64,
+// transforms back and writes once.  Each pass is one read and one write of
+// the half spectrum, with the lines staged in shared memory and transformed
+// there by a mixed-radix (4, 2, 3, 5, generic) Stockham FFT.
+//
+// Mixed precision: the charge grid is accumulated in int64 fixed point
+// (deterministic), the FFT and gather run in FP32.  FP64: double grid with
+// FP64 atomics, FP64 FFT and gather.
+#include "pm_kernels.h"
+#include "../../include/pmgpu.h"
+
+namespace pm {
+
+template <typename R> struct Cx;
+template <> struct Cx<float> { typedef float2 T; };
+template <> struct Cx<double> { typedef double2 T; };
+
+template <typename C> __device__ __forceinline__ C cmul(C a, C b)
+{
+    C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <typename C> __device__ __forceinline__ C cconj_if(C a, bool c) { if (c) a.y = -a.y; return a; }
+
+struct FftPlan {
+    int n;
+    int nrad;
+    int rad[24];
+};
+
+// twiddle exp(sign 2 pi i m / M) from the table of n-th roots exp(-2 pi i k / n)
+template <typename C>
+__device__ __forceinline__ C twid(const C* tw, int n, int m, int M, int sign)
+{
+    int k = (int)(((long long)m * (n / M)) % n);
+    C w = tw[k];
+    if (sign > 0) w.y = -w.y;
+    return w;
+}
+
+// R-point DFT of v[0..R-1] in place, exp(sign 2 pi i jk / R).
+template <typename C, typename R>
+__device__ __forceinline__ void small_dft(C* v, int Rn, int sign, const C* tw, int n)
+{
+    if (Rn == 2) {
+        C a = v[0], b = v[1];
+        v[0] = cadd(a, b); v[1] = csub(a, b);
+    } else if (Rn == 4) {
+        C a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+        C c = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+        // d * (sign i)
+        C di; di.x = -sign * d.y; di.y = sign * d.x;
+        v[0] = cadd(a, c); v[2] = csub(a, c);
+        v[1] = cadd(b, di); v[3] = csub(b, di);
+    } else if (Rn == 3) {
+        const R c1 = (R)-0.5, s1 = (R)0.86602540378443864676 * (R)sign;
+        C a = v[0], b = v[1], c = v[2];
+        C t; t.x = b.x + c.x; t.y = b.y + c.y;
+        C m; m.x = a.x + c1 * t.x; m.y = a.y + c1 * t.y;
+        C d; d.x = -s1 * (b.y - c.y); d.y = s1 * (b.x - c.x);
+        v[0].x = a.x + t.x; v[0].y = a.y + t.y;
+        v[1] = cadd(m, d); v[2] = csub(m, d);
+    } else if (Rn == 5) {
+        const R c1 = (R)0.30901699437494742410, c2 = (R)-0.80901699437494742410;
+        const R s1 = (R)0.95105651629515357212 * (R)sign, s2 = (R)0.58778525229247312917 * (R)sign;
+        C a = v[0];
+        C t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        C u1 = csub(v[1], v[4]), u2 = csub(v[2], v[3]);
+        C m1; m1.x = a.x + c1 * t1.x + c2 * t2.x; m1.y = a.y + c1 * t1.y + c2 * t2.y;
+        C m2; m2.x = a.x + c2 * t1.x + c1 * t2.x; m2.y = a.y + c2 * t1.y + c1 * t2.y;
+        C n1; n1.x = -(s1 * u1.y + s2 * u2.y); n1.y = s1 * u1.x + s2 * u2.x;
+        C n2; n2.x = -(s2 * u1.y - s1 * u2.y); n2.y = s2 * u1.x - s1 * u2.x;
+        v[0].x = a.x + t1.x + t2.x; v[0].y = a.y + t1.y + t2.y;
+        v[1] = cadd(m1, n1); v[4] = csub(m1, n1);
+        v[2] = cadd(m2, n2); v[3] = csub(m2, n2);
+    } else {
+        C out[16];
+        for (int k = 0; k < Rn; ++k) {
+            C s; s.x = 0; s.y = 0;
+            for (int j = 0; j < Rn; ++j) s = cadd(s, cmul(v[j], twid(tw, n, (j * k) % Rn, Rn, sign)));
+            out[k] = s;
+        }
+        for (int k = 0; k < Rn; ++k) v[k] = out[k];
+    }
+}
+
+// Stockham auto-sort FFT of `lines` lines of length n held in shared memory
+// (line stride ld); returns the buffer that holds the result.
+template <typename C, typename R>
+__device__ C* fft_lines(C* a, C* b, int lines, int ld, const FftPlan& pl, const C* tw, int sign)
+{
+    int n = pl.n;
+    int Ns = 1;
+    for (int s = 0; s < pl.nrad; ++s) {
+        int Rn = pl.rad[s];
+        int m = n / Rn;
+        for (int idx = threadIdx.x; idx < lines * m; idx += blockDim.x) {
+            int line = idx / m, j = idx - line * m;
+            const C* in = a + line * ld;
+            C* out = b + line * ld;
+            int k = j % Ns;
+            C v[16];
+            for (int r = 0; r < Rn; ++r) v[r] = in[j + r * m];
+            if (Ns > 1)
+                for (int r = 1; r < Rn; ++r) v[r] = cmul(v[r], twid(tw, n, k * r, Ns * Rn, sign));
+            small_dft<C, R>(v, Rn, sign, tw, n);
+            int base = (j / Ns) * Ns * Rn + k;
+            for (int r = 0; r < Rn; ++r) out[base + r * Ns] = v[r];
+        }
+        __syncthreads();
+        C* t = a; a = b; b = t;
+        Ns *= Rn;
+    }
+    return a;
+}
+
+// ------------------------------------------------------------------ spread
+__device__ __forceinline__ double wrap_grid(double x, int K)
+{
+    // while (x < 0.0) x += K; while (x >= K) x -= K;  (bounded: positions
+    // more than 64 boxes away are reduced with floor first)
+    if (!(fabs(x) < 64.0 * K)) x = x - (double)K * floor(x / (double)K);
+    int it = 0;
+    while (x < 0.0 && it < 256) { x += K; ++it; }
+    while (x >= (double)K && it < 512) { x -= K; ++it; }
+    return x;
+}
+
+template <typename R>
+__device__ __forceinline__ void bspline4(R w, R* th, R* dth, int order)
+{
+    // BSpline::set (base/BSpline.cpp:64-117) for any order >= 3
+    th[order - 1] = (R)0;
+    th[1] = w;
+    th[0] = (R)1 - w;
+    for (int k = 2; k < order - 1; k++) {
+        R div = (R)1 / (R)k;
+        th[k] = div * w * th[k - 1];
+        for (int j = 1; j < k; j++)
+            th[k - j] = div * ((w + (R)j) * th[k - j - 1] + ((R)(k + 1 - j) - w) * th[k - j]);
+        th[0] = div * ((R)1 - w) * th[0];
+    }
+    dth[0] = -th[0];
+    for (int j = 1; j <= order - 1; j++) dth[j] = th[j - 1] - th[j];
+    R div = (R)1 / (R)(order - 1);
+    th[order - 1] = div * w * th[order - 2];
+    for (int j = 1; j < order - 1; j++)
+        th[order - 1 - j] = div * ((w + (R)j) * th[order - j - 2] + ((R)(order - j) - w) * th[order - 1 - j]);
+    th[0] = div * ((R)1 - w) * th[0];
+}
+
+constexpr int kMaxOrder = 12;
+
+template <typename R>
+__device__ __forceinline__ void grid_point(const PmeArgs& a, int atom, int& i0, int& j0, int& k0,
+                                           R* tx, R* dtx, R* ty, R* dty, R* tz, R* dtz)
+{
+    double x = wrap_grid(a.pos[3 * (size_t)atom] * a.hxr, a.kx);
+    double y = wrap_grid(a.pos[3 * (size_t)atom + 1] * a.hyr, a.ky);
+    double z = wrap_grid(a.pos[3 * (size_t)atom + 2] * a.hzr, a.kz);
+    int ix = (int)x, iy = (int)y, iz = (int)z;
+    i0 = ix + a.offx; j0 = iy + a.offy; k0 = iz + a.offz;
+    if (a.order == 2) {
+        R wx = (R)(x - ix), wy = (R)(y - iy), wz = (R)(z - iz);
+        tx[1] = wx; tx[0] = (R)1 - wx; dtx[1] = 1; dtx[0] = -1;
+        ty[1] = wy; ty[0] = (R)1 - wy; dty[1] = 1; dty[0] = -1;
+        tz[1] = wz; tz[0] = (R)1 - wz; dtz[1] = 1; dtz[0] = -1;
+    } else {
+        bspline4<R>((R)(x - ix), tx, dtx, a.order);
+        bspline4<R>((R)(y - iy), ty, dty, a.order);
+        bspline4<R>((R)(z - iz), tz, dtz, a.order);
+    }
+}
+
+template <typename R>
+__global__ void k_spread(PmeArgs a)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.n) return;
+    int atom = a.sorted ? a.sorted[s] : s;
+    R tx[kMaxOrder], dtx[kMaxOrder], ty[kMaxOrder], dty[kMaxOrder], tz[kMaxOrder], dtz[kMaxOrder];
+    int i0, j0, k0;
+    grid_point<R>(a, atom, i0, j0, k0, tx, dtx, ty, dty, tz, dtz);
+    R q = (R)a.q[atom];
+    const int P = a.order;
+    for (int i = 0; i < P; i++) {
+        R aa = q * tx[i];
+        int i1 = (i + i0) % a.kx;
+        for (int j = 0; j < P; j++) {
+            R ab = aa * ty[j];
+            int j1 = (j + j0) % a.ky;
+            size_t row = ((size_t)i1 * a.ky + j1) * a.kz;
+            for (int k = 0; k < P; k++) {
+                int k1 = (k + k0) % a.kz;
+                R v = ab * tz[k];
+                if (sizeof(R) == 4) {
+                    long long qv = __double2ll_rn((double)v * a.qscale);
+                    if (qv) atomicAdd((unsigned long long*)(a.qgrid + row + k1), (unsigned long long)qv);
+                } else {
+                    atomicAdd((double*)a.rgrid + row + k1, (double)v);
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ FFT passes
+constexpr int kModeZR2C = 0, kModeY = 1, kModeXConv = 2, kModeZC2R = 3;
+
+struct PassArgs {
+    PmeArgs a;
+    FftPlan plan;
+    int lines;        // lines per CTA
+    int ld;           // smem line stride
+    int sign;
+    int tw_off;
+    int erec_off;
+};
+
+template <typename R, int MODE>
+__global__ void k_fft_pass(PassArgs pa)
+{
+    typedef typename Cx<R>::T C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* buf0 = (C*)smem_raw;
+    C* buf1 = buf0 + pa.lines * pa.ld;
+    const PmeArgs& a = pa.a;
+    const FftPlan& pl = pa.plan;
+    const int n = pl.n;
+    const C* tw = (const C*)a.tw + pa.tw_off;
+    C* cg = (C*)a.cgrid;
+    int L = pa.lines;
+    double acc[kERec];
+    for (int k = 0; k < kERec; ++k) acc[k] = 0.0;
+
+    if (MODE == kModeZR2C || MODE == kModeZC2R) {
+        // lines along z (contiguous); CTA handles L consecutive (x, y) lines
+        int nlines = a.kx * a.ky;
+        int l0 = blockIdx.x * L;
+        int nl = min(L, nlines - l0);
+        if (MODE == kModeZR2C) {
+            for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+                int l = idx / n, z = idx - l * n;
+                size_t g = (size_t)(l0 + l) * a.kz + z;
+                R v = sizeof(R) == 4 ? (R)((double)a.qgrid[g] * (1.0 / a.qscale)) : ((const R*)a.rgrid)[g];
+                C c; c.x = v; c.y = 0;
+                buf0[l * pa.ld + z] = c;
+            }
+        } else {
+            for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+                int l = idx / n, z = idx - l * n;
+                C c;
+                if (z < a.kzh) c = cg[(size_t)(l0 + l) * a.kzh + z];
+                else { c = cg[(size_t)(l0 + l) * a.kzh + (n - z)]; c.y = -c.y; }
+                buf0[l * pa.ld + z] = c;
+            }
+        }
+        __syncthreads();
+        C* r = fft_lines<C, R>(buf0, buf1, nl, pa.ld, pl, tw, pa.sign);
+        if (MODE == kModeZR2C) {
+            for (int idx = threadIdx.x; idx < nl * a.kzh; idx += blockDim.x) {
+                int l = idx / a.kzh, z = idx - l * a.kzh;
+                cg[(size_t)(l0 + l) * a.kzh + z] = r[l * pa.ld + z];
+            }
+        } else {
+            R* rg = (R*)a.rgrid;
+            for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+                int l = idx / n, z = idx - l * n;
+                rg[(size_t)(l0 + l) * a.kz + z] = r[l * pa.ld + z].x;
+            }
+        }
+        return;
+    }
+
+    // lines along y (fixed x) or x (fixed y): tile of L consecutive zh
+    int ntile = (a.kzh + L - 1) / L;
+    int outer = blockIdx.x / ntile;         // x for Y pass, y for X pass
+    int zh0 = (blockIdx.x - outer * ntile) * L;
+    int nl = min(L, a.kzh - zh0);
+    size_t stride, base;
+    if (MODE == kModeY) { stride = a.kzh; base = (size_t)outer * a.ky * a.kzh + zh0; }
+    else { stride = (size_t)a.ky * a.kzh; base = (size_t)outer * a.kzh + zh0; }
+    for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+        int e = idx / nl, l = idx - e * nl;     // consecutive threads: consecutive zh
+        buf0[l * pa.ld + e] = cg[base + e * stride + l];
+    }
+    __syncthreads();
+    C* r = fft_lines<C, R>(buf0, buf1, nl, pa.ld, pl, tw, pa.sign);
+    if (MODE == kModeXConv) {
+        // theta(m) multiply + energy / virial (Grid::scalarSum) on the
+        // forward-transformed x-lines, then the inverse x transform
+        int y = outer;
+        int y0 = y <= a.ky / 2 ? y : y - a.ky;
+        double my = y0 * a.lr;
+        double by = a.bfac[a.kx + y], ey = a.efac[a.kx + y];
+        for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+            int l = idx / n, x = idx - l * n;
+            int z = zh0 + l;
+            int x0 = x <= a.kx / 2 ? x : x - a.kx;
+            double mx = x0 * a.wr, mz = z * a.hr;
+            C& c = r[l * pa.ld + x];
+            if (x == 0 && y == 0 && z == 0) { c.x = 0; c.y = 0; continue; }
+            double m2 = mx * mx + my * my + mz * mz;
+            double theta = a.bfac[x] * by * a.bfac[a.kx + a.ky + z] * a.efac[x] * ey *
+                           a.efac[a.kx + a.ky + z] * a.piVr / m2;
+            double qv = (double)c.x * (double)c.x + (double)c.y * (double)c.y;
+            double e = qv * theta;
+            if (z > 0 && (z != a.kz / 2 || (a.kz & 1))) e *= 2.0;
+            acc[1] += e;
+            if (a.virial) {
+                double v = 2.0 * (1.0 / m2 + a.fac);
+                acc[2] += e * (1.0 - v * mx * mx); acc[3] -= e * (v * mx * my); acc[4] -= e * (v * mx * mz);
+                acc[6] += e * (1.0 - v * my * my); acc[7] -= e * (v * my * mz);
+                acc[10] += e * (1.0 - v * mz * mz);
+            }
+            c.x = (R)(c.x * theta);
+            c.y = (R)(c.y * theta);
+        }
+        __syncthreads();
+        C* other = (r == buf0) ? buf1 : buf0;
+        r = fft_lines<C, R>(r, other, nl, pa.ld, pl, tw, +1);
+    }
+    for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+        int e = idx / nl, l = idx - e * nl;
+        cg[base + e * stride + l] = r[l * pa.ld + e];
+    }
+    if (MODE == kModeXConv) {
+        for (int k = 0; k < kERec; ++k) acc[k] *= 0.5;
+        acc[5] = acc[3]; acc[8] = acc[4]; acc[9] = acc[7];
+        block_reduce_store<8>(acc, a.erec + ((size_t)pa.erec_off + blockIdx.x) * kERec);
+    }
+}
+
+// ------------------------------------------------------------------ gather
+template <typename R>
+__global__ void k_gather(PmeArgs a)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.n) return;
+    int atom = a.sorted ? a.sorted[s] : s;
+    R tx[kMaxOrder], dtx[kMaxOrder], ty[kMaxOrder], dty[kMaxOrder], tz[kMaxOrder], dtz[kMaxOrder];
+    int i0, j0, k0;
+    grid_point<R>(a, atom, i0, j0, k0, tx, dtx, ty, dty, tz, dtz);
+    const R* g = (const R*)a.rgrid;
+    R fx = 0, fy = 0, fz = 0;
+    const int P = a.order;
+    for (int i = 0; i < P; i++) {
+        int i1 = (i + i0) % a.kx;
+        for (int j = 0; j < P; j++) {
+            int j1 = (j + j0) % a.ky;
+            R xij = dtx[i] * ty[j], yij = tx[i] * dty[j], zij = tx[i] * ty[j];
+            size_t row = ((size_t)i1 * a.ky + j1) * a.kz;
+            for (int k = 0; k < P; k++) {
+                int k1 = (k + k0) % a.kz;
+                R term = g[row + k1];
+                fx -= term * xij * tz[k];
+                fy -= term * yij * tz[k];
+                fz -= term * zij * dtz[k];
+            }
+        }
+    }
+    double q = a.q[atom];
+    int slot = a.sorted ? s : a.slot_of[atom];
+    fixed_add3(a.facc + 3 * (size_t)slot, (double)fx * a.hxr * q, (double)fy * a.hyr * q,
+               (double)fz * a.hzr * q, a.scale, a.status);
+}
+
+static void make_plan(int n, FftPlan& p)
+{
+    p.n = n;
+    p.nrad = 0;
+    int m = n;
+    while (m % 4 == 0 && p.nrad < 24) { p.rad[p.nrad++] = 4; m /= 4; }
+    while (m % 2 == 0 && p.nrad < 24) { p.rad[p.nrad++] = 2; m /= 2; }
+    while (m % 3 == 0 && p.nrad < 24) { p.rad[p.nrad++] = 3; m /= 3; }
+    while (m % 5 == 0 && p.nrad < 24) { p.rad[p.nrad++] = 5; m /= 5; }
+    for (int f = 7; m > 1 && f <= 16; f += 2)
+        while (m % f == 0 && p.nrad < 24) { p.rad[p.nrad++] = f; m /= f; }
+    if (m > 1) p.nrad = -1;   // prime factor > 16: unsupported
+}
+
+template <typename R>
+static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches, int* erec_used)
+{
+    typedef typename Cx<R>::T C;
+    int nb = (a.n + 127) / 128;
+    size_t nreal = (size_t)a.kx * a.ky * a.kz;
+    if (sizeof(R) == 4) cudaMemsetAsync(a.qgrid, 0, sizeof(long long) * nreal, s);
+    else cudaMemsetAsync(a.rgrid, 0, sizeof(double) * nreal, s);
+    if (a.n > 0) { k_spread<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+
+    FftPlan px, py, pz;
+    make_plan(a.kx, px); make_plan(a.ky, py); make_plan(a.kz, pz);
+    if (px.nrad < 0 || py.nrad < 0 || pz.nrad < 0) return (int)cudaErrorInvalidValue;
+    const int threads = 256;
+    auto lines_for = [](int n) { int l = (16384 / (int)sizeof(C)) / n; return l < 1 ? 1 : (l > 32 ? 32 : l); };
+    // z r2c
+    {
+        PassArgs pa; pa.a = a; pa.plan = pz; pa.lines = lines_for(a.kz); pa.ld = a.kz + 1; pa.sign = -1;
+        pa.tw_off = a.twz; pa.erec_off = 0;
+        int blocks = (a.kx * a.ky + pa.lines - 1) / pa.lines;
+        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        cudaFuncSetAttribute(k_fft_pass<R, kModeZR2C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_fft_pass<R, kModeZR2C><<<blocks, threads, sm, s>>>(pa);
+    }
+    int tile = 16;
+    // y forward
+    {
+        PassArgs pa; pa.a = a; pa.plan = py; pa.lines = tile; pa.ld = a.ky + 1; pa.sign = -1;
+        pa.tw_off = a.twy; pa.erec_off = 0;
+        int blocks = a.kx * ((a.kzh + tile - 1) / tile);
+        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        cudaFuncSetAttribute(k_fft_pass<R, kModeY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_fft_pass<R, kModeY><<<blocks, threads, sm, s>>>(pa);
+    }
+    // x forward + convolution + x inverse
+    int xblocks = a.ky * ((a.kzh + tile - 1) / tile);
+    {
+        PassArgs pa; pa.a = a; pa.plan = px; pa.lines = tile; pa.ld = a.kx + 1; pa.sign = -1;
+        pa.tw_off = a.twx; pa.erec_off = 0;
+        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        cudaFuncSetAttribute(k_fft_pass<R, kModeXConv>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_fft_pass<R, kModeXConv><<<xblocks, threads, sm, s>>>(pa);
+    }
+    // y inverse
+    {
+        PassArgs pa; pa.a = a; pa.plan = py; pa.lines = tile; pa.ld = a.ky + 1; pa.sign = +1;
+        pa.tw_off = a.twy; pa.erec_off = 0;
+        int blocks = a.kx * ((a.kzh + tile - 1) / tile);
+        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        k_fft_pass<R, kModeY><<<blocks, threads, sm, s>>>(pa);
+    }
+    // z c2r
+    {
+        PassArgs pa; pa.a = a; pa.plan = pz; pa.lines = lines_for(a.kz); pa.ld = a.kz + 1; pa.sign = +1;
+        pa.tw_off = a.twz; pa.erec_off = 0;
+        int blocks = (a.kx * a.ky + pa.lines - 1) / pa.lines;
+        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        cudaFuncSetAttribute(k_fft_pass<R, kModeZC2R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_fft_pass<R, kModeZC2R><<<blocks, threads, sm, s>>>(pa);
+    }
+    if (a.n > 0) { k_gather<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+    *launches += 5;
+    *erec_used = xblocks;
+    return (int)cudaGetLastError();
+}
+
+int launch_pme_reciprocal(const PmeArgs& a, int fp64, cudaStream_t s, long long* launches,
+                          double* erec_base, int* erec_used)
+{
+    PmeArgs b = a;
+    b.erec = erec_base;
+    return fp64 ? run_reciprocal<double>(b, s, launches, erec_used)
+                : run_reciprocal<float>(b, s, launches, erec_used);
+}
+
+// ------------------------------------------------------------------ correction
+// correctionTerm (forces/NonbondedPMEwaldSystemForce.h:942-981), FP64, over
+// the exclusion table (FULL and MODIFIED pairs, molecules not consulted).
+__global__ void k_pme_correction(CorrArgs a)
+{
+    double acc[kERec];
+    for (int k = 0; k < kERec; ++k) acc[k] = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.n_excl; k += gridDim.x * blockDim.x) {
+        int2 pr = a.pairs[k];
+        const double* p1 = a.pos + 3 * (size_t)pr.x;
+        const double* p2 = a.pos + 3 * (size_t)pr.y;
+        double rx, ry, rz;
+        double r2 = pbc_min_diff(a.pbc, p1[0], p1[1], p1[2], p2[0], p2[1], p2[2], rx, ry, rz);
+        double qq = a.q[pr.x] * a.q[pr.y];
+        if (a.cls[k] == PMGPU_EXCL_MODIFIED) qq *= 1 - a.csf;
+        double r = sqrt(r2);
+        double rr = 1 / r;
+        double e = erf(a.alpha * r) * rr;
+        acc[1] -= qq * e;
+        double f = (qq * (a.two_alpha_pi * exp(-a.alpha2 * r2) - e) * rr * rr);
+        double fx = rx * f, fy = ry * f, fz = rz * f;
+        fixed_add3(a.facc + 3 * (size_t)a.slot_of[pr.x], -fx, -fy, -fz, a.scale, a.status);
+        fixed_add3(a.facc + 3 * (size_t)a.slot_of[pr.y], fx, fy, fz, a.scale, a.status);
+        if (a.virial) {
+            double xy = fx * ry, xz = fx * rz, yz = fy * rz;
+            acc[2] += fx * rx; acc[3] += xy; acc[4] += xz;
+            acc[5] += xy; acc[6] += fy * ry; acc[7] += yz;
+            acc[8] += xz; acc[9] += yz; acc[10] += fz * rz;
+        }
+    }
+    block_reduce_store<8>(acc, a.erec + (size_t)blockIdx.x * kERec);
+}
+
+int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches, int* blocks_used)
+{
+    int blocks = (a.n_excl + 255) / 256;
+    if (blocks < 1) blocks = 1;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_pme_correction<<<blocks, 256, 0, s>>>(a);
+    *launches += 1;
+    *blocks_used = blocks;
+    return (int)cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ finalize
+__global__ void k_finalize(int n, const unsigned long long* facc, const int* sorted, double inv_scale, double* fout)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int i = sorted[s];
+    for (int c = 0; c < 3; ++c)
+        fout[3 * (size_t)i + c] += (double)(long long)facc[3 * (size_t)s + c] * inv_scale;
+}
+
+int launch_finalize(int n, const unsigned long long* facc, const int* sorted, double inv_scale,
+                    double* fout, cudaStream_t s, long long* launches)
+{
+    if (n <= 0) return 0;
+    k_finalize<<<(n + 255) / 256, 256, 0, s>>>(n, facc, sorted, inv_scale, fout);
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+// deterministic sum of energy records: warp k sums component k
+__global__ void k_energy_reduce(const double* erec, int nrec, double* out)
+{
+    int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (k >= kERec) return;
+    double s = 0.0;
+    for (int r = lane; r < nrec; r += 32) s += erec[(size_t)r * kERec + k];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[k] += s;
+}
+
+int launch_energy_reduce(const double* erec, int nrec, double* out, cudaStream_t s, long long* launches)
+{
+    k_energy_reduce<<<1, 32 * kERec, 0, s>>>(erec, nrec, out);
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+}  // namespace pm

@@ -1,0 +1,933 @@
+// pmgpu_api.cu -- the C ABI (include/pmgpu.h) over the libpmgpu kernels.
+//
+// Host-side set-up follows the reference's constructors and initialize()
+// methods (cited per function); everything per evaluation runs on the
+// system's CUDA stream.  No CPU fallback: a missing or failing device is an
+// error status.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/pmgpu.h"
+#include "pm_kernels.h"
+
+using namespace pm;
+
+static const double kPi = 3.14159265358979323846;   // Constant::M_PI (base/pmconstants.cpp:56)
+static const double kEpsilon = 1.0e-14;              // Constant::EPSILON (base/pmconstants.cpp:45)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct pmgpu_system {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    long long launches = 0;
+    // topology
+    int n = 0, t = 0, e = 0;
+    double csf = 1.0;
+    std::vector<double> q;
+    std::vector<int> excl_pairs, excl_cls;
+    double* d_q = nullptr;
+    int* d_type = nullptr;
+    int* d_mol = nullptr;
+    float4* d_ljf = nullptr;
+    double4* d_ljd = nullptr;
+    uint32_t* d_xfull = nullptr;
+    uint32_t* d_xmod = nullptr;
+    int* d_xrow = nullptr;
+    int2* d_xent = nullptr;
+    int2* d_epairs = nullptr;
+    int* d_ecls = nullptr;
+    // box
+    bool box_set = false;
+    int box_version = 0;
+    double box[12];
+    double cell_size = 0.0;
+    Pbc pbc;
+    CellGrid grid;
+    // per-evaluation buffers
+    double* d_pos = nullptr;
+    double* d_fout = nullptr;
+    double* d_energy = nullptr;        // 11
+    double* h_energy = nullptr;        // pinned 11
+    unsigned long long* d_facc32 = nullptr;   // mixed (2^32)
+    unsigned long long* d_facc40 = nullptr;   // FP64 (2^40)
+    int* d_cell_lin = nullptr;
+    int* d_cell3 = nullptr;
+    int* d_counts = nullptr;
+    int* d_fill = nullptr;
+    int* d_start = nullptr;
+    int* d_tmp = nullptr;
+    int* d_sorted = nullptr;
+    int* d_slot = nullptr;
+    float4* d_spos = nullptr;
+    int4* d_smeta = nullptr;
+    double4* d_spos64 = nullptr;
+    int* d_status = nullptr;
+    int ncell_cap = 0;
+    double* d_erec = nullptr;
+    int erec_cap = 0;
+    std::vector<double> h_fbuf;
+    bool binned = false;
+};
+
+struct pmgpu_force {
+    pmgpu_system* sys = nullptr;
+    int kind = 0;   // 0 cutoff, 1 PME
+    int precision = 0;
+    pmgpu_cutoff_params cp;
+    pmgpu_pme_params pp;
+    // cutoff
+    int combo = -1;
+    int box_version = -1;
+    int nd = 0;
+    int4* d_deltas = nullptr;
+    float4* d_doff = nullptr;
+    int wrap = 0;
+    TermF tf[2];
+    TermD td[2];
+    double cut2 = 0.0;
+    // PME
+    double alpha = 0.0;
+    int kzh = 0;
+    long long* d_qgrid = nullptr;
+    void* d_cgrid = nullptr;
+    void* d_rgrid = nullptr;
+    void* d_tw = nullptr;
+    double* d_bfac = nullptr;
+    double* d_efac = nullptr;
+    double self_energy = 0.0, charged_energy = 0.0;
+    double* d_const_rec = nullptr;   // 2 records: without / with virial
+    int twx = 0, twy = 0, twz = 0;
+};
+
+// ------------------------------------------------------------------ helpers
+static int fail(pmgpu_system* s, int code, const std::string& msg)
+{
+    if (s) s->err = msg;
+    return code;
+}
+
+static int cuda_fail(pmgpu_system* s, cudaError_t e, const char* where)
+{
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    if (s) s->err = m;
+    return e == cudaErrorMemoryAllocation ? PMGPU_ERR_NOMEM : PMGPU_ERR_CUDA;
+}
+
+#define CK(call, where)                                         \
+    do {                                                        \
+        cudaError_t _e = (call);                                \
+        if (_e != cudaSuccess) return cuda_fail(sys, _e, where); \
+    } while (0)
+
+template <typename T>
+static cudaError_t dalloc(T** p, size_t count)
+{
+    if (*p) { cudaFree(*p); *p = nullptr; }
+    if (count == 0) count = 1;
+    return cudaMalloc((void**)p, sizeof(T) * count);
+}
+
+template <typename T>
+static void dfree(T*& p)
+{
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+// ------------------------------------------------------------------ context
+extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
+{
+    if (!out) return PMGPU_ERR_ARG;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= device || device < 0) return PMGPU_ERR_CUDA;
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return PMGPU_ERR_CUDA;
+    pmgpu_system* sys = new pmgpu_system();
+    sys->device = device;
+    e = cudaStreamCreateWithFlags(&sys->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete sys; return PMGPU_ERR_CUDA; }
+    if (cudaMalloc((void**)&sys->d_status, sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&sys->d_energy, sizeof(double) * kERec) != cudaSuccess ||
+        cudaMallocHost((void**)&sys->h_energy, sizeof(double) * kERec) != cudaSuccess) {
+        delete sys;
+        return PMGPU_ERR_NOMEM;
+    }
+    *out = sys;
+    return PMGPU_OK;
+}
+
+static void free_atom_buffers(pmgpu_system* s)
+{
+    dfree(s->d_q); dfree(s->d_type); dfree(s->d_mol); dfree(s->d_ljf); dfree(s->d_ljd);
+    dfree(s->d_xfull); dfree(s->d_xmod); dfree(s->d_xrow); dfree(s->d_xent);
+    dfree(s->d_epairs); dfree(s->d_ecls);
+    dfree(s->d_pos); dfree(s->d_fout); dfree(s->d_facc32); dfree(s->d_facc40);
+    dfree(s->d_cell_lin); dfree(s->d_cell3); dfree(s->d_tmp); dfree(s->d_sorted); dfree(s->d_slot);
+    dfree(s->d_spos); dfree(s->d_smeta); dfree(s->d_spos64);
+}
+
+extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
+{
+    if (!sys) return PMGPU_OK;
+    cudaSetDevice(sys->device);
+    cudaStreamSynchronize(sys->stream);
+    free_atom_buffers(sys);
+    dfree(sys->d_counts); dfree(sys->d_fill); dfree(sys->d_start); dfree(sys->d_erec);
+    dfree(sys->d_status); dfree(sys->d_energy);
+    if (sys->h_energy) cudaFreeHost(sys->h_energy);
+    cudaStreamDestroy(sys->stream);
+    delete sys;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_last_error(pmgpu_system* sys, char* buf, int len)
+{
+    if (!buf || len <= 0) return PMGPU_ERR_ARG;
+    std::string m = sys ? sys->err : std::string("no system");
+    snprintf(buf, (size_t)len, "%s", m.c_str());
+    return PMGPU_OK;
+}
+
+extern "C" void* pmgpu_stream(pmgpu_system* sys) { return sys ? (void*)sys->stream : nullptr; }
+extern "C" long long pmgpu_launch_count(pmgpu_system* sys) { return sys ? sys->launches : 0; }
+
+extern "C" int pmgpu_synchronize(pmgpu_system* sys)
+{
+    if (!sys) return PMGPU_ERR_ARG;
+    cudaSetDevice(sys->device);
+    CK(cudaStreamSynchronize(sys->stream), "synchronize");
+    int st = 0;
+    CK(cudaMemcpy(&st, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status");
+    if (st & kStatusOverflow)
+        return fail(sys, PMGPU_ERR_OVERFLOW, "non-finite or out-of-range force (fixed-point range exceeded)");
+    return PMGPU_OK;
+}
+
+// ------------------------------------------------------------------ topology
+extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* scaled_charge,
+                                  const int* type, const int* molecule, int n_types,
+                                  const double* lj_table, int n_excl, const int* excl_pairs,
+                                  const int* excl_class, const int* excl_check_class,
+                                  double coulomb_scaling_factor)
+{
+    if (!sys) return PMGPU_ERR_ARG;
+    if (n_atoms < 0 || n_types < 0 || n_excl < 0) return fail(sys, PMGPU_ERR_ARG, "negative size");
+    if (n_atoms > 0 && (!scaled_charge || !type || !molecule)) return fail(sys, PMGPU_ERR_ARG, "null atom array");
+    if (n_types > 0 && !lj_table) return fail(sys, PMGPU_ERR_ARG, "null Lennard-Jones table");
+    if (n_excl > 0 && (!excl_pairs || !excl_class)) return fail(sys, PMGPU_ERR_ARG, "null exclusion array");
+    for (int i = 0; i < n_atoms; ++i)
+        if (type[i] < 0 || type[i] >= n_types) return fail(sys, PMGPU_ERR_ARG, "atom type out of range");
+    cudaSetDevice(sys->device);
+    CK(cudaStreamSynchronize(sys->stream), "set_topology");
+    free_atom_buffers(sys);
+    sys->n = n_atoms; sys->t = n_types; sys->e = n_excl; sys->csf = coulomb_scaling_factor;
+    sys->q.assign(scaled_charge, scaled_charge + n_atoms);
+    sys->binned = false;
+    int n = n_atoms;
+    CK(dalloc(&sys->d_q, n), "alloc"); CK(dalloc(&sys->d_type, n), "alloc"); CK(dalloc(&sys->d_mol, n), "alloc");
+    CK(cudaMemcpy(sys->d_q, scaled_charge, sizeof(double) * n, cudaMemcpyHostToDevice), "copy");
+    CK(cudaMemcpy(sys->d_type, type, sizeof(int) * n, cudaMemcpyHostToDevice), "copy");
+    CK(cudaMemcpy(sys->d_mol, molecule, sizeof(int) * n, cudaMemcpyHostToDevice), "copy");
+    // Lennard-Jones table (LennardJonesParameterTable, T x T)
+    size_t tt = (size_t)n_types * n_types;
+    std::vector<float4> ljf(tt);
+    std::vector<double4> ljd(tt);
+    for (size_t k = 0; k < tt; ++k) {
+        const double* p = lj_table + 4 * k;
+        ljf[k] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3]);
+        ljd[k] = make_double4(p[0], p[1], p[2], p[3]);
+    }
+    CK(dalloc(&sys->d_ljf, tt), "alloc"); CK(dalloc(&sys->d_ljd, tt), "alloc");
+    CK(cudaMemcpy(sys->d_ljf, ljf.data(), sizeof(float4) * tt, cudaMemcpyHostToDevice), "copy");
+    CK(cudaMemcpy(sys->d_ljd, ljd.data(), sizeof(double4) * tt, cudaMemcpyHostToDevice), "copy");
+    // exclusions: check() classes as window bit masks (index delta 1..32) and
+    // a CSR list for larger deltas (ExclusionTable's lowDeltas / highDeltas)
+    std::vector<uint32_t> xfull(n, 0u), xmod(n, 0u);
+    std::vector<std::vector<int2>> far(n);
+    sys->excl_pairs.assign(2 * (size_t)n_excl, 0);
+    sys->excl_cls.assign(n_excl, 0);
+    for (int k = 0; k < n_excl; ++k) {
+        int a = excl_pairs[2 * k], b = excl_pairs[2 * k + 1];
+        if (a < 0 || b < 0 || a >= n || b >= n || a == b) return fail(sys, PMGPU_ERR_ARG, "bad exclusion pair");
+        if (a > b) std::swap(a, b);
+        int tcls = excl_class[k];
+        int ccls = excl_check_class ? excl_check_class[k] : tcls;
+        sys->excl_pairs[2 * k] = a; sys->excl_pairs[2 * k + 1] = b;
+        sys->excl_cls[k] = tcls;
+        int d = b - a;
+        if (d <= kExclWindow) {
+            uint32_t bit = 1u << (d - 1);
+            xfull[a] &= ~bit; xmod[a] &= ~bit;
+            if (ccls == PMGPU_EXCL_FULL) xfull[a] |= bit;
+            else if (ccls == PMGPU_EXCL_MODIFIED) xmod[a] |= bit;
+        } else {
+            far[a].push_back(make_int2(b, ccls));
+        }
+    }
+    std::vector<int> xrow(n + 1, 0);
+    std::vector<int2> xent;
+    for (int a = 0; a < n; ++a) {
+        std::sort(far[a].begin(), far[a].end(), [](int2 u, int2 v) { return u.x < v.x; });
+        xrow[a] = (int)xent.size();
+        for (auto& v : far[a]) xent.push_back(v);
+    }
+    xrow[n] = (int)xent.size();
+    CK(dalloc(&sys->d_xfull, n), "alloc"); CK(dalloc(&sys->d_xmod, n), "alloc");
+    CK(dalloc(&sys->d_xrow, n + 1), "alloc"); CK(dalloc(&sys->d_xent, xent.size()), "alloc");
+    CK(cudaMemcpy(sys->d_xfull, xfull.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice), "copy");
+    CK(cudaMemcpy(sys->d_xmod, xmod.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice), "copy");
+    CK(cudaMemcpy(sys->d_xrow, xrow.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice), "copy");
+    if (!xent.empty())
+        CK(cudaMemcpy(sys->d_xent, xent.data(), sizeof(int2) * xent.size(), cudaMemcpyHostToDevice), "copy");
+    CK(dalloc(&sys->d_epairs, n_excl), "alloc"); CK(dalloc(&sys->d_ecls, n_excl), "alloc");
+    if (n_excl) {
+        CK(cudaMemcpy(sys->d_epairs, sys->excl_pairs.data(), sizeof(int) * 2 * n_excl, cudaMemcpyHostToDevice), "copy");
+        CK(cudaMemcpy(sys->d_ecls, sys->excl_cls.data(), sizeof(int) * n_excl, cudaMemcpyHostToDevice), "copy");
+    }
+    // per-evaluation atom buffers
+    CK(dalloc(&sys->d_pos, 3 * (size_t)n), "alloc"); CK(dalloc(&sys->d_fout, 3 * (size_t)n), "alloc");
+    CK(dalloc(&sys->d_facc32, 3 * (size_t)n), "alloc"); CK(dalloc(&sys->d_facc40, 3 * (size_t)n), "alloc");
+    CK(dalloc(&sys->d_cell_lin, n), "alloc"); CK(dalloc(&sys->d_cell3, 3 * (size_t)n), "alloc");
+    CK(dalloc(&sys->d_tmp, n), "alloc"); CK(dalloc(&sys->d_sorted, n), "alloc"); CK(dalloc(&sys->d_slot, n), "alloc");
+    CK(dalloc(&sys->d_spos, n), "alloc"); CK(dalloc(&sys->d_smeta, n), "alloc"); CK(dalloc(&sys->d_spos64, n), "alloc");
+    sys->h_fbuf.assign(3 * (size_t)n, 0.0);
+    return PMGPU_OK;
+}
+
+// ------------------------------------------------------------------ box
+extern "C" int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* e2, const double* e3,
+                             const double* origin, double cell_size)
+{
+    if (!sys || !e1 || !e2 || !e3 || !origin) return PMGPU_ERR_ARG;
+    if (!(cell_size > 0.0)) return fail(sys, PMGPU_ERR_ARG, "Cubic cellmanager: cutoff > 0");
+    bool orth = !(e1[1] != 0.0 || e1[2] != 0.0 || e2[0] != 0.0 || e2[2] != 0.0 || e3[0] != 0.0 || e3[1] != 0.0);
+    if (!orth) return fail(sys, PMGPU_ERR_UNSUPPORTED, "only orthogonal periodic boxes are supported");
+    if (!(e1[0] > 0.0 && e2[1] > 0.0 && e3[2] > 0.0)) return fail(sys, PMGPU_ERR_ARG, "box edges must be positive");
+    cudaSetDevice(sys->device);
+    CK(cudaStreamSynchronize(sys->stream), "set_box");
+    for (int k = 0; k < 3; ++k) {
+        sys->box[k] = e1[k]; sys->box[3 + k] = e2[k]; sys->box[6 + k] = e3[k]; sys->box[9 + k] = origin[k];
+    }
+    sys->cell_size = cell_size;
+    // PeriodicBoundaryConditions::set (topology/PeriodicBoundaryConditions.cpp:40-77)
+    Pbc& b = sys->pbc;
+    double ex = e1[0], ey = e2[1], ez = e3[2];
+    b.e1x = ex; b.e2y = ey; b.e3z = ez;
+    // myE1r = (e2 x e3) / e1.(e2 x e3): for an orthogonal box the x component
+    double a1x = e2[1] * e3[2] - e2[2] * e3[1];
+    b.e1rx = a1x / (e1[0] * a1x + e1[1] * (e2[2] * e3[0] - e2[0] * e3[2]) + e1[2] * (e2[0] * e3[1] - e2[1] * e3[0]));
+    double a2y = e3[2] * e1[0] - e3[0] * e1[2];
+    b.e2ry = a2y / (e2[0] * (e3[1] * e1[2] - e3[2] * e1[1]) + e2[1] * a2y + e2[2] * (e3[0] * e1[1] - e3[1] * e1[0]));
+    double a3z = e1[0] * e2[1] - e1[1] * e2[0];
+    b.e3rz = a3z / (e3[0] * (e1[1] * e2[2] - e1[2] * e2[1]) + e3[1] * (e1[2] * e2[0] - e1[0] * e2[2]) + e3[2] * a3z);
+    double sx = (e1[0] + e2[0]) + e3[0], sy = (e1[1] + e2[1]) + e3[1], sz = (e1[2] + e2[2]) + e3[2];
+    double ax = origin[0] - sx * 0.5, ay = origin[1] - sy * 0.5, az = origin[2] - sz * 0.5;
+    double cx = origin[0] + sx * 0.5, cy = origin[1] + sy * 0.5, cz = origin[2] + sz * 0.5;
+    double mnx = std::min(ax, cx), mny = std::min(ay, cy), mnz = std::min(az, cz);
+    double mxx = std::max(ax, cx), mxy = std::max(ay, cy), mxz = std::max(az, cz);
+    double dx = (ex * 0.5) * (ex * 0.5), dy = (ey * 0.5) * (ey * 0.5), dz = (ez * 0.5) * (ez * 0.5);
+    b.d = std::min(dx, std::min(dy, dz));
+    b.hx = mxx - mnx; b.hy = mxy - mny; b.hz = mxz - mnz;
+    b.h2x = b.hx * 0.5; b.h2y = b.hy * 0.5; b.h2z = b.hz * 0.5;
+    b.ox = origin[0]; b.oy = origin[1]; b.oz = origin[2];
+    b.dx = origin[0] - mnx; b.dy = origin[1] - mny; b.dz = origin[2] - mnz;
+    // CubicCellManager::initialize + ArrayCellListStructure::initialize
+    CellGrid& g = sys->grid;
+    double hx = mxx - mnx, hy = mxy - mny, hz = mxz - mnz;
+    g.csx = hx / std::max(1.0, std::floor(hx / cell_size));
+    g.csy = hy / std::max(1.0, std::floor(hy / cell_size));
+    g.csz = hz / std::max(1.0, std::floor(hz / cell_size));
+    g.rcsx = 1.0 / g.csx; g.rcsy = 1.0 / g.csy; g.rcsz = 1.0 / g.csz;
+    g.nx = std::max(1, (int)std::floor(hx / g.csx + kEpsilon));
+    g.ny = std::max(1, (int)std::floor(hy / g.csy + kEpsilon));
+    g.nz = std::max(1, (int)std::floor(hz / g.csz + kEpsilon));
+    long long nc = (long long)g.nx * g.ny * g.nz;
+    if (nc > (1ll << 28)) return fail(sys, PMGPU_ERR_ARG, "simulation box / cell size ratio too big");
+    g.ncell = (int)nc;
+    if (g.ncell > sys->ncell_cap) {
+        CK(dalloc(&sys->d_counts, g.ncell), "alloc"); CK(dalloc(&sys->d_fill, g.ncell), "alloc");
+        CK(dalloc(&sys->d_start, g.ncell + 1), "alloc");
+        sys->ncell_cap = g.ncell;
+    }
+    sys->box_set = true;
+    sys->box_version++;
+    sys->binned = false;
+    return PMGPU_OK;
+}
+
+// ------------------------------------------------------------------ forces
+static void term_setup(const pmgpu_cutoff_params* p, int k, TermF& f, TermD& d)
+{
+    memset(&f, 0, sizeof(f));
+    memset(&d, 0, sizeof(d));
+    d.pot = f.pot = p->pot[k];
+    d.sw = f.sw = p->sw[k];
+    double c = p->cutoff[k], on = p->switchon[k];
+    d.cut2 = c * c;
+    if (d.sw == PMGPU_SW_C2) {       // C2SwitchingFunction.cpp:15-23
+        double q = c * c - on * on;
+        d.on2 = on * on;
+        d.s1 = 1.0 / (q * q * q);
+        d.s2 = c * c - 3.0 * on * on;
+        d.s3 = 4.0 / (q * q * q);
+    } else if (d.sw == PMGPU_SW_C1) { // C1SwitchingFunction.cpp:18-25
+        d.c1_15_1 = 1.5 / c;
+        d.c1_05_3 = 0.5 / (c * c * c);
+        d.c1_15_3 = 1.5 / (c * c * c);
+    } else if (d.sw == PMGPU_SW_SHIFT) {
+        d.sh_a = 1.0 / (c * c);
+        d.sh_b = -4.0 / (c * c);
+    }
+    d.alpha = p->alpha[k];
+    d.two_alpha_pi = 2.0 * d.alpha / std::sqrt(kPi);   // CoulombEwaldRealForce.cpp:17-21
+    f.cut2 = (float)d.cut2; f.on2 = (float)d.on2; f.s1 = (float)d.s1; f.s2 = (float)d.s2; f.s3 = (float)d.s3;
+    f.c1_15_1 = (float)d.c1_15_1; f.c1_05_3 = (float)d.c1_05_3; f.c1_15_3 = (float)d.c1_15_3;
+    f.sh_a = (float)d.sh_a; f.sh_b = (float)d.sh_b;
+    f.alpha = (float)d.alpha; f.two_alpha_pi = (float)d.two_alpha_pi;
+}
+
+extern "C" int pmgpu_cutoff_create(pmgpu_system* sys, const pmgpu_cutoff_params* p, pmgpu_force** out)
+{
+    if (!sys || !p || !out) return PMGPU_ERR_ARG;
+    *out = nullptr;
+    if (p->n_terms < 1 || p->n_terms > 2) return fail(sys, PMGPU_ERR_ARG, "n_terms must be 1 or 2");
+    if (p->precision != PMGPU_PRECISION_MIXED && p->precision != PMGPU_PRECISION_FP64)
+        return fail(sys, PMGPU_ERR_ARG, "unknown precision");
+    for (int k = 0; k < p->n_terms; ++k) {
+        if (p->sw[k] == PMGPU_SW_C2 && !(p->switchon[k] >= 0.0 && p->cutoff[k] > 0.0 && p->switchon[k] < p->cutoff[k]))
+            return fail(sys, PMGPU_ERR_ARG, "C2 switching function: 0 <= switchon < cutoff");
+        if (p->sw[k] != PMGPU_SW_UNIVERSAL && !(p->cutoff[k] > 0.0))
+            return fail(sys, PMGPU_ERR_ARG, "switching function cutoff > 0");
+        if (p->pot[k] == PMGPU_POT_EWALD_REAL && !(p->alpha[k] > 0.0))
+            return fail(sys, PMGPU_ERR_ARG, "CoulombEwaldReal -alpha > 0");
+    }
+    if (!(p->algorithm_cutoff > 0.0)) return fail(sys, PMGPU_ERR_ARG, "NonbondedCutoff -cutoff > 0");
+    int combo = pair_combo_id(p->n_terms, p->pot, p->sw);
+    if (combo < 0) return fail(sys, PMGPU_ERR_UNSUPPORTED, "force combination not registered for periodic boundaries");
+    pmgpu_force* f = new pmgpu_force();
+    f->sys = sys;
+    f->kind = 0;
+    f->precision = p->precision;
+    f->cp = *p;
+    f->combo = combo;
+    double c2 = 0.0;
+    for (int k = 0; k < p->n_terms; ++k) {
+        term_setup(p, k, f->tf[k], f->td[k]);
+        // Cutoff<>::cutoff of each term is its switching function's cutoff^2;
+        // the pair test uses the largest (OneAtomPairTwo.h:48)
+        c2 = std::max(c2, f->td[k].cut2);
+    }
+    f->cut2 = c2;
+    *out = f;
+    return PMGPU_OK;
+}
+
+// Neighbour-delta list of CellListEnumerator<Periodic, Cubic>::initialize
+// (topology/CellListEnumerator_periodicBoundaries.h:37-108).
+static void build_deltas(const CellGrid& g, double cutoff, std::vector<int4>& out, int& reach_ok)
+{
+    double cutoff2 = cutoff * cutoff;
+    int nx = (int)(cutoff / g.csx + 1.0 + kEpsilon);
+    int ny = (int)(cutoff / g.csy + 1.0 + kEpsilon);
+    int nz = (int)(cutoff / g.csz + 1.0 + kEpsilon);
+    int n0 = std::min(nx, g.nx), n1 = std::min(ny, g.ny), n2 = std::min(nz, g.nz);
+    reach_ok = (g.nx >= 2 * nx + 1) && (g.ny >= 2 * ny + 1) && (g.nz >= 2 * nz + 1);
+    int max2 = 2147483647 / 2;
+    int maxNX = max2 - max2 % g.nx, maxNY = max2 - max2 % g.ny, maxNZ = max2 - max2 % g.nz;
+    int nx1 = -g.nx / 2, ny1 = -g.ny / 2, nz1 = -g.nz / 2;
+    int maxNX1 = maxNX - nx1, maxNY1 = maxNY - ny1, maxNZ1 = maxNZ - nz1;
+    double xx = g.csx * g.csx, yy = g.csy * g.csy, zz = g.csz * g.csz;
+    struct C3 { int x, y, z; bool operator<(const C3& o) const { return x != o.x ? x < o.x : (y != o.y ? y < o.y : z < o.z); } };
+    std::set<C3> seen;
+    std::vector<C3> list;
+    seen.insert(C3{0, 0, 0});
+    for (int k = -n0; k <= n0; k++) {
+        int x = std::abs(k) - 1; if (x < 0) x = 0;
+        double d0 = x * x * xx;
+        for (int l = -n1; l <= n1; l++) {
+            int y = std::abs(l) - 1; if (y < 0) y = 0;
+            double d1 = d0 + y * y * yy;
+            for (int m = -n2; m <= n2; m++) {
+                int z = std::abs(m) - 1; if (z < 0) z = 0;
+                if (d1 + z * z * zz < cutoff2) {
+                    C3 md{(k + maxNX1) % g.nx + nx1, (l + maxNY1) % g.ny + ny1, (m + maxNZ1) % g.nz + nz1};
+                    if (seen.insert(md).second) list.push_back(md);
+                }
+            }
+        }
+    }
+    std::sort(list.begin(), list.end());
+    out.clear();
+    for (auto& c : list) out.push_back(make_int4(c.x, c.y, c.z, 0));
+}
+
+static int prepare_cutoff(pmgpu_force* f)
+{
+    pmgpu_system* sys = f->sys;
+    if (f->box_version == sys->box_version) return PMGPU_OK;
+    std::vector<int4> deltas;
+    int reach_ok = 0;
+    build_deltas(sys->grid, f->cp.algorithm_cutoff, deltas, reach_ok);
+    if ((int)deltas.size() > kMaxDeltas) return fail(sys, PMGPU_ERR_ARG, "cutoff / cell size ratio too large");
+    std::vector<float4> off(deltas.size());
+    for (size_t k = 0; k < deltas.size(); ++k)
+        off[k] = make_float4((float)(deltas[k].x * sys->grid.csx), (float)(deltas[k].y * sys->grid.csy),
+                             (float)(deltas[k].z * sys->grid.csz), 0.f);
+    f->nd = (int)deltas.size();
+    f->wrap = reach_ok ? 0 : 1;
+    CK(dalloc(&f->d_deltas, deltas.size()), "alloc");
+    CK(dalloc(&f->d_doff, deltas.size()), "alloc");
+    if (!deltas.empty()) {
+        CK(cudaMemcpy(f->d_deltas, deltas.data(), sizeof(int4) * deltas.size(), cudaMemcpyHostToDevice), "copy");
+        CK(cudaMemcpy(f->d_doff, off.data(), sizeof(float4) * off.size(), cudaMemcpyHostToDevice), "copy");
+    }
+    f->box_version = sys->box_version;
+    return PMGPU_OK;
+}
+
+// Grid::dftmod (base/Grid.h:650-665) of the order-P B-spline at w = 0
+static void dftmod(int order, int n, std::vector<double>& mod)
+{
+    std::vector<double> th(order), dth(order);
+    // BSpline::set(0.0) (base/BSpline.cpp:64-117)
+    double w = 0.0;
+    if (order == 2) { th[1] = w; th[0] = 1.0 - w; }
+    else {
+        th[order - 1] = 0.0; th[1] = w; th[0] = 1.0 - w;
+        for (int k = 2; k < order - 1; k++) {
+            double div = 1.0 / k;
+            th[k] = div * w * th[k - 1];
+            for (int j = 1; j < k; j++)
+                th[k - j] = div * ((w + j) * th[k - j - 1] + (k + 1 - j - w) * th[k - j]);
+            th[0] = div * (1 - w) * th[0];
+        }
+        double div = 1.0 / (order - 1.0);
+        th[order - 1] = div * w * th[order - 2];
+        for (int j = 1; j < order - 1; j++)
+            th[order - 1 - j] = div * ((w + j) * th[order - j - 2] + (order - j - w) * th[order - 1 - j]);
+        th[0] = div * (1 - w) * th[0];
+    }
+    mod.resize(n);
+    for (unsigned int i = 0; i < (unsigned)n; i++) {
+        double sc = 0.0, ss = 0.0;
+        for (unsigned int j = 0; j < (unsigned)order; j++) {
+            double x = kPi * 2.0 * i * j / (double)n;
+            sc += th[j] * std::cos(x);
+            ss += th[j] * std::sin(x);
+        }
+        mod[i] = 1.0 / (sc * sc + ss * ss);
+    }
+}
+
+static bool smooth_ok(int n)
+{
+    int m = n;
+    for (int f = 2; f <= 16 && m > 1; ++f)
+        while (m % f == 0) m /= f;
+    return m == 1;
+}
+
+extern "C" int pmgpu_pme_create(pmgpu_system* sys, const pmgpu_pme_params* p, pmgpu_force** out)
+{
+    if (!sys || !p || !out) return PMGPU_ERR_ARG;
+    *out = nullptr;
+    // NonbondedPMEwaldSystemForce::doMake validation (:1099-1139)
+    std::string err;
+    if (p->order < 2 || (p->order % 2) != 0) err += "PMEwald order (=" + std::to_string(p->order) + ") > 1 and even.";
+    if (p->grid[0] < p->order || p->grid[1] < p->order || p->grid[2] < p->order)
+        err += "PMEwald force: order <= nx, ny, nz.";
+    if (!(p->cutoff > 0.0)) err += "PMEwald cutoff > 0.";
+    if (!(p->accuracy > 0.0)) err += "PMEwald accuracy > 0.";
+    if (!err.empty()) return fail(sys, PMGPU_ERR_ARG, " force PMEwald :" + err);
+    if (p->order > 12) return fail(sys, PMGPU_ERR_UNSUPPORTED, "PME order > 12");
+    for (int k = 0; k < 3; ++k)
+        if (!smooth_ok(p->grid[k]) || p->grid[k] > 4096)
+            return fail(sys, PMGPU_ERR_UNSUPPORTED, "PME grid size needs prime factors <= 16 and <= 4096");
+    if (p->real) return fail(sys, PMGPU_ERR_UNSUPPORTED, "PMEwald -real on the GPU: use the split form "
+                                                         "(CoulombEwaldReal cutoff force + -reciprocal -correction)");
+    if (p->precision != PMGPU_PRECISION_MIXED && p->precision != PMGPU_PRECISION_FP64)
+        return fail(sys, PMGPU_ERR_ARG, "unknown precision");
+    if (!sys->box_set || sys->n == 0 && sys->q.empty()) {
+        // allowed: tables are built lazily at the first evaluation
+    }
+    pmgpu_force* f = new pmgpu_force();
+    f->sys = sys;
+    f->kind = 1;
+    f->precision = p->precision;
+    f->pp = *p;
+    // alpha: bisection of erfc(alpha Rc)/Rc = accuracy (:564-586)
+    double alpha = p->alpha, rc = p->cutoff;
+    if (alpha <= 0.0) {
+        alpha = 1.0;
+        while (std::erfc(alpha * rc) / rc >= p->accuracy) alpha *= 2.0;
+        double low = 0., high = alpha;
+        for (unsigned int i = 0; i < 100; ++i) {
+            alpha = 0.5 * (low + high);
+            if (std::erfc(alpha * rc) / rc >= p->accuracy) low = alpha; else high = alpha;
+        }
+    }
+    f->alpha = alpha;
+    *out = f;
+    return PMGPU_OK;
+}
+
+static int prepare_pme(pmgpu_force* f)
+{
+    pmgpu_system* sys = f->sys;
+    if (f->box_version == sys->box_version) return PMGPU_OK;
+    const pmgpu_pme_params& p = f->pp;
+    int kx = p.grid[0], ky = p.grid[1], kz = p.grid[2];
+    f->kzh = kz / 2 + 1;
+    double LX = sys->box[0], LY = sys->box[4], LZ = sys->box[8];
+    double alpha = f->alpha;
+    double fac = kPi * kPi / (alpha * alpha);
+    // exp tables and B-spline moduli (Grid::initialize, base/Grid.h:557-648)
+    std::vector<double> ex(kx), ey(ky), ez(f->kzh);
+    for (unsigned i = 0; i < (unsigned)kx; i++) {
+        int i0 = i <= (unsigned)kx / 2 ? (int)i : (int)i - kx;
+        double m = i0 * (1.0 / LX);
+        ex[i] = std::exp(-fac * (m * m));
+    }
+    for (unsigned j = 0; j < (unsigned)ky; j++) {
+        int j0 = j <= (unsigned)ky / 2 ? (int)j : (int)j - ky;
+        double m = j0 * (1.0 / LY);
+        ey[j] = std::exp(-fac * (m * m));
+    }
+    for (int k = 0; k < f->kzh; k++) {
+        double m = k * (1.0 / LZ);
+        ez[k] = std::exp(-fac * (m * m));
+    }
+    std::vector<double> mx, my, mz;
+    dftmod(p.order, kx, mx); dftmod(p.order, ky, my); dftmod(p.order, kz, mz);
+    std::vector<double> bf, ef;
+    bf.insert(bf.end(), mx.begin(), mx.end()); bf.insert(bf.end(), my.begin(), my.end());
+    bf.insert(bf.end(), mz.begin(), mz.begin() + f->kzh);
+    ef.insert(ef.end(), ex.begin(), ex.end()); ef.insert(ef.end(), ey.begin(), ey.end());
+    ef.insert(ef.end(), ez.begin(), ez.end());
+    CK(dalloc(&f->d_bfac, bf.size()), "alloc"); CK(dalloc(&f->d_efac, ef.size()), "alloc");
+    CK(cudaMemcpy(f->d_bfac, bf.data(), sizeof(double) * bf.size(), cudaMemcpyHostToDevice), "copy");
+    CK(cudaMemcpy(f->d_efac, ef.data(), sizeof(double) * ef.size(), cudaMemcpyHostToDevice), "copy");
+    // twiddles exp(-2 pi i k / n) per axis
+    f->twx = 0; f->twy = kx; f->twz = kx + ky;
+    int ntw = kx + ky + kz;
+    std::vector<double> tw(2 * (size_t)ntw);
+    int ns[3] = {kx, ky, kz};
+    int offs[3] = {f->twx, f->twy, f->twz};
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < ns[a]; ++k) {
+            long double ang = 2.0L * 3.141592653589793238462643383279502884L * k / ns[a];
+            tw[2 * (offs[a] + k)] = (double)cosl(ang);
+            tw[2 * (offs[a] + k) + 1] = (double)-sinl(ang);
+        }
+    size_t nreal = (size_t)kx * ky * kz, nhalf = (size_t)kx * ky * f->kzh;
+    if (f->precision == PMGPU_PRECISION_FP64) {
+        CK(dalloc((double2**)&f->d_tw, ntw), "alloc");
+        CK(cudaMemcpy(f->d_tw, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice), "copy");
+        CK(dalloc((double2**)&f->d_cgrid, nhalf), "alloc");
+        CK(dalloc((double**)&f->d_rgrid, nreal), "alloc");
+    } else {
+        std::vector<float> twf(tw.size());
+        for (size_t k = 0; k < tw.size(); ++k) twf[k] = (float)tw[k];
+        CK(dalloc((float2**)&f->d_tw, ntw), "alloc");
+        CK(cudaMemcpy(f->d_tw, twf.data(), sizeof(float) * twf.size(), cudaMemcpyHostToDevice), "copy");
+        CK(dalloc((float2**)&f->d_cgrid, nhalf), "alloc");
+        CK(dalloc((float**)&f->d_rgrid, nreal), "alloc");
+        CK(dalloc(&f->d_qgrid, nreal), "alloc");
+    }
+    // point self energy and charged-system term (:604-628)
+    double V = std::fabs(sys->box[0] * sys->box[4] * sys->box[8]);
+    double q2 = 0.0, q1 = 0.0;
+    for (int i = 0; i < sys->n; ++i) q2 += sys->q[i] * sys->q[i];
+    for (int i = 0; i < sys->n; ++i) q1 += sys->q[i];
+    f->self_energy = p.correction ? -q2 * alpha / std::sqrt(kPi) : 0.0;
+    f->charged_energy = 0.0;
+    if (p.correction && std::fabs(q1 * 0.00268283) > 1.0e-5)
+        f->charged_energy = -kPi / (2.0 * V * (alpha * alpha)) * q1 * q1;
+    double rec[2 * kERec];
+    memset(rec, 0, sizeof(rec));
+    rec[1] = f->self_energy + f->charged_energy;
+    rec[kERec + 1] = rec[1];
+    rec[kERec + 2] = rec[kERec + 6] = rec[kERec + 10] = f->charged_energy;
+    CK(dalloc(&f->d_const_rec, 2 * kERec), "alloc");
+    CK(cudaMemcpy(f->d_const_rec, rec, sizeof(rec), cudaMemcpyHostToDevice), "copy");
+    f->box_version = sys->box_version;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_force_destroy(pmgpu_force* f)
+{
+    if (!f) return PMGPU_OK;
+    cudaSetDevice(f->sys->device);
+    cudaStreamSynchronize(f->sys->stream);
+    dfree(f->d_deltas); dfree(f->d_doff); dfree(f->d_qgrid);
+    if (f->d_cgrid) cudaFree(f->d_cgrid);
+    if (f->d_rgrid) cudaFree(f->d_rgrid);
+    if (f->d_tw) cudaFree(f->d_tw);
+    dfree(f->d_bfac); dfree(f->d_efac); dfree(f->d_const_rec);
+    delete f;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_pme_alpha(pmgpu_force* f, double* alpha)
+{
+    if (!f || !alpha || f->kind != 1) return PMGPU_ERR_ARG;
+    *alpha = f->alpha;
+    return PMGPU_OK;
+}
+
+// ------------------------------------------------------------------ evaluate
+static int bin(pmgpu_system* sys, const double* d_pos)
+{
+    BinArgs a;
+    a.n = sys->n; a.pos = d_pos; a.q = sys->d_q; a.type = sys->d_type; a.mol = sys->d_mol;
+    a.pbc = sys->pbc; a.grid = sys->grid;
+    a.cell_lin = sys->d_cell_lin; a.cell3 = sys->d_cell3; a.counts = sys->d_counts; a.fill = sys->d_fill;
+    a.start = sys->d_start; a.tmp = sys->d_tmp; a.sorted = sys->d_sorted; a.slot_of = sys->d_slot;
+    a.spos = sys->d_spos; a.smeta = sys->d_smeta; a.spos64 = sys->d_spos64; a.status = sys->d_status;
+    int e = launch_bin(a, sys->stream, &sys->launches);
+    if (e) return cuda_fail(sys, (cudaError_t)e, "binning");
+    sys->binned = true;
+    return PMGPU_OK;
+}
+
+static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_pos, PairArgs& a)
+{
+    memset(&a, 0, sizeof(a));
+    a.start = sys->d_start; a.spos = sys->d_spos; a.smeta = sys->d_smeta; a.spos64 = sys->d_spos64;
+    a.pos = d_pos;
+    a.xfull = sys->d_xfull; a.xmod = sys->d_xmod; a.xrow = sys->d_xrow; a.xent = sys->d_xent;
+    a.ljf = sys->d_ljf; a.ljd = sys->d_ljd; a.n_types = sys->t;
+    a.deltas = f->d_deltas; a.doff = f->d_doff; a.nd = f->nd;
+    a.grid = sys->grid; a.pbc = sys->pbc; a.wrap = f->wrap;
+    a.lx = (float)sys->box[0]; a.ly = (float)sys->box[4]; a.lz = (float)sys->box[8];
+    a.ilx = (float)(1.0 / sys->box[0]); a.ily = (float)(1.0 / sys->box[4]); a.ilz = (float)(1.0 / sys->box[8]);
+    a.n_terms = f->cp.n_terms;
+    a.tf[0] = f->tf[0]; a.tf[1] = f->tf[1]; a.td[0] = f->td[0]; a.td[1] = f->td[1];
+    a.cut2f = (float)f->cut2; a.cut2d = f->cut2;
+    a.guard = 2.0e-5f;
+    a.csf = (float)sys->csf; a.csfd = sys->csf;
+    a.status = sys->d_status;
+    if (f->precision == PMGPU_PRECISION_FP64) { a.facc = sys->d_facc40; a.scale = kScaleFp64; }
+    else { a.facc = sys->d_facc32; a.scale = kScaleMixed; }
+}
+
+static int ensure_erec(pmgpu_system* sys, int need)
+{
+    if (need <= sys->erec_cap) return PMGPU_OK;
+    int cap = std::max(need, 2 * sys->erec_cap);
+    CK(dalloc(&sys->d_erec, (size_t)cap * kERec), "alloc");
+    sys->erec_cap = cap;
+    return PMGPU_OK;
+}
+
+static int pme_xblocks(const pmgpu_force* f) { return f->pp.grid[1] * ((f->kzh + 15) / 16); }
+
+static int eval_core(pmgpu_system* sys, int nf, pmgpu_force* const* forces, const double* d_pos,
+                     double* d_fout, double* d_energy, unsigned flags)
+{
+    if (!sys->box_set) return fail(sys, PMGPU_ERR_STATE, "box not set (pmgpu_set_box)");
+    if (nf < 0 || (nf > 0 && !forces)) return fail(sys, PMGPU_ERR_ARG, "bad force list");
+    int virial = (flags & PMGPU_FLAG_VIRIAL) ? 1 : 0;
+    bool use32 = false, use40 = false;
+    int need = 1;
+    for (int k = 0; k < nf; ++k) {
+        pmgpu_force* f = forces[k];
+        if (!f || f->sys != sys) return fail(sys, PMGPU_ERR_ARG, "force belongs to another system");
+        int r = f->kind == 0 ? prepare_cutoff(f) : prepare_pme(f);
+        if (r) return r;
+        (f->precision == PMGPU_PRECISION_FP64 ? use40 : use32) = true;
+        if (f->kind == 0) need += pair_blocks(sys->grid, f->nd);
+        else need += pme_xblocks(f) + 148 * 4 + 1;
+    }
+    int r = ensure_erec(sys, need);
+    if (r) return r;
+    cudaStream_t s = sys->stream;
+    size_t n3 = 3 * (size_t)sys->n;
+    CK(cudaMemsetAsync(sys->d_status, 0, sizeof(int), s), "memset");
+    if (use32) CK(cudaMemsetAsync(sys->d_facc32, 0, sizeof(unsigned long long) * n3, s), "memset");
+    if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
+    r = bin(sys, d_pos);
+    if (r) return r;
+    int used = 0;
+    for (int k = 0; k < nf; ++k) {
+        pmgpu_force* f = forces[k];
+        bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+        unsigned long long* facc = fp64 ? sys->d_facc40 : sys->d_facc32;
+        double scale = fp64 ? kScaleFp64 : kScaleMixed;
+        if (f->kind == 0) {
+            PairArgs a;
+            fill_pair_args(sys, f, d_pos, a);
+            a.virial = virial;
+            a.erec = sys->d_erec + (size_t)used * kERec;
+            int blocks = pair_blocks(sys->grid, f->nd);
+            int e = fp64 ? launch_pair_fp64(a, f->combo, blocks, s, &sys->launches)
+                         : launch_pair_mixed(a, f->combo, blocks, s, &sys->launches);
+            if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
+            used += blocks;
+        } else {
+            const pmgpu_pme_params& p = f->pp;
+            if (p.correction) {
+                CorrArgs c;
+                c.n_excl = sys->e; c.pairs = sys->d_epairs; c.cls = sys->d_ecls; c.pos = d_pos; c.q = sys->d_q;
+                c.slot_of = sys->d_slot; c.pbc = sys->pbc; c.alpha = f->alpha; c.alpha2 = f->alpha * f->alpha;
+                c.two_alpha_pi = 2.0 * f->alpha / std::sqrt(kPi); c.csf = sys->csf;
+                c.facc = facc; c.scale = scale; c.erec = sys->d_erec + (size_t)used * kERec; c.status = sys->d_status;
+                c.virial = virial;
+                int b = 0;
+                int e = launch_pme_correction(c, s, &sys->launches, &b);
+                if (e) return cuda_fail(sys, (cudaError_t)e, "PME correction");
+                used += b;
+                CK(cudaMemcpyAsync(sys->d_erec + (size_t)used * kERec, f->d_const_rec + (virial ? kERec : 0),
+                                   sizeof(double) * kERec, cudaMemcpyDeviceToDevice, s), "copy");
+                used += 1;
+            }
+            if (p.reciprocal) {
+                PmeArgs a;
+                memset(&a, 0, sizeof(a));
+                a.n = sys->n; a.pos = d_pos; a.q = sys->d_q; a.sorted = sys->d_sorted; a.slot_of = sys->d_slot;
+                a.kx = p.grid[0]; a.ky = p.grid[1]; a.kz = p.grid[2]; a.kzh = f->kzh; a.order = p.order;
+                double LX = sys->box[0], LY = sys->box[4], LZ = sys->box[8];
+                a.hxr = p.grid[0] / LX; a.hyr = p.grid[1] / LY; a.hzr = p.grid[2] / LZ;
+                a.offx = -(p.order - 1) / 2 + p.grid[0];
+                a.offy = -(p.order - 1) / 2 + p.grid[1];
+                a.offz = -(p.order - 1) / 2 + p.grid[2];
+                a.qgrid = f->d_qgrid; a.cgrid = f->d_cgrid; a.rgrid = f->d_rgrid; a.tw = f->d_tw;
+                a.twx = f->twx; a.twy = f->twy; a.twz = f->twz;
+                a.bfac = f->d_bfac; a.efac = f->d_efac;
+                a.piVr = 1.0 / (kPi * (LX * LY * LZ));
+                a.fac = kPi * kPi / (f->alpha * f->alpha);
+                a.wr = 1.0 / LX; a.lr = 1.0 / LY; a.hr = 1.0 / LZ;
+                a.facc = facc; a.scale = scale; a.qscale = kScaleFp64;
+                a.status = sys->d_status; a.virial = virial;
+                int u = 0;
+                int e = launch_pme_reciprocal(a, fp64 ? 1 : 0, s, &sys->launches, sys->d_erec + (size_t)used * kERec, &u);
+                if (e) return cuda_fail(sys, (cudaError_t)e, "PME reciprocal");
+                used += u;
+            }
+        }
+    }
+    if (use32) {
+        int e = launch_finalize(sys->n, sys->d_facc32, sys->d_sorted, 1.0 / kScaleMixed, d_fout, s, &sys->launches);
+        if (e) return cuda_fail(sys, (cudaError_t)e, "finalize");
+    }
+    if (use40) {
+        int e = launch_finalize(sys->n, sys->d_facc40, sys->d_sorted, 1.0 / kScaleFp64, d_fout, s, &sys->launches);
+        if (e) return cuda_fail(sys, (cudaError_t)e, "finalize");
+    }
+    if (used > 0) {
+        int e = launch_energy_reduce(sys->d_erec, used, d_energy, s, &sys->launches);
+        if (e) return cuda_fail(sys, (cudaError_t)e, "energy reduce");
+    }
+    if (!virial) {
+        // the virial slots are only written when ScalarStructure::virial() is set
+    }
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_evaluate_device(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces,
+                                     const double* d_positions, double* d_forces_accum,
+                                     double* d_energies, unsigned flags)
+{
+    if (!sys || !d_positions || !d_forces_accum || !d_energies) return PMGPU_ERR_ARG;
+    cudaSetDevice(sys->device);
+    // without PMGPU_FLAG_VIRIAL every kernel adds zero to the virial slots
+    return eval_core(sys, n_forces, forces, d_positions, d_forces_accum, d_energies, flags);
+}
+
+extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces,
+                              const double* positions, double* forces_accum,
+                              pmgpu_energies* energies, unsigned flags)
+{
+    if (!sys || !positions || !forces_accum || !energies) return PMGPU_ERR_ARG;
+    cudaSetDevice(sys->device);
+    if (sys->n == 0 && sys->q.empty() && sys->d_pos == nullptr) return fail(sys, PMGPU_ERR_STATE, "topology not set");
+    size_t n3 = 3 * (size_t)sys->n;
+    cudaStream_t s = sys->stream;
+    CK(cudaMemcpyAsync(sys->d_pos, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, s), "H2D positions");
+    CK(cudaMemsetAsync(sys->d_fout, 0, sizeof(double) * n3, s), "memset");
+    CK(cudaMemsetAsync(sys->d_energy, 0, sizeof(double) * kERec, s), "memset");
+    int r = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy, flags);
+    if (r) return r;
+    CK(cudaMemcpyAsync(sys->h_fbuf.data(), sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
+    CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kERec, cudaMemcpyDeviceToHost, s), "D2H energies");
+    r = pmgpu_synchronize(sys);
+    if (r) return r;
+    for (size_t k = 0; k < n3; ++k) forces_accum[k] += sys->h_fbuf[k];
+    energies->lennard_jones += sys->h_energy[0];
+    energies->coulomb += sys->h_energy[1];
+    if (flags & PMGPU_FLAG_VIRIAL)
+        for (int k = 0; k < 9; ++k) energies->virial[k] += sys->h_energy[2 + k];
+    return PMGPU_OK;
+}
+
+// ------------------------------------------------------------------ diagnostics
+extern "C" int pmgpu_get_cells(pmgpu_system* sys, int* cells, int* dims)
+{
+    if (!sys || !cells || !dims) return PMGPU_ERR_ARG;
+    if (!sys->binned) return fail(sys, PMGPU_ERR_STATE, "no evaluation yet");
+    cudaSetDevice(sys->device);
+    CK(cudaStreamSynchronize(sys->stream), "sync");
+    CK(cudaMemcpy(cells, sys->d_cell3, sizeof(int) * 3 * (size_t)sys->n, cudaMemcpyDeviceToHost), "copy");
+    dims[0] = sys->grid.nx; dims[1] = sys->grid.ny; dims[2] = sys->grid.nz;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* positions,
+                               long long* count, int* pairs, long long cap)
+{
+    if (!sys || !f || !positions || !count || (cap > 0 && !pairs)) return PMGPU_ERR_ARG;
+    if (f->kind != 0) return fail(sys, PMGPU_ERR_UNSUPPORTED, "pair recording is for cutoff forces");
+    if (!sys->box_set) return fail(sys, PMGPU_ERR_STATE, "box not set");
+    cudaSetDevice(sys->device);
+    int r = prepare_cutoff(f);
+    if (r) return r;
+    cudaStream_t s = sys->stream;
+    size_t n3 = 3 * (size_t)sys->n;
+    CK(cudaMemcpyAsync(sys->d_pos, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, s), "H2D");
+    CK(cudaMemsetAsync(sys->d_status, 0, sizeof(int), s), "memset");
+    CK(cudaMemsetAsync(sys->d_facc32, 0, sizeof(unsigned long long) * n3, s), "memset");
+    CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
+    r = bin(sys, sys->d_pos);
+    if (r) return r;
+    int blocks = pair_blocks(sys->grid, f->nd);
+    r = ensure_erec(sys, blocks);
+    if (r) return r;
+    int* d_pairs = nullptr;
+    unsigned long long* d_count = nullptr;
+    long long dcap = cap > 0 ? cap : 1;
+    CK(cudaMalloc((void**)&d_pairs, sizeof(int) * 2 * (size_t)dcap), "alloc");
+    CK(cudaMalloc((void**)&d_count, sizeof(unsigned long long)), "alloc");
+    CK(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s), "memset");
+    PairArgs a;
+    fill_pair_args(sys, f, sys->d_pos, a);
+    a.erec = sys->d_erec;
+    a.rec_pairs = d_pairs; a.rec_count = d_count; a.rec_cap = dcap;
+    int e = f->precision == PMGPU_PRECISION_FP64 ? launch_pair_fp64(a, f->combo, blocks, s, &sys->launches)
+                                                 : launch_pair_mixed(a, f->combo, blocks, s, &sys->launches);
+    unsigned long long cnt = 0;
+    if (!e) e = (int)cudaMemcpyAsync(&cnt, d_count, sizeof(cnt), cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    if (!e && cnt > 0 && cap > 0)
+        e = (int)cudaMemcpy(pairs, d_pairs, sizeof(int) * 2 * (size_t)std::min<long long>(cnt, cap), cudaMemcpyDeviceToHost);
+    cudaFree(d_pairs);
+    cudaFree(d_count);
+    if (e) return cuda_fail(sys, (cudaError_t)e, "pair recording");
+    *count = (long long)cnt;
+    if ((long long)cnt > cap) return fail(sys, PMGPU_ERR_CAPACITY, "pair capacity too small");
+    return PMGPU_OK;
+}

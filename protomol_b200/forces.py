@@ -1,0 +1,346 @@
+"""Host-side mirror of ProtoMol's force interface for the nonbonded path.
+
+The classes here mirror what a ProtoMol user sees:
+
+* :class:`Topology` -- ``Topology<PeriodicBoundaryConditions,
+  CubicCellManager>`` (``topology/Topology.h``): atoms, exclusions, the
+  Lennard-Jones table, coulombScalingFactor, box and cell size;
+* :class:`ForceFactory` -- ``ForceFactory::make`` (``frontend/ForceFactoryDetails.cpp:48-293``):
+  a force definition string such as
+  ``"LennardJones CoulombEwaldReal -algorithm NonbondedCutoff -switchingFunction C2
+  -switchingFunction Cutoff -switchon 10 -cutoff 12 -alpha 0.32 -cutoff 12 -cutoff 12"``
+  or ``"Coulomb -algorithm PMEwald -reciprocal -correction -interpolation BSpline
+  -gridsize 64 64 64 -cutoff 12 -alpha 0.32"`` becomes a force object;
+* :class:`SystemForce` -- ``SystemForce::evaluate(topo, positions, forces,
+  energies)`` (``forces/SystemForce.h:18-76``): forces and energies are
+  accumulated (+=) into the caller's arrays.
+
+Every evaluation runs on the GPU through libpmgpu.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+_VP = C.c_void_p
+
+
+class ScalarStructure:
+    """The slots of ``ScalarStructure`` (``base/ScalarStructure.h:25-54``)
+    this path writes, with the ``virial()`` switch."""
+
+    def __init__(self, virial: bool = True):
+        self.lennard_jones = 0.0
+        self.coulomb = 0.0
+        self.virial_tensor = np.zeros(9)
+        self.virial = virial
+
+    def clear(self):
+        self.lennard_jones = 0.0
+        self.coulomb = 0.0
+        self.virial_tensor[:] = 0.0
+
+    def potential_energy(self) -> float:
+        return self.lennard_jones + self.coulomb
+
+
+class Topology:
+    """A pmgpu_system built from a :class:`protomol_b200.systems.System`."""
+
+    def __init__(self, system, device: int = 0):
+        lib = _lib.load()
+        h = _VP()
+        check(lib.pmgpu_system_create(device, C.byref(h)))
+        self.handle = h
+        self.system = system
+        self.n_atoms = system.n_atoms
+        self._keep = []
+        self.set_topology(system)
+        self.set_box(system.box, system.cell_size)
+
+    def set_topology(self, s):
+        lib = _lib.load()
+        q = np.ascontiguousarray(s.scaled_charge, np.float64)
+        ty = np.ascontiguousarray(s.atom_type, np.int32)
+        mol = np.ascontiguousarray(s.molecule, np.int32)
+        lj = np.ascontiguousarray(s.lj_table, np.float64)
+        ex = np.ascontiguousarray(s.exclusions[:, :2], np.int32)
+        cl = np.ascontiguousarray(s.exclusions[:, 2], np.int32)
+        ck = np.ascontiguousarray(s.exclusion_check, np.int32)
+        p = lambda a: a.ctypes.data_as(_VP) if a.size else None
+        check(lib.pmgpu_set_topology(self.handle, s.n_atoms, p(q), p(ty), p(mol), s.n_types, p(lj),
+                                     int(ex.shape[0]), p(ex), p(cl), p(ck), float(s.csf)), self.handle)
+        self.n_atoms = s.n_atoms
+
+    def set_box(self, box, cell_size):
+        lib = _lib.load()
+        b = np.ascontiguousarray(box, np.float64).reshape(4, 3)
+        arr = [(C.c_double * 3)(*b[k]) for k in range(4)]
+        check(lib.pmgpu_set_box(self.handle, *arr, float(cell_size)), self.handle)
+
+    @property
+    def stream(self) -> int:
+        return _lib.load().pmgpu_stream(self.handle) or 0
+
+    def launch_count(self) -> int:
+        return int(_lib.load().pmgpu_launch_count(self.handle))
+
+    def cells(self):
+        cells = np.zeros((self.n_atoms, 3), np.int32)
+        dims = np.zeros(3, np.int32)
+        check(_lib.load().pmgpu_get_cells(self.handle, cells.ctypes.data_as(_VP), dims.ctypes.data_as(_VP)),
+              self.handle)
+        return cells, tuple(int(d) for d in dims)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().pmgpu_system_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SystemForce:
+    """One GPU force object (a pmgpu_force)."""
+
+    keyword = ""
+
+    def __init__(self, topo: Topology, handle, ident: str, params):
+        self.topo = topo
+        self.handle = handle
+        self.id = ident
+        self.params = params
+
+    def getKeyword(self) -> str:  # noqa: N802 (mirrors Force::getKeyword)
+        return self.keyword
+
+    def getIdNoAlias(self) -> str:  # noqa: N802
+        return self.id
+
+    def evaluate(self, topo: Topology, positions: np.ndarray, forces: np.ndarray,
+                 energies: ScalarStructure):
+        evaluate_group(topo, [self], positions, forces, energies)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().pmgpu_force_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NonbondedCutoffSystemForce(SystemForce):
+    keyword = "NonbondedCutoff"
+
+    def pairs(self, positions, cap=None):
+        """Within-cutoff pair set of this force on ``positions`` (diagnostic)."""
+        pos = np.ascontiguousarray(positions, np.float64)
+        cap = cap or max(1024, pos.shape[0] * 1200)
+        out = np.zeros((cap, 2), np.int32)
+        cnt = C.c_longlong(0)
+        check(_lib.load().pmgpu_get_pairs(self.topo.handle, self.handle, pos.ctypes.data_as(_VP), C.byref(cnt),
+                                          out.ctypes.data_as(_VP), cap), self.topo.handle)
+        return out[: cnt.value]
+
+
+class NonbondedPMEwaldSystemForce(SystemForce):
+    keyword = "PMEwald"
+
+    @property
+    def alpha(self) -> float:
+        a = C.c_double(0.0)
+        check(_lib.load().pmgpu_pme_alpha(self.handle, C.byref(a)))
+        return a.value
+
+
+def evaluate_group(topo: Topology, forces, positions, force_accum, energies: ScalarStructure):
+    """ForceGroup::evaluateSystemForces (forces/ForceGroup.cpp:43-96) for GPU
+    forces: one host->device copy, all forces, one device->host copy."""
+    lib = _lib.load()
+    pos = np.ascontiguousarray(positions, np.float64)
+    if force_accum.dtype != np.float64 or not force_accum.flags.c_contiguous:
+        raise ValueError("forces must be a C-contiguous float64 (N, 3) array")
+    if pos.shape != (topo.n_atoms, 3) or force_accum.shape != (topo.n_atoms, 3):
+        raise ValueError("positions / forces must have shape (N, 3)")
+    arr = (_VP * len(forces))(*[f.handle for f in forces])
+    e = _lib.Energies()
+    flags = _lib.FLAG_VIRIAL if energies.virial else 0
+    check(lib.pmgpu_evaluate(topo.handle, len(forces), arr, pos.ctypes.data_as(_VP),
+                             force_accum.ctypes.data_as(_VP), C.byref(e), flags), topo.handle)
+    energies.lennard_jones += e.lennard_jones
+    energies.coulomb += e.coulomb
+    if energies.virial:
+        energies.virial_tensor += np.array(list(e.virial))
+
+
+# --------------------------------------------------------------------------
+# keyword parsing
+# --------------------------------------------------------------------------
+_POTENTIALS = ("LennardJones", "Coulomb", "CoulombEwaldReal")
+_SWITCHES = ("Universal", "Cutoff", "C1", "C2", "Shift")
+
+
+@dataclass
+class _Param:
+    keyword: str
+    default: object = None
+
+
+def _switch_params(sw):
+    # getParameters() of each switching function
+    return {"C2": [_Param("-switchon"), _Param("-cutoff")], "C1": [_Param("-cutoff")],
+            "Cutoff": [_Param("-cutoff")], "Shift": [_Param("-cutoff")], "Universal": []}[sw]
+
+
+def _pot_params(pot):
+    return [_Param("-alpha")] if pot == "CoulombEwaldReal" else []
+
+
+def _parse_values(tokens, params):
+    """Positional keyword matching of ForceFactoryDetails::doMake
+    (frontend/ForceFactoryDetails.cpp:192-249): for each parameter in
+    getParameters() order, scan forward for its keyword (wrapping around once)
+    and take the next token; an empty keyword takes the token after the
+    previous match."""
+    values = []
+    pos = 0
+    found_last = False
+    for p in params:
+        val = None
+        if p.keyword == "":
+            if found_last and pos < len(tokens):
+                val = tokens[pos]
+                pos += 1
+        else:
+            scanned = 0
+            k = pos
+            while scanned < len(tokens) + 1:
+                if k >= len(tokens):
+                    k = 0
+                if k < len(tokens) and tokens[k].lower() == p.keyword.lower() and k + 1 < len(tokens):
+                    val = tokens[k + 1]
+                    pos = k + 2
+                    break
+                k += 1
+                scanned += 1
+        found_last = val is not None
+        if val is None:
+            val = p.default
+        values.append(val)
+    return values
+
+
+def parse_definition(definition: str) -> dict:
+    """Parses a force definition string into its parameters (no GPU needed).
+
+    Returns ``{"kind": "cut", "terms": [(sw, pot, switchon, cutoff, alpha)],
+    "algo_cutoff": rc}`` or ``{"kind": "pme", "real": .., "reciprocal": ..,
+    "correction": .., "grid": (nx, ny, nz), "order": P, "cutoff": rc,
+    "accuracy": a, "alpha": alpha}``; raises ValueError with the
+    reference's kind of message when the definition does not match.
+    """
+    toks = definition.split()
+    if toks and toks[0].lower() == "force":
+        toks = toks[1:]
+    names, sws, algorithm, interp, flags, rest = [], [], None, None, set(), []
+    i = 0
+    while i < len(toks):
+        t = toks[i]
+        if t in _POTENTIALS:
+            names.append(t)
+        elif t == "-switchingFunction" and i + 1 < len(toks):
+            sws.append(toks[i + 1]); i += 1
+        elif t == "-algorithm" and i + 1 < len(toks):
+            algorithm = toks[i + 1]; i += 1
+        elif t == "-interpolation" and i + 1 < len(toks):
+            interp = toks[i + 1]; i += 1
+        elif t in ("-real", "-reciprocal", "-correction"):
+            flags.add(t[1:])
+        else:
+            rest.append(t)
+        i += 1
+    if algorithm == "NonbondedCutoff":
+        if not 1 <= len(names) <= 2 or len(sws) != len(names) or any(s not in _SWITCHES for s in sws):
+            raise ValueError(f"Could not find a complete match for '{definition}'")
+        params = []
+        for n, s in zip(names, sws):
+            # OneAtomPair[Two]::getParameters order: force1, switch1, force2, switch2
+            params += _pot_params(n) + _switch_params(s)
+        params.append(_Param("-cutoff"))
+        vals = _parse_values(rest, params)
+        if any(v is None for v in vals):
+            raise ValueError(f"force {definition}: missing parameter(s)")
+        vals = [float(v) for v in vals]
+        terms, k = [], 0
+        for n, s in zip(names, sws):
+            alpha = on = rc = 0.0
+            if n == "CoulombEwaldReal":
+                alpha = vals[k]; k += 1
+            if s == "C2":
+                on, rc = vals[k], vals[k + 1]; k += 2
+            elif s in ("C1", "Cutoff", "Shift"):
+                rc = vals[k]; k += 1
+            terms.append((s, n, on, rc, alpha))
+        return {"kind": "cut", "terms": terms, "algo_cutoff": vals[k]}
+    if algorithm == "PMEwald":
+        if names != ["Coulomb"] or (interp or "BSpline") != "BSpline":
+            raise ValueError(f"Could not find a complete match for '{definition}'")
+        params = [_Param("-gridsize"), _Param(""), _Param(""), _Param("-cutoff"),
+                  _Param("-order", 4), _Param("-accuracy", 1e-6), _Param("-alpha", -1.0)]
+        vals = _parse_values(rest, params)
+        if any(v is None for v in vals):
+            raise ValueError(f"force {definition}: missing parameter(s)")
+        return {"kind": "pme", "real": int("real" in flags), "reciprocal": int("reciprocal" in flags),
+                "correction": int("correction" in flags), "grid": tuple(int(v) for v in vals[:3]),
+                "cutoff": float(vals[3]), "order": int(vals[4]), "accuracy": float(vals[5]),
+                "alpha": float(vals[6])}
+    raise ValueError(f"Could not find a complete match for '{definition}'")
+
+
+class ForceFactory:
+    """``ForceFactory::make`` for the GPU nonbonded forces."""
+
+    @staticmethod
+    def make(topo: Topology, definition: str, precision: str = "mixed") -> SystemForce:
+        lib = _lib.load()
+        spec = parse_definition(definition)
+        prec = _lib.PRECISION[precision]
+        h = _VP()
+        if spec["kind"] == "cut":
+            cp = _lib.CutoffParams()
+            cp.n_terms = len(spec["terms"])
+            for t, (s, n, on, rc, alpha) in enumerate(spec["terms"]):
+                cp.pot[t] = _lib.POT[n]
+                cp.sw[t] = _lib.SW[s]
+                cp.switchon[t] = on
+                cp.cutoff[t] = rc
+                cp.alpha[t] = alpha
+            cp.algorithm_cutoff = spec["algo_cutoff"]
+            cp.precision = prec
+            check(lib.pmgpu_cutoff_create(topo.handle, C.byref(cp), C.byref(h)), topo.handle)
+            ident = (" ".join(t[1] for t in spec["terms"]) +
+                     "".join(f" -switchingFunction {t[0]}" for t in spec["terms"]) + " -algorithm NonbondedCutoff")
+            return NonbondedCutoffSystemForce(topo, h, ident, spec)
+        pp = _lib.PmeParams()
+        pp.real, pp.reciprocal, pp.correction = spec["real"], spec["reciprocal"], spec["correction"]
+        for k in range(3):
+            pp.grid[k] = spec["grid"][k]
+        pp.cutoff, pp.order, pp.accuracy, pp.alpha = spec["cutoff"], spec["order"], spec["accuracy"], spec["alpha"]
+        pp.precision = prec
+        check(lib.pmgpu_pme_create(topo.handle, C.byref(pp), C.byref(h)), topo.handle)
+        ident = ("Coulomb -algorithm PMEwald" + "".join(f" -{f}" for f in ("real", "reciprocal", "correction")
+                                                       if spec[f]) + " -interpolation BSpline")
+        return NonbondedPMEwaldSystemForce(topo, h, ident, spec)

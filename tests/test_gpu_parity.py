@@ -1,0 +1,247 @@
+"""GPU parity of libpmgpu against the oracle (the CPU restatement that is
+itself pinned bit-exact to the reference, see test_oracle_golden.py).
+
+Tolerances (from the reference-parity requirements of this path):
+  * cell assignment and within-cutoff pair set: bit-exact;
+  * FP64 kernels: forces within 1e-9 of the force RMS, energies / virial
+    within 1e-10 relative;
+  * mixed precision: relative RMS force error <= 1e-5, total energy and
+    virial within 1e-7 relative of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from protomol_b200 import _lib
+from protomol_b200 import forces as F
+from protomol_b200 import systems, workloads
+
+pytestmark = pytest.mark.gpu
+
+MIXED_FORCE_RTOL = 1e-5
+MIXED_ENERGY_RTOL = 1e-7
+FP64_FORCE_RTOL = 1e-9
+FP64_ENERGY_RTOL = 1e-10
+
+
+def gpu_eval(system, defs, precision, positions=None, virial=True):
+    topo = F.Topology(system)
+    fs = [F.ForceFactory.make(topo, d, precision) for d in defs]
+    pos = system.positions if positions is None else positions
+    out = np.zeros((system.n_atoms, 3))
+    e = F.ScalarStructure(virial=virial)
+    F.evaluate_group(topo, fs, pos, out, e)
+    return topo, fs, out, e
+
+
+def rel_rms(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def small_chain():
+    return systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+
+
+CASES = {
+    "water216_c2": (systems.water_box_216, workloads.water216().forces),
+    "small_split_pme": (small_chain, [workloads.lj_ewald_split(7, 9, 0.35),
+                                      workloads.pme_reciprocal((24, 24, 24), 9, 0.35)]),
+    "small_c1lj_ewald": (small_chain, ["LennardJones CoulombEwaldReal -switchingFunction C1 -switchingFunction Cutoff "
+                                       "-algorithm NonbondedCutoff -cutoff 9 -alpha 0.35 -cutoff 9 -cutoff 9"]),
+    "small_c2lj_c1coul": (small_chain, ["LennardJones Coulomb -switchingFunction C2 -switchingFunction C1 "
+                                        "-algorithm NonbondedCutoff -switchon 7 -cutoff 10 -cutoff 8 -cutoff 10"]),
+    "small_c2lj_shiftcoul": (small_chain, ["LennardJones Coulomb -switchingFunction C2 -switchingFunction Shift "
+                                           "-algorithm NonbondedCutoff -switchon 7 -cutoff 9 -cutoff 10 -cutoff 10"]),
+    "small_cutlj_cutewald": (small_chain, ["LennardJones CoulombEwaldReal -switchingFunction Cutoff "
+                                           "-switchingFunction Cutoff -algorithm NonbondedCutoff -cutoff 8 -alpha 0.35 "
+                                           "-cutoff 9 -cutoff 9"]),
+    "small_c2_fused": (small_chain, ["LennardJones Coulomb -switchingFunction C2 -switchingFunction C2 -algorithm "
+                                     "NonbondedCutoff -switchon 8 -cutoff 9 -switchon 6 -cutoff 9 -cutoff 9"]),
+    "small_shift_lj": (small_chain, ["LennardJones -switchingFunction Shift -algorithm NonbondedCutoff -cutoff 9 "
+                                     "-cutoff 9"]),
+    "small_cutoff_coulomb": (small_chain, ["Coulomb -switchingFunction Cutoff -algorithm NonbondedCutoff -cutoff 9 "
+                                           "-cutoff 9"]),
+    "small_pme_default_alpha": (small_chain, ["Coulomb -algorithm PMEwald -reciprocal -correction -interpolation "
+                                              "BSpline -gridsize 25 27 30 -cutoff 9"]),
+    "smallbox_wrap": (lambda: systems.water_box(100, seed=7), workloads.water_box_workload(100, 7).forces),
+}
+
+
+def energy_scale(r):
+    return abs(r["lennard_jones"]) + abs(r["coulomb"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_forces_energies_virial_against_oracle(name, precision):
+    factory, defs = CASES[name]
+    s = factory()
+    ref = oracle.evaluate(s, [F.parse_definition(d) for d in defs])
+    _, _, f, e = gpu_eval(s, defs, precision)
+    scale = energy_scale(ref)
+    vscale = np.abs(ref["virial"]).max()
+    if precision == "fp64":
+        rms = np.sqrt((ref["forces"] ** 2).sum(1).mean())
+        assert np.abs(f - ref["forces"]).max() <= FP64_FORCE_RTOL * rms
+        assert abs(e.lennard_jones - ref["lennard_jones"]) <= FP64_ENERGY_RTOL * scale
+        assert abs(e.coulomb - ref["coulomb"]) <= FP64_ENERGY_RTOL * scale
+        assert np.abs(e.virial_tensor - ref["virial"]).max() <= FP64_ENERGY_RTOL * vscale
+    else:
+        assert rel_rms(f, ref["forces"]) <= MIXED_FORCE_RTOL
+        etot = e.lennard_jones + e.coulomb
+        rtot = ref["lennard_jones"] + ref["coulomb"]
+        assert abs(etot - rtot) <= MIXED_ENERGY_RTOL * scale
+        assert np.abs(e.virial_tensor - ref["virial"]).max() <= MIXED_ENERGY_RTOL * max(vscale, 1.0) * 10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_chain14281_metric_config(chain14281, precision):
+    w = workloads.chain14281()
+    ref = oracle.evaluate(chain14281, [F.parse_definition(d) for d in w.forces])
+    _, _, f, e = gpu_eval(chain14281, w.forces, precision)
+    err = rel_rms(f, ref["forces"])
+    scale = energy_scale(ref)
+    etot = e.lennard_jones + e.coulomb
+    rtot = ref["lennard_jones"] + ref["coulomb"]
+    print(f"\n{precision}: force rel RMS {err:.3e}  total energy rel {abs(etot - rtot) / abs(rtot):.3e} "
+          f"(scale {abs(etot - rtot) / scale:.3e})  LJ {e.lennard_jones:.9f}/{ref['lennard_jones']:.9f} "
+          f"Coul {e.coulomb:.9f}/{ref['coulomb']:.9f}")
+    if precision == "fp64":
+        assert err <= FP64_FORCE_RTOL
+        assert abs(etot - rtot) <= FP64_ENERGY_RTOL * scale
+    else:
+        assert err <= MIXED_FORCE_RTOL
+        assert abs(etot - rtot) <= MIXED_ENERGY_RTOL * scale
+
+
+@pytest.mark.parametrize("name", ["water_box_216", "chain_in_water_14281"])
+def test_cell_assignment_bit_exact(name):
+    s = getattr(systems, name)()
+    for pos in (s.positions, s.positions + np.array([40.1, -77.7, 13.3])):
+        topo, _, _, _ = gpu_eval(s, [workloads.water216().forces[0]], "mixed", positions=pos)
+        cells, dims = topo.cells()
+        ocells, odims, _ = oracle.cell_assign(s, pos)
+        assert dims == odims
+        assert np.array_equal(cells, ocells)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["water216", "chain14281", "wrap", "c2_fused"])
+def test_pair_set_bit_exact(case, precision, chain14281):
+    if case == "water216":
+        s, d = systems.water_box_216(), workloads.water216().forces[0]
+    elif case == "chain14281":
+        s, d = chain14281, workloads.chain14281().forces[0]
+    elif case == "wrap":
+        s, d = systems.water_box(100, seed=7), workloads.water_box_workload(100, 7).forces[0]
+    else:
+        s, d = small_chain(), CASES["small_c2_fused"][1][0]
+    topo = F.Topology(s)
+    force = F.ForceFactory.make(topo, d, precision)
+    gp = force.pairs(s.positions)
+    op = oracle.evaluate(s, [F.parse_definition(d)], want_pairs=True)["pairs"]
+    key = lambda p: np.sort(p[:, 0].astype(np.int64) * s.n_atoms + p[:, 1])
+    assert len(gp) == len(op)
+    assert np.array_equal(key(gp), key(op))
+
+
+def test_pairs_near_the_cutoff_are_decided_in_fp64():
+    """Atoms placed at distances rc(1 +- 1e-9): the FP32 distance cannot tell
+    them apart, the FP64 re-decision must."""
+    s = systems.water_box_216()
+    pos = s.positions.copy()
+    rc = 9.0
+    rng = np.random.default_rng(5)
+    for k, i in enumerate(range(0, 600, 60)):
+        j = i + 30
+        direction = rng.normal(size=3)
+        direction /= np.linalg.norm(direction)
+        pos[j] = pos[i] + direction * rc * (1 + (1e-9 if k % 2 else -1e-9))
+    d = workloads.water216().forces[0]
+    topo = F.Topology(s)
+    force = F.ForceFactory.make(topo, d, "mixed")
+    gp = force.pairs(pos)
+    op = oracle.evaluate(s, [F.parse_definition(d)], positions=pos, want_pairs=True)["pairs"]
+    key = lambda p: np.sort(p[:, 0].astype(np.int64) * s.n_atoms + p[:, 1])
+    assert np.array_equal(key(gp), key(op))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_deterministic_and_accumulating(precision, small_chain):
+    defs = CASES["small_split_pme"][1]
+    topo = F.Topology(small_chain)
+    fs = [F.ForceFactory.make(topo, d, precision) for d in defs]
+    out1 = np.zeros((small_chain.n_atoms, 3))
+    e1 = F.ScalarStructure()
+    F.evaluate_group(topo, fs, small_chain.positions, out1, e1)
+    out2 = np.ones((small_chain.n_atoms, 3))
+    e2 = F.ScalarStructure()
+    e2.lennard_jones = 5.0
+    F.evaluate_group(topo, fs, small_chain.positions, out2, e2)
+    # fixed-point sums are order independent: bitwise identical reruns
+    assert np.array_equal(out2 - 1.0, (out1 + 1.0) - 1.0)
+    assert e2.lennard_jones - 5.0 == pytest.approx(e1.lennard_jones, rel=1e-15)
+    out3 = np.zeros((small_chain.n_atoms, 3))
+    F.evaluate_group(topo, fs, small_chain.positions, out3, F.ScalarStructure())
+    assert np.array_equal(out1, out3)
+
+
+def test_virial_only_when_requested(small_chain):
+    _, _, _, e = gpu_eval(small_chain, CASES["small_split_pme"][1], "mixed", virial=False)
+    assert not e.virial_tensor.any()
+
+
+def test_overlapping_atoms_report_overflow():
+    s = systems.water_box_216()
+    pos = s.positions.copy()
+    pos[3] = pos[0]          # two oxygens of different waters on top of each other
+    with pytest.raises(_lib.PmgpuError) as ei:
+        gpu_eval(s, workloads.water216().forces, "mixed", positions=pos)
+    assert ei.value.code == 3
+
+
+def test_empty_and_sparse_systems():
+    s = systems.water_box_216()
+    empty = s.copy()
+    empty.positions = np.zeros((0, 3))
+    empty.scaled_charge = np.zeros(0)
+    empty.atom_type = np.zeros(0, np.int32)
+    empty.molecule = np.zeros(0, np.int32)
+    empty.mass = np.zeros(0)
+    empty.exclusions = np.zeros((0, 3), np.int32)
+    empty.exclusion_check = np.zeros(0, np.int32)
+    _, _, f, e = gpu_eval(empty, workloads.water216().forces, "mixed")
+    assert f.shape == (0, 3) and e.lennard_jones == 0.0 and e.coulomb == 0.0
+    # three waters in the big box: almost every cell empty (ragged cells)
+    sparse = s.copy()
+    keep = np.arange(9)
+    sparse.positions = s.positions[keep] * np.array([1.0, 1.0, 1.0])
+    sparse.positions[3:6] += 2.0
+    sparse.scaled_charge = s.scaled_charge[keep]
+    sparse.atom_type = s.atom_type[keep]
+    sparse.molecule = s.molecule[keep]
+    sparse.mass = s.mass[keep]
+    m = (s.exclusions[:, 0] < 9) & (s.exclusions[:, 1] < 9)
+    sparse.exclusions = s.exclusions[m]
+    sparse.exclusion_check = s.exclusion_check[m]
+    for precision in ("fp64", "mixed"):
+        ref = oracle.evaluate(sparse, [F.parse_definition(d) for d in workloads.water216().forces])
+        _, _, f, e = gpu_eval(sparse, workloads.water216().forces, precision)
+        assert rel_rms(f, ref["forces"]) <= MIXED_FORCE_RTOL
+
+
+def test_pme_rejects_what_the_reference_rejects(small_chain):
+    topo = F.Topology(small_chain)
+    for bad in ("Coulomb -algorithm PMEwald -reciprocal -correction -interpolation BSpline -gridsize 24 24 24 "
+                "-cutoff 9 -order 3",
+                "Coulomb -algorithm PMEwald -reciprocal -correction -interpolation BSpline -gridsize 2 24 24 -cutoff 9"):
+        with pytest.raises(_lib.PmgpuError) as ei:
+            F.ForceFactory.make(topo, bad)
+        assert ei.value.code == 1
+
+
+def test_pme_default_alpha_matches_reference_bisection(small_chain):
+    topo = F.Topology(small_chain)
+    f = F.ForceFactory.make(topo, CASES["small_pme_default_alpha"][1][0])
+    r = oracle.evaluate(small_chain, [F.parse_definition(CASES["small_pme_default_alpha"][1][0])])
+    assert f.alpha == r["alpha"] == systems.ewald_alpha(9.0)
