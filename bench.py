@@ -265,19 +265,31 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         t_e2e = float(t[0])
 
-    # roofline of the dominant kernel (pair kernel) from a separate timing
-    pair_ms = pair_kernel_ms(lib, topo, mixed[0], dpos, dfor, den, stream, flush, torch)
+    # per-phase device times (CUDA events on the library's stream) over a
+    # profiled copy of the timed loop, for the rooflines
+    phases = profile_phases(lib, topo, mixed, step, flush, stream, torch, max(50, min(args.steps, 400)))
     peaks, peak_src = measured_peaks()
-    n_pairs = 5212013   # within-cutoff pairs of this input (oracle pair set)
+    # within-cutoff pair set of this input, recorded by the pair kernel itself
+    # (bit-exact with the oracle's, tests/test_gpu_parity.py)
+    n_pairs = int(len(mixed[0].pairs(s.positions)))
     flops_per_pair = 95
     fp32_peak = N_SMS * FP32_LANES_PER_SM * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    pair_ms = phases["pair"]
     achieved = n_pairs * flops_per_pair / (pair_ms * 1e-3) / 1e12
     roofline = {"bound": "fp32", "kernel": "k_pair_mixed<LJ C2 + EwaldReal Cutoff>",
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                 "traffic": None, "launch_ms": pair_ms,
                 "peak_source": f"nominal FP32 CUDA-core rate at sm_max_mhz of MEASURED_PEAKS.json ({peak_src}): "
                                "148 SMs x 128 lanes x 2 flop",
-                "algorithmic": f"{n_pairs} pairs x {flops_per_pair} flop"}
+                "algorithmic": f"{n_pairs} pairs x {flops_per_pair} flop per launch"}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    kx = 64
+    kzh = kx // 2 + 1
+    pme_bytes = {"pme_spread": 16 * n + 4 * kx ** 3, "pme_fft": 2 * 2 * 8 * kx * kx * kzh,
+                 "pme_gather": 4 * kx ** 3 + 16 * n + 12 * n}
+    pme_roof = {k: {"achieved_gbs": b / (phases[k] * 1e-3) / 1e9, "peak_gbs": hbm,
+                    "frac": b / (phases[k] * 1e-3) / 1e9 / hbm, "bytes": b, "launch_ms": phases[k]}
+                for k, b in pme_bytes.items() if phases.get(k)}
 
     if rank == 0:
         value = world * 1000.0 / t_local
@@ -294,6 +306,8 @@ def main():
                     "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 88},
             "gpu_launches": int(launches),
             "roofline": roofline,
+            "phases_ms": phases,
+            "pme_roofline_hbm": pme_roof,
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline:
@@ -304,26 +318,21 @@ def main():
         pg.destroy_process_group()
 
 
-def pair_kernel_ms(lib, topo, force, dpos, dfor, den, stream, flush, torch, reps=50):
-    """Average duration of one cutoff-force evaluation (binning + pair kernel
-    + finalize) minus binning alone is not separable from outside; time the
-    cutoff force alone as the pair-kernel bound."""
-    VP = C.c_void_p
-    arr = (VP * 1)(force.handle)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
-    for _ in range(5):
-        lib.pmgpu_evaluate_device(topo.handle, 1, arr, VP(dpos.data_ptr()), VP(dfor.data_ptr()),
-                                  VP(den.data_ptr()), 1)
-    torch.cuda.synchronize()
+def profile_phases(lib, topo, forces, step, flush, stream, torch, steps):
+    """Average device milliseconds per evaluation phase: the library records
+    CUDA events around each phase on its own stream (profiling mode)."""
+    from protomol_b200 import _lib
+    _lib.check(lib.pmgpu_set_profiling(topo.handle, 1), topo.handle)
     with torch.cuda.stream(stream):
-        for k in range(reps):
+        for _ in range(steps):
             flush.zero_()
-            evs[k][0].record(stream)
-            lib.pmgpu_evaluate_device(topo.handle, 1, arr, VP(dpos.data_ptr()), VP(dfor.data_ptr()),
-                                      VP(den.data_ptr()), 1)
-            evs[k][1].record(stream)
-    torch.cuda.synchronize()
-    return float(np.mean([a.elapsed_time(b) for a, b in evs]))
+            step(forces)
+    ms = (C.c_double * 8)()
+    n = C.c_longlong(0)
+    _lib.check(lib.pmgpu_phase_times(topo.handle, ms, 8, C.byref(n)), topo.handle)
+    _lib.check(lib.pmgpu_set_profiling(topo.handle, 0), topo.handle)
+    evals = max(int(n.value), 1)
+    return {name: ms[k] / evals for k, name in enumerate(_lib.PHASES)}
 
 
 if __name__ == "__main__":

@@ -122,6 +122,8 @@ typedef struct {
 /* Replaces: constructing Topology<PeriodicBoundaryConditions, CubicCellManager>
  * (topology/Topology.h:19-72). Selects the CUDA device and creates a stream. */
 int pmgpu_system_create(int device, pmgpu_system** out);
+/* Also destroys every force still alive on the system; do not call
+ * pmgpu_force_destroy on those afterwards. */
 int pmgpu_system_destroy(pmgpu_system* sys);
 
 /* Replaces the GenericTopology members the nonbonded forces read
@@ -184,6 +186,18 @@ void* pmgpu_stream(pmgpu_system* sys);
 
 /* Number of kernels the library launched since the system was created. */
 long long pmgpu_launch_count(pmgpu_system* sys);
+
+/* Profiling mode: while enabled, every evaluation records CUDA events around
+ * its phases (and is not replayed from a CUDA graph).  Enabling resets the
+ * accumulated times.  Replaces the reference's TimerStatistic / "force time"
+ * wrappers (base/TimerStatistic.h:19-31, forces/SystemTimeForce.cpp). */
+int pmgpu_set_profiling(pmgpu_system* sys, int enable);
+
+/* Accumulated device milliseconds per phase since profiling was enabled:
+ * ms[0] binning, [1] cutoff pair kernels, [2] PME correction, [3] PME
+ * spread, [4] PME FFT + convolution, [5] PME gather, [6] finalize + energy
+ * reduction; *evals = number of profiled evaluations.  Synchronizes. */
+int pmgpu_phase_times(pmgpu_system* sys, double* ms, int n, long long* evals);
 
 /* Copies the last error message (NUL-terminated) into buf. */
 int pmgpu_last_error(pmgpu_system* sys, char* buf, int len);

@@ -122,11 +122,13 @@ __device__ __forceinline__ void fixed_add3(unsigned long long* base, double x, d
 }
 
 // ---- energy / virial partial records ---------------------------------------
-// 11 doubles: LENNARDJONES, COULOMB, VIRIALXX..VIRIALZZ.
+// 11 components: LENNARDJONES, COULOMB, VIRIALXX..VIRIALZZ.  Records are
+// stored component-major: component k of record r at erec[k * stride + r],
+// so the final reduction reads each component contiguously.
 constexpr int kERec = 11;
 
 template <int NW>
-__device__ __forceinline__ void block_reduce_store(double (&v)[kERec], double* out_rec)
+__device__ __forceinline__ void block_reduce_store(double (&v)[kERec], double* erec, int stride, int rec)
 {
     // warp reduce
     for (int k = 0; k < kERec; ++k)
@@ -139,7 +141,21 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[kERec], double* o
     if (threadIdx.x < kERec) {
         double s = 0.0;
         for (int q = 0; q < NW; ++q) s += red[q][threadIdx.x];
-        out_rec[threadIdx.x] = s;
+        erec[(size_t)threadIdx.x * stride + rec] = s;
+    }
+}
+
+// one record per warp, no block barrier (warps of a block finish unevenly)
+__device__ __forceinline__ void warp_reduce_store(double (&v)[kERec], double* erec, int stride, int rec)
+{
+    for (int k = 0; k < kERec; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    int lane = threadIdx.x & 31;
+    if (lane < kERec) {
+        double s = v[0];
+#pragma unroll
+        for (int k = 1; k < kERec; ++k) if (lane == k) s = v[k];
+        erec[(size_t)lane * stride + rec] = s;
     }
 }
 

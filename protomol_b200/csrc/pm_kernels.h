@@ -25,22 +25,36 @@ struct BinArgs {
     int* tmp;                   // N
     int* sorted;                // N: original index per sorted slot
     int* slot_of;               // N: sorted slot per original index
-    float4* spos;               // N
+    float4* spos;               // N: FP32 (hi) cell-relative x, y, z and charge
+    float4* slo;                // N: FP32 remainders (lo) of the same four values
     int4* smeta;                // N
     double4* spos64;            // N (raw FP64 position + charge) or null
+    int* skey;                  // N: Morton key of the cell-relative position
+    int* cstart;                // ncell + 1: first cluster of each cell
+    int* ccell;                 // cluster -> cell
+    float4* cbox;               // 2 per cluster: bounding box lo, hi
+    int ncl_cap;                // capacity of ccell / cbox
     int* status;
 };
+constexpr int kCluster = 8;     // atoms per cluster (z-sorted slab of a cell)
 // Cell binning by counting sort (K1): buildCellLists' cell of every atom in
 // exact FP64, CSR cell offsets, stable (ascending index) order within a cell.
 int launch_bin(const BinArgs& a, cudaStream_t s, long long* launches);
 
 // ---------------------------------------------------------------- pair force
+// FP32 constants of one term; the *_lo members are the FP32 remainders of
+// constants that multiply every pair (their rounding would otherwise bias
+// the energy sum the same way for all pairs)
 struct TermF {
     int pot, sw;
     float cut2, on2, s1, s2, s3;          // C2
+    float s1_lo, s3_lo;
     float c1_15_1, c1_05_3, c1_15_3;      // C1
+    float c1_15_1_lo, c1_05_3_lo, c1_15_3_lo;
     float sh_a, sh_b;                      // Shift
+    float sh_a_lo, sh_b_lo;
     float alpha, two_alpha_pi;             // EwaldReal
+    float alpha_lo, two_alpha_pi_lo;
 };
 
 struct TermD {
@@ -54,7 +68,11 @@ struct TermD {
 struct PairArgs {
     // cell-sorted system
     const int* start;
+    const int* cstart;           // first 8-atom cluster of each cell
+    const int* ccell;            // cluster -> cell
+    const float4* cbox;          // cluster bounding boxes (lo, hi)
     const float4* spos;
+    const float4* slo;
     const int4* smeta;
     const double4* spos64;
     const double* pos;           // raw positions, original order (exact rechecks)
@@ -63,18 +81,29 @@ struct PairArgs {
     const uint32_t* xmod;
     const int* xrow;             // N + 1
     const int2* xent;            // (partner, class) for deltas > window
-    // LJ table
-    const float4* ljf;
+    // LJ table: FP32 hi/lo pairs {A_hi, B_hi, A_lo, B_lo} for normal pairs
+    // (ljn) and for 1-4 modified pairs (ljm); FP64 {A, B, A14, B14} (ljd)
+    const float4* ljn;
+    const float4* ljm;
     const double4* ljd;
     int n_types;
     // enumeration
     const int4* deltas;          // nd neighbour-cell deltas (reference order)
     const float4* doff;          // FP32 offset delta * real cell size
     int nd;
+    // the mixed kernel's half shell: the positive half of the deltas (each
+    // unordered cell pair once, every cell the same work), or in the
+    // small-grid mode the reference's deltas with the B > A rule
+    const int4* hdeltas;
+    const float4* hoff;          // FP32 hi offsets
+    const float4* hoff_lo;       // FP32 remainders of the offsets
+    int nh;
+    int half_rule;               // 1: skip B < A (small-grid mode)
     CellGrid grid;
     Pbc pbc;
     int wrap;                    // per-pair minimal image in FP32 (small grids)
     float lx, ly, lz, ilx, ily, ilz;
+    float lx_lo, ly_lo, lz_lo;   // FP32 remainders of the box lengths
     // physics
     int n_terms;
     TermF tf[2];
@@ -88,7 +117,8 @@ struct PairArgs {
     // outputs
     unsigned long long* facc;    // 3 per sorted slot
     double scale;
-    double* erec;                // energy records, one per block
+    double* erec;                // energy records (component-major, see kERec)
+    int erec_stride;
     int* status;
     int* rec_pairs;              // pair recording (diagnostic) or null
     unsigned long long* rec_count;
@@ -100,6 +130,8 @@ int pair_combo_id(int n_terms, const int* pot, const int* sw);
 int launch_pair_mixed(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches);
 int launch_pair_fp64(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches);
 int pair_blocks(const CellGrid& g, int nd);
+// blocks of the mixed kernel (4 warps, one energy record per warp)
+int pair_blocks_mixed(const CellGrid& g, int nh);
 
 // ---------------------------------------------------------------- PME
 struct PmeArgs {
@@ -125,11 +157,16 @@ struct PmeArgs {
     double scale;
     double qscale;               // fixed-point scale of the charge grid
     double* erec;
+    int erec_stride;
     int* status;
     int virial;
 };
+constexpr int kStageSpread = 0, kStageFft = 1, kStageGather = 2;
+// One stage of the reciprocal term: K3 spread, the five FFT passes with the
+// fused convolution (K4/K5, writes energy records), or K6 gather.
 int launch_pme_reciprocal(const PmeArgs& a, int fp64, cudaStream_t s, long long* launches,
-                          double* erec_base, int* erec_used);
+                          double* erec_base, int* erec_used, int stage);
+void pme_init_attributes();
 
 struct CorrArgs {
     int n_excl;
@@ -143,14 +180,17 @@ struct CorrArgs {
     unsigned long long* facc;
     double scale;
     double* erec;
+    int erec_stride;
     int* status;
     int virial;
+    double const_energy;         // point self + charged-system energy (added once)
+    double const_virial;         // charged-system term on the virial diagonal
 };
 int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches, int* blocks_used);
 
 // ---------------------------------------------------------------- finalize
 int launch_finalize(int n, const unsigned long long* facc, const int* sorted, double inv_scale,
                     double* fout, cudaStream_t s, long long* launches);
-int launch_energy_reduce(const double* erec, int nrec, double* out, cudaStream_t s, long long* launches);
+int launch_energy_reduce(const double* erec, int stride, int nrec, double* out, cudaStream_t s, long long* launches);
 
 }  // namespace pm

@@ -136,41 +136,52 @@ __device__ __forceinline__ int excl_class(const PairArgs& p, int oi, int oj)
 }
 
 // ---------------------------------------------------------------- FP32 math
+// FP32 hi part and remainder of a double constant
+#define PM_HI(x) ((float)(x))
+#define PM_LO(x) ((float)((x) - (double)(float)(x)))
+
 __device__ __forceinline__ float poly5f(float ar)
 {
-    // poly5 (base/mathutilities.cpp:29-40), Abramowitz & Stegun 7.1.26
-    const float E1 = 0.254829592f, E2 = -0.284496736f, E3 = 1.421413741f,
-                E4 = -1.453152027f, E5 = 1.061405429f, PP = 0.3275911f;
-    float t = __frcp_rn(fmaf(PP, ar, 1.0f));
-    return t * (E1 + t * (E2 + t * (E3 + t * (E4 + t * E5))));
+    // poly5 (base/mathutilities.cpp:29-40), Abramowitz & Stegun 7.1.26.  The
+    // coefficients are the same for every pair, so their FP32 rounding is
+    // compensated (hi + lo) instead of biasing the real-space Ewald sum.
+    const double E1 = 0.254829592, E2 = -0.284496736, E3 = 1.421413741,
+                 E4 = -1.453152027, E5 = 1.061405429, PP = 0.3275911;
+    float t = __frcp_rn(fmaf(PM_HI(PP), ar, fmaf(PM_LO(PP), ar, 1.0f)));
+    // each remainder is added after the O(1) partial result it corrects
+    float h = fmaf(t, PM_HI(E5), PM_HI(E4)) + fmaf(t, PM_LO(E5), PM_LO(E4));
+    h = fmaf(t, h, PM_HI(E3)) + PM_LO(E3);
+    h = fmaf(t, h, PM_HI(E2)) + PM_LO(E2);
+    h = fmaf(t, h, PM_HI(E1)) + PM_LO(E1);
+    return t * h;
 }
 
+// qq is the compensated charge product (hi*hi exact inside the FMA plus the
+// hi*lo cross terms), so the FP32 rounding of each atom's charge cancels
 template <int POT>
 __device__ __forceinline__ void pot_f32(const PairArgs& p, const TermF& t, float r2, float rd2, float rinv,
-                                        float qi, float qj, int ti, int tj, int excl, float& e, float& f)
+                                        float qq, int ti, int tj, int excl, float& e, float& f)
 {
     if (POT == LJ) {
-        float4 par = __ldg(p.ljf + (size_t)ti * p.n_types + tj);
-        float A = excl == PMGPU_EXCL_MODIFIED ? par.z : par.x;
-        float B = excl == PMGPU_EXCL_MODIFIED ? par.w : par.y;
+        const float4* tab = excl == PMGPU_EXCL_MODIFIED ? p.ljm : p.ljn;
+        float4 par = __ldg(tab + (size_t)ti * p.n_types + tj);   // A_hi, B_hi, A_lo, B_lo
         float r6 = rd2 * rd2 * rd2;
         float r12 = r6 * r6;
-        float r6B = B * r6;
-        float r12A = A * r12;
+        float r6B = fmaf(par.y, r6, par.w * r6);
+        float r12A = fmaf(par.x, r12, par.z * r12);
         e = r12A - r6B;
         f = (12.0f * r12A - 6.0f * r6B) * rd2;
     } else if (POT == CO) {
-        e = qi * qj * rinv;
+        e = qq * rinv;
         if (excl == PMGPU_EXCL_MODIFIED) e *= p.csf;
         f = e * rd2;
     } else if (POT == EW) {
-        float qq = qi * qj;
         if (p.csfd != 1.0 && excl == PMGPU_EXCL_MODIFIED) qq *= p.csf;
         float r = r2 * rinv;
-        float ar = t.alpha * r;
+        float ar = fmaf(t.alpha, r, t.alpha_lo * r);     // compensated alpha
         float ex = qq * expf(-ar * ar);
         e = poly5f(ar) * ex * rinv;
-        f = (e + t.two_alpha_pi * ex) * rinv * rinv;
+        f = fmaf(t.two_alpha_pi, ex, fmaf(t.two_alpha_pi_lo, ex, e)) * rinv * rinv;
     } else {
         e = 0.f; f = 0.f;
     }
@@ -185,19 +196,22 @@ __device__ __forceinline__ void sw_f32(const TermF& t, float r2, float rinv, boo
         else if (r2 >= t.on2) {
             float c2 = t.cut2 - r2;
             float c4 = c2 * (t.s2 + 2.0f * r2);
-            v = t.s1 * (c2 * c4);
-            d = t.s3 * (c2 * c2 - c4);
+            float c24 = c2 * c4;
+            v = fmaf(t.s1, c24, t.s1_lo * c24);
+            float dd = c2 * c2 - c4;
+            d = fmaf(t.s3, dd, t.s3_lo * dd);
         } else v = 1.f;
     } else if (SW == SC1) {
         if (r2 > t.cut2) { v = 0.f; d = 0.f; return; }
         float dist = r2 * rinv;
-        v = 1.0f - dist * (t.c1_15_1 - r2 * t.c1_05_3);
-        d = -t.c1_15_1 * rinv + dist * t.c1_15_3;
+        float in = fmaf(-r2, t.c1_05_3, t.c1_15_1) + fmaf(-r2, t.c1_05_3_lo, t.c1_15_1_lo);
+        v = fmaf(-dist, in, 1.0f);
+        d = fmaf(dist, t.c1_15_3, -t.c1_15_1 * rinv) + fmaf(dist, t.c1_15_3_lo, -t.c1_15_1_lo * rinv);
     } else if (SW == SSH) {
         if (r2 > t.cut2) { v = 0.f; d = 0.f; return; }
-        float x = 1.0f - r2 * t.sh_a;
+        float x = fmaf(-r2, t.sh_a, 1.0f) - r2 * t.sh_a_lo;
         v = x * x;
-        d = t.sh_b * x;
+        d = fmaf(t.sh_b, x, t.sh_b_lo * x);
     } else if (SW == SCUT) {
         d = 0.f;
         v = inside ? 1.f : 0.f;
@@ -215,133 +229,7 @@ __device__ __forceinline__ double exact_d2(const PairArgs& p, int oi, int oj)
     return pbc_min_diff(p.pbc, pi[0], pi[1], pi[2], pj[0], pj[1], pj[2], dx, dy, dz);
 }
 
-template <int NT, int P0, int S0, int P1, int S1>
-__global__ void __launch_bounds__(128) k_pair_mixed(PairArgs p)
-{
-    constexpr bool kMod = sw_modifies(S0) || (NT > 1 && sw_modifies(S1));
-    constexpr bool kUse0 = S0 != SUN;
-    __shared__ float4 sjp[4][32];
-    __shared__ int4 sjm[4][32];
-    __shared__ float4 sjf[4][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int warps_total = gridDim.x * 4;
-    const int n_items = p.grid.ncell * (p.nd + 1);
-    const float g_lo = 1.0f - p.guard, g_hi = 1.0f + p.guard;
-    const float t0c2 = p.tf[0].cut2, t1c2 = NT > 1 ? p.tf[1].cut2 : 0.f;
-    double acc[kERec];
-    for (int k = 0; k < kERec; ++k) acc[k] = 0.0;
-
-    for (int item = blockIdx.x * 4 + w; item < n_items; item += warps_total) {
-        ItemGeom g = decode_item(p, item);
-        if (!g.valid) continue;
-        int sa = p.start[g.a], ea = p.start[g.a + 1];
-        int sb = p.start[g.b], eb = p.start[g.b + 1];
-        if (sa == ea || sb == eb) continue;
-        for (int ia = sa; ia < ea; ia += 32) {
-            int i = ia + lane;
-            bool vi = i < ea;
-            float4 pi = vi ? p.spos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            int4 mi = vi ? p.smeta[i] : make_int4(-1, 0, -2, 0);
-            float fix = 0.f, fiy = 0.f, fiz = 0.f;
-            for (int jb = g.same ? ia : sb; jb < eb; jb += 32) {
-                int j = jb + lane;
-                bool vj = j < eb;
-                sjp[w][lane] = vj ? p.spos[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-                sjm[w][lane] = vj ? p.smeta[j] : make_int4(-1, 0, -3, 0);
-                sjf[w][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
-                __syncwarp();
-                int nj = min(32, eb - jb);
-                bool diag = g.same && jb == ia;
-                float el = 0.f, ec = 0.f, vxx = 0.f, vxy = 0.f, vxz = 0.f, vyy = 0.f, vyz = 0.f, vzz = 0.f;
-                for (int t = 0; t < 32; ++t) {
-                    int jl = (lane + t) & 31;
-                    bool ok = vi && jl < nj && (!diag || jb + jl > i);
-                    if (!ok) continue;
-                    float4 pj = sjp[w][jl];
-                    float dx = (pj.x + g.ox) - pi.x;
-                    float dy = (pj.y + g.oy) - pi.y;
-                    float dz = (pj.z + g.oz) - pi.z;
-                    if (p.wrap) {
-                        dx -= p.lx * rintf(dx * p.ilx);
-                        dy -= p.ly * rintf(dy * p.ily);
-                        dz -= p.lz * rintf(dz * p.ilz);
-                    }
-                    float r2 = dx * dx + dy * dy + dz * dz;
-                    // pair test (with exact FP64 re-decision in the guard band)
-                    bool near = (r2 >= p.cut2f * g_lo && r2 <= p.cut2f * g_hi);
-                    if (S0 == SCUT && t0c2 != p.cut2f) near |= (r2 >= t0c2 * g_lo && r2 <= t0c2 * g_hi);
-                    if (NT > 1 && S1 == SCUT && t1c2 != p.cut2f) near |= (r2 >= t1c2 * g_lo && r2 <= t1c2 * g_hi);
-                    int4 mj = sjm[w][jl];
-                    bool in_pair, in0, in1;
-                    if (near) {
-                        double d2 = exact_d2(p, mi.x, mj.x);
-                        in_pair = !(d2 > p.cut2d);
-                        in0 = !(d2 > p.td[0].cut2);
-                        in1 = NT > 1 ? !(d2 > p.td[1].cut2) : false;
-                    } else {
-                        in_pair = !(r2 > p.cut2f);
-                        in0 = !(r2 > t0c2);
-                        in1 = NT > 1 ? !(r2 > t1c2) : false;
-                    }
-                    if ((kUse0 || (NT > 1 && S1 != SUN)) && !in_pair) continue;
-                    int excl = PMGPU_EXCL_NONE;
-                    if (mi.z == mj.z) {
-                        excl = excl_class(p, mi.x, mj.x);
-                        if (excl == PMGPU_EXCL_FULL) continue;
-                    }
-                    float rinv = rsqrtf(r2);
-                    rinv = rinv * fmaf(-0.5f * r2, rinv * rinv, 1.5f);
-                    float rd2 = rinv * rinv;
-                    float e0, f0, e1 = 0.f, f1 = 0.f;
-                    pot_f32<P0>(p, p.tf[0], r2, rd2, rinv, pi.w, pj.w, mi.y, mj.y, excl, e0, f0);
-                    if (NT > 1) pot_f32<P1>(p, p.tf[1], r2, rd2, rinv, pi.w, pj.w, mi.y, mj.y, excl, e1, f1);
-                    if (kMod) {
-                        float sv, sd;
-                        sw_f32<S0>(p.tf[0], r2, rinv, in0, sv, sd);
-                        f0 = f0 * sv - e0 * sd;
-                        e0 = e0 * sv;
-                        if (NT > 1) {
-                            sw_f32<S1>(p.tf[1], r2, rinv, in1, sv, sd);
-                            f1 = f1 * sv - e1 * sd;
-                            e1 = e1 * sv;
-                        }
-                    }
-                    if (P0 == LJ) el += e0; else ec += e0;
-                    if (NT > 1) { if (P1 == LJ) el += e1; else ec += e1; }
-                    float ft = NT > 1 ? f0 + f1 : f0;
-                    float fx = dx * ft, fy = dy * ft, fz = dz * ft;
-                    fix -= fx; fiy -= fy; fiz -= fz;
-                    float4 acc_j = sjf[w][jl];
-                    acc_j.x += fx; acc_j.y += fy; acc_j.z += fz;
-                    sjf[w][jl] = acc_j;
-                    if (p.virial) {
-                        vxx += fx * dx; vxy += fx * dy; vxz += fx * dz;
-                        vyy += fy * dy; vyz += fy * dz; vzz += fz * dz;
-                    }
-                    if (p.rec_pairs) {
-                        unsigned long long k = atomicAdd(p.rec_count, 1ull);
-                        if ((long long)k < p.rec_cap) {
-                            p.rec_pairs[2 * k] = min(mi.x, mj.x);
-                            p.rec_pairs[2 * k + 1] = max(mi.x, mj.x);
-                        }
-                    }
-                }
-                __syncwarp();
-                if (vj) {
-                    float4 fj = sjf[w][lane];
-                    fixed_add3(p.facc + 3 * (size_t)j, fj.x, fj.y, fj.z, p.scale, p.status);
-                }
-                acc[0] += el; acc[1] += ec;
-                acc[2] += vxx; acc[3] += vxy; acc[4] += vxz;
-                acc[5] += vxy; acc[6] += vyy; acc[7] += vyz;
-                acc[8] += vxz; acc[9] += vyz; acc[10] += vzz;
-                __syncwarp();
-            }
-            if (vi) fixed_add3(p.facc + 3 * (size_t)i, fix, fiy, fiz, p.scale, p.status);
-        }
-    }
-    block_reduce_store<4>(acc, p.erec + (size_t)blockIdx.x * kERec);
-}
+#include "pm_pair_mixed.cuh"
 
 // ---------------------------------------------------------------- FP64 math
 template <int POT>
@@ -510,10 +398,18 @@ __global__ void __launch_bounds__(128) k_pair_fp64(PairArgs p)
             if (vi) fixed_add3(p.facc + 3 * (size_t)i, fix, fiy, fiz, p.scale, p.status);
         }
     }
-    block_reduce_store<4>(acc, p.erec + (size_t)blockIdx.x * kERec);
+    block_reduce_store<4>(acc, p.erec, p.erec_stride, blockIdx.x);
 }
 
 // ---------------------------------------------------------------- launch
+int pair_blocks_mixed(const CellGrid& g, int nh)
+{
+    long long items = (long long)g.ncell * ((nh + 1 + kBatch - 1) / kBatch);
+    long long b = (items + 3) / 4;
+    long long cap = 148 * 16;
+    return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
 int pair_blocks(const CellGrid& g, int nd)
 {
     long long items = (long long)g.ncell * (nd + 1);

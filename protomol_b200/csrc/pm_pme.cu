@@ -198,24 +198,22 @@ __global__ void k_spread(PmeArgs a)
     R tx[kMaxOrder], dtx[kMaxOrder], ty[kMaxOrder], dty[kMaxOrder], tz[kMaxOrder], dtz[kMaxOrder];
     int i0, j0, k0;
     grid_point<R>(a, atom, i0, j0, k0, tx, dtx, ty, dty, tz, dtz);
-    R q = (R)a.q[atom];
+    // the charge multiplies in FP64: every atom of a type shares its charge,
+    // so an FP32-rounded charge would scale the whole grid systematically
+    const double qs = a.q[atom] * a.qscale;
     const int P = a.order;
     for (int i = 0; i < P; i++) {
-        R aa = q * tx[i];
         int i1 = (i + i0) % a.kx;
         for (int j = 0; j < P; j++) {
-            R ab = aa * ty[j];
+            R ab = tx[i] * ty[j];
             int j1 = (j + j0) % a.ky;
             size_t row = ((size_t)i1 * a.ky + j1) * a.kz;
             for (int k = 0; k < P; k++) {
                 int k1 = (k + k0) % a.kz;
                 R v = ab * tz[k];
-                if (sizeof(R) == 4) {
-                    long long qv = __double2ll_rn((double)v * a.qscale);
-                    if (qv) atomicAdd((unsigned long long*)(a.qgrid + row + k1), (unsigned long long)qv);
-                } else {
-                    atomicAdd((double*)a.rgrid + row + k1, (double)v);
-                }
+                // int64 fixed point: deterministic, order-independent grid sums
+                long long qv = __double2ll_rn(qs * (double)v);
+                if (qv) atomicAdd((unsigned long long*)(a.qgrid + row + k1), (unsigned long long)qv);
             }
         }
     }
@@ -259,7 +257,7 @@ __global__ void k_fft_pass(PassArgs pa)
             for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
                 int l = idx / n, z = idx - l * n;
                 size_t g = (size_t)(l0 + l) * a.kz + z;
-                R v = sizeof(R) == 4 ? (R)((double)a.qgrid[g] * (1.0 / a.qscale)) : ((const R*)a.rgrid)[g];
+                R v = (R)((double)a.qgrid[g] * (1.0 / a.qscale));
                 C c; c.x = v; c.y = 0;
                 buf0[l * pa.ld + z] = c;
             }
@@ -344,7 +342,7 @@ __global__ void k_fft_pass(PassArgs pa)
     if (MODE == kModeXConv) {
         for (int k = 0; k < kERec; ++k) acc[k] *= 0.5;
         acc[5] = acc[3]; acc[8] = acc[4]; acc[9] = acc[7];
-        block_reduce_store<8>(acc, a.erec + ((size_t)pa.erec_off + blockIdx.x) * kERec);
+        block_reduce_store<8>(acc, a.erec, a.erec_stride, pa.erec_off + blockIdx.x);
     }
 }
 
@@ -397,14 +395,21 @@ static void make_plan(int n, FftPlan& p)
 }
 
 template <typename R>
-static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches, int* erec_used)
+static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches, int* erec_used, int stage)
 {
     typedef typename Cx<R>::T C;
     int nb = (a.n + 127) / 128;
     size_t nreal = (size_t)a.kx * a.ky * a.kz;
-    if (sizeof(R) == 4) cudaMemsetAsync(a.qgrid, 0, sizeof(long long) * nreal, s);
-    else cudaMemsetAsync(a.rgrid, 0, sizeof(double) * nreal, s);
-    if (a.n > 0) { k_spread<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+    *erec_used = 0;
+    if (stage == kStageSpread) {
+        cudaMemsetAsync(a.qgrid, 0, sizeof(long long) * nreal, s);
+        if (a.n > 0) { k_spread<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+        return (int)cudaGetLastError();
+    }
+    if (stage == kStageGather) {
+        if (a.n > 0) { k_gather<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+        return (int)cudaGetLastError();
+    }
 
     FftPlan px, py, pz;
     make_plan(a.kx, px); make_plan(a.ky, py); make_plan(a.kz, pz);
@@ -417,26 +422,30 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         pa.tw_off = a.twz; pa.erec_off = 0;
         int blocks = (a.kx * a.ky + pa.lines - 1) / pa.lines;
         size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
-        cudaFuncSetAttribute(k_fft_pass<R, kModeZR2C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_fft_pass<R, kModeZR2C><<<blocks, threads, sm, s>>>(pa);
     }
-    int tile = 16;
+    // lines per CTA for the strided passes: 16 (128 B coalesced rows for
+    // float2) unless two line buffers would exceed ~200 KB of shared memory
+    auto tile_for = [](int n) {
+        int t = (200 * 1024) / (2 * (n + 1) * (int)sizeof(C));
+        return t < 1 ? 1 : (t > 16 ? 16 : t);
+    };
+    int tile = tile_for(a.ky);
     // y forward
     {
         PassArgs pa; pa.a = a; pa.plan = py; pa.lines = tile; pa.ld = a.ky + 1; pa.sign = -1;
         pa.tw_off = a.twy; pa.erec_off = 0;
         int blocks = a.kx * ((a.kzh + tile - 1) / tile);
         size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
-        cudaFuncSetAttribute(k_fft_pass<R, kModeY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_fft_pass<R, kModeY><<<blocks, threads, sm, s>>>(pa);
     }
     // x forward + convolution + x inverse
-    int xblocks = a.ky * ((a.kzh + tile - 1) / tile);
+    int xtile = tile_for(a.kx);
+    int xblocks = a.ky * ((a.kzh + xtile - 1) / xtile);
     {
-        PassArgs pa; pa.a = a; pa.plan = px; pa.lines = tile; pa.ld = a.kx + 1; pa.sign = -1;
+        PassArgs pa; pa.a = a; pa.plan = px; pa.lines = xtile; pa.ld = a.kx + 1; pa.sign = -1;
         pa.tw_off = a.twx; pa.erec_off = 0;
         size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
-        cudaFuncSetAttribute(k_fft_pass<R, kModeXConv>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_fft_pass<R, kModeXConv><<<xblocks, threads, sm, s>>>(pa);
     }
     // y inverse
@@ -453,22 +462,41 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         pa.tw_off = a.twz; pa.erec_off = 0;
         int blocks = (a.kx * a.ky + pa.lines - 1) / pa.lines;
         size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
-        cudaFuncSetAttribute(k_fft_pass<R, kModeZC2R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_fft_pass<R, kModeZC2R><<<blocks, threads, sm, s>>>(pa);
     }
-    if (a.n > 0) { k_gather<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
     *launches += 5;
     *erec_used = xblocks;
     return (int)cudaGetLastError();
 }
 
 int launch_pme_reciprocal(const PmeArgs& a, int fp64, cudaStream_t s, long long* launches,
-                          double* erec_base, int* erec_used)
+                          double* erec_base, int* erec_used, int stage)
 {
     PmeArgs b = a;
     b.erec = erec_base;
-    return fp64 ? run_reciprocal<double>(b, s, launches, erec_used)
-                : run_reciprocal<float>(b, s, launches, erec_used);
+    return fp64 ? run_reciprocal<double>(b, s, launches, erec_used, stage)
+                : run_reciprocal<float>(b, s, launches, erec_used, stage);
+}
+
+// The FFT passes stage two line buffers in dynamic shared memory; allow the
+// opt-in maximum once so that launches (also inside graph capture) need no
+// attribute calls.
+void pme_init_attributes()
+{
+    static bool done = false;
+    if (done) return;
+    int dev = 0, mx = 48 * 1024;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncSetAttribute(k_fft_pass<float, kModeZR2C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_fft_pass<float, kModeY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_fft_pass<float, kModeXConv>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_fft_pass<float, kModeZC2R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_fft_pass<double, kModeZR2C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_fft_pass<double, kModeY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_fft_pass<double, kModeXConv>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_fft_pass<double, kModeZC2R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    done = true;
 }
 
 // ------------------------------------------------------------------ correction
@@ -478,6 +506,12 @@ __global__ void k_pme_correction(CorrArgs a)
 {
     double acc[kERec];
     for (int k = 0; k < kERec; ++k) acc[k] = 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // point self energy and charged-system term (initialize, :604-628),
+        // the latter also on the virial diagonal (evaluate, :296-301)
+        acc[1] = a.const_energy;
+        if (a.virial) acc[2] = acc[6] = acc[10] = a.const_virial;
+    }
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.n_excl; k += gridDim.x * blockDim.x) {
         int2 pr = a.pairs[k];
         const double* p1 = a.pos + 3 * (size_t)pr.x;
@@ -501,7 +535,7 @@ __global__ void k_pme_correction(CorrArgs a)
             acc[8] += xz; acc[9] += yz; acc[10] += fz * rz;
         }
     }
-    block_reduce_store<8>(acc, a.erec + (size_t)blockIdx.x * kERec);
+    block_reduce_store<8>(acc, a.erec, a.erec_stride, blockIdx.x);
 }
 
 int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches, int* blocks_used)
@@ -534,20 +568,28 @@ int launch_finalize(int n, const unsigned long long* facc, const int* sorted, do
     return (int)cudaGetLastError();
 }
 
-// deterministic sum of energy records: warp k sums component k
-__global__ void k_energy_reduce(const double* erec, int nrec, double* out)
+// deterministic sum of energy records: block k sums component k (contiguous)
+__global__ void k_energy_reduce(const double* erec, int stride, int nrec, double* out)
 {
-    int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (k >= kERec) return;
+    int k = blockIdx.x;
+    const double* c = erec + (size_t)k * stride;
     double s = 0.0;
-    for (int r = lane; r < nrec; r += 32) s += erec[(size_t)r * kERec + k];
+    for (int r = threadIdx.x; r < nrec; r += blockDim.x) s += c[r];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) out[k] += s;
+    __shared__ double part[8];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) part[w] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += part[q];
+        out[k] += t;
+    }
 }
 
-int launch_energy_reduce(const double* erec, int nrec, double* out, cudaStream_t s, long long* launches)
+int launch_energy_reduce(const double* erec, int stride, int nrec, double* out, cudaStream_t s, long long* launches)
 {
-    k_energy_reduce<<<1, 32 * kERec, 0, s>>>(erec, nrec, out);
+    k_energy_reduce<<<kERec, 256, 0, s>>>(erec, stride, nrec, out);
     *launches += 1;
     return (int)cudaGetLastError();
 }

@@ -23,10 +23,30 @@ using namespace pm;
 static const double kPi = 3.14159265358979323846;   // Constant::M_PI (base/pmconstants.cpp:56)
 static const double kEpsilon = 1.0e-14;              // Constant::EPSILON (base/pmconstants.cpp:45)
 
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
+// evaluation phases timed in profiling mode (pmgpu_phase_times)
+enum { kPhaseBin = 0, kPhasePair, kPhaseCorrection, kPhaseSpread, kPhaseFft, kPhaseGather, kPhaseFinalize,
+       kNumPhases };
+
+struct ProfMark {
+    int phase;
+    cudaEvent_t b, e;
 };
+
+struct GraphKey {
+    std::vector<long long> ids;
+    const void* pos = nullptr;
+    const void* fout = nullptr;
+    const void* energy = nullptr;
+    unsigned flags = 0;
+    int box_version = -1, topo_version = -1, buf_version = -1;
+    bool operator==(const GraphKey& o) const
+    {
+        return ids == o.ids && pos == o.pos && fout == o.fout && energy == o.energy && flags == o.flags &&
+               box_version == o.box_version && topo_version == o.topo_version && buf_version == o.buf_version;
+    }
+};
+
+static long long g_next_force_id = 1;
 
 struct pmgpu_system {
     int device = 0;
@@ -41,7 +61,8 @@ struct pmgpu_system {
     double* d_q = nullptr;
     int* d_type = nullptr;
     int* d_mol = nullptr;
-    float4* d_ljf = nullptr;
+    float4* d_ljn = nullptr;
+    float4* d_ljm = nullptr;
     double4* d_ljd = nullptr;
     uint32_t* d_xfull = nullptr;
     uint32_t* d_xmod = nullptr;
@@ -68,10 +89,16 @@ struct pmgpu_system {
     int* d_counts = nullptr;
     int* d_fill = nullptr;
     int* d_start = nullptr;
+    int* d_cstart = nullptr;
+    float4* d_cbox = nullptr;
+    int cbox_cap = 0;
+    int* d_ccell = nullptr;
+    int* d_skey = nullptr;
     int* d_tmp = nullptr;
     int* d_sorted = nullptr;
     int* d_slot = nullptr;
     float4* d_spos = nullptr;
+    float4* d_slo = nullptr;
     int4* d_smeta = nullptr;
     double4* d_spos64 = nullptr;
     int* d_status = nullptr;
@@ -80,10 +107,26 @@ struct pmgpu_system {
     int erec_cap = 0;
     std::vector<double> h_fbuf;
     bool binned = false;
+    std::set<pmgpu_force*> forces;     // live forces made on this system
+    int topo_version = 0;
+    int buf_version = 0;               // bumped when a per-evaluation buffer moves
+    // CUDA graph of the last evaluation (replayed when the key matches)
+    bool use_graphs = true;
+    cudaGraphExec_t graph_exec = nullptr;
+    GraphKey graph_key;
+    long long graph_launches = 0;
+    // profiling
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_pool;
+    size_t prof_next = 0;
+    std::vector<ProfMark> prof_marks;
+    double prof_ms[kNumPhases] = {0};
+    long long prof_evals = 0;
 };
 
 struct pmgpu_force {
     pmgpu_system* sys = nullptr;
+    long long id = g_next_force_id++;   // never reused (graph keys)
     int kind = 0;   // 0 cutoff, 1 PME
     int precision = 0;
     pmgpu_cutoff_params cp;
@@ -94,6 +137,11 @@ struct pmgpu_force {
     int nd = 0;
     int4* d_deltas = nullptr;
     float4* d_doff = nullptr;
+    int4* d_hdeltas = nullptr;      // half shell of the mixed kernel
+    float4* d_hoff = nullptr;
+    float4* d_hoff_lo = nullptr;
+    int nh = 0;
+    int half_rule = 0;
     int wrap = 0;
     TermF tf[2];
     TermD td[2];
@@ -108,7 +156,6 @@ struct pmgpu_force {
     double* d_bfac = nullptr;
     double* d_efac = nullptr;
     double self_energy = 0.0, charged_energy = 0.0;
-    double* d_const_rec = nullptr;   // 2 records: without / with virial
     int twx = 0, twy = 0, twz = 0;
 };
 
@@ -173,7 +220,8 @@ extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
 
 static void free_atom_buffers(pmgpu_system* s)
 {
-    dfree(s->d_q); dfree(s->d_type); dfree(s->d_mol); dfree(s->d_ljf); dfree(s->d_ljd);
+    dfree(s->d_q); dfree(s->d_type); dfree(s->d_mol); dfree(s->d_ljn); dfree(s->d_ljm); dfree(s->d_ljd);
+    dfree(s->d_slo); dfree(s->d_skey);
     dfree(s->d_xfull); dfree(s->d_xmod); dfree(s->d_xrow); dfree(s->d_xent);
     dfree(s->d_epairs); dfree(s->d_ecls);
     dfree(s->d_pos); dfree(s->d_fout); dfree(s->d_facc32); dfree(s->d_facc40);
@@ -181,11 +229,19 @@ static void free_atom_buffers(pmgpu_system* s)
     dfree(s->d_spos); dfree(s->d_smeta); dfree(s->d_spos64);
 }
 
+static void free_force(pmgpu_force* f);
+
 extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
 {
     if (!sys) return PMGPU_OK;
     cudaSetDevice(sys->device);
     cudaStreamSynchronize(sys->stream);
+    // forces still alive belong to this system: release them too
+    std::set<pmgpu_force*> live;
+    live.swap(sys->forces);
+    for (pmgpu_force* f : live) free_force(f);
+    if (sys->graph_exec) cudaGraphExecDestroy(sys->graph_exec);
+    for (cudaEvent_t e : sys->prof_pool) cudaEventDestroy(e);
     free_atom_buffers(sys);
     dfree(sys->d_counts); dfree(sys->d_fill); dfree(sys->d_start); dfree(sys->d_erec);
     dfree(sys->d_status); dfree(sys->d_energy);
@@ -204,6 +260,39 @@ extern "C" int pmgpu_last_error(pmgpu_system* sys, char* buf, int len)
 }
 
 extern "C" void* pmgpu_stream(pmgpu_system* sys) { return sys ? (void*)sys->stream : nullptr; }
+
+extern "C" int pmgpu_set_profiling(pmgpu_system* sys, int enable)
+{
+    if (!sys) return PMGPU_ERR_ARG;
+    cudaSetDevice(sys->device);
+    CK(cudaStreamSynchronize(sys->stream), "sync");
+    sys->profiling = enable != 0;
+    sys->prof_marks.clear();
+    sys->prof_next = 0;
+    for (int k = 0; k < kNumPhases; ++k) sys->prof_ms[k] = 0.0;
+    sys->prof_evals = 0;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_phase_times(pmgpu_system* sys, double* ms, int n, long long* evals)
+{
+    if (!sys || !ms || n <= 0) return PMGPU_ERR_ARG;
+    cudaSetDevice(sys->device);
+    CK(cudaStreamSynchronize(sys->stream), "sync");
+    long long bins = 0;
+    for (const ProfMark& m : sys->prof_marks) {
+        float t = 0.f;
+        if (m.e && cudaEventElapsedTime(&t, m.b, m.e) == cudaSuccess) sys->prof_ms[m.phase] += t;
+        if (m.phase == kPhaseBin) ++bins;
+    }
+    sys->prof_evals += bins;
+    sys->prof_marks.clear();
+    sys->prof_next = 0;
+    for (int k = 0; k < n && k < kNumPhases; ++k) ms[k] = sys->prof_ms[k];
+    for (int k = kNumPhases; k < n; ++k) ms[k] = 0.0;
+    if (evals) *evals = sys->prof_evals;
+    return PMGPU_OK;
+}
 extern "C" long long pmgpu_launch_count(pmgpu_system* sys) { return sys ? sys->launches : 0; }
 
 extern "C" int pmgpu_synchronize(pmgpu_system* sys)
@@ -235,6 +324,8 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     cudaSetDevice(sys->device);
     CK(cudaStreamSynchronize(sys->stream), "set_topology");
     free_atom_buffers(sys);
+    sys->topo_version++;
+    if (sys->graph_exec) { cudaGraphExecDestroy(sys->graph_exec); sys->graph_exec = nullptr; }
     sys->n = n_atoms; sys->t = n_types; sys->e = n_excl; sys->csf = coulomb_scaling_factor;
     sys->q.assign(scaled_charge, scaled_charge + n_atoms);
     sys->binned = false;
@@ -245,15 +336,23 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     CK(cudaMemcpy(sys->d_mol, molecule, sizeof(int) * n, cudaMemcpyHostToDevice), "copy");
     // Lennard-Jones table (LennardJonesParameterTable, T x T)
     size_t tt = (size_t)n_types * n_types;
-    std::vector<float4> ljf(tt);
+    // FP32 hi/lo pairs: a type pair's A and B are shared by many atom pairs,
+    // so their rounding must not bias the Lennard-Jones sum
+    std::vector<float4> ljn(tt), ljm(tt);
     std::vector<double4> ljd(tt);
+    auto hilo = [](double v, float& h, float& l) { h = (float)v; l = (float)(v - (double)h); };
     for (size_t k = 0; k < tt; ++k) {
         const double* p = lj_table + 4 * k;
-        ljf[k] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3]);
+        float ah, al, bh, bl;
+        hilo(p[0], ah, al); hilo(p[1], bh, bl);
+        ljn[k] = make_float4(ah, bh, al, bl);
+        hilo(p[2], ah, al); hilo(p[3], bh, bl);
+        ljm[k] = make_float4(ah, bh, al, bl);
         ljd[k] = make_double4(p[0], p[1], p[2], p[3]);
     }
-    CK(dalloc(&sys->d_ljf, tt), "alloc"); CK(dalloc(&sys->d_ljd, tt), "alloc");
-    CK(cudaMemcpy(sys->d_ljf, ljf.data(), sizeof(float4) * tt, cudaMemcpyHostToDevice), "copy");
+    CK(dalloc(&sys->d_ljn, tt), "alloc"); CK(dalloc(&sys->d_ljm, tt), "alloc"); CK(dalloc(&sys->d_ljd, tt), "alloc");
+    CK(cudaMemcpy(sys->d_ljn, ljn.data(), sizeof(float4) * tt, cudaMemcpyHostToDevice), "copy");
+    CK(cudaMemcpy(sys->d_ljm, ljm.data(), sizeof(float4) * tt, cudaMemcpyHostToDevice), "copy");
     CK(cudaMemcpy(sys->d_ljd, ljd.data(), sizeof(double4) * tt, cudaMemcpyHostToDevice), "copy");
     // exclusions: check() classes as window bit masks (index delta 1..32) and
     // a CSR list for larger deltas (ExclusionTable's lowDeltas / highDeltas)
@@ -305,6 +404,8 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     CK(dalloc(&sys->d_cell_lin, n), "alloc"); CK(dalloc(&sys->d_cell3, 3 * (size_t)n), "alloc");
     CK(dalloc(&sys->d_tmp, n), "alloc"); CK(dalloc(&sys->d_sorted, n), "alloc"); CK(dalloc(&sys->d_slot, n), "alloc");
     CK(dalloc(&sys->d_spos, n), "alloc"); CK(dalloc(&sys->d_smeta, n), "alloc"); CK(dalloc(&sys->d_spos64, n), "alloc");
+    CK(dalloc(&sys->d_slo, n), "alloc"); CK(dalloc(&sys->d_skey, n), "alloc");
+    sys->cbox_cap = 0;   // cluster boxes depend on N and the cell grid: sized at evaluation
     sys->h_fbuf.assign(3 * (size_t)n, 0.0);
     return PMGPU_OK;
 }
@@ -361,7 +462,7 @@ extern "C" int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* 
     g.ncell = (int)nc;
     if (g.ncell > sys->ncell_cap) {
         CK(dalloc(&sys->d_counts, g.ncell), "alloc"); CK(dalloc(&sys->d_fill, g.ncell), "alloc");
-        CK(dalloc(&sys->d_start, g.ncell + 1), "alloc");
+        CK(dalloc(&sys->d_start, g.ncell + 1), "alloc"); CK(dalloc(&sys->d_cstart, g.ncell + 1), "alloc");
         sys->ncell_cap = g.ncell;
     }
     sys->box_set = true;
@@ -399,6 +500,15 @@ static void term_setup(const pmgpu_cutoff_params* p, int k, TermF& f, TermD& d)
     f.c1_15_1 = (float)d.c1_15_1; f.c1_05_3 = (float)d.c1_05_3; f.c1_15_3 = (float)d.c1_15_3;
     f.sh_a = (float)d.sh_a; f.sh_b = (float)d.sh_b;
     f.alpha = (float)d.alpha; f.two_alpha_pi = (float)d.two_alpha_pi;
+    f.alpha_lo = (float)(d.alpha - (double)f.alpha);
+    f.two_alpha_pi_lo = (float)(d.two_alpha_pi - (double)f.two_alpha_pi);
+    f.s1_lo = (float)(d.s1 - (double)f.s1);
+    f.s3_lo = (float)(d.s3 - (double)f.s3);
+    f.c1_15_1_lo = (float)(d.c1_15_1 - (double)f.c1_15_1);
+    f.c1_05_3_lo = (float)(d.c1_05_3 - (double)f.c1_05_3);
+    f.c1_15_3_lo = (float)(d.c1_15_3 - (double)f.c1_15_3);
+    f.sh_a_lo = (float)(d.sh_a - (double)f.sh_a);
+    f.sh_b_lo = (float)(d.sh_b - (double)f.sh_b);
 }
 
 extern "C" int pmgpu_cutoff_create(pmgpu_system* sys, const pmgpu_cutoff_params* p, pmgpu_force** out)
@@ -433,6 +543,7 @@ extern "C" int pmgpu_cutoff_create(pmgpu_system* sys, const pmgpu_cutoff_params*
         c2 = std::max(c2, f->td[k].cut2);
     }
     f->cut2 = c2;
+    sys->forces.insert(f);
     *out = f;
     return PMGPU_OK;
 }
@@ -495,6 +606,31 @@ static int prepare_cutoff(pmgpu_force* f)
     if (!deltas.empty()) {
         CK(cudaMemcpy(f->d_deltas, deltas.data(), sizeof(int4) * deltas.size(), cudaMemcpyHostToDevice), "copy");
         CK(cudaMemcpy(f->d_doff, off.data(), sizeof(float4) * off.size(), cudaMemcpyHostToDevice), "copy");
+    }
+    // half shell of the mixed kernel: when every delta of the reach is a
+    // distinct cell (reach_ok), the lexicographically positive half of the
+    // (symmetric) delta list visits each unordered cell pair exactly once;
+    // otherwise the reference's list with its B > A rule
+    std::vector<int4> hd;
+    for (const int4& d : deltas)
+        if (!reach_ok || d.x > 0 || (d.x == 0 && (d.y > 0 || (d.y == 0 && d.z > 0)))) hd.push_back(d);
+    std::vector<float4> ho(hd.size()), hl(hd.size());
+    for (size_t k = 0; k < hd.size(); ++k) {
+        double o[3] = {hd[k].x * sys->grid.csx, hd[k].y * sys->grid.csy, hd[k].z * sys->grid.csz};
+        float h[3], l[3];
+        for (int c = 0; c < 3; ++c) { h[c] = (float)o[c]; l[c] = (float)(o[c] - (double)h[c]); }
+        ho[k] = make_float4(h[0], h[1], h[2], 0.f);
+        hl[k] = make_float4(l[0], l[1], l[2], 0.f);
+    }
+    f->nh = (int)hd.size();
+    f->half_rule = reach_ok ? 0 : 1;
+    CK(dalloc(&f->d_hdeltas, hd.size()), "alloc");
+    CK(dalloc(&f->d_hoff, hd.size()), "alloc");
+    CK(dalloc(&f->d_hoff_lo, hd.size()), "alloc");
+    if (!hd.empty()) {
+        CK(cudaMemcpy(f->d_hdeltas, hd.data(), sizeof(int4) * hd.size(), cudaMemcpyHostToDevice), "copy");
+        CK(cudaMemcpy(f->d_hoff, ho.data(), sizeof(float4) * ho.size(), cudaMemcpyHostToDevice), "copy");
+        CK(cudaMemcpy(f->d_hoff_lo, hl.data(), sizeof(float4) * hl.size(), cudaMemcpyHostToDevice), "copy");
     }
     f->box_version = sys->box_version;
     return PMGPU_OK;
@@ -582,6 +718,7 @@ extern "C" int pmgpu_pme_create(pmgpu_system* sys, const pmgpu_pme_params* p, pm
         }
     }
     f->alpha = alpha;
+    sys->forces.insert(f);
     *out = f;
     return PMGPU_OK;
 }
@@ -640,6 +777,7 @@ static int prepare_pme(pmgpu_force* f)
         CK(cudaMemcpy(f->d_tw, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice), "copy");
         CK(dalloc((double2**)&f->d_cgrid, nhalf), "alloc");
         CK(dalloc((double**)&f->d_rgrid, nreal), "alloc");
+        CK(dalloc(&f->d_qgrid, nreal), "alloc");
     } else {
         std::vector<float> twf(tw.size());
         for (size_t k = 0; k < tw.size(); ++k) twf[k] = (float)tw[k];
@@ -658,28 +796,29 @@ static int prepare_pme(pmgpu_force* f)
     f->charged_energy = 0.0;
     if (p.correction && std::fabs(q1 * 0.00268283) > 1.0e-5)
         f->charged_energy = -kPi / (2.0 * V * (alpha * alpha)) * q1 * q1;
-    double rec[2 * kERec];
-    memset(rec, 0, sizeof(rec));
-    rec[1] = f->self_energy + f->charged_energy;
-    rec[kERec + 1] = rec[1];
-    rec[kERec + 2] = rec[kERec + 6] = rec[kERec + 10] = f->charged_energy;
-    CK(dalloc(&f->d_const_rec, 2 * kERec), "alloc");
-    CK(cudaMemcpy(f->d_const_rec, rec, sizeof(rec), cudaMemcpyHostToDevice), "copy");
     f->box_version = sys->box_version;
     return PMGPU_OK;
+}
+
+static void free_force(pmgpu_force* f)
+{
+    dfree(f->d_deltas); dfree(f->d_doff); dfree(f->d_qgrid);
+    dfree(f->d_hdeltas); dfree(f->d_hoff); dfree(f->d_hoff_lo);
+    if (f->d_cgrid) cudaFree(f->d_cgrid);
+    if (f->d_rgrid) cudaFree(f->d_rgrid);
+    if (f->d_tw) cudaFree(f->d_tw);
+    dfree(f->d_bfac); dfree(f->d_efac);
+    delete f;
 }
 
 extern "C" int pmgpu_force_destroy(pmgpu_force* f)
 {
     if (!f) return PMGPU_OK;
-    cudaSetDevice(f->sys->device);
-    cudaStreamSynchronize(f->sys->stream);
-    dfree(f->d_deltas); dfree(f->d_doff); dfree(f->d_qgrid);
-    if (f->d_cgrid) cudaFree(f->d_cgrid);
-    if (f->d_rgrid) cudaFree(f->d_rgrid);
-    if (f->d_tw) cudaFree(f->d_tw);
-    dfree(f->d_bfac); dfree(f->d_efac); dfree(f->d_const_rec);
-    delete f;
+    pmgpu_system* sys = f->sys;
+    cudaSetDevice(sys->device);
+    cudaStreamSynchronize(sys->stream);
+    sys->forces.erase(f);
+    free_force(f);
     return PMGPU_OK;
 }
 
@@ -694,11 +833,14 @@ extern "C" int pmgpu_pme_alpha(pmgpu_force* f, double* alpha)
 static int bin(pmgpu_system* sys, const double* d_pos)
 {
     BinArgs a;
+    a.skey = sys->d_skey; a.cstart = sys->d_cstart; a.cbox = sys->d_cbox; a.ccell = sys->d_ccell;
+    a.ncl_cap = sys->cbox_cap;
     a.n = sys->n; a.pos = d_pos; a.q = sys->d_q; a.type = sys->d_type; a.mol = sys->d_mol;
     a.pbc = sys->pbc; a.grid = sys->grid;
     a.cell_lin = sys->d_cell_lin; a.cell3 = sys->d_cell3; a.counts = sys->d_counts; a.fill = sys->d_fill;
     a.start = sys->d_start; a.tmp = sys->d_tmp; a.sorted = sys->d_sorted; a.slot_of = sys->d_slot;
-    a.spos = sys->d_spos; a.smeta = sys->d_smeta; a.spos64 = sys->d_spos64; a.status = sys->d_status;
+    a.spos = sys->d_spos; a.slo = sys->d_slo; a.smeta = sys->d_smeta; a.spos64 = sys->d_spos64;
+    a.status = sys->d_status;
     int e = launch_bin(a, sys->stream, &sys->launches);
     if (e) return cuda_fail(sys, (cudaError_t)e, "binning");
     sys->binned = true;
@@ -708,12 +850,19 @@ static int bin(pmgpu_system* sys, const double* d_pos)
 static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_pos, PairArgs& a)
 {
     memset(&a, 0, sizeof(a));
-    a.start = sys->d_start; a.spos = sys->d_spos; a.smeta = sys->d_smeta; a.spos64 = sys->d_spos64;
+    a.start = sys->d_start; a.spos = sys->d_spos; a.slo = sys->d_slo; a.smeta = sys->d_smeta;
+    a.spos64 = sys->d_spos64; a.cstart = sys->d_cstart; a.cbox = sys->d_cbox;
     a.pos = d_pos;
     a.xfull = sys->d_xfull; a.xmod = sys->d_xmod; a.xrow = sys->d_xrow; a.xent = sys->d_xent;
-    a.ljf = sys->d_ljf; a.ljd = sys->d_ljd; a.n_types = sys->t;
+    a.ljn = sys->d_ljn; a.ljm = sys->d_ljm; a.ljd = sys->d_ljd; a.n_types = sys->t;
     a.deltas = f->d_deltas; a.doff = f->d_doff; a.nd = f->nd;
+    a.hdeltas = f->d_hdeltas; a.hoff = f->d_hoff; a.hoff_lo = f->d_hoff_lo; a.nh = f->nh;
+    a.half_rule = f->half_rule; a.ccell = sys->d_ccell;
     a.grid = sys->grid; a.pbc = sys->pbc; a.wrap = f->wrap;
+    a.lx_lo = (float)(sys->box[0] - (double)(float)sys->box[0]);
+    a.ly_lo = (float)(sys->box[4] - (double)(float)sys->box[4]);
+    a.lz_lo = (float)(sys->box[8] - (double)(float)sys->box[8]);
+    a.erec_stride = sys->erec_cap;
     a.lx = (float)sys->box[0]; a.ly = (float)sys->box[4]; a.lz = (float)sys->box[8];
     a.ilx = (float)(1.0 / sys->box[0]); a.ily = (float)(1.0 / sys->box[4]); a.ilz = (float)(1.0 / sys->box[8]);
     a.n_terms = f->cp.n_terms;
@@ -732,37 +881,97 @@ static int ensure_erec(pmgpu_system* sys, int need)
     int cap = std::max(need, 2 * sys->erec_cap);
     CK(dalloc(&sys->d_erec, (size_t)cap * kERec), "alloc");
     sys->erec_cap = cap;
+    sys->buf_version++;          // a captured graph holds the old buffer
     return PMGPU_OK;
 }
 
-static int pme_xblocks(const pmgpu_force* f) { return f->pp.grid[1] * ((f->kzh + 15) / 16); }
+// energy records one cutoff force writes
+static int pair_records(pmgpu_system* sys, pmgpu_force* f)
+{
+    return f->precision == PMGPU_PRECISION_FP64 ? pair_blocks(sys->grid, f->nd)
+                                                : 4 * pair_blocks_mixed(sys->grid, f->nh);
+}
 
-static int eval_core(pmgpu_system* sys, int nf, pmgpu_force* const* forces, const double* d_pos,
-                     double* d_fout, double* d_energy, unsigned flags)
+// upper bound of the energy records of the fused x pass (one per CTA, at
+// least one x-line per CTA)
+static int pme_xblocks(const pmgpu_force* f) { return f->pp.grid[1] * f->kzh; }
+
+// Everything that allocates or copies synchronously: force tables, buffer
+// capacities.  Runs before an evaluation is enqueued (or captured).
+static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
 {
     if (!sys->box_set) return fail(sys, PMGPU_ERR_STATE, "box not set (pmgpu_set_box)");
     if (nf < 0 || (nf > 0 && !forces)) return fail(sys, PMGPU_ERR_ARG, "bad force list");
-    int virial = (flags & PMGPU_FLAG_VIRIAL) ? 1 : 0;
-    bool use32 = false, use40 = false;
     int need = 1;
     for (int k = 0; k < nf; ++k) {
         pmgpu_force* f = forces[k];
         if (!f || f->sys != sys) return fail(sys, PMGPU_ERR_ARG, "force belongs to another system");
         int r = f->kind == 0 ? prepare_cutoff(f) : prepare_pme(f);
         if (r) return r;
-        (f->precision == PMGPU_PRECISION_FP64 ? use40 : use32) = true;
-        if (f->kind == 0) need += pair_blocks(sys->grid, f->nd);
-        else need += pme_xblocks(f) + 148 * 4 + 1;
+        if (f->kind == 0) need += pair_records(sys, f);
+        else need += pme_xblocks(f) + 148 * 4;
     }
     int r = ensure_erec(sys, need);
     if (r) return r;
+    // clusters: at most N / 8 full ones plus one partial per cell
+    int ncl = sys->n / kCluster + sys->grid.ncell + 1;
+    if (ncl > sys->cbox_cap) {
+        CK(dalloc(&sys->d_cbox, 2 * (size_t)ncl), "alloc");
+        CK(dalloc(&sys->d_ccell, (size_t)ncl), "alloc");
+        sys->cbox_cap = ncl;
+        sys->buf_version++;
+    }
+    pme_init_attributes();
+    return PMGPU_OK;
+}
+
+static cudaEvent_t prof_event(pmgpu_system* sys)
+{
+    if (sys->prof_next == sys->prof_pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        sys->prof_pool.push_back(e);
+    }
+    return sys->prof_pool[sys->prof_next++];
+}
+
+// CUDA-event timing of one phase of an evaluation (profiling mode only)
+static int prof_begin(pmgpu_system* sys, int phase)
+{
+    if (!sys->profiling) return -1;
+    ProfMark m;
+    m.phase = phase;
+    m.b = prof_event(sys);
+    m.e = nullptr;
+    cudaEventRecord(m.b, sys->stream);
+    sys->prof_marks.push_back(m);
+    return (int)sys->prof_marks.size() - 1;
+}
+
+static void prof_end(pmgpu_system* sys, int m)
+{
+    if (m < 0) return;
+    sys->prof_marks[m].e = prof_event(sys);
+    cudaEventRecord(sys->prof_marks[m].e, sys->stream);
+}
+
+// Only asynchronous work on the system's stream (capturable in a graph).
+static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, const double* d_pos,
+                        double* d_fout, double* d_energy, unsigned flags)
+{
+    int virial = (flags & PMGPU_FLAG_VIRIAL) ? 1 : 0;
+    bool use32 = false, use40 = false;
+    for (int k = 0; k < nf; ++k) (forces[k]->precision == PMGPU_PRECISION_FP64 ? use40 : use32) = true;
+    int r;
     cudaStream_t s = sys->stream;
     size_t n3 = 3 * (size_t)sys->n;
+    int mbin = prof_begin(sys, kPhaseBin);
     CK(cudaMemsetAsync(sys->d_status, 0, sizeof(int), s), "memset");
     if (use32) CK(cudaMemsetAsync(sys->d_facc32, 0, sizeof(unsigned long long) * n3, s), "memset");
     if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
     r = bin(sys, d_pos);
     if (r) return r;
+    prof_end(sys, mbin);
     int used = 0;
     for (int k = 0; k < nf; ++k) {
         pmgpu_force* f = forces[k];
@@ -773,12 +982,14 @@ static int eval_core(pmgpu_system* sys, int nf, pmgpu_force* const* forces, cons
             PairArgs a;
             fill_pair_args(sys, f, d_pos, a);
             a.virial = virial;
-            a.erec = sys->d_erec + (size_t)used * kERec;
-            int blocks = pair_blocks(sys->grid, f->nd);
+            a.erec = sys->d_erec + used;
+            int blocks = fp64 ? pair_blocks(sys->grid, f->nd) : pair_blocks_mixed(sys->grid, f->nh);
+            int m = prof_begin(sys, kPhasePair);
             int e = fp64 ? launch_pair_fp64(a, f->combo, blocks, s, &sys->launches)
                          : launch_pair_mixed(a, f->combo, blocks, s, &sys->launches);
             if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
-            used += blocks;
+            prof_end(sys, m);
+            used += pair_records(sys, f);
         } else {
             const pmgpu_pme_params& p = f->pp;
             if (p.correction) {
@@ -786,15 +997,17 @@ static int eval_core(pmgpu_system* sys, int nf, pmgpu_force* const* forces, cons
                 c.n_excl = sys->e; c.pairs = sys->d_epairs; c.cls = sys->d_ecls; c.pos = d_pos; c.q = sys->d_q;
                 c.slot_of = sys->d_slot; c.pbc = sys->pbc; c.alpha = f->alpha; c.alpha2 = f->alpha * f->alpha;
                 c.two_alpha_pi = 2.0 * f->alpha / std::sqrt(kPi); c.csf = sys->csf;
-                c.facc = facc; c.scale = scale; c.erec = sys->d_erec + (size_t)used * kERec; c.status = sys->d_status;
+                c.facc = facc; c.scale = scale; c.erec = sys->d_erec + used; c.erec_stride = sys->erec_cap;
+                c.status = sys->d_status;
                 c.virial = virial;
+                c.const_energy = f->self_energy + f->charged_energy;
+                c.const_virial = f->charged_energy;
                 int b = 0;
+                int m = prof_begin(sys, kPhaseCorrection);
                 int e = launch_pme_correction(c, s, &sys->launches, &b);
                 if (e) return cuda_fail(sys, (cudaError_t)e, "PME correction");
+                prof_end(sys, m);
                 used += b;
-                CK(cudaMemcpyAsync(sys->d_erec + (size_t)used * kERec, f->d_const_rec + (virial ? kERec : 0),
-                                   sizeof(double) * kERec, cudaMemcpyDeviceToDevice, s), "copy");
-                used += 1;
             }
             if (p.reciprocal) {
                 PmeArgs a;
@@ -812,15 +1025,23 @@ static int eval_core(pmgpu_system* sys, int nf, pmgpu_force* const* forces, cons
                 a.piVr = 1.0 / (kPi * (LX * LY * LZ));
                 a.fac = kPi * kPi / (f->alpha * f->alpha);
                 a.wr = 1.0 / LX; a.lr = 1.0 / LY; a.hr = 1.0 / LZ;
-                a.facc = facc; a.scale = scale; a.qscale = kScaleFp64;
+                a.facc = facc; a.scale = scale; a.qscale = kScaleFp64; a.erec_stride = sys->erec_cap;
                 a.status = sys->d_status; a.virial = virial;
-                int u = 0;
-                int e = launch_pme_reciprocal(a, fp64 ? 1 : 0, s, &sys->launches, sys->d_erec + (size_t)used * kERec, &u);
-                if (e) return cuda_fail(sys, (cudaError_t)e, "PME reciprocal");
-                used += u;
+                const int phases[3] = {kPhaseSpread, kPhaseFft, kPhaseGather};
+                const int stages[3] = {kStageSpread, kStageFft, kStageGather};
+                for (int st = 0; st < 3; ++st) {
+                    int m = prof_begin(sys, phases[st]);
+                    int u = 0;
+                    int e = launch_pme_reciprocal(a, fp64 ? 1 : 0, s, &sys->launches,
+                                                  sys->d_erec + used, &u, stages[st]);
+                    if (e) return cuda_fail(sys, (cudaError_t)e, "PME reciprocal");
+                    used += u;
+                    prof_end(sys, m);
+                }
             }
         }
     }
+    int mfin = prof_begin(sys, kPhaseFinalize);
     if (use32) {
         int e = launch_finalize(sys->n, sys->d_facc32, sys->d_sorted, 1.0 / kScaleMixed, d_fout, s, &sys->launches);
         if (e) return cuda_fail(sys, (cudaError_t)e, "finalize");
@@ -830,12 +1051,44 @@ static int eval_core(pmgpu_system* sys, int nf, pmgpu_force* const* forces, cons
         if (e) return cuda_fail(sys, (cudaError_t)e, "finalize");
     }
     if (used > 0) {
-        int e = launch_energy_reduce(sys->d_erec, used, d_energy, s, &sys->launches);
+        int e = launch_energy_reduce(sys->d_erec, sys->erec_cap, used, d_energy, s, &sys->launches);
         if (e) return cuda_fail(sys, (cudaError_t)e, "energy reduce");
     }
-    if (!virial) {
-        // the virial slots are only written when ScalarStructure::virial() is set
+    prof_end(sys, mfin);
+    return PMGPU_OK;
+}
+
+// prepare, then enqueue -- replaying a captured CUDA graph when the same
+// forces run on the same buffers again (the evaluation is one graph launch)
+static int eval_core(pmgpu_system* sys, int nf, pmgpu_force* const* forces, const double* d_pos,
+                     double* d_fout, double* d_energy, unsigned flags)
+{
+    int r = eval_prepare(sys, nf, forces);
+    if (r) return r;
+    if (sys->profiling || !sys->use_graphs) return eval_enqueue(sys, nf, forces, d_pos, d_fout, d_energy, flags);
+    GraphKey key;
+    for (int k = 0; k < nf; ++k) key.ids.push_back(forces[k]->id);
+    key.pos = d_pos; key.fout = d_fout; key.energy = d_energy; key.flags = flags;
+    key.box_version = sys->box_version; key.topo_version = sys->topo_version; key.buf_version = sys->buf_version;
+    cudaStream_t s = sys->stream;
+    if (!(sys->graph_exec && key == sys->graph_key)) {
+        if (sys->graph_exec) { cudaGraphExecDestroy(sys->graph_exec); sys->graph_exec = nullptr; }
+        long long l0 = sys->launches;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
+        r = eval_enqueue(sys, nf, forces, d_pos, d_fout, d_energy, flags);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (r) { if (graph) cudaGraphDestroy(graph); return r; }
+        if (e != cudaSuccess) return cuda_fail(sys, e, "graph capture");
+        e = cudaGraphInstantiate(&sys->graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) { sys->graph_exec = nullptr; return cuda_fail(sys, e, "graph instantiate"); }
+        sys->graph_launches = sys->launches - l0;
+        sys->launches = l0;
+        sys->graph_key = key;
     }
+    CK(cudaGraphLaunch(sys->graph_exec, s), "graph launch");
+    sys->launches += sys->graph_launches;
     return PMGPU_OK;
 }
 
@@ -894,7 +1147,7 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     if (f->kind != 0) return fail(sys, PMGPU_ERR_UNSUPPORTED, "pair recording is for cutoff forces");
     if (!sys->box_set) return fail(sys, PMGPU_ERR_STATE, "box not set");
     cudaSetDevice(sys->device);
-    int r = prepare_cutoff(f);
+    int r = eval_prepare(sys, 1, &f);
     if (r) return r;
     cudaStream_t s = sys->stream;
     size_t n3 = 3 * (size_t)sys->n;
@@ -904,8 +1157,9 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
     r = bin(sys, sys->d_pos);
     if (r) return r;
-    int blocks = pair_blocks(sys->grid, f->nd);
-    r = ensure_erec(sys, blocks);
+    bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+    int blocks = fp64 ? pair_blocks(sys->grid, f->nd) : pair_blocks_mixed(sys->grid, f->nh);
+    r = ensure_erec(sys, pair_records(sys, f));
     if (r) return r;
     int* d_pairs = nullptr;
     unsigned long long* d_count = nullptr;

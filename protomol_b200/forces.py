@@ -20,6 +20,7 @@ Every evaluation runs on the GPU through libpmgpu.so; there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -59,7 +60,7 @@ class Topology:
         self.handle = h
         self.system = system
         self.n_atoms = system.n_atoms
-        self._keep = []
+        self._forces = weakref.WeakSet()
         self.set_topology(system)
         self.set_box(system.box, system.cell_size)
 
@@ -98,7 +99,11 @@ class Topology:
         return cells, tuple(int(d) for d in dims)
 
     def close(self):
+        """Destroys the forces made on this topology, then the system (the
+        C side frees a force's buffers through its system)."""
         if getattr(self, "handle", None):
+            for f in list(getattr(self, "_forces", ())):
+                f.close()
             _lib.load().pmgpu_system_destroy(self.handle)
             self.handle = None
 
@@ -119,6 +124,7 @@ class SystemForce:
         self.handle = handle
         self.id = ident
         self.params = params
+        topo._forces.add(self)
 
     def getKeyword(self) -> str:  # noqa: N802 (mirrors Force::getKeyword)
         return self.keyword
@@ -131,9 +137,11 @@ class SystemForce:
         evaluate_group(topo, [self], positions, forces, energies)
 
     def close(self):
-        if getattr(self, "handle", None):
+        # only while the owning system is alive: Topology.close() closes its
+        # forces first, so a force collected after its topology is a no-op
+        if getattr(self, "handle", None) and getattr(self.topo, "handle", None):
             _lib.load().pmgpu_force_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:

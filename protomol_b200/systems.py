@@ -39,6 +39,9 @@ _Q_O, _Q_H = -0.834, 0.417
 _EPS_O, _RMIN2_O = 0.1521, 1.7682
 _EPS_H, _RMIN2_H = 0.0, 0.2245
 _M_O, _M_H = 15.9994, 1.008
+# seeded liquid-like disorder of the water oxygens (A, per component); the
+# 216-water box keeps its exact 6x6x6 lattice
+WATER_JITTER = 0.1
 
 
 @dataclass
@@ -179,9 +182,15 @@ def _random_rotations(rng: np.random.Generator, n: int) -> np.ndarray:
     return r
 
 
-def _water_atoms(rng, oxygens: np.ndarray) -> np.ndarray:
-    """Rigid TIP3P waters with uniform random orientation; returns (3n, 3)."""
+def _water_atoms(rng, oxygens: np.ndarray, jitter: float = 0.0) -> np.ndarray:
+    """Rigid TIP3P waters with uniform random orientation; returns (3n, 3).
+
+    ``jitter`` > 0 displaces each oxygen by N(0, jitter) per component
+    (liquid-like disorder; on an exact lattice thousands of O-O pairs share
+    bit-identical distances, which no liquid configuration has)."""
     n = oxygens.shape[0]
+    if jitter > 0.0:
+        oxygens = oxygens + rng.normal(0.0, jitter, oxygens.shape)
     half = 0.5 * _HOH
     local = np.array([
         [0.0, 0.0, 0.0],
@@ -390,7 +399,7 @@ def chain_in_water(n_chain: int, n_water: int, length: float, seed: int, lattice
             break
         radius -= 0.1
     idx = np.sort(rng.choice(np.flatnonzero(keep), n_water, replace=False))
-    water = _water_atoms(rng, sites[idx])
+    water = _water_atoms(rng, sites[idx], jitter=WATER_JITTER)
     return _assemble(name or f"chain{n_chain + 3 * n_water}", chain, q, params, water, box_len=length,
                      csf=0.5, cell_size=6.0, scheme="scaled1-4")
 
@@ -419,7 +428,7 @@ def water_box(n_water: int, seed: int, density: float = 0.0334,
     n_side = int(math.ceil(n_water ** (1.0 / 3.0)))
     sites = _lattice(n_side, length)
     idx = np.sort(rng.choice(len(sites), n_water, replace=False))
-    water = _water_atoms(rng, sites[idx])
+    water = _water_atoms(rng, sites[idx], jitter=WATER_JITTER)
     return _assemble(f"water{n_water}", None, None, None, water, box_len=length,
                      csf=1.0, cell_size=cell_size, scheme="1-3")
 
@@ -439,7 +448,7 @@ def water_box_1m(seed: int = 5) -> System:
     pick = rng.choice(len(sites), 333_334, replace=False)
     ion_site = sites[pick[0]]
     idx = np.sort(pick[1:])
-    water = _water_atoms(rng, sites[idx])
+    water = _water_atoms(rng, sites[idx], jitter=WATER_JITTER)
     return _assemble("water1M", None, None, None, water,
                      extra=[(ion_site, 1.0, 0.0469, 1.3638, 22.98977)],
                      box_len=length, csf=1.0, cell_size=6.0, scheme="1-3")

@@ -1,0 +1,56 @@
+"""The drop-in path end to end: GPU forces made by ProtoMol's OWN
+ForceFactory from force-definition strings (protomol_b200/adapter:
+GpuNonbondedForce + registerGpuForceExemplars, linked with the reference's
+framework objects), evaluated through SystemForce::evaluate into a
+Vector3DBlock / ScalarStructure, compared with the oracle."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from protomol_b200 import forces as F
+from protomol_b200 import systems, workloads
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "protomol_b200", "adapter", "_build", "gpu_force_driver")
+
+
+def run_driver(system, defs, precision="mixed", repeat=1):
+    if not os.path.exists(DRIVER):
+        pytest.skip("drop-in driver not built (needs the ProtoMol sources at build time)")
+    env = dict(os.environ, PMGPU_PRECISION=precision)
+    with tempfile.TemporaryDirectory() as td:
+        sp, op = os.path.join(td, "s.bin"), os.path.join(td, "o.bin")
+        system.save(sp)
+        p = subprocess.run([DRIVER, sp, op, str(repeat), *defs], env=env, capture_output=True, text=True,
+                           timeout=300)
+        assert p.returncode == 0, p.stderr
+        raw = open(op, "rb").read()
+    n = system.n_atoms
+    hdr = np.frombuffer(raw[:104], np.float64)
+    f = np.frombuffer(raw[104:104 + 24 * n], np.float64).reshape(n, 3)
+    made = [line[6:] for line in p.stderr.splitlines() if line.startswith("made: ")]
+    return {"lennard_jones": hdr[0], "coulomb": hdr[1], "virial": hdr[2:11], "forces": f,
+            "seconds": hdr[11], "made": made}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["water216", "chain14281"])
+def test_force_factory_keywords_run_on_the_gpu(case, precision):
+    w = workloads.water216() if case == "water216" else workloads.chain14281()
+    r = run_driver(w.system, w.forces, precision)
+    ref = oracle.evaluate(w.system, [F.parse_definition(d) for d in w.forces])
+    # the factory matched the reference ids (same strings as the reference)
+    for d, made in zip(w.forces, r["made"]):
+        assert made.split()[0] == d.split()[0]
+        assert "-algorithm" in made
+    err = np.sqrt(((r["forces"] - ref["forces"]) ** 2).sum() / (ref["forces"] ** 2).sum())
+    scale = abs(ref["lennard_jones"]) + abs(ref["coulomb"])
+    tol_f, tol_e = (1e-9, 1e-10) if precision == "fp64" else (1e-5, 1e-6)
+    assert err <= tol_f
+    assert abs(r["lennard_jones"] + r["coulomb"] - ref["lennard_jones"] - ref["coulomb"]) <= tol_e * scale
