@@ -27,7 +27,7 @@ EXPORTS = [
     "pmgpu_launch_count", "pmgpu_last_error", "pmgpu_get_cells", "pmgpu_get_pairs",
     "pmgpu_set_profiling", "pmgpu_phase_times",
 ]
-PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize"]
+PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
 
 
 class CutoffParams(C.Structure):

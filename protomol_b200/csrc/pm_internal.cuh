@@ -27,6 +27,7 @@ constexpr double kFixedLimit = 4.0e18;               // |value * scale| bound be
 // status bits written by kernels
 constexpr int kStatusOverflow = 1;
 constexpr int kStatusOutOfGrid = 2;
+constexpr int kStatusListFull = 4;     // cluster-pair list or chunk capacity exceeded
 
 // FP64 constants of PeriodicBoundaryConditions::set
 // (topology/PeriodicBoundaryConditions.cpp:40-77), orthogonal box.

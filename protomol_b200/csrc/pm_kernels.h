@@ -71,6 +71,7 @@ struct PairArgs {
     const int* cstart;           // first 8-atom cluster of each cell
     const int* ccell;            // cluster -> cell
     const float4* cbox;          // cluster bounding boxes (lo, hi)
+    int ncl_cap;                 // bound on the number of clusters
     const float4* spos;
     const float4* slo;
     const int4* smeta;
@@ -123,15 +124,31 @@ struct PairArgs {
     int* rec_pairs;              // pair recording (diagnostic) or null
     unsigned long long* rec_count;
     long long rec_cap;
+    // mixed kernel: cluster-pair list, chunks of work, fixed-point sums
+    int2* plist;                 // {first j slot, (delta + 1) | nj << 16 | i-cluster mask << 24}
+    int plist_cap;
+    int4* chunks;                // {first i slot, i atoms (<= 32), first entry, entries}
+    int chunk_cap;
+    int* plist_count;            // entries written (zeroed before the list kernel)
+    int* plist_need;             // entries needed when a capacity was exceeded
+    int* chunk_count;
+    int* chunk_need;
+    int* chunk_next;             // work counter of the pair kernel
+    const double4* hoff64;       // FP64 half-shell offsets (hi + lo), virial
+    unsigned long long* efix;    // 11 int64 sums (scale 2^32): LJ, Coulomb, virial
 };
 
 // Combination id of the registered OneAtomPair[Two] templates.
 int pair_combo_id(int n_terms, const int* pot, const int* sw);
-int launch_pair_mixed(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches);
+// K2a: the cluster-pair list; K2b: the mixed kernel over it
+int launch_cluster_list(const PairArgs& a, cudaStream_t s, long long* launches);
+int launch_pair_mixed(const PairArgs& a, int combo, cudaStream_t s, long long* launches);
 int launch_pair_fp64(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches);
 int pair_blocks(const CellGrid& g, int nd);
 // blocks of the mixed kernel (4 warps, one energy record per warp)
-int pair_blocks_mixed(const CellGrid& g, int nh);
+// estimated cluster-pair list entries and chunks of a system
+long long plist_estimate(int n_atoms, const CellGrid& g, int nh);
+long long chunk_estimate(int n_atoms, const CellGrid& g, int nh);
 
 // ---------------------------------------------------------------- PME
 struct PmeArgs {
@@ -189,8 +206,25 @@ struct CorrArgs {
 int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches, int* blocks_used);
 
 // ---------------------------------------------------------------- finalize
-int launch_finalize(int n, const unsigned long long* facc, const int* sorted, double inv_scale,
-                    double* fout, cudaStream_t s, long long* launches);
-int launch_energy_reduce(const double* erec, int stride, int nrec, double* out, cudaStream_t s, long long* launches);
+// forces of the three fixed-point accumulators (any may be null) added into
+// fout in the caller's order; with pair_virial, the per-atom term
+// sum p (x) F of the mixed pair forces (f32) as one FP64 record per block
+struct FinArgs {
+    int n;
+    const unsigned long long* f32;      // mixed pair forces (whole-cell shifts), 2^32
+    const unsigned long long* f32p;     // other mixed forces (PME, per-pair minimal image), 2^32
+    const unsigned long long* f40;      // FP64 forces, 2^40
+    const int* sorted;
+    const float4* spos;
+    const float4* slo;
+    int pair_virial;
+    double* fout;
+    double* erec;
+    int erec_stride;
+};
+int launch_finalize(const FinArgs& a, cudaStream_t s, long long* launches, int* records);
+// sums the FP64 records and adds the int64 fixed-point sums (efix, scale 2^32)
+int launch_energy_reduce(const double* erec, int stride, int nrec, const unsigned long long* efix,
+                         double* out, cudaStream_t s, long long* launches);
 
 }  // namespace pm

@@ -164,7 +164,7 @@ __device__ __forceinline__ void pot_f32(const PairArgs& p, const TermF& t, float
 {
     if (POT == LJ) {
         const float4* tab = excl == PMGPU_EXCL_MODIFIED ? p.ljm : p.ljn;
-        float4 par = __ldg(tab + (size_t)ti * p.n_types + tj);   // A_hi, B_hi, A_lo, B_lo
+        float4 par = __ldg(tab + (ti * p.n_types + tj));   // A_hi, B_hi, A_lo, B_lo
         float r6 = rd2 * rd2 * rd2;
         float r12 = r6 * r6;
         float r6B = fmaf(par.y, r6, par.w * r6);
@@ -173,10 +173,10 @@ __device__ __forceinline__ void pot_f32(const PairArgs& p, const TermF& t, float
         f = (12.0f * r12A - 6.0f * r6B) * rd2;
     } else if (POT == CO) {
         e = qq * rinv;
-        if (excl == PMGPU_EXCL_MODIFIED) e *= p.csf;
+        e = excl == PMGPU_EXCL_MODIFIED ? e * p.csf : e;
         f = e * rd2;
     } else if (POT == EW) {
-        if (p.csfd != 1.0 && excl == PMGPU_EXCL_MODIFIED) qq *= p.csf;
+        qq = (p.csfd != 1.0 && excl == PMGPU_EXCL_MODIFIED) ? qq * p.csf : qq;
         float r = r2 * rinv;
         float ar = fmaf(t.alpha, r, t.alpha_lo * r);     // compensated alpha
         float ex = qq * expf(-ar * ar);
@@ -187,31 +187,30 @@ __device__ __forceinline__ void pot_f32(const PairArgs& p, const TermF& t, float
     }
 }
 
+// switching functions as selects (no branches: the two pair evaluations of
+// a lane interleave)
 template <int SW>
 __device__ __forceinline__ void sw_f32(const TermF& t, float r2, float rinv, bool inside, float& v, float& d)
 {
     if (SW == SC2) {
-        d = 0.f;
-        if (r2 > t.cut2) v = 0.f;
-        else if (r2 >= t.on2) {
-            float c2 = t.cut2 - r2;
-            float c4 = c2 * (t.s2 + 2.0f * r2);
-            float c24 = c2 * c4;
-            v = fmaf(t.s1, c24, t.s1_lo * c24);
-            float dd = c2 * c2 - c4;
-            d = fmaf(t.s3, dd, t.s3_lo * dd);
-        } else v = 1.f;
+        const float c2 = t.cut2 - r2;
+        const float c4 = c2 * (t.s2 + 2.0f * r2);
+        const float c24 = c2 * c4;
+        const float dd = c2 * c2 - c4;
+        const bool out = r2 > t.cut2, mid = r2 >= t.on2;
+        v = out ? 0.f : (mid ? fmaf(t.s1, c24, t.s1_lo * c24) : 1.f);
+        d = (out || !mid) ? 0.f : fmaf(t.s3, dd, t.s3_lo * dd);
     } else if (SW == SC1) {
-        if (r2 > t.cut2) { v = 0.f; d = 0.f; return; }
-        float dist = r2 * rinv;
-        float in = fmaf(-r2, t.c1_05_3, t.c1_15_1) + fmaf(-r2, t.c1_05_3_lo, t.c1_15_1_lo);
-        v = fmaf(-dist, in, 1.0f);
-        d = fmaf(dist, t.c1_15_3, -t.c1_15_1 * rinv) + fmaf(dist, t.c1_15_3_lo, -t.c1_15_1_lo * rinv);
+        const float dist = r2 * rinv;
+        const float in = fmaf(-r2, t.c1_05_3, t.c1_15_1) + fmaf(-r2, t.c1_05_3_lo, t.c1_15_1_lo);
+        const bool out = r2 > t.cut2;
+        v = out ? 0.f : fmaf(-dist, in, 1.0f);
+        d = out ? 0.f : fmaf(dist, t.c1_15_3, -t.c1_15_1 * rinv) + fmaf(dist, t.c1_15_3_lo, -t.c1_15_1_lo * rinv);
     } else if (SW == SSH) {
-        if (r2 > t.cut2) { v = 0.f; d = 0.f; return; }
-        float x = fmaf(-r2, t.sh_a, 1.0f) - r2 * t.sh_a_lo;
-        v = x * x;
-        d = fmaf(t.sh_b, x, t.sh_b_lo * x);
+        const float x = fmaf(-r2, t.sh_a, 1.0f) - r2 * t.sh_a_lo;
+        const bool out = r2 > t.cut2;
+        v = out ? 0.f : x * x;
+        d = out ? 0.f : fmaf(t.sh_b, x, t.sh_b_lo * x);
     } else if (SW == SCUT) {
         d = 0.f;
         v = inside ? 1.f : 0.f;
@@ -402,12 +401,19 @@ __global__ void __launch_bounds__(128) k_pair_fp64(PairArgs p)
 }
 
 // ---------------------------------------------------------------- launch
-int pair_blocks_mixed(const CellGrid& g, int nh)
+long long plist_estimate(int n_atoms, const CellGrid& g, int nh)
 {
-    long long items = (long long)g.ncell * ((nh + 1 + kBatch - 1) / kBatch);
-    long long b = (items + 3) / 4;
-    long long cap = 148 * 16;
-    return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+    // every i-supercluster against every cluster of its half shell, at the
+    // mean cell occupancy plus one partial cluster, with 50% slack for uneven
+    // cells
+    double per_cell = (double)n_atoms / (kCluster * (double)g.ncell) + 1.0;
+    double supers = (double)n_atoms / (kCluster * kSuper) + g.ncell;
+    return (long long)(1.5 * supers * (nh + 1) * per_cell) + 4096;
+}
+
+long long chunk_estimate(int n_atoms, const CellGrid& g, int nh)
+{
+    return plist_estimate(n_atoms, g, nh) / kChunk + (long long)n_atoms / (kCluster * kSuper) + g.ncell + 1024;
 }
 
 int pair_blocks(const CellGrid& g, int nd)
@@ -443,11 +449,63 @@ struct Dispatch;
     default: return (int)cudaErrorInvalidValue;                                                        \
     }
 
-int launch_pair_mixed(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches)
+// one full wave of the mixed kernel (persistent warps take chunks of work)
+template <int NT, int P0, int S0, int P1, int S1, bool WRAP>
+static int run_mixed_w(const PairArgs& a, cudaStream_t s, long long* launches)
 {
-    PM_COMBO_SWITCH(k_pair_mixed)
+    static int blocks = 0;
+    if (blocks == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_mixed<NT, P0, S0, P1, S1, WRAP>, 128, 0);
+        blocks = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
+    }
+    k_pair_mixed<NT, P0, S0, P1, S1, WRAP><<<blocks, 128, 0, s>>>(a);
     *launches += 1;
     return (int)cudaGetLastError();
+}
+
+template <int NT, int P0, int S0, int P1, int S1>
+static int run_mixed(const PairArgs& a, cudaStream_t s, long long* launches)
+{
+    return a.wrap ? run_mixed_w<NT, P0, S0, P1, S1, true>(a, s, launches)
+                  : run_mixed_w<NT, P0, S0, P1, S1, false>(a, s, launches);
+}
+
+int launch_cluster_list(const PairArgs& a, cudaStream_t s, long long* launches)
+{
+    // one warp per cell
+    int lb = (int)(((long long)a.grid.ncell + 3) / 4);
+    k_cluster_list<<<lb > 0 ? lb : 1, 128, 0, s>>>(a);
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+int launch_pair_mixed(const PairArgs& a, int combo, cudaStream_t s, long long* launches)
+{
+    switch (combo) {
+#define PM_MIXED_CASE(ID, ...) case ID: return run_mixed<__VA_ARGS__>(a, s, launches);
+    PM_MIXED_CASE(0, 1, CO, SC1, NP, SUN)
+    PM_MIXED_CASE(1, 1, CO, SC2, NP, SUN)
+    PM_MIXED_CASE(2, 1, CO, SCUT, NP, SUN)
+    PM_MIXED_CASE(3, 1, CO, SSH, NP, SUN)
+    PM_MIXED_CASE(4, 1, EW, SCUT, NP, SUN)
+    PM_MIXED_CASE(5, 1, LJ, SC1, NP, SUN)
+    PM_MIXED_CASE(6, 1, LJ, SC2, NP, SUN)
+    PM_MIXED_CASE(7, 1, LJ, SCUT, NP, SUN)
+    PM_MIXED_CASE(8, 1, LJ, SSH, NP, SUN)
+    PM_MIXED_CASE(9, 2, LJ, SC1, EW, SCUT)
+    PM_MIXED_CASE(10, 2, LJ, SC1, CO, SSH)
+    PM_MIXED_CASE(11, 2, LJ, SC2, CO, SC1)
+    PM_MIXED_CASE(12, 2, LJ, SC2, EW, SCUT)
+    PM_MIXED_CASE(13, 2, LJ, SC2, CO, SCUT)
+    PM_MIXED_CASE(14, 2, LJ, SC2, CO, SSH)
+    PM_MIXED_CASE(15, 2, LJ, SCUT, EW, SCUT)
+    PM_MIXED_CASE(16, 2, LJ, SC2, CO, SC2)
+#undef PM_MIXED_CASE
+    default: return (int)cudaErrorInvalidValue;
+    }
 }
 
 int launch_pair_fp64(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches)

@@ -550,26 +550,50 @@ int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches
 }
 
 // ------------------------------------------------------------------ finalize
-__global__ void k_finalize(int n, const unsigned long long* facc, const int* sorted, double inv_scale, double* fout)
+__global__ void __launch_bounds__(256) k_finalize(FinArgs a)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    int i = sorted[s];
-    for (int c = 0; c < 3; ++c)
-        fout[3 * (size_t)i + c] += (double)(long long)facc[3 * (size_t)s + c] * inv_scale;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[kERec];
+#pragma unroll
+    for (int k = 0; k < kERec; ++k) v[k] = 0.0;
+    if (s < a.n) {
+        const int i = a.sorted[s];
+        double fp[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (a.f32) fp[c] = (double)(long long)a.f32[3 * (size_t)s + c] * (1.0 / kScaleMixed);
+            double f = fp[c];
+            if (a.f32p) f += (double)(long long)a.f32p[3 * (size_t)s + c] * (1.0 / kScaleMixed);
+            if (a.f40) f += (double)(long long)a.f40[3 * (size_t)s + c] * (1.0 / kScaleFp64);
+            a.fout[3 * (size_t)i + c] += f;
+        }
+        if (a.pair_virial) {
+            // the cell-relative position the FP32 pair vectors were formed from
+            const float4 h = a.spos[s], l = a.slo[s];
+            const double p[3] = {(double)h.x + (double)l.x, (double)h.y + (double)l.y, (double)h.z + (double)l.z};
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) v[2 + 3 * r + c] = p[r] * fp[c];
+        }
+    }
+    if (a.pair_virial) block_reduce_store<8>(v, a.erec, a.erec_stride, blockIdx.x);
 }
 
-int launch_finalize(int n, const unsigned long long* facc, const int* sorted, double inv_scale,
-                    double* fout, cudaStream_t s, long long* launches)
+int launch_finalize(const FinArgs& a, cudaStream_t s, long long* launches, int* records)
 {
-    if (n <= 0) return 0;
-    k_finalize<<<(n + 255) / 256, 256, 0, s>>>(n, facc, sorted, inv_scale, fout);
+    *records = 0;
+    if (a.n <= 0) return 0;
+    const int blocks = (a.n + 255) / 256;
+    k_finalize<<<blocks, 256, 0, s>>>(a);
     *launches += 1;
+    if (a.pair_virial) *records = blocks;
     return (int)cudaGetLastError();
 }
 
 // deterministic sum of energy records: block k sums component k (contiguous)
-__global__ void k_energy_reduce(const double* erec, int stride, int nrec, double* out)
+__global__ void k_energy_reduce(const double* erec, int stride, int nrec, const unsigned long long* efix,
+                                double* out)
 {
     int k = blockIdx.x;
     const double* c = erec + (size_t)k * stride;
@@ -583,13 +607,15 @@ __global__ void k_energy_reduce(const double* erec, int stride, int nrec, double
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += part[q];
+        if (efix) t += (double)(long long)efix[k] * (1.0 / 4294967296.0);
         out[k] += t;
     }
 }
 
-int launch_energy_reduce(const double* erec, int stride, int nrec, double* out, cudaStream_t s, long long* launches)
+int launch_energy_reduce(const double* erec, int stride, int nrec, const unsigned long long* efix,
+                         double* out, cudaStream_t s, long long* launches)
 {
-    k_energy_reduce<<<kERec, 256, 0, s>>>(erec, stride, nrec, out);
+    k_energy_reduce<<<kERec, 256, 0, s>>>(erec, stride, nrec, efix, out);
     *launches += 1;
     return (int)cudaGetLastError();
 }

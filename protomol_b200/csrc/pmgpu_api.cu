@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -22,10 +23,13 @@ using namespace pm;
 
 static const double kPi = 3.14159265358979323846;   // Constant::M_PI (base/pmconstants.cpp:56)
 static const double kEpsilon = 1.0e-14;              // Constant::EPSILON (base/pmconstants.cpp:45)
+// status word, list count and need, chunk count and need, work counter, pad,
+// then 11 int64 energy/virial sums
+static const size_t kSmallBytes = 32 + 8 * kERec;
 
 // evaluation phases timed in profiling mode (pmgpu_phase_times)
 enum { kPhaseBin = 0, kPhasePair, kPhaseCorrection, kPhaseSpread, kPhaseFft, kPhaseGather, kPhaseFinalize,
-       kNumPhases };
+       kPhaseList, kNumPhases };
 
 struct ProfMark {
     int phase;
@@ -82,7 +86,8 @@ struct pmgpu_system {
     double* d_fout = nullptr;
     double* d_energy = nullptr;        // 11
     double* h_energy = nullptr;        // pinned 11
-    unsigned long long* d_facc32 = nullptr;   // mixed (2^32)
+    unsigned long long* d_facc32 = nullptr;   // mixed (2^32): 3N pair forces + 3N other (d_facc32p)
+    unsigned long long* d_facc32p = nullptr;
     unsigned long long* d_facc40 = nullptr;   // FP64 (2^40)
     int* d_cell_lin = nullptr;
     int* d_cell3 = nullptr;
@@ -101,7 +106,23 @@ struct pmgpu_system {
     float4* d_slo = nullptr;
     int4* d_smeta = nullptr;
     double4* d_spos64 = nullptr;
+    // small per-evaluation scratch, zeroed by one memset: status word,
+    // cluster-pair list and chunk counters, int64 energy/virial sums
+    void* d_small = nullptr;
     int* d_status = nullptr;
+    int* d_plist_count = nullptr;
+    int* d_plist_need = nullptr;
+    int* d_chunk_count = nullptr;
+    int* d_chunk_need = nullptr;
+    int* d_chunk_next = nullptr;
+    unsigned long long* d_efix = nullptr;
+    // cluster-pair list and chunks of the mixed kernel
+    int2* d_plist = nullptr;
+    long long plist_cap = 0;
+    long long plist_need = 0;          // reported by the last evaluation that overflowed
+    int4* d_chunks = nullptr;
+    long long chunk_cap = 0;
+    long long chunk_need = 0;
     int ncell_cap = 0;
     double* d_erec = nullptr;
     int erec_cap = 0;
@@ -140,6 +161,7 @@ struct pmgpu_force {
     int4* d_hdeltas = nullptr;      // half shell of the mixed kernel
     float4* d_hoff = nullptr;
     float4* d_hoff_lo = nullptr;
+    double4* d_hoff64 = nullptr;
     int nh = 0;
     int half_rule = 0;
     int wrap = 0;
@@ -208,12 +230,19 @@ extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
     sys->device = device;
     e = cudaStreamCreateWithFlags(&sys->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete sys; return PMGPU_ERR_CUDA; }
-    if (cudaMalloc((void**)&sys->d_status, sizeof(int)) != cudaSuccess ||
+    if (cudaMalloc(&sys->d_small, kSmallBytes) != cudaSuccess ||
         cudaMalloc((void**)&sys->d_energy, sizeof(double) * kERec) != cudaSuccess ||
         cudaMallocHost((void**)&sys->h_energy, sizeof(double) * kERec) != cudaSuccess) {
         delete sys;
         return PMGPU_ERR_NOMEM;
     }
+    sys->d_status = (int*)sys->d_small;
+    sys->d_plist_count = sys->d_status + 1;
+    sys->d_plist_need = sys->d_status + 2;
+    sys->d_chunk_count = sys->d_status + 3;
+    sys->d_chunk_need = sys->d_status + 4;
+    sys->d_chunk_next = sys->d_status + 5;
+    sys->d_efix = (unsigned long long*)((char*)sys->d_small + 32);
     *out = sys;
     return PMGPU_OK;
 }
@@ -225,6 +254,7 @@ static void free_atom_buffers(pmgpu_system* s)
     dfree(s->d_xfull); dfree(s->d_xmod); dfree(s->d_xrow); dfree(s->d_xent);
     dfree(s->d_epairs); dfree(s->d_ecls);
     dfree(s->d_pos); dfree(s->d_fout); dfree(s->d_facc32); dfree(s->d_facc40);
+    s->d_facc32p = nullptr;   // second half of d_facc32
     dfree(s->d_cell_lin); dfree(s->d_cell3); dfree(s->d_tmp); dfree(s->d_sorted); dfree(s->d_slot);
     dfree(s->d_spos); dfree(s->d_smeta); dfree(s->d_spos64);
 }
@@ -244,7 +274,8 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     for (cudaEvent_t e : sys->prof_pool) cudaEventDestroy(e);
     free_atom_buffers(sys);
     dfree(sys->d_counts); dfree(sys->d_fill); dfree(sys->d_start); dfree(sys->d_erec);
-    dfree(sys->d_status); dfree(sys->d_energy);
+    dfree(sys->d_small); dfree(sys->d_energy);
+    dfree(sys->d_cstart); dfree(sys->d_cbox); dfree(sys->d_ccell); dfree(sys->d_plist); dfree(sys->d_chunks);
     if (sys->h_energy) cudaFreeHost(sys->h_energy);
     cudaStreamDestroy(sys->stream);
     delete sys;
@@ -304,6 +335,13 @@ extern "C" int pmgpu_synchronize(pmgpu_system* sys)
     CK(cudaMemcpy(&st, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status");
     if (st & kStatusOverflow)
         return fail(sys, PMGPU_ERR_OVERFLOW, "non-finite or out-of-range force (fixed-point range exceeded)");
+    if (st & kStatusListFull) {
+        int need[3] = {0, 0, 0};   // list need, chunk count, chunk need
+        CK(cudaMemcpy(need, sys->d_plist_need, sizeof(need), cudaMemcpyDeviceToHost), "status");
+        sys->plist_need = std::max<long long>(sys->plist_need, need[0]);
+        sys->chunk_need = std::max<long long>(sys->chunk_need, need[2]);
+        return fail(sys, PMGPU_ERR_CAPACITY, "cluster-pair list capacity exceeded (grown for the next evaluation)");
+    }
     return PMGPU_OK;
 }
 
@@ -400,7 +438,8 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     }
     // per-evaluation atom buffers
     CK(dalloc(&sys->d_pos, 3 * (size_t)n), "alloc"); CK(dalloc(&sys->d_fout, 3 * (size_t)n), "alloc");
-    CK(dalloc(&sys->d_facc32, 3 * (size_t)n), "alloc"); CK(dalloc(&sys->d_facc40, 3 * (size_t)n), "alloc");
+    CK(dalloc(&sys->d_facc32, 6 * (size_t)n), "alloc"); CK(dalloc(&sys->d_facc40, 3 * (size_t)n), "alloc");
+    sys->d_facc32p = sys->d_facc32 + 3 * (size_t)n;
     CK(dalloc(&sys->d_cell_lin, n), "alloc"); CK(dalloc(&sys->d_cell3, 3 * (size_t)n), "alloc");
     CK(dalloc(&sys->d_tmp, n), "alloc"); CK(dalloc(&sys->d_sorted, n), "alloc"); CK(dalloc(&sys->d_slot, n), "alloc");
     CK(dalloc(&sys->d_spos, n), "alloc"); CK(dalloc(&sys->d_smeta, n), "alloc"); CK(dalloc(&sys->d_spos64, n), "alloc");
@@ -615,22 +654,28 @@ static int prepare_cutoff(pmgpu_force* f)
     for (const int4& d : deltas)
         if (!reach_ok || d.x > 0 || (d.x == 0 && (d.y > 0 || (d.y == 0 && d.z > 0)))) hd.push_back(d);
     std::vector<float4> ho(hd.size()), hl(hd.size());
+    std::vector<double4> h64(hd.size());
     for (size_t k = 0; k < hd.size(); ++k) {
         double o[3] = {hd[k].x * sys->grid.csx, hd[k].y * sys->grid.csy, hd[k].z * sys->grid.csz};
         float h[3], l[3];
         for (int c = 0; c < 3; ++c) { h[c] = (float)o[c]; l[c] = (float)(o[c] - (double)h[c]); }
         ho[k] = make_float4(h[0], h[1], h[2], 0.f);
         hl[k] = make_float4(l[0], l[1], l[2], 0.f);
+        // the offset the FP32 pair vectors carry (hi + lo), for the virial
+        h64[k] = make_double4((double)h[0] + (double)l[0], (double)h[1] + (double)l[1],
+                              (double)h[2] + (double)l[2], 0.0);
     }
     f->nh = (int)hd.size();
     f->half_rule = reach_ok ? 0 : 1;
     CK(dalloc(&f->d_hdeltas, hd.size()), "alloc");
     CK(dalloc(&f->d_hoff, hd.size()), "alloc");
     CK(dalloc(&f->d_hoff_lo, hd.size()), "alloc");
+    CK(dalloc(&f->d_hoff64, hd.size()), "alloc");
     if (!hd.empty()) {
         CK(cudaMemcpy(f->d_hdeltas, hd.data(), sizeof(int4) * hd.size(), cudaMemcpyHostToDevice), "copy");
         CK(cudaMemcpy(f->d_hoff, ho.data(), sizeof(float4) * ho.size(), cudaMemcpyHostToDevice), "copy");
         CK(cudaMemcpy(f->d_hoff_lo, hl.data(), sizeof(float4) * hl.size(), cudaMemcpyHostToDevice), "copy");
+        CK(cudaMemcpy(f->d_hoff64, h64.data(), sizeof(double4) * h64.size(), cudaMemcpyHostToDevice), "copy");
     }
     f->box_version = sys->box_version;
     return PMGPU_OK;
@@ -803,7 +848,7 @@ static int prepare_pme(pmgpu_force* f)
 static void free_force(pmgpu_force* f)
 {
     dfree(f->d_deltas); dfree(f->d_doff); dfree(f->d_qgrid);
-    dfree(f->d_hdeltas); dfree(f->d_hoff); dfree(f->d_hoff_lo);
+    dfree(f->d_hdeltas); dfree(f->d_hoff); dfree(f->d_hoff_lo); dfree(f->d_hoff64);
     if (f->d_cgrid) cudaFree(f->d_cgrid);
     if (f->d_rgrid) cudaFree(f->d_rgrid);
     if (f->d_tw) cudaFree(f->d_tw);
@@ -857,7 +902,12 @@ static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_po
     a.ljn = sys->d_ljn; a.ljm = sys->d_ljm; a.ljd = sys->d_ljd; a.n_types = sys->t;
     a.deltas = f->d_deltas; a.doff = f->d_doff; a.nd = f->nd;
     a.hdeltas = f->d_hdeltas; a.hoff = f->d_hoff; a.hoff_lo = f->d_hoff_lo; a.nh = f->nh;
-    a.half_rule = f->half_rule; a.ccell = sys->d_ccell;
+    a.half_rule = f->half_rule; a.ccell = sys->d_ccell; a.ncl_cap = sys->cbox_cap;
+    a.plist = sys->d_plist; a.plist_cap = (int)sys->plist_cap;
+    a.chunks = sys->d_chunks; a.chunk_cap = (int)sys->chunk_cap;
+    a.plist_count = sys->d_plist_count; a.plist_need = sys->d_plist_need;
+    a.chunk_count = sys->d_chunk_count; a.chunk_need = sys->d_chunk_need; a.chunk_next = sys->d_chunk_next;
+    a.hoff64 = f->d_hoff64; a.efix = sys->d_efix;
     a.grid = sys->grid; a.pbc = sys->pbc; a.wrap = f->wrap;
     a.lx_lo = (float)(sys->box[0] - (double)(float)sys->box[0]);
     a.ly_lo = (float)(sys->box[4] - (double)(float)sys->box[4]);
@@ -871,8 +921,10 @@ static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_po
     a.guard = 2.0e-5f;
     a.csf = (float)sys->csf; a.csfd = sys->csf;
     a.status = sys->d_status;
+    // mixed forces on whole-cell shifts go to the pair accumulator (their
+    // virial is completed from it at finalize), the small-grid mode to the other
     if (f->precision == PMGPU_PRECISION_FP64) { a.facc = sys->d_facc40; a.scale = kScaleFp64; }
-    else { a.facc = sys->d_facc32; a.scale = kScaleMixed; }
+    else { a.facc = f->wrap ? sys->d_facc32p : sys->d_facc32; a.scale = kScaleMixed; }
 }
 
 static int ensure_erec(pmgpu_system* sys, int need)
@@ -888,8 +940,8 @@ static int ensure_erec(pmgpu_system* sys, int need)
 // energy records one cutoff force writes
 static int pair_records(pmgpu_system* sys, pmgpu_force* f)
 {
-    return f->precision == PMGPU_PRECISION_FP64 ? pair_blocks(sys->grid, f->nd)
-                                                : 4 * pair_blocks_mixed(sys->grid, f->nh);
+    // the mixed kernel sums energies in fixed point (d_efix), no records
+    return f->precision == PMGPU_PRECISION_FP64 ? pair_blocks(sys->grid, f->nd) : 0;
 }
 
 // upper bound of the energy records of the fused x pass (one per CTA, at
@@ -911,6 +963,7 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
         if (f->kind == 0) need += pair_records(sys, f);
         else need += pme_xblocks(f) + 148 * 4;
     }
+    need += (sys->n + 255) / 256;   // finalize: pair virial records
     int r = ensure_erec(sys, need);
     if (r) return r;
     // clusters: at most N / 8 full ones plus one partial per cell
@@ -920,6 +973,28 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
         CK(dalloc(&sys->d_ccell, (size_t)ncl), "alloc");
         sys->cbox_cap = ncl;
         sys->buf_version++;
+    }
+    long long lneed = 0, cneed = 0;
+    for (int k = 0; k < nf; ++k)
+        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) {
+            lneed = std::max(lneed, plist_estimate(sys->n, sys->grid, forces[k]->nh));
+            cneed = std::max(cneed, chunk_estimate(sys->n, sys->grid, forces[k]->nh));
+        }
+    if (lneed > 0) {
+        lneed = std::max(lneed, sys->plist_need + sys->plist_need / 4);
+        cneed = std::max(cneed, sys->chunk_need + sys->chunk_need / 4);
+        if (lneed > INT_MAX || cneed > INT_MAX)
+            return fail(sys, PMGPU_ERR_CAPACITY, "cluster-pair list above 2^31 entries");
+        if (lneed > sys->plist_cap) {
+            CK(dalloc(&sys->d_plist, (size_t)lneed), "alloc");
+            sys->plist_cap = lneed;
+            sys->buf_version++;
+        }
+        if (cneed > sys->chunk_cap) {
+            CK(dalloc(&sys->d_chunks, (size_t)cneed), "alloc");
+            sys->chunk_cap = cneed;
+            sys->buf_version++;
+        }
     }
     pme_init_attributes();
     return PMGPU_OK;
@@ -966,27 +1041,37 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     cudaStream_t s = sys->stream;
     size_t n3 = 3 * (size_t)sys->n;
     int mbin = prof_begin(sys, kPhaseBin);
-    CK(cudaMemsetAsync(sys->d_status, 0, sizeof(int), s), "memset");
-    if (use32) CK(cudaMemsetAsync(sys->d_facc32, 0, sizeof(unsigned long long) * n3, s), "memset");
+    CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
+    if (use32) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
     r = bin(sys, d_pos);
     if (r) return r;
     prof_end(sys, mbin);
     int used = 0;
+    int lists = 0;
+    int pair_virial = 0;
     for (int k = 0; k < nf; ++k) {
         pmgpu_force* f = forces[k];
         bool fp64 = f->precision == PMGPU_PRECISION_FP64;
-        unsigned long long* facc = fp64 ? sys->d_facc40 : sys->d_facc32;
+        unsigned long long* facc = fp64 ? sys->d_facc40 : sys->d_facc32p;
         double scale = fp64 ? kScaleFp64 : kScaleMixed;
         if (f->kind == 0) {
+            if (!fp64 && !f->wrap && virial) pair_virial = 1;
             PairArgs a;
             fill_pair_args(sys, f, d_pos, a);
             a.virial = virial;
             a.erec = sys->d_erec + used;
-            int blocks = fp64 ? pair_blocks(sys->grid, f->nd) : pair_blocks_mixed(sys->grid, f->nh);
+            if (!fp64) {
+                // list count and need, chunk count and need, work counter
+                if (lists++ > 0) CK(cudaMemsetAsync(sys->d_plist_count, 0, 5 * sizeof(int), s), "memset");
+                int ml = prof_begin(sys, kPhaseList);
+                int e = launch_cluster_list(a, s, &sys->launches);
+                if (e) return cuda_fail(sys, (cudaError_t)e, "cluster-pair list");
+                prof_end(sys, ml);
+            }
             int m = prof_begin(sys, kPhasePair);
-            int e = fp64 ? launch_pair_fp64(a, f->combo, blocks, s, &sys->launches)
-                         : launch_pair_mixed(a, f->combo, blocks, s, &sys->launches);
+            int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
+                         : launch_pair_mixed(a, f->combo, s, &sys->launches);
             if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
             prof_end(sys, m);
             used += pair_records(sys, f);
@@ -1042,16 +1127,23 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         }
     }
     int mfin = prof_begin(sys, kPhaseFinalize);
-    if (use32) {
-        int e = launch_finalize(sys->n, sys->d_facc32, sys->d_sorted, 1.0 / kScaleMixed, d_fout, s, &sys->launches);
+    if (use32 || use40) {
+        FinArgs fa;
+        fa.n = sys->n;
+        fa.f32 = use32 ? sys->d_facc32 : nullptr;
+        fa.f32p = use32 ? sys->d_facc32p : nullptr;
+        fa.f40 = use40 ? sys->d_facc40 : nullptr;
+        fa.sorted = sys->d_sorted; fa.spos = sys->d_spos; fa.slo = sys->d_slo;
+        fa.pair_virial = pair_virial;
+        fa.fout = d_fout;
+        fa.erec = sys->d_erec + used; fa.erec_stride = sys->erec_cap;
+        int rec = 0;
+        int e = launch_finalize(fa, s, &sys->launches, &rec);
         if (e) return cuda_fail(sys, (cudaError_t)e, "finalize");
+        used += rec;
     }
-    if (use40) {
-        int e = launch_finalize(sys->n, sys->d_facc40, sys->d_sorted, 1.0 / kScaleFp64, d_fout, s, &sys->launches);
-        if (e) return cuda_fail(sys, (cudaError_t)e, "finalize");
-    }
-    if (used > 0) {
-        int e = launch_energy_reduce(sys->d_erec, sys->erec_cap, used, d_energy, s, &sys->launches);
+    if (nf > 0) {
+        int e = launch_energy_reduce(sys->d_erec, sys->erec_cap, used, sys->d_efix, d_energy, s, &sys->launches);
         if (e) return cuda_fail(sys, (cudaError_t)e, "energy reduce");
     }
     prof_end(sys, mfin);
@@ -1112,13 +1204,20 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
     size_t n3 = 3 * (size_t)sys->n;
     cudaStream_t s = sys->stream;
     CK(cudaMemcpyAsync(sys->d_pos, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, s), "H2D positions");
-    CK(cudaMemsetAsync(sys->d_fout, 0, sizeof(double) * n3, s), "memset");
-    CK(cudaMemsetAsync(sys->d_energy, 0, sizeof(double) * kERec, s), "memset");
-    int r = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy, flags);
-    if (r) return r;
-    CK(cudaMemcpyAsync(sys->h_fbuf.data(), sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
-    CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kERec, cudaMemcpyDeviceToHost, s), "D2H energies");
-    r = pmgpu_synchronize(sys);
+    int r = PMGPU_OK;
+    // a second attempt only when the cluster-pair list outgrew its estimate
+    // (the first attempt recorded the size it needs)
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        CK(cudaMemsetAsync(sys->d_fout, 0, sizeof(double) * n3, s), "memset");
+        CK(cudaMemsetAsync(sys->d_energy, 0, sizeof(double) * kERec, s), "memset");
+        r = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy, flags);
+        if (r) return r;
+        CK(cudaMemcpyAsync(sys->h_fbuf.data(), sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
+        CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kERec, cudaMemcpyDeviceToHost, s), "D2H energies");
+        r = pmgpu_synchronize(sys);
+        if (!(r == PMGPU_ERR_CAPACITY && (sys->plist_need > sys->plist_cap || sys->chunk_need > sys->chunk_cap)))
+            break;
+    }
     if (r) return r;
     for (size_t k = 0; k < n3; ++k) forces_accum[k] += sys->h_fbuf[k];
     energies->lennard_jones += sys->h_energy[0];
@@ -1152,14 +1251,13 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     cudaStream_t s = sys->stream;
     size_t n3 = 3 * (size_t)sys->n;
     CK(cudaMemcpyAsync(sys->d_pos, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, s), "H2D");
-    CK(cudaMemsetAsync(sys->d_status, 0, sizeof(int), s), "memset");
-    CK(cudaMemsetAsync(sys->d_facc32, 0, sizeof(unsigned long long) * n3, s), "memset");
+    CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
+    CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
     r = bin(sys, sys->d_pos);
     if (r) return r;
     bool fp64 = f->precision == PMGPU_PRECISION_FP64;
-    int blocks = fp64 ? pair_blocks(sys->grid, f->nd) : pair_blocks_mixed(sys->grid, f->nh);
-    r = ensure_erec(sys, pair_records(sys, f));
+    r = ensure_erec(sys, std::max(1, pair_records(sys, f)));
     if (r) return r;
     int* d_pairs = nullptr;
     unsigned long long* d_count = nullptr;
@@ -1171,8 +1269,9 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     fill_pair_args(sys, f, sys->d_pos, a);
     a.erec = sys->d_erec;
     a.rec_pairs = d_pairs; a.rec_count = d_count; a.rec_cap = dcap;
-    int e = f->precision == PMGPU_PRECISION_FP64 ? launch_pair_fp64(a, f->combo, blocks, s, &sys->launches)
-                                                 : launch_pair_mixed(a, f->combo, blocks, s, &sys->launches);
+    int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
+                 : launch_cluster_list(a, s, &sys->launches);
+    if (!e && !fp64) e = launch_pair_mixed(a, f->combo, s, &sys->launches);
     unsigned long long cnt = 0;
     if (!e) e = (int)cudaMemcpyAsync(&cnt, d_count, sizeof(cnt), cudaMemcpyDeviceToHost, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
