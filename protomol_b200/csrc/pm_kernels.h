@@ -136,6 +136,7 @@ struct PairArgs {
     int* chunk_next;             // work counter of the pair kernel
     const double4* hoff64;       // FP64 half-shell offsets (hi + lo), virial
     unsigned long long* efix;    // 11 int64 sums (scale 2^32): LJ, Coulomb, virial
+    int reserve;                 // block slots per SM left free for concurrent PME kernels
 };
 
 // Combination id of the registered OneAtomPair[Two] templates.

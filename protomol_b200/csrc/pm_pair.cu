@@ -453,14 +453,17 @@ struct Dispatch;
 template <int NT, int P0, int S0, int P1, int S1, bool WRAP>
 static int run_mixed_w(const PairArgs& a, cudaStream_t s, long long* launches)
 {
-    static int blocks = 0;
-    if (blocks == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
+    static int sms = 0, per_sm = 0;
+    if (sms == 0) {
+        int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_mixed<NT, P0, S0, P1, S1, WRAP>, 128, 0);
-        blocks = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
+        if (sms <= 0) sms = 148;
+        if (per_sm <= 0) per_sm = 1;
     }
+    // with PME kernels running beside it, leave them block slots
+    const int blocks = sms * (per_sm > a.reserve ? per_sm - a.reserve : 1);
     k_pair_mixed<NT, P0, S0, P1, S1, WRAP><<<blocks, 128, 0, s>>>(a);
     *launches += 1;
     return (int)cudaGetLastError();

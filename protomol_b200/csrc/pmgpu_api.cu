@@ -55,6 +55,10 @@ static long long g_next_force_id = 1;
 struct pmgpu_system {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // PME runs on a second, higher-priority stream beside the pair kernels
+    // (forked after binning, joined before finalize)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     long long launches = 0;
     // topology
@@ -230,6 +234,15 @@ extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
     sys->device = device;
     e = cudaStreamCreateWithFlags(&sys->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete sys; return PMGPU_ERR_CUDA; }
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&sys->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sys->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sys->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaStreamDestroy(sys->stream);
+        delete sys;
+        return PMGPU_ERR_CUDA;
+    }
     if (cudaMalloc(&sys->d_small, kSmallBytes) != cudaSuccess ||
         cudaMalloc((void**)&sys->d_energy, sizeof(double) * kERec) != cudaSuccess ||
         cudaMallocHost((void**)&sys->h_energy, sizeof(double) * kERec) != cudaSuccess) {
@@ -277,6 +290,9 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     dfree(sys->d_small); dfree(sys->d_energy);
     dfree(sys->d_cstart); dfree(sys->d_cbox); dfree(sys->d_ccell); dfree(sys->d_plist); dfree(sys->d_chunks);
     if (sys->h_energy) cudaFreeHost(sys->h_energy);
+    cudaEventDestroy(sys->ev_fork);
+    cudaEventDestroy(sys->ev_join);
+    cudaStreamDestroy(sys->side);
     cudaStreamDestroy(sys->stream);
     delete sys;
     return PMGPU_OK;
@@ -1050,6 +1066,16 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     int used = 0;
     int lists = 0;
     int pair_virial = 0;
+    // PME beside the cutoff forces on the side stream (not while profiling,
+    // which times every phase on its own)
+    bool any_cut = false, any_pme = false;
+    for (int k = 0; k < nf; ++k) (forces[k]->kind == 0 ? any_cut : any_pme) = true;
+    const bool fork = any_cut && any_pme && !sys->profiling;
+    cudaStream_t ps = fork ? sys->side : s;
+    if (fork) {
+        CK(cudaEventRecord(sys->ev_fork, s), "fork");
+        CK(cudaStreamWaitEvent(sys->side, sys->ev_fork, 0), "fork");
+    }
     for (int k = 0; k < nf; ++k) {
         pmgpu_force* f = forces[k];
         bool fp64 = f->precision == PMGPU_PRECISION_FP64;
@@ -1070,6 +1096,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 prof_end(sys, ml);
             }
             int m = prof_begin(sys, kPhasePair);
+            a.reserve = fork ? 1 : 0;
             int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
                          : launch_pair_mixed(a, f->combo, s, &sys->launches);
             if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
@@ -1089,7 +1116,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 c.const_virial = f->charged_energy;
                 int b = 0;
                 int m = prof_begin(sys, kPhaseCorrection);
-                int e = launch_pme_correction(c, s, &sys->launches, &b);
+                int e = launch_pme_correction(c, ps, &sys->launches, &b);
                 if (e) return cuda_fail(sys, (cudaError_t)e, "PME correction");
                 prof_end(sys, m);
                 used += b;
@@ -1117,7 +1144,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 for (int st = 0; st < 3; ++st) {
                     int m = prof_begin(sys, phases[st]);
                     int u = 0;
-                    int e = launch_pme_reciprocal(a, fp64 ? 1 : 0, s, &sys->launches,
+                    int e = launch_pme_reciprocal(a, fp64 ? 1 : 0, ps, &sys->launches,
                                                   sys->d_erec + used, &u, stages[st]);
                     if (e) return cuda_fail(sys, (cudaError_t)e, "PME reciprocal");
                     used += u;
@@ -1125,6 +1152,10 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 }
             }
         }
+    }
+    if (fork) {
+        CK(cudaEventRecord(sys->ev_join, sys->side), "join");
+        CK(cudaStreamWaitEvent(s, sys->ev_join, 0), "join");
     }
     int mfin = prof_begin(sys, kPhaseFinalize);
     if (use32 || use40) {
