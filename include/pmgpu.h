@@ -217,6 +217,39 @@ int pmgpu_get_cells(pmgpu_system* sys, int* cells, int* dims);
 int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* force, const double* positions,
                     long long* count, int* pairs, long long cap);
 
+/* ---- allocation-free PME reciprocal term --------------------------------- */
+
+/* No counterpart in the reference.  The PME reciprocal-space term (spread,
+ * FFT with the convolution, gather; the mixed-precision kernels of a PME
+ * force made with -reciprocal only) for callers that must not allocate GPU
+ * memory: code whose device memory is owned by another allocator (a
+ * framework's caching allocator or a memory pool sized to the whole GPU,
+ * where a cudaMalloc fails or breaks the pool's accounting), or code that
+ * may not call cudaMalloc / cudaFree at the point where the force is needed.
+ * Nothing is allocated: the charge grid, spectrum, fixed-point forces and
+ * energy records live in about 8.4 MB of statically reserved memory that
+ * every GPU loading this library holds until the process exits.
+ *   d_positions        N x 3 FP64 (absolute coordinates, orthogonal box),
+ *   d_scaled_charges   N FP64 (charge * sqrt(332.0636), as the topology's),
+ *   box                the three edge lengths, grid the K per axis,
+ *   order              even, 2..12; alpha > 0 (the Ewald splitting);
+ *   d_forces_accum     N x 3 FP64, the forces are added (+=);
+ *   d_energies         11 FP64: [1] += reciprocal energy and, with
+ *                      PMGPU_FLAG_VIRIAL, [2..10] += virial (xx xy xz yx ...).
+ * All pointers d_* are device memory on `device`.  Limits: N <= 65,536
+ * atoms, Kx*Ky*Kz <= 262,144 (64^3), each K <= 1,024, Kx*Ky*(Kz/2+1) <=
+ * 196,608 and Ky*(Kz/2+1) <= 8,192; larger sizes return PMGPU_ERR_CAPACITY.
+ * Runs on `stream` (NULL: the legacy default stream) and returns when the
+ * results are written; PMGPU_ERR_OVERFLOW for non-finite forces.  The first
+ * call on a device looks up the scratch address and initialises it (and
+ * synchronizes the device), so it should come before any stream capture.
+ * Every call shares the one scratch area: calls that overlap on the GPU
+ * (from several host threads) race and must be serialised by the caller. */
+int pmgpu_pme_reciprocal_static(int device, int n_atoms, const double* d_positions,
+                                const double* d_scaled_charges, const double box[3], const int grid[3],
+                                int order, double alpha, double* d_forces_accum, double* d_energies,
+                                unsigned flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,7 +25,7 @@ EXPORTS = [
     "pmgpu_cutoff_create", "pmgpu_pme_create", "pmgpu_force_destroy", "pmgpu_pme_alpha",
     "pmgpu_evaluate", "pmgpu_evaluate_device", "pmgpu_synchronize", "pmgpu_stream",
     "pmgpu_launch_count", "pmgpu_last_error", "pmgpu_get_cells", "pmgpu_get_pairs",
-    "pmgpu_set_profiling", "pmgpu_phase_times",
+    "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
 ]
 PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
 
@@ -89,6 +89,8 @@ def load():
     lib.pmgpu_get_pairs.argtypes = [vp, vp, vp, C.POINTER(C.c_longlong), vp, C.c_longlong]
     lib.pmgpu_set_profiling.argtypes = [vp, C.c_int]
     lib.pmgpu_phase_times.argtypes = [vp, vp, C.c_int, C.POINTER(C.c_longlong)]
+    lib.pmgpu_pme_reciprocal_static.argtypes = [C.c_int, C.c_int, vp, vp, dp, ip, C.c_int, C.c_double,
+                                                vp, vp, C.c_uint, vp]
     _lib = lib
     return lib
 

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <set>
 #include <string>
 #include <vector>
@@ -1314,4 +1315,164 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     *count = (long long)cnt;
     if ((long long)cnt > cap) return fail(sys, PMGPU_ERR_CAPACITY, "pair capacity too small");
     return PMGPU_OK;
+}
+
+// ------------------------------------------------------------------ allocation-free PME reciprocal
+// pmgpu_pme_reciprocal_static: the PME reciprocal-space term (spread, FFT
+// with the convolution, gather) in mixed precision, on scratch memory that
+// the library reserves statically in every GPU that loads it, so that the
+// call itself never allocates.  The kernels are the ones the PME force uses.
+//
+// Layout of the scratch (each part 256-byte aligned):
+//   charge grid   int64  x kStaticGrid
+//   half spectrum float2 x kStaticHalf
+//   real grid     float  x kStaticGrid
+//   forces        int64  x 3 kStaticAtoms (fixed point, 2^32)
+//   identity      int    x kStaticAtoms (atom order = slot order)
+//   records       double x 11 kStaticRecords (energy/virial per FFT block)
+//   twiddles      float2 x 3 kStaticAxis
+//   moduli, exp   double x 3 kStaticAxis each
+//   status        int
+namespace {
+constexpr int kStaticAtoms = 65536;
+constexpr int kStaticGrid = 64 * 64 * 64;
+constexpr int kStaticHalf = 3 * 65536;
+constexpr int kStaticAxis = 1024;
+constexpr int kStaticRecords = 8192;
+
+constexpr size_t st_align(size_t x) { return (x + 255) / 256 * 256; }
+constexpr size_t kOffQgrid = 0;
+constexpr size_t kOffCgrid = kOffQgrid + st_align(sizeof(long long) * kStaticGrid);
+constexpr size_t kOffRgrid = kOffCgrid + st_align(sizeof(float2) * kStaticHalf);
+constexpr size_t kOffFacc = kOffRgrid + st_align(sizeof(float) * kStaticGrid);
+constexpr size_t kOffIdent = kOffFacc + st_align(sizeof(unsigned long long) * 3 * kStaticAtoms);
+constexpr size_t kOffErec = kOffIdent + st_align(sizeof(int) * kStaticAtoms);
+constexpr size_t kOffTw = kOffErec + st_align(sizeof(double) * kERec * kStaticRecords);
+constexpr size_t kOffBfac = kOffTw + st_align(sizeof(float2) * 3 * kStaticAxis);
+constexpr size_t kOffEfac = kOffBfac + st_align(sizeof(double) * 3 * kStaticAxis);
+constexpr size_t kOffStatus = kOffEfac + st_align(sizeof(double) * 3 * kStaticAxis);
+constexpr size_t kStaticBytes = kOffStatus + 256;   // about 8.4 MB
+}  // namespace
+
+// The scratch itself.  In host code this name is only a stand-in for the
+// device symbol: its device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_pme_scratch[kStaticBytes];
+
+__global__ void k_static_identity(int* ident, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) ident[i] = i;
+}
+
+// Device address of the scratch on the current device, looked up (and the
+// identity map filled) on the first call per device.
+static std::mutex g_static_mutex;
+static std::map<int, unsigned char*> g_static_base;
+
+static int static_scratch(int device, unsigned char** base)
+{
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    auto it = g_static_base.find(device);
+    if (it != g_static_base.end()) { *base = it->second; return PMGPU_OK; }
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_pme_scratch) != cudaSuccess || !ptr) return PMGPU_ERR_CUDA;
+    unsigned char* b = (unsigned char*)ptr;
+    k_static_identity<<<(kStaticAtoms + 255) / 256, 256>>>((int*)(b + kOffIdent), kStaticAtoms);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return PMGPU_ERR_CUDA;
+    g_static_base[device] = b;
+    *base = b;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_pme_reciprocal_static(int device, int n_atoms, const double* d_positions,
+                                           const double* d_scaled_charges, const double box[3], const int grid[3],
+                                           int order, double alpha, double* d_forces_accum, double* d_energies,
+                                           unsigned flags, void* stream)
+{
+    if (!box || !grid || !d_forces_accum || !d_energies) return PMGPU_ERR_ARG;
+    if (n_atoms < 0 || (n_atoms > 0 && (!d_positions || !d_scaled_charges))) return PMGPU_ERR_ARG;
+    if (order < 2 || order % 2 != 0 || order > 12) return PMGPU_ERR_ARG;
+    if (!(alpha > 0.0) || !(box[0] > 0.0) || !(box[1] > 0.0) || !(box[2] > 0.0)) return PMGPU_ERR_ARG;
+    const int kx = grid[0], ky = grid[1], kz = grid[2];
+    if (kx < order || ky < order || kz < order) return PMGPU_ERR_ARG;
+    const int kzh = kz / 2 + 1;
+    // the sizes the static scratch holds
+    if (n_atoms > kStaticAtoms || kx > kStaticAxis || ky > kStaticAxis || kz > kStaticAxis ||
+        (long long)kx * ky * kz > kStaticGrid || (long long)kx * ky * kzh > kStaticHalf ||
+        (long long)ky * kzh > kStaticRecords)
+        return PMGPU_ERR_CAPACITY;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess) return PMGPU_ERR_CUDA;
+    unsigned char* base = nullptr;
+    int r = static_scratch(device, &base);
+    if (r) { cudaSetDevice(prev); return r; }
+    cudaStream_t s = (cudaStream_t)stream;
+    const double LX = box[0], LY = box[1], LZ = box[2];
+    const double fac = kPi * kPi / (alpha * alpha);
+    // exp tables, B-spline moduli and twiddles, as for the PME force
+    std::vector<double> ef, bf;
+    for (int i = 0; i < kx; i++) { double m = (i <= kx / 2 ? i : i - kx) / LX; ef.push_back(std::exp(-fac * m * m)); }
+    for (int j = 0; j < ky; j++) { double m = (j <= ky / 2 ? j : j - ky) / LY; ef.push_back(std::exp(-fac * m * m)); }
+    for (int k = 0; k < kzh; k++) { double m = k / LZ; ef.push_back(std::exp(-fac * m * m)); }
+    std::vector<double> mx, my, mz;
+    dftmod(order, kx, mx); dftmod(order, ky, my); dftmod(order, kz, mz);
+    bf.insert(bf.end(), mx.begin(), mx.end()); bf.insert(bf.end(), my.begin(), my.end());
+    bf.insert(bf.end(), mz.begin(), mz.begin() + kzh);
+    std::vector<float> tw;
+    const int ns[3] = {kx, ky, kz};
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < ns[a]; ++k) {
+            long double ang = 2.0L * 3.141592653589793238462643383279502884L * k / ns[a];
+            tw.push_back((float)cosl(ang));
+            tw.push_back((float)-sinl(ang));
+        }
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    ok(cudaMemcpyAsync(base + kOffEfac, ef.data(), sizeof(double) * ef.size(), cudaMemcpyHostToDevice, s));
+    ok(cudaMemcpyAsync(base + kOffBfac, bf.data(), sizeof(double) * bf.size(), cudaMemcpyHostToDevice, s));
+    ok(cudaMemcpyAsync(base + kOffTw, tw.data(), sizeof(float) * tw.size(), cudaMemcpyHostToDevice, s));
+    // what must start at zero: status and the fixed-point forces (the
+    // charge grid is cleared by the spread stage itself)
+    ok(cudaMemsetAsync(base + kOffStatus, 0, sizeof(int), s));
+    if (n_atoms > 0) ok(cudaMemsetAsync(base + kOffFacc, 0, sizeof(unsigned long long) * 3 * (size_t)n_atoms, s));
+    PmeArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = n_atoms; a.pos = d_positions; a.q = d_scaled_charges;
+    a.sorted = (const int*)(base + kOffIdent); a.slot_of = (const int*)(base + kOffIdent);
+    a.kx = kx; a.ky = ky; a.kz = kz; a.kzh = kzh; a.order = order;
+    a.hxr = kx / LX; a.hyr = ky / LY; a.hzr = kz / LZ;
+    a.offx = -(order - 1) / 2 + kx; a.offy = -(order - 1) / 2 + ky; a.offz = -(order - 1) / 2 + kz;
+    a.qgrid = (long long*)(base + kOffQgrid); a.cgrid = base + kOffCgrid; a.rgrid = base + kOffRgrid;
+    a.tw = base + kOffTw; a.twx = 0; a.twy = kx; a.twz = kx + ky;
+    a.bfac = (const double*)(base + kOffBfac); a.efac = (const double*)(base + kOffEfac);
+    a.piVr = 1.0 / (kPi * (LX * LY * LZ)); a.fac = fac;
+    a.wr = 1.0 / LX; a.lr = 1.0 / LY; a.hr = 1.0 / LZ;
+    a.facc = (unsigned long long*)(base + kOffFacc); a.scale = kScaleMixed; a.qscale = kScaleFp64;
+    a.erec_stride = kStaticRecords; a.status = (int*)(base + kOffStatus);
+    a.virial = (flags & PMGPU_FLAG_VIRIAL) ? 1 : 0;
+    pme_init_attributes();
+    long long launches = 0;
+    int records = 0;
+    double* erec = (double*)(base + kOffErec);
+    const int stages[3] = {kStageSpread, kStageFft, kStageGather};
+    for (int st = 0; st < 3 && e == cudaSuccess; ++st) {
+        int u = 0;
+        ok((cudaError_t)launch_pme_reciprocal(a, 0, s, &launches, erec + records, &u, stages[st]));
+        records += u;
+    }
+    if (e == cudaSuccess) {
+        FinArgs fa;
+        memset(&fa, 0, sizeof(fa));
+        fa.n = n_atoms; fa.f32p = a.facc; fa.sorted = a.sorted; fa.fout = d_forces_accum;
+        int rec = 0;
+        ok((cudaError_t)launch_finalize(fa, s, &launches, &rec));
+    }
+    if (e == cudaSuccess) ok((cudaError_t)launch_energy_reduce(erec, kStaticRecords, records, nullptr, d_energies, s, &launches));
+    ok(cudaStreamSynchronize(s));
+    int st = 0;
+    ok(cudaMemcpy(&st, base + kOffStatus, sizeof(int), cudaMemcpyDeviceToHost));
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return PMGPU_ERR_CUDA;
+    return (st & kStatusOverflow) ? PMGPU_ERR_OVERFLOW : PMGPU_OK;
 }
