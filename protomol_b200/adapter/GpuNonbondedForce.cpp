@@ -289,8 +289,8 @@ namespace ProtoMol
 		reg2<CutoffSwitchingFunction, CutoffSwitchingFunction, CoulombEwaldRealForce>(CUT, CUT, EW);
 		// new: LennardJones Coulomb -switchingFunction C2 -switchingFunction C2 (one fused pass)
 		reg2<C2SwitchingFunction, C2SwitchingFunction, CoulombForce>(C2, C2, CO);
-		// registerForceExemplarsFastElectrostatic.cpp:50-55 (the -real variants
-		// are registered too; pmgpu rejects -real until the GPU real term exists)
+		// registerForceExemplarsFastElectrostatic.cpp:50-55; -real runs on the GPU
+		// for boxes whose every edge exceeds 2 cutoff (no lattice images)
 		std::vector<std::string> none, pme;
 		pme.push_back("CoulombPME");
 		regpme<true, true, true>(pme);

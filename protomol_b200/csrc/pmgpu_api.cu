@@ -184,6 +184,9 @@ struct pmgpu_force {
     double* d_efac = nullptr;
     double self_energy = 0.0, charged_energy = 0.0;
     int twx = 0, twy = 0, twz = 0;
+    // -real: the real-space term as an internal CoulombEwaldReal / Cutoff
+    // pair force (owned by this force, evaluated before it)
+    pmgpu_force* real_sub = nullptr;
 };
 
 // ------------------------------------------------------------------ helpers
@@ -756,8 +759,6 @@ extern "C" int pmgpu_pme_create(pmgpu_system* sys, const pmgpu_pme_params* p, pm
     for (int k = 0; k < 3; ++k)
         if (!smooth_ok(p->grid[k]) || p->grid[k] > 4096)
             return fail(sys, PMGPU_ERR_UNSUPPORTED, "PME grid size needs prime factors <= 16 and <= 4096");
-    if (p->real) return fail(sys, PMGPU_ERR_UNSUPPORTED, "PMEwald -real on the GPU: use the split form "
-                                                         "(CoulombEwaldReal cutoff force + -reciprocal -correction)");
     if (p->precision != PMGPU_PRECISION_MIXED && p->precision != PMGPU_PRECISION_FP64)
         return fail(sys, PMGPU_ERR_ARG, "unknown precision");
     if (!sys->box_set || sys->n == 0 && sys->q.empty()) {
@@ -780,6 +781,23 @@ extern "C" int pmgpu_pme_create(pmgpu_system* sys, const pmgpu_pme_params* p, pm
         }
     }
     f->alpha = alpha;
+    if (p->real) {
+        // realTerm (:658-768) with only the zero lattice vector (every box
+        // edge > 2 Rc, checked at evaluation) is the CoulombEwaldReal pair
+        // force with a Cutoff switch at Rc: same pair set, exclusions (FULL
+        // skipped, MODIFIED scaled by csf), poly5 energy and force
+        pmgpu_cutoff_params cp;
+        memset(&cp, 0, sizeof(cp));
+        cp.n_terms = 1;
+        cp.pot[0] = PMGPU_POT_EWALD_REAL; cp.sw[0] = PMGPU_SW_CUTOFF;
+        cp.cutoff[0] = rc; cp.alpha[0] = alpha; cp.algorithm_cutoff = rc;
+        cp.precision = p->precision;
+        pmgpu_force* sub = nullptr;
+        int r = pmgpu_cutoff_create(sys, &cp, &sub);
+        if (r) { delete f; return r; }
+        sys->forces.erase(sub);
+        f->real_sub = sub;
+    }
     sys->forces.insert(f);
     *out = f;
     return PMGPU_OK;
@@ -789,6 +807,10 @@ static int prepare_pme(pmgpu_force* f)
 {
     pmgpu_system* sys = f->sys;
     if (f->box_version == sys->box_version) return PMGPU_OK;
+    if (f->real_sub && !(std::fabs(sys->box[0]) > 2.0 * f->pp.cutoff && std::fabs(sys->box[4]) > 2.0 * f->pp.cutoff &&
+                         std::fabs(sys->box[8]) > 2.0 * f->pp.cutoff))
+        return fail(sys, PMGPU_ERR_UNSUPPORTED, "PMEwald -real needs every box edge > 2 cutoff on the GPU "
+                                                "(no lattice images)");
     const pmgpu_pme_params& p = f->pp;
     int kx = p.grid[0], ky = p.grid[1], kz = p.grid[2];
     f->kzh = kz / 2 + 1;
@@ -864,6 +886,7 @@ static int prepare_pme(pmgpu_force* f)
 
 static void free_force(pmgpu_force* f)
 {
+    if (f->real_sub) free_force(f->real_sub);
     dfree(f->d_deltas); dfree(f->d_doff); dfree(f->d_qgrid);
     dfree(f->d_hdeltas); dfree(f->d_hoff); dfree(f->d_hoff_lo); dfree(f->d_hoff64);
     if (f->d_cgrid) cudaFree(f->d_cgrid);
@@ -1184,9 +1207,18 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
 
 // prepare, then enqueue -- replaying a captured CUDA graph when the same
 // forces run on the same buffers again (the evaluation is one graph launch)
-static int eval_core(pmgpu_system* sys, int nf, pmgpu_force* const* forces, const double* d_pos,
+static int eval_core(pmgpu_system* sys, int nf_in, pmgpu_force* const* forces_in, const double* d_pos,
                      double* d_fout, double* d_energy, unsigned flags)
 {
+    // a PME force with -real brings its real-space pair force along
+    std::vector<pmgpu_force*> all;
+    for (int k = 0; k < nf_in; ++k) {
+        if (!forces_in || !forces_in[k]) return fail(sys, PMGPU_ERR_ARG, "bad force list");
+        if (forces_in[k]->real_sub) all.push_back(forces_in[k]->real_sub);
+        all.push_back(forces_in[k]);
+    }
+    const int nf = (int)all.size();
+    pmgpu_force* const* forces = all.data();
     int r = eval_prepare(sys, nf, forces);
     if (r) return r;
     if (sys->profiling || !sys->use_graphs) return eval_enqueue(sys, nf, forces, d_pos, d_fout, d_energy, flags);
@@ -1275,6 +1307,7 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
                                long long* count, int* pairs, long long cap)
 {
     if (!sys || !f || !positions || !count || (cap > 0 && !pairs)) return PMGPU_ERR_ARG;
+    if (f->kind != 0 && f->real_sub) f = f->real_sub;   // PME -real: its real-space pairs
     if (f->kind != 0) return fail(sys, PMGPU_ERR_UNSUPPORTED, "pair recording is for cutoff forces");
     if (!sys->box_set) return fail(sys, PMGPU_ERR_STATE, "box not set");
     cudaSetDevice(sys->device);

@@ -149,12 +149,9 @@ class SystemForce:
         except Exception:
             pass
 
-
-class NonbondedCutoffSystemForce(SystemForce):
-    keyword = "NonbondedCutoff"
-
     def pairs(self, positions, cap=None):
-        """Within-cutoff pair set of this force on ``positions`` (diagnostic)."""
+        """Within-cutoff pair set of this force on ``positions`` (diagnostic; for
+        PMEwald -real the pairs of its real-space term)."""
         pos = np.ascontiguousarray(positions, np.float64)
         cap = cap or max(1024, pos.shape[0] * 1200)
         out = np.zeros((cap, 2), np.int32)
@@ -162,6 +159,10 @@ class NonbondedCutoffSystemForce(SystemForce):
         check(_lib.load().pmgpu_get_pairs(self.topo.handle, self.handle, pos.ctypes.data_as(_VP), C.byref(cnt),
                                           out.ctypes.data_as(_VP), cap), self.topo.handle)
         return out[: cnt.value]
+
+
+class NonbondedCutoffSystemForce(SystemForce):
+    keyword = "NonbondedCutoff"
 
 
 class NonbondedPMEwaldSystemForce(SystemForce):

@@ -40,13 +40,19 @@ def run_driver(system, defs, precision="mixed", repeat=1):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("case", ["water216", "chain14281"])
+@pytest.mark.parametrize("case", ["water216", "chain14281", "chain14281_pme_full"])
 def test_force_factory_keywords_run_on_the_gpu(case, precision):
     w = workloads.water216() if case == "water216" else workloads.chain14281()
-    r = run_driver(w.system, w.forces, precision)
-    ref = oracle.evaluate(w.system, [F.parse_definition(d) for d in w.forces])
+    system, defs = w.system, w.forces
+    if case == "chain14281_pme_full":
+        # LJ cutoff force + the whole PME force (-real -reciprocal -correction)
+        defs = ["LennardJones -switchingFunction C2 -algorithm NonbondedCutoff -switchon 10 -cutoff 12 -cutoff 12",
+                "Coulomb -algorithm PMEwald -real -reciprocal -correction -interpolation BSpline "
+                "-gridsize 64 64 64 -cutoff 12 -order 4 -alpha 0.32"]
+    r = run_driver(system, defs, precision)
+    ref = oracle.evaluate(system, [F.parse_definition(d) for d in defs])
     # the factory matched the reference ids (same strings as the reference)
-    for d, made in zip(w.forces, r["made"]):
+    for d, made in zip(defs, r["made"]):
         assert made.split()[0] == d.split()[0]
         assert "-algorithm" in made
     err = np.sqrt(((r["forces"] - ref["forces"]) ** 2).sum() / (ref["forces"] ** 2).sum())

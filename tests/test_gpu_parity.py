@@ -48,6 +48,12 @@ def small_chain():
     return systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
 
 
+PME_FULL = ("Coulomb -algorithm PMEwald -real -reciprocal -correction -interpolation BSpline "
+            "-gridsize 24 24 24 -cutoff 9 -alpha 0.35")
+EWALD_REAL_9 = ("CoulombEwaldReal -switchingFunction Cutoff -algorithm NonbondedCutoff -cutoff 9 -alpha 0.35 "
+                "-cutoff 9")
+
+
 CASES = {
     "water216_c2": (systems.water_box_216, workloads.water216().forces),
     "small_split_pme": (small_chain, [workloads.lj_ewald_split(7, 9, 0.35),
@@ -70,6 +76,8 @@ CASES = {
     "small_pme_default_alpha": (small_chain, ["Coulomb -algorithm PMEwald -reciprocal -correction -interpolation "
                                               "BSpline -gridsize 25 27 30 -cutoff 9"]),
     "smallbox_wrap": (lambda: systems.water_box(100, seed=7), workloads.water_box_workload(100, 7).forces),
+    # realTerm on the GPU: the whole PME force in one keyword (box edge 24 > 2 Rc)
+    "small_pme_full": (small_chain, [PME_FULL]),
 }
 
 
@@ -132,9 +140,14 @@ def test_cell_assignment_bit_exact(name):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("case", ["water216", "chain14281", "wrap", "c2_fused"])
+@pytest.mark.parametrize("case", ["water216", "chain14281", "wrap", "c2_fused", "pme_real"])
 def test_pair_set_bit_exact(case, precision, chain14281):
-    if case == "water216":
+    oracle_def = None
+    if case == "pme_real":
+        # the real-space pairs of PMEwald -real are those of the Ewald-real
+        # cutoff force at the same cutoff (realTerm with no lattice images)
+        s, d, oracle_def = small_chain(), PME_FULL, EWALD_REAL_9
+    elif case == "water216":
         s, d = systems.water_box_216(), workloads.water216().forces[0]
     elif case == "chain14281":
         s, d = chain14281, workloads.chain14281().forces[0]
@@ -145,7 +158,7 @@ def test_pair_set_bit_exact(case, precision, chain14281):
     topo = F.Topology(s)
     force = F.ForceFactory.make(topo, d, precision)
     gp = force.pairs(s.positions)
-    op = oracle.evaluate(s, [F.parse_definition(d)], want_pairs=True)["pairs"]
+    op = oracle.evaluate(s, [F.parse_definition(oracle_def or d)], want_pairs=True)["pairs"]
     key = lambda p: np.sort(p[:, 0].astype(np.int64) * s.n_atoms + p[:, 1])
     assert len(gp) == len(op)
     assert np.array_equal(key(gp), key(op))
@@ -234,6 +247,14 @@ def test_empty_and_sparse_systems():
         ref = oracle.evaluate(sparse, [F.parse_definition(d) for d in workloads.water216().forces])
         _, _, f, e = gpu_eval(sparse, workloads.water216().forces, precision)
         assert rel_rms(f, ref["forces"]) <= MIXED_FORCE_RTOL
+
+
+def test_pme_real_needs_boxes_without_lattice_images():
+    s = systems.water_box(100, seed=7)           # edge < 2 x 9 A: realTerm would add images
+    assert min(s.box[k][k] for k in range(3)) < 18.0
+    with pytest.raises(_lib.PmgpuError) as ei:
+        gpu_eval(s, [PME_FULL.replace("-gridsize 24 24 24", "-gridsize 16 16 16")], "mixed")
+    assert ei.value.code == 5
 
 
 def test_pme_rejects_what_the_reference_rejects(small_chain):
