@@ -479,24 +479,34 @@ int launch_pme_reciprocal(const PmeArgs& a, int fp64, cudaStream_t s, long long*
 }
 
 // The FFT passes stage two line buffers in dynamic shared memory; allow the
-// opt-in maximum once so that launches (also inside graph capture) need no
-// attribute calls.
+// opt-in maximum (less the kernel's static shared memory, or the attribute is
+// refused) once per device, so that launches (also inside graph capture)
+// need no attribute calls.
+template <typename K>
+static void allow_dynamic_smem(K kernel, int optin)
+{
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 void pme_init_attributes()
 {
-    static bool done = false;
-    if (done) return;
+    static unsigned long long done = 0;   // one bit per device
     int dev = 0, mx = 48 * 1024;
     cudaGetDevice(&dev);
+    if (dev < 64 && (done >> dev) & 1ull) return;
     cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncSetAttribute(k_fft_pass<float, kModeZR2C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_fft_pass<float, kModeY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_fft_pass<float, kModeXConv>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_fft_pass<float, kModeZC2R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_fft_pass<double, kModeZR2C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_fft_pass<double, kModeY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_fft_pass<double, kModeXConv>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_fft_pass<double, kModeZC2R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    done = true;
+    allow_dynamic_smem(k_fft_pass<float, kModeZR2C>, mx);
+    allow_dynamic_smem(k_fft_pass<float, kModeY>, mx);
+    allow_dynamic_smem(k_fft_pass<float, kModeXConv>, mx);
+    allow_dynamic_smem(k_fft_pass<float, kModeZC2R>, mx);
+    allow_dynamic_smem(k_fft_pass<double, kModeZR2C>, mx);
+    allow_dynamic_smem(k_fft_pass<double, kModeY>, mx);
+    allow_dynamic_smem(k_fft_pass<double, kModeXConv>, mx);
+    allow_dynamic_smem(k_fft_pass<double, kModeZC2R>, mx);
+    cudaGetLastError();   // a refused attribute surfaces at the launch that needs it
+    if (dev < 64) done |= 1ull << dev;
 }
 
 // ------------------------------------------------------------------ correction

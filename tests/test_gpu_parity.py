@@ -272,3 +272,25 @@ def test_pme_default_alpha_matches_reference_bisection(small_chain):
     f = F.ForceFactory.make(topo, CASES["small_pme_default_alpha"][1][0])
     r = oracle.evaluate(small_chain, [F.parse_definition(CASES["small_pme_default_alpha"][1][0])])
     assert f.alpha == r["alpha"] == systems.ewald_alpha(9.0)
+
+
+def test_million_atom_box_at_full_size():
+    """The 1,000,000-atom configuration (333,333 waters + Na+, 215.4 A, cutoff
+    12, PME 216^3) at full size, through size-independent properties: the
+    binning is bit-exact with the oracle's cell assignment, and the mixed
+    path agrees with the FP64 kernels (themselves pinned to the oracle on the
+    smaller systems) within the mixed tolerances."""
+    w = workloads.water1m()
+    s = w.system
+    assert s.n_atoms == 1_000_000
+    topo_m, _, fm, em = gpu_eval(s, w.forces, "mixed")
+    cells, dims = topo_m.cells()
+    ocells, odims, _ = oracle.cell_assign(s, s.positions)
+    assert dims == odims and np.array_equal(cells, ocells)
+    topo_m.close()
+    _, _, fd, ed = gpu_eval(s, w.forces, "fp64")
+    assert np.isfinite(fm).all() and np.abs(fd).max() > 0
+    assert rel_rms(fm, fd) <= MIXED_FORCE_RTOL
+    assert np.abs(em.virial_tensor - ed.virial_tensor).max() <= MIXED_ENERGY_RTOL * np.abs(ed.virial_tensor).max() * 10
+    # the LJ sum has no FP32 FFT in it: within the metric-system bound
+    assert abs(em.lennard_jones - ed.lennard_jones) <= MIXED_METRIC_ENERGY_RTOL * abs(ed.lennard_jones)
