@@ -140,6 +140,15 @@ __device__ __forceinline__ int excl_class(const PairArgs& p, int oi, int oj)
 #define PM_HI(x) ((float)(x))
 #define PM_LO(x) ((float)((x) - (double)(float)(x)))
 
+// 1/x: the hardware approximation and one Newton-Raphson step
+// (y' = y + y (1 - x y)), faithful to ~1 ulp for normal x
+__device__ __forceinline__ float rcp_nr(float x)
+{
+    float y = __fdividef(1.0f, x);
+    float e = fmaf(-x, y, 1.0f);
+    return fmaf(y, e, y);
+}
+
 __device__ __forceinline__ float poly5f(float ar)
 {
     // poly5 (base/mathutilities.cpp:29-40), Abramowitz & Stegun 7.1.26.  The
@@ -147,7 +156,7 @@ __device__ __forceinline__ float poly5f(float ar)
     // compensated (hi + lo) instead of biasing the real-space Ewald sum.
     const double E1 = 0.254829592, E2 = -0.284496736, E3 = 1.421413741,
                  E4 = -1.453152027, E5 = 1.061405429, PP = 0.3275911;
-    float t = __frcp_rn(fmaf(PM_HI(PP), ar, fmaf(PM_LO(PP), ar, 1.0f)));
+    float t = rcp_nr(fmaf(PM_HI(PP), ar, fmaf(PM_LO(PP), ar, 1.0f)));
     // each remainder is added after the O(1) partial result it corrects
     float h = fmaf(t, PM_HI(E5), PM_HI(E4)) + fmaf(t, PM_LO(E5), PM_LO(E4));
     h = fmaf(t, h, PM_HI(E3)) + PM_LO(E3);

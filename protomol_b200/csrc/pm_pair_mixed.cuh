@@ -410,9 +410,20 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
                     const bool vb = vi && jg + 4 < nj && (!diag || jg + 4 > il);
                     const PairGeo ga = pair_geo<NT, S0, S1, WRAP>(p, ia, ca, ox, oy, oz, olx, oly, olz, va);
                     const PairGeo gb = pair_geo<NT, S0, S1, WRAP>(p, ia, cb, ox, oy, oz, olx, oly, olz, vb);
-                    float fta, ela, eca, ftb, elb, ecb;
-                    pair_math<NT, P0, S0, P1, S1>(p, ga, ia, ca, fta, ela, eca);
-                    pair_math<NT, P0, S0, P1, S1>(p, gb, ia, cb, ftb, elb, ecb);
+                    // the math only for the 8x4 half-tiles (j-atoms 0-3 and
+                    // 4-7, spatially separate halves of the cluster) that hold a
+                    // pair inside the cutoff: about 40% of them hold none
+                    const bool any_a = __any_sync(FULL, ga.act), any_b = __any_sync(FULL, gb.act);
+                    if (!(any_a || any_b)) goto next_cluster;
+                    float fta = 0.f, ela = 0.f, eca = 0.f, ftb = 0.f, elb = 0.f, ecb = 0.f;
+                    if (any_a && any_b) {
+                        pair_math<NT, P0, S0, P1, S1>(p, ga, ia, ca, fta, ela, eca);
+                        pair_math<NT, P0, S0, P1, S1>(p, gb, ia, cb, ftb, elb, ecb);
+                    } else {
+                        float ft, e1, e2;
+                        pair_math<NT, P0, S0, P1, S1>(p, any_a ? ga : gb, ia, any_a ? ca : cb, ft, e1, e2);
+                        if (any_a) { fta = ft; ela = e1; eca = e2; } else { ftb = ft; elb = e1; ecb = e2; }
+                    }
                     const float x1 = ga.dx * fta, y1 = ga.dy * fta, z1 = ga.dz * fta;
                     const float x2 = gb.dx * ftb, y2 = gb.dy * ftb, z2 = gb.dz * ftb;
                     fi[0][0] -= x1 + x2; fi[0][1] -= y1 + y2; fi[0][2] -= z1 + z2;
@@ -442,6 +453,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
                         }
                     }
                 }
+              next_cluster:
                 // rotate: the next cluster's forces become fi[0]
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
