@@ -215,6 +215,8 @@ struct FinArgs {
     const unsigned long long* f32;      // mixed pair forces (whole-cell shifts), 2^32
     const unsigned long long* f32p;     // other mixed forces (PME, per-pair minimal image), 2^32
     const unsigned long long* f40;      // FP64 forces, 2^40
+    const unsigned long long* a32;      // in atom order (PME): mixed, 2^32
+    const unsigned long long* a40;      // in atom order (PME): FP64, 2^40
     const int* sorted;
     const float4* spos;
     const float4* slo;

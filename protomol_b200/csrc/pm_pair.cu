@@ -487,8 +487,9 @@ static int run_mixed(const PairArgs& a, cudaStream_t s, long long* launches)
 
 int launch_cluster_list(const PairArgs& a, cudaStream_t s, long long* launches)
 {
-    // one warp per cell
-    int lb = (int)(((long long)a.grid.ncell + 3) / 4);
+    // one warp per cell and block of 32 half-shell cells
+    long long warps = (long long)a.grid.ncell * ((a.nh + 1 + 31) / 32);
+    int lb = (int)((warps + 3) / 4);
     k_cluster_list<<<lb > 0 ? lb : 1, 128, 0, s>>>(a);
     *launches += 1;
     return (int)cudaGetLastError();

@@ -7,15 +7,16 @@
 // (k_cluster_box).  Up to four consecutive clusters of a cell form an
 // i-supercluster (32 atoms).
 //
-// K2a k_cluster_list: one warp per cell.  For each i-supercluster of the cell
-// it lists every j-cluster of the half shell -- the cell itself (j-clusters
-// >= the supercluster's first) and the positive half of the reference's
+// K2a k_cluster_list: one warp per cell and block of 32 half-shell cells.
+// For each i-supercluster of the cell it lists every j-cluster of those
+// cells of the half shell -- the cell itself (j-clusters >= the
+// supercluster's first) and the positive half of the reference's
 // neighbour-cell deltas, which covers every unordered cell pair once (in the
 // small-grid mode, where a periodic image can occur twice among the deltas,
 // the reference's list with its B > A rule) -- whose bounding box comes within
 // the cutoff (plus the FP32 guard band) of at least one of the supercluster's
-// cluster boxes, with a 4-bit mask of those i-clusters.  The entries of a
-// supercluster are contiguous and cut into chunks of kChunk entries.  The
+// cluster boxes, with a 4-bit mask of those i-clusters.  A warp's entries of
+// a supercluster are contiguous and cut into chunks of kChunk entries.  The
 // interacting pair set is the reference's: only the order in which a pair's
 // two atoms are visited differs, and forces are accumulated in
 // order-independent fixed point.
@@ -107,17 +108,21 @@ __device__ __forceinline__ unsigned near_mask(const PairArgs& p, const Cand& c, 
 
 __global__ void __launch_bounds__(128) k_cluster_list(PairArgs p)
 {
+    // one warp per (cell, block of 32 half-shell cells): the warp's entries of
+    // a supercluster are contiguous and cut into their own chunks
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int A = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int gw = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const CellGrid& cg = p.grid;
+    const int nkb = (p.nh + 1 + 31) / 32;                    // slot 0: the cell itself
+    const int A = gw / nkb;
     if (A >= cg.ncell) return;                               // warp-uniform
+    const int k = (gw - A * nkb) * 32 + lane - 1;
     const int ca0 = p.cstart[A], ca1 = p.cstart[A + 1];
     const int sa = p.start[A], ea = p.start[A + 1];
     const int ax = A / (cg.ny * cg.nz), ay = (A / cg.nz) % cg.ny, az = A % cg.nz;
     // tiles farther apart than this (FP32 box distance^2) hold no pair
     const float lim = p.cut2f * (1.0f + 8.0f * p.guard) + 1e-3f;
-    const int nk = p.nh + 1;                                 // slot 0: the cell itself
     for (int ic0 = ca0; ic0 < ca1; ic0 += kSuper) {
         const int nsc = min(kSuper, ca1 - ic0);
         const int ifirst = sa + (ic0 - ca0) * kCluster;
@@ -128,13 +133,17 @@ __global__ void __launch_bounds__(128) k_cluster_list(PairArgs p)
             const int ic = min(ic0 + q, ca1 - 1);
             ilo[q] = p.cbox[2 * ic]; ihi[q] = p.cbox[2 * ic + 1];
         }
-        // count, reserve, then count again per lane and write at scanned offsets
-        int ne = 0;
-        for (int kb = 0; kb < nk; kb += 32) {
-            const Cand c = candidate(p, A, ax, ay, az, ic0, ca1, kb + lane - 1);
-            for (int jc = c.jb; jc < c.je; ++jc) ne += near_mask(p, c, jc, ilo, ihi, nsc, ic0, lim) ? 1 : 0;
+        const Cand c = candidate(p, A, ax, ay, az, ic0, ca1, k);
+        int cnt = 0;
+        for (int jc = c.jb; jc < c.je; ++jc) cnt += near_mask(p, c, jc, ilo, ihi, nsc, ic0, lim) ? 1 : 0;
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int v = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += v;
         }
-        for (int o = 16; o > 0; o >>= 1) ne += __shfl_xor_sync(FULL, ne, o);
+        const int ne = __shfl_sync(FULL, incl, 31);
+        if (ne == 0) continue;
         const int nch = (ne + kChunk - 1) / kChunk;
         int b0 = 0, b1 = 0;
         if (lane == 0) {
@@ -144,28 +153,15 @@ __global__ void __launch_bounds__(128) k_cluster_list(PairArgs p)
             if (b1 + nch > p.chunk_cap) { atomicOr(p.status, kStatusListFull); atomicMax(p.chunk_need, b1 + nch); }
         }
         const int ebase = __shfl_sync(FULL, b0, 0), cbase = __shfl_sync(FULL, b1, 0);
-        int run = 0;
-        for (int kb = 0; kb < nk; kb += 32) {
-            const Cand c = candidate(p, A, ax, ay, az, ic0, ca1, kb + lane - 1);
-            int cnt = 0;
-            for (int jc = c.jb; jc < c.je; ++jc) cnt += near_mask(p, c, jc, ilo, ihi, nsc, ic0, lim) ? 1 : 0;
-            int incl = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int v = __shfl_up_sync(FULL, incl, o);
-                if (lane >= o) incl += v;
+        int w = ebase + incl - cnt;
+        for (int jc = c.jb; jc < c.je && cnt > 0; ++jc) {
+            const unsigned m = near_mask(p, c, jc, ilo, ihi, nsc, ic0, lim);
+            if (!m) continue;
+            if (w < p.plist_cap) {
+                const int jfirst = c.sb + (jc - c.cb0) * kCluster;
+                p.plist[w] = make_int2(jfirst, entry_y(c.k, min(kCluster, c.eb - jfirst), m));
             }
-            int w = ebase + run + incl - cnt;
-            run += __shfl_sync(FULL, incl, 31);
-            for (int jc = c.jb; jc < c.je && cnt > 0; ++jc) {
-                const unsigned m = near_mask(p, c, jc, ilo, ihi, nsc, ic0, lim);
-                if (!m) continue;
-                if (w < p.plist_cap) {
-                    const int jfirst = c.sb + (jc - c.cb0) * kCluster;
-                    p.plist[w] = make_int2(jfirst, entry_y(c.k, min(kCluster, c.eb - jfirst), m));
-                }
-                ++w;
-            }
+            ++w;
         }
         // chunk descriptors: {first i slot, i atoms, first entry, entries}
         for (int t = lane; t < nch; t += 32)

@@ -375,7 +375,8 @@ __global__ void k_gather(PmeArgs a)
         }
     }
     double q = a.q[atom];
-    int slot = a.sorted ? s : a.slot_of[atom];
+    // cell-sorted slot, or the atom itself when neither map is given
+    int slot = a.sorted ? s : (a.slot_of ? a.slot_of[atom] : atom);
     fixed_add3(a.facc + 3 * (size_t)slot, (double)fx * a.hxr * q, (double)fy * a.hyr * q,
                (double)fz * a.hzr * q, a.scale, a.status);
 }
@@ -536,8 +537,9 @@ __global__ void k_pme_correction(CorrArgs a)
         acc[1] -= qq * e;
         double f = (qq * (a.two_alpha_pi * exp(-a.alpha2 * r2) - e) * rr * rr);
         double fx = rx * f, fy = ry * f, fz = rz * f;
-        fixed_add3(a.facc + 3 * (size_t)a.slot_of[pr.x], -fx, -fy, -fz, a.scale, a.status);
-        fixed_add3(a.facc + 3 * (size_t)a.slot_of[pr.y], fx, fy, fz, a.scale, a.status);
+        const int si = a.slot_of ? a.slot_of[pr.x] : pr.x, sj = a.slot_of ? a.slot_of[pr.y] : pr.y;
+        fixed_add3(a.facc + 3 * (size_t)si, -fx, -fy, -fz, a.scale, a.status);
+        fixed_add3(a.facc + 3 * (size_t)sj, fx, fy, fz, a.scale, a.status);
         if (a.virial) {
             double xy = fx * ry, xz = fx * rz, yz = fy * rz;
             acc[2] += fx * rx; acc[3] += xy; acc[4] += xz;
@@ -575,6 +577,8 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
             double f = fp[c];
             if (a.f32p) f += (double)(long long)a.f32p[3 * (size_t)s + c] * (1.0 / kScaleMixed);
             if (a.f40) f += (double)(long long)a.f40[3 * (size_t)s + c] * (1.0 / kScaleFp64);
+            if (a.a32) f += (double)(long long)a.a32[3 * (size_t)i + c] * (1.0 / kScaleMixed);
+            if (a.a40) f += (double)(long long)a.a40[3 * (size_t)i + c] * (1.0 / kScaleFp64);
             a.fout[3 * (size_t)i + c] += f;
         }
         if (a.pair_virial) {

@@ -94,6 +94,9 @@ struct pmgpu_system {
     unsigned long long* d_facc32 = nullptr;   // mixed (2^32): 3N pair forces + 3N other (d_facc32p)
     unsigned long long* d_facc32p = nullptr;
     unsigned long long* d_facc40 = nullptr;   // FP64 (2^40)
+    // PME forces in atom order (PME needs no binning, so it runs beside it):
+    // 3N mixed (2^32) then 3N FP64 (2^40)
+    unsigned long long* d_faccA = nullptr;
     int* d_cell_lin = nullptr;
     int* d_cell3 = nullptr;
     int* d_counts = nullptr;
@@ -270,7 +273,7 @@ static void free_atom_buffers(pmgpu_system* s)
     dfree(s->d_slo); dfree(s->d_skey);
     dfree(s->d_xfull); dfree(s->d_xmod); dfree(s->d_xrow); dfree(s->d_xent);
     dfree(s->d_epairs); dfree(s->d_ecls);
-    dfree(s->d_pos); dfree(s->d_fout); dfree(s->d_facc32); dfree(s->d_facc40);
+    dfree(s->d_pos); dfree(s->d_fout); dfree(s->d_facc32); dfree(s->d_facc40); dfree(s->d_faccA);
     s->d_facc32p = nullptr;   // second half of d_facc32
     dfree(s->d_cell_lin); dfree(s->d_cell3); dfree(s->d_tmp); dfree(s->d_sorted); dfree(s->d_slot);
     dfree(s->d_spos); dfree(s->d_smeta); dfree(s->d_spos64);
@@ -459,6 +462,7 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     // per-evaluation atom buffers
     CK(dalloc(&sys->d_pos, 3 * (size_t)n), "alloc"); CK(dalloc(&sys->d_fout, 3 * (size_t)n), "alloc");
     CK(dalloc(&sys->d_facc32, 6 * (size_t)n), "alloc"); CK(dalloc(&sys->d_facc40, 3 * (size_t)n), "alloc");
+    CK(dalloc(&sys->d_faccA, 6 * (size_t)n), "alloc");
     sys->d_facc32p = sys->d_facc32 + 3 * (size_t)n;
     CK(dalloc(&sys->d_cell_lin, n), "alloc"); CK(dalloc(&sys->d_cell3, 3 * (size_t)n), "alloc");
     CK(dalloc(&sys->d_tmp, n), "alloc"); CK(dalloc(&sys->d_sorted, n), "alloc"); CK(dalloc(&sys->d_slot, n), "alloc");
@@ -1084,54 +1088,23 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
     if (use32) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
-    r = bin(sys, d_pos);
-    if (r) return r;
-    prof_end(sys, mbin);
-    int used = 0;
-    int lists = 0;
-    int pair_virial = 0;
-    // PME beside the cutoff forces on the side stream (not while profiling,
-    // which times every phase on its own)
     bool any_cut = false, any_pme = false;
     for (int k = 0; k < nf; ++k) (forces[k]->kind == 0 ? any_cut : any_pme) = true;
-    const bool fork = any_cut && any_pme && !sys->profiling;
-    cudaStream_t ps = fork ? sys->side : s;
-    if (fork) {
-        CK(cudaEventRecord(sys->ev_fork, s), "fork");
-        CK(cudaStreamWaitEvent(sys->side, sys->ev_fork, 0), "fork");
-    }
-    for (int k = 0; k < nf; ++k) {
-        pmgpu_force* f = forces[k];
-        bool fp64 = f->precision == PMGPU_PRECISION_FP64;
-        unsigned long long* facc = fp64 ? sys->d_facc40 : sys->d_facc32p;
-        double scale = fp64 ? kScaleFp64 : kScaleMixed;
-        if (f->kind == 0) {
-            if (!fp64 && !f->wrap && virial) pair_virial = 1;
-            PairArgs a;
-            fill_pair_args(sys, f, d_pos, a);
-            a.virial = virial;
-            a.erec = sys->d_erec + used;
-            if (!fp64) {
-                // list count and need, chunk count and need, work counter
-                if (lists++ > 0) CK(cudaMemsetAsync(sys->d_plist_count, 0, 5 * sizeof(int), s), "memset");
-                int ml = prof_begin(sys, kPhaseList);
-                int e = launch_cluster_list(a, s, &sys->launches);
-                if (e) return cuda_fail(sys, (cudaError_t)e, "cluster-pair list");
-                prof_end(sys, ml);
-            }
-            int m = prof_begin(sys, kPhasePair);
-            a.reserve = fork ? 1 : 0;
-            int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
-                         : launch_pair_mixed(a, f->combo, s, &sys->launches);
-            if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
-            prof_end(sys, m);
-            used += pair_records(sys, f);
-        } else {
+    if (any_pme) CK(cudaMemsetAsync(sys->d_faccA, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
+    int used = 0;
+    // PME: reads only positions and charges and accumulates in atom order
+    auto enqueue_pme = [&](cudaStream_t ps) -> int {
+        for (int k = 0; k < nf; ++k) {
+            pmgpu_force* f = forces[k];
+            if (f->kind != 1) continue;
+            const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+            unsigned long long* facc = fp64 ? sys->d_faccA + n3 : sys->d_faccA;
+            const double scale = fp64 ? kScaleFp64 : kScaleMixed;
             const pmgpu_pme_params& p = f->pp;
             if (p.correction) {
                 CorrArgs c;
                 c.n_excl = sys->e; c.pairs = sys->d_epairs; c.cls = sys->d_ecls; c.pos = d_pos; c.q = sys->d_q;
-                c.slot_of = sys->d_slot; c.pbc = sys->pbc; c.alpha = f->alpha; c.alpha2 = f->alpha * f->alpha;
+                c.slot_of = nullptr; c.pbc = sys->pbc; c.alpha = f->alpha; c.alpha2 = f->alpha * f->alpha;
                 c.two_alpha_pi = 2.0 * f->alpha / std::sqrt(kPi); c.csf = sys->csf;
                 c.facc = facc; c.scale = scale; c.erec = sys->d_erec + used; c.erec_stride = sys->erec_cap;
                 c.status = sys->d_status;
@@ -1148,7 +1121,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
             if (p.reciprocal) {
                 PmeArgs a;
                 memset(&a, 0, sizeof(a));
-                a.n = sys->n; a.pos = d_pos; a.q = sys->d_q; a.sorted = sys->d_sorted; a.slot_of = sys->d_slot;
+                a.n = sys->n; a.pos = d_pos; a.q = sys->d_q; a.sorted = nullptr; a.slot_of = nullptr;
                 a.kx = p.grid[0]; a.ky = p.grid[1]; a.kz = p.grid[2]; a.kzh = f->kzh; a.order = p.order;
                 double LX = sys->box[0], LY = sys->box[4], LZ = sys->box[8];
                 a.hxr = p.grid[0] / LX; a.hyr = p.grid[1] / LY; a.hzr = p.grid[2] / LZ;
@@ -1176,18 +1149,68 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 }
             }
         }
+        return PMGPU_OK;
+    };
+    // with cutoff forces too, PME runs on the side stream from the start,
+    // beside binning, the list and the pair kernels, and is joined before
+    // finalize (not while profiling, which times every phase alone)
+    const bool fork = any_cut && any_pme && !sys->profiling;
+    if (fork) {
+        CK(cudaEventRecord(sys->ev_fork, s), "fork");
+        CK(cudaStreamWaitEvent(sys->side, sys->ev_fork, 0), "fork");
+        r = enqueue_pme(sys->side);
+        if (r) return r;
+        CK(cudaEventRecord(sys->ev_join, sys->side), "join");
+    }
+    r = bin(sys, d_pos);
+    if (r) return r;
+    prof_end(sys, mbin);
+    int lists = 0;
+    int pair_virial = 0;
+    for (int k = 0; k < nf; ++k) {
+        pmgpu_force* f = forces[k];
+        if (f->kind != 0) continue;
+        const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+        if (!fp64 && !f->wrap && virial) pair_virial = 1;
+        PairArgs a;
+        fill_pair_args(sys, f, d_pos, a);
+        a.virial = virial;
+        a.erec = sys->d_erec + used;
+        if (!fp64) {
+            // list count and need, chunk count and need, work counter
+            if (lists++ > 0) CK(cudaMemsetAsync(sys->d_plist_count, 0, 5 * sizeof(int), s), "memset");
+            int ml = prof_begin(sys, kPhaseList);
+            int e = launch_cluster_list(a, s, &sys->launches);
+            if (e) return cuda_fail(sys, (cudaError_t)e, "cluster-pair list");
+            prof_end(sys, ml);
+        }
+        int m = prof_begin(sys, kPhasePair);
+        a.reserve = 0;
+        int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
+                     : launch_pair_mixed(a, f->combo, s, &sys->launches);
+        if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
+        prof_end(sys, m);
+        used += pair_records(sys, f);
     }
     if (fork) {
-        CK(cudaEventRecord(sys->ev_join, sys->side), "join");
         CK(cudaStreamWaitEvent(s, sys->ev_join, 0), "join");
+    } else if (any_pme) {
+        r = enqueue_pme(s);
+        if (r) return r;
     }
     int mfin = prof_begin(sys, kPhaseFinalize);
     if (use32 || use40) {
         FinArgs fa;
+        memset(&fa, 0, sizeof(fa));
         fa.n = sys->n;
         fa.f32 = use32 ? sys->d_facc32 : nullptr;
         fa.f32p = use32 ? sys->d_facc32p : nullptr;
         fa.f40 = use40 ? sys->d_facc40 : nullptr;
+        for (int k = 0; k < nf; ++k)
+            if (forces[k]->kind == 1) {
+                if (forces[k]->precision == PMGPU_PRECISION_FP64) fa.a40 = sys->d_faccA + n3;
+                else fa.a32 = sys->d_faccA;
+            }
         fa.sorted = sys->d_sorted; fa.spos = sys->d_spos; fa.slo = sys->d_slo;
         fa.pair_virial = pair_virial;
         fa.fout = d_fout;
