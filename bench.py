@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=20)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extra", action="store_true",
+                   help="skip the batched (96 boxes) and 1,000,000-atom measurements")
     return p.parse_args()
 
 
@@ -291,6 +293,11 @@ def main():
                     "frac": b / (phases[k] * 1e-3) / 1e9 / hbm, "bytes": b, "launch_ms": phases[k]}
                 for k, b in pme_bytes.items() if phases.get(k)}
 
+    extra = {}
+    if not args.no_extra:
+        extra["batched"] = measure_batched(local, rank, world, pg, torch, flush, max(20, min(args.steps // 10, 200)))
+        if rank == 0:
+            extra["scale_1m"] = measure_1m(local, torch, 10)
     if rank == 0:
         value = world * 1000.0 / t_local
         line = {
@@ -305,6 +312,7 @@ def main():
             "e2e": {"value": world * 1000.0 / t_e2e, "unit": UNIT, "ms_per_step": t_e2e,
                     "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 88},
             "gpu_launches": int(launches),
+            "pair_interactions_per_s": n_pairs * world * 1000.0 / t_local,
             "roofline": roofline,
             "phases_ms": phases,
             "pme_roofline_hbm": pme_roof,
@@ -312,10 +320,156 @@ def main():
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(s, w.forces, 12)
+        if extra:
+            line.update(extra)
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def measure_batched(local, rank, world, pg, torch, flush, steps):
+    """The 96 uneven water boxes (300-9,000 atoms, cutoff 9, PME ~1 A grid),
+    sharded over the ranks by atom count; each rank evaluates its shard with
+    one graph launch per step.  Compared with the same boxes evaluated one at
+    a time (each box's own graph launch, waited for before the next)."""
+    from protomol_b200 import forces as F
+    from protomol_b200 import workloads
+    from protomol_b200.batch import Batch, shard_by_atoms
+    ws = workloads.batched96()
+    mine = shard_by_atoms([w.system.n_atoms for w in ws], world)[rank]
+    batch = Batch(local)
+    keep = []
+    for k in mine:
+        w = ws[k]
+        topo = F.Topology(w.system, device=local)
+        fs = [F.ForceFactory.make(topo, d, "mixed") for d in w.forces]
+        batch.add(topo, fs, w.system.positions)
+        keep.append((topo, fs))
+    atoms = sum(ws[k].system.n_atoms for k in mine)
+    bstream = torch.cuda.ExternalStream(batch.stream)
+    for _ in range(3):
+        batch.evaluate()
+    batch.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(bstream):
+        for a, b in evs:
+            flush.zero_()
+            a.record(bstream)
+            batch.evaluate()
+            b.record(bstream)
+    torch.cuda.synchronize()
+    batch.synchronize()
+    t_batch = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    # one system at a time through the single-system device API
+    lib = _lib_load()
+    VP = C.c_void_p
+    seq = []
+    for (topo, fs), (_, _, pos, fout, energy, _) in zip(keep, batch.members):
+        arr = (VP * len(fs))(*[f.handle for f in fs])
+        seq.append((topo, arr, len(fs), pos, fout, energy))
+
+    def one_by_one():
+        for topo, arr, nfs, pos, fout, energy in seq:
+            lib.pmgpu_evaluate_device(topo.handle, nfs, arr, VP(pos.data_ptr()), VP(fout.data_ptr()),
+                                      VP(energy.data_ptr()), 1)
+            lib.pmgpu_synchronize(topo.handle)
+    one_by_one()
+    reps = max(3, steps // 4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        one_by_one()
+    t_seq = (time.perf_counter() - t0) * 1000.0 / reps
+    if pg:
+        t = torch.tensor([t_batch, t_seq], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_batch, t_seq = float(t[0]), float(t[1])
+    total_atoms = sum(w.system.n_atoms for w in ws)
+    batch.close()
+    return {"workload": "96 water boxes of 100-3,000 waters, cutoff 9 (C2 8->9), PME ~1 A grid, mixed",
+            "systems": len(ws), "atoms": total_atoms, "sharding": f"{world} rank(s), greedy by atom count",
+            "ms_per_step": t_batch, "batch_evals_per_s": 1000.0 / t_batch,
+            "atom_evals_per_s": total_atoms * 1000.0 / t_batch,
+            "one_at_a_time_ms": t_seq, "one_at_a_time_atom_evals_per_s": total_atoms * 1000.0 / t_seq,
+            "speedup_vs_one_at_a_time": t_seq / t_batch,
+            "timing": "CUDA events on the batch stream (batched, L2 flushed between steps); "
+                      "wall clock for one at a time (each box synchronized)"}
+
+
+def measure_1m(local, torch, steps):
+    """The 1,000,000-atom box (cutoff 12, PME 216^3): mixed and FP64
+    evaluations/s, pair interactions/s and the PME kernels' HBM rates."""
+    from protomol_b200 import forces as F
+    from protomol_b200 import workloads
+    lib = _lib_load()
+    w = workloads.water1m()
+    s = w.system
+    n = s.n_atoms
+    topo = F.Topology(s, device=local)
+    stream = torch.cuda.ExternalStream(topo.stream)
+    dpos = torch.tensor(s.positions, dtype=torch.float64, device=f"cuda:{local}")
+    dfor = torch.zeros((n, 3), dtype=torch.float64, device=f"cuda:{local}")
+    den = torch.zeros(11, dtype=torch.float64, device=f"cuda:{local}")
+    VP = C.c_void_p
+    out = {"workload": "333,333 TIP3P waters + Na+, 215.4 A, LJ C2 10->12 + Ewald real 12 + PME 216^3", "atoms": n}
+    for prec in ("mixed", "fp64"):
+        fs = [F.ForceFactory.make(topo, d, prec) for d in w.forces]
+        arr = (VP * len(fs))(*[f.handle for f in fs])
+
+        def step():
+            lib.pmgpu_evaluate_device(topo.handle, len(fs), arr, VP(dpos.data_ptr()), VP(dfor.data_ptr()),
+                                      VP(den.data_ptr()), 1)
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        with torch.cuda.stream(stream):
+            for a, b in evs:
+                a.record(stream)
+                step()
+                b.record(stream)
+        torch.cuda.synchronize()
+        ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+        out[prec] = {"ms_per_step": ms, "evals_per_s": 1000.0 / ms}
+        if prec == "mixed":
+            lib.pmgpu_set_profiling(topo.handle, 1)
+            with torch.cuda.stream(stream):
+                for _ in range(3):
+                    step()
+            msp = (C.c_double * 8)()
+            cnt = C.c_longlong(0)
+            lib.pmgpu_phase_times(topo.handle, msp, 8, C.byref(cnt))
+            lib.pmgpu_set_profiling(topo.handle, 0)
+            from protomol_b200 import _lib
+            ph = {k: msp[i] / max(1, cnt.value) for i, k in enumerate(_lib.PHASES)}
+            # count only (capacity 0: the call reports the count it would need)
+            cnt = C.c_longlong(0)
+            pos = np.ascontiguousarray(s.positions, np.float64)
+            lib.pmgpu_get_pairs(topo.handle, fs[0].handle, pos.ctypes.data_as(VP), C.byref(cnt), None, 0)
+            npairs = int(cnt.value)
+            out["pairs_within_cutoff"] = npairs
+            out["pair_interactions_per_s"] = npairs * 1000.0 / ms
+            out["pair_kernel_ms"] = ph["pair"]
+            kx = 216
+            kzh = kx // 2 + 1
+            b = {"pme_spread": 16 * n + 4 * kx ** 3, "pme_fft": 2 * 2 * 8 * kx * kx * kzh,
+                 "pme_gather": 4 * kx ** 3 + 16 * n + 12 * n}
+            out["pme_hbm_gbs"] = {k: v / (ph[k] * 1e-3) / 1e9 for k, v in b.items() if ph.get(k)}
+            out["phases_ms"] = ph
+        for f in fs:
+            f.close()
+    out["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    topo.close()
+    return out
+
+
+def _lib_load():
+    from protomol_b200 import _lib
+    return _lib.load()
 
 
 def profile_phases(lib, topo, forces, step, flush, stream, torch, steps):

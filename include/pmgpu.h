@@ -203,6 +203,32 @@ int pmgpu_phase_times(pmgpu_system* sys, double* ms, int n, long long* evals);
 /* Copies the last error message (NUL-terminated) into buf. */
 int pmgpu_last_error(pmgpu_system* sys, char* buf, int len);
 
+/* ---- batches of independent systems ---------------------------------------
+ * The reference evaluates one system per process (ForceGroup::
+ * evaluateSystemForces, forces/ForceGroup.cpp:70-82, once per replica or
+ * per MPI rank).  A batch evaluates many independent systems of uneven size
+ * with ONE CUDA graph launch: every member's forces run on that member's own
+ * streams, all branching from the batch's stream, so small systems fill the
+ * GPU together.  Members are (system, forces, device buffers) triples; the
+ * results are those of pmgpu_evaluate_device on each member (accumulated,
+ * +=).  The graph is captured on the first pmgpu_batch_evaluate and again
+ * whenever a member's buffers, box, topology or forces change. */
+typedef struct pmgpu_batch pmgpu_batch;
+int pmgpu_batch_create(int device, pmgpu_batch** out);
+int pmgpu_batch_destroy(pmgpu_batch* batch);
+/* Adds a member: n_forces forces of sys evaluated on the device buffers
+ * d_positions (N x 3), d_forces_accum (N x 3, +=), d_energies (11, +=). */
+int pmgpu_batch_add(pmgpu_batch* batch, pmgpu_system* sys, int n_forces, pmgpu_force* const* forces,
+                    const double* d_positions, double* d_forces_accum, double* d_energies, unsigned flags);
+/* One graph launch of every member's evaluation, asynchronous on the batch's
+ * stream (pmgpu_batch_stream). */
+int pmgpu_batch_evaluate(pmgpu_batch* batch);
+/* Waits for the batch and reports the first member failure (for
+ * PMGPU_ERR_CAPACITY, the member's list has been grown: evaluate again). */
+int pmgpu_batch_synchronize(pmgpu_batch* batch);
+int pmgpu_batch_last_error(pmgpu_batch* batch, char* buf, int len);
+void* pmgpu_batch_stream(pmgpu_batch* batch);
+
 /* ---- diagnostics (parity tests) ----------------------------------------- */
 
 /* Cell of every atom from the GPU binning of the last evaluation, as

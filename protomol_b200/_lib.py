@@ -26,6 +26,8 @@ EXPORTS = [
     "pmgpu_evaluate", "pmgpu_evaluate_device", "pmgpu_synchronize", "pmgpu_stream",
     "pmgpu_launch_count", "pmgpu_last_error", "pmgpu_get_cells", "pmgpu_get_pairs",
     "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
+    "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
+    "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream",
 ]
 PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
 
@@ -91,6 +93,14 @@ def load():
     lib.pmgpu_phase_times.argtypes = [vp, vp, C.c_int, C.POINTER(C.c_longlong)]
     lib.pmgpu_pme_reciprocal_static.argtypes = [C.c_int, C.c_int, vp, vp, dp, ip, C.c_int, C.c_double,
                                                 vp, vp, C.c_uint, vp]
+    lib.pmgpu_batch_create.argtypes = [C.c_int, C.POINTER(vp)]
+    lib.pmgpu_batch_destroy.argtypes = [vp]
+    lib.pmgpu_batch_add.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp, C.c_uint]
+    lib.pmgpu_batch_evaluate.argtypes = [vp]
+    lib.pmgpu_batch_synchronize.argtypes = [vp]
+    lib.pmgpu_batch_last_error.argtypes = [vp, C.c_char_p, C.c_int]
+    lib.pmgpu_batch_stream.argtypes = [vp]
+    lib.pmgpu_batch_stream.restype = vp
     _lib = lib
     return lib
 

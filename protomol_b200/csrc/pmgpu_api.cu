@@ -1532,3 +1532,167 @@ extern "C" int pmgpu_pme_reciprocal_static(int device, int n_atoms, const double
     if (e != cudaSuccess) return PMGPU_ERR_CUDA;
     return (st & kStatusOverflow) ? PMGPU_ERR_OVERFLOW : PMGPU_OK;
 }
+
+// ------------------------------------------------------------------ batches
+// Many independent systems evaluated by one CUDA graph launch: each member's
+// evaluation (its forces on its device buffers) is captured on the member's
+// own streams, all branching from and joining back into the batch's stream,
+// so the small systems of a batch run concurrently and fill the GPU.
+struct pmgpu_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr;
+    struct Member {
+        pmgpu_system* sys;
+        std::vector<pmgpu_force*> forces;    // -real expanded
+        const double* pos;
+        double* fout;
+        double* energy;
+        unsigned flags;
+        cudaEvent_t done;
+    };
+    std::vector<Member> members;
+    std::vector<GraphKey> keys;               // of the captured graph
+    cudaGraphExec_t exec = nullptr;
+    std::vector<long long> member_launches;   // kernels per member in the graph
+    std::string err;
+};
+
+static int batch_fail(pmgpu_batch* b, int code, const std::string& msg)
+{
+    b->err = msg;
+    return code;
+}
+
+extern "C" int pmgpu_batch_create(int device, pmgpu_batch** out)
+{
+    if (!out) return PMGPU_ERR_ARG;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return PMGPU_ERR_CUDA;
+    pmgpu_batch* b = new pmgpu_batch();
+    b->device = device;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming) != cudaSuccess) {
+        delete b;
+        return PMGPU_ERR_CUDA;
+    }
+    *out = b;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_batch_destroy(pmgpu_batch* b)
+{
+    if (!b) return PMGPU_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    for (auto& m : b->members) cudaEventDestroy(m.done);
+    cudaEventDestroy(b->ev_start);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_batch_add(pmgpu_batch* b, pmgpu_system* sys, int n_forces, pmgpu_force* const* forces,
+                               const double* d_positions, double* d_forces_accum, double* d_energies,
+                               unsigned flags)
+{
+    if (!b || !sys || n_forces < 1 || !forces || !d_positions || !d_forces_accum || !d_energies)
+        return PMGPU_ERR_ARG;
+    if (sys->device != b->device) return batch_fail(b, PMGPU_ERR_ARG, "system on another device");
+    pmgpu_batch::Member m;
+    m.sys = sys; m.pos = d_positions; m.fout = d_forces_accum; m.energy = d_energies; m.flags = flags;
+    for (int k = 0; k < n_forces; ++k) {
+        if (!forces[k] || forces[k]->sys != sys) return batch_fail(b, PMGPU_ERR_ARG, "force of another system");
+        if (forces[k]->real_sub) m.forces.push_back(forces[k]->real_sub);
+        m.forces.push_back(forces[k]);
+    }
+    cudaSetDevice(b->device);
+    if (cudaEventCreateWithFlags(&m.done, cudaEventDisableTiming) != cudaSuccess) return PMGPU_ERR_CUDA;
+    b->members.push_back(m);
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_batch_evaluate(pmgpu_batch* b)
+{
+    if (!b) return PMGPU_ERR_ARG;
+    if (b->members.empty()) return PMGPU_OK;
+    cudaSetDevice(b->device);
+    std::vector<GraphKey> keys;
+    for (auto& m : b->members) {
+        if (m.sys->profiling) return batch_fail(b, PMGPU_ERR_STATE, "a member system is in profiling mode");
+        int r = eval_prepare(m.sys, (int)m.forces.size(), m.forces.data());
+        if (r) return batch_fail(b, r, m.sys->err);
+        GraphKey k;
+        for (pmgpu_force* f : m.forces) k.ids.push_back(f->id);
+        k.pos = m.pos; k.fout = m.fout; k.energy = m.energy; k.flags = m.flags;
+        k.box_version = m.sys->box_version; k.topo_version = m.sys->topo_version;
+        k.buf_version = m.sys->buf_version;
+        keys.push_back(k);
+    }
+    if (!(b->exec && keys == b->keys)) {
+        if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+        std::vector<long long> l0;
+        for (auto& m : b->members) l0.push_back(m.sys->launches);
+        if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return batch_fail(b, PMGPU_ERR_CUDA, "batch graph capture");
+        int r = PMGPU_OK;
+        cudaError_t e = cudaEventRecord(b->ev_start, b->stream);
+        for (size_t k = 0; k < b->members.size() && r == PMGPU_OK && e == cudaSuccess; ++k) {
+            auto& m = b->members[k];
+            e = cudaStreamWaitEvent(m.sys->stream, b->ev_start, 0);
+            if (e != cudaSuccess) break;
+            r = eval_enqueue(m.sys, (int)m.forces.size(), m.forces.data(), m.pos, m.fout, m.energy, m.flags);
+            if (r) { b->err = m.sys->err; break; }
+            e = cudaEventRecord(m.done, m.sys->stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, m.done, 0);
+        }
+        cudaGraph_t graph = nullptr;
+        cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
+        if (r || e != cudaSuccess || ec != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            for (size_t k = 0; k < b->members.size(); ++k) b->members[k].sys->launches = l0[k];
+            return r ? r : batch_fail(b, PMGPU_ERR_CUDA, std::string("batch graph capture: ") +
+                                          cudaGetErrorString(e != cudaSuccess ? e : ec));
+        }
+        e = cudaGraphInstantiate(&b->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            b->exec = nullptr;
+            return batch_fail(b, PMGPU_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(e));
+        }
+        b->member_launches.clear();
+        for (size_t k = 0; k < b->members.size(); ++k) {
+            b->member_launches.push_back(b->members[k].sys->launches - l0[k]);
+            b->members[k].sys->launches = l0[k];
+        }
+        b->keys = keys;
+    }
+    cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
+    if (e != cudaSuccess) return batch_fail(b, PMGPU_ERR_CUDA, std::string("batch graph launch: ") + cudaGetErrorString(e));
+    for (size_t k = 0; k < b->members.size(); ++k) b->members[k].sys->launches += b->member_launches[k];
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_batch_synchronize(pmgpu_batch* b)
+{
+    if (!b) return PMGPU_ERR_ARG;
+    cudaSetDevice(b->device);
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, PMGPU_ERR_CUDA, cudaGetErrorString(e));
+    // the members' status words: the first failure is reported
+    for (size_t k = 0; k < b->members.size(); ++k) {
+        int r = pmgpu_synchronize(b->members[k].sys);
+        if (r) return batch_fail(b, r, "member " + std::to_string(k) + ": " + b->members[k].sys->err);
+    }
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_batch_last_error(pmgpu_batch* b, char* buf, int len)
+{
+    if (!b || !buf || len <= 0) return PMGPU_ERR_ARG;
+    snprintf(buf, (size_t)len, "%s", b->err.c_str());
+    return PMGPU_OK;
+}
+
+extern "C" void* pmgpu_batch_stream(pmgpu_batch* b) { return b ? (void*)b->stream : nullptr; }
