@@ -203,6 +203,30 @@ int pmgpu_phase_times(pmgpu_system* sys, double* ms, int n, long long* evals);
 /* Copies the last error message (NUL-terminated) into buf. */
 int pmgpu_last_error(pmgpu_system* sys, char* buf, int len);
 
+/* ---- differentiation (backward of pmgpu_evaluate) --------------------------
+ * The reference has no adjoint; its analytic Hessian (integrators/
+ * Hessian.cpp:456-623 with ReducedHessLennardJones.cpp:7-51,
+ * ReducedHessCoulomb.cpp:8-43 and the switches' hessian(),
+ * C2SwitchingFunction.cpp:45-53) is what the Hessian-vector product below
+ * reproduces for the pair terms, for the NML integrators
+ * (integrators/NormModeInt.cpp:368-415).  pmgpu_evaluate is the forward pass;
+ * this backward pass recomputes the pair terms (nothing is stored) in the
+ * forces' precision (FP64 or mixed) and ACCUMULATES (+=), host arrays:
+ *   dE_dq   N:  dE/d(scaled charge) of all the forces (pair terms, PME
+ *               reciprocal via the convolved potential, correction, self and
+ *               charged-system terms);
+ *   dE_dlj  T*T*4: dE/d(LJ table entry) in pmgpu_set_topology's layout
+ *               {A, B, A14, B14}; each pair's derivative is split evenly
+ *               between (t_i, t_j) and (t_j, t_i), so the gradient w.r.t. a
+ *               symmetric entry t != t' is G[t][t'] + G[t'][t];
+ *   hv      N*3: (H v), the Hessian of the pair energy applied to v (the
+ *               negative force Jacobian-vector product); PMGPU_ERR_UNSUPPORTED
+ *               when a PME reciprocal or correction term is in the list;
+ *   energies 2: the pair terms' LJ and Coulomb energies (a check).
+ * Any output may be NULL. */
+int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,
+                  const double* v, double* dE_dq, double* dE_dlj, double* hv, double* energies);
+
 /* ---- batches of independent systems ---------------------------------------
  * The reference evaluates one system per process (ForceGroup::
  * evaluateSystemForces, forces/ForceGroup.cpp:70-82, once per replica or

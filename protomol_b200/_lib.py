@@ -27,7 +27,7 @@ EXPORTS = [
     "pmgpu_launch_count", "pmgpu_last_error", "pmgpu_get_cells", "pmgpu_get_pairs",
     "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
-    "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream",
+    "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
 ]
 PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
 
@@ -101,6 +101,7 @@ def load():
     lib.pmgpu_batch_last_error.argtypes = [vp, C.c_char_p, C.c_int]
     lib.pmgpu_batch_stream.argtypes = [vp]
     lib.pmgpu_batch_stream.restype = vp
+    lib.pmgpu_adjoint.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]
     _lib = lib
     return lib
 

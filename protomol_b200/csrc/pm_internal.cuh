@@ -100,6 +100,32 @@ __device__ __forceinline__ void pbc_min_pos(const Pbc& b, double x, double y, do
     rx = dx; ry = dy; rz = dz;
 }
 
+// ---- exclusions --------------------------------------------------------------
+// ExclusionTable::check (topology/ExclusionTable.h:130-146) for a pair of the
+// same molecule: bit masks of the index deltas 1..kExclWindow per atom, then
+// a CSR of (partner, class) sorted by partner; returns the class.
+__device__ __forceinline__ int excl_lookup(const uint32_t* xfull, const uint32_t* xmod, const int* xrow,
+                                           const int2* xent, int oi, int oj)
+{
+    int lo = min(oi, oj), hi = max(oi, oj);
+    int dl = hi - lo;
+    if (dl <= 0) return 0;                       // PMGPU_EXCL_NONE
+    if (dl <= kExclWindow) {
+        uint32_t bit = 1u << (dl - 1);
+        if (__ldg(xfull + lo) & bit) return 2;    // PMGPU_EXCL_FULL
+        if (__ldg(xmod + lo) & bit) return 1;     // PMGPU_EXCL_MODIFIED
+        return 0;
+    }
+    int b = __ldg(xrow + lo), e = __ldg(xrow + lo + 1);
+    while (b < e) {   // binary search on partner index
+        int m = (b + e) >> 1;
+        int2 v = xent[m];
+        if (v.x == hi) return v.y;
+        if (v.x < hi) b = m + 1; else e = m;
+    }
+    return 0;
+}
+
 // ---- fixed-point force accumulation ---------------------------------------
 // Each contribution is rounded to an int64 multiple of 1/scale and added with
 // an integer atomic, so the total is independent of summation order.

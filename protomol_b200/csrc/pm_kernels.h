@@ -151,6 +151,38 @@ int pair_blocks(const CellGrid& g, int nd);
 long long plist_estimate(int n_atoms, const CellGrid& g, int nh);
 long long chunk_estimate(int n_atoms, const CellGrid& g, int nh);
 
+// ---------------------------------------------------------------- adjoint
+// K10: gradients of the pair energy w.r.t. charges and the LJ table, and the
+// Hessian-vector product, recomputed pair by pair (all ordered pairs, exact
+// FP64 minimal image and cutoff decision; math in FP64 or FP32)
+struct AdjArgs {
+    int n;
+    const double* pos;           // 3N, original order
+    const double* q;             // N scaled charges
+    const int* type;
+    const int* mol;
+    Pbc pbc;
+    int periodic;                // 0: vacuum (plain differences)
+    const uint32_t* xfull;
+    const uint32_t* xmod;
+    const int* xrow;
+    const int2* xent;
+    const double4* ljd;          // T x T of {A, B, A14, B14}
+    int n_types;
+    int n_terms;
+    TermD td[2];
+    int modify;                  // the switches are applied (one of them modifies)
+    int use_cut;                 // pair test r^2 <= cut2d (0: all pairs)
+    double cut2d;
+    double csf;
+    const double* v;             // 3N displacement for H v, or null
+    double* dq;                  // N (+=) or null
+    double* dlj;                 // T x T x 4 (+=) or null
+    double* hv;                  // 3N (+=) or null
+    double* energy;              // 2 (+=): LJ, Coulomb, or null
+};
+int launch_pair_adjoint(const AdjArgs& a, int fp64, cudaStream_t s, long long* launches);
+
 // ---------------------------------------------------------------- PME
 struct PmeArgs {
     int n;
@@ -180,6 +212,7 @@ struct PmeArgs {
     int virial;
 };
 constexpr int kStageSpread = 0, kStageFft = 1, kStageGather = 2;
+constexpr int kStagePotential = 3;   // dE/dq~ = phi at the atoms, into (double*)facc
 // One stage of the reciprocal term: K3 spread, the five FFT passes with the
 // fused convolution (K4/K5, writes energy records), or K6 gather.
 int launch_pme_reciprocal(const PmeArgs& a, int fp64, cudaStream_t s, long long* launches,
@@ -205,6 +238,7 @@ struct CorrArgs {
     double const_virial;         // charged-system term on the virial diagonal
 };
 int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches, int* blocks_used);
+int launch_pme_correction_adjoint(const CorrArgs& a, double* dq, cudaStream_t s, long long* launches);
 
 // ---------------------------------------------------------------- finalize
 // forces of the three fixed-point accumulators (any may be null) added into

@@ -112,27 +112,10 @@ __device__ __forceinline__ ItemGeom decode_item(const PairArgs& p, int item)
     return g;
 }
 
-// ExclusionTable::check (topology/ExclusionTable.h:130-146) for a pair of the
-// same molecule; returns the class.
+// ExclusionTable::check for a pair of the same molecule; returns the class
 __device__ __forceinline__ int excl_class(const PairArgs& p, int oi, int oj)
 {
-    int lo = min(oi, oj), hi = max(oi, oj);
-    int dl = hi - lo;
-    if (dl <= 0) return PMGPU_EXCL_NONE;
-    if (dl <= kExclWindow) {
-        uint32_t bit = 1u << (dl - 1);
-        if (__ldg(p.xfull + lo) & bit) return PMGPU_EXCL_FULL;
-        if (__ldg(p.xmod + lo) & bit) return PMGPU_EXCL_MODIFIED;
-        return PMGPU_EXCL_NONE;
-    }
-    int b = __ldg(p.xrow + lo), e = __ldg(p.xrow + lo + 1);
-    while (b < e) {   // binary search on partner index
-        int m = (b + e) >> 1;
-        int2 v = p.xent[m];
-        if (v.x == hi) return v.y;
-        if (v.x < hi) b = m + 1; else e = m;
-    }
-    return PMGPU_EXCL_NONE;
+    return excl_lookup(p.xfull, p.xmod, p.xrow, p.xent, oi, oj);
 }
 
 // ---------------------------------------------------------------- FP32 math

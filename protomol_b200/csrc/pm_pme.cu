@@ -381,6 +381,34 @@ __global__ void k_gather(PmeArgs a)
                (double)fz * a.hzr * q, a.scale, a.status);
 }
 
+// dE_recip/dq~_i: the convolved grid interpolated at the atom (the gather
+// above without the derivative), so that E_recip = 1/2 sum_i q~_i phi_i
+template <typename R>
+__global__ void k_gather_potential(PmeArgs a, double* phi)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.n) return;
+    int atom = a.sorted ? a.sorted[s] : s;
+    R tx[kMaxOrder], dtx[kMaxOrder], ty[kMaxOrder], dty[kMaxOrder], tz[kMaxOrder], dtz[kMaxOrder];
+    int i0, j0, k0;
+    grid_point<R>(a, atom, i0, j0, k0, tx, dtx, ty, dty, tz, dtz);
+    const R* g = (const R*)a.rgrid;
+    double acc = 0.0;
+    const int P = a.order;
+    for (int i = 0; i < P; i++) {
+        int i1 = (i + i0) % a.kx;
+        for (int j = 0; j < P; j++) {
+            int j1 = (j + j0) % a.ky;
+            R ab = tx[i] * ty[j];
+            size_t row = ((size_t)i1 * a.ky + j1) * a.kz;
+            R sum = 0;
+            for (int k = 0; k < P; k++) sum += g[row + (k + k0) % a.kz] * tz[k];
+            acc += (double)(ab * sum);
+        }
+    }
+    phi[atom] += acc;
+}
+
 static void make_plan(int n, FftPlan& p)
 {
     p.n = n;
@@ -409,6 +437,10 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     }
     if (stage == kStageGather) {
         if (a.n > 0) { k_gather<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+        return (int)cudaGetLastError();
+    }
+    if (stage == kStagePotential) {   // a.facc holds the double phi[N] output here
+        if (a.n > 0) { k_gather_potential<R><<<nb, 128, 0, s>>>(a, (double*)a.facc); *launches += 1; }
         return (int)cudaGetLastError();
     }
 
@@ -548,6 +580,34 @@ __global__ void k_pme_correction(CorrArgs a)
         }
     }
     block_reduce_store<8>(acc, a.erec, a.erec_stride, blockIdx.x);
+}
+
+// dE_correction/dq~: each exclusion pair's -kappa q~_i q~_j erf(alpha r)/r
+// (kappa = 1, or 1 - csf for MODIFIED) differentiated w.r.t. both charges
+__global__ void k_pme_correction_adjoint(CorrArgs a, double* dq)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.n_excl; k += gridDim.x * blockDim.x) {
+        int2 pr = a.pairs[k];
+        const double* p1 = a.pos + 3 * (size_t)pr.x;
+        const double* p2 = a.pos + 3 * (size_t)pr.y;
+        double rx, ry, rz;
+        double r2 = pbc_min_diff(a.pbc, p1[0], p1[1], p1[2], p2[0], p2[1], p2[2], rx, ry, rz);
+        double kappa = a.cls[k] == PMGPU_EXCL_MODIFIED ? 1 - a.csf : 1.0;
+        double r = sqrt(r2);
+        double e = kappa * erf(a.alpha * r) / r;
+        atomicAdd(dq + pr.x, -e * a.q[pr.y]);
+        atomicAdd(dq + pr.y, -e * a.q[pr.x]);
+    }
+}
+
+int launch_pme_correction_adjoint(const CorrArgs& a, double* dq, cudaStream_t s, long long* launches)
+{
+    if (a.n_excl <= 0) return 0;
+    int blocks = (a.n_excl + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_pme_correction_adjoint<<<blocks, 256, 0, s>>>(a, dq);
+    *launches += 1;
+    return (int)cudaGetLastError();
 }
 
 int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches, int* blocks_used)

@@ -1696,3 +1696,130 @@ extern "C" int pmgpu_batch_last_error(pmgpu_batch* b, char* buf, int len)
 }
 
 extern "C" void* pmgpu_batch_stream(pmgpu_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+// ------------------------------------------------------------------ adjoint
+static void adj_pme_args(pmgpu_system* sys, pmgpu_force* f, PmeArgs& a)
+{
+    const pmgpu_pme_params& p = f->pp;
+    memset(&a, 0, sizeof(a));
+    a.n = sys->n; a.pos = sys->d_pos; a.q = sys->d_q;
+    a.kx = p.grid[0]; a.ky = p.grid[1]; a.kz = p.grid[2]; a.kzh = f->kzh; a.order = p.order;
+    double LX = sys->box[0], LY = sys->box[4], LZ = sys->box[8];
+    a.hxr = p.grid[0] / LX; a.hyr = p.grid[1] / LY; a.hzr = p.grid[2] / LZ;
+    a.offx = -(p.order - 1) / 2 + p.grid[0];
+    a.offy = -(p.order - 1) / 2 + p.grid[1];
+    a.offz = -(p.order - 1) / 2 + p.grid[2];
+    a.qgrid = f->d_qgrid; a.cgrid = f->d_cgrid; a.rgrid = f->d_rgrid; a.tw = f->d_tw;
+    a.twx = f->twx; a.twy = f->twy; a.twz = f->twz;
+    a.bfac = f->d_bfac; a.efac = f->d_efac;
+    a.piVr = 1.0 / (kPi * (LX * LY * LZ));
+    a.fac = kPi * kPi / (f->alpha * f->alpha);
+    a.wr = 1.0 / LX; a.lr = 1.0 / LY; a.hr = 1.0 / LZ;
+    a.qscale = kScaleFp64; a.erec_stride = sys->erec_cap;
+    a.status = sys->d_status;
+}
+
+extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces_in, const double* positions,
+                             const double* v, double* dE_dq, double* dE_dlj, double* hv, double* energies)
+{
+    if (!sys || !positions || n_forces < 1 || !forces_in) return PMGPU_ERR_ARG;
+    cudaSetDevice(sys->device);
+    std::vector<pmgpu_force*> fl;
+    for (int k = 0; k < n_forces; ++k) {
+        if (!forces_in[k] || forces_in[k]->sys != sys) return fail(sys, PMGPU_ERR_ARG, "bad force list");
+        if (forces_in[k]->real_sub) fl.push_back(forces_in[k]->real_sub);
+        fl.push_back(forces_in[k]);
+    }
+    if (hv && !v) return fail(sys, PMGPU_ERR_ARG, "Hessian-vector product needs v");
+    for (pmgpu_force* f : fl)
+        if (hv && f->kind == 1 && (f->pp.reciprocal || f->pp.correction))
+            return fail(sys, PMGPU_ERR_UNSUPPORTED, "Hessian-vector product of the PME reciprocal / correction "
+                                                    "terms is not available (the real-space pairs are)");
+    int r = eval_prepare(sys, (int)fl.size(), fl.data());
+    if (r) return r;
+    const int n = sys->n, T = sys->t;
+    cudaStream_t s = sys->stream;
+    size_t n3 = 3 * (size_t)n;
+    double *d_v = nullptr, *d_dq = nullptr, *d_lj = nullptr, *d_hv = nullptr, *d_e = nullptr;
+    auto cleanup = [&]() { dfree(d_v); dfree(d_dq); dfree(d_lj); dfree(d_hv); dfree(d_e); };
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    ok(cudaMemcpyAsync(sys->d_pos, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+    ok(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s));
+    ok(dalloc(&d_dq, (size_t)n)); ok(dalloc(&d_lj, (size_t)T * T * 4)); ok(dalloc(&d_e, 2));
+    if (hv) { ok(dalloc(&d_v, n3)); ok(dalloc(&d_hv, n3)); }
+    if (e == cudaSuccess) {
+        ok(cudaMemsetAsync(d_dq, 0, sizeof(double) * n, s));
+        ok(cudaMemsetAsync(d_lj, 0, sizeof(double) * T * T * 4, s));
+        ok(cudaMemsetAsync(d_e, 0, sizeof(double) * 2, s));
+        if (hv) {
+            ok(cudaMemcpyAsync(d_v, v, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+            ok(cudaMemsetAsync(d_hv, 0, sizeof(double) * n3, s));
+        }
+    }
+    if (e != cudaSuccess) { cleanup(); return cuda_fail(sys, e, "adjoint setup"); }
+    std::vector<double> host_dq(n, 0.0);
+    for (pmgpu_force* f : fl) {
+        const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+        if (f->kind == 0) {
+            AdjArgs a;
+            memset(&a, 0, sizeof(a));
+            a.n = n; a.pos = sys->d_pos; a.q = sys->d_q; a.type = sys->d_type; a.mol = sys->d_mol;
+            a.pbc = sys->pbc; a.periodic = 1;
+            a.xfull = sys->d_xfull; a.xmod = sys->d_xmod; a.xrow = sys->d_xrow; a.xent = sys->d_xent;
+            a.ljd = sys->d_ljd; a.n_types = T;
+            a.n_terms = f->cp.n_terms; a.td[0] = f->td[0]; a.td[1] = f->td[1];
+            bool mod = false, use = false;
+            for (int t = 0; t < f->cp.n_terms; ++t) {
+                const int sw = f->cp.sw[t];
+                mod |= sw == PMGPU_SW_C1 || sw == PMGPU_SW_C2 || sw == PMGPU_SW_SHIFT;
+                use |= sw != PMGPU_SW_UNIVERSAL;
+            }
+            a.modify = mod ? 1 : 0; a.use_cut = use ? 1 : 0; a.cut2d = f->cut2; a.csf = sys->csf;
+            a.v = d_v; a.dq = d_dq; a.dlj = d_lj; a.hv = d_hv; a.energy = d_e;
+            ok((cudaError_t)launch_pair_adjoint(a, fp64 ? 1 : 0, s, &sys->launches));
+        } else {
+            const pmgpu_pme_params& p = f->pp;
+            if (p.reciprocal) {
+                PmeArgs a;
+                adj_pme_args(sys, f, a);
+                a.scale = fp64 ? kScaleFp64 : kScaleMixed;
+                const int stages[3] = {kStageSpread, kStageFft, kStagePotential};
+                for (int st = 0; st < 3 && e == cudaSuccess; ++st) {
+                    int u = 0;
+                    a.facc = (unsigned long long*)d_dq;   // phi output of the potential stage
+                    ok((cudaError_t)launch_pme_reciprocal(a, fp64 ? 1 : 0, s, &sys->launches, sys->d_erec, &u,
+                                                          stages[st]));
+                }
+            }
+            if (p.correction) {
+                CorrArgs c;
+                memset(&c, 0, sizeof(c));
+                c.n_excl = sys->e; c.pairs = sys->d_epairs; c.cls = sys->d_ecls; c.pos = sys->d_pos; c.q = sys->d_q;
+                c.pbc = sys->pbc; c.alpha = f->alpha; c.alpha2 = f->alpha * f->alpha; c.csf = sys->csf;
+                ok((cudaError_t)launch_pme_correction_adjoint(c, d_dq, s, &sys->launches));
+                // point self energy -alpha/sqrt(pi) sum q~^2 and the charged-system term
+                // -pi/(2 V alpha^2) (sum q~)^2 (initialize, :604-628), differentiated
+                double q1 = 0.0;
+                for (int i = 0; i < n; ++i) q1 += sys->q[i];
+                const double V = std::fabs(sys->box[0] * sys->box[4] * sys->box[8]);
+                const double charged = std::fabs(q1 * 0.00268283) > 1.0e-5
+                                           ? -kPi / (V * f->alpha * f->alpha) * q1 : 0.0;
+                for (int i = 0; i < n; ++i) host_dq[i] += -2.0 * f->alpha / std::sqrt(kPi) * sys->q[i] + charged;
+            }
+        }
+    }
+    std::vector<double> out_dq(n), out_lj((size_t)T * T * 4), out_hv(hv ? n3 : 0), out_e(2);
+    ok(cudaMemcpyAsync(out_dq.data(), d_dq, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    ok(cudaMemcpyAsync(out_lj.data(), d_lj, sizeof(double) * out_lj.size(), cudaMemcpyDeviceToHost, s));
+    ok(cudaMemcpyAsync(out_e.data(), d_e, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+    if (hv) ok(cudaMemcpyAsync(out_hv.data(), d_hv, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    ok(cudaStreamSynchronize(s));
+    cleanup();
+    if (e != cudaSuccess) return cuda_fail(sys, e, "adjoint");
+    if (dE_dq) for (int i = 0; i < n; ++i) dE_dq[i] += out_dq[i] + host_dq[i];
+    if (dE_dlj) for (size_t k = 0; k < out_lj.size(); ++k) dE_dlj[k] += out_lj[k];
+    if (hv) for (size_t k = 0; k < n3; ++k) hv[k] += out_hv[k];
+    if (energies) { energies[0] += out_e[0]; energies[1] += out_e[1]; }
+    return PMGPU_OK;
+}

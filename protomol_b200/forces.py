@@ -77,6 +77,7 @@ class Topology:
         check(lib.pmgpu_set_topology(self.handle, s.n_atoms, p(q), p(ty), p(mol), s.n_types, p(lj),
                                      int(ex.shape[0]), p(ex), p(cl), p(ck), float(s.csf)), self.handle)
         self.n_atoms = s.n_atoms
+        self.n_types = s.n_types
 
     def set_box(self, box, cell_size):
         lib = _lib.load()
@@ -193,6 +194,30 @@ def evaluate_group(topo: Topology, forces, positions, force_accum, energies: Sca
     energies.coulomb += e.coulomb
     if energies.virial:
         energies.virial_tensor += np.array(list(e.virial))
+
+
+def adjoint(topo: Topology, forces, positions, v=None):
+    """Backward pass of ``evaluate_group`` (pmgpu_adjoint): gradients of the
+    forces' total energy w.r.t. the scaled charges (N) and the LJ table
+    (T x T x 4, {A, B, A14, B14}), and with ``v`` (N x 3) the Hessian-vector
+    product of the pair terms.  Returns a dict of numpy arrays."""
+    lib = _lib.load()
+    pos = np.ascontiguousarray(positions, np.float64)
+    n, t = topo.n_atoms, topo.n_types
+    dq = np.zeros(n)
+    dlj = np.zeros((t, t, 4))
+    en = np.zeros(2)
+    hv = None
+    vv = None
+    if v is not None:
+        vv = np.ascontiguousarray(v, np.float64)
+        hv = np.zeros((n, 3))
+    arr = (_VP * len(forces))(*[f.handle for f in forces])
+    check(lib.pmgpu_adjoint(topo.handle, len(forces), arr, pos.ctypes.data_as(_VP),
+                            vv.ctypes.data_as(_VP) if vv is not None else None, dq.ctypes.data_as(_VP),
+                            dlj.ctypes.data_as(_VP), hv.ctypes.data_as(_VP) if hv is not None else None,
+                            en.ctypes.data_as(_VP)), topo.handle)
+    return {"dE_dq": dq, "dE_dlj": dlj, "hv": hv, "lennard_jones": en[0], "coulomb": en[1]}
 
 
 # --------------------------------------------------------------------------
