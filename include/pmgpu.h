@@ -151,6 +151,13 @@ int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* e2, const d
 /* Replaces NonbondedCutoffForce::doMake (forces/NonbondedCutoffForce.h:119-123). */
 int pmgpu_cutoff_create(pmgpu_system* sys, const pmgpu_cutoff_params* params, pmgpu_force** out);
 
+/* Replaces NonbondedSimpleFullSystemForce<OneAtomPair[Two]<Vacuum...>> made by
+ * the factory (forces/NonbondedSimpleFullSystemForce.h:165-182,
+ * factories/registerForceExemplarsSimpleFull.cpp:88-152): every pair once,
+ * plain differences (no periodic image), the same potentials and switches
+ * (algorithm_cutoff unused).  Needs no box. */
+int pmgpu_full_create(pmgpu_system* sys, const pmgpu_cutoff_params* params, pmgpu_force** out);
+
 /* Replaces NonbondedPMEwaldSystemForce::doMake (forces/NonbondedPMEwaldSystemForce.h:1099-1139);
  * rejects the same parameter sets with PMGPU_ERR_ARG (order < 2 or odd,
  * grid < order, cutoff <= 0, accuracy <= 0). */

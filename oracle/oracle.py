@@ -200,6 +200,22 @@ def evaluate(system, specs, positions=None, want_pairs=False, pair_cap=None):
     return out
 
 
+def pair_hessian(system, spec, positions=None):
+    """Dense (3N, 3N) Hessian of a cutoff / all-pairs force's pair terms as
+    integrators/Hessian.cpp:456-623 assembles it (LennardJones and Coulomb
+    under Universal, C1 or C2 switching); all-pairs forces use plain
+    differences (vacuum), cutoff forces the minimal image."""
+    keep = _Keep(system, positions)
+    n3 = 3 * keep.pos.shape[0]
+    H = np.zeros((n3, n3), np.float64)
+    p = _cut_params(spec)
+    rc = lib().pmo_pair_hessian(C.byref(keep.s), C.byref(p), 1 if spec["kind"] == "full" else 0,
+                                H.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise ValueError("no Hessian block for these terms (Hessian.cpp: LJ / Coulomb, Universal / C1 / C2)")
+    return H
+
+
 def cell_assign(system, positions=None):
     keep = _Keep(system, positions)
     cells = np.zeros((keep.pos.shape[0], 3), np.int32)

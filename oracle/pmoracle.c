@@ -944,3 +944,93 @@ int pmo_pme_force(const pmo_system* s, const pmo_pme_params* p, double* forces, 
     r->e_self += self; r->e_charged += charged;
     return 0;
 }
+
+/* ------------------------------------------------------------ Hessian */
+/* Switching-function Hessians (C2SwitchingFunction.cpp:45-53,
+ * C1SwitchingFunction.cpp:39-49): the matrix is s_i I + s_r rr^T. */
+static void switch_hessian(const term_t* t, double a, double* s_i, double* s_r)
+{
+    if (t->sw == PMO_SW_C2) {
+        double tm1 = t->cut2 - t->on2;
+        double tm2 = tm1 * tm1 * tm1;
+        *s_i = 12.0 * (a - t->cut2) * (a - t->on2) / tm2;
+        *s_r = 24.0 * (2.0 * a - t->cut2 - t->on2) / tm2;
+    } else {   /* C1 */
+        double r = sqrt(a);
+        double tm1 = 1.5 / (t->cut * r);
+        double tm2 = 1.5 / (t->cut * t->cut * t->cut) * r;
+        *s_i = -tm1 + tm2;
+        *s_r = (tm1 + tm2) / a;
+    }
+}
+
+/* Dense Hessian of the pair terms as integrators/Hessian.cpp:456-623 builds
+ * it: for every pair i < j that is not FULL-excluded, with rij the minimal
+ * difference, ReducedHessLennardJones (forces/ReducedHessLennardJones.cpp:7-51)
+ * or ReducedHessCoulomb (forces/ReducedHessCoulomb.cpp:8-43) gives
+ *   H = (tm1 I + tm2 rr) S + Shess E_raw - 2 F_raw S' rr
+ * (E_raw, F_raw and Shess only where 0 < S < 1), added to the ii and jj
+ * blocks and subtracted from the ij and ji blocks.  H: 3N x 3N, +=.
+ * Returns -1 for terms Hessian.cpp has no block for (Ewald real; switches
+ * other than Universal, C1, C2). */
+int pmo_pair_hessian(const pmo_system* s, const pmo_cutoff_params* p, int vacuum, double* H)
+{
+    pair_ctx pc;
+    pair_ctx_init(&pc, s, p);
+    for (int k = 0; k < p->n_terms; ++k) {
+        if (pc.t[k].pot != PMO_POT_LJ && pc.t[k].pot != PMO_POT_COULOMB) return -1;
+        if (pc.t[k].sw != PMO_SW_UNIVERSAL && pc.t[k].sw != PMO_SW_C1 && pc.t[k].sw != PMO_SW_C2) return -1;
+    }
+    pbc_t b;
+    if (!vacuum) pbc_set(&b, s->box);
+    excl_t ex; excl_build(&ex, s);
+    const size_t n3 = 3 * (size_t)s->n_atoms;
+    for (int i = 0; i < s->n_atoms; ++i)
+        for (int j = i + 1; j < s->n_atoms; ++j) {
+            int excl = s->mol[i] == s->mol[j] ? excl_check(&ex, i, j) : PMO_EXCL_NONE;
+            if (excl == PMO_EXCL_FULL) continue;
+            double a;
+            v3 r;
+            if (vacuum) { r = vsub(vload(s->pos + 3 * j), vload(s->pos + 3 * i)); a = vnorm2(r); }
+            else r = pbc_min_diff(&b, vload(s->pos + 3 * i), vload(s->pos + 3 * j), &a);
+            double rr[3] = {r.x, r.y, r.z};
+            double hi = 0.0, hr = 0.0;   /* H = hi I + hr rr^T */
+            for (int k = 0; k < p->n_terms; ++k) {
+                const term_t* t = &pc.t[k];
+                double sv = 1.0, sd = 0.0, shi = 0.0, shr = 0.0, e = 0.0, f = 0.0;
+                if (t->sw != PMO_SW_UNIVERSAL) {
+                    term_switch(t, a, &sv, &sd);
+                    if (sv > 0.0 && sv < 1.0) {
+                        term_potential(t, s, i, j, excl, a, 1.0 / a, &e, &f);
+                        switch_hessian(t, a, &shi, &shr);
+                    }
+                }
+                double ti, tr;
+                if (t->pot == PMO_POT_LJ) {
+                    const double* lp = s->lj + 4 * ((size_t)s->type[i] * s->n_types + s->type[j]);
+                    double A = excl == PMO_EXCL_MODIFIED ? lp[2] : lp[0];
+                    double B = excl == PMO_EXCL_MODIFIED ? lp[3] : lp[1];
+                    double a4 = a * a * a * a, a5 = a4 * a, a7 = a4 * a * a * a, a8 = a4 * a4;
+                    ti = 6 * B / a4 - 12 * A / a7;
+                    tr = -48 * B / a5 + 168 * A / a8;
+                } else {
+                    double csf = excl == PMO_EXCL_MODIFIED ? s->csf : 1.0;
+                    double tm1 = -csf * s->q[i] * s->q[j] / a / sqrt(a);
+                    ti = tm1;
+                    tr = -3.0 / a * tm1;
+                }
+                hi += ti * sv + shi * e;
+                hr += tr * sv + shr * e - 2.0 * f * sd;
+            }
+            for (int l = 0; l < 3; ++l)
+                for (int m = 0; m < 3; ++m) {
+                    double v = (l == m ? hi : 0.0) + hr * rr[l] * rr[m];
+                    H[(3 * (size_t)i + l) * n3 + 3 * (size_t)i + m] += v;
+                    H[(3 * (size_t)j + l) * n3 + 3 * (size_t)j + m] += v;
+                    H[(3 * (size_t)i + l) * n3 + 3 * (size_t)j + m] -= v;
+                    H[(3 * (size_t)j + l) * n3 + 3 * (size_t)i + m] -= v;
+                }
+        }
+    free(ex.e);
+    return 0;
+}

@@ -99,6 +99,11 @@ int pmo_pme_force(const pmo_system* s, const pmo_pme_params* p,
 int pmo_simple_full_force(const pmo_system* s, const pmo_cutoff_params* p,
                           double* forces, pmo_result* r);
 
+/* Dense 3N x 3N Hessian of the pair terms (integrators/Hessian.cpp:456-623),
+ * vacuum (plain differences) or periodic (minimal image); H +=.  Returns -1
+ * for terms without a Hessian block there. */
+int pmo_pair_hessian(const pmo_system* s, const pmo_cutoff_params* p, int vacuum, double* H);
+
 /* The poly5 erfc approximation (base/mathutilities.cpp:29-40). */
 double pmo_poly5(double ar);
 

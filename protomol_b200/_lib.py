@@ -28,6 +28,7 @@ EXPORTS = [
     "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
     "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
+    "pmgpu_full_create",
 ]
 PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
 
@@ -102,6 +103,7 @@ def load():
     lib.pmgpu_batch_stream.argtypes = [vp]
     lib.pmgpu_batch_stream.restype = vp
     lib.pmgpu_adjoint.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]
+    lib.pmgpu_full_create.argtypes = [vp, C.POINTER(CutoffParams), C.POINTER(vp)]
     _lib = lib
     return lib
 

@@ -144,6 +144,7 @@ __global__ void __launch_bounds__(kTile) k_pair_adjoint(AdjArgs p)
     }
     __syncthreads();
     double dq = 0.0, hv[3] = {0.0, 0.0, 0.0}, el = 0.0, ec = 0.0;
+    double fi[3] = {0.0, 0.0, 0.0}, vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (i < p.n) {
         const double xi = p.pos[3 * (size_t)i], yi = p.pos[3 * (size_t)i + 1], zi = p.pos[3 * (size_t)i + 2];
         const double qi = p.q[i];
@@ -189,6 +190,15 @@ __global__ void __launch_bounds__(kTile) k_pair_adjoint(AdjArgs p)
                 else ec += 0.5 * (double)(e * s);
             }
             dq += (double)pqq * s_q[jj];
+            if (p.facc) {   // F_i = -d F; the pair's virial d (x) d F, half per ordered pair
+                const double fd = (double)F;
+                fi[0] -= dx * fd; fi[1] -= dy * fd; fi[2] -= dz * fd;
+                if (p.virial) {
+                    const double h = 0.5 * fd;
+                    vir[0] += h * dx * dx; vir[1] += h * dx * dy; vir[2] += h * dx * dz;
+                    vir[3] += h * dy * dy; vir[4] += h * dy * dz; vir[5] += h * dz * dz;
+                }
+            }
             if (p.v) {
                 // (H v)_i += -K (v_j - v_i),  K = -(F I + 2 F' d d^T)
                 const double ux = s_v[jj][0] - vi[0], uy = s_v[jj][1] - vi[1], uz = s_v[jj][2] - vi[2];
@@ -217,6 +227,11 @@ __global__ void __launch_bounds__(kTile) k_pair_adjoint(AdjArgs p)
             if (el != 0.0) atomicAdd(p.energy, el);
             if (ec != 0.0) atomicAdd(p.energy + 1, ec);
         }
+        if (p.facc) fixed_add3(p.facc + 3 * (size_t)i, fi[0], fi[1], fi[2], p.scale, p.status);
+    }
+    if (p.erec) {
+        double acc[kERec] = {el, ec, vir[0], vir[1], vir[2], vir[1], vir[3], vir[4], vir[2], vir[4], vir[5]};
+        block_reduce_store<kTile / 32>(acc, p.erec, p.erec_stride, blockIdx.y * gridDim.x + blockIdx.x);
     }
     if (lj_smem) {
         __syncthreads();
@@ -226,6 +241,12 @@ __global__ void __launch_bounds__(kTile) k_pair_adjoint(AdjArgs p)
 }
 
 }  // namespace
+
+int adjoint_blocks(int n)
+{
+    const int t = (n + kTile - 1) / kTile;
+    return t * t;
+}
 
 int launch_pair_adjoint(const AdjArgs& a, int fp64, cudaStream_t s, long long* launches)
 {

@@ -180,8 +180,18 @@ struct AdjArgs {
     double* dlj;                 // T x T x 4 (+=) or null
     double* hv;                  // 3N (+=) or null
     double* energy;              // 2 (+=): LJ, Coulomb, or null
+    // forward mode (the vacuum all-pairs force): forces in atom order
+    // (fixed point) and one energy/virial record per block
+    unsigned long long* facc;    // 3N or null
+    double scale;
+    int* status;
+    double* erec;                // records or null
+    int erec_stride;
+    int virial;
 };
 int launch_pair_adjoint(const AdjArgs& a, int fp64, cudaStream_t s, long long* launches);
+// records (blocks) of one launch_pair_adjoint
+int adjoint_blocks(int n);
 
 // ---------------------------------------------------------------- PME
 struct PmeArgs {

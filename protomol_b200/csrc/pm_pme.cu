@@ -629,7 +629,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
 #pragma unroll
     for (int k = 0; k < kERec; ++k) v[k] = 0.0;
     if (s < a.n) {
-        const int i = a.sorted[s];
+        const int i = a.sorted ? a.sorted[s] : s;   // no cell-sorted order: atom order
         double fp[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int c = 0; c < 3; ++c) {

@@ -611,6 +611,62 @@ extern "C" int pmgpu_cutoff_create(pmgpu_system* sys, const pmgpu_cutoff_params*
     return PMGPU_OK;
 }
 
+// NonbondedSimpleFullSystemForce with VacuumBoundaryConditions
+// (forces/NonbondedSimpleFullSystemForce.h:165-182,
+// factories/registerForceExemplarsSimpleFull.cpp:88-152): every pair once, no
+// minimal image, the OneAtomPair[Two] potentials and switches
+extern "C" int pmgpu_full_create(pmgpu_system* sys, const pmgpu_cutoff_params* p, pmgpu_force** out)
+{
+    if (!sys || !p || !out) return PMGPU_ERR_ARG;
+    *out = nullptr;
+    if (p->n_terms < 1 || p->n_terms > 2) return fail(sys, PMGPU_ERR_ARG, "n_terms must be 1 or 2");
+    if (p->precision != PMGPU_PRECISION_MIXED && p->precision != PMGPU_PRECISION_FP64)
+        return fail(sys, PMGPU_ERR_ARG, "unknown precision");
+    for (int k = 0; k < p->n_terms; ++k) {
+        if (p->pot[k] < PMGPU_POT_LENNARD_JONES || p->pot[k] > PMGPU_POT_EWALD_REAL)
+            return fail(sys, PMGPU_ERR_ARG, "unknown potential");
+        if (p->sw[k] == PMGPU_SW_C2 && !(p->switchon[k] >= 0.0 && p->cutoff[k] > 0.0 && p->switchon[k] < p->cutoff[k]))
+            return fail(sys, PMGPU_ERR_ARG, "C2 switching function: 0 <= switchon < cutoff");
+        if (p->sw[k] != PMGPU_SW_UNIVERSAL && !(p->cutoff[k] > 0.0))
+            return fail(sys, PMGPU_ERR_ARG, "switching function cutoff > 0");
+        if (p->pot[k] == PMGPU_POT_EWALD_REAL && !(p->alpha[k] > 0.0))
+            return fail(sys, PMGPU_ERR_ARG, "CoulombEwaldReal -alpha > 0");
+    }
+    pmgpu_force* f = new pmgpu_force();
+    f->sys = sys;
+    f->kind = 2;
+    f->precision = p->precision;
+    f->cp = *p;
+    double c2 = 0.0;
+    for (int k = 0; k < p->n_terms; ++k) {
+        term_setup(p, k, f->tf[k], f->td[k]);
+        c2 = std::max(c2, f->td[k].cut2);
+    }
+    f->cut2 = c2;
+    sys->forces.insert(f);
+    *out = f;
+    return PMGPU_OK;
+}
+
+// the recompute kernel's arguments for a pair force (cutoff or vacuum)
+static void adj_pair_args(pmgpu_system* sys, pmgpu_force* f, AdjArgs& a)
+{
+    memset(&a, 0, sizeof(a));
+    a.n = sys->n; a.pos = sys->d_pos; a.q = sys->d_q; a.type = sys->d_type; a.mol = sys->d_mol;
+    a.pbc = sys->pbc; a.periodic = f->kind == 2 ? 0 : 1;
+    a.xfull = sys->d_xfull; a.xmod = sys->d_xmod; a.xrow = sys->d_xrow; a.xent = sys->d_xent;
+    a.ljd = sys->d_ljd; a.n_types = sys->t;
+    a.n_terms = f->cp.n_terms; a.td[0] = f->td[0]; a.td[1] = f->td[1];
+    bool mod = false, use = false;
+    for (int t = 0; t < f->cp.n_terms; ++t) {
+        const int sw = f->cp.sw[t];
+        mod |= sw == PMGPU_SW_C1 || sw == PMGPU_SW_C2 || sw == PMGPU_SW_SHIFT;
+        use |= sw != PMGPU_SW_UNIVERSAL;
+    }
+    a.modify = mod ? 1 : 0; a.use_cut = use ? 1 : 0; a.cut2d = f->cut2; a.csf = sys->csf;
+    a.status = sys->d_status;
+}
+
 // Neighbour-delta list of CellListEnumerator<Periodic, Cubic>::initialize
 // (topology/CellListEnumerator_periodicBoundaries.h:37-108).
 static void build_deltas(const CellGrid& g, double cutoff, std::vector<int4>& out, int& reach_ok)
@@ -985,6 +1041,7 @@ static int ensure_erec(pmgpu_system* sys, int need)
 static int pair_records(pmgpu_system* sys, pmgpu_force* f)
 {
     // the mixed kernel sums energies in fixed point (d_efix), no records
+    if (f->kind == 2) return adjoint_blocks(sys->n);
     return f->precision == PMGPU_PRECISION_FP64 ? pair_blocks(sys->grid, f->nd) : 0;
 }
 
@@ -996,15 +1053,17 @@ static int pme_xblocks(const pmgpu_force* f) { return f->pp.grid[1] * f->kzh; }
 // capacities.  Runs before an evaluation is enqueued (or captured).
 static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
 {
-    if (!sys->box_set) return fail(sys, PMGPU_ERR_STATE, "box not set (pmgpu_set_box)");
     if (nf < 0 || (nf > 0 && !forces)) return fail(sys, PMGPU_ERR_ARG, "bad force list");
+    bool periodic = false;
+    for (int k = 0; k < nf; ++k) periodic |= forces[k] && forces[k]->kind != 2;
+    if (periodic && !sys->box_set) return fail(sys, PMGPU_ERR_STATE, "box not set (pmgpu_set_box)");
     int need = 1;
     for (int k = 0; k < nf; ++k) {
         pmgpu_force* f = forces[k];
         if (!f || f->sys != sys) return fail(sys, PMGPU_ERR_ARG, "force belongs to another system");
-        int r = f->kind == 0 ? prepare_cutoff(f) : prepare_pme(f);
+        int r = f->kind == 0 ? prepare_cutoff(f) : (f->kind == 1 ? prepare_pme(f) : PMGPU_OK);
         if (r) return r;
-        if (f->kind == 0) need += pair_records(sys, f);
+        if (f->kind != 1) need += pair_records(sys, f);
         else need += pme_xblocks(f) + 148 * 4;
     }
     need += (sys->n + 255) / 256;   // finalize: pair virial records
@@ -1088,9 +1147,13 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
     if (use32) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
-    bool any_cut = false, any_pme = false;
-    for (int k = 0; k < nf; ++k) (forces[k]->kind == 0 ? any_cut : any_pme) = true;
-    if (any_pme) CK(cudaMemsetAsync(sys->d_faccA, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
+    bool any_cut = false, any_pme = false, any_full = false;
+    for (int k = 0; k < nf; ++k) {
+        any_cut |= forces[k]->kind == 0;
+        any_pme |= forces[k]->kind == 1;
+        any_full |= forces[k]->kind == 2;
+    }
+    if (any_pme || any_full) CK(cudaMemsetAsync(sys->d_faccA, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     int used = 0;
     // PME: reads only positions and charges and accumulates in atom order
     auto enqueue_pme = [&](cudaStream_t ps) -> int {
@@ -1162,9 +1225,29 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         if (r) return r;
         CK(cudaEventRecord(sys->ev_join, sys->side), "join");
     }
-    r = bin(sys, d_pos);
-    if (r) return r;
+    if (any_cut) {   // the cell-sorted order is for the cutoff forces only
+        r = bin(sys, d_pos);
+        if (r) return r;
+    }
     prof_end(sys, mbin);
+    // vacuum all-pairs forces: the recompute kernel in forward mode, forces in
+    // atom order like PME
+    for (int k = 0; k < nf; ++k) {
+        pmgpu_force* f = forces[k];
+        if (f->kind != 2) continue;
+        const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+        AdjArgs a;
+        adj_pair_args(sys, f, a);
+        a.pos = d_pos;
+        a.facc = fp64 ? sys->d_faccA + n3 : sys->d_faccA;
+        a.scale = fp64 ? kScaleFp64 : kScaleMixed;
+        a.erec = sys->d_erec + used; a.erec_stride = sys->erec_cap; a.virial = virial;
+        int m = prof_begin(sys, kPhasePair);
+        int e = launch_pair_adjoint(a, fp64 ? 1 : 0, s, &sys->launches);
+        if (e) return cuda_fail(sys, (cudaError_t)e, "all-pairs force");
+        prof_end(sys, m);
+        used += pair_records(sys, f);
+    }
     int lists = 0;
     int pair_virial = 0;
     for (int k = 0; k < nf; ++k) {
@@ -1203,15 +1286,16 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         FinArgs fa;
         memset(&fa, 0, sizeof(fa));
         fa.n = sys->n;
-        fa.f32 = use32 ? sys->d_facc32 : nullptr;
-        fa.f32p = use32 ? sys->d_facc32p : nullptr;
-        fa.f40 = use40 ? sys->d_facc40 : nullptr;
+        // the slot-ordered accumulators exist only with the cell-sorted order
+        fa.f32 = use32 && any_cut ? sys->d_facc32 : nullptr;
+        fa.f32p = use32 && any_cut ? sys->d_facc32p : nullptr;
+        fa.f40 = use40 && any_cut ? sys->d_facc40 : nullptr;
         for (int k = 0; k < nf; ++k)
-            if (forces[k]->kind == 1) {
+            if (forces[k]->kind != 0) {
                 if (forces[k]->precision == PMGPU_PRECISION_FP64) fa.a40 = sys->d_faccA + n3;
                 else fa.a32 = sys->d_faccA;
             }
-        fa.sorted = sys->d_sorted; fa.spos = sys->d_spos; fa.slo = sys->d_slo;
+        fa.sorted = any_cut ? sys->d_sorted : nullptr; fa.spos = sys->d_spos; fa.slo = sys->d_slo;
         fa.pair_virial = pair_virial;
         fa.fout = d_fout;
         fa.erec = sys->d_erec + used; fa.erec_stride = sys->erec_cap;
@@ -1761,21 +1845,9 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
     std::vector<double> host_dq(n, 0.0);
     for (pmgpu_force* f : fl) {
         const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
-        if (f->kind == 0) {
+        if (f->kind == 0 || f->kind == 2) {
             AdjArgs a;
-            memset(&a, 0, sizeof(a));
-            a.n = n; a.pos = sys->d_pos; a.q = sys->d_q; a.type = sys->d_type; a.mol = sys->d_mol;
-            a.pbc = sys->pbc; a.periodic = 1;
-            a.xfull = sys->d_xfull; a.xmod = sys->d_xmod; a.xrow = sys->d_xrow; a.xent = sys->d_xent;
-            a.ljd = sys->d_ljd; a.n_types = T;
-            a.n_terms = f->cp.n_terms; a.td[0] = f->td[0]; a.td[1] = f->td[1];
-            bool mod = false, use = false;
-            for (int t = 0; t < f->cp.n_terms; ++t) {
-                const int sw = f->cp.sw[t];
-                mod |= sw == PMGPU_SW_C1 || sw == PMGPU_SW_C2 || sw == PMGPU_SW_SHIFT;
-                use |= sw != PMGPU_SW_UNIVERSAL;
-            }
-            a.modify = mod ? 1 : 0; a.use_cut = use ? 1 : 0; a.cut2d = f->cut2; a.csf = sys->csf;
+            adj_pair_args(sys, f, a);
             a.v = d_v; a.dq = d_dq; a.dlj = d_lj; a.hv = d_hv; a.energy = d_e;
             ok((cudaError_t)launch_pair_adjoint(a, fp64 ? 1 : 0, s, &sys->launches));
         } else {

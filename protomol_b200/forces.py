@@ -62,7 +62,8 @@ class Topology:
         self.n_atoms = system.n_atoms
         self._forces = weakref.WeakSet()
         self.set_topology(system)
-        self.set_box(system.box, system.cell_size)
+        if getattr(system, "periodic", True):   # a vacuum system needs no box
+            self.set_box(system.box, system.cell_size)
 
     def set_topology(self, s):
         lib = _lib.load()
@@ -166,6 +167,10 @@ class NonbondedCutoffSystemForce(SystemForce):
     keyword = "NonbondedCutoff"
 
 
+class NonbondedSimpleFullSystemForce(SystemForce):
+    keyword = "NonbondedSimpleFull"
+
+
 class NonbondedPMEwaldSystemForce(SystemForce):
     keyword = "PMEwald"
 
@@ -218,6 +223,30 @@ def adjoint(topo: Topology, forces, positions, v=None):
                             dlj.ctypes.data_as(_VP), hv.ctypes.data_as(_VP) if hv is not None else None,
                             en.ctypes.data_as(_VP)), topo.handle)
     return {"dE_dq": dq, "dE_dlj": dlj, "hv": hv, "lennard_jones": en[0], "coulomb": en[1]}
+
+
+def lj_parameter_gradient(type_params, dE_dlj):
+    """Chain rule from the LJ-table gradient of ``adjoint`` to the per-type
+    parameters of the PAR file: returns (T, 4) = dE/d(eps, Rmin/2, eps14,
+    Rmin14/2), the table being built by the CHARMM combination rule
+    (frontend/buildTopology.cpp:646-664): A = (R_x + R_y)^12 sqrt(e_x e_y),
+    B = 2 (R_x + R_y)^6 sqrt(e_x e_y), likewise A14 / B14."""
+    tp = np.asarray(type_params, np.float64)
+    g = np.asarray(dE_dlj, np.float64)
+    out = np.zeros_like(tp)
+    for k, (ie, ir) in enumerate(((0, 1), (2, 3))):
+        eps, rh = tp[:, ie], tp[:, ir]
+        r = rh[:, None] + rh[None, :]
+        e = np.sqrt(eps[:, None] * eps[None, :])
+        A = r ** 12 * e
+        B = 2.0 * r ** 6 * e
+        gA, gB = g[:, :, 2 * k], g[:, :, 2 * k + 1]
+        m = gA * A + gB * B                  # d/d ln(e): both entries scale with sqrt(e_x e_y)
+        with np.errstate(divide="ignore", invalid="ignore"):   # undefined (nan) where eps = 0
+            out[:, ie] = (m.sum(1) + m.sum(0)) / (2.0 * eps)
+        nr = (12.0 * gA * A + 6.0 * gB * B) / r
+        out[:, ir] = nr.sum(1) + nr.sum(0)
+    return out
 
 
 # --------------------------------------------------------------------------
@@ -329,6 +358,31 @@ def parse_definition(definition: str) -> dict:
                 rc = vals[k]; k += 1
             terms.append((s, n, on, rc, alpha))
         return {"kind": "cut", "terms": terms, "algo_cutoff": vals[k]}
+    if algorithm == "NonbondedSimpleFull":
+        # vacuum all pairs; a Universal switch is not written in the id, so
+        # either every term names its switch or none does
+        if not 1 <= len(names) <= 2 or (sws and len(sws) != len(names)) or any(s not in _SWITCHES for s in sws):
+            raise ValueError(f"Could not find a complete match for '{definition}'")
+        sws = sws or ["Universal"] * len(names)
+        params = []
+        for n, s in zip(names, sws):
+            params += _pot_params(n) + _switch_params(s)
+        params.append(_Param("-blocksize", 32))
+        vals = _parse_values(rest, params)
+        if any(v is None for v in vals):
+            raise ValueError(f"force {definition}: missing parameter(s)")
+        vals = [float(v) for v in vals]
+        terms, k = [], 0
+        for n, s in zip(names, sws):
+            alpha = on = rc = 0.0
+            if n == "CoulombEwaldReal":
+                alpha = vals[k]; k += 1
+            if s == "C2":
+                on, rc = vals[k], vals[k + 1]; k += 2
+            elif s in ("C1", "Cutoff", "Shift"):
+                rc = vals[k]; k += 1
+            terms.append((s, n, on, rc, alpha))
+        return {"kind": "full", "terms": terms}
     if algorithm == "PMEwald":
         if names != ["Coulomb"] or (interp or "BSpline") != "BSpline":
             raise ValueError(f"Could not find a complete match for '{definition}'")
@@ -368,6 +422,21 @@ class ForceFactory:
             ident = (" ".join(t[1] for t in spec["terms"]) +
                      "".join(f" -switchingFunction {t[0]}" for t in spec["terms"]) + " -algorithm NonbondedCutoff")
             return NonbondedCutoffSystemForce(topo, h, ident, spec)
+        if spec["kind"] == "full":
+            cp = _lib.CutoffParams()
+            cp.n_terms = len(spec["terms"])
+            for t, (s, n, on, rc, alpha) in enumerate(spec["terms"]):
+                cp.pot[t] = _lib.POT[n]
+                cp.sw[t] = _lib.SW[s]
+                cp.switchon[t] = on
+                cp.cutoff[t] = rc
+                cp.alpha[t] = alpha
+            cp.precision = prec
+            check(lib.pmgpu_full_create(topo.handle, C.byref(cp), C.byref(h)), topo.handle)
+            ident = (" ".join(t[1] for t in spec["terms"]) +
+                     "".join(f" -switchingFunction {t[0]}" for t in spec["terms"] if t[0] != "Universal") +
+                     " -algorithm NonbondedSimpleFull")
+            return NonbondedSimpleFullSystemForce(topo, h, ident, spec)
         pp = _lib.PmeParams()
         pp.real, pp.reciprocal, pp.correction = spec["real"], spec["reciprocal"], spec["correction"]
         for k in range(3):
