@@ -37,6 +37,9 @@ METRIC = "force evals/s (cutoff+PME) mixed vs FP64 on one B200 at ≤1e-5 force 
 UNIT = "evals/s"
 FP32_LANES_PER_SM = 128
 N_SMS = 148
+# DRAM bytes (read + write) of one k_pair_mixed launch on this workload, from
+# the ncu capture summarised in profiles/k_pair_mixed_chain14281.md
+PAIR_DRAM_BYTES_PER_LAUNCH = 4_687_616
 
 
 def parse():
@@ -280,7 +283,8 @@ def main():
     achieved = n_pairs * flops_per_pair / (pair_ms * 1e-3) / 1e12
     roofline = {"bound": "fp32", "kernel": "k_pair_mixed<LJ C2 + EwaldReal Cutoff>",
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": None, "launch_ms": pair_ms,
+                "traffic": PAIR_DRAM_BYTES_PER_LAUNCH, "traffic_unit": "B per launch (ncu)",
+                "launch_ms": pair_ms,
                 "peak_source": f"nominal FP32 CUDA-core rate at sm_max_mhz of MEASURED_PEAKS.json ({peak_src}): "
                                "148 SMs x 128 lanes x 2 flop",
                 "algorithmic": f"{n_pairs} pairs x {flops_per_pair} flop per launch"}
