@@ -237,6 +237,36 @@ def poly5(x: float) -> float:
 
 
 # --------------------------------------------------------------- reference
+def run_reference_parallel(system, specs, repeat: int, procs: int, fast: bool = True, timeout=None):
+    """``procs`` independent processes of the compiled reference, all running
+    at once, each timing ``repeat`` evaluations of the same system (the
+    reference's force path is single-threaded: one evaluation uses one core,
+    so the host's cores are used by replicas).  Returns the per-process
+    seconds per evaluation; the host's throughput is the sum of the rates."""
+    exe = os.path.join(REF_DIR, "pmref_fast" if fast else "pmref")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    with tempfile.TemporaryDirectory() as td:
+        sp = os.path.join(td, "sys.bin")
+        system.save(sp)
+        extra = []
+        for spec in specs:
+            extra += _spec_args(spec)
+        outs = [os.path.join(td, f"out{k}.bin") for k in range(procs)]
+        ps = [subprocess.Popen([exe, sp, o, str(int(repeat))] + extra, stdout=subprocess.DEVNULL)
+              for o in outs]
+        try:
+            for p in ps:
+                if p.wait(timeout=timeout) != 0:
+                    raise RuntimeError(f"reference process exited with {p.returncode}")
+        finally:
+            for p in ps:
+                if p.poll() is None:
+                    p.kill()
+                    p.wait()
+        return [float(np.frombuffer(open(o, "rb").read(13 * 8), np.float64)[11]) for o in outs]
+
+
 def reference_available(fast: bool = False) -> bool:
     return os.path.exists(os.path.join(REF_DIR, "pmref_fast" if fast else "pmref"))
 

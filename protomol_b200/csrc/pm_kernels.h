@@ -112,6 +112,11 @@ struct PairArgs {
     float cut2f;                 // pair test (largest switching cutoff^2)
     double cut2d;
     float guard;                 // relative guard band of the FP32 tests
+    float near2;                 // mixed kernel: pairs with FP32 r^2 below this get FP64 energies (0: none)
+    int2* near;                  // those pairs: sorted slots i, j | 1 << 30 for a 1-4 (modified) pair
+    int* near_count;
+    int* near_need;
+    int near_cap;
     float csf;
     double csfd;
     int virial;
@@ -144,6 +149,8 @@ int pair_combo_id(int n_terms, const int* pot, const int* sw);
 // K2a: the cluster-pair list; K2b: the mixed kernel over it
 int launch_cluster_list(const PairArgs& a, cudaStream_t s, long long* launches);
 int launch_pair_mixed(const PairArgs& a, int combo, cudaStream_t s, long long* launches);
+// K2c: FP64 energies of the near pairs listed by the mixed pair kernel
+int launch_near_energy(const PairArgs& a, int combo, int n_atoms, cudaStream_t s, long long* launches);
 int launch_pair_fp64(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches);
 int pair_blocks(const CellGrid& g, int nd);
 // blocks of the mixed kernel (4 warps, one energy record per warp)

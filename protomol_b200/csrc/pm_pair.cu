@@ -36,6 +36,8 @@
 //
 // FP64 kernel: every pair through the reference's minimalDifference on the
 // FP64 positions, reference operation order throughout.
+#include <algorithm>
+
 #include "pm_kernels.h"
 #include "../../include/pmgpu.h"
 
@@ -220,7 +222,6 @@ __device__ __forceinline__ double exact_d2(const PairArgs& p, int oi, int oj)
     return pbc_min_diff(p.pbc, pi[0], pi[1], pi[2], pj[0], pj[1], pj[2], dx, dy, dz);
 }
 
-#include "pm_pair_mixed.cuh"
 
 // ---------------------------------------------------------------- FP64 math
 template <int POT>
@@ -291,6 +292,8 @@ __device__ __forceinline__ void sw_f64(const TermD& t, double d2, double& v, dou
         v = 1.0; d = 0.0;
     }
 }
+
+#include "pm_pair_mixed.cuh"
 
 template <int NT, int P0, int S0, int P1, int S1>
 __global__ void __launch_bounds__(128) k_pair_fp64(PairArgs p)
@@ -502,6 +505,24 @@ int launch_pair_mixed(const PairArgs& a, int combo, cudaStream_t s, long long* l
 #undef PM_MIXED_CASE
     default: return (int)cudaErrorInvalidValue;
     }
+}
+
+int launch_near_energy(const PairArgs& a, int combo, int n_atoms, cudaStream_t s, long long* launches)
+{
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    // about 26 near pairs per atom in water, one per thread; at most one
+    // resident wave (16 blocks per SM; the kernel is grid-stride)
+    long long want = (30LL * n_atoms + 127) / 128;
+    const int blocks = (int)std::max(1LL, std::min<long long>(want, 16LL * sms));
+    PM_COMBO_SWITCH(k_near_energy)
+    *launches += 1;
+    return (int)cudaGetLastError();
 }
 
 int launch_pair_fp64(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches)

@@ -34,6 +34,16 @@
 // rounded to int64 fixed point and summed as integers, so all results are
 // independent of the order of the list and of the chunk-to-warp assignment.
 //
+// Near pairs (FP32 r^2 < near2, 5 A): on water their energies reach ~30
+// kcal/mol each while the total is a ~1e-3 cancellation of the sum of |e|,
+// so their FP32 rounding is nearly all of the energy error (1.8e-7 of |E_LJ|
+// + |E_C| on the 14,281-atom box with FP32 energies everywhere).  K2b leaves
+// their energies out and queues the pairs per warp in shared memory, then
+// appends the queue to the near-pair list once per chunk (one atomic); K2c
+// (k_near_energy) evaluates their energies in FP64 with the FP64 kernel's
+// arithmetic, one pair per thread, each rounded to fixed point on its own.
+// Their forces stay FP32.
+//
 // Virial: with the whole-cell offsets o of the half shell, the pair vector is
 // d = (p_j + o) - p_i with p the atom's position relative to its cell
 // corner, so sum_pairs d (x) f = sum_atoms p (x) F_pair + sum_entries o (x)
@@ -45,6 +55,7 @@
 constexpr float kFarAway = 1.0e4f;   // position of the padding lanes of partial clusters
 constexpr int kSuper = 4;            // clusters per i-supercluster
 constexpr int kChunk = 16;           // list entries per chunk of work
+constexpr int kNearCap = 512;        // near pairs a warp queues for FP64 energies
 
 // ---------------------------------------------------------------- K2a: list
 __device__ __forceinline__ bool box_near(const float4& ilo, const float4& ihi, const float4& jlo, const float4& jhi,
@@ -282,6 +293,52 @@ __device__ __forceinline__ void pair_math(const PairArgs& p, const PairGeo& g, c
     ec = g.act ? c : 0.f;
 }
 
+// FP64 energies of one pair of sorted slots, the FP64 kernel's arithmetic
+// (pot_f64, sw_f64) on the raw positions and charges (spos64) and the exact
+// minimal image: the FP64 kernel's value of the pair
+template <int NT, int P0, int S0, int P1, int S1>
+__device__ __forceinline__ void pair_energy_f64(const PairArgs& p, int si, int sj, int excl, double& el, double& ec)
+{
+    constexpr bool kMod = sw_modifies(S0) || (NT > 1 && sw_modifies(S1));
+    const double4 pi = p.spos64[si], pj = p.spos64[sj];
+    const int ti = p.smeta[si].y, tj = p.smeta[sj].y;
+    double dx, dy, dz;
+    const double d2 = pbc_min_diff(p.pbc, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+    const double rd2 = 1.0 / d2;
+    double e0, f0, e1 = 0.0, f1 = 0.0;
+    pot_f64<P0>(p, p.td[0], d2, rd2, pi.w, pj.w, ti, tj, excl, e0, f0);
+    if (NT > 1) pot_f64<P1>(p, p.td[1], d2, rd2, pi.w, pj.w, ti, tj, excl, e1, f1);
+    if (kMod) {
+        double sv, sd;
+        sw_f64<S0>(p.td[0], d2, sv, sd);
+        e0 *= sv;
+        if (NT > 1) {
+            sw_f64<S1>(p.td[1], d2, sv, sd);
+            e1 *= sv;
+        }
+    }
+    el += (P0 == LJ ? e0 : 0.0) + (NT > 1 && P1 == LJ ? e1 : 0.0);
+    ec += (P0 != LJ ? e0 : 0.0) + (NT > 1 && P1 != LJ ? e1 : 0.0);
+}
+
+// the warp's queued near pairs -> the near-pair list (called by the whole
+// warp); a full list sets the capacity status and the size it needs
+__device__ __forceinline__ void append_near(const PairArgs& p, const int2* q, int nq, int lane)
+{
+    const unsigned FULL = 0xffffffffu;
+    __syncwarp();                                    // the other lanes' entries are visible
+    int base = 0;
+    if (lane == 0) base = atomicAdd(p.near_count, nq);
+    base = __shfl_sync(FULL, base, 0);
+    if (base <= p.near_cap - nq) {
+        for (int k = lane; k < nq; k += 32) p.near[base + k] = q[k];
+    } else if (lane == 0) {
+        atomicOr(p.status, kStatusListFull);
+        atomicMax(p.near_need, base + nq);
+    }
+    __syncwarp();                                    // the queue is refilled next
+}
+
 // int64 fixed-point add of one FP32 value (value * 2^32 is exact in FP32)
 __device__ __forceinline__ void fixed_addf(unsigned long long* slot, float v, int* status)
 {
@@ -334,6 +391,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, il = lane & 7, jg = lane >> 3;
     __shared__ float4 s_p[4][kSuper * kCluster], s_l[4][kSuper * kCluster];
     __shared__ int4 s_m[4][kSuper * kCluster];
+    __shared__ int2 s_near[4][kNearCap];
     __shared__ unsigned long long s_e[kERec];
     if (threadIdx.x < kERec) s_e[threadIdx.x] = 0ull;
     __syncthreads();
@@ -364,6 +422,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
 #pragma unroll
         for (int q = 0; q < kSuper; ++q) fi[q][0] = fi[q][1] = fi[q][2] = 0.f;
         double el = 0.0, ec = 0.0;
+        int nq = 0;                                // queued near pairs
         double wv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
         const int e_end = cd.z + cd.w;
@@ -376,6 +435,10 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
             load_atom(p, ent.x + jg + 4, jg + 4 < nj, -kFarAway, jb);
         }
         for (int e = cd.z; e < e_end; ++e) {
+            if (nq > kNearCap - 2 * kSuper * 32) {         // room for one more entry
+                append_near(p, s_near[w], nq, lane);
+                nq = 0;
+            }
             const int2 cur = ent;
             const JAtom ca = ja, cb = jb;
             if (e + 1 < e_end) {                   // software pipeline
@@ -424,6 +487,27 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
                     const float x2 = gb.dx * ftb, y2 = gb.dy * ftb, z2 = gb.dz * ftb;
                     fi[0][0] -= x1 + x2; fi[0][1] -= y1 + y2; fi[0][2] -= z1 + z2;
                     fax += x1; fay += y1; faz += z1; fbx += x2; fby += y2; fbz += z2;
+                    // near pairs: queued for FP64 energies in place of the FP32 ones
+                    {
+                        const bool na = ga.act && ga.r2 < p.near2, nb = gb.act && gb.r2 < p.near2;   // near2 = 0: none
+                        const unsigned ba = __ballot_sync(FULL, na), bb = __ballot_sync(FULL, nb);
+                        if (ba | bb) {
+                            const unsigned lt = (1u << lane) - 1u;
+                            const int si = cd.x + q * kCluster + il, sj = cur.x + jg;
+                            if (na) {
+                                s_near[w][nq + __popc(ba & lt)] =
+                                    make_int2(si, sj | (ga.excl == PMGPU_EXCL_MODIFIED ? 1 << 30 : 0));
+                                ela = 0.f; eca = 0.f;
+                            }
+                            nq += __popc(ba);
+                            if (nb) {
+                                s_near[w][nq + __popc(bb & lt)] =
+                                    make_int2(si, (sj + 4) | (gb.excl == PMGPU_EXCL_MODIFIED ? 1 << 30 : 0));
+                                elb = 0.f; ecb = 0.f;
+                            }
+                            nq += __popc(bb);
+                        }
+                    }
                     el += (double)(ela + elb);
                     ec += (double)(eca + ecb);
                     if (WRAP && p.virial) {
@@ -475,6 +559,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
             const int s = q * kCluster + il;
             if (jg < 3 && s < cd.y && v != 0.f) fixed_addf(p.facc + 3 * (size_t)(cd.x + s) + jg, v, p.status);
         }
+        if (nq > 0) append_near(p, s_near[w], nq, lane);
         acc[0] += fixed_of(el, bad);
         acc[1] += fixed_of(ec, bad);
         if (p.virial) {
@@ -514,4 +599,38 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
     }
     __syncthreads();
     if (threadIdx.x < kERec && s_e[threadIdx.x] != 0ull) atomicAdd(p.efix + threadIdx.x, s_e[threadIdx.x]);
+}
+
+// K2c: the FP64 energies of the near pairs the mixed pair kernel listed (it
+// left their FP32 energies out).  Each pair's energies are rounded to int64
+// fixed point on their own, so the sums do not depend on the list's order.
+template <int NT, int P0, int S0, int P1, int S1>
+__global__ void __launch_bounds__(128) k_near_energy(PairArgs p)
+{
+    const unsigned FULL = 0xffffffffu;
+    __shared__ long long s_acc[2][4];
+    if (*p.status & kStatusListFull) return;               // block-uniform
+    const int n = min(*p.near_count, p.near_cap);
+    long long al = 0, ac = 0;
+    bool bad = false;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int2 e = p.near[k];
+        double el = 0.0, ec = 0.0;
+        pair_energy_f64<NT, P0, S0, P1, S1>(p, e.x, e.y & 0x3fffffff,
+                                            (e.y >> 30) ? PMGPU_EXCL_MODIFIED : PMGPU_EXCL_NONE, el, ec);
+        al += fixed_of(el, bad);
+        ac += fixed_of(ec, bad);
+    }
+    if (bad) atomicOr(p.status, kStatusOverflow);
+    for (int o = 16; o > 0; o >>= 1) {
+        al += __shfl_xor_sync(FULL, al, o);
+        ac += __shfl_xor_sync(FULL, ac, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { s_acc[0][w] = al; s_acc[1][w] = ac; }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        long long t = s_acc[threadIdx.x][0] + s_acc[threadIdx.x][1] + s_acc[threadIdx.x][2] + s_acc[threadIdx.x][3];
+        if (t != 0) atomicAdd(p.efix + threadIdx.x, (unsigned long long)t);
+    }
 }

@@ -131,6 +131,9 @@ struct pmgpu_system {
     int4* d_chunks = nullptr;
     long long chunk_cap = 0;
     long long chunk_need = 0;
+    int2* d_near = nullptr;            // near pairs of the mixed kernels (FP64 energies)
+    long long near_cap = 0;
+    long long near_need = 0;
     int ncell_cap = 0;
     double* d_erec = nullptr;
     int erec_cap = 0;
@@ -296,6 +299,7 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     dfree(sys->d_counts); dfree(sys->d_fill); dfree(sys->d_start); dfree(sys->d_erec);
     dfree(sys->d_small); dfree(sys->d_energy);
     dfree(sys->d_cstart); dfree(sys->d_cbox); dfree(sys->d_ccell); dfree(sys->d_plist); dfree(sys->d_chunks);
+    dfree(sys->d_near);
     if (sys->h_energy) cudaFreeHost(sys->h_energy);
     cudaEventDestroy(sys->ev_fork);
     cudaEventDestroy(sys->ev_join);
@@ -359,10 +363,12 @@ extern "C" int pmgpu_synchronize(pmgpu_system* sys)
     if (st & kStatusOverflow)
         return fail(sys, PMGPU_ERR_OVERFLOW, "non-finite or out-of-range force (fixed-point range exceeded)");
     if (st & kStatusListFull) {
-        int need[3] = {0, 0, 0};   // list need, chunk count, chunk need
+        // list need, chunk count, chunk need, work counter, near count, near need
+        int need[6] = {0, 0, 0, 0, 0, 0};
         CK(cudaMemcpy(need, sys->d_plist_need, sizeof(need), cudaMemcpyDeviceToHost), "status");
         sys->plist_need = std::max<long long>(sys->plist_need, need[0]);
         sys->chunk_need = std::max<long long>(sys->chunk_need, need[2]);
+        sys->near_need = std::max<long long>(sys->near_need, need[5]);
         return fail(sys, PMGPU_ERR_CAPACITY, "cluster-pair list capacity exceeded (grown for the next evaluation)");
     }
     return PMGPU_OK;
@@ -1005,6 +1011,8 @@ static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_po
     a.half_rule = f->half_rule; a.ccell = sys->d_ccell; a.ncl_cap = sys->cbox_cap;
     a.plist = sys->d_plist; a.plist_cap = (int)sys->plist_cap;
     a.chunks = sys->d_chunks; a.chunk_cap = (int)sys->chunk_cap;
+    a.near = sys->d_near; a.near_cap = (int)sys->near_cap;
+    a.near_count = sys->d_status + 6; a.near_need = sys->d_status + 7;
     a.plist_count = sys->d_plist_count; a.plist_need = sys->d_plist_need;
     a.chunk_count = sys->d_chunk_count; a.chunk_need = sys->d_chunk_need; a.chunk_next = sys->d_chunk_next;
     a.hoff64 = f->d_hoff64; a.efix = sys->d_efix;
@@ -1019,6 +1027,10 @@ static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_po
     a.tf[0] = f->tf[0]; a.tf[1] = f->tf[1]; a.td[0] = f->td[0]; a.td[1] = f->td[1];
     a.cut2f = (float)f->cut2; a.cut2d = f->cut2;
     a.guard = 2.0e-5f;
+    // the energies of pairs closer than 5 A are recomputed in FP64: they hold
+    // nearly all of the FP32 energy rounding (|e| up to ~30 kcal/mol each on
+    // water, where the total is a ~1e-3 cancellation of the sum of |e|)
+    a.near2 = sys->d_near ? 25.0f : 0.0f;
     a.csf = (float)sys->csf; a.csfd = sys->csf;
     a.status = sys->d_status;
     // mixed forces on whole-cell shifts go to the pair accumulator (their
@@ -1096,6 +1108,14 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
         if (cneed > sys->chunk_cap) {
             CK(dalloc(&sys->d_chunks, (size_t)cneed), "alloc");
             sys->chunk_cap = cneed;
+            sys->buf_version++;
+        }
+        // near pairs (< 5 A): ~26 per atom in water
+        long long nneed = std::max(30LL * sys->n + 4096, sys->near_need + sys->near_need / 4);
+        if (nneed > INT_MAX / 2) return fail(sys, PMGPU_ERR_CAPACITY, "near-pair list above 2^30 entries");
+        if (nneed > sys->near_cap) {
+            CK(dalloc(&sys->d_near, (size_t)nneed), "alloc");
+            sys->near_cap = nneed;
             sys->buf_version++;
         }
     }
@@ -1261,7 +1281,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         a.erec = sys->d_erec + used;
         if (!fp64) {
             // list count and need, chunk count and need, work counter
-            if (lists++ > 0) CK(cudaMemsetAsync(sys->d_plist_count, 0, 5 * sizeof(int), s), "memset");
+            if (lists++ > 0) CK(cudaMemsetAsync(sys->d_plist_count, 0, 6 * sizeof(int), s), "memset");
             int ml = prof_begin(sys, kPhaseList);
             int e = launch_cluster_list(a, s, &sys->launches);
             if (e) return cuda_fail(sys, (cudaError_t)e, "cluster-pair list");
@@ -1271,6 +1291,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         a.reserve = 0;
         int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
                      : launch_pair_mixed(a, f->combo, s, &sys->launches);
+        if (!e && !fp64 && a.near2 > 0.0f) e = launch_near_energy(a, f->combo, sys->n, s, &sys->launches);
         if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
         prof_end(sys, m);
         used += pair_records(sys, f);
@@ -1386,7 +1407,8 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
         CK(cudaMemcpyAsync(sys->h_fbuf.data(), sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
         CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kERec, cudaMemcpyDeviceToHost, s), "D2H energies");
         r = pmgpu_synchronize(sys);
-        if (!(r == PMGPU_ERR_CAPACITY && (sys->plist_need > sys->plist_cap || sys->chunk_need > sys->chunk_cap)))
+        if (!(r == PMGPU_ERR_CAPACITY && (sys->plist_need > sys->plist_cap || sys->chunk_need > sys->chunk_cap ||
+                                          sys->near_need > sys->near_cap)))
             break;
     }
     if (r) return r;
@@ -1439,6 +1461,7 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     CK(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s), "memset");
     PairArgs a;
     fill_pair_args(sys, f, sys->d_pos, a);
+    a.near2 = 0.0f;                                    // recording only: no near-pair list
     a.erec = sys->d_erec;
     a.rec_pairs = d_pairs; a.rec_count = d_count; a.rec_cap = dcap;
     int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)

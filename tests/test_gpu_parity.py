@@ -6,12 +6,15 @@ Tolerances (from the reference-parity requirements of this path):
   * FP64 kernels: forces within 1e-9 of the force RMS, energies / virial
     within 1e-10 relative;
   * mixed precision: relative RMS force error <= 1e-5 (the headline
-    criterion).  Energies and virial are sums of FP32 pair terms: each term
-    carries a few ulp (2^-24) of rounding, so the total carries a random error
-    of about 1e-7 of |E_LJ| + |E_Coulomb| on the 14,281-atom metric system and
-    up to ~1e-6 on small boxes, exact lattices (where equal distances round
-    alike) and PME-only systems (FP32 FFT).  The bound asserted is 5e-7 on the
-    metric system and 2e-6 elsewhere; the FP64 kernels meet 1e-10.
+    criterion).  On the 14,281-atom cutoff + PME metric system the total
+    energy and the virial are within 1e-7 relative of the FP64 oracle: the
+    energies of the pairs closer than 5 A, which carry nearly all of the FP32
+    rounding there, are evaluated in FP64 (measured: 1e-8 energy, 6e-8
+    virial).  Elsewhere the bound is 2e-6 of |E_LJ| + |E_Coulomb|: plain
+    Coulomb gives every pair inside the cutoff an O(1) kcal/mol energy, so
+    its FP32 rounding (a few ulp per pair, 2^-24) is spread over all pairs
+    (1e-7 to 4e-7 measured), and on small PME-only systems the FP32 FFT
+    leaves ~1e-6.  The FP64 kernels meet 1e-10.
 """
 import numpy as np
 import pytest
@@ -25,7 +28,7 @@ pytestmark = pytest.mark.gpu
 
 MIXED_FORCE_RTOL = 1e-5
 MIXED_ENERGY_RTOL = 2e-6           # relative to |E_LJ| + |E_Coulomb|
-MIXED_METRIC_ENERGY_RTOL = 5e-7    # the 14,281-atom cutoff + PME system
+MIXED_METRIC_ENERGY_RTOL = 1e-7    # the 14,281-atom cutoff + PME system, relative to |E_total|
 FP64_FORCE_RTOL = 1e-9
 FP64_ENERGY_RTOL = 1e-10
 
@@ -125,7 +128,9 @@ def test_chain14281_metric_config(chain14281, precision):
         assert abs(etot - rtot) <= FP64_ENERGY_RTOL * scale
     else:
         assert err <= MIXED_FORCE_RTOL
-        assert abs(etot - rtot) <= MIXED_METRIC_ENERGY_RTOL * scale
+        assert abs(etot - rtot) <= MIXED_METRIC_ENERGY_RTOL * abs(rtot)
+        dv = e.virial_tensor - ref["virial"]
+        assert np.linalg.norm(dv) <= MIXED_METRIC_ENERGY_RTOL * np.linalg.norm(ref["virial"])
 
 
 @pytest.mark.parametrize("name", ["water_box_216", "chain_in_water_14281"])
@@ -292,5 +297,9 @@ def test_million_atom_box_at_full_size():
     assert np.isfinite(fm).all() and np.abs(fd).max() > 0
     assert rel_rms(fm, fd) <= MIXED_FORCE_RTOL
     assert np.abs(em.virial_tensor - ed.virial_tensor).max() <= MIXED_ENERGY_RTOL * np.abs(ed.virial_tensor).max() * 10
+    etot, dtot = em.lennard_jones + em.coulomb, ed.lennard_jones + ed.coulomb
+    print(f"\n1M: force rel RMS {rel_rms(fm, fd):.2e}  total energy rel {abs(etot - dtot) / abs(dtot):.2e}  "
+          f"LJ rel {abs(em.lennard_jones - ed.lennard_jones) / abs(ed.lennard_jones):.2e}  virial frob rel "
+          f"{np.linalg.norm(em.virial_tensor - ed.virial_tensor) / np.linalg.norm(ed.virial_tensor):.2e}")
     # the LJ sum has no FP32 FFT in it: within the metric-system bound
     assert abs(em.lennard_jones - ed.lennard_jones) <= MIXED_METRIC_ENERGY_RTOL * abs(ed.lennard_jones)
