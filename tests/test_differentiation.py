@@ -140,3 +140,102 @@ def test_charge_and_lj_gradients_on_the_14281_atom_pme_box(chain14281):
     oxygen = 892 + 3 * 1369                # a water oxygen (waters follow the 892 chain atoms)
     assert chain14281.type_params[chain14281.atom_type[oxygen], 0] > 0
     _check_gradients(chain14281, w.forces, [3, 400, 891, oxygen])
+
+
+# ---------------------------------------------------------------- autograd
+# The forward/backward pair as a torch.autograd.Function, for the test
+# harness only: E(x, q~) forward through pmgpu_evaluate; its backward is -F
+# and dE/dq~ (pmgpu_adjoint).  The position gradient is itself a Function
+# whose backward is the adjoint's Hessian-vector product, so double backward
+# (torch.autograd.functional.vhp; H is symmetric, v^T H = (H v)^T) runs on
+# the GPU kernels as well.
+
+class _Graph:
+    """Topology + forces of one system, rebuilt when the charges change."""
+
+    def __init__(self, s, defs, precision="fp64"):
+        self.s, self.defs, self.precision = s, defs, precision
+        self.key = None
+
+    def forces_for(self, q):
+        key = q.tobytes()
+        if key != self.key:
+            self.topo = F.Topology(dataclasses.replace(self.s, scaled_charge=q.copy()))
+            self.fs = [F.ForceFactory.make(self.topo, d, self.precision) for d in self.defs]
+            self.key = key
+        return self.topo, self.fs
+
+
+def _energy_fn(graph):
+    import torch
+
+    class GradFn(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, x, q):
+            topo, fs = graph.forces_for(q.detach().numpy())
+            out = np.zeros((topo.n_atoms, 3))
+            F.evaluate_group(topo, fs, x.detach().numpy(), out, F.ScalarStructure())
+            ctx.save_for_backward(x, q)
+            return torch.from_numpy(-out)                 # dE/dx = -F
+
+        @staticmethod
+        def backward(ctx, v):
+            x, q = ctx.saved_tensors
+            topo, fs = graph.forces_for(q.detach().numpy())
+            hv = F.adjoint(topo, fs, x.detach().numpy(), v.detach().numpy())["hv"]
+            return torch.from_numpy(hv), None
+
+    class EnergyFn(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, x, q):
+            topo, fs = graph.forces_for(q.detach().numpy())
+            e = F.ScalarStructure()
+            F.evaluate_group(topo, fs, x.detach().numpy(), np.zeros((topo.n_atoms, 3)), e)
+            ctx.save_for_backward(x, q)
+            return torch.tensor(e.potential_energy(), dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, g):
+            x, q = ctx.saved_tensors
+            topo, fs = graph.forces_for(q.detach().numpy())
+            dq = F.adjoint(topo, fs, x.detach().numpy())["dE_dq"]
+            return g * GradFn.apply(x, q), g * torch.from_numpy(dq)
+
+    return EnergyFn.apply
+
+
+def test_autograd_gradients_pass_gradcheck(chain):
+    import torch
+    energy = _energy_fn(_Graph(chain, [FULL]))
+    x = torch.tensor(chain.positions, dtype=torch.float64, requires_grad=True)
+    q = torch.tensor(chain.scaled_charge, dtype=torch.float64, requires_grad=True)
+    # central differences of E against -F and dE/dq~ (step 1e-4 A / 1e-4 e~:
+    # truncation O(h^2) in x, exact in the quadratic q~)
+    assert torch.autograd.gradcheck(energy, (x, q), eps=1e-4, atol=1e-5, rtol=1e-4)
+
+
+def test_autograd_double_backward_is_the_reference_hessian(chain):
+    import torch
+    energy = _energy_fn(_Graph(chain, [FULL]))
+    q = torch.tensor(chain.scaled_charge, dtype=torch.float64)
+    H = oracle.pair_hessian(chain, F.parse_definition(FULL))
+    rng = np.random.default_rng(66)
+    x = torch.tensor(chain.positions, dtype=torch.float64)
+    for _ in range(4):
+        v = rng.normal(size=(chain.n_atoms, 3))
+        v /= np.linalg.norm(v)
+        _, hv = torch.autograd.functional.vhp(lambda xx: energy(xx, q), x, torch.from_numpy(v))
+        assert rel(hv.numpy().reshape(-1), H @ v.reshape(-1)) <= 1e-10
+
+
+def test_autograd_charge_gradient_on_the_14281_atom_pme_box(chain14281):
+    import torch
+    w = workloads.chain14281()
+    energy = _energy_fn(_Graph(chain14281, w.forces, "mixed"))
+    x = torch.tensor(chain14281.positions, dtype=torch.float64)
+    q = torch.tensor(chain14281.scaled_charge, dtype=torch.float64, requires_grad=True)
+    (gq,) = torch.autograd.grad(energy(x, q), q)
+    topo = F.Topology(chain14281)
+    fs = [F.ForceFactory.make(topo, d, "fp64") for d in w.forces]
+    ref = F.adjoint(topo, fs, chain14281.positions)["dE_dq"]
+    assert rel(gq.numpy(), ref) <= 1e-5               # mixed against the FP64 backward pass
