@@ -19,8 +19,8 @@ struct BinArgs {
     CellGrid grid;
     int* cell_lin;              // N
     int* cell3;                 // 3N
-    int* counts;                // ncell (zeroed by the launcher)
-    int* fill;                  // ncell (zeroed by the launcher)
+    int* counts;                // ncell; zero on entry, and again on exit
+    int* done;                  // blocks of k_bin_count finished (zero on entry)
     int* start;                 // ncell + 1
     int* tmp;                   // N
     int* sorted;                // N: original index per sorted slot

@@ -26,7 +26,7 @@ static const double kPi = 3.14159265358979323846;   // Constant::M_PI (base/pmco
 static const double kEpsilon = 1.0e-14;              // Constant::EPSILON (base/pmconstants.cpp:45)
 // status word, list count and need, chunk count and need, work counter, pad,
 // then 11 int64 energy/virial sums
-static const size_t kSmallBytes = 32 + 8 * kERec;
+static const size_t kSmallBytes = 64 + 8 * kERec;
 
 // evaluation phases timed in profiling mode (pmgpu_phase_times)
 enum { kPhaseBin = 0, kPhasePair, kPhaseCorrection, kPhaseSpread, kPhaseFft, kPhaseGather, kPhaseFinalize,
@@ -100,7 +100,6 @@ struct pmgpu_system {
     int* d_cell_lin = nullptr;
     int* d_cell3 = nullptr;
     int* d_counts = nullptr;
-    int* d_fill = nullptr;
     int* d_start = nullptr;
     int* d_cstart = nullptr;
     float4* d_cbox = nullptr;
@@ -265,7 +264,7 @@ extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
     sys->d_chunk_count = sys->d_status + 3;
     sys->d_chunk_need = sys->d_status + 4;
     sys->d_chunk_next = sys->d_status + 5;
-    sys->d_efix = (unsigned long long*)((char*)sys->d_small + 32);
+    sys->d_efix = (unsigned long long*)((char*)sys->d_small + 64);   // ints 8..15: binning
     *out = sys;
     return PMGPU_OK;
 }
@@ -296,7 +295,7 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     if (sys->graph_exec) cudaGraphExecDestroy(sys->graph_exec);
     for (cudaEvent_t e : sys->prof_pool) cudaEventDestroy(e);
     free_atom_buffers(sys);
-    dfree(sys->d_counts); dfree(sys->d_fill); dfree(sys->d_start); dfree(sys->d_erec);
+    dfree(sys->d_counts); dfree(sys->d_start); dfree(sys->d_erec);
     dfree(sys->d_small); dfree(sys->d_energy);
     dfree(sys->d_cstart); dfree(sys->d_cbox); dfree(sys->d_ccell); dfree(sys->d_plist); dfree(sys->d_chunks);
     dfree(sys->d_near);
@@ -530,10 +529,12 @@ extern "C" int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* 
     if (nc > (1ll << 28)) return fail(sys, PMGPU_ERR_ARG, "simulation box / cell size ratio too big");
     g.ncell = (int)nc;
     if (g.ncell > sys->ncell_cap) {
-        CK(dalloc(&sys->d_counts, g.ncell), "alloc"); CK(dalloc(&sys->d_fill, g.ncell), "alloc");
+        CK(dalloc(&sys->d_counts, g.ncell), "alloc");
         CK(dalloc(&sys->d_start, g.ncell + 1), "alloc"); CK(dalloc(&sys->d_cstart, g.ncell + 1), "alloc");
         sys->ncell_cap = g.ncell;
     }
+    // the binning leaves the counts at zero; they start there
+    CK(cudaMemsetAsync(sys->d_counts, 0, sizeof(int) * (size_t)g.ncell, sys->stream), "memset");
     sys->box_set = true;
     sys->box_version++;
     sys->binned = false;
@@ -988,7 +989,7 @@ static int bin(pmgpu_system* sys, const double* d_pos)
     a.ncl_cap = sys->cbox_cap;
     a.n = sys->n; a.pos = d_pos; a.q = sys->d_q; a.type = sys->d_type; a.mol = sys->d_mol;
     a.pbc = sys->pbc; a.grid = sys->grid;
-    a.cell_lin = sys->d_cell_lin; a.cell3 = sys->d_cell3; a.counts = sys->d_counts; a.fill = sys->d_fill;
+    a.cell_lin = sys->d_cell_lin; a.cell3 = sys->d_cell3; a.counts = sys->d_counts; a.done = sys->d_status + 8;
     a.start = sys->d_start; a.tmp = sys->d_tmp; a.sorted = sys->d_sorted; a.slot_of = sys->d_slot;
     a.spos = sys->d_spos; a.slo = sys->d_slo; a.smeta = sys->d_smeta; a.spos64 = sys->d_spos64;
     a.status = sys->d_status;
