@@ -125,6 +125,17 @@ __device__ __forceinline__ int excl_class(const PairArgs& p, int oi, int oj)
 #define PM_HI(x) ((float)(x))
 #define PM_LO(x) ((float)((x) - (double)(float)(x)))
 
+// e^-x for x >= 0 as 2^(-x log2 e) on the hardware base-2 exponential
+// (ex2.approx: relative error ~2^-22); the rounding of the scaled argument
+// adds |x| log2(e) 2^-24 relative, the same order as the rounding of x itself
+__device__ __forceinline__ float exp_neg(float x)
+{
+    float y;
+    const float a = x * -1.4426950408889634f;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
+    return y;
+}
+
 // 1/x: the hardware approximation and one Newton-Raphson step
 // (y' = y + y (1 - x y)), faithful to ~1 ulp for normal x
 __device__ __forceinline__ float rcp_nr(float x)
@@ -173,7 +184,7 @@ __device__ __forceinline__ void pot_f32(const PairArgs& p, const TermF& t, float
         qq = (p.csfd != 1.0 && excl == PMGPU_EXCL_MODIFIED) ? qq * p.csf : qq;
         float r = r2 * rinv;
         float ar = fmaf(t.alpha, r, t.alpha_lo * r);     // compensated alpha
-        float ex = qq * expf(-ar * ar);
+        float ex = qq * exp_neg(ar * ar);
         e = poly5f(ar) * ex * rinv;
         f = fmaf(t.two_alpha_pi, ex, fmaf(t.two_alpha_pi_lo, ex, e)) * rinv * rinv;
     } else {

@@ -2,9 +2,9 @@
 // (included by pm_pair.cu, which provides the helpers).
 //
 // Clusters: inside a reference cell the atoms are ordered by the Morton key of
-// their position on an 8x8x8 sub-grid of the cell (k_bin_finish), so every run
-// of 8 consecutive atoms is a compact cluster with a bounding box
-// (k_cluster_box).  Up to four consecutive clusters of a cell form an
+// their position on an 8x8x8 sub-grid of the cell (k_bin_cells), so every run
+// of 8 consecutive atoms is a compact cluster with a bounding box (also
+// k_bin_cells).  Up to four consecutive clusters of a cell form an
 // i-supercluster (32 atoms).
 //
 // K2a k_cluster_list: one warp per cell and block of 32 half-shell cells.
