@@ -260,6 +260,37 @@ int pmgpu_batch_synchronize(pmgpu_batch* batch);
 int pmgpu_batch_last_error(pmgpu_batch* batch, char* buf, int len);
 void* pmgpu_batch_stream(pmgpu_batch* batch);
 
+/* ---- launch tuning -----------------------------------------------------
+ * No counterpart in the reference (its CPU loops have nothing to tune).  The
+ * launch shapes of a system's evaluation: the cluster-pair list's work
+ * chunks, the mixed pair kernel's resident blocks, the PME FFT's lines per
+ * block, and whether PME runs on a second stream beside the pair kernels.
+ * Results do not depend on them beyond the last bits of the fixed-point
+ * grouping (a chunk's partial sums are rounded together).  Defaults: 16, 0
+ * (the occupancy limit), 16, 1. */
+typedef struct pmgpu_tuning {
+    int chunk_entries;        /* cluster-list entries per chunk of pair work: 4..64 */
+    int pair_blocks_per_sm;   /* resident blocks of the mixed pair kernel per SM: 0 (occupancy limit) or 1..8 */
+    int fft_lines;            /* lines per block of the strided PME FFT passes, at most: 1..16 */
+    int pme_concurrent;       /* 1: PME on a second stream beside the pair kernels; 0: after them */
+    double ms_per_eval;       /* pmgpu_autotune: the measured time of the chosen tuning */
+} pmgpu_tuning;
+int pmgpu_get_tuning(pmgpu_system* sys, pmgpu_tuning* out);
+/* PMGPU_ERR_ARG for a value out of range; the next evaluation is recaptured. */
+int pmgpu_set_tuning(pmgpu_system* sys, const pmgpu_tuning* tuning);
+/* Project-written autotuner: times candidate tunings on these forces and
+ * these positions (host, N x 3), evals evaluations each after two warm-up
+ * ones, with CUDA events on the system's stream; a coordinate search over
+ * the four parameters, two sweeps.  Keeps the fastest for the system's later
+ * evaluations and returns it (with its time) in *best.  Synchronous; uses
+ * the system's own scratch buffers (no caller output is touched). */
+int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,
+                   unsigned flags, int evals, pmgpu_tuning* best);
+/* The same search for a batch: each candidate is applied to every member and
+ * timed as whole batch launches.  The members' output buffers receive the
+ * timed evaluations (zero them before the next real one). */
+int pmgpu_batch_autotune(pmgpu_batch* batch, int evals, pmgpu_tuning* best);
+
 /* ---- diagnostics (parity tests) ----------------------------------------- */
 
 /* Cell of every atom from the GPU binning of the last evaluation, as

@@ -28,7 +28,7 @@ EXPORTS = [
     "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
     "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
-    "pmgpu_full_create",
+    "pmgpu_full_create", "pmgpu_get_tuning", "pmgpu_set_tuning", "pmgpu_autotune", "pmgpu_batch_autotune",
 ]
 PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
 
@@ -47,6 +47,14 @@ class PmeParams(C.Structure):
         ("grid", C.c_int * 3), ("order", C.c_int), ("cutoff", C.c_double),
         ("accuracy", C.c_double), ("alpha", C.c_double), ("precision", C.c_int),
     ]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("chunk_entries", C.c_int), ("pair_blocks_per_sm", C.c_int), ("fft_lines", C.c_int),
+                ("pme_concurrent", C.c_int), ("ms_per_eval", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Energies(C.Structure):
@@ -104,6 +112,10 @@ def load():
     lib.pmgpu_batch_stream.restype = vp
     lib.pmgpu_adjoint.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]
     lib.pmgpu_full_create.argtypes = [vp, C.POINTER(CutoffParams), C.POINTER(vp)]
+    lib.pmgpu_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+    lib.pmgpu_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+    lib.pmgpu_autotune.argtypes = [vp, C.c_int, C.POINTER(vp), vp, C.c_uint, C.c_int, C.POINTER(Tuning)]
+    lib.pmgpu_batch_autotune.argtypes = [vp, C.c_int, C.POINTER(Tuning)]
     _lib = lib
     return lib
 

@@ -83,6 +83,14 @@ class Batch:
     def evaluate(self):
         self._check(self.lib.pmgpu_batch_evaluate(self.handle))
 
+    def autotune(self, evals: int = 5) -> dict:
+        """pmgpu_batch_autotune: one tuning for every member, timed as whole
+        batch launches; the members' outputs are zeroed afterwards."""
+        t = _lib.Tuning()
+        self._check(self.lib.pmgpu_batch_autotune(self.handle, int(evals), C.byref(t)))
+        self.zero()
+        return t.as_dict()
+
     def synchronize(self):
         self._check(self.lib.pmgpu_batch_synchronize(self.handle))
 

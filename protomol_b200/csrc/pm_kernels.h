@@ -141,7 +141,8 @@ struct PairArgs {
     int* chunk_next;             // work counter of the pair kernel
     const double4* hoff64;       // FP64 half-shell offsets (hi + lo), virial
     unsigned long long* efix;    // 11 int64 sums (scale 2^32): LJ, Coulomb, virial
-    int reserve;                 // block slots per SM left free for concurrent PME kernels
+    int blocks_per_sm;           // resident blocks of the mixed pair kernel per SM (0: the occupancy limit)
+    int chunk;                   // cluster-list entries per chunk of pair work
 };
 
 // Combination id of the registered OneAtomPair[Two] templates.
@@ -156,7 +157,7 @@ int pair_blocks(const CellGrid& g, int nd);
 // blocks of the mixed kernel (4 warps, one energy record per warp)
 // estimated cluster-pair list entries and chunks of a system
 long long plist_estimate(int n_atoms, const CellGrid& g, int nh);
-long long chunk_estimate(int n_atoms, const CellGrid& g, int nh);
+long long chunk_estimate(int n_atoms, const CellGrid& g, int nh, int chunk);
 
 // ---------------------------------------------------------------- adjoint
 // K10: gradients of the pair energy w.r.t. charges and the LJ table, and the
@@ -227,6 +228,7 @@ struct PmeArgs {
     int erec_stride;
     int* status;
     int virial;
+    int fft_lines;               // lines per CTA of the strided FFT passes, at most (0: 16)
 };
 constexpr int kStageSpread = 0, kStageFft = 1, kStageGather = 2;
 constexpr int kStagePotential = 3;   // dE/dq~ = phi at the atoms, into (double*)facc

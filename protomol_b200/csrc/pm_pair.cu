@@ -417,9 +417,9 @@ long long plist_estimate(int n_atoms, const CellGrid& g, int nh)
     return (long long)(1.5 * supers * (nh + 1) * per_cell) + 4096;
 }
 
-long long chunk_estimate(int n_atoms, const CellGrid& g, int nh)
+long long chunk_estimate(int n_atoms, const CellGrid& g, int nh, int chunk)
 {
-    return plist_estimate(n_atoms, g, nh) / kChunk + (long long)n_atoms / (kCluster * kSuper) + g.ncell + 1024;
+    return plist_estimate(n_atoms, g, nh) / chunk + (long long)n_atoms / (kCluster * kSuper) + g.ncell + 1024;
 }
 
 int pair_blocks(const CellGrid& g, int nd)
@@ -468,8 +468,10 @@ static int run_mixed_w(const PairArgs& a, cudaStream_t s, long long* launches)
         if (sms <= 0) sms = 148;
         if (per_sm <= 0) per_sm = 1;
     }
-    // with PME kernels running beside it, leave them block slots
-    const int blocks = sms * (per_sm > a.reserve ? per_sm - a.reserve : 1);
+    // a tuned number of resident blocks per SM (fewer leave room for the PME
+    // kernels running beside it), else the occupancy limit
+    const int bps = a.blocks_per_sm > 0 ? std::min(per_sm, a.blocks_per_sm) : per_sm;
+    const int blocks = sms * bps;
     k_pair_mixed<NT, P0, S0, P1, S1, WRAP><<<blocks, 128, 0, s>>>(a);
     *launches += 1;
     return (int)cudaGetLastError();

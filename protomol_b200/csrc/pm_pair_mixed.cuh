@@ -16,7 +16,7 @@
 // the reference's list with its B > A rule) -- whose bounding box comes within
 // the cutoff (plus the FP32 guard band) of at least one of the supercluster's
 // cluster boxes, with a 4-bit mask of those i-clusters.  A warp's entries of
-// a supercluster are contiguous and cut into chunks of kChunk entries.  The
+// a supercluster are contiguous and cut into chunks of p.chunk entries.  The
 // interacting pair set is the reference's: only the order in which a pair's
 // two atoms are visited differs, and forces are accumulated in
 // order-independent fixed point.
@@ -54,7 +54,6 @@
 
 constexpr float kFarAway = 1.0e4f;   // position of the padding lanes of partial clusters
 constexpr int kSuper = 4;            // clusters per i-supercluster
-constexpr int kChunk = 16;           // list entries per chunk of work
 constexpr int kNearCap = 512;        // near pairs a warp queues for FP64 energies
 
 // ---------------------------------------------------------------- K2a: list
@@ -155,7 +154,7 @@ __global__ void __launch_bounds__(128) k_cluster_list(PairArgs p)
         }
         const int ne = __shfl_sync(FULL, incl, 31);
         if (ne == 0) continue;
-        const int nch = (ne + kChunk - 1) / kChunk;
+        const int nch = (ne + p.chunk - 1) / p.chunk;
         int b0 = 0, b1 = 0;
         if (lane == 0) {
             b0 = atomicAdd(p.plist_count, ne);
@@ -177,7 +176,7 @@ __global__ void __launch_bounds__(128) k_cluster_list(PairArgs p)
         // chunk descriptors: {first i slot, i atoms, first entry, entries}
         for (int t = lane; t < nch; t += 32)
             if (cbase + t < p.chunk_cap && ebase + ne <= p.plist_cap)
-                p.chunks[cbase + t] = make_int4(ifirst, nit, ebase + t * kChunk, min(kChunk, ne - t * kChunk));
+                p.chunks[cbase + t] = make_int4(ifirst, nit, ebase + t * p.chunk, min(p.chunk, ne - t * p.chunk));
     }
 }
 

@@ -22,6 +22,8 @@
 // Mixed precision: the charge grid is accumulated in int64 fixed point
 // (deterministic), the FFT and gather run in FP32.  FP64: double grid with
 // FP64 atomics, FP64 FFT and gather.
+#include <algorithm>
+
 #include "pm_kernels.h"
 #include "../../include/pmgpu.h"
 
@@ -459,9 +461,10 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     }
     // lines per CTA for the strided passes: 16 (128 B coalesced rows for
     // float2) unless two line buffers would exceed ~200 KB of shared memory
-    auto tile_for = [](int n) {
+    const int max_lines = a.fft_lines > 0 ? std::min(a.fft_lines, 16) : 16;
+    auto tile_for = [max_lines](int n) {
         int t = (200 * 1024) / (2 * (n + 1) * (int)sizeof(C));
-        return t < 1 ? 1 : (t > 16 ? 16 : t);
+        return t < 1 ? 1 : (t > max_lines ? max_lines : t);
     };
     int tile = tile_for(a.ky);
     // y forward

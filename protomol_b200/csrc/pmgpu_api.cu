@@ -141,6 +141,7 @@ struct pmgpu_system {
     std::set<pmgpu_force*> forces;     // live forces made on this system
     int topo_version = 0;
     int buf_version = 0;               // bumped when a per-evaluation buffer moves
+    pmgpu_tuning tuning = {16, 0, 16, 1, 0.0};   // launch shapes (pmgpu_set_tuning, pmgpu_autotune)
     // CUDA graph of the last evaluation (replayed when the key matches)
     bool use_graphs = true;
     cudaGraphExec_t graph_exec = nullptr;
@@ -1013,6 +1014,7 @@ static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_po
     a.plist = sys->d_plist; a.plist_cap = (int)sys->plist_cap;
     a.chunks = sys->d_chunks; a.chunk_cap = (int)sys->chunk_cap;
     a.near = sys->d_near; a.near_cap = (int)sys->near_cap;
+    a.chunk = sys->tuning.chunk_entries; a.blocks_per_sm = sys->tuning.pair_blocks_per_sm;
     a.near_count = sys->d_status + 6; a.near_need = sys->d_status + 7;
     a.plist_count = sys->d_plist_count; a.plist_need = sys->d_plist_need;
     a.chunk_count = sys->d_chunk_count; a.chunk_need = sys->d_chunk_need; a.chunk_next = sys->d_chunk_next;
@@ -1094,7 +1096,7 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
     for (int k = 0; k < nf; ++k)
         if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) {
             lneed = std::max(lneed, plist_estimate(sys->n, sys->grid, forces[k]->nh));
-            cneed = std::max(cneed, chunk_estimate(sys->n, sys->grid, forces[k]->nh));
+            cneed = std::max(cneed, chunk_estimate(sys->n, sys->grid, forces[k]->nh, sys->tuning.chunk_entries));
         }
     if (lneed > 0) {
         lneed = std::max(lneed, sys->plist_need + sys->plist_need / 4);
@@ -1219,7 +1221,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 a.fac = kPi * kPi / (f->alpha * f->alpha);
                 a.wr = 1.0 / LX; a.lr = 1.0 / LY; a.hr = 1.0 / LZ;
                 a.facc = facc; a.scale = scale; a.qscale = kScaleFp64; a.erec_stride = sys->erec_cap;
-                a.status = sys->d_status; a.virial = virial;
+                a.status = sys->d_status; a.virial = virial; a.fft_lines = sys->tuning.fft_lines;
                 const int phases[3] = {kPhaseSpread, kPhaseFft, kPhaseGather};
                 const int stages[3] = {kStageSpread, kStageFft, kStageGather};
                 for (int st = 0; st < 3; ++st) {
@@ -1238,7 +1240,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     // with cutoff forces too, PME runs on the side stream from the start,
     // beside binning, the list and the pair kernels, and is joined before
     // finalize (not while profiling, which times every phase alone)
-    const bool fork = any_cut && any_pme && !sys->profiling;
+    const bool fork = any_cut && any_pme && !sys->profiling && sys->tuning.pme_concurrent;
     if (fork) {
         CK(cudaEventRecord(sys->ev_fork, s), "fork");
         CK(cudaStreamWaitEvent(sys->side, sys->ev_fork, 0), "fork");
@@ -1289,7 +1291,6 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
             prof_end(sys, ml);
         }
         int m = prof_begin(sys, kPhasePair);
-        a.reserve = 0;
         int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
                      : launch_pair_mixed(a, f->combo, s, &sys->launches);
         if (!e && !fp64 && a.near2 > 0.0f) e = launch_near_energy(a, f->combo, sys->n, s, &sys->launches);
@@ -1804,6 +1805,182 @@ extern "C" int pmgpu_batch_last_error(pmgpu_batch* b, char* buf, int len)
 }
 
 extern "C" void* pmgpu_batch_stream(pmgpu_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+// ------------------------------------------------------------------ tuning
+static bool tuning_valid(const pmgpu_tuning& t)
+{
+    return t.chunk_entries >= 4 && t.chunk_entries <= 64 && t.pair_blocks_per_sm >= 0 &&
+           t.pair_blocks_per_sm <= 8 && t.fft_lines >= 1 && t.fft_lines <= 16 &&
+           (t.pme_concurrent == 0 || t.pme_concurrent == 1);
+}
+
+static void apply_tuning(pmgpu_system* sys, const pmgpu_tuning& t)
+{
+    sys->tuning = t;
+    sys->buf_version++;                  // the captured graph holds the old launch shapes
+}
+
+extern "C" int pmgpu_get_tuning(pmgpu_system* sys, pmgpu_tuning* out)
+{
+    if (!sys || !out) return PMGPU_ERR_ARG;
+    *out = sys->tuning;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_set_tuning(pmgpu_system* sys, const pmgpu_tuning* t)
+{
+    if (!sys || !t) return PMGPU_ERR_ARG;
+    if (!tuning_valid(*t)) return fail(sys, PMGPU_ERR_ARG, "tuning value out of range");
+    apply_tuning(sys, *t);
+    return PMGPU_OK;
+}
+
+// coordinate search over the four launch parameters: each is tried at its
+// candidate values with the others at the best so far, two sweeps; time(t)
+// measures one candidate in ms per evaluation
+template <class TimeFn>
+static int tune_search(pmgpu_tuning start, bool has_pme, bool has_pairs, TimeFn time, pmgpu_tuning* best)
+{
+    double best_ms = 0.0;
+    int r = time(start, &best_ms);
+    if (r) return r;
+    pmgpu_tuning b = start;
+    const int chunks[3] = {8, 16, 32}, bps[3] = {0, 3, 2}, lines[3] = {16, 8, 4}, conc[2] = {1, 0};
+    for (int sweep = 0; sweep < 2; ++sweep) {
+        for (int param = 0; param < 4; ++param) {
+            if ((param == 0 || param == 1) && !has_pairs) continue;
+            if ((param == 2 || param == 3) && !has_pme) continue;
+            if (param == 3 && !has_pairs) continue;
+            const int nv = param == 3 ? 2 : 3;
+            for (int v = 0; v < nv; ++v) {
+                pmgpu_tuning t = b;
+                int* slot = param == 0 ? &t.chunk_entries : param == 1 ? &t.pair_blocks_per_sm
+                          : param == 2 ? &t.fft_lines : &t.pme_concurrent;
+                const int val = param == 0 ? chunks[v] : param == 1 ? bps[v] : param == 2 ? lines[v] : conc[v];
+                if (*slot == val) continue;
+                *slot = val;
+                double ms = 0.0;
+                r = time(t, &ms);
+                if (r) return r;
+                if (ms < best_ms) { best_ms = ms; b = t; }
+            }
+        }
+    }
+    b.ms_per_eval = best_ms;
+    *best = b;
+    return PMGPU_OK;
+}
+
+static void force_kinds(int nf, pmgpu_force* const* forces, bool& has_pme, bool& has_pairs)
+{
+    has_pme = has_pairs = false;
+    for (int k = 0; k < nf; ++k) {
+        if (forces[k]->kind == 1 && forces[k]->pp.reciprocal) has_pme = true;
+        if ((forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) ||
+            (forces[k]->kind == 1 && forces[k]->real_sub))
+            has_pairs = true;
+    }
+}
+
+extern "C" int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,
+                              unsigned flags, int evals, pmgpu_tuning* best)
+{
+    if (!sys || n_forces <= 0 || !forces || !positions || evals < 1 || !best) return PMGPU_ERR_ARG;
+    if (sys->profiling) return fail(sys, PMGPU_ERR_STATE, "autotune in profiling mode");
+    cudaSetDevice(sys->device);
+    int r = eval_prepare(sys, n_forces, forces);
+    if (r) return r;
+    cudaStream_t s = sys->stream;
+    const size_t n3 = 3 * (size_t)sys->n;
+    CK(cudaMemcpyAsync(sys->d_pos, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, s), "H2D positions");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0), "event");
+    if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return cuda_fail(sys, cudaErrorUnknown, "event"); }
+    auto time = [&](const pmgpu_tuning& t, double* ms) -> int {
+        apply_tuning(sys, t);
+        // two warm-up evaluations; a second round when they outgrew a list
+        // (the chunk count depends on the tuning; eval_core grows it)
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            int q = PMGPU_OK;
+            for (int w = 0; w < 2 && q == PMGPU_OK; ++w)
+                q = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy, flags);
+            if (q) return q;
+            q = pmgpu_synchronize(sys);
+            if (q == PMGPU_OK) break;
+            if (q != PMGPU_ERR_CAPACITY || attempt == 1) return q;
+        }
+        cudaEventRecord(e0, s);
+        for (int k = 0; k < evals; ++k) {
+            int q = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy, flags);
+            if (q) return q;
+        }
+        cudaEventRecord(e1, s);
+        int q = pmgpu_synchronize(sys);
+        if (q) return q;
+        float el = 0.f;
+        cudaEventElapsedTime(&el, e0, e1);
+        *ms = el / evals;
+        return PMGPU_OK;
+    };
+    bool has_pme = false, has_pairs = false;
+    force_kinds(n_forces, forces, has_pme, has_pairs);
+    pmgpu_tuning b;
+    r = tune_search(sys->tuning, has_pme, has_pairs, time, &b);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (r) return r;
+    apply_tuning(sys, b);
+    *best = b;
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_batch_autotune(pmgpu_batch* b, int evals, pmgpu_tuning* best)
+{
+    if (!b || evals < 1 || !best) return PMGPU_ERR_ARG;
+    if (b->members.empty()) return batch_fail(b, PMGPU_ERR_STATE, "empty batch");
+    cudaSetDevice(b->device);
+    bool has_pme = false, has_pairs = false;
+    for (auto& m : b->members) {
+        bool p1 = false, p2 = false;
+        force_kinds((int)m.forces.size(), m.forces.data(), p1, p2);
+        has_pme = has_pme || p1;
+        has_pairs = has_pairs || p2;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess) return batch_fail(b, PMGPU_ERR_CUDA, "event");
+    if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return batch_fail(b, PMGPU_ERR_CUDA, "event"); }
+    auto time = [&](const pmgpu_tuning& t, double* ms) -> int {
+        for (auto& m : b->members) apply_tuning(m.sys, t);
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            int q = PMGPU_OK;
+            for (int w = 0; w < 2 && q == PMGPU_OK; ++w) q = pmgpu_batch_evaluate(b);
+            if (q) return q;
+            q = pmgpu_batch_synchronize(b);
+            if (q == PMGPU_OK) break;
+            if (q != PMGPU_ERR_CAPACITY || attempt == 1) return q;
+        }
+        cudaEventRecord(e0, b->stream);
+        for (int k = 0; k < evals; ++k) {
+            int q = pmgpu_batch_evaluate(b);
+            if (q) return q;
+        }
+        cudaEventRecord(e1, b->stream);
+        int q = pmgpu_batch_synchronize(b);
+        if (q) return q;
+        float el = 0.f;
+        cudaEventElapsedTime(&el, e0, e1);
+        *ms = el / evals;
+        return PMGPU_OK;
+    };
+    pmgpu_tuning t;
+    int r = tune_search(b->members[0].sys->tuning, has_pme, has_pairs, time, &t);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (r) return r;
+    for (auto& m : b->members) apply_tuning(m.sys, t);
+    *best = t;
+    return PMGPU_OK;
+}
 
 // ------------------------------------------------------------------ adjoint
 static void adj_pme_args(pmgpu_system* sys, pmgpu_force* f, PmeArgs& a)

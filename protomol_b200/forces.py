@@ -93,6 +93,33 @@ class Topology:
     def launch_count(self) -> int:
         return int(_lib.load().pmgpu_launch_count(self.handle))
 
+    @property
+    def tuning(self) -> dict:
+        """The launch shapes of this system's evaluations (pmgpu_get_tuning)."""
+        t = _lib.Tuning()
+        check(_lib.load().pmgpu_get_tuning(self.handle, C.byref(t)), self.handle)
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        """pmgpu_set_tuning with the given fields changed."""
+        t = _lib.Tuning()
+        lib = _lib.load()
+        check(lib.pmgpu_get_tuning(self.handle, C.byref(t)), self.handle)
+        for k, v in kw.items():
+            setattr(t, k, v)
+        check(lib.pmgpu_set_tuning(self.handle, C.byref(t)), self.handle)
+
+    def autotune(self, forces, positions, evals: int = 5, virial: bool = True) -> dict:
+        """pmgpu_autotune: times candidate launch shapes on these forces and
+        positions and keeps the fastest; returns it with its ms per evaluation."""
+        lib = _lib.load()
+        pos = np.ascontiguousarray(positions, np.float64)
+        arr = (_VP * len(forces))(*[f.handle for f in forces])
+        t = _lib.Tuning()
+        check(lib.pmgpu_autotune(self.handle, len(forces), arr, pos.ctypes.data_as(_VP),
+                                 _lib.FLAG_VIRIAL if virial else 0, int(evals), C.byref(t)), self.handle)
+        return t.as_dict()
+
     def cells(self):
         cells = np.zeros((self.n_atoms, 3), np.int32)
         dims = np.zeros(3, np.int32)
