@@ -328,6 +328,7 @@ def main():
         extra["batched"] = measure_batched(local, rank, world, pg, torch, flush, max(20, min(args.steps // 10, 200)))
         if rank == 0:
             extra["scale_1m"] = measure_1m(local, torch, 10)
+            extra["leapfrog"] = measure_leapfrog(local, torch)
     if rank == 0:
         value = world * 1000.0 / t_local
         line = {
@@ -430,6 +431,37 @@ def measure_batched(local, rank, world, pg, torch, flush, steps):
             "speedup_vs_one_at_a_time": t_seq / t_batch, "tuning": tuning,
             "timing": "CUDA events on the batch stream (batched, L2 flushed between steps); "
                       "wall clock for one at a time (each box synchronized)"}
+
+
+def measure_leapfrog(local, torch, steps=1000):
+    """GPU-resident Leapfrog (pmgpu_leapfrog_run): one force evaluation plus
+    ``steps`` steps of 1 fs on the 216-oxygen LJ fluid (cutoff 9, C2 8 -> 9),
+    positions, velocities and forces staying in HBM; CUDA events around the
+    run on the system's stream."""
+    from protomol_b200 import forces as F
+    from protomol_b200 import integrate, workloads
+    w = workloads.lj_fluid216()
+    s = w.system
+    v = integrate.maxwell_boltzmann(s.mass, 300.0, seed=216)
+    out = {"workload": "216-oxygen LJ fluid (the 648-atom water box without hydrogens), cutoff 9 C2 8->9, "
+                       "1 fs steps", "atoms": s.n_atoms, "steps": steps}
+    for prec in ("fp64", "mixed"):
+        topo = F.Topology(s, device=local)
+        fs = [F.ForceFactory.make(topo, d, prec) for d in w.forces]
+        lf = integrate.Leapfrog(topo, fs, s.positions, v, s.mass, 1.0, device=local).initialize()
+        lf.run(20)                                       # warm-up (graph capture)
+        lf.synchronize()
+        stream = torch.cuda.ExternalStream(topo.stream)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        lf.run(steps)
+        b.record(stream)
+        lf.synchronize()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        out[prec] = {"ms_per_step": ms / steps, "steps_per_s": steps * 1000.0 / ms}
+        topo.close()
+    return out
 
 
 def measure_1m(local, torch, steps):

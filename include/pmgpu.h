@@ -291,6 +291,25 @@ int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, 
  * timed evaluations (zero them before the next real one). */
 int pmgpu_batch_autotune(pmgpu_batch* batch, int evals, pmgpu_tuning* best);
 
+/* ---- integration ---------------------------------------------------------
+ * LeapfrogIntegrator::run(n_steps) (integrators/LeapfrogIntegrator.cpp:
+ * 107-120; doHalfKickdoDrift :47-68, doKickdoDrift :70-101, doHalfKick
+ * StandardIntegrator.cpp:83-96) without modifiers, on device buffers that
+ * stay in HBM: per step one kick/drift kernel and one evaluation of the
+ * forces (the captured graph), with no host round trip.  d_forces must hold
+ * the forces at d_positions on entry (the integrator's forces after
+ * initialize(), or after the previous run); on return d_positions and
+ * d_velocities are advanced by n_steps * timestep (fs), d_forces and
+ * d_energies (11, cleared per evaluation like calculateForces) belong to the
+ * final positions.  d_mass: N atom masses (amu, atoms[i].scaledMass).
+ * Asynchronous on the system's stream; failures of the evaluations
+ * (PMGPU_ERR_CAPACITY: a list outgrew its size, grown for the next run)
+ * surface at pmgpu_synchronize, and the run is then to be repeated from its
+ * starting state. */
+int pmgpu_leapfrog_run(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* d_mass,
+                       double* d_positions, double* d_velocities, double* d_forces, double* d_energies,
+                       double timestep, int n_steps, unsigned flags);
+
 /* ---- diagnostics (parity tests) ----------------------------------------- */
 
 /* Cell of every atom from the GPU binning of the last evaluation, as

@@ -325,3 +325,41 @@ def run_reference(system, specs, repeat: int = 1, fast: bool = False, timeout=No
         "virial": hdr[2:11].copy(), "seconds_per_eval": float(hdr[11]),
         "cells": cells, "dims": dims,
     }
+
+
+# ---------------------------------------------------------------- integration
+INV_TIMEFACTOR = 0.02045482828087295          # Constant::INV_TIMEFACTOR (base/pmconstants.cpp:49)
+
+
+def leapfrog(system, specs, velocities, timestep, steps, positions=None, forces=None):
+    """LeapfrogIntegrator::run(steps) without modifiers
+    (integrators/LeapfrogIntegrator.cpp:107-120) on the oracle's forces, in the
+    reference's operation order:
+
+    * doHalfKickdoDrift (:47-68): v += F h 0.5 / m, x += v h, h = dt / T;
+    * doKickdoDrift (:70-101) for the later steps: v += F h / m, x += v h;
+    * calculateForces after every drift;
+    * doHalfKick (StandardIntegrator.cpp:83-96) at the end: v += F h' / m,
+      h' = 0.5 dt / T.
+
+    numpy multiplies and adds without fusing them, as the reference's build
+    without FMA contraction does.  ``forces`` are the forces at the starting
+    positions (evaluated here when not given).  Returns (positions,
+    velocities, forces, result of the last evaluation)."""
+    x = np.array(system.positions if positions is None else positions, np.float64)
+    v = np.array(velocities, np.float64)
+    m = np.asarray(system.mass, np.float64)[:, None]
+    r = None
+    f = np.array(forces, np.float64) if forces is not None else evaluate(system, specs, positions=x)["forces"]
+    h = timestep * INV_TIMEFACTOR
+    for step in range(steps):
+        if step == 0:
+            v = v + ((f * h) * 0.5) / m
+        else:
+            v = v + (f * h) / m
+        x = x + v * h
+        r = evaluate(system, specs, positions=x)
+        f = r["forces"]
+    hk = 0.5 * timestep * INV_TIMEFACTOR
+    v = v + (f * hk) / m
+    return x, v, f, r

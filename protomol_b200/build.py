@@ -18,7 +18,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpmgpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["pm_cells.cu", "pm_pair.cu", "pm_pme.cu", "pm_adjoint.cu", "pmgpu_api.cu"]
+SOURCES = ["pm_cells.cu", "pm_pair.cu", "pm_pme.cu", "pm_adjoint.cu", "pm_integrate.cu", "pmgpu_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I" + CSRC, "-I" + INCLUDE]

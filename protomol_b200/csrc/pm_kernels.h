@@ -283,4 +283,10 @@ int launch_finalize(const FinArgs& a, cudaStream_t s, long long* launches, int* 
 int launch_energy_reduce(const double* erec, int stride, int nrec, const unsigned long long* efix,
                          double* out, cudaStream_t s, long long* launches);
 
+// Leapfrog kick / drift (LeapfrogIntegrator.cpp): the first step's half kick
+// and drift, a middle step's kick and drift, the last half kick
+constexpr int kLeapfrogFirst = 0, kLeapfrogMiddle = 1, kLeapfrogLast = 2;
+int launch_leapfrog(int n, const double* mass, double* pos, double* vel, const double* force, double h, double hk,
+                    int mode, cudaStream_t s, long long* launches);
+
 }  // namespace pm

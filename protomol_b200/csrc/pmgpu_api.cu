@@ -1982,6 +1982,38 @@ extern "C" int pmgpu_batch_autotune(pmgpu_batch* b, int evals, pmgpu_tuning* bes
     return PMGPU_OK;
 }
 
+// ------------------------------------------------------------------ leapfrog
+static const double kInvTimeFactor = 0.02045482828087295;   // Constant::INV_TIMEFACTOR (base/pmconstants.cpp:49)
+
+extern "C" int pmgpu_leapfrog_run(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* d_mass,
+                                  double* d_positions, double* d_velocities, double* d_forces, double* d_energies,
+                                  double timestep, int n_steps, unsigned flags)
+{
+    if (!sys || n_forces <= 0 || !forces || !d_mass || !d_positions || !d_velocities || !d_forces || !d_energies)
+        return PMGPU_ERR_ARG;
+    if (!(timestep > 0.0) || n_steps < 0) return fail(sys, PMGPU_ERR_ARG, "timestep must be positive, steps >= 0");
+    if (n_steps == 0) return PMGPU_OK;
+    cudaSetDevice(sys->device);
+    cudaStream_t s = sys->stream;
+    const size_t n3 = 3 * (size_t)sys->n;
+    const double h = timestep * kInvTimeFactor;              // getTimestep() * Constant::INV_TIMEFACTOR
+    const double hk = 0.5 * timestep * kInvTimeFactor;       // doHalfKick's step
+    for (int step = 0; step < n_steps; ++step) {
+        int e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_forces, h, h,
+                                step == 0 ? kLeapfrogFirst : kLeapfrogMiddle, s, &sys->launches);
+        if (e) return cuda_fail(sys, (cudaError_t)e, "leapfrog step");
+        // calculateForces: forces and energies cleared, then evaluated
+        CK(cudaMemsetAsync(d_forces, 0, sizeof(double) * n3, s), "memset");
+        CK(cudaMemsetAsync(d_energies, 0, sizeof(double) * kERec, s), "memset");
+        int r = eval_core(sys, n_forces, forces, d_positions, d_forces, d_energies, flags);
+        if (r) return r;
+    }
+    int e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_forces, h, hk, kLeapfrogLast, s,
+                            &sys->launches);
+    if (e) return cuda_fail(sys, (cudaError_t)e, "leapfrog half kick");
+    return PMGPU_OK;
+}
+
 // ------------------------------------------------------------------ adjoint
 static void adj_pme_args(pmgpu_system* sys, pmgpu_force* f, PmeArgs& a)
 {

@@ -1,0 +1,82 @@
+"""The Leapfrog integrator on the GPU force path, with positions, velocities
+and forces resident in device memory (pmgpu_leapfrog_run).
+
+Mirrors LeapfrogIntegrator (integrators/LeapfrogIntegrator.cpp): ``initialize``
+evaluates the forces at the starting positions (initializeForces), ``run(n)``
+advances n steps of ``timestep`` fs with one force evaluation per step and
+ends with a half kick, so the velocities are synchronous with the positions.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from . import forces as F
+
+_VP = C.c_void_p
+BOLTZMANN = 0.001987191         # kcal / mol / K (Constant::BOLTZMANN, base/pmconstants.cpp)
+
+
+def maxwell_boltzmann(masses: np.ndarray, temperature: float, seed: int) -> np.ndarray:
+    """Seeded velocities of a temperature (N x 3, A per internal time unit):
+    each component N(0, kT / m), the net momentum removed."""
+    m = np.asarray(masses, np.float64)
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(len(m), 3)) * np.sqrt(BOLTZMANN * temperature / m)[:, None]
+    v -= (m[:, None] * v).sum(0) / m.sum()
+    return v
+
+
+def kinetic_energy(masses: np.ndarray, velocities: np.ndarray) -> float:
+    """0.5 sum m v^2 (kcal/mol), as topologyutilities' kineticEnergy."""
+    return float(0.5 * (np.asarray(masses)[:, None] * np.asarray(velocities) ** 2).sum())
+
+
+class Leapfrog:
+    def __init__(self, topo: F.Topology, forces: Sequence[F.SystemForce], positions, velocities, masses,
+                 timestep: float, device: int = 0, virial: bool = False):
+        import torch
+        self.topo, self.forces, self.timestep = topo, list(forces), float(timestep)
+        self.flags = _lib.FLAG_VIRIAL if virial else 0
+        dev = torch.device(f"cuda:{device}")
+        self.pos = torch.tensor(np.ascontiguousarray(positions, np.float64), device=dev)
+        self.vel = torch.tensor(np.ascontiguousarray(velocities, np.float64), device=dev)
+        self.mass = torch.tensor(np.ascontiguousarray(masses, np.float64), device=dev)
+        self.force = torch.zeros_like(self.pos)
+        self.energy = torch.zeros(11, dtype=torch.float64, device=dev)
+        self.masses = np.asarray(masses, np.float64)
+        self._arr = (_VP * len(self.forces))(*[f.handle for f in self.forces])
+        self.lib = _lib.load()
+
+    def initialize(self):
+        """initializeForces: the forces (and energies) at the starting positions."""
+        self.force.zero_()
+        self.energy.zero_()
+        F.check(self.lib.pmgpu_evaluate_device(self.topo.handle, len(self.forces), self._arr,
+                                               _VP(self.pos.data_ptr()), _VP(self.force.data_ptr()),
+                                               _VP(self.energy.data_ptr()), self.flags), self.topo.handle)
+        return self
+
+    def run(self, n_steps: int):
+        F.check(self.lib.pmgpu_leapfrog_run(self.topo.handle, len(self.forces), self._arr, _VP(self.mass.data_ptr()),
+                                            _VP(self.pos.data_ptr()), _VP(self.vel.data_ptr()),
+                                            _VP(self.force.data_ptr()), _VP(self.energy.data_ptr()),
+                                            self.timestep, int(n_steps), self.flags), self.topo.handle)
+        return self
+
+    def synchronize(self):
+        F.check(self.lib.pmgpu_synchronize(self.topo.handle), self.topo.handle)
+
+    def state(self):
+        """(positions, velocities, forces, ScalarStructure) after synchronizing."""
+        self.synchronize()
+        e = F.ScalarStructure(virial=bool(self.flags & _lib.FLAG_VIRIAL))
+        v = self.energy.cpu().numpy()
+        e.lennard_jones += float(v[0])
+        e.coulomb += float(v[1])
+        if self.flags & _lib.FLAG_VIRIAL:
+            e.virial_tensor += v[2:11]
+        return self.pos.cpu().numpy(), self.vel.cpu().numpy(), self.force.cpu().numpy(), e

@@ -362,6 +362,21 @@ def water_box_216(seed: int = 1) -> System:
                      cell_size=4.5, scheme="1-3")
 
 
+def oxygen_fluid_216(seed: int = 1) -> System:
+    """The 216 oxygens of :func:`water_box_216` as a Lennard-Jones fluid (eps
+    0.1521 kcal/mol, Rmin/2 1.7682 A, no charges, no molecules): dynamics
+    without the SHAKE/RATTLE constraints that keep rigid waters together."""
+    import dataclasses
+    s = water_box_216(seed)
+    o = np.flatnonzero(s.atom_type == 0)
+    tp = s.type_params[:1].copy()
+    return dataclasses.replace(
+        s, name="oxygen216", positions=s.positions[o].copy(), scaled_charge=np.zeros(len(o)),
+        atom_type=np.zeros(len(o), np.int32), molecule=np.arange(len(o), dtype=np.int32), mass=s.mass[o].copy(),
+        type_params=tp, lj_table=lj_table_from_types(tp), exclusions=np.zeros((0, 3), np.int32),
+        exclusion_check=np.zeros(0, np.int32), bonds=[], angles=[], dihedrals=[])
+
+
 def chain_in_water_14281(seed: int = 2) -> System:
     """4,463 TIP3P waters + an 892-atom random-walk chain in a 52.3 A cube.
 

@@ -51,6 +51,13 @@ def water1m() -> Workload:
                     [lj_ewald_split(10, 12, 0.32), pme_reciprocal((216, 216, 216), 12, 0.32)])
 
 
+def lj_fluid216() -> Workload:
+    """216 LJ oxygens (the 648-atom water box without its hydrogens), LJ C2
+    8 -> 9 A: the Leapfrog runs of the plain-cutoff configuration."""
+    return Workload("oxygen216_lj_c2", systems.oxygen_fluid_216(),
+                    ["LennardJones -switchingFunction C2 -algorithm NonbondedCutoff -switchon 8 -cutoff 9 -cutoff 9"])
+
+
 def water_box_workload(n_water: int, seed: int) -> Workload:
     """One of the batched boxes: cutoff 9 (C2 8 -> 9), alpha from the default
     accuracy 1e-6, PME grid ~1 A rounded to 2^a 3^b 5^c."""

@@ -1,0 +1,114 @@
+"""The Leapfrog integrator on device-resident state (pmgpu_leapfrog_run)
+against the oracle's restatement of LeapfrogIntegrator::run, 1 fs steps from
+seeded 300 K Maxwell-Boltzmann velocities:
+
+* ten steps of the 648-atom water box of the plain-cutoff configuration
+  (LJ + Coulomb, C2 8 -> 9 A, intra-water pairs excluded);
+* one force evaluation plus 1,000 steps of the same box's 216 oxygens as a
+  Lennard-Jones fluid.  The configuration's waters are rigid in the
+  reference, held by the SHAKE/RATTLE modifiers of the integrator; without
+  them (this integrator runs without modifiers) nothing holds a water's
+  hydrogens, so the long runs use the molecule-free fluid."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from protomol_b200 import forces as F
+from protomol_b200 import integrate, workloads
+
+DT = 1.0                     # fs
+
+
+def water648():
+    w = workloads.water216()
+    v = integrate.maxwell_boltzmann(w.system.mass, 300.0, seed=648)
+    return w, v
+
+
+def oxygen_fluid():
+    w = workloads.lj_fluid216()
+    return w, integrate.maxwell_boltzmann(w.system.mass, 300.0, seed=216)
+
+
+def test_maxwell_boltzmann_velocities_have_the_temperature():
+    w, v = water648()
+    n = w.system.n_atoms
+    # 3N - 3 degrees of freedom after removing the net momentum
+    t = 2.0 * integrate.kinetic_energy(w.system.mass, v) / ((3 * n - 3) * integrate.BOLTZMANN)
+    assert abs(t - 300.0) < 300.0 * 4.0 / np.sqrt(3 * n)       # within ~4 sigma of the sample
+    assert np.abs((w.system.mass[:, None] * v).sum(0)).max() < 1e-9
+
+
+def test_oracle_leapfrog_conserves_energy():
+    w, v = oxygen_fluid()
+    specs = [F.parse_definition(d) for d in w.forces]
+    r0 = oracle.evaluate(w.system, specs)
+    e0 = r0["lennard_jones"] + r0["coulomb"] + integrate.kinetic_energy(w.system.mass, v)
+    x, v1, f, r = oracle.leapfrog(w.system, specs, v, DT, 40, forces=r0["forces"])
+    e1 = r["lennard_jones"] + r["coulomb"] + integrate.kinetic_energy(w.system.mass, v1)
+    ke = integrate.kinetic_energy(w.system.mass, v)
+    assert abs(e1 - e0) < 0.01 * ke
+
+
+def _gpu_run(w, v, precision, chunks):
+    topo = F.Topology(w.system)
+    fs = [F.ForceFactory.make(topo, d, precision) for d in w.forces]
+    lf = integrate.Leapfrog(topo, fs, w.system.positions, v, w.system.mass, DT).initialize()
+    out = []
+    for n in chunks:
+        lf.run(n)
+        out.append(lf.state())
+    return topo, out
+
+
+@pytest.mark.gpu
+def test_ten_steps_match_the_oracle():
+    w, v = water648()
+    specs = [F.parse_definition(d) for d in w.forces]
+    x, v1, f, r = oracle.leapfrog(w.system, specs, v, DT, 10)
+    _, [(xg, vg, fg, eg)] = _gpu_run(w, v, "fp64", [10])
+    print(f"\n10 steps: |dx| {np.abs(xg - x).max():.2e} A  |dv| {np.abs(vg - v1).max():.2e}  "
+          f"|dF| {np.abs(fg - f).max():.2e}")
+    # the FP64 forces agree with the oracle to ~1e-12; ten steps keep that
+    assert np.abs(xg - x).max() <= 1e-10
+    assert np.abs(vg - v1).max() <= 1e-10 * np.abs(v1).max()
+    assert np.abs(fg - f).max() <= 1e-8 * np.sqrt((f ** 2).sum(1).mean())
+    assert abs(eg.lennard_jones + eg.coulomb - r["lennard_jones"] - r["coulomb"]) <= 1e-9 * (
+        abs(r["lennard_jones"]) + abs(r["coulomb"]))
+
+
+@pytest.mark.gpu
+def test_one_evaluation_plus_a_thousand_steps():
+    """One evaluation plus 1,000 steps, FP64 on the GPU against the oracle:
+    the trajectories separate only by the amplified rounding of the forces (a
+    fluid's trajectories diverge exponentially), and both conserve the total
+    energy alike."""
+    w, v = oxygen_fluid()
+    specs = [F.parse_definition(d) for d in w.forces]
+    r0 = oracle.evaluate(w.system, specs)
+    x, v1, f, r = oracle.leapfrog(w.system, specs, v, DT, 1000, forces=r0["forces"])
+    _, [(xg, vg, fg, eg)] = _gpu_run(w, v, "fp64", [1000])
+    ke0 = integrate.kinetic_energy(w.system.mass, v)
+    e0 = r0["lennard_jones"] + r0["coulomb"] + ke0
+    e_ref = r["lennard_jones"] + r["coulomb"] + integrate.kinetic_energy(w.system.mass, v1)
+    e_gpu = eg.lennard_jones + eg.coulomb + integrate.kinetic_energy(w.system.mass, vg)
+    print(f"\n1000 steps: |dx| {np.abs(xg - x).max():.2e} A  energy drift oracle {e_ref - e0:+.4f} "
+          f"gpu {e_gpu - e0:+.4f} kcal/mol (KE {ke0:.1f})")
+    # measured: 1.6e-11 A apart after 1,000 steps, the same energy drift
+    assert np.abs(xg - x).max() <= 1e-8
+    assert abs(e_gpu - e_ref) <= 1e-6 * ke0
+    assert abs(e_gpu - e0) <= 0.01 * ke0
+
+
+@pytest.mark.gpu
+def test_mixed_precision_trajectory_conserves_energy_like_fp64():
+    w, v = oxygen_fluid()
+    ke0 = integrate.kinetic_energy(w.system.mass, v)
+    drifts = {}
+    for precision in ("fp64", "mixed"):
+        topo, states = _gpu_run(w, v, precision, [100] * 10)
+        e = [s[3].lennard_jones + s[3].coulomb + integrate.kinetic_energy(w.system.mass, s[1]) for s in states]
+        drifts[precision] = np.ptp(e)
+    print(f"\ntotal energy range over 1000 steps: fp64 {drifts['fp64']:.4f}  mixed {drifts['mixed']:.4f} "
+          f"kcal/mol (KE {ke0:.1f})")
+    assert drifts["mixed"] <= 2.0 * drifts["fp64"] + 1e-3 * ke0
