@@ -215,7 +215,7 @@ def main():
     mixed = [F.ForceFactory.make(topo, d, "mixed") for d in w.forces]
     fp64 = [F.ForceFactory.make(topo, d, "fp64") for d in w.forces]
     # the project's autotuner picks the launch shapes for this system
-    tuning = topo.autotune(mixed, s.positions, evals=20)
+    tuning = topo.autotune(mixed, s.positions, evals=50)
     stream = torch.cuda.ExternalStream(topo.stream)
     dpos = torch.tensor(s.positions, dtype=torch.float64, device=f"cuda:{local}")
     dfor = torch.zeros((n, 3), dtype=torch.float64, device=f"cuda:{local}")

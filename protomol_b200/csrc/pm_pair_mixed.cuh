@@ -199,11 +199,15 @@ __device__ __forceinline__ void load_atom(const PairArgs& p, int slot, bool vali
 struct PairGeo {
     float dx, dy, dz, r2;
     bool act, in0, in1;
+    bool near, same;             // inside a cutoff's guard band; the same molecule
     int excl;
 };
 
-// geometry, the within-cutoff decision (FP32 with a guard band, exact FP64
-// inside the band) and the exclusion class of one pair
+// geometry and the FP32 within-cutoff decision of one pair; the two rare
+// cases -- a distance inside a cutoff's guard band (exact FP64 decision) and
+// a pair of one molecule (the exclusion class) -- are only flagged here and
+// resolved by resolve_rare, which a warp enters only when one of its lanes
+// holds such a pair
 template <int NT, int S0, int S1, bool WRAP>
 __device__ __forceinline__ PairGeo pair_geo(const PairArgs& p, const JAtom& ia, const JAtom& ja,
                                             float ox, float oy, float oz, float olx, float oly, float olz,
@@ -228,24 +232,33 @@ __device__ __forceinline__ PairGeo pair_geo(const PairArgs& p, const JAtom& ia, 
     bool near = !far && r2 >= p.cut2f * g_lo;
     if (S0 == SCUT && t0c2 != p.cut2f) near |= (r2 >= t0c2 * g_lo && r2 <= t0c2 * g_hi);
     if (NT > 1 && S1 == SCUT && t1c2 != p.cut2f) near |= (r2 >= t1c2 * g_lo && r2 <= t1c2 * g_hi);
-    near = near && valid;
-    bool in_pair = !far;
+    g.near = near && valid;
     g.in0 = r2 <= t0c2;
     g.in1 = NT > 1 ? r2 <= t1c2 : false;
-    if (near) {                                   // rare: the exact FP64 decision
-        double d2 = exact_d2(p, ia.m.x, ja.m.x);
-        in_pair = !(d2 > p.cut2d);
+    g.act = valid && !far;
+    g.same = ia.m.z == ja.m.z;
+    g.excl = PMGPU_EXCL_NONE;
+    g.dx = dx; g.dy = dy; g.dz = dz; g.r2 = r2;
+    return g;
+}
+
+__device__ __forceinline__ bool is_rare(const PairGeo& g) { return g.near || (g.act && g.same); }
+
+// the exact FP64 decision inside the guard band, then the exclusion class of
+// a pair of one molecule (ExclusionTable::check)
+template <int NT>
+__device__ __forceinline__ void resolve_rare(const PairArgs& p, PairGeo& g, const JAtom& ia, const JAtom& ja)
+{
+    if (g.near) {
+        const double d2 = exact_d2(p, ia.m.x, ja.m.x);
+        g.act = !(d2 > p.cut2d);                  // near implies a valid pair
         g.in0 = !(d2 > p.td[0].cut2);
         g.in1 = NT > 1 ? !(d2 > p.td[1].cut2) : false;
     }
-    g.act = valid && in_pair;
-    g.excl = PMGPU_EXCL_NONE;
-    if (g.act && ia.m.z == ja.m.z) {              // same molecule: ExclusionTable::check
+    if (g.act && g.same) {
         g.excl = excl_class(p, ia.m.x, ja.m.x);
         if (g.excl == PMGPU_EXCL_FULL) g.act = false;
     }
-    g.dx = dx; g.dy = dy; g.dz = dz; g.r2 = r2;
-    return g;
 }
 
 // 1/sqrt(x) and 1/x: the hardware approximation and one Newton-Raphson step
@@ -456,6 +469,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
                 ox = o.x; oy = o.y; oz = o.z; olx = ol.x; oly = ol.y; olz = ol.z;
             }
             float fax = 0.f, fay = 0.f, faz = 0.f, fbx = 0.f, fby = 0.f, fbz = 0.f;
+            bool entry_math = false;                       // warp-uniform: a tile of this entry ran the math
 #pragma unroll 1
             for (int q = 0; q < kSuper; ++q) {
                 if (imask & (1u << q)) {                   // warp-uniform
@@ -466,13 +480,18 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
                     const bool diag = k < 0 && cur.x == cd.x + q * kCluster;   // i-cluster with itself
                     const bool va = vi && jg < nj && (!diag || jg > il);
                     const bool vb = vi && jg + 4 < nj && (!diag || jg + 4 > il);
-                    const PairGeo ga = pair_geo<NT, S0, S1, WRAP>(p, ia, ca, ox, oy, oz, olx, oly, olz, va);
-                    const PairGeo gb = pair_geo<NT, S0, S1, WRAP>(p, ia, cb, ox, oy, oz, olx, oly, olz, vb);
+                    PairGeo ga = pair_geo<NT, S0, S1, WRAP>(p, ia, ca, ox, oy, oz, olx, oly, olz, va);
+                    PairGeo gb = pair_geo<NT, S0, S1, WRAP>(p, ia, cb, ox, oy, oz, olx, oly, olz, vb);
+                    if (__any_sync(FULL, is_rare(ga) || is_rare(gb))) {   // warp-uniform, rare
+                        resolve_rare<NT>(p, ga, ia, ca);
+                        resolve_rare<NT>(p, gb, ia, cb);
+                    }
                     // the math only for the 8x4 half-tiles (j-atoms 0-3 and
                     // 4-7, spatially separate halves of the cluster) that hold a
                     // pair inside the cutoff: about 40% of them hold none
                     const bool any_a = __any_sync(FULL, ga.act), any_b = __any_sync(FULL, gb.act);
                     if (!(any_a || any_b)) goto next_cluster;
+                    entry_math = true;
                     float fta = 0.f, ela = 0.f, eca = 0.f, ftb = 0.f, elb = 0.f, ecb = 0.f;
                     if (any_a && any_b) {
                         pair_math<NT, P0, S0, P1, S1>(p, ga, ia, ca, fta, ela, eca);
@@ -489,8 +508,8 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
                     // near pairs: queued for FP64 energies in place of the FP32 ones
                     {
                         const bool na = ga.act && ga.r2 < p.near2, nb = gb.act && gb.r2 < p.near2;   // near2 = 0: none
-                        const unsigned ba = __ballot_sync(FULL, na), bb = __ballot_sync(FULL, nb);
-                        if (ba | bb) {
+                        if (__any_sync(FULL, na || nb)) {
+                            const unsigned ba = __ballot_sync(FULL, na), bb = __ballot_sync(FULL, nb);
                             const unsigned lt = (1u << lane) - 1u;
                             const int si = cd.x + q * kCluster + il, sj = cur.x + jg;
                             if (na) {
@@ -541,14 +560,17 @@ __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
                 }
             }
             // j-forces: lane il ends with component comp of j-atom jg + jsel
-            const float v = j_reduce_scatter(fax, fay, faz, fbx, fby, fbz, il);
-            if (il < 6 && jg + jsel < nj && v != 0.f)
-                fixed_addf(p.facc + 3 * (size_t)(cur.x + jg + jsel) + comp, v, p.status);
-            if (!WRAP && p.virial && il < 6 && k >= 0) {   // o (x) F_entry, column comp
-                const double4 o64 = p.hoff64[k];
-                wv[0] = fma(o64.x, (double)v, wv[0]);
-                wv[1] = fma(o64.y, (double)v, wv[1]);
-                wv[2] = fma(o64.z, (double)v, wv[2]);
+            // (nothing to add when no tile of the entry held a pair)
+            if (entry_math) {
+                const float v = j_reduce_scatter(fax, fay, faz, fbx, fby, fbz, il);
+                if (il < 6 && jg + jsel < nj && v != 0.f)
+                    fixed_addf(p.facc + 3 * (size_t)(cur.x + jg + jsel) + comp, v, p.status);
+                if (!WRAP && p.virial && il < 6 && k >= 0) {   // o (x) F_entry, column comp
+                    const double4 o64 = p.hoff64[k];
+                    wv[0] = fma(o64.x, (double)v, wv[0]);
+                    wv[1] = fma(o64.y, (double)v, wv[1]);
+                    wv[2] = fma(o64.z, (double)v, wv[2]);
+                }
             }
         }
         // chunk end: i-forces, then the chunk's partials in fixed point
