@@ -144,8 +144,15 @@ __global__ void __launch_bounds__(128) k_cluster_list(PairArgs p)
             ilo[q] = p.cbox[2 * ic]; ihi[q] = p.cbox[2 * ic + 1];
         }
         const Cand c = candidate(p, A, ax, ay, az, ic0, ca1, k);
+        // the masks of the first 8 j-clusters are kept (4 bits each) for the
+        // writing pass; a cell with more clusters recomputes the rest
         int cnt = 0;
-        for (int jc = c.jb; jc < c.je; ++jc) cnt += near_mask(p, c, jc, ilo, ihi, nsc, ic0, lim) ? 1 : 0;
+        unsigned kept = 0u;
+        for (int jc = c.jb; jc < c.je; ++jc) {
+            const unsigned m = near_mask(p, c, jc, ilo, ihi, nsc, ic0, lim);
+            if (jc - c.jb < 8) kept |= m << (4 * (jc - c.jb));
+            cnt += m ? 1 : 0;
+        }
         int incl = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -165,7 +172,8 @@ __global__ void __launch_bounds__(128) k_cluster_list(PairArgs p)
         const int ebase = __shfl_sync(FULL, b0, 0), cbase = __shfl_sync(FULL, b1, 0);
         int w = ebase + incl - cnt;
         for (int jc = c.jb; jc < c.je && cnt > 0; ++jc) {
-            const unsigned m = near_mask(p, c, jc, ilo, ihi, nsc, ic0, lim);
+            const unsigned m = jc - c.jb < 8 ? (kept >> (4 * (jc - c.jb))) & 0xfu
+                                             : near_mask(p, c, jc, ilo, ihi, nsc, ic0, lim);
             if (!m) continue;
             if (w < p.plist_cap) {
                 const int jfirst = c.sb + (jc - c.cb0) * kCluster;

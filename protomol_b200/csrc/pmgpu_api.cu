@@ -60,6 +60,7 @@ struct pmgpu_system {
     // (forked after binning, joined before finalize)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_pair = nullptr, ev_near = nullptr;   // the last near-pair energies on the side stream
     std::string err;
     long long launches = 0;
     // topology
@@ -248,7 +249,9 @@ extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
     cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     if (cudaStreamCreateWithPriority(&sys->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaEventCreateWithFlags(&sys->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&sys->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&sys->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sys->ev_pair, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sys->ev_near, cudaEventDisableTiming) != cudaSuccess) {
         cudaStreamDestroy(sys->stream);
         delete sys;
         return PMGPU_ERR_CUDA;
@@ -303,6 +306,8 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     if (sys->h_energy) cudaFreeHost(sys->h_energy);
     cudaEventDestroy(sys->ev_fork);
     cudaEventDestroy(sys->ev_join);
+    cudaEventDestroy(sys->ev_pair);
+    cudaEventDestroy(sys->ev_near);
     cudaStreamDestroy(sys->side);
     cudaStreamDestroy(sys->stream);
     delete sys;
@@ -1271,6 +1276,10 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         prof_end(sys, m);
         used += pair_records(sys, f);
     }
+    int last_mixed = -1;                // the last mixed cutoff force (its near pairs may go to the side stream)
+    for (int k = 0; k < nf; ++k)
+        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) last_mixed = k;
+    bool near_on_side = false;
     int lists = 0;
     int pair_virial = 0;
     for (int k = 0; k < nf; ++k) {
@@ -1293,7 +1302,20 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         int m = prof_begin(sys, kPhasePair);
         int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
                      : launch_pair_mixed(a, f->combo, s, &sys->launches);
-        if (!e && !fp64 && a.near2 > 0.0f) e = launch_near_energy(a, f->combo, sys->n, s, &sys->launches);
+        if (!e && !fp64 && a.near2 > 0.0f) {
+            // the last cutoff force's near-pair energies (needed only by the
+            // energy reduction) run on the side stream, after PME, beside
+            // finalize; earlier forces' before the next list reuses the buffer
+            if (fork && k == last_mixed) {
+                CK(cudaEventRecord(sys->ev_pair, s), "event");
+                CK(cudaStreamWaitEvent(sys->side, sys->ev_pair, 0), "event");
+                e = launch_near_energy(a, f->combo, sys->n, sys->side, &sys->launches);
+                CK(cudaEventRecord(sys->ev_near, sys->side), "event");
+                near_on_side = true;
+            } else {
+                e = launch_near_energy(a, f->combo, sys->n, s, &sys->launches);
+            }
+        }
         if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
         prof_end(sys, m);
         used += pair_records(sys, f);
@@ -1328,6 +1350,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         used += rec;
     }
     if (nf > 0) {
+        if (near_on_side) CK(cudaStreamWaitEvent(s, sys->ev_near, 0), "join");
         int e = launch_energy_reduce(sys->d_erec, sys->erec_cap, used, sys->d_efix, d_energy, s, &sys->launches);
         if (e) return cuda_fail(sys, (cudaError_t)e, "energy reduce");
     }
