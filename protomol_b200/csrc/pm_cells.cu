@@ -129,6 +129,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(BinArgs a)
 
 __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(BinArgs a)
 {
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int c = a.cell_lin[i];
@@ -172,6 +173,7 @@ __device__ __forceinline__ bool key_before(int kj, int ij, int ki, int ii)
 
 __global__ void __launch_bounds__(128) k_bin_cells(BinArgs a)
 {
+    pdl_wait();
     __shared__ int s_idx[4][kCellStage], s_key[4][kCellStage];
     __shared__ float s_px[4][kCellStage], s_py[4][kCellStage], s_pz[4][kCellStage];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -238,8 +240,8 @@ int launch_bin(const BinArgs& a, cudaStream_t s, long long* launches)
     k_bin_count<<<nb, kBinThreads, 0, s>>>(a);
     *launches += 1;
     if (a.n > 0) {
-        k_bin_scatter<<<nb, kBinThreads, 0, s>>>(a);
-        k_bin_cells<<<(a.grid.ncell + 3) / 4, 128, 0, s>>>(a);
+        launch_pdl(k_bin_scatter, nb, kBinThreads, 0, s, a);
+        launch_pdl(k_bin_cells, (a.grid.ncell + 3) / 4, 128, 0, s, a);
         *launches += 2;
     }
     return (int)cudaGetLastError();

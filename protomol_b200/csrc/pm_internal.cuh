@@ -15,6 +15,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <utility>
 
 namespace pm {
 
@@ -48,6 +49,33 @@ struct CellGrid {
     double csx, csy, csz;       // myRealCellSize
     double rcsx, rcsy, rcsz;    // myRealRCellSize
 };
+
+// ---- programmatic dependent launch ----------------------------------------
+// The kernels of one evaluation's critical path are launched with
+// programmatic stream serialization: a kernel's blocks may be scheduled while
+// the previous kernel's last blocks finish, and wait here (griddepcontrol.wait,
+// sm_90+) until that kernel has completed and its memory is visible.  For a
+// kernel launched without the attribute the wait returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+#ifdef __CUDACC__
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+#endif
 
 // ---- exact FP64 arithmetic in the reference's operation order ------------
 // (no FMA contraction: every product and sum rounded on its own)

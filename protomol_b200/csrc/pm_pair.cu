@@ -472,7 +472,7 @@ static int run_mixed_w(const PairArgs& a, cudaStream_t s, long long* launches)
     // kernels running beside it), else the occupancy limit
     const int bps = a.blocks_per_sm > 0 ? std::min(per_sm, a.blocks_per_sm) : per_sm;
     const int blocks = sms * bps;
-    k_pair_mixed<NT, P0, S0, P1, S1, WRAP><<<blocks, 128, 0, s>>>(a);
+    launch_pdl(k_pair_mixed<NT, P0, S0, P1, S1, WRAP>, blocks, 128, 0, s, a);
     *launches += 1;
     return (int)cudaGetLastError();
 }
@@ -489,7 +489,7 @@ int launch_cluster_list(const PairArgs& a, cudaStream_t s, long long* launches)
     // one warp per cell and block of 32 half-shell cells
     long long warps = (long long)a.grid.ncell * ((a.nh + 1 + 31) / 32);
     int lb = (int)((warps + 3) / 4);
-    k_cluster_list<<<lb > 0 ? lb : 1, 128, 0, s>>>(a);
+    launch_pdl(k_cluster_list, lb > 0 ? lb : 1, 128, 0, s, a);
     *launches += 1;
     return (int)cudaGetLastError();
 }

@@ -118,6 +118,7 @@ __device__ __forceinline__ unsigned near_mask(const PairArgs& p, const Cand& c, 
 
 __global__ void __launch_bounds__(128) k_cluster_list(PairArgs p)
 {
+    pdl_wait();
     // one warp per (cell, block of 32 half-shell cells): the warp's entries of
     // a supercluster are contiguous and cut into their own chunks
     const unsigned FULL = 0xffffffffu;
@@ -407,6 +408,7 @@ __device__ __forceinline__ float j_reduce_scatter(float ax, float ay, float az, 
 template <int NT, int P0, int S0, int P1, int S1, bool WRAP>
 __global__ void __launch_bounds__(128, 4) k_pair_mixed(PairArgs p)
 {
+    pdl_wait();
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, il = lane & 7, jg = lane >> 3;
     __shared__ float4 s_p[4][kSuper * kCluster], s_l[4][kSuper * kCluster];

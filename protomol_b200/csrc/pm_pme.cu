@@ -627,6 +627,7 @@ int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches
 // ------------------------------------------------------------------ finalize
 __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
 {
+    pdl_wait();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double v[kERec];
 #pragma unroll
@@ -662,7 +663,7 @@ int launch_finalize(const FinArgs& a, cudaStream_t s, long long* launches, int* 
     *records = 0;
     if (a.n <= 0) return 0;
     const int blocks = (a.n + 255) / 256;
-    k_finalize<<<blocks, 256, 0, s>>>(a);
+    launch_pdl(k_finalize, blocks, 256, 0, s, a);
     *launches += 1;
     if (a.pair_virial) *records = blocks;
     return (int)cudaGetLastError();
@@ -672,6 +673,7 @@ int launch_finalize(const FinArgs& a, cudaStream_t s, long long* launches, int* 
 __global__ void k_energy_reduce(const double* erec, int stride, int nrec, const unsigned long long* efix,
                                 double* out)
 {
+    pdl_wait();
     int k = blockIdx.x;
     const double* c = erec + (size_t)k * stride;
     double s = 0.0;
@@ -692,7 +694,7 @@ __global__ void k_energy_reduce(const double* erec, int stride, int nrec, const 
 int launch_energy_reduce(const double* erec, int stride, int nrec, const unsigned long long* efix,
                          double* out, cudaStream_t s, long long* launches)
 {
-    k_energy_reduce<<<kERec, 256, 0, s>>>(erec, stride, nrec, efix, out);
+    launch_pdl(k_energy_reduce, kERec, 256, 0, s, erec, stride, nrec, efix, out);
     *launches += 1;
     return (int)cudaGetLastError();
 }
