@@ -291,6 +291,18 @@ int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, 
  * timed evaluations (zero them before the next real one). */
 int pmgpu_batch_autotune(pmgpu_batch* batch, int evals, pmgpu_tuning* best);
 
+/* ---- dense Hessian ----------------------------------------------------------
+ * Hessian::evaluate's LJ / Coulomb pair blocks (integrators/Hessian.cpp:
+ * 456-623; ReducedHessLennardJones.cpp:7-51, ReducedHessCoulomb.cpp:8-43,
+ * switches C2SwitchingFunction::hessian C2SwitchingFunction.cpp:45-53) of the
+ * pair terms of cutoff, all-pairs and PME-real forces: the 3N x 3N second
+ * derivative of their energy at the host positions, row-major, added (+=)
+ * to hessian.  The matrix the normal-mode integrators diagonalise
+ * (NormalModeUtilities).  Up to 8,192 atoms (PMGPU_ERR_CAPACITY);
+ * PMGPU_ERR_UNSUPPORTED for the PME reciprocal and correction terms. */
+int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,
+                  double* hessian);
+
 /* ---- integration ---------------------------------------------------------
  * LeapfrogIntegrator::run(n_steps) (integrators/LeapfrogIntegrator.cpp:
  * 107-120; doHalfKickdoDrift :47-68, doKickdoDrift :70-101, doHalfKick

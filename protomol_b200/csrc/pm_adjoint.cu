@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(kTile) k_pair_adjoint(AdjArgs p)
     __syncthreads();
     double dq = 0.0, hv[3] = {0.0, 0.0, 0.0}, el = 0.0, ec = 0.0;
     double fi[3] = {0.0, 0.0, 0.0}, vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double hd[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};   // the ii block of the dense Hessian
     if (i < p.n) {
         const double xi = p.pos[3 * (size_t)i], yi = p.pos[3 * (size_t)i + 1], zi = p.pos[3 * (size_t)i + 2];
         const double qi = p.q[i];
@@ -208,6 +209,22 @@ __global__ void __launch_bounds__(kTile) k_pair_adjoint(AdjArgs p)
                 hv[1] += (double)F * uy + two_f1 * du * dy;
                 hv[2] += (double)F * uz + two_f1 * du * dz;
             }
+            if (p.hess) {
+                // H_ij = F I + 2 F' d d^T (the HVP's block above); H_ii = -sum_j H_ij.
+                // Row block i belongs to this thread: no other thread writes H_ij.
+                const double fF = (double)F, t2 = 2.0 * (double)F1;
+                const double d[3] = {dx, dy, dz};
+                const size_t ld = 3 * (size_t)p.n;
+                double* row = p.hess + 3 * (size_t)i * ld + 3 * (size_t)j;
+#pragma unroll
+                for (int ra = 0; ra < 3; ++ra)
+#pragma unroll
+                    for (int cb = 0; cb < 3; ++cb) {
+                        const double b = (ra == cb ? fF : 0.0) + t2 * d[ra] * d[cb];
+                        row[ra * ld + cb] += b;
+                        hd[3 * ra + cb] -= b;
+                    }
+            }
             if (p.dlj && (pA != 0 || pB != 0)) {
                 const size_t k = ((size_t)ti * p.n_types + s_type[jj]) * 4 + (mod ? 2 : 0);
                 if (lj_smem) {
@@ -220,6 +237,13 @@ __global__ void __launch_bounds__(kTile) k_pair_adjoint(AdjArgs p)
             }
         }
         if (p.dq && dq != 0.0) atomicAdd(p.dq + i, dq);
+        if (p.hess) {   // the diagonal block sums over the j tiles of other blocks too
+            const size_t ld = 3 * (size_t)p.n;
+            for (int ra = 0; ra < 3; ++ra)
+                for (int cb = 0; cb < 3; ++cb)
+                    if (hd[3 * ra + cb] != 0.0) atomicAdd(p.hess + (3 * (size_t)i + ra) * ld + 3 * (size_t)i + cb,
+                                                          hd[3 * ra + cb]);
+        }
         if (p.hv)
             for (int c = 0; c < 3; ++c)
                 if (hv[c] != 0.0) atomicAdd(p.hv + 3 * (size_t)i + c, hv[c]);

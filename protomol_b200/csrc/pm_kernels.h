@@ -187,6 +187,7 @@ struct AdjArgs {
     double* dq;                  // N (+=) or null
     double* dlj;                 // T x T x 4 (+=) or null
     double* hv;                  // 3N (+=) or null
+    double* hess;                // 3N x 3N row-major (+=) or null: the dense pair Hessian
     double* energy;              // 2 (+=): LJ, Coulomb, or null
     // forward mode (the vacuum all-pairs force): forces in atom order
     // (fixed point) and one energy/virial record per block

@@ -2005,6 +2005,48 @@ extern "C" int pmgpu_batch_autotune(pmgpu_batch* b, int evals, pmgpu_tuning* bes
     return PMGPU_OK;
 }
 
+// ------------------------------------------------------------------ dense Hessian
+static const int kHessianMaxAtoms = 8192;    // 3N x 3N doubles: 4.8 GB at the limit
+
+extern "C" int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces_in, const double* positions,
+                             double* hessian)
+{
+    if (!sys || !positions || !hessian || n_forces < 1 || !forces_in) return PMGPU_ERR_ARG;
+    cudaSetDevice(sys->device);
+    std::vector<pmgpu_force*> fl;
+    for (int k = 0; k < n_forces; ++k) {
+        if (!forces_in[k] || forces_in[k]->sys != sys) return fail(sys, PMGPU_ERR_ARG, "bad force list");
+        if (forces_in[k]->real_sub) fl.push_back(forces_in[k]->real_sub);
+        if (forces_in[k]->kind == 1 && (forces_in[k]->pp.reciprocal || forces_in[k]->pp.correction))
+            return fail(sys, PMGPU_ERR_UNSUPPORTED, "the Hessian of the PME reciprocal / correction terms is not "
+                                                    "available (the real-space pairs are)");
+        if (forces_in[k]->kind != 1) fl.push_back(forces_in[k]);
+    }
+    if (sys->n > kHessianMaxAtoms) return fail(sys, PMGPU_ERR_CAPACITY, "dense Hessian above 8192 atoms");
+    int r = eval_prepare(sys, (int)fl.size(), fl.data());
+    if (r) return r;
+    const size_t n3 = 3 * (size_t)sys->n, nh = n3 * n3;
+    cudaStream_t s = sys->stream;
+    double* d_h = nullptr;
+    cudaError_t e = dalloc(&d_h, nh);
+    auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    ok(cudaMemcpyAsync(sys->d_pos, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+    ok(cudaMemsetAsync(d_h, 0, sizeof(double) * nh, s));
+    for (pmgpu_force* f : fl) {
+        AdjArgs a;
+        adj_pair_args(sys, f, a);
+        a.hess = d_h;
+        ok((cudaError_t)launch_pair_adjoint(a, f->precision == PMGPU_PRECISION_FP64 ? 1 : 0, s, &sys->launches));
+    }
+    std::vector<double> out(e == cudaSuccess ? nh : 0);
+    if (e == cudaSuccess) ok(cudaMemcpyAsync(out.data(), d_h, sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
+    ok(cudaStreamSynchronize(s));
+    dfree(d_h);
+    if (e != cudaSuccess) return cuda_fail(sys, e, "Hessian");
+    for (size_t k = 0; k < nh; ++k) hessian[k] += out[k];
+    return PMGPU_OK;
+}
+
 // ------------------------------------------------------------------ leapfrog
 static const double kInvTimeFactor = 0.02045482828087295;   // Constant::INV_TIMEFACTOR (base/pmconstants.cpp:49)
 

@@ -252,6 +252,19 @@ def adjoint(topo: Topology, forces, positions, v=None):
     return {"dE_dq": dq, "dE_dlj": dlj, "hv": hv, "lennard_jones": en[0], "coulomb": en[1]}
 
 
+def hessian(topo: Topology, forces, positions) -> np.ndarray:
+    """pmgpu_hessian: the dense 3N x 3N Hessian of the forces' pair terms
+    (Hessian::evaluate's blocks, integrators/Hessian.cpp:456-623)."""
+    lib = _lib.load()
+    pos = np.ascontiguousarray(positions, np.float64)
+    n3 = 3 * topo.n_atoms
+    h = np.zeros((n3, n3))
+    arr = (_VP * len(forces))(*[f.handle for f in forces])
+    check(lib.pmgpu_hessian(topo.handle, len(forces), arr, pos.ctypes.data_as(_VP), h.ctypes.data_as(_VP)),
+          topo.handle)
+    return h
+
+
 def lj_parameter_gradient(type_params, dE_dlj):
     """Chain rule from the LJ-table gradient of ``adjoint`` to the per-type
     parameters of the PAR file: returns (T, 4) = dE/d(eps, Rmin/2, eps14,

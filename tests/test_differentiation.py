@@ -239,3 +239,29 @@ def test_autograd_charge_gradient_on_the_14281_atom_pme_box(chain14281):
     fs = [F.ForceFactory.make(topo, d, "fp64") for d in w.forces]
     ref = F.adjoint(topo, fs, chain14281.positions)["dE_dq"]
     assert rel(gq.numpy(), ref) <= 1e-5               # mixed against the FP64 backward pass
+
+
+# ---------------------------------------------------------------- dense Hessian
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-5)])
+def test_dense_hessian_is_the_reference_hessian(chain, precision, tol):
+    H = oracle.pair_hessian(chain, F.parse_definition(FULL))
+    topo = F.Topology(chain)
+    fs = [F.ForceFactory.make(topo, FULL, precision)]
+    Hg = F.hessian(topo, fs, chain.positions)
+    assert rel(Hg, H) <= tol
+    assert np.abs(Hg - Hg.T).max() <= 10 * tol * np.abs(H).max()
+    v = np.random.default_rng(67).normal(size=(chain.n_atoms, 3))
+    hv = F.adjoint(topo, fs, chain.positions, v)["hv"].reshape(-1)
+    assert rel(Hg @ v.reshape(-1), hv) <= tol                 # the same blocks as the HVP
+
+
+def test_dense_hessian_of_a_periodic_cutoff_force():
+    """The minimal image and the cutoff: a 1,260-atom chain in water with LJ
+    C2 + Coulomb C1 (cutoff 9), against the oracle's periodic Hessian."""
+    s = systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+    d = ("LennardJones Coulomb -switchingFunction C2 -switchingFunction C1 -algorithm NonbondedCutoff "
+         "-switchon 7 -cutoff 9 -cutoff 9 -cutoff 9")
+    H = oracle.pair_hessian(s, F.parse_definition(d))
+    topo = F.Topology(s)
+    Hg = F.hessian(topo, [F.ForceFactory.make(topo, d, "fp64")], s.positions)
+    assert rel(Hg, H) <= 1e-10
