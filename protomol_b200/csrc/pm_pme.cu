@@ -41,37 +41,60 @@ template <typename C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
 template <typename C> __device__ __forceinline__ C cconj_if(C a, bool c) { if (c) a.y = -a.y; return a; }
 
+// Stockham plan of one line length: radices (8 first, then 4, 2, 3, 5, 7:
+// the reference's FFT handles the same factors) and, per stage, the sizes the kernel divides by
+// (exact multiply-high reciprocals: every index here is below 2^15) and the
+// twiddle stride n / (Ns R)
 struct FftPlan {
     int n;
     int nrad;
-    int rad[24];
+    int rad[16];
+    int m[16];                 // n / R
+    int ns[16];                // product of the earlier radices
+    unsigned m_rcp[16];        // ceil(2^32 / m)
+    unsigned ns_rcp[16];       // ceil(2^32 / ns)
+    int tws[16];               // n / (ns R)
 };
 
-// twiddle exp(sign 2 pi i m / M) from the table of n-th roots exp(-2 pi i k / n)
+__device__ __forceinline__ int fdiv(int x, unsigned rcp) { return (int)__umulhi((unsigned)x, rcp); }
+
+// the table's n-th roots exp(-2 pi i k / n), conjugated for sign > 0
 template <typename C>
-__device__ __forceinline__ C twid(const C* tw, int n, int m, int M, int sign)
+__device__ __forceinline__ C tw_at(const C* tw, int k, int sign)
 {
-    int k = (int)(((long long)m * (n / M)) % n);
     C w = tw[k];
     if (sign > 0) w.y = -w.y;
     return w;
 }
 
-// R-point DFT of v[0..R-1] in place, exp(sign 2 pi i jk / R).
-template <typename C, typename R>
-__device__ __forceinline__ void small_dft(C* v, int Rn, int sign, const C* tw, int n)
+// RAD-point DFT of v in registers, exp(sign 2 pi i jk / RAD)
+template <typename C, typename R, int RAD>
+__device__ __forceinline__ void dft_fixed(C (&v)[RAD], int sign, const C* tw, int n)
 {
-    if (Rn == 2) {
+    if (RAD == 2) {
         C a = v[0], b = v[1];
         v[0] = cadd(a, b); v[1] = csub(a, b);
-    } else if (Rn == 4) {
+    } else if (RAD == 4) {
         C a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
         C c = cadd(v[1], v[3]), d = csub(v[1], v[3]);
-        // d * (sign i)
-        C di; di.x = -sign * d.y; di.y = sign * d.x;
+        C di; di.x = -sign * d.y; di.y = sign * d.x;          // d * (sign i)
         v[0] = cadd(a, c); v[2] = csub(a, c);
         v[1] = cadd(b, di); v[3] = csub(b, di);
-    } else if (Rn == 3) {
+    } else if (RAD == 8) {
+        // even / odd halves as 4-point DFTs, then X[k] = E[k] +- w8^k O[k]
+        C e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        dft_fixed<C, R, 4>(e, sign, tw, n);
+        dft_fixed<C, R, 4>(o, sign, tw, n);
+        const R h = (R)0.70710678118654752440;
+        C w1, w3, o2;
+        w1.x = h * (o[1].x - sign * o[1].y); w1.y = h * (o[1].y + sign * o[1].x);     // o1 (1 + sign i) / sqrt 2
+        o2.x = -sign * o[2].y; o2.y = sign * o[2].x;                                  // o2 (sign i)
+        w3.x = h * (-o[3].x - sign * o[3].y); w3.y = h * (-o[3].y + sign * o[3].x);   // o3 (-1 + sign i) / sqrt 2
+        v[0] = cadd(e[0], o[0]); v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], w1);   v[5] = csub(e[1], w1);
+        v[2] = cadd(e[2], o2);   v[6] = csub(e[2], o2);
+        v[3] = cadd(e[3], w3);   v[7] = csub(e[3], w3);
+    } else if (RAD == 3) {
         const R c1 = (R)-0.5, s1 = (R)0.86602540378443864676 * (R)sign;
         C a = v[0], b = v[1], c = v[2];
         C t; t.x = b.x + c.x; t.y = b.y + c.y;
@@ -79,7 +102,7 @@ __device__ __forceinline__ void small_dft(C* v, int Rn, int sign, const C* tw, i
         C d; d.x = -s1 * (b.y - c.y); d.y = s1 * (b.x - c.x);
         v[0].x = a.x + t.x; v[0].y = a.y + t.y;
         v[1] = cadd(m, d); v[2] = csub(m, d);
-    } else if (Rn == 5) {
+    } else if (RAD == 5) {
         const R c1 = (R)0.30901699437494742410, c2 = (R)-0.80901699437494742410;
         const R s1 = (R)0.95105651629515357212 * (R)sign, s2 = (R)0.58778525229247312917 * (R)sign;
         C a = v[0];
@@ -93,42 +116,64 @@ __device__ __forceinline__ void small_dft(C* v, int Rn, int sign, const C* tw, i
         v[1] = cadd(m1, n1); v[4] = csub(m1, n1);
         v[2] = cadd(m2, n2); v[3] = csub(m2, n2);
     } else {
-        C out[16];
-        for (int k = 0; k < Rn; ++k) {
-            C s; s.x = 0; s.y = 0;
-            for (int j = 0; j < Rn; ++j) s = cadd(s, cmul(v[j], twid(tw, n, (j * k) % Rn, Rn, sign)));
+        // 7: direct DFT with the roots exp(sign 2 pi i jk / RAD) = table[(jk mod RAD) n / RAD]
+        C out[RAD];
+#pragma unroll
+        for (int k = 0; k < RAD; ++k) {
+            C s = v[0];
+#pragma unroll
+            for (int j = 1; j < RAD; ++j) s = cadd(s, cmul(v[j], tw_at(tw, ((j * k) % RAD) * (n / RAD), sign)));
             out[k] = s;
         }
-        for (int k = 0; k < Rn; ++k) v[k] = out[k];
+#pragma unroll
+        for (int k = 0; k < RAD; ++k) v[k] = out[k];
     }
 }
 
-// Stockham auto-sort FFT of `lines` lines of length n held in shared memory
-// (line stride ld); returns the buffer that holds the result.
+// one Stockham stage of radix RAD over `lines` lines (stride ld) in shared memory
+template <typename C, typename R, int RAD>
+__device__ __forceinline__ void fft_stage(const C* a, C* b, int lines, int ld, const FftPlan& pl, int s,
+                                          const C* tw, int sign)
+{
+    const int m = pl.m[s], Ns = pl.ns[s], tws = pl.tws[s];
+    for (int idx = threadIdx.x; idx < lines * m; idx += blockDim.x) {
+        const int line = m > 1 ? fdiv(idx, pl.m_rcp[s]) : idx;
+        const int j = idx - line * m;
+        const int jq = Ns > 1 ? fdiv(j, pl.ns_rcp[s]) : j;
+        const int k = j - jq * Ns;
+        const C* in = a + line * ld;
+        C* out = b + line * ld;
+        C v[RAD];
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) v[r] = in[j + r * m];
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < RAD; ++r) v[r] = cmul(v[r], tw_at(tw, k * r * tws, sign));   // k r < Ns RAD
+        }
+        dft_fixed<C, R, RAD>(v, sign, tw, pl.n);
+        const int base = jq * Ns * RAD + k;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) out[base + r * Ns] = v[r];
+    }
+}
+
+// Stockham FFT of `lines` lines of length pl.n in shared memory (a -> b ->
+// a ...), exp(sign 2 pi i jk / n), unnormalised; returns the buffer holding
+// the result.  tw: the n-th roots, staged in shared memory by the caller.
 template <typename C, typename R>
 __device__ C* fft_lines(C* a, C* b, int lines, int ld, const FftPlan& pl, const C* tw, int sign)
 {
-    int n = pl.n;
-    int Ns = 1;
     for (int s = 0; s < pl.nrad; ++s) {
-        int Rn = pl.rad[s];
-        int m = n / Rn;
-        for (int idx = threadIdx.x; idx < lines * m; idx += blockDim.x) {
-            int line = idx / m, j = idx - line * m;
-            const C* in = a + line * ld;
-            C* out = b + line * ld;
-            int k = j % Ns;
-            C v[16];
-            for (int r = 0; r < Rn; ++r) v[r] = in[j + r * m];
-            if (Ns > 1)
-                for (int r = 1; r < Rn; ++r) v[r] = cmul(v[r], twid(tw, n, k * r, Ns * Rn, sign));
-            small_dft<C, R>(v, Rn, sign, tw, n);
-            int base = (j / Ns) * Ns * Rn + k;
-            for (int r = 0; r < Rn; ++r) out[base + r * Ns] = v[r];
+        switch (pl.rad[s]) {
+        case 2: fft_stage<C, R, 2>(a, b, lines, ld, pl, s, tw, sign); break;
+        case 3: fft_stage<C, R, 3>(a, b, lines, ld, pl, s, tw, sign); break;
+        case 4: fft_stage<C, R, 4>(a, b, lines, ld, pl, s, tw, sign); break;
+        case 5: fft_stage<C, R, 5>(a, b, lines, ld, pl, s, tw, sign); break;
+        case 7: fft_stage<C, R, 7>(a, b, lines, ld, pl, s, tw, sign); break;
+        default: fft_stage<C, R, 8>(a, b, lines, ld, pl, s, tw, sign); break;
         }
         __syncthreads();
         C* t = a; a = b; b = t;
-        Ns *= Rn;
     }
     return a;
 }
@@ -235,7 +280,7 @@ struct PassArgs {
 };
 
 template <typename R, int MODE>
-__global__ void k_fft_pass(PassArgs pa)
+__global__ void __launch_bounds__(256, 2) k_fft_pass(PassArgs pa)
 {
     typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -244,7 +289,14 @@ __global__ void k_fft_pass(PassArgs pa)
     const PmeArgs& a = pa.a;
     const FftPlan& pl = pa.plan;
     const int n = pl.n;
-    const C* tw = (const C*)a.tw + pa.tw_off;
+    // the n-th roots of this axis in shared memory (read by every stage);
+    // the barrier after the line loads below covers them
+    C* stw = buf1 + pa.lines * pa.ld;
+    {
+        const C* gtw = (const C*)a.tw + pa.tw_off;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) stw[k] = gtw[k];
+    }
+    const C* tw = stw;
     C* cg = (C*)a.cgrid;
     int L = pa.lines;
     double acc[kERec];
@@ -416,13 +468,21 @@ static void make_plan(int n, FftPlan& p)
     p.n = n;
     p.nrad = 0;
     int m = n;
-    while (m % 4 == 0 && p.nrad < 24) { p.rad[p.nrad++] = 4; m /= 4; }
-    while (m % 2 == 0 && p.nrad < 24) { p.rad[p.nrad++] = 2; m /= 2; }
-    while (m % 3 == 0 && p.nrad < 24) { p.rad[p.nrad++] = 3; m /= 3; }
-    while (m % 5 == 0 && p.nrad < 24) { p.rad[p.nrad++] = 5; m /= 5; }
-    for (int f = 7; m > 1 && f <= 16; f += 2)
-        while (m % f == 0 && p.nrad < 24) { p.rad[p.nrad++] = f; m /= f; }
-    if (m > 1) p.nrad = -1;   // prime factor > 16: unsupported
+    const int radices[6] = {8, 4, 2, 3, 5, 7};
+    for (int r : radices)
+        while (m % r == 0 && p.nrad < 16) { p.rad[p.nrad++] = r; m /= r; }
+    if (m > 1) { p.nrad = -1; return; }   // a prime factor above 7: unsupported
+    int ns = 1;
+    for (int s = 0; s < p.nrad; ++s) {
+        const int r = p.rad[s];
+        p.m[s] = n / r;
+        p.ns[s] = ns;
+        // ceil(2^32 / d); d = 1 is handled without a division in the kernel
+        p.m_rcp[s] = p.m[s] > 1 ? (unsigned)((0x100000000ull + p.m[s] - 1) / p.m[s]) : 0u;
+        p.ns_rcp[s] = ns > 1 ? (unsigned)((0x100000000ull + ns - 1) / ns) : 0u;
+        p.tws[s] = n / (ns * r);
+        ns *= r;
+    }
 }
 
 template <typename R>
@@ -456,7 +516,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         PassArgs pa; pa.a = a; pa.plan = pz; pa.lines = lines_for(a.kz); pa.ld = a.kz + 1; pa.sign = -1;
         pa.tw_off = a.twz; pa.erec_off = 0;
         int blocks = (a.kx * a.ky + pa.lines - 1) / pa.lines;
-        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
         k_fft_pass<R, kModeZR2C><<<blocks, threads, sm, s>>>(pa);
     }
     // lines per CTA for the strided passes: 16 (128 B coalesced rows for
@@ -472,7 +532,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         PassArgs pa; pa.a = a; pa.plan = py; pa.lines = tile; pa.ld = a.ky + 1; pa.sign = -1;
         pa.tw_off = a.twy; pa.erec_off = 0;
         int blocks = a.kx * ((a.kzh + tile - 1) / tile);
-        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
         k_fft_pass<R, kModeY><<<blocks, threads, sm, s>>>(pa);
     }
     // x forward + convolution + x inverse
@@ -481,7 +541,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     {
         PassArgs pa; pa.a = a; pa.plan = px; pa.lines = xtile; pa.ld = a.kx + 1; pa.sign = -1;
         pa.tw_off = a.twx; pa.erec_off = 0;
-        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
         k_fft_pass<R, kModeXConv><<<xblocks, threads, sm, s>>>(pa);
     }
     // y inverse
@@ -489,7 +549,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         PassArgs pa; pa.a = a; pa.plan = py; pa.lines = tile; pa.ld = a.ky + 1; pa.sign = +1;
         pa.tw_off = a.twy; pa.erec_off = 0;
         int blocks = a.kx * ((a.kzh + tile - 1) / tile);
-        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
         k_fft_pass<R, kModeY><<<blocks, threads, sm, s>>>(pa);
     }
     // z c2r
@@ -497,7 +557,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         PassArgs pa; pa.a = a; pa.plan = pz; pa.lines = lines_for(a.kz); pa.ld = a.kz + 1; pa.sign = +1;
         pa.tw_off = a.twz; pa.erec_off = 0;
         int blocks = (a.kx * a.ky + pa.lines - 1) / pa.lines;
-        size_t sm = 2 * (size_t)pa.lines * pa.ld * sizeof(C);
+        size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
         k_fft_pass<R, kModeZC2R><<<blocks, threads, sm, s>>>(pa);
     }
     *launches += 5;

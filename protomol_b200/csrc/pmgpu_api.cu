@@ -808,11 +808,13 @@ static void dftmod(int order, int n, std::vector<double>& mod)
     }
 }
 
+// grid sizes of prime factors 2, 3, 5 and 7 (the reference's FFT, base/fft.c
+// fftfact_, handles the same: radices 2, 3, 4, 5, 7)
 static bool smooth_ok(int n)
 {
     int m = n;
-    for (int f = 2; f <= 16 && m > 1; ++f)
-        while (m % f == 0) m /= f;
+    for (int f : {2, 3, 5, 7})
+        while (m > 1 && m % f == 0) m /= f;
     return m == 1;
 }
 
@@ -831,7 +833,7 @@ extern "C" int pmgpu_pme_create(pmgpu_system* sys, const pmgpu_pme_params* p, pm
     if (p->order > 12) return fail(sys, PMGPU_ERR_UNSUPPORTED, "PME order > 12");
     for (int k = 0; k < 3; ++k)
         if (!smooth_ok(p->grid[k]) || p->grid[k] > 4096)
-            return fail(sys, PMGPU_ERR_UNSUPPORTED, "PME grid size needs prime factors <= 16 and <= 4096");
+            return fail(sys, PMGPU_ERR_UNSUPPORTED, "PME grid size needs prime factors 2, 3, 5, 7 and <= 4096");
     if (p->precision != PMGPU_PRECISION_MIXED && p->precision != PMGPU_PRECISION_FP64)
         return fail(sys, PMGPU_ERR_ARG, "unknown precision");
     if (!sys->box_set || sys->n == 0 && sys->q.empty()) {
