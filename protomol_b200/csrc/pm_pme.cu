@@ -485,6 +485,118 @@ static void make_plan(int n, FftPlan& p)
     }
 }
 
+// ---- order-P kernels with the order known at compile time (P = 4, the
+// default): spline weights and grid indices in registers, every index
+// wrapped once per axis (i0 + p lies in [K - 1, 2K + 1] for P = 4)
+template <typename R, int P>
+__device__ __forceinline__ void bspline_fixed(R w, R (&th)[P], R (&dth)[P])
+{
+    // BSpline::set (base/BSpline.cpp:64-117), the recurrences of bspline4
+    th[P - 1] = (R)0;
+    th[1] = w;
+    th[0] = (R)1 - w;
+#pragma unroll
+    for (int k = 2; k < P - 1; k++) {
+        const R div = (R)1 / (R)k;
+        th[k] = div * w * th[k - 1];
+#pragma unroll
+        for (int j = 1; j < k; j++)
+            th[k - j] = div * ((w + (R)j) * th[k - j - 1] + ((R)(k + 1 - j) - w) * th[k - j]);
+        th[0] = div * ((R)1 - w) * th[0];
+    }
+    dth[0] = -th[0];
+#pragma unroll
+    for (int j = 1; j <= P - 1; j++) dth[j] = th[j - 1] - th[j];
+    const R div = (R)1 / (R)(P - 1);
+    th[P - 1] = div * w * th[P - 2];
+#pragma unroll
+    for (int j = 1; j < P - 1; j++)
+        th[P - 1 - j] = div * ((w + (R)j) * th[P - j - 2] + ((R)(P - j) - w) * th[P - 1 - j]);
+    th[0] = div * ((R)1 - w) * th[0];
+}
+
+__device__ __forceinline__ int wrap_index(int v, int K)
+{
+    v = v >= K ? v - K : v;
+    return v >= K ? v - K : v;
+}
+
+template <typename R, int P>
+__device__ __forceinline__ void grid_point_p(const PmeArgs& a, int atom, int (&ix)[P], int (&iy)[P], int (&iz)[P],
+                                             R (&tx)[P], R (&dtx)[P], R (&ty)[P], R (&dty)[P], R (&tz)[P],
+                                             R (&dtz)[P])
+{
+    const double x = wrap_grid(a.pos[3 * (size_t)atom] * a.hxr, a.kx);
+    const double y = wrap_grid(a.pos[3 * (size_t)atom + 1] * a.hyr, a.ky);
+    const double z = wrap_grid(a.pos[3 * (size_t)atom + 2] * a.hzr, a.kz);
+    const int x0 = (int)x, y0 = (int)y, z0 = (int)z;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        ix[p] = wrap_index(x0 + a.offx + p, a.kx);
+        iy[p] = wrap_index(y0 + a.offy + p, a.ky);
+        iz[p] = wrap_index(z0 + a.offz + p, a.kz);
+    }
+    bspline_fixed<R, P>((R)(x - x0), tx, dtx);
+    bspline_fixed<R, P>((R)(y - y0), ty, dty);
+    bspline_fixed<R, P>((R)(z - z0), tz, dtz);
+}
+
+template <typename R, int P>
+__global__ void __launch_bounds__(128) k_spread_p(PmeArgs a)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.n) return;
+    const int atom = a.sorted ? a.sorted[s] : s;
+    R tx[P], dtx[P], ty[P], dty[P], tz[P], dtz[P];
+    int ix[P], iy[P], iz[P];
+    grid_point_p<R, P>(a, atom, ix, iy, iz, tx, dtx, ty, dty, tz, dtz);
+    // the charge multiplies in FP64 (see k_spread)
+    const double qs = a.q[atom] * a.qscale;
+#pragma unroll
+    for (int i = 0; i < P; i++)
+#pragma unroll
+        for (int j = 0; j < P; j++) {
+            const R ab = tx[i] * ty[j];
+            unsigned long long* row = (unsigned long long*)a.qgrid + ((size_t)ix[i] * a.ky + iy[j]) * a.kz;
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                const long long qv = __double2ll_rn(qs * (double)(ab * tz[k]));
+                if (qv) atomicAdd(row + iz[k], (unsigned long long)qv);
+            }
+        }
+}
+
+template <typename R, int P>
+__global__ void __launch_bounds__(128) k_gather_p(PmeArgs a)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.n) return;
+    const int atom = a.sorted ? a.sorted[s] : s;
+    R tx[P], dtx[P], ty[P], dty[P], tz[P], dtz[P];
+    int ix[P], iy[P], iz[P];
+    grid_point_p<R, P>(a, atom, ix, iy, iz, tx, dtx, ty, dty, tz, dtz);
+    const R* g = (const R*)a.rgrid;
+    R fx = 0, fy = 0, fz = 0;
+#pragma unroll
+    for (int i = 0; i < P; i++)
+#pragma unroll
+        for (int j = 0; j < P; j++) {
+            const R xij = dtx[i] * ty[j], yij = tx[i] * dty[j], zij = tx[i] * ty[j];
+            const R* row = g + ((size_t)ix[i] * a.ky + iy[j]) * a.kz;
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                const R term = row[iz[k]];
+                fx -= term * xij * tz[k];
+                fy -= term * yij * tz[k];
+                fz -= term * zij * dtz[k];
+            }
+        }
+    const double q = a.q[atom];
+    const int slot = a.sorted ? s : (a.slot_of ? a.slot_of[atom] : atom);
+    fixed_add3(a.facc + 3 * (size_t)slot, (double)fx * a.hxr * q, (double)fy * a.hyr * q,
+               (double)fz * a.hzr * q, a.scale, a.status);
+}
+
 template <typename R>
 static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches, int* erec_used, int stage)
 {
@@ -494,11 +606,19 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     *erec_used = 0;
     if (stage == kStageSpread) {
         cudaMemsetAsync(a.qgrid, 0, sizeof(long long) * nreal, s);
-        if (a.n > 0) { k_spread<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+        if (a.n > 0) {
+            if (a.order == 4) k_spread_p<R, 4><<<nb, 128, 0, s>>>(a);
+            else k_spread<R><<<nb, 128, 0, s>>>(a);
+            *launches += 1;
+        }
         return (int)cudaGetLastError();
     }
     if (stage == kStageGather) {
-        if (a.n > 0) { k_gather<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+        if (a.n > 0) {
+            if (a.order == 4) k_gather_p<R, 4><<<nb, 128, 0, s>>>(a);
+            else k_gather<R><<<nb, 128, 0, s>>>(a);
+            *launches += 1;
+        }
         return (int)cudaGetLastError();
     }
     if (stage == kStagePotential) {   // a.facc holds the double phi[N] output here
