@@ -271,7 +271,7 @@ void* pmgpu_batch_stream(pmgpu_batch* batch);
 typedef struct pmgpu_tuning {
     int chunk_entries;        /* cluster-list entries per chunk of pair work: 4..64 */
     int pair_blocks_per_sm;   /* resident blocks of the mixed pair kernel per SM: 0 (occupancy limit) or 1..8 */
-    int fft_lines;            /* lines per block of the strided PME FFT passes, at most: 1..16 */
+    int fft_lines;            /* lines per block of the strided PME FFT passes, at most: 1..16 (z passes: twice) */
     int pme_concurrent;       /* 1: PME on a second stream beside the pair kernels; 0: after them */
     double ms_per_eval;       /* pmgpu_autotune: the measured time of the chosen tuning */
 } pmgpu_tuning;

@@ -282,6 +282,7 @@ struct PassArgs {
 template <typename R, int MODE>
 __global__ void __launch_bounds__(256, 2) k_fft_pass(PassArgs pa)
 {
+    pdl_wait();
     typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* buf0 = (C*)smem_raw;
@@ -569,6 +570,7 @@ __global__ void __launch_bounds__(128) k_spread_p(PmeArgs a)
 template <typename R, int P>
 __global__ void __launch_bounds__(128) k_gather_p(PmeArgs a)
 {
+    pdl_wait();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.n) return;
     const int atom = a.sorted ? a.sorted[s] : s;
@@ -615,7 +617,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     }
     if (stage == kStageGather) {
         if (a.n > 0) {
-            if (a.order == 4) k_gather_p<R, 4><<<nb, 128, 0, s>>>(a);
+            if (a.order == 4) launch_pdl(k_gather_p<R, 4>, nb, 128, 0, s, a);
             else k_gather<R><<<nb, 128, 0, s>>>(a);
             *launches += 1;
         }
@@ -630,14 +632,22 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     make_plan(a.kx, px); make_plan(a.ky, py); make_plan(a.kz, pz);
     if (px.nrad < 0 || py.nrad < 0 || pz.nrad < 0) return (int)cudaErrorInvalidValue;
     const int threads = 256;
-    auto lines_for = [](int n) { int l = (16384 / (int)sizeof(C)) / n; return l < 1 ? 1 : (l > 32 ? 32 : l); };
+    // z lines per block: up to 16 KB of line data and twice the tuned line
+    // count of the strided passes (fewer lines: more, smaller blocks, for
+    // small grids that are latency-bound)
+    const int zmax = a.fft_lines > 0 ? 2 * std::min(a.fft_lines, 16) : 32;
+    auto lines_for = [zmax](int n) {
+        int l = (16384 / (int)sizeof(C)) / n;
+        l = std::min(l, zmax);
+        return l < 1 ? 1 : (l > 32 ? 32 : l);
+    };
     // z r2c
     {
         PassArgs pa; pa.a = a; pa.plan = pz; pa.lines = lines_for(a.kz); pa.ld = a.kz + 1; pa.sign = -1;
         pa.tw_off = a.twz; pa.erec_off = 0;
         int blocks = (a.kx * a.ky + pa.lines - 1) / pa.lines;
         size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
-        k_fft_pass<R, kModeZR2C><<<blocks, threads, sm, s>>>(pa);
+        launch_pdl(k_fft_pass<R, kModeZR2C>, blocks, threads, sm, s, pa);
     }
     // lines per CTA for the strided passes: 16 (128 B coalesced rows for
     // float2) unless two line buffers would exceed ~200 KB of shared memory
@@ -653,7 +663,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         pa.tw_off = a.twy; pa.erec_off = 0;
         int blocks = a.kx * ((a.kzh + tile - 1) / tile);
         size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
-        k_fft_pass<R, kModeY><<<blocks, threads, sm, s>>>(pa);
+        launch_pdl(k_fft_pass<R, kModeY>, blocks, threads, sm, s, pa);
     }
     // x forward + convolution + x inverse
     int xtile = tile_for(a.kx);
@@ -662,7 +672,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         PassArgs pa; pa.a = a; pa.plan = px; pa.lines = xtile; pa.ld = a.kx + 1; pa.sign = -1;
         pa.tw_off = a.twx; pa.erec_off = 0;
         size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
-        k_fft_pass<R, kModeXConv><<<xblocks, threads, sm, s>>>(pa);
+        launch_pdl(k_fft_pass<R, kModeXConv>, xblocks, threads, sm, s, pa);
     }
     // y inverse
     {
@@ -670,7 +680,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         pa.tw_off = a.twy; pa.erec_off = 0;
         int blocks = a.kx * ((a.kzh + tile - 1) / tile);
         size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
-        k_fft_pass<R, kModeY><<<blocks, threads, sm, s>>>(pa);
+        launch_pdl(k_fft_pass<R, kModeY>, blocks, threads, sm, s, pa);
     }
     // z c2r
     {
@@ -678,7 +688,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         pa.tw_off = a.twz; pa.erec_off = 0;
         int blocks = (a.kx * a.ky + pa.lines - 1) / pa.lines;
         size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
-        k_fft_pass<R, kModeZC2R><<<blocks, threads, sm, s>>>(pa);
+        launch_pdl(k_fft_pass<R, kModeZC2R>, blocks, threads, sm, s, pa);
     }
     *launches += 5;
     *erec_used = xblocks;
