@@ -39,7 +39,7 @@ FP32_LANES_PER_SM = 128
 N_SMS = 148
 # DRAM bytes (read + write) of one k_pair_mixed launch on this workload, from
 # the ncu capture summarised in profiles/k_pair_mixed_chain14281.md
-PAIR_DRAM_BYTES_PER_LAUNCH = 4_687_616
+PAIR_DRAM_BYTES_PER_LAUNCH = 4_994_304
 
 
 def parse():
@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extra", action="store_true",
                    help="skip the batched (96 boxes) and 1,000,000-atom measurements")
+    p.add_argument("--workload", default="chain14281", choices=["chain14281", "water1m"],
+                   help="water1m: only the 1,000,000-atom box (one GPU; --steps evaluations)")
     return p.parse_args()
 
 
@@ -205,6 +207,18 @@ def main():
     from protomol_b200 import _lib
     from protomol_b200 import forces as F
     from protomol_b200 import workloads
+    if args.workload == "water1m":              # the large-system configuration alone
+        torch.cuda.set_device(local)
+        if rank == 0:
+            m = measure_1m(local, torch, max(1, min(args.steps, 50)))
+            print(json.dumps({"metric": "force evals/s (cutoff+PME), 1,000,000 atoms", "value": m["mixed"]["evals_per_s"],
+                              "unit": "evals/s", "n_gpus": 1, "steps": max(1, min(args.steps, 50)),
+                              "ms_per_step": m["mixed"]["ms_per_step"], "higher_is_better": True, "data": "synthetic",
+                              "config": {"workload": m["workload"], "atoms": m["atoms"]}, "scale_1m": m}), flush=True)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
 
     torch.cuda.set_device(local)
     lib = _lib.load()
