@@ -322,6 +322,21 @@ int pmgpu_leapfrog_run(pmgpu_system* sys, int n_forces, pmgpu_force* const* forc
                        double* d_positions, double* d_velocities, double* d_forces, double* d_energies,
                        double timestep, int n_steps, unsigned flags);
 
+/* ImpulseIntegrator::run(n_steps) (integrators/ImpulseIntegrator.cpp,
+ * MTSIntegrator.cpp, StandardIntegrator.cpp:24-35) over an inner Leapfrog of
+ * `timestep` fs, without modifiers: per outer step a half kick with the slow
+ * forces (outer timestep = cyclelength * timestep), pmgpu_leapfrog_run of
+ * cyclelength steps with the fast forces, the slow forces at the new
+ * positions, a half kick.  On entry d_slow_forces / d_fast_forces hold the
+ * two groups' forces at d_positions; on return all of positions,
+ * velocities, forces and the two energy arrays (11 each) belong to the final
+ * positions (the reference adds both levels into one ScalarStructure: their
+ * sum).  Asynchronous on the system's stream, like pmgpu_leapfrog_run. */
+int pmgpu_impulse_run(pmgpu_system* sys, int n_slow, pmgpu_force* const* slow, int n_fast, pmgpu_force* const* fast,
+                      const double* d_mass, double* d_positions, double* d_velocities, double* d_slow_forces,
+                      double* d_fast_forces, double* d_slow_energies, double* d_fast_energies, double timestep,
+                      int cyclelength, int n_steps, unsigned flags);
+
 /* ---- diagnostics (parity tests) ----------------------------------------- */
 
 /* Cell of every atom from the GPU binning of the last evaluation, as

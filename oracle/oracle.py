@@ -363,3 +363,26 @@ def leapfrog(system, specs, velocities, timestep, steps, positions=None, forces=
     hk = 0.5 * timestep * INV_TIMEFACTOR
     v = v + (f * hk) / m
     return x, v, f, r
+
+
+def impulse(system, slow_specs, fast_specs, velocities, timestep, cyclelength, steps):
+    """ImpulseIntegrator::run(steps) over an inner Leapfrog of ``timestep``
+    without modifiers (StandardIntegrator.cpp:24-35, MTSIntegrator.cpp):
+    doHalfKick with the slow forces (h = 0.5 (cyclelength dt) / T), the
+    inner LeapfrogIntegrator::run(cyclelength) on the fast forces,
+    calculateForces of the slow group, doHalfKick.  Returns (positions,
+    velocities, slow forces, fast forces, total potential energy)."""
+    x = np.array(system.positions, np.float64)
+    v = np.array(velocities, np.float64)
+    m = np.asarray(system.mass, np.float64)[:, None]
+    rs = evaluate(system, slow_specs, positions=x)
+    rf = evaluate(system, fast_specs, positions=x)
+    fs, ff = rs["forces"], rf["forces"]
+    h = 0.5 * (cyclelength * timestep) * INV_TIMEFACTOR
+    for _ in range(steps):
+        v = v + (fs * h) / m
+        x, v, ff, rf = leapfrog(system, fast_specs, v, timestep, cyclelength, positions=x, forces=ff)
+        rs = evaluate(system, slow_specs, positions=x)
+        fs = rs["forces"]
+        v = v + (fs * h) / m
+    return x, v, fs, ff, rs["lennard_jones"] + rs["coulomb"] + rf["lennard_jones"] + rf["coulomb"]

@@ -29,7 +29,7 @@ EXPORTS = [
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
     "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
     "pmgpu_full_create", "pmgpu_get_tuning", "pmgpu_set_tuning", "pmgpu_autotune", "pmgpu_batch_autotune",
-    "pmgpu_leapfrog_run", "pmgpu_hessian",
+    "pmgpu_leapfrog_run", "pmgpu_hessian", "pmgpu_impulse_run",
 ]
 PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
 
@@ -118,6 +118,8 @@ def load():
     lib.pmgpu_autotune.argtypes = [vp, C.c_int, C.POINTER(vp), vp, C.c_uint, C.c_int, C.POINTER(Tuning)]
     lib.pmgpu_batch_autotune.argtypes = [vp, C.c_int, C.POINTER(Tuning)]
     lib.pmgpu_hessian.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp]
+    lib.pmgpu_impulse_run.argtypes = [vp, C.c_int, C.POINTER(vp), C.c_int, C.POINTER(vp), vp, vp, vp, vp, vp, vp, vp,
+                                      C.c_double, C.c_int, C.c_int, C.c_uint]
     lib.pmgpu_leapfrog_run.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp, vp, vp, vp, C.c_double, C.c_int,
                                        C.c_uint]
     _lib = lib

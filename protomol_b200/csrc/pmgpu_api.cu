@@ -143,11 +143,18 @@ struct pmgpu_system {
     int topo_version = 0;
     int buf_version = 0;               // bumped when a per-evaluation buffer moves
     pmgpu_tuning tuning = {16, 0, 16, 1, 0.0};   // launch shapes (pmgpu_set_tuning, pmgpu_autotune)
-    // CUDA graph of the last evaluation (replayed when the key matches)
+    // CUDA graphs of the last few distinct evaluations (force groups,
+    // buffers, flags), replayed when the key matches; the least recently
+    // used is replaced (a multiple-time-step integrator alternates groups)
     bool use_graphs = true;
-    cudaGraphExec_t graph_exec = nullptr;
-    GraphKey graph_key;
-    long long graph_launches = 0;
+    struct GraphEntry {
+        GraphKey key;
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;
+        unsigned long long last_use = 0;
+    };
+    std::vector<GraphEntry> graphs;
+    unsigned long long graph_clock = 0;
     // profiling
     bool profiling = false;
     std::vector<cudaEvent_t> prof_pool;
@@ -296,7 +303,8 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     std::set<pmgpu_force*> live;
     live.swap(sys->forces);
     for (pmgpu_force* f : live) free_force(f);
-    if (sys->graph_exec) cudaGraphExecDestroy(sys->graph_exec);
+    for (auto& g : sys->graphs) cudaGraphExecDestroy(g.exec);
+    sys->graphs.clear();
     for (cudaEvent_t e : sys->prof_pool) cudaEventDestroy(e);
     free_atom_buffers(sys);
     dfree(sys->d_counts); dfree(sys->d_start); dfree(sys->d_erec);
@@ -397,7 +405,8 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     CK(cudaStreamSynchronize(sys->stream), "set_topology");
     free_atom_buffers(sys);
     sys->topo_version++;
-    if (sys->graph_exec) { cudaGraphExecDestroy(sys->graph_exec); sys->graph_exec = nullptr; }
+    for (auto& g : sys->graphs) cudaGraphExecDestroy(g.exec);
+    sys->graphs.clear();
     sys->n = n_atoms; sys->t = n_types; sys->e = n_excl; sys->csf = coulomb_scaling_factor;
     sys->q.assign(scaled_charge, scaled_charge + n_atoms);
     sys->binned = false;
@@ -1382,8 +1391,11 @@ static int eval_core(pmgpu_system* sys, int nf_in, pmgpu_force* const* forces_in
     key.pos = d_pos; key.fout = d_fout; key.energy = d_energy; key.flags = flags;
     key.box_version = sys->box_version; key.topo_version = sys->topo_version; key.buf_version = sys->buf_version;
     cudaStream_t s = sys->stream;
-    if (!(sys->graph_exec && key == sys->graph_key)) {
-        if (sys->graph_exec) { cudaGraphExecDestroy(sys->graph_exec); sys->graph_exec = nullptr; }
+    pmgpu_system::GraphEntry* hit = nullptr;
+    for (auto& g : sys->graphs)
+        if (g.key == key) { hit = &g; break; }
+    if (!hit) {
+        const size_t kGraphCache = 4;
         long long l0 = sys->launches;
         CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
         r = eval_enqueue(sys, nf, forces, d_pos, d_fout, d_energy, flags);
@@ -1391,15 +1403,28 @@ static int eval_core(pmgpu_system* sys, int nf_in, pmgpu_force* const* forces_in
         cudaError_t e = cudaStreamEndCapture(s, &graph);
         if (r) { if (graph) cudaGraphDestroy(graph); return r; }
         if (e != cudaSuccess) return cuda_fail(sys, e, "graph capture");
-        e = cudaGraphInstantiate(&sys->graph_exec, graph, 0);
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
-        if (e != cudaSuccess) { sys->graph_exec = nullptr; return cuda_fail(sys, e, "graph instantiate"); }
-        sys->graph_launches = sys->launches - l0;
+        if (e != cudaSuccess) return cuda_fail(sys, e, "graph instantiate");
+        if (sys->graphs.size() >= kGraphCache) {    // replace the least recently used
+            auto lru = sys->graphs.begin();
+            for (auto it = sys->graphs.begin(); it != sys->graphs.end(); ++it)
+                if (it->last_use < lru->last_use) lru = it;
+            cudaGraphExecDestroy(lru->exec);
+            sys->graphs.erase(lru);
+        }
+        pmgpu_system::GraphEntry g;
+        g.key = key;
+        g.exec = exec;
+        g.launches = sys->launches - l0;
         sys->launches = l0;
-        sys->graph_key = key;
+        sys->graphs.push_back(g);
+        hit = &sys->graphs.back();
     }
-    CK(cudaGraphLaunch(sys->graph_exec, s), "graph launch");
-    sys->launches += sys->graph_launches;
+    hit->last_use = ++sys->graph_clock;
+    CK(cudaGraphLaunch(hit->exec, s), "graph launch");
+    sys->launches += hit->launches;
     return PMGPU_OK;
 }
 
@@ -2078,6 +2103,40 @@ extern "C" int pmgpu_leapfrog_run(pmgpu_system* sys, int n_forces, pmgpu_force* 
     int e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_forces, h, hk, kLeapfrogLast, s,
                             &sys->launches);
     if (e) return cuda_fail(sys, (cudaError_t)e, "leapfrog half kick");
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_impulse_run(pmgpu_system* sys, int n_slow, pmgpu_force* const* slow, int n_fast,
+                                 pmgpu_force* const* fast, const double* d_mass, double* d_positions,
+                                 double* d_velocities, double* d_slow_forces, double* d_fast_forces,
+                                 double* d_slow_energies, double* d_fast_energies, double timestep, int cyclelength,
+                                 int n_steps, unsigned flags)
+{
+    if (!sys || n_slow <= 0 || !slow || n_fast <= 0 || !fast || !d_mass || !d_positions || !d_velocities ||
+        !d_slow_forces || !d_fast_forces || !d_slow_energies || !d_fast_energies)
+        return PMGPU_ERR_ARG;
+    if (!(timestep > 0.0) || cyclelength < 1 || n_steps < 0)
+        return fail(sys, PMGPU_ERR_ARG, "timestep must be positive, cyclelength >= 1, steps >= 0");
+    cudaSetDevice(sys->device);
+    cudaStream_t s = sys->stream;
+    const size_t n3 = 3 * (size_t)sys->n;
+    // MTSIntegrator::getTimestep = cyclelength * the inner timestep; doHalfKick's step
+    const double h_half = 0.5 * ((double)cyclelength * timestep) * kInvTimeFactor;
+    for (int step = 0; step < n_steps; ++step) {
+        int e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_slow_forces, 0.0, h_half,
+                                kLeapfrogLast, s, &sys->launches);     // doHalfKick (a kick, no drift)
+        if (e) return cuda_fail(sys, (cudaError_t)e, "impulse half kick");
+        int r = pmgpu_leapfrog_run(sys, n_fast, fast, d_mass, d_positions, d_velocities, d_fast_forces,
+                                   d_fast_energies, timestep, cyclelength, flags);   // doDriftOrNextIntegrator
+        if (r) return r;
+        CK(cudaMemsetAsync(d_slow_forces, 0, sizeof(double) * n3, s), "memset");    // calculateForces
+        CK(cudaMemsetAsync(d_slow_energies, 0, sizeof(double) * kERec, s), "memset");
+        r = eval_core(sys, n_slow, slow, d_positions, d_slow_forces, d_slow_energies, flags);
+        if (r) return r;
+        e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_slow_forces, 0.0, h_half,
+                            kLeapfrogLast, s, &sys->launches);         // doHalfKick
+        if (e) return cuda_fail(sys, (cudaError_t)e, "impulse half kick");
+    }
     return PMGPU_OK;
 }
 

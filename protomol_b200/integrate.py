@@ -80,3 +80,52 @@ class Leapfrog:
         if self.flags & _lib.FLAG_VIRIAL:
             e.virial_tensor += v[2:11]
         return self.pos.cpu().numpy(), self.vel.cpu().numpy(), self.force.cpu().numpy(), e
+
+
+class Impulse:
+    """ImpulseIntegrator (integrators/ImpulseIntegrator.cpp) over an inner
+    Leapfrog, device-resident (pmgpu_impulse_run): the slow forces kick every
+    ``cyclelength`` inner steps of ``timestep`` fs, the fast forces drive the
+    inner Leapfrog.  ``initialize`` evaluates both groups at the starting
+    positions (the integrators' initializeForces)."""
+
+    def __init__(self, topo: F.Topology, slow, fast, positions, velocities, masses, timestep: float,
+                 cyclelength: int, device: int = 0, virial: bool = False):
+        import torch
+        self.topo, self.slow, self.fast = topo, list(slow), list(fast)
+        self.timestep, self.cyclelength = float(timestep), int(cyclelength)
+        self.flags = _lib.FLAG_VIRIAL if virial else 0
+        dev = torch.device(f"cuda:{device}")
+        self.pos = torch.tensor(np.ascontiguousarray(positions, np.float64), device=dev)
+        self.vel = torch.tensor(np.ascontiguousarray(velocities, np.float64), device=dev)
+        self.mass = torch.tensor(np.ascontiguousarray(masses, np.float64), device=dev)
+        self.f_slow, self.f_fast = torch.zeros_like(self.pos), torch.zeros_like(self.pos)
+        self.e_slow = torch.zeros(11, dtype=torch.float64, device=dev)
+        self.e_fast = torch.zeros(11, dtype=torch.float64, device=dev)
+        self._slow = (_VP * len(self.slow))(*[f.handle for f in self.slow])
+        self._fast = (_VP * len(self.fast))(*[f.handle for f in self.fast])
+        self.lib = _lib.load()
+
+    def initialize(self):
+        for arr, n, f, e in ((self._slow, len(self.slow), self.f_slow, self.e_slow),
+                             (self._fast, len(self.fast), self.f_fast, self.e_fast)):
+            f.zero_()
+            e.zero_()
+            F.check(self.lib.pmgpu_evaluate_device(self.topo.handle, n, arr, _VP(self.pos.data_ptr()),
+                                                   _VP(f.data_ptr()), _VP(e.data_ptr()), self.flags), self.topo.handle)
+        return self
+
+    def run(self, n_steps: int):
+        F.check(self.lib.pmgpu_impulse_run(
+            self.topo.handle, len(self.slow), self._slow, len(self.fast), self._fast, _VP(self.mass.data_ptr()),
+            _VP(self.pos.data_ptr()), _VP(self.vel.data_ptr()), _VP(self.f_slow.data_ptr()),
+            _VP(self.f_fast.data_ptr()), _VP(self.e_slow.data_ptr()), _VP(self.e_fast.data_ptr()),
+            self.timestep, self.cyclelength, int(n_steps), self.flags), self.topo.handle)
+        return self
+
+    def state(self):
+        """(positions, velocities, slow forces, fast forces, total potential energy)."""
+        F.check(self.lib.pmgpu_synchronize(self.topo.handle), self.topo.handle)
+        es, ef = self.e_slow.cpu().numpy(), self.e_fast.cpu().numpy()
+        return (self.pos.cpu().numpy(), self.vel.cpu().numpy(), self.f_slow.cpu().numpy(), self.f_fast.cpu().numpy(),
+                float(es[0] + es[1] + ef[0] + ef[1]))

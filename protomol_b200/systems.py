@@ -377,6 +377,15 @@ def oxygen_fluid_216(seed: int = 1) -> System:
         exclusion_check=np.zeros(0, np.int32), bonds=[], angles=[], dihedrals=[])
 
 
+def ionic_fluid_216(seed: int = 1, charge: float = 0.4) -> System:
+    """:func:`oxygen_fluid_216` with charges +-``charge`` e alternating
+    (neutral): a fluid with electrostatics and no molecules."""
+    import dataclasses
+    s = oxygen_fluid_216(seed)
+    q = np.where(np.arange(s.n_atoms) % 2 == 0, charge, -charge) * 18.2226123264
+    return dataclasses.replace(s, name="ionic216", scaled_charge=q)
+
+
 def chain_in_water_14281(seed: int = 2) -> System:
     """4,463 TIP3P waters + an 892-atom random-walk chain in a 52.3 A cube.
 

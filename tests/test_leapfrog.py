@@ -112,3 +112,47 @@ def test_mixed_precision_trajectory_conserves_energy_like_fp64():
     print(f"\ntotal energy range over 1000 steps: fp64 {drifts['fp64']:.4f}  mixed {drifts['mixed']:.4f} "
           f"kcal/mol (KE {ke0:.1f})")
     assert drifts["mixed"] <= 2.0 * drifts["fp64"] + 1e-3 * ke0
+
+
+# ---------------------------------------------------------------- Impulse (MTS)
+FAST = "LennardJones -switchingFunction C2 -algorithm NonbondedCutoff -switchon 8 -cutoff 9 -cutoff 9"
+SLOW = ("Coulomb -algorithm PMEwald -real -reciprocal -correction -interpolation BSpline -gridsize 20 20 20 "
+        "-cutoff 8.5 -alpha 0.35")
+
+
+@pytest.mark.gpu
+def test_impulse_matches_the_oracle():
+    """ImpulseIntegrator over Leapfrog, PME as the slow force: 10 outer steps
+    of 4 x 0.5 fs on the 216-particle ionic fluid, FP64 on the GPU against the
+    oracle's restatement."""
+    from protomol_b200 import systems
+    s = systems.ionic_fluid_216()
+    v = integrate.maxwell_boltzmann(s.mass, 300.0, seed=21)
+    slow, fast = [F.parse_definition(SLOW)], [F.parse_definition(FAST)]
+    x, v1, fs, ff, epot = oracle.impulse(s, slow, fast, v, 0.5, 4, 10)
+    topo = F.Topology(s)
+    imp = integrate.Impulse(topo, [F.ForceFactory.make(topo, SLOW, "fp64")], [F.ForceFactory.make(topo, FAST, "fp64")],
+                            s.positions, v, s.mass, 0.5, 4).initialize().run(10)
+    xg, vg, fsg, ffg, eg = imp.state()
+    print(f"\nimpulse 10 x 4 steps: |dx| {np.abs(xg - x).max():.2e} A  |dv| {np.abs(vg - v1).max():.2e}  "
+          f"dE {eg - epot:+.2e}")
+    assert np.abs(xg - x).max() <= 1e-10
+    assert np.abs(vg - v1).max() <= 1e-10 * np.abs(v1).max()
+    assert np.abs(fsg - fs).max() <= 1e-8 * np.sqrt((fs ** 2).sum(1).mean())
+    assert abs(eg - epot) <= 1e-9 * abs(epot)
+
+
+@pytest.mark.gpu
+def test_impulse_with_cyclelength_one_is_leapfrog_with_all_forces():
+    """One inner step per outer step: the same trajectory as a Leapfrog on
+    the sum of the two groups, up to the order of the kicks' additions."""
+    from protomol_b200 import systems
+    s = systems.ionic_fluid_216()
+    v = integrate.maxwell_boltzmann(s.mass, 300.0, seed=22)
+    topo = F.Topology(s)
+    slow, fast = F.ForceFactory.make(topo, SLOW, "fp64"), F.ForceFactory.make(topo, FAST, "fp64")
+    imp = integrate.Impulse(topo, [slow], [fast], s.positions, v, s.mass, 1.0, 1).initialize().run(20)
+    xi = imp.state()[0]
+    lf = integrate.Leapfrog(topo, [slow, fast], s.positions, v, s.mass, 1.0).initialize().run(20)
+    xl = lf.state()[0]
+    assert np.abs(xi - xl).max() <= 1e-9
