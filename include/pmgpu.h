@@ -56,6 +56,19 @@ extern "C" {
 #define PMGPU_POT_LENNARD_JONES 1     /* forces/LennardJonesForce.h:37-74 */
 #define PMGPU_POT_COULOMB 2           /* forces/CoulombForce.h:41-57 */
 #define PMGPU_POT_EWALD_REAL 3        /* forces/CoulombEwaldRealForce.h:45-73 */
+/* look-up-table potentials over base/LookUpTableBase.h (cubic Hermite in
+ * r^2, 2^PRE points per octave from 2^-4 A^2 to the octave holding rc^2).
+ * For these the term's sw is the TABULATED switching function and the pair
+ * applies UniversalSwitchingFunction with the table's cutoff
+ * (forces/oneAtomContraints.h:24-31); registered
+ * (factories/registerForceExemplarsCutoff.cpp:47-48,58,69,86,101,132-134):
+ *   LENNARD_JONES_TABLE + C2; COULOMB_TABLE + CUTOFF or SHIFT;
+ *   EWALD_REAL_TABLE + CUTOFF;
+ *   LENNARD_JONES (C1, C2, CUTOFF) + EWALD_REAL_TABLE;
+ *   LENNARD_JONES_TABLE + EWALD_REAL_TABLE or COULOMB_TABLE (SHIFT). */
+#define PMGPU_POT_LENNARD_JONES_TABLE 4   /* forces/LennardJonesTableForce.h:81-101, PRE 7 */
+#define PMGPU_POT_COULOMB_TABLE 5         /* forces/CoulombTableForce.h:83-108, PRE 6 */
+#define PMGPU_POT_EWALD_REAL_TABLE 6      /* forces/CoulombEwaldRealTableForce.h:85-107, PRE 6 */
 
 /* switching functions */
 #define PMGPU_SW_UNIVERSAL 0          /* topology/UniversalSwitchingFunction.h */
@@ -151,6 +164,18 @@ int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* e2, const d
 /* Replaces NonbondedCutoffForce::doMake (forces/NonbondedCutoffForce.h:119-123). */
 int pmgpu_cutoff_create(pmgpu_system* sys, const pmgpu_cutoff_params* params, pmgpu_force** out);
 
+/* The look-up table a table potential evaluates; host only, needs no GPU.
+ * Replaces the LookUpTableBase constructor of LennardJonesTableForce /
+ * CoulombTableForce / CoulombEwaldRealTableForce (base/LookUpTableBase.h:115-205)
+ * for the tabulated switching function sw (switchon, cutoff) and alpha: per
+ * entry 4 doubles per tabulated function (value, gradient, 2nd and 3rd
+ * interpolation coefficient; LennardJonesTable: the A part, then the B part),
+ * entries 2^PRE per octave of r^2 from 2^-4.  Writes at most cap doubles
+ * (table may be NULL) and returns the table's length, or -1 for a potential
+ * or switching function that is not a registered table. */
+long long pmgpu_lookup_table(int pot, int sw, double switchon, double cutoff, double alpha,
+                             double* table, long long cap);
+
 /* Replaces NonbondedSimpleFullSystemForce<OneAtomPair[Two]<Vacuum...>> made by
  * the factory (forces/NonbondedSimpleFullSystemForce.h:165-182,
  * factories/registerForceExemplarsSimpleFull.cpp:88-152): every pair once,
@@ -230,7 +255,8 @@ int pmgpu_last_error(pmgpu_system* sys, char* buf, int len);
  *               negative force Jacobian-vector product); PMGPU_ERR_UNSUPPORTED
  *               when a PME reciprocal or correction term is in the list;
  *   energies 2: the pair terms' LJ and Coulomb energies (a check).
- * Any output may be NULL. */
+ * Any output may be NULL.  PMGPU_ERR_UNSUPPORTED for a force with a table
+ * potential. */
 int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,
                   const double* v, double* dE_dq, double* dE_dlj, double* hv, double* energies);
 
@@ -299,7 +325,8 @@ int pmgpu_batch_autotune(pmgpu_batch* batch, int evals, pmgpu_tuning* best);
  * derivative of their energy at the host positions, row-major, added (+=)
  * to hessian.  The matrix the normal-mode integrators diagonalise
  * (NormalModeUtilities).  Up to 8,192 atoms (PMGPU_ERR_CAPACITY);
- * PMGPU_ERR_UNSUPPORTED for the PME reciprocal and correction terms. */
+ * PMGPU_ERR_UNSUPPORTED for the PME reciprocal and correction terms and for
+ * table potentials. */
 int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,
                   double* hessian);
 

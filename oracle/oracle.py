@@ -33,7 +33,8 @@ REF_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(BUILD, "libpmoracle.so")
 
 SW = {"Universal": 0, "Cutoff": 1, "C1": 2, "C2": 3, "Shift": 4}
-POT = {"LennardJones": 1, "Coulomb": 2, "CoulombEwaldReal": 3}
+POT = {"LennardJones": 1, "Coulomb": 2, "CoulombEwaldReal": 3,
+       "LennardJonesTable": 4, "CoulombTable": 5, "CoulombEwaldRealTable": 6}
 
 
 def build(force: bool = False) -> str:
@@ -91,7 +92,21 @@ def lib():
         _lib = C.CDLL(build())
         _lib.pmo_poly5.restype = C.c_double
         _lib.pmo_poly5.argtypes = [C.c_double]
+        _lib.pmo_lookup_table.restype = C.c_longlong
+        _lib.pmo_lookup_table.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                          C.c_void_p, C.c_longlong]
     return _lib
+
+
+def lookup_table(pot, sw, switchon, cutoff, alpha=0.0) -> np.ndarray:
+    """The LookUpTableBase table of a table potential (pmo_lookup_table)."""
+    p, s = POT[pot] if isinstance(pot, str) else pot, SW[sw] if isinstance(sw, str) else sw
+    n = lib().pmo_lookup_table(p, s, switchon, cutoff, alpha, None, 0)
+    if n < 0:
+        raise ValueError(f"{pot} is not a table potential")
+    out = np.zeros(n)
+    lib().pmo_lookup_table(p, s, switchon, cutoff, alpha, out.ctypes.data, n)
+    return out
 
 
 class _Keep:

@@ -280,7 +280,144 @@ typedef struct {
     double sh_c_2, sh_4c_2;                      /* Shift */
     int use, modify;
     double alpha, two_alpha_pi;                 /* EwaldReal */
+    /* table potentials: LookUpTableBase's table and hashing constants */
+    double* tab;
+    long long tab_first, tab_last;
+    int tab_step, tab_shift;
 } term_t;
+
+static void term_switch(const term_t* t, double d2, double* value, double* deriv);
+
+static int is_table(int pot)
+{
+    return pot == PMO_POT_LJ_TABLE || pot == PMO_POT_COULOMB_TABLE || pot == PMO_POT_EWALD_REAL_TABLE;
+}
+
+/* ---- look-up tables (base/LookUpTableBase.h) ---- */
+/* lowerboundExp2 (base/mathutilities.cpp:43-51) */
+static double lowerbound_exp2(double r)
+{
+    double res = 1.0;
+    while (res < r) res *= 2.0;
+    while (res > r) res /= 2.0;
+    return res;
+}
+
+static long long dbits(double x) { long long u; memcpy(&u, &x, 8); return u; }
+static double dfrombits(long long u) { double x; memcpy(&x, &u, 8); return x; }
+
+/* LookUpTableBase::expn: the biased binary exponent of lowerboundExp2(a) */
+static long long lut_expn(double a) { return dbits(lowerbound_exp2(a)) >> 52; }
+
+/* power<n> for the negative powers the tabulated functions use
+ * (base/mathutilities.h:72-94: square(power<n/2>) * power<n - 2 (n/2)>,
+ * C++ division truncating towards zero) */
+static double pw_m1(double x) { return 1. / x; }
+static double pw_m2(double x) { double y = pw_m1(x); return (y * y) * 1; }
+static double pw_m3(double x) { double y = pw_m1(x); return (y * y) * pw_m1(x); }
+static double pw_m4(double x) { double y = pw_m2(x); return (y * y) * 1; }
+static double pw_m6(double x) { double y = pw_m3(x); return (y * y) * 1; }
+static double pw_m7(double x) { double y = pw_m3(x); return (y * y) * pw_m1(x); }
+static double pw_m8(double x) { double y = pw_m4(x); return (y * y) * 1; }
+static double pw_m12(double x) { double y = pw_m6(x); return (y * y) * 1; }
+static double pw_m14(double x) { double y = pw_m7(x); return (y * y) * 1; }
+
+/* LookUpValues::assign of the three table potentials, lookUpExp = 2 (the
+ * table variable r is r^2, r1 = sqrt(r)):
+ * forces/LennardJonesTableForceBase.h:35-45, CoulombTableForceBase.h:33-39,
+ * CoulombEwaldRealTableForceBase.h:36-43 */
+static void lut_assign(int pot, double alpha, double r, double r1, double v, double d, double* val)
+{
+    if (pot == PMO_POT_LJ_TABLE) {
+        double e = pw_m12(r1);
+        double f = 12.0 * pw_m14(r1);
+        val[0] = e * v;
+        val[1] = -0.5 * (f * v - e * d);
+        e = -pw_m6(r1);
+        f = -6.0 * pw_m8(r1);
+        val[4] = e * v;
+        val[5] = -0.5 * (f * v - e * d);
+    } else if (pot == PMO_POT_COULOMB_TABLE) {
+        double e = pw_m1(r1);
+        double f = pw_m3(r1);
+        val[0] = e * v;
+        val[1] = -0.5 * (f * v - e * d);
+    } else {
+        double r2 = r;
+        double e = erfc(alpha * r1) / r1;
+        double f = (e + 2.0 * alpha / sqrt(PMO_PI) * exp(-alpha * alpha * r2)) / r2;
+        val[0] = e * v;
+        val[1] = -0.5 * (f * v - e * d);
+    }
+}
+
+/* LookUpTableBase(from = 0.1, to = rc^2, lookUpExp = 2, ...) constructor
+ * (base/LookUpTableBase.h:115-205) with the precision the registered
+ * templates use: PRE = 7 for LennardJonesTable, 6 for the Coulomb tables
+ * (factories/registerForceExemplarsCutoff.cpp:47-48,58,69).  The tabulated
+ * switching function is sw_term's. */
+static long long lut_build(int pot, const term_t* sw_term, double alpha, double to, double* out, long long cap,
+                           long long* first, long long* last, int* step, int* shift)
+{
+    const int pre = pot == PMO_POT_LJ_TABLE ? 7 : 6;
+    const int n = 1 << pre;
+    const int stp = (pot == PMO_POT_LJ_TABLE ? 2 : 1) * 4;
+    double from = 0.1;
+    const long long octaves = lut_expn(to) + 1 - lut_expn(from);
+    const long long size = (octaves * n + 1) * stp;
+    if (out == NULL || size > cap) return size;
+    *shift = 52 - pre;
+    *first = (dbits(lowerbound_exp2(from)) >> *shift) * stp;
+    *last = octaves * n * stp;
+    *step = stp;
+    from = lowerbound_exp2(from);
+    for (long long i = 0; i < size / stp; ++i) {
+        double base = from * (double)(1 << (i / n));
+        double del = base / (double)n;
+        double r = base + del * (double)(i % n);
+        double r1 = sqrt(r);
+        double v, d;
+        term_switch(sw_term, r, &v, &d);
+        lut_assign(pot, alpha, r, r1, v, d, out + i * stp);
+        for (int j = 0; j < stp; j += 4) { out[2 + i * stp + j] = 0.0; out[3 + i * stp + j] = 0.0; }
+        if (i > 0) {
+            double x = from * (double)(1 << ((i - 1) / n)) / (double)n;
+            double* t = out + (i - 1) * stp;
+            for (int j = 0; j < stp; j += 4) {
+                double v1 = t[0 + j], g1 = t[1 + j], v2 = t[0 + stp + j], g2 = t[1 + stp + j];
+                double c = (3.0 * (v2 - v1) - x * (2.0 * g1 + g2)) / (x * x);
+                double dd = (-2.0 * (v2 - v1) + x * (g1 + g2)) / (x * x * x);
+                for (int k = 0; k < 2; ++k) {
+                    double dv = (v1 - v2) + ((dd * x + c) * x + g1) * x;
+                    double dg = (g1 - g2) + (3.0 * dd * x + 2.0 * c) * x;
+                    c -= (3.0 * dv - x * dg) / (x * x);
+                    dd -= (-2.0 * dv + x * dg) / (x * x * x);
+                }
+                t[2 + j] = c;
+                t[3 + j] = dd;
+            }
+        }
+    }
+    return size;
+}
+
+/* LookUpTableBase::index and ::interpolate (base/LookUpTableBase.h:243-272):
+ * the entry from the top bits of r^2's representation, the remainder dt */
+static void lut_index(const term_t* t, double r2, long long* i, double* dt)
+{
+    long long u = dbits(r2);
+    *i = (u >> t->tab_shift) * t->tab_step - t->tab_first;
+    *dt = 0.0;
+    if (*i < 0) *i = 0;
+    else if (*i > t->tab_last) *i = t->tab_last;
+    else *dt = r2 - dfrombits(u & ~((1LL << t->tab_shift) - 1LL));
+}
+
+static void lut_interpolate(double a, double b, double c, double d, double dt, double* energy, double* force)
+{
+    *energy = ((dt * d + c) * dt + b) * dt + a;
+    *force = -2.0 * ((3.0 * dt * d + 2.0 * c) * dt + b);
+}
 
 static void term_init(term_t* t, int pot, int sw, double on, double cut, double alpha)
 {
@@ -307,6 +444,28 @@ static void term_init(term_t* t, int pot, int sw, double on, double cut, double 
     }
     t->alpha = alpha;
     t->two_alpha_pi = 2.0 * alpha / sqrt(PMO_PI);
+    if (is_table(pot)) {
+        /* the pair applies UniversalSwitchingFunction and tests the table's
+         * cutoff (Cutoff<true>, forces/oneAtomContraints.h:24-31;
+         * OneAtomPair.h:141) */
+        long long n = lut_build(pot, t, alpha, t->cut2, NULL, 0, NULL, NULL, NULL, NULL);
+        t->tab = (double*)malloc(sizeof(double) * (size_t)n);
+        lut_build(pot, t, alpha, t->cut2, t->tab, n, &t->tab_first, &t->tab_last, &t->tab_step, &t->tab_shift);
+        t->sw = PMO_SW_UNIVERSAL;
+        t->use = 1;
+        t->modify = 0;
+    }
+}
+
+long long pmo_lookup_table(int pot, int sw, double switchon, double cutoff, double alpha,
+                           double* table, long long cap)
+{
+    if (!is_table(pot)) return -1;
+    term_t t;
+    term_init(&t, PMO_POT_NONE, sw, switchon, cutoff, alpha);
+    long long first, last;
+    int step, shift;
+    return lut_build(pot, &t, alpha, t.cut2, table, cap, &first, &last, &step, &shift);
 }
 
 /* Switching functions: value and derivOverD as in the reference operator()s. */
@@ -375,6 +534,29 @@ static void term_potential(const term_t* t, const pmo_system* s, int i, int j, i
         double e = qq * exp(-ar * ar);
         *energy = pmo_poly5(ar) * e * rr;
         *force = ((*energy + t->two_alpha_pi * e) * rr * rr);
+    } else if (t->pot == PMO_POT_LJ_TABLE) {
+        /* LennardJonesTableForce::operator() (forces/LennardJonesTableForce.h:81-101) */
+        const double* p = s->lj + 4 * ((size_t)s->type[i] * s->n_types + s->type[j]);
+        double A = (excl != PMO_EXCL_MODIFIED ? p[0] : p[2]);
+        double B = (excl != PMO_EXCL_MODIFIED ? p[1] : p[3]);
+        long long k;
+        double dt;
+        lut_index(t, d2, &k, &dt);
+        const double* T = t->tab + k;
+        double a = T[0] * A + T[4] * B;
+        double b = T[1] * A + T[5] * B;
+        double c = T[2] * A + T[6] * B;
+        double d = T[3] * A + T[7] * B;
+        lut_interpolate(a, b, c, d, dt, energy, force);
+    } else if (t->pot == PMO_POT_COULOMB_TABLE || t->pot == PMO_POT_EWALD_REAL_TABLE) {
+        /* CoulombTableForce::operator() (forces/CoulombTableForce.h:83-108),
+         * CoulombEwaldRealTableForce::operator() (CoulombEwaldRealTableForce.h:85-107) */
+        double q = s->q[i] * s->q[j] * ((s->csf != 1.0 && excl == PMO_EXCL_MODIFIED) ? s->csf : 1.0);
+        long long k;
+        double dt;
+        lut_index(t, d2, &k, &dt);
+        const double* T = t->tab + k;
+        lut_interpolate(T[0] * q, T[1] * q, T[2] * q, T[3] * q, dt, energy, force);
     } else {
         *energy = 0.0; *force = 0.0;
     }
@@ -430,7 +612,7 @@ static void one_atom_pair(pair_ctx* c, int i, int j)
         }
     }
     for (int k = 0; k < c->n_terms; ++k) {
-        if (c->t[k].pot == PMO_POT_LJ) c->r->lennard_jones += e[k];
+        if (c->t[k].pot == PMO_POT_LJ || c->t[k].pot == PMO_POT_LJ_TABLE) c->r->lennard_jones += e[k];
         else c->r->coulomb += e[k];
     }
     double ftot = c->n_terms > 1 ? (f[0] + f[1]) : f[0];
@@ -462,6 +644,11 @@ static void pair_ctx_init(pair_ctx* c, const pmo_system* s, const pmo_cutoff_par
         if (c->t[k].modify) c->any_modify = 1;
     }
     c->cut2 = cut2;
+}
+
+static void pair_ctx_free(pair_ctx* c)
+{
+    for (int k = 0; k < 2; ++k) { free(c->t[k].tab); c->t[k].tab = NULL; }
 }
 
 int pmo_cell_assign(const pmo_system* s, int* cells, int* dims)
@@ -512,6 +699,7 @@ int pmo_cutoff_force(const pmo_system* s, const pmo_cutoff_params* p,
     free(deltas);
     free(ex.e);
     cells_free(&c);
+    pair_ctx_free(&pc);
     return 0;
 }
 
@@ -527,6 +715,7 @@ int pmo_simple_full_force(const pmo_system* s, const pmo_cutoff_params* p,
         for (int j = i + 1; j < s->n_atoms; ++j)
             one_atom_pair(&pc, i, j);
     free(ex.e);
+    pair_ctx_free(&pc);
     return 0;
 }
 
@@ -978,8 +1167,9 @@ int pmo_pair_hessian(const pmo_system* s, const pmo_cutoff_params* p, int vacuum
     pair_ctx pc;
     pair_ctx_init(&pc, s, p);
     for (int k = 0; k < p->n_terms; ++k) {
-        if (pc.t[k].pot != PMO_POT_LJ && pc.t[k].pot != PMO_POT_COULOMB) return -1;
-        if (pc.t[k].sw != PMO_SW_UNIVERSAL && pc.t[k].sw != PMO_SW_C1 && pc.t[k].sw != PMO_SW_C2) return -1;
+        int bad = (pc.t[k].pot != PMO_POT_LJ && pc.t[k].pot != PMO_POT_COULOMB) ||
+                  (pc.t[k].sw != PMO_SW_UNIVERSAL && pc.t[k].sw != PMO_SW_C1 && pc.t[k].sw != PMO_SW_C2);
+        if (bad) { pair_ctx_free(&pc); return -1; }
     }
     pbc_t b;
     if (!vacuum) pbc_set(&b, s->box);

@@ -23,7 +23,12 @@ enum { PMO_EXCL_NONE = 0, PMO_EXCL_MODIFIED = 1, PMO_EXCL_FULL = 2 };
 
 /* pair potentials (forces/LennardJonesForce.h, CoulombForce.h,
  * CoulombEwaldRealForce.h) */
-enum { PMO_POT_NONE = 0, PMO_POT_LJ = 1, PMO_POT_COULOMB = 2, PMO_POT_EWALD_REAL = 3 };
+enum { PMO_POT_NONE = 0, PMO_POT_LJ = 1, PMO_POT_COULOMB = 2, PMO_POT_EWALD_REAL = 3,
+       /* look-up-table potentials (forces/LennardJonesTableForce.h,
+        * CoulombTableForce.h, CoulombEwaldRealTableForce.h over
+        * base/LookUpTableBase.h): sw is the tabulated switching function,
+        * the pair itself is Universal with the table's cutoff */
+       PMO_POT_LJ_TABLE = 4, PMO_POT_COULOMB_TABLE = 5, PMO_POT_EWALD_REAL_TABLE = 6 };
 
 /* switching functions (topology/C1SwitchingFunction.h, C2..., Cutoff...,
  * Shift...); UNIVERSAL = no
@@ -103,6 +108,14 @@ int pmo_simple_full_force(const pmo_system* s, const pmo_cutoff_params* p,
  * vacuum (plain differences) or periodic (minimal image); H +=.  Returns -1
  * for terms without a Hessian block there. */
 int pmo_pair_hessian(const pmo_system* s, const pmo_cutoff_params* p, int vacuum, double* H);
+
+/* One LookUpTableBase of a table potential over r^2 in [2^floor(log2 0.1),
+ * the octave holding rc^2]: values per entry (4 per tabulated function: value,
+ * gradient, 2nd and 3rd interpolation coefficients); entries = 2 for
+ * LennardJonesTable (A and B parts), 1 otherwise.  Returns the number of
+ * doubles written to table (at most cap), -1 for a bad term. */
+long long pmo_lookup_table(int pot, int sw, double switchon, double cutoff, double alpha,
+                           double* table, long long cap);
 
 /* The poly5 erfc approximation (base/mathutilities.cpp:29-40). */
 double pmo_poly5(double ar);

@@ -43,6 +43,9 @@ using namespace ProtoMol::Report;
 #include "NonbondedPMEwaldSystemForce.h"
 #include "OneAtomPair.h"
 #include "OneAtomPairTwo.h"
+#include "LennardJonesTableForce.h"
+#include "CoulombTableForce.h"
+#include "CoulombEwaldRealTableForce.h"
 #include "LennardJonesForce.h"
 #include "CoulombForce.h"
 #include "CoulombEwaldRealForce.h"
@@ -143,6 +146,20 @@ template <> LennardJonesForce make_pot<LennardJonesForce>(const Term&) { return 
 template <> CoulombForce make_pot<CoulombForce>(const Term&) { return CoulombForce(); }
 template <> CoulombEwaldRealForce make_pot<CoulombEwaldRealForce>(const Term& t) { return CoulombEwaldRealForce(t.alpha); }
 
+// the registered look-up-table potentials (factories/registerForceExemplarsCutoff.cpp:47-48,58,69):
+// the term's switching function is the tabulated one; the pair applies Universal
+typedef LennardJonesTableForce<C2SwitchingFunction, 7, Real> LJTableC2;
+typedef CoulombTableForce<CutoffSwitchingFunction, 6, Real> CoulombTableCutoff;
+typedef CoulombTableForce<ShiftSwitchingFunction, 6, Real> CoulombTableShift;
+typedef CoulombEwaldRealTableForce<CutoffSwitchingFunction, 6, Real> EwaldRealTableCutoff;
+template <> LJTableC2 make_pot<LJTableC2>(const Term& t) { return LJTableC2(C2SwitchingFunction(t.on, t.rc)); }
+template <> CoulombTableCutoff make_pot<CoulombTableCutoff>(const Term& t) { return CoulombTableCutoff(CutoffSwitchingFunction(t.rc)); }
+template <> CoulombTableShift make_pot<CoulombTableShift>(const Term& t) { return CoulombTableShift(ShiftSwitchingFunction(t.rc)); }
+template <> EwaldRealTableCutoff make_pot<EwaldRealTableCutoff>(const Term& t)
+{
+    return EwaldRealTableCutoff(CutoffSwitchingFunction(t.rc), t.alpha);
+}
+
 template <class SW1, class P1>
 static SystemForce* cut1(const Term& a, double algo)
 {
@@ -175,6 +192,9 @@ static SystemForce* make_cut(const std::vector<Term>& t, double algo)
         ONE(Shift, CoulombForce, 4, 2) ONE(Cutoff, CoulombEwaldRealForce, 1, 3)
         ONE(C1, LennardJonesForce, 2, 1) ONE(C2, LennardJonesForce, 3, 1)
         ONE(Cutoff, LennardJonesForce, 1, 1) ONE(Shift, LennardJonesForce, 4, 1)
+        // table potentials: pot 4 LennardJonesTable, 5 CoulombTable, 6 CoulombEwaldRealTable
+        ONE(Universal, LJTableC2, 3, 4) ONE(Universal, CoulombTableCutoff, 1, 5)
+        ONE(Universal, CoulombTableShift, 4, 5) ONE(Universal, EwaldRealTableCutoff, 1, 6)
 #undef ONE
     } else if (t.size() == 2) {
         const Term& a = t[0];
@@ -186,6 +206,17 @@ static SystemForce* make_cut(const std::vector<Term>& t, double algo)
         TWO(C2, C1, CoulombForce, 3, 2, 2) TWO(C2, Cutoff, CoulombEwaldRealForce, 3, 1, 3)
         TWO(C2, Cutoff, CoulombForce, 3, 1, 2) TWO(C2, Shift, CoulombForce, 3, 4, 2)
         TWO(Cutoff, Cutoff, CoulombEwaldRealForce, 1, 1, 3) TWO(C2, C2, CoulombForce, 3, 3, 2)
+        // LennardJones + CoulombEwaldRealTable (registerForceExemplarsCutoff.cpp:86,101,132)
+        if (a.pot == 1 && b.pot == 6 && b.sw == 1) {
+            if (a.sw == 2) return cut2<SWC(C1), LennardJonesForce, SWC(Universal), EwaldRealTableCutoff>(a, b, algo);
+            if (a.sw == 3) return cut2<SWC(C2), LennardJonesForce, SWC(Universal), EwaldRealTableCutoff>(a, b, algo);
+            if (a.sw == 1) return cut2<SWC(Cutoff), LennardJonesForce, SWC(Universal), EwaldRealTableCutoff>(a, b, algo);
+        }
+        // LennardJonesTable + CoulombEwaldRealTable / CoulombTable (:133-134)
+        if (a.pot == 4 && a.sw == 3 && b.pot == 6 && b.sw == 1)
+            return cut2<SWC(Universal), LJTableC2, SWC(Universal), EwaldRealTableCutoff>(a, b, algo);
+        if (a.pot == 4 && a.sw == 3 && b.pot == 5 && b.sw == 4)
+            return cut2<SWC(Universal), LJTableC2, SWC(Universal), CoulombTableShift>(a, b, algo);
 #undef TWO
     }
     return NULL;

@@ -14,7 +14,8 @@ PMGPU_OK = 0
 ERRORS = {1: "PMGPU_ERR_ARG", 2: "PMGPU_ERR_CUDA", 3: "PMGPU_ERR_OVERFLOW", 4: "PMGPU_ERR_STATE",
           5: "PMGPU_ERR_UNSUPPORTED", 6: "PMGPU_ERR_NOMEM", 7: "PMGPU_ERR_CAPACITY"}
 
-POT = {"LennardJones": 1, "Coulomb": 2, "CoulombEwaldReal": 3}
+POT = {"LennardJones": 1, "Coulomb": 2, "CoulombEwaldReal": 3,
+       "LennardJonesTable": 4, "CoulombTable": 5, "CoulombEwaldRealTable": 6}
 SW = {"Universal": 0, "Cutoff": 1, "C1": 2, "C2": 3, "Shift": 4}
 PRECISION = {"mixed": 0, "fp64": 1}
 FLAG_VIRIAL = 1
@@ -28,7 +29,7 @@ EXPORTS = [
     "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
     "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
-    "pmgpu_full_create", "pmgpu_get_tuning", "pmgpu_set_tuning", "pmgpu_autotune", "pmgpu_batch_autotune",
+    "pmgpu_full_create", "pmgpu_lookup_table", "pmgpu_get_tuning", "pmgpu_set_tuning", "pmgpu_autotune", "pmgpu_batch_autotune",
     "pmgpu_leapfrog_run", "pmgpu_hessian", "pmgpu_impulse_run",
 ]
 PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
@@ -113,6 +114,8 @@ def load():
     lib.pmgpu_batch_stream.restype = vp
     lib.pmgpu_adjoint.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]
     lib.pmgpu_full_create.argtypes = [vp, C.POINTER(CutoffParams), C.POINTER(vp)]
+    lib.pmgpu_lookup_table.restype = C.c_longlong
+    lib.pmgpu_lookup_table.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, vp, C.c_longlong]
     lib.pmgpu_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
     lib.pmgpu_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
     lib.pmgpu_autotune.argtypes = [vp, C.c_int, C.POINTER(vp), vp, C.c_uint, C.c_int, C.POINTER(Tuning)]

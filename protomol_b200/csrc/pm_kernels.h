@@ -55,6 +55,11 @@ struct TermF {
     float sh_a_lo, sh_b_lo;
     float alpha, two_alpha_pi;             // EwaldReal
     float alpha_lo, two_alpha_pi_lo;
+    // table potentials: the FP32 copy of the look-up table (tab_step floats
+    // per entry), hashed on the top bits of the FP32 r^2 (tab_shift = 23 -
+    // PRE); tab_first and tab_last are float offsets
+    const float* tab;
+    int tab_step, tab_first, tab_last, tab_shift;
 };
 
 struct TermD {
@@ -63,6 +68,11 @@ struct TermD {
     double c1_15_1, c1_05_3, c1_15_3;
     double sh_a, sh_b;
     double alpha, two_alpha_pi;
+    // table potentials: LookUpTableBase's FP64 table, hashed on the top
+    // bits of the FP64 r^2 (tab_shift = 52 - PRE); double offsets
+    const double* tab;
+    int tab_step, tab_last, tab_shift;
+    long long tab_first;
 };
 
 struct PairArgs {

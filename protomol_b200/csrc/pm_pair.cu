@@ -54,24 +54,39 @@ struct Combo { int n, p0, s0, p1, s1; };
 #define SC2 PMGPU_SW_C2
 #define SSH PMGPU_SW_SHIFT
 #define SUN PMGPU_SW_UNIVERSAL
+#define LJT PMGPU_POT_LENNARD_JONES_TABLE
+#define COT PMGPU_POT_COULOMB_TABLE
+#define EWT PMGPU_POT_EWALD_REAL_TABLE
 // The registered periodic OneAtomPair[Two] templates
-// (factories/registerForceExemplarsCutoff.cpp:36-131) plus the fused
-// LennardJones Coulomb -switchingFunction C2 -switchingFunction C2.
+// (factories/registerForceExemplarsCutoff.cpp:36-137) plus the fused
+// LennardJones Coulomb -switchingFunction C2 -switchingFunction C2.  A table
+// potential's own switching function is inside its table; the pair applies
+// UniversalSwitchingFunction to it (combos 17-24).
 static const Combo kCombos[] = {
     {1, CO, SC1, NP, SUN}, {1, CO, SC2, NP, SUN}, {1, CO, SCUT, NP, SUN}, {1, CO, SSH, NP, SUN},
     {1, EW, SCUT, NP, SUN}, {1, LJ, SC1, NP, SUN}, {1, LJ, SC2, NP, SUN}, {1, LJ, SCUT, NP, SUN},
     {1, LJ, SSH, NP, SUN},
     {2, LJ, SC1, EW, SCUT}, {2, LJ, SC1, CO, SSH}, {2, LJ, SC2, CO, SC1}, {2, LJ, SC2, EW, SCUT},
     {2, LJ, SC2, CO, SCUT}, {2, LJ, SC2, CO, SSH}, {2, LJ, SCUT, EW, SCUT}, {2, LJ, SC2, CO, SC2},
+    {1, LJT, SUN, NP, SUN}, {1, COT, SUN, NP, SUN}, {1, EWT, SUN, NP, SUN},
+    {2, LJ, SC1, EWT, SUN}, {2, LJ, SC2, EWT, SUN}, {2, LJ, SCUT, EWT, SUN},
+    {2, LJT, SUN, EWT, SUN}, {2, LJT, SUN, COT, SUN},
 };
 constexpr int kNumCombos = sizeof(kCombos) / sizeof(kCombos[0]);
 
+__host__ __device__ constexpr bool pot_table(int p) { return p == LJT || p == COT || p == EWT; }
+// the ScalarStructure slot of a potential's energy
+__host__ __device__ constexpr bool pot_lj_slot(int p) { return p == LJ || p == LJT; }
+
 int pair_combo_id(int n_terms, const int* pot, const int* sw)
 {
+    // a table term's sw is the tabulated switching function
+    const int s0 = pot_table(pot[0]) ? SUN : sw[0];
+    const int s1 = n_terms > 1 && pot_table(pot[1]) ? SUN : (n_terms > 1 ? sw[1] : SUN);
     for (int k = 0; k < kNumCombos; ++k) {
         const Combo& c = kCombos[k];
         if (c.n != n_terms) continue;
-        if (c.p0 == pot[0] && c.s0 == sw[0] && (n_terms == 1 || (c.p1 == pot[1] && c.s1 == sw[1])))
+        if (c.p0 == pot[0] && c.s0 == s0 && (n_terms == 1 || (c.p1 == pot[1] && c.s1 == s1)))
             return k;
     }
     return -1;
@@ -79,6 +94,9 @@ int pair_combo_id(int n_terms, const int* pot, const int* sw)
 
 __host__ __device__ constexpr bool sw_modifies(int s) { return s == SC1 || s == SC2 || s == SSH; }
 __host__ __device__ constexpr bool pot_r2(int p) { return p == LJ || p == CO; }
+// the pair's rough cutoff test runs when a switching function is used or the
+// potential has its own cutoff (OneAtomPair.h:141, OneAtomPairTwo.h:145)
+__host__ __device__ constexpr bool term_cut(int p, int s) { return s != SUN || pot_table(p); }
 
 // ---------------------------------------------------------------- shared
 struct ItemGeom {
@@ -187,6 +205,34 @@ __device__ __forceinline__ void pot_f32(const PairArgs& p, const TermF& t, float
         float ex = qq * exp_neg(ar * ar);
         e = poly5f(ar) * ex * rinv;
         f = fmaf(t.two_alpha_pi, ex, fmaf(t.two_alpha_pi_lo, ex, e)) * rinv * rinv;
+    } else if (pot_table(POT)) {
+        // LookUpTableBase::index on the FP32 r^2 (its top exponent and PRE
+        // mantissa bits pick the entry) and the cubic of ::interpolate
+        // (base/LookUpTableBase.h:243-272) in FP32 on the FP32 copy of the
+        // table; out of range -> the first / last entry with dt = 0
+        const unsigned u = __float_as_uint(r2);
+        int k = (int)(u >> t.tab_shift) * t.tab_step - t.tab_first;
+        const bool clamp = k < 0 || k > t.tab_last;
+        k = k < 0 ? 0 : (k > t.tab_last ? t.tab_last : k);
+        const float dt = clamp ? 0.f : r2 - __uint_as_float(u & ~((1u << t.tab_shift) - 1u));
+        const float4* T = reinterpret_cast<const float4*>(t.tab + k);
+        float a, b, c, d;
+        if (POT == LJT) {
+            // A part and B part of the entry; compensated A, B
+            const float4* tab = excl == PMGPU_EXCL_MODIFIED ? p.ljm : p.ljn;
+            const float4 par = __ldg(tab + (ti * p.n_types + tj));   // A_hi, B_hi, A_lo, B_lo
+            const float4 ta = __ldg(T), tb = __ldg(T + 1);
+            a = fmaf(par.x, ta.x, par.z * ta.x) + fmaf(par.y, tb.x, par.w * tb.x);
+            b = fmaf(par.x, ta.y, par.z * ta.y) + fmaf(par.y, tb.y, par.w * tb.y);
+            c = fmaf(par.x, ta.z, par.z * ta.z) + fmaf(par.y, tb.z, par.w * tb.z);
+            d = fmaf(par.x, ta.w, par.z * ta.w) + fmaf(par.y, tb.w, par.w * tb.w);
+        } else {
+            const float q = (p.csfd != 1.0 && excl == PMGPU_EXCL_MODIFIED) ? qq * p.csf : qq;
+            const float4 tc = __ldg(T);
+            a = tc.x * q; b = tc.y * q; c = tc.z * q; d = tc.w * q;
+        }
+        e = fmaf(fmaf(fmaf(dt, d, c), dt, b), dt, a);
+        f = -2.0f * fmaf(fmaf(3.0f * dt, d, 2.0f * c), dt, b);
     } else {
         e = 0.f; f = 0.f;
     }
@@ -269,6 +315,35 @@ __device__ __forceinline__ void pot_f64(const PairArgs& p, const TermD& t, doubl
         double poly = tt * (E1 + tt * (E2 + tt * (E3 + tt * (E4 + tt * E5))));
         e = poly * ex * rr;
         f = ((e + t.two_alpha_pi * ex) * rr * rr);
+    } else if (pot_table(POT)) {
+        // LookUpTableBase::index / ::interpolate (base/LookUpTableBase.h:243-272)
+        // with LennardJonesTableForce::operator() (forces/LennardJonesTableForce.h:81-101),
+        // CoulombTableForce::operator() (CoulombTableForce.h:83-108) and
+        // CoulombEwaldRealTableForce::operator() (CoulombEwaldRealTableForce.h:85-107)
+        const long long u = __double_as_longlong(d2);
+        long long k = (u >> t.tab_shift) * t.tab_step - t.tab_first;
+        double dt = 0.0;
+        if (k < 0) k = 0;
+        else if (k > t.tab_last) k = t.tab_last;
+        else dt = d2 - __longlong_as_double(u & ~((1ll << t.tab_shift) - 1ll));
+        const double4* T = reinterpret_cast<const double4*>(t.tab + k);
+        double a, b, c, d;
+        if (POT == LJT) {
+            const double4 par = p.ljd[(size_t)ti * p.n_types + tj];
+            const double A = excl != PMGPU_EXCL_MODIFIED ? par.x : par.z;
+            const double B = excl != PMGPU_EXCL_MODIFIED ? par.y : par.w;
+            const double4 ta = T[0], tb = T[1];
+            a = ta.x * A + tb.x * B;
+            b = ta.y * A + tb.y * B;
+            c = ta.z * A + tb.z * B;
+            d = ta.w * A + tb.w * B;
+        } else {
+            const double q = qi * qj * ((p.csfd != 1.0 && excl == PMGPU_EXCL_MODIFIED) ? p.csfd : 1.0);
+            const double4 tc = T[0];
+            a = tc.x * q; b = tc.y * q; c = tc.z * q; d = tc.w * q;
+        }
+        e = ((dt * d + c) * dt + b) * dt + a;
+        f = -2.0 * ((3.0 * dt * d + 2.0 * c) * dt + b);
     } else {
         e = 0.0; f = 0.0;
     }
@@ -310,7 +385,7 @@ template <int NT, int P0, int S0, int P1, int S1>
 __global__ void __launch_bounds__(128) k_pair_fp64(PairArgs p)
 {
     constexpr bool kMod = sw_modifies(S0) || (NT > 1 && sw_modifies(S1));
-    constexpr bool kUse = S0 != SUN || (NT > 1 && S1 != SUN);
+    constexpr bool kUse = term_cut(P0, S0) || (NT > 1 && term_cut(P1, S1));
     constexpr bool kR2 = pot_r2(P0) || (NT > 1 && pot_r2(P1));
     __shared__ double4 sjp[4][32];
     __shared__ int4 sjm[4][32];
@@ -371,8 +446,8 @@ __global__ void __launch_bounds__(128) k_pair_fp64(PairArgs p)
                             e1 = e1 * sv;
                         }
                     }
-                    if (P0 == LJ) acc[0] += e0; else acc[1] += e0;
-                    if (NT > 1) { if (P1 == LJ) acc[0] += e1; else acc[1] += e1; }
+                    if (pot_lj_slot(P0)) acc[0] += e0; else acc[1] += e0;
+                    if (NT > 1) { if (pot_lj_slot(P1)) acc[0] += e1; else acc[1] += e1; }
                     double ft = NT > 1 ? (f0 + f1) : f0;
                     double fx = dx * ft, fy = dy * ft, fz = dz * ft;
                     fix -= fx; fiy -= fy; fiz -= fz;
@@ -452,6 +527,14 @@ struct Dispatch;
     case 14: KERNEL<2, LJ, SC2, CO, SSH><<<blocks, 128, 0, s>>>(a); break;                              \
     case 15: KERNEL<2, LJ, SCUT, EW, SCUT><<<blocks, 128, 0, s>>>(a); break;                            \
     case 16: KERNEL<2, LJ, SC2, CO, SC2><<<blocks, 128, 0, s>>>(a); break;                              \
+    case 17: KERNEL<1, LJT, SUN, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                             \
+    case 18: KERNEL<1, COT, SUN, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                             \
+    case 19: KERNEL<1, EWT, SUN, NP, SUN><<<blocks, 128, 0, s>>>(a); break;                             \
+    case 20: KERNEL<2, LJ, SC1, EWT, SUN><<<blocks, 128, 0, s>>>(a); break;                             \
+    case 21: KERNEL<2, LJ, SC2, EWT, SUN><<<blocks, 128, 0, s>>>(a); break;                             \
+    case 22: KERNEL<2, LJ, SCUT, EWT, SUN><<<blocks, 128, 0, s>>>(a); break;                            \
+    case 23: KERNEL<2, LJT, SUN, EWT, SUN><<<blocks, 128, 0, s>>>(a); break;                            \
+    case 24: KERNEL<2, LJT, SUN, COT, SUN><<<blocks, 128, 0, s>>>(a); break;                            \
     default: return (int)cudaErrorInvalidValue;                                                        \
     }
 
@@ -515,6 +598,14 @@ int launch_pair_mixed(const PairArgs& a, int combo, cudaStream_t s, long long* l
     PM_MIXED_CASE(14, 2, LJ, SC2, CO, SSH)
     PM_MIXED_CASE(15, 2, LJ, SCUT, EW, SCUT)
     PM_MIXED_CASE(16, 2, LJ, SC2, CO, SC2)
+    PM_MIXED_CASE(17, 1, LJT, SUN, NP, SUN)
+    PM_MIXED_CASE(18, 1, COT, SUN, NP, SUN)
+    PM_MIXED_CASE(19, 1, EWT, SUN, NP, SUN)
+    PM_MIXED_CASE(20, 2, LJ, SC1, EWT, SUN)
+    PM_MIXED_CASE(21, 2, LJ, SC2, EWT, SUN)
+    PM_MIXED_CASE(22, 2, LJ, SCUT, EWT, SUN)
+    PM_MIXED_CASE(23, 2, LJT, SUN, EWT, SUN)
+    PM_MIXED_CASE(24, 2, LJT, SUN, COT, SUN)
 #undef PM_MIXED_CASE
     default: return (int)cudaErrorInvalidValue;
     }

@@ -307,8 +307,8 @@ __device__ __forceinline__ void pair_math(const PairArgs& p, const PairGeo& g, c
         }
     }
     float l = 0.f, c = 0.f;
-    if (P0 == LJ) l += e0; else c += e0;
-    if (NT > 1) { if (P1 == LJ) l += e1; else c += e1; }
+    if (pot_lj_slot(P0)) l += e0; else c += e0;
+    if (NT > 1) { if (pot_lj_slot(P1)) l += e1; else c += e1; }
     ft = g.act ? f0 + f1 : 0.f;
     el = g.act ? l : 0.f;
     ec = g.act ? c : 0.f;
@@ -338,8 +338,8 @@ __device__ __forceinline__ void pair_energy_f64(const PairArgs& p, int si, int s
             e1 *= sv;
         }
     }
-    el += (P0 == LJ ? e0 : 0.0) + (NT > 1 && P1 == LJ ? e1 : 0.0);
-    ec += (P0 != LJ ? e0 : 0.0) + (NT > 1 && P1 != LJ ? e1 : 0.0);
+    el += (pot_lj_slot(P0) ? e0 : 0.0) + (NT > 1 && pot_lj_slot(P1) ? e1 : 0.0);
+    ec += (!pot_lj_slot(P0) ? e0 : 0.0) + (NT > 1 && !pot_lj_slot(P1) ? e1 : 0.0);
 }
 
 // the warp's queued near pairs -> the near-pair list (called by the whole

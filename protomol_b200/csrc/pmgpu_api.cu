@@ -186,6 +186,8 @@ struct pmgpu_force {
     int wrap = 0;
     TermF tf[2];
     TermD td[2];
+    double* d_tab64[2] = {nullptr, nullptr};   // look-up tables of table potentials
+    float* d_tab32[2] = {nullptr, nullptr};
     double cut2 = 0.0;
     // PME
     double alpha = 0.0;
@@ -557,6 +559,159 @@ extern "C" int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* 
 }
 
 // ------------------------------------------------------------------ forces
+static bool pot_is_table(int pot)
+{
+    return pot == PMGPU_POT_LENNARD_JONES_TABLE || pot == PMGPU_POT_COULOMB_TABLE ||
+           pot == PMGPU_POT_EWALD_REAL_TABLE;
+}
+
+// the switching functions a table can hold, value and derivOverD
+// (C2SwitchingFunction.h:64-82, CutoffSwitchingFunction.h:64-68,
+// ShiftSwitchingFunction.h)
+static void host_switch(const TermD& t, double r2, double& v, double& d)
+{
+    if (t.sw == PMGPU_SW_C2) {
+        d = 0.0;
+        if (r2 > t.cut2) v = 0.0;
+        else if (r2 >= t.on2) {
+            double c2 = t.cut2 - r2;
+            double c4 = c2 * (t.s2 + 2.0 * r2);
+            v = t.s1 * (c2 * c4);
+            d = t.s3 * (c2 * c2 - c4);
+        } else v = 1.0;
+    } else if (t.sw == PMGPU_SW_SHIFT) {
+        if (r2 > t.cut2) { v = 0.0; d = 0.0; return; }
+        double x = 1.0 - r2 * t.sh_a;
+        v = x * x;
+        d = t.sh_b * x;
+    } else if (t.sw == PMGPU_SW_CUTOFF) {
+        d = 0.0;
+        v = r2 > t.cut2 ? 0.0 : 1.0;
+    } else {
+        v = 1.0; d = 0.0;
+    }
+}
+
+static double lowerbound_exp2(double r)      // base/mathutilities.cpp:43-51
+{
+    double res = 1.0;
+    while (res < r) res *= 2.0;
+    while (res > r) res /= 2.0;
+    return res;
+}
+
+static long long dbits(double x) { long long u; memcpy(&u, &x, 8); return u; }
+
+// square(power<n/2>(x)) * power<n - 2 (n/2)>(x) for the negative powers of
+// the tabulated functions (base/mathutilities.h:72-94)
+static double ipow_neg(double x, int n)
+{
+    if (n == -1) return 1. / x;
+    if (n == 0) return 1;
+    double h = ipow_neg(x, n / 2);
+    return (h * h) * ipow_neg(x, n - 2 * (n / 2));
+}
+
+// The look-up table of a table potential: LookUpTableBase(0.1, rc^2, 2,
+// LookUpValues, swf) (base/LookUpTableBase.h:115-205) with PRE 7 for
+// LennardJonesTable and 6 for the Coulomb tables (the registered templates,
+// factories/registerForceExemplarsCutoff.cpp:47-48,58,69), the values of
+// LookUpValues::assign (forces/LennardJonesTableForceBase.h:35-45,
+// CoulombTableForceBase.h:33-39, CoulombEwaldRealTableForceBase.h:36-43) and
+// the Hermite coefficients with their two refinement steps, in FP64 and the
+// reference's operation order, so the table is the reference's bit for bit.
+static std::vector<double> build_lookup_table(int pot, const TermD& sw, double alpha, int& pre, int& step,
+                                              long long& first, long long& last)
+{
+    pre = pot == PMGPU_POT_LENNARD_JONES_TABLE ? 7 : 6;
+    step = (pot == PMGPU_POT_LENNARD_JONES_TABLE ? 2 : 1) * 4;
+    const int n = 1 << pre;
+    double from = 0.1;
+    const long long octaves = (dbits(lowerbound_exp2(sw.cut2)) >> 52) + 1 - (dbits(lowerbound_exp2(from)) >> 52);
+    const long long entries = octaves * n + 1;
+    std::vector<double> t((size_t)(entries * step), 0.0);
+    first = (dbits(lowerbound_exp2(from)) >> (52 - pre)) * step;
+    last = (entries - 1) * step;
+    from = lowerbound_exp2(from);
+    for (long long i = 0; i < entries; ++i) {
+        double base = from * (double)(1 << (i / n));
+        double del = base / (double)n;
+        double r = base + del * (double)(i % n);
+        double r1 = std::sqrt(r);
+        double v, d;
+        host_switch(sw, r, v, d);
+        double* val = t.data() + i * step;
+        if (pot == PMGPU_POT_LENNARD_JONES_TABLE) {
+            double e = ipow_neg(r1, -12), f = 12.0 * ipow_neg(r1, -14);
+            val[0] = e * v;
+            val[1] = -0.5 * (f * v - e * d);
+            e = -ipow_neg(r1, -6); f = -6.0 * ipow_neg(r1, -8);
+            val[4] = e * v;
+            val[5] = -0.5 * (f * v - e * d);
+        } else if (pot == PMGPU_POT_COULOMB_TABLE) {
+            double e = ipow_neg(r1, -1), f = ipow_neg(r1, -3);
+            val[0] = e * v;
+            val[1] = -0.5 * (f * v - e * d);
+        } else {
+            double r2 = r;
+            double e = std::erfc(alpha * r1) / r1;
+            double f = (e + 2.0 * alpha / std::sqrt(kPi) * std::exp(-alpha * alpha * r2)) / r2;
+            val[0] = e * v;
+            val[1] = -0.5 * (f * v - e * d);
+        }
+        if (i == 0) continue;
+        const double x = from * (double)(1 << ((i - 1) / n)) / (double)n;
+        double* pv = t.data() + (i - 1) * step;
+        for (int j = 0; j < step; j += 4) {
+            const double v1 = pv[j], g1 = pv[j + 1], v2 = pv[j + step], g2 = pv[j + 1 + step];
+            double c = (3.0 * (v2 - v1) - x * (2.0 * g1 + g2)) / (x * x);
+            double dd = (-2.0 * (v2 - v1) + x * (g1 + g2)) / (x * x * x);
+            for (int it = 0; it < 2; ++it) {
+                double dv = (v1 - v2) + ((dd * x + c) * x + g1) * x;
+                double dg = (g1 - g2) + (3.0 * dd * x + 2.0 * c) * x;
+                c -= (3.0 * dv - x * dg) / (x * x);
+                dd -= (-2.0 * dv + x * dg) / (x * x * x);
+            }
+            pv[j + 2] = c;
+            pv[j + 3] = dd;
+        }
+    }
+    return t;
+}
+
+// uploads a table potential's table (FP64 and its FP32 rounding) and sets
+// the terms' look-up constants
+static cudaError_t table_setup(pmgpu_force* f, int k)
+{
+    int pre = 0, step = 0;
+    long long first = 0, last = 0;
+    std::vector<double> t = build_lookup_table(f->td[k].pot, f->td[k], f->td[k].alpha, pre, step, first, last);
+    std::vector<float> t32(t.size());
+    for (size_t i = 0; i < t.size(); ++i) t32[i] = (float)t[i];
+    cudaError_t e = dalloc(&f->d_tab64[k], t.size());
+    if (e == cudaSuccess) e = dalloc(&f->d_tab32[k], t.size());
+    if (e == cudaSuccess) e = cudaMemcpy(f->d_tab64[k], t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(f->d_tab32[k], t32.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+    TermD& d = f->td[k];
+    d.tab = f->d_tab64[k]; d.tab_step = step; d.tab_first = first; d.tab_last = (int)last; d.tab_shift = 52 - pre;
+    TermF& g = f->tf[k];
+    uint32_t ub;
+    const float from32 = 0.0625f;            // lowerboundExp2(0.1)
+    memcpy(&ub, &from32, 4);
+    g.tab = f->d_tab32[k]; g.tab_step = step; g.tab_shift = 23 - pre;
+    g.tab_first = (int)(ub >> g.tab_shift) * step; g.tab_last = (int)last;
+    return cudaSuccess;
+}
+
+static bool force_has_table(const pmgpu_force* f)
+{
+    if (f->kind != 0) return false;
+    for (int k = 0; k < f->cp.n_terms; ++k)
+        if (pot_is_table(f->cp.pot[k])) return true;
+    return false;
+}
+
 static void term_setup(const pmgpu_cutoff_params* p, int k, TermF& f, TermD& d)
 {
     memset(&f, 0, sizeof(f));
@@ -608,8 +763,14 @@ extern "C" int pmgpu_cutoff_create(pmgpu_system* sys, const pmgpu_cutoff_params*
             return fail(sys, PMGPU_ERR_ARG, "C2 switching function: 0 <= switchon < cutoff");
         if (p->sw[k] != PMGPU_SW_UNIVERSAL && !(p->cutoff[k] > 0.0))
             return fail(sys, PMGPU_ERR_ARG, "switching function cutoff > 0");
-        if (p->pot[k] == PMGPU_POT_EWALD_REAL && !(p->alpha[k] > 0.0))
+        if ((p->pot[k] == PMGPU_POT_EWALD_REAL || p->pot[k] == PMGPU_POT_EWALD_REAL_TABLE) && !(p->alpha[k] > 0.0))
             return fail(sys, PMGPU_ERR_ARG, "CoulombEwaldReal -alpha > 0");
+        // the tabulated switching functions of the registered table templates
+        const int pk = p->pot[k], sk = p->sw[k];
+        if ((pk == PMGPU_POT_LENNARD_JONES_TABLE && sk != PMGPU_SW_C2) ||
+            (pk == PMGPU_POT_COULOMB_TABLE && sk != PMGPU_SW_CUTOFF && sk != PMGPU_SW_SHIFT) ||
+            (pk == PMGPU_POT_EWALD_REAL_TABLE && sk != PMGPU_SW_CUTOFF))
+            return fail(sys, PMGPU_ERR_UNSUPPORTED, "table potential with a switching function not registered for it");
     }
     if (!(p->algorithm_cutoff > 0.0)) return fail(sys, PMGPU_ERR_ARG, "NonbondedCutoff -cutoff > 0");
     int combo = pair_combo_id(p->n_terms, p->pot, p->sw);
@@ -623,14 +784,44 @@ extern "C" int pmgpu_cutoff_create(pmgpu_system* sys, const pmgpu_cutoff_params*
     double c2 = 0.0;
     for (int k = 0; k < p->n_terms; ++k) {
         term_setup(p, k, f->tf[k], f->td[k]);
-        // Cutoff<>::cutoff of each term is its switching function's cutoff^2;
-        // the pair test uses the largest (OneAtomPairTwo.h:48)
+        // Cutoff<>::cutoff of each term is its switching function's cutoff^2,
+        // a table potential's the tabulated one's; the pair test uses the
+        // largest (OneAtomPairTwo.h:48)
         c2 = std::max(c2, f->td[k].cut2);
+        if (pot_is_table(p->pot[k])) {
+            cudaSetDevice(sys->device);
+            cudaError_t e = table_setup(f, k);
+            if (e != cudaSuccess) {
+                free_force(f);
+                return cuda_fail(sys, e, "look-up table");
+            }
+        }
     }
     f->cut2 = c2;
     sys->forces.insert(f);
     *out = f;
     return PMGPU_OK;
+}
+
+extern "C" long long pmgpu_lookup_table(int pot, int sw, double switchon, double cutoff, double alpha,
+                                        double* table, long long cap)
+{
+    if (!pot_is_table(pot) || !(cutoff > 0.0) || cap < 0) return -1;
+    if ((pot == PMGPU_POT_LENNARD_JONES_TABLE && !(sw == PMGPU_SW_C2 && switchon >= 0.0 && switchon < cutoff)) ||
+        (pot == PMGPU_POT_COULOMB_TABLE && sw != PMGPU_SW_CUTOFF && sw != PMGPU_SW_SHIFT) ||
+        (pot == PMGPU_POT_EWALD_REAL_TABLE && (sw != PMGPU_SW_CUTOFF || !(alpha > 0.0))))
+        return -1;
+    pmgpu_cutoff_params p;
+    memset(&p, 0, sizeof(p));
+    p.n_terms = 1; p.pot[0] = pot; p.sw[0] = sw; p.switchon[0] = switchon; p.cutoff[0] = cutoff; p.alpha[0] = alpha;
+    TermF f;
+    TermD d;
+    term_setup(&p, 0, f, d);
+    int pre = 0, step = 0;
+    long long first = 0, last = 0;
+    std::vector<double> t = build_lookup_table(pot, d, alpha, pre, step, first, last);
+    if (table) memcpy(table, t.data(), sizeof(double) * (size_t)std::min<long long>(cap, (long long)t.size()));
+    return (long long)t.size();
 }
 
 // NonbondedSimpleFullSystemForce with VacuumBoundaryConditions
@@ -977,6 +1168,7 @@ static void free_force(pmgpu_force* f)
     if (f->d_rgrid) cudaFree(f->d_rgrid);
     if (f->d_tw) cudaFree(f->d_tw);
     dfree(f->d_bfac); dfree(f->d_efac);
+    for (int k = 0; k < 2; ++k) { dfree(f->d_tab64[k]); dfree(f->d_tab32[k]); }
     delete f;
 }
 
@@ -2048,6 +2240,8 @@ extern "C" int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const
             return fail(sys, PMGPU_ERR_UNSUPPORTED, "the Hessian of the PME reciprocal / correction terms is not "
                                                     "available (the real-space pairs are)");
         if (forces_in[k]->kind != 1) fl.push_back(forces_in[k]);
+        if (force_has_table(forces_in[k]))
+            return fail(sys, PMGPU_ERR_UNSUPPORTED, "no Hessian of a table potential");
     }
     if (sys->n > kHessianMaxAtoms) return fail(sys, PMGPU_ERR_CAPACITY, "dense Hessian above 8192 atoms");
     int r = eval_prepare(sys, (int)fl.size(), fl.data());
@@ -2174,6 +2368,9 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
         fl.push_back(forces_in[k]);
     }
     if (hv && !v) return fail(sys, PMGPU_ERR_ARG, "Hessian-vector product needs v");
+    for (pmgpu_force* f : fl)
+        if (force_has_table(f))
+            return fail(sys, PMGPU_ERR_UNSUPPORTED, "no adjoint of a table potential");
     for (pmgpu_force* f : fl)
         if (hv && f->kind == 1 && (f->pp.reciprocal || f->pp.correction))
             return fail(sys, PMGPU_ERR_UNSUPPORTED, "Hessian-vector product of the PME reciprocal / correction "

@@ -292,8 +292,14 @@ def lj_parameter_gradient(type_params, dE_dlj):
 # --------------------------------------------------------------------------
 # keyword parsing
 # --------------------------------------------------------------------------
-_POTENTIALS = ("LennardJones", "Coulomb", "CoulombEwaldReal")
+_POTENTIALS = ("LennardJones", "Coulomb", "CoulombEwaldReal",
+               "LennardJonesTable", "CoulombTable", "CoulombEwaldRealTable")
 _SWITCHES = ("Universal", "Cutoff", "C1", "C2", "Shift")
+# Table potentials (forces/*TableForce.h): the switching function is the
+# tabulated one and the pair applies Universal.  LennardJonesTable and
+# CoulombTable name it in their id; CoulombEwaldRealTable's is Cutoff and
+# hidden (CoulombEwaldRealTableForce.h:120-124).
+_TABLES = ("LennardJonesTable", "CoulombTable", "CoulombEwaldRealTable")
 
 
 @dataclass
@@ -309,7 +315,43 @@ def _switch_params(sw):
 
 
 def _pot_params(pot):
-    return [_Param("-alpha")] if pot == "CoulombEwaldReal" else []
+    return [_Param("-alpha")] if pot in ("CoulombEwaldReal", "CoulombEwaldRealTable") else []
+
+
+def _term_params(pot, sw):
+    """OneAtomPair::getParameters of one term: the potential's parameters,
+    then the switching function's.  A table potential's parameters are its
+    tabulated switching function's (its cutoff is that function's), then
+    -alpha (forces/CoulombEwaldRealTableForce.h:126-131); the pair's Universal
+    switch has none."""
+    if pot in _TABLES:
+        return _switch_params(sw) + _pot_params(pot)
+    return _pot_params(pot) + _switch_params(sw)
+
+
+def _term_values(pot, sw, vals, k):
+    """(switchon, cutoff, alpha, next k) from the parsed values of a term."""
+    alpha = on = rc = 0.0
+    if pot in ("CoulombEwaldReal",):
+        alpha = vals[k]; k += 1
+    if sw == "C2":
+        on, rc = vals[k], vals[k + 1]; k += 2
+    elif sw in ("C1", "Cutoff", "Shift"):
+        rc = vals[k]; k += 1
+    if pot == "CoulombEwaldRealTable":
+        alpha = vals[k]; k += 1
+    return on, rc, alpha, k
+
+
+def _assign_switches(names, sws):
+    """The -switchingFunction words of an id in term order: every term names
+    one except CoulombEwaldRealTable (tabulated Cutoff, hidden); None when the
+    count does not match."""
+    shown = [n != "CoulombEwaldRealTable" for n in names]
+    if sum(shown) != len(sws):
+        return None
+    it = iter(sws)
+    return [next(it) if s else "Cutoff" for s in shown]
 
 
 def _parse_values(tokens, params):
@@ -376,32 +418,27 @@ def parse_definition(definition: str) -> dict:
             rest.append(t)
         i += 1
     if algorithm == "NonbondedCutoff":
-        if not 1 <= len(names) <= 2 or len(sws) != len(names) or any(s not in _SWITCHES for s in sws):
+        term_sws = _assign_switches(names, sws) if 1 <= len(names) <= 2 else None
+        if term_sws is None or any(s not in _SWITCHES for s in term_sws):
             raise ValueError(f"Could not find a complete match for '{definition}'")
         params = []
-        for n, s in zip(names, sws):
+        for n, s in zip(names, term_sws):
             # OneAtomPair[Two]::getParameters order: force1, switch1, force2, switch2
-            params += _pot_params(n) + _switch_params(s)
+            params += _term_params(n, s)
         params.append(_Param("-cutoff"))
         vals = _parse_values(rest, params)
         if any(v is None for v in vals):
             raise ValueError(f"force {definition}: missing parameter(s)")
         vals = [float(v) for v in vals]
         terms, k = [], 0
-        for n, s in zip(names, sws):
-            alpha = on = rc = 0.0
-            if n == "CoulombEwaldReal":
-                alpha = vals[k]; k += 1
-            if s == "C2":
-                on, rc = vals[k], vals[k + 1]; k += 2
-            elif s in ("C1", "Cutoff", "Shift"):
-                rc = vals[k]; k += 1
+        for n, s in zip(names, term_sws):
+            on, rc, alpha, k = _term_values(n, s, vals, k)
             terms.append((s, n, on, rc, alpha))
         return {"kind": "cut", "terms": terms, "algo_cutoff": vals[k]}
     if algorithm == "NonbondedSimpleFull":
         # vacuum all pairs; a Universal switch is not written in the id, so
         # either every term names its switch or none does
-        if not 1 <= len(names) <= 2 or (sws and len(sws) != len(names)) or any(s not in _SWITCHES for s in sws):
+        if any(n in _TABLES for n in names) or not 1 <= len(names) <= 2 or (sws and len(sws) != len(names)) or any(s not in _SWITCHES for s in sws):
             raise ValueError(f"Could not find a complete match for '{definition}'")
         sws = sws or ["Universal"] * len(names)
         params = []
@@ -438,6 +475,18 @@ def parse_definition(definition: str) -> dict:
     raise ValueError(f"Could not find a complete match for '{definition}'")
 
 
+def cutoff_ident(terms) -> str:
+    """getIdNoAlias of a NonbondedCutoffSystemForce: OneAtomPair[Two]::getId
+    (forces/OneAtomPairTwo.h:97-106) -- the potentials' keywords, their own
+    (tabulated) switching functions, then the pair's switching functions
+    (Universal is not written) -- and the algorithm."""
+    heads = " ".join(t[1] for t in terms)
+    tails = "".join(f" -switchingFunction {t[0]}" for t in terms
+                    if t[1] in ("LennardJonesTable", "CoulombTable"))
+    outer = "".join(f" -switchingFunction {t[0]}" for t in terms if t[1] not in _TABLES)
+    return heads + tails + outer + " -algorithm NonbondedCutoff"
+
+
 class ForceFactory:
     """``ForceFactory::make`` for the GPU nonbonded forces."""
 
@@ -459,9 +508,7 @@ class ForceFactory:
             cp.algorithm_cutoff = spec["algo_cutoff"]
             cp.precision = prec
             check(lib.pmgpu_cutoff_create(topo.handle, C.byref(cp), C.byref(h)), topo.handle)
-            ident = (" ".join(t[1] for t in spec["terms"]) +
-                     "".join(f" -switchingFunction {t[0]}" for t in spec["terms"]) + " -algorithm NonbondedCutoff")
-            return NonbondedCutoffSystemForce(topo, h, ident, spec)
+            return NonbondedCutoffSystemForce(topo, h, cutoff_ident(spec["terms"]), spec)
         if spec["kind"] == "full":
             cp = _lib.CutoffParams()
             cp.n_terms = len(spec["terms"])

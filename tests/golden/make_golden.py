@@ -1,6 +1,6 @@
 """Generates the golden fixtures in this directory from the REFERENCE itself.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 
 Needs oracle/_ref/pmref (built from the ProtoMol sources by
 ``make -C oracle/ref``), i.e. it runs where the reference sources exist.  For
@@ -31,6 +31,12 @@ from protomol_b200 import systems, workloads  # noqa: E402
 def cases():
     """name -> (system factory, [force definitions], store all forces)"""
     small = lambda: systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+
+    def small_csf():             # coulombScalingFactor 1: the 1-4 pairs unscaled
+        s = small()
+        s.csf = 1.0
+        return s
+
     wb = lambda: systems.water_box(100, seed=7)
     alpha_s = 0.35
     return {
@@ -54,6 +60,27 @@ def cases():
                                          "-cutoff 9"], False),
         "small_pme_default_alpha": (small, ["Coulomb -algorithm PMEwald -reciprocal -correction -interpolation BSpline "
                                             "-gridsize 25 27 30 -cutoff 9"], False),
+        # look-up-table potentials (registerForceExemplarsCutoff.cpp:47-48,58,69,86,101,132-134)
+        "small_table_lj_c2": (small, ["LennardJonesTable -switchingFunction C2 -algorithm NonbondedCutoff "
+                                      "-switchon 7 -cutoff 9 -cutoff 9"], False),
+        "small_table_coulomb_shift": (small, ["CoulombTable -switchingFunction Shift -algorithm NonbondedCutoff "
+                                              "-cutoff 9 -cutoff 9"], False),
+        "small_csf1_table_coulomb_cutoff": (small_csf, ["CoulombTable -switchingFunction Cutoff -algorithm "
+                                                       "NonbondedCutoff -cutoff 9 -cutoff 9"], False),
+        "small_table_ewald": (small, ["CoulombEwaldRealTable -algorithm NonbondedCutoff -cutoff 9 -alpha 0.35 "
+                                      "-cutoff 9"], False),
+        "small_table_c2lj_ewald": (small, ["LennardJones CoulombEwaldRealTable -switchingFunction C2 -algorithm "
+                                           "NonbondedCutoff -switchon 7 -cutoff 10 -cutoff 8.5 -alpha 0.35 "
+                                           "-cutoff 10"], False),
+        "small_csf1_table_c1lj_ewald": (small_csf, ["LennardJones CoulombEwaldRealTable -switchingFunction C1 "
+                                                   "-algorithm NonbondedCutoff -cutoff 9 -cutoff 9 -alpha 0.35 "
+                                                   "-cutoff 9"], False),
+        "small_table_ljt_ewald": (small, ["LennardJonesTable CoulombEwaldRealTable -switchingFunction C2 "
+                                          "-algorithm NonbondedCutoff -switchon 8 -cutoff 9 -cutoff 10 -alpha 0.3 "
+                                          "-cutoff 10"], False),
+        "small_table_ljt_coult": (small, ["LennardJonesTable CoulombTable -switchingFunction C2 -switchingFunction "
+                                          "Shift -algorithm NonbondedCutoff -switchon 1 -cutoff 9 -cutoff 9.5 "
+                                          "-cutoff 9.5"], False),
         "smallbox_wrap": (wb, workloads.water_box_workload(100, 7).forces, True),
     }
 
@@ -62,10 +89,12 @@ def pos_sha(s) -> str:
     return hashlib.sha256(np.ascontiguousarray(s.positions).tobytes()).hexdigest()[:16]
 
 
-def main():
+def main(only=()):
     if not oracle.reference_available():
         raise SystemExit("oracle/_ref/pmref missing: make -C oracle/ref")
     for name, (factory, defs, full) in cases().items():
+        if only and name not in only:
+            continue
         s = factory()
         specs = [F.parse_definition(d) for d in defs]
         r = oracle.run_reference(s, specs)
@@ -82,4 +111,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))     # names of the cases to regenerate (default: all)

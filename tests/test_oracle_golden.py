@@ -19,7 +19,10 @@ def _case_system(name):
         return systems.water_box_216()
     if name == "smallbox_wrap":
         return systems.water_box(100, seed=7)
-    return systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+    s = systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+    if "_csf1" in name:
+        s.csf = 1.0
+    return s
 
 
 CASES = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
@@ -50,7 +53,8 @@ def test_oracle_matches_reference_golden(name):
 def test_cutoff_cases_are_bit_exact_with_reference_golden():
     """Without an FFT in the path the restatement reproduces the reference
     bit for bit."""
-    for name in ("water216_c2", "small_c2lj_c1coul", "small_c2_fused", "small_cutoff_coulomb"):
+    for name in ["water216_c2", "small_c2lj_c1coul", "small_c2_fused", "small_cutoff_coulomb"] + \
+            [c for c in CASES if "table" in c]:
         g = np.load(os.path.join(GOLDEN, name + ".npz"))
         s = _case_system(name)
         r = oracle.evaluate(s, [F.parse_definition(str(d)) for d in g["definitions"]])
