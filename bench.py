@@ -343,6 +343,7 @@ def main():
         if rank == 0:
             extra["scale_1m"] = measure_1m(local, torch, 10)
             extra["leapfrog"] = measure_leapfrog(local, torch)
+            extra["table_potentials"] = measure_table(local, torch, flush, 200)
     if rank == 0:
         value = world * 1000.0 / t_local
         line = {
@@ -475,6 +476,57 @@ def measure_leapfrog(local, torch, steps=1000):
         ms = a.elapsed_time(b)
         out[prec] = {"ms_per_step": ms / steps, "steps_per_s": steps * 1000.0 / ms}
         topo.close()
+    return out
+
+
+def measure_table(local, torch, flush, steps):
+    """The 14,281-atom system with the Ewald real part tabulated
+    (LennardJones CoulombEwaldRealTable, the look-up table of
+    CoulombEwaldRealTableForce) beside the analytic form, both with the PME
+    reciprocal + correction force: evaluations/s per precision, L2 flushed
+    between evaluations, CUDA events on the system's stream."""
+    from protomol_b200 import forces as F
+    from protomol_b200 import workloads
+    lib = _lib_load()
+    w = workloads.chain14281()
+    s = w.system
+    n = s.n_atoms
+    table = ("LennardJones CoulombEwaldRealTable -switchingFunction C2 -algorithm NonbondedCutoff "
+             "-switchon 10 -cutoff 12 -cutoff 12 -alpha 0.32 -cutoff 12")
+    out = {"workload": "14,281-atom chain in water, LJ C2 10->12 + Ewald real 12 (analytic or tabulated) "
+                       "+ PME 64^3", "atoms": n, "table_definition": table}
+    dpos = torch.tensor(s.positions, dtype=torch.float64, device=f"cuda:{local}")
+    dfor = torch.zeros((n, 3), dtype=torch.float64, device=f"cuda:{local}")
+    den = torch.zeros(11, dtype=torch.float64, device=f"cuda:{local}")
+    VP = C.c_void_p
+    for form, cut in (("analytic", w.forces[0]), ("table", table)):
+        for prec in ("mixed", "fp64"):
+            topo = F.Topology(s, device=local)
+            stream = torch.cuda.ExternalStream(topo.stream)
+            fs = [F.ForceFactory.make(topo, d, prec) for d in (cut, w.forces[1])]
+            arr = (VP * len(fs))(*[f.handle for f in fs])
+            topo.autotune(fs, s.positions, evals=20)
+
+            def step():
+                lib.pmgpu_evaluate_device(topo.handle, len(fs), arr, VP(dpos.data_ptr()), VP(dfor.data_ptr()),
+                                          VP(den.data_ptr()), 1)
+            for _ in range(3):
+                step()
+            torch.cuda.synchronize()
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(steps)]
+            with torch.cuda.stream(stream):
+                for a, b in evs:
+                    flush.zero_()                  # L2 flush, outside the timed events
+                    a.record(stream)
+                    step()
+                    b.record(stream)
+            torch.cuda.synchronize()
+            ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+            out.setdefault(form, {})[prec] = {"ms_per_eval": ms, "evals_per_s": 1000.0 / ms}
+            for f in fs:
+                f.close()
+            topo.close()
     return out
 
 

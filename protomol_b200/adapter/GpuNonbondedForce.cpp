@@ -13,11 +13,14 @@ using namespace ProtoMol::Report;
 #include "C2SwitchingFunction.h"
 #include "CellListEnumerator_periodicBoundaries.h"
 #include "CoulombEwaldRealForce.h"
+#include "CoulombEwaldRealTableForce.h"
 #include "CoulombForce.h"
+#include "CoulombTableForce.h"
 #include "CubicCellManager.h"
 #include "CutoffSwitchingFunction.h"
 #include "ForceFactory.h"
 #include "LennardJonesForce.h"
+#include "LennardJonesTableForce.h"
 #include "NonbondedCutoffSystemForce.h"
 #include "NonbondedPMEwaldSystemForce.h"
 #include "OneAtomPair.h"
@@ -26,6 +29,7 @@ using namespace ProtoMol::Report;
 #include "ScalarStructure.h"
 #include "ShiftSwitchingFunction.h"
 #include "Topology.h"
+#include "UniversalSwitchingFunction.h"
 #include "Vector3DBlock.h"
 
 namespace ProtoMol
@@ -182,9 +186,14 @@ namespace ProtoMol
 			for (int t = 0; t < myTerms; ++t) {
 				cp.pot[t] = myPot[t];
 				cp.sw[t] = mySw[t];
+				// a table potential's parameters are its tabulated switching
+				// function's, then -alpha (CoulombEwaldRealTableForce.h:126-131);
+				// the pair's Universal switch has none
+				const bool table = myPot[t] >= PMGPU_POT_LENNARD_JONES_TABLE;
 				if (myPot[t] == PMGPU_POT_EWALD_REAL) cp.alpha[t] = real_of(par[k++]);
 				if (mySw[t] == PMGPU_SW_C2) { cp.switchon[t] = real_of(par[k++]); cp.cutoff[t] = real_of(par[k++]); }
 				else if (mySw[t] != PMGPU_SW_UNIVERSAL) cp.cutoff[t] = real_of(par[k++]);
+				if (table && myPot[t] == PMGPU_POT_EWALD_REAL_TABLE) cp.alpha[t] = real_of(par[k++]);
 			}
 			cp.algorithm_cutoff = real_of(par[k]);
 			cp.precision = myPrecision;
@@ -257,6 +266,26 @@ namespace ProtoMol
 			0, 2, p, s, GpuNonbondedForce::defaultPrecision()));
 	}
 
+	// a table potential: its tabulated switching function is sw; the pair is Universal
+	template <class P>
+	static void reg1t(int pot, int sw)
+	{
+		int p[1] = {pot}, s[1] = {sw};
+		ForceFactory::registerExemplar(new GpuNonbondedForce(
+			new NonbondedCutoffSystemForce<CubicCellManager, OneAtomPair<PBC, UniversalSwitchingFunction, P>>(), 0, 1,
+			p, s, GpuNonbondedForce::defaultPrecision()));
+	}
+
+	template <class SW1, class P1, class P2>
+	static void reg2t(int pot1, int sw1, int pot2, int sw2)
+	{
+		int p[2] = {pot1, pot2}, s[2] = {sw1, sw2};
+		ForceFactory::registerExemplar(new GpuNonbondedForce(
+			new NonbondedCutoffSystemForce<CubicCellManager,
+			                               OneAtomPairTwo<PBC, SW1, P1, UniversalSwitchingFunction, P2>>(),
+			0, 2, p, s, GpuNonbondedForce::defaultPrecision()));
+	}
+
 	template <bool REAL, bool RECIP, bool CORR>
 	static void regpme(const std::vector<std::string>& aliases)
 	{
@@ -279,6 +308,24 @@ namespace ProtoMol
 		reg1<C2SwitchingFunction, LennardJonesForce>(LJ, C2);
 		reg1<CutoffSwitchingFunction, LennardJonesForce>(LJ, CUT);
 		reg1<ShiftSwitchingFunction, LennardJonesForce>(LJ, SH);
+		// look-up-table potentials (registerForceExemplarsCutoff.cpp:47-48,58,69)
+		typedef LennardJonesTableForce<C2SwitchingFunction, 7, Real> LJT;
+		typedef CoulombTableForce<CutoffSwitchingFunction, 6, Real> COTC;
+		typedef CoulombTableForce<ShiftSwitchingFunction, 6, Real> COTS;
+		typedef CoulombEwaldRealTableForce<CutoffSwitchingFunction, 6, Real> EWT;
+		const int LJTP = PMGPU_POT_LENNARD_JONES_TABLE, COTP = PMGPU_POT_COULOMB_TABLE;
+		const int EWTP = PMGPU_POT_EWALD_REAL_TABLE;
+		reg1t<COTC>(COTP, CUT);
+		reg1t<COTS>(COTP, SH);
+		reg1t<EWT>(EWTP, CUT);
+		reg1t<LJT>(LJTP, C2);
+		// LennardJones + CoulombEwaldRealTable (:86,101,132), LennardJonesTable
+		// + CoulombEwaldRealTable / CoulombTable (:133-134)
+		reg2t<C1SwitchingFunction, LennardJonesForce, EWT>(LJ, C1, EWTP, CUT);
+		reg2t<C2SwitchingFunction, LennardJonesForce, EWT>(LJ, C2, EWTP, CUT);
+		reg2t<CutoffSwitchingFunction, LennardJonesForce, EWT>(LJ, CUT, EWTP, CUT);
+		reg2t<UniversalSwitchingFunction, LJT, EWT>(LJTP, C2, EWTP, CUT);
+		reg2t<UniversalSwitchingFunction, LJT, COTS>(LJTP, C2, COTP, SH);
 		// registerForceExemplarsCutoff.cpp:76-131 (LennardJones + Coulomb-type pairs)
 		reg2<C1SwitchingFunction, CutoffSwitchingFunction, CoulombEwaldRealForce>(C1, CUT, EW);
 		reg2<C1SwitchingFunction, ShiftSwitchingFunction, CoulombForce>(C1, SH, CO);

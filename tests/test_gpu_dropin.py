@@ -60,3 +60,29 @@ def test_force_factory_keywords_run_on_the_gpu(case, precision):
     tol_f, tol_e = (1e-9, 1e-10) if precision == "fp64" else (1e-5, 2e-6)
     assert err <= tol_f
     assert abs(r["lennard_jones"] + r["coulomb"] - ref["lennard_jones"] - ref["coulomb"]) <= tol_e * scale
+
+
+TABLE_DEFS = [
+    "LennardJonesTable -switchingFunction C2 -algorithm NonbondedCutoff -switchon 7 -cutoff 9 -cutoff 9",
+    "CoulombTable -switchingFunction Shift -algorithm NonbondedCutoff -cutoff 9 -cutoff 9",
+    "CoulombEwaldRealTable -algorithm NonbondedCutoff -cutoff 9 -alpha 0.35 -cutoff 9",
+    "LennardJones CoulombEwaldRealTable -switchingFunction C2 -algorithm NonbondedCutoff -switchon 7 -cutoff 10 "
+    "-cutoff 8.5 -alpha 0.35 -cutoff 10",
+    "LennardJonesTable CoulombTable -switchingFunction C2 -switchingFunction Shift -algorithm NonbondedCutoff "
+    "-switchon 1 -cutoff 9 -cutoff 9.5 -cutoff 9.5",
+]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("definition", TABLE_DEFS)
+def test_table_force_keywords_run_on_the_gpu(definition, precision):
+    """Table potentials made by ProtoMol's ForceFactory from their own ids."""
+    system = systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+    r = run_driver(system, [definition], precision)
+    ref = oracle.evaluate(system, [F.parse_definition(definition)])
+    assert r["made"][0] == F.cutoff_ident(F.parse_definition(definition)["terms"])
+    err = np.sqrt(((r["forces"] - ref["forces"]) ** 2).sum() / (ref["forces"] ** 2).sum())
+    scale = abs(ref["lennard_jones"]) + abs(ref["coulomb"])
+    tol_f, tol_e = (1e-9, 1e-10) if precision == "fp64" else (1e-5, 2e-6)
+    assert err <= tol_f
+    assert abs(r["lennard_jones"] + r["coulomb"] - ref["lennard_jones"] - ref["coulomb"]) <= tol_e * scale
