@@ -240,6 +240,11 @@ struct PmeArgs {
     int* status;
     int virial;
     int fft_lines;               // lines per CTA of the strided FFT passes, at most (0: 16)
+    // mixed precision: the reciprocal energy and virial from an FP64 forward
+    // transform of the charge grid (double2 half spectrum, FP64 twiddles),
+    // launched after the gather; null: from the FP32 convolution pass
+    void* cgrid64;
+    const void* tw64;
 };
 constexpr int kStageSpread = 0, kStageFft = 1, kStageGather = 2;
 constexpr int kStagePotential = 3;   // dE/dq~ = phi at the atoms, into (double*)facc

@@ -253,6 +253,9 @@ __global__ void k_spread(PmeArgs a)
 
 // ------------------------------------------------------------------ FFT passes
 constexpr int kModeZR2C = 0, kModeY = 1, kModeXConv = 2, kModeZC2R = 3;
+// forward x transform and Grid::scalarSum's energy / virial only (no
+// convolution written back, no inverse): the FP64 energy of a mixed force
+constexpr int kModeXEnergy = 4;
 
 struct PassArgs {
     PmeArgs a;
@@ -262,6 +265,7 @@ struct PassArgs {
     int sign;
     int tw_off;
     int erec_off;
+    int store_energy;  // kModeXConv: write the energy / virial records
 };
 
 template <typename R, int MODE>
@@ -341,7 +345,7 @@ __global__ void __launch_bounds__(256, 2) k_fft_pass(PassArgs pa)
     }
     __syncthreads();
     C* r = fft_lines<C, R>(buf0, buf1, nl, pa.ld, pl, tw, pa.sign);
-    if (MODE == kModeXConv) {
+    if (MODE == kModeXConv || MODE == kModeXEnergy) {
         // theta(m) multiply + energy / virial (Grid::scalarSum) on the
         // forward-transformed x-lines, then the inverse x transform
         int y = outer;
@@ -368,18 +372,24 @@ __global__ void __launch_bounds__(256, 2) k_fft_pass(PassArgs pa)
                 acc[6] += e * (1.0 - v * my * my); acc[7] -= e * (v * my * mz);
                 acc[10] += e * (1.0 - v * mz * mz);
             }
-            c.x = (R)(c.x * theta);
-            c.y = (R)(c.y * theta);
+            if (MODE == kModeXConv) {
+                c.x = (R)(c.x * theta);
+                c.y = (R)(c.y * theta);
+            }
         }
-        __syncthreads();
-        C* other = (r == buf0) ? buf1 : buf0;
-        r = fft_lines<C, R>(r, other, nl, pa.ld, pl, tw, +1);
+        if (MODE == kModeXConv) {
+            __syncthreads();
+            C* other = (r == buf0) ? buf1 : buf0;
+            r = fft_lines<C, R>(r, other, nl, pa.ld, pl, tw, +1);
+        }
     }
-    for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
-        int e = idx / nl, l = idx - e * nl;
-        cg[base + e * stride + l] = r[l * pa.ld + e];
+    if (MODE != kModeXEnergy) {
+        for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+            int e = idx / nl, l = idx - e * nl;
+            cg[base + e * stride + l] = r[l * pa.ld + e];
+        }
     }
-    if (MODE == kModeXConv) {
+    if ((MODE == kModeXConv && pa.store_energy) || MODE == kModeXEnergy) {
         for (int k = 0; k < kERec; ++k) acc[k] *= 0.5;
         acc[5] = acc[3]; acc[8] = acc[4]; acc[9] = acc[7];
         block_reduce_store<8>(acc, a.erec, a.erec_stride, pa.erec_off + blockIdx.x);
@@ -586,6 +596,8 @@ __global__ void __launch_bounds__(128) k_gather_p(PmeArgs a)
                (double)fz * a.hzr * q, a.scale, a.status);
 }
 
+static int run_energy64(const PmeArgs& a0, cudaStream_t s, long long* launches, int* erec_used);
+
 template <typename R>
 static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches, int* erec_used, int stage)
 {
@@ -596,8 +608,19 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     if (stage == kStageSpread) {
         cudaMemsetAsync(a.qgrid, 0, sizeof(long long) * nreal, s);
         if (a.n > 0) {
-            if (a.order == 4) k_spread_p<R, 4><<<nb, 128, 0, s>>>(a);
-            else k_spread<R><<<nb, 128, 0, s>>>(a);
+            // with the FP64 energy transform (large grids, see run_energy64)
+            // the B-spline weights are FP64 too: FP32 weights (~1e-7 each)
+            // move the reciprocal energy by ~1.5e-7, which the FP32
+            // transform's own rounding happened to offset on small grids
+            // (measured at 64^3: 1.0e-3 and -1.0e-3 of 6,974 kcal/mol); the
+            // spread is bound by its 64 integer atomics per atom either way
+            if (a.cgrid64) {
+                if (a.order == 4) k_spread_p<double, 4><<<nb, 128, 0, s>>>(a);
+                else k_spread<double><<<nb, 128, 0, s>>>(a);
+            } else {
+                if (a.order == 4) k_spread_p<R, 4><<<nb, 128, 0, s>>>(a);
+                else k_spread<R><<<nb, 128, 0, s>>>(a);
+            }
             *launches += 1;
         }
         return (int)cudaGetLastError();
@@ -607,6 +630,11 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
             if (a.order == 4) launch_pdl(k_gather_p<R, 4>, nb, 128, 0, s, a);
             else k_gather<R><<<nb, 128, 0, s>>>(a);
             *launches += 1;
+        }
+        if (sizeof(R) == 4 && a.cgrid64) {
+            int e = (int)cudaGetLastError();
+            if (e) return e;
+            return run_energy64(a, s, launches, erec_used);
         }
         return (int)cudaGetLastError();
     }
@@ -657,7 +685,7 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     int xblocks = a.ky * ((a.kzh + xtile - 1) / xtile);
     {
         PassArgs pa; pa.a = a; pa.plan = px; pa.lines = xtile; pa.ld = a.kx + 1; pa.sign = -1;
-        pa.tw_off = a.twx; pa.erec_off = 0;
+        pa.tw_off = a.twx; pa.erec_off = 0; pa.store_energy = a.cgrid64 ? 0 : 1;
         size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
         launch_pdl(k_fft_pass<R, kModeXConv>, xblocks, threads, sm, s, pa);
     }
@@ -678,6 +706,56 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
         launch_pdl(k_fft_pass<R, kModeZC2R>, blocks, threads, sm, s, pa);
     }
     *launches += 5;
+    *erec_used = a.cgrid64 ? 0 : xblocks;
+    return (int)cudaGetLastError();
+}
+
+// The FP64 forward transform of the charge grid (z r2c, y, x) with the
+// energy and virial of Grid::scalarSum, for a mixed-precision force: its
+// energy records replace those of the FP32 convolution pass.  Same passes,
+// FP64 twiddles, a double2 half spectrum of its own.
+static int run_energy64(const PmeArgs& a0, cudaStream_t s, long long* launches, int* erec_used)
+{
+    typedef double2 C;
+    PmeArgs a = a0;
+    a.cgrid = a0.cgrid64;
+    a.tw = a0.tw64;
+    FftPlan px, py, pz;
+    make_plan(a.kx, px); make_plan(a.ky, py); make_plan(a.kz, pz);
+    if (px.nrad < 0 || py.nrad < 0 || pz.nrad < 0) return (int)cudaErrorInvalidValue;
+    const int threads = 256;
+    const int zmax = a.fft_lines > 0 ? 2 * std::min(a.fft_lines, 16) : 32;
+    int zl = std::min((16384 / (int)sizeof(C)) / a.kz, zmax);
+    zl = zl < 1 ? 1 : (zl > 32 ? 32 : zl);
+    const int max_lines = a.fft_lines > 0 ? std::min(a.fft_lines, 16) : 16;
+    auto tile_for = [max_lines](int n) {
+        int t = (200 * 1024) / (2 * (n + 1) * (int)sizeof(C));
+        return t < 1 ? 1 : (t > max_lines ? max_lines : t);
+    };
+    {
+        PassArgs pa; pa.a = a; pa.plan = pz; pa.lines = zl; pa.ld = a.kz + 1; pa.sign = -1;
+        pa.tw_off = a.twz; pa.erec_off = 0; pa.store_energy = 0;
+        int blocks = (a.kx * a.ky + pa.lines - 1) / pa.lines;
+        size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
+        launch_pdl(k_fft_pass<double, kModeZR2C>, blocks, threads, sm, s, pa);
+    }
+    const int tile = tile_for(a.ky);
+    {
+        PassArgs pa; pa.a = a; pa.plan = py; pa.lines = tile; pa.ld = a.ky + 1; pa.sign = -1;
+        pa.tw_off = a.twy; pa.erec_off = 0; pa.store_energy = 0;
+        int blocks = a.kx * ((a.kzh + tile - 1) / tile);
+        size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
+        launch_pdl(k_fft_pass<double, kModeY>, blocks, threads, sm, s, pa);
+    }
+    const int xtile = tile_for(a.kx);
+    const int xblocks = a.ky * ((a.kzh + xtile - 1) / xtile);
+    {
+        PassArgs pa; pa.a = a; pa.plan = px; pa.lines = xtile; pa.ld = a.kx + 1; pa.sign = -1;
+        pa.tw_off = a.twx; pa.erec_off = 0; pa.store_energy = 1;
+        size_t sm = (2 * (size_t)pa.lines * pa.ld + (size_t)pa.plan.n) * sizeof(C);
+        launch_pdl(k_fft_pass<double, kModeXEnergy>, xblocks, threads, sm, s, pa);
+    }
+    *launches += 3;
     *erec_used = xblocks;
     return (int)cudaGetLastError();
 }
@@ -718,6 +796,7 @@ void pme_init_attributes()
     allow_dynamic_smem(k_fft_pass<double, kModeY>, mx);
     allow_dynamic_smem(k_fft_pass<double, kModeXConv>, mx);
     allow_dynamic_smem(k_fft_pass<double, kModeZC2R>, mx);
+    allow_dynamic_smem(k_fft_pass<double, kModeXEnergy>, mx);
     cudaGetLastError();   // a refused attribute surfaces at the launch that needs it
     if (dev < 64) done |= 1ull << dev;
 }

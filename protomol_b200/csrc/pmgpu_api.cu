@@ -23,6 +23,8 @@
 using namespace pm;
 
 static const double kPi = 3.14159265358979323846;   // Constant::M_PI (base/pmconstants.cpp:56)
+// mixed PME grids from this size on take the FP64 energy path (prepare_pme)
+static const size_t kEnergy64Points = (size_t)128 * 128 * 128;
 static const double kEpsilon = 1.0e-14;              // Constant::EPSILON (base/pmconstants.cpp:45)
 // status word, list count and need, chunk count and need, work counter, pad,
 // then 11 int64 energy/virial sums
@@ -196,6 +198,8 @@ struct pmgpu_force {
     void* d_cgrid = nullptr;
     void* d_rgrid = nullptr;
     void* d_tw = nullptr;
+    void* d_cgrid64 = nullptr;      // mixed: FP64 half spectrum and twiddles of the energy transform
+    void* d_tw64 = nullptr;
     double* d_bfac = nullptr;
     double* d_efac = nullptr;
     double self_energy = 0.0, charged_energy = 0.0;
@@ -1145,6 +1149,22 @@ static int prepare_pme(pmgpu_force* f)
         CK(dalloc((float2**)&f->d_cgrid, nhalf), "alloc");
         CK(dalloc((float**)&f->d_rgrid, nreal), "alloc");
         CK(dalloc(&f->d_qgrid, nreal), "alloc");
+        // grids of 128^3 points and more: the reciprocal energy and virial
+        // from FP64 B-spline weights and an FP64 forward transform of the
+        // fixed-point charge grid.  With FP32 there the transform's rounding
+        // reaches the total energy of the large boxes, where the real-space,
+        // reciprocal and self terms nearly cancel (1,000,000 atoms at 216^3:
+        // 5.9e-7 of the total with FP32, 1.3e-7 with FP64).  On smaller grids
+        // the FP32 energy meets 1e-7 and the FP64 passes would cost ~8% of
+        // the evaluation (they share the SMs with the pair kernel).
+        if (nreal >= kEnergy64Points) {
+            CK(dalloc((double2**)&f->d_tw64, ntw), "alloc");
+            CK(cudaMemcpy(f->d_tw64, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice), "copy");
+            CK(dalloc((double2**)&f->d_cgrid64, nhalf), "alloc");
+        } else {
+            if (f->d_tw64) { cudaFree(f->d_tw64); f->d_tw64 = nullptr; }
+            if (f->d_cgrid64) { cudaFree(f->d_cgrid64); f->d_cgrid64 = nullptr; }
+        }
     }
     // point self energy and charged-system term (:604-628)
     double V = std::fabs(sys->box[0] * sys->box[4] * sys->box[8]);
@@ -1167,6 +1187,8 @@ static void free_force(pmgpu_force* f)
     if (f->d_cgrid) cudaFree(f->d_cgrid);
     if (f->d_rgrid) cudaFree(f->d_rgrid);
     if (f->d_tw) cudaFree(f->d_tw);
+    if (f->d_cgrid64) cudaFree(f->d_cgrid64);
+    if (f->d_tw64) cudaFree(f->d_tw64);
     dfree(f->d_bfac); dfree(f->d_efac);
     for (int k = 0; k < 2; ++k) { dfree(f->d_tab64[k]); dfree(f->d_tab32[k]); }
     delete f;
@@ -1423,6 +1445,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 a.offy = -(p.order - 1) / 2 + p.grid[1];
                 a.offz = -(p.order - 1) / 2 + p.grid[2];
                 a.qgrid = f->d_qgrid; a.cgrid = f->d_cgrid; a.rgrid = f->d_rgrid; a.tw = f->d_tw;
+                a.cgrid64 = fp64 ? nullptr : f->d_cgrid64; a.tw64 = f->d_tw64;
                 a.twx = f->twx; a.twy = f->twy; a.twz = f->twz;
                 a.bfac = f->d_bfac; a.efac = f->d_efac;
                 a.piVr = 1.0 / (kPi * (LX * LY * LZ));
