@@ -255,8 +255,8 @@ int pmgpu_last_error(pmgpu_system* sys, char* buf, int len);
  *               negative force Jacobian-vector product); PMGPU_ERR_UNSUPPORTED
  *               when a PME reciprocal or correction term is in the list;
  *   energies 2: the pair terms' LJ and Coulomb energies (a check).
- * Any output may be NULL.  PMGPU_ERR_UNSUPPORTED for a force with a table
- * potential. */
+ * Any output may be NULL.  Table potentials differentiate their cubic
+ * interpolant (exact inside an interval; C1 across intervals). */
 int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,
                   const double* v, double* dE_dq, double* dE_dlj, double* hv, double* energies);
 
@@ -325,8 +325,7 @@ int pmgpu_batch_autotune(pmgpu_batch* batch, int evals, pmgpu_tuning* best);
  * derivative of their energy at the host positions, row-major, added (+=)
  * to hessian.  The matrix the normal-mode integrators diagonalise
  * (NormalModeUtilities).  Up to 8,192 atoms (PMGPU_ERR_CAPACITY);
- * PMGPU_ERR_UNSUPPORTED for the PME reciprocal and correction terms and for
- * table potentials. */
+ * PMGPU_ERR_UNSUPPORTED for the PME reciprocal and correction terms. */
 int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,
                   double* hessian);
 

@@ -117,6 +117,56 @@ __device__ __forceinline__ void term_raw(int pot, const TermD& t, R a, R qq, R A
     }
 }
 
+__device__ __forceinline__ bool adj_table(int pot)
+{
+    return pot == PMGPU_POT_LENNARD_JONES_TABLE || pot == PMGPU_POT_COULOMB_TABLE ||
+           pot == PMGPU_POT_EWALD_REAL_TABLE;
+}
+
+// A table potential: in each interval the table is a cubic in a = r^2
+// (LookUpTableBase::interpolate, base/LookUpTableBase.h:266-272), so its
+// value, de/da and d^2e/da^2 come from the same coefficients; f = -2 de/da
+// is the reference's force.  Inside an interval the derivatives are exact;
+// the table is C1 across intervals (value and gradient match), its second
+// derivative is piecewise linear.  Per unit q~_i q~_j (Coulomb tables, the
+// 1-4 factor in kappa) or per unit A and B (LennardJonesTable).
+__device__ __forceinline__ void term_table(int pot, const TermD& t, double a, double qq, double A, double B,
+                                           double kappa, double& e, double& e1, double& f, double& f1,
+                                           double& pqq, double& pA, double& pB)
+{
+    const long long u = __double_as_longlong(a);
+    long long k = (u >> t.tab_shift) * t.tab_step - t.tab_first;
+    double dt = 0.0;
+    if (k < 0) k = 0;
+    else if (k > t.tab_last) k = t.tab_last;
+    else dt = a - __longlong_as_double(u & ~((1ll << t.tab_shift) - 1ll));
+    const double* T = t.tab + k;
+    auto cubic = [dt](const double* c, double& v, double& v1, double& v2) {
+        v = ((dt * c[3] + c[2]) * dt + c[1]) * dt + c[0];
+        v1 = (3.0 * dt * c[3] + 2.0 * c[2]) * dt + c[1];
+        v2 = 6.0 * dt * c[3] + 2.0 * c[2];
+    };
+    double v, v1, v2;
+    pqq = pA = pB = 0.0;
+    if (pot == PMGPU_POT_LENNARD_JONES_TABLE) {
+        double w, w1, w2;
+        cubic(T, v, v1, v2);
+        cubic(T + 4, w, w1, w2);
+        e = A * v + B * w;
+        e1 = A * v1 + B * w1;
+        f1 = -2.0 * (A * v2 + B * w2);
+        pA = v;
+        pB = w;
+    } else {
+        cubic(T, v, v1, v2);
+        e = qq * kappa * v;
+        e1 = qq * kappa * v1;
+        f1 = -2.0 * qq * kappa * v2;
+        pqq = kappa * v;
+    }
+    f = -2.0 * e1;
+}
+
 template <typename R>
 __global__ void __launch_bounds__(kTile) k_pair_adjoint(AdjArgs p)
 {
@@ -179,15 +229,25 @@ __global__ void __launch_bounds__(kTile) k_pair_adjoint(AdjArgs p)
             for (int t = 0; t < p.n_terms; ++t) {
                 const TermD& td = p.td[t];
                 R e, e1, f, f1, q1, a1, b1;
-                term_raw<R>(td.pot, td, ar, qq, A, B, kappa, e, e1, f, f1, q1, a1, b1);
+                const bool tab = adj_table(td.pot);
+                if (tab) {
+                    // FP64 look-up whatever R; the table's switch is inside it
+                    double de, de1, df, df1, dq1, da1, db1;
+                    term_table(td.pot, td, a, qi * s_q[jj], mod ? par.z : par.x, mod ? par.w : par.y,
+                               mod ? p.csf : 1.0, de, de1, df, df1, dq1, da1, db1);
+                    e = (R)de; e1 = (R)de1; f = (R)df; f1 = (R)df1; q1 = (R)dq1; a1 = (R)da1; b1 = (R)db1;
+                } else {
+                    term_raw<R>(td.pot, td, ar, qq, A, B, kappa, e, e1, f, f1, q1, a1, b1);
+                }
                 R s = 1, s1 = 0, s2 = 0;
-                if (p.modify) switch_a<R>(td.sw, td, a, ar, s, s1, s2);
+                if (p.modify && !tab) switch_a<R>(td.sw, td, a, ar, s, s1, s2);
                 F += f * s - 2 * e * s1;
                 F1 += f1 * s + f * s1 - 2 * e1 * s1 - 2 * e * s2;
                 pqq += q1 * s;
                 pA += a1 * s;
                 pB += b1 * s;
-                if (td.pot == PMGPU_POT_LENNARD_JONES) el += 0.5 * (double)(e * s);
+                if (td.pot == PMGPU_POT_LENNARD_JONES || td.pot == PMGPU_POT_LENNARD_JONES_TABLE)
+                    el += 0.5 * (double)(e * s);
                 else ec += 0.5 * (double)(e * s);
             }
             dq += (double)pqq * s_q[jj];

@@ -708,14 +708,6 @@ static cudaError_t table_setup(pmgpu_force* f, int k)
     return cudaSuccess;
 }
 
-static bool force_has_table(const pmgpu_force* f)
-{
-    if (f->kind != 0) return false;
-    for (int k = 0; k < f->cp.n_terms; ++k)
-        if (pot_is_table(f->cp.pot[k])) return true;
-    return false;
-}
-
 static void term_setup(const pmgpu_cutoff_params* p, int k, TermF& f, TermD& d)
 {
     memset(&f, 0, sizeof(f));
@@ -2263,8 +2255,6 @@ extern "C" int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const
             return fail(sys, PMGPU_ERR_UNSUPPORTED, "the Hessian of the PME reciprocal / correction terms is not "
                                                     "available (the real-space pairs are)");
         if (forces_in[k]->kind != 1) fl.push_back(forces_in[k]);
-        if (force_has_table(forces_in[k]))
-            return fail(sys, PMGPU_ERR_UNSUPPORTED, "no Hessian of a table potential");
     }
     if (sys->n > kHessianMaxAtoms) return fail(sys, PMGPU_ERR_CAPACITY, "dense Hessian above 8192 atoms");
     int r = eval_prepare(sys, (int)fl.size(), fl.data());
@@ -2391,9 +2381,6 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
         fl.push_back(forces_in[k]);
     }
     if (hv && !v) return fail(sys, PMGPU_ERR_ARG, "Hessian-vector product needs v");
-    for (pmgpu_force* f : fl)
-        if (force_has_table(f))
-            return fail(sys, PMGPU_ERR_UNSUPPORTED, "no adjoint of a table potential");
     for (pmgpu_force* f : fl)
         if (hv && f->kind == 1 && (f->pp.reciprocal || f->pp.correction))
             return fail(sys, PMGPU_ERR_UNSUPPORTED, "Hessian-vector product of the PME reciprocal / correction "

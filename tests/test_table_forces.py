@@ -10,7 +10,8 @@ small_*table*; the tables approximate the analytic potentials.
 GPU: FP64 and mixed kernels against the oracle on a chain in water (57 1-4
 pairs, coulombScalingFactor 0.5), a perturbed water box and a box small
 enough for the per-pair minimal image; the 14,281-atom system with the
-tabulated Ewald real part next to PME."""
+tabulated Ewald real part next to PME; the adjoint, HVP and dense Hessian
+of the table forces."""
 import numpy as np
 import pytest
 
@@ -166,12 +167,39 @@ def test_table_forces_other_boxes(sysname, precision):
 
 
 @pytest.mark.gpu
-def test_table_forces_refuse_the_adjoint():
+@pytest.mark.parametrize("case", ["ljt_ewald", "ljt_coult", "c2lj_ewald"])
+def test_table_adjoint_and_hessian(case):
+    """The backward pass of a table force differentiates the cubic
+    interpolant: energies equal the forward's; the charge and LJ-table
+    gradients reproduce the energy through its bilinearity in the charges
+    and linearity in A, B; H v against central differences of the oracle's
+    forces (h = 1e-7 A, so that hardly a pair crosses an interval boundary,
+    where the interpolant's second derivative jumps); the dense Hessian
+    applied to v is the HVP."""
     s = _small_chain()
+    d = DEFS[case]
+    specs = [F.parse_definition(d)]
     topo = F.Topology(s)
-    f = F.ForceFactory.make(topo, DEFS["ljt_ewald"], "fp64")
-    with pytest.raises(RuntimeError):
-        F.adjoint(topo, [f], s.positions)
+    f = F.ForceFactory.make(topo, d, "fp64")
+    v = np.random.default_rng(5).standard_normal((s.n_atoms, 3))
+    g = F.adjoint(topo, [f], s.positions, v)
+    ref = oracle.evaluate(s, specs)
+    scale = abs(ref["lennard_jones"]) + abs(ref["coulomb"])
+    assert abs(g["lennard_jones"] - ref["lennard_jones"]) <= 1e-10 * scale
+    assert abs(g["coulomb"] - ref["coulomb"]) <= 1e-10 * scale
+    assert abs(np.dot(s.scaled_charge, g["dE_dq"]) - 2.0 * ref["coulomb"]) <= 1e-9 * scale
+    assert abs((s.lj_table * g["dE_dlj"]).sum() - ref["lennard_jones"]) <= 1e-9 * scale
+    h = 1e-7
+    fp = oracle.evaluate(s, specs, positions=s.positions + h * v)["forces"]
+    fm = oracle.evaluate(s, specs, positions=s.positions - h * v)["forces"]
+    hv_fd = -(fp - fm) / (2.0 * h)
+    err = np.sqrt(((g["hv"] - hv_fd) ** 2).sum() / (hv_fd ** 2).sum())
+    print(f"\n{case}: H v vs central differences {err:.2e}")
+    assert err <= 1e-5
+    H = F.hessian(topo, [f], s.positions)
+    assert np.abs(H - H.T).max() <= 1e-9 * np.abs(H).max()
+    hv = H @ v.ravel()
+    assert np.abs(hv - g["hv"].ravel()).max() <= 1e-9 * np.abs(hv).max()
 
 
 @pytest.mark.gpu
