@@ -400,20 +400,26 @@ def parse_definition(definition: str) -> dict:
     toks = definition.split()
     if toks and toks[0].lower() == "force":
         toks = toks[1:]
+    # the factory compares keywords, policies and values without case
+    # (frontend/ForceFactoryDetails.cpp:68-122, ltstrNocase / equalNocase)
+    canon = {w.lower(): w for w in _POTENTIALS + _SWITCHES +
+             ("NonbondedCutoff", "NonbondedSimpleFull", "PMEwald", "BSpline")}
     names, sws, algorithm, interp, flags, rest = [], [], None, None, set(), []
     i = 0
     while i < len(toks):
         t = toks[i]
-        if t in _POTENTIALS:
-            names.append(t)
-        elif t == "-switchingFunction" and i + 1 < len(toks):
-            sws.append(toks[i + 1]); i += 1
-        elif t == "-algorithm" and i + 1 < len(toks):
-            algorithm = toks[i + 1]; i += 1
-        elif t == "-interpolation" and i + 1 < len(toks):
-            interp = toks[i + 1]; i += 1
-        elif t in ("-real", "-reciprocal", "-correction"):
-            flags.add(t[1:])
+        tl = t.lower()
+        nxt = canon.get(toks[i + 1].lower(), toks[i + 1]) if i + 1 < len(toks) else None
+        if canon.get(tl) in _POTENTIALS:
+            names.append(canon[tl])
+        elif tl == "-switchingfunction" and nxt is not None:
+            sws.append(nxt); i += 1
+        elif tl == "-algorithm" and nxt is not None:
+            algorithm = nxt; i += 1
+        elif tl == "-interpolation" and nxt is not None:
+            interp = nxt; i += 1
+        elif tl in ("-real", "-reciprocal", "-correction"):
+            flags.add(tl[1:])
         else:
             rest.append(t)
         i += 1

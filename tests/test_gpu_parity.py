@@ -279,6 +279,23 @@ def test_pme_default_alpha_matches_reference_bisection(small_chain):
     assert f.alpha == r["alpha"] == systems.ewald_alpha(9.0)
 
 
+def test_million_atom_cutoff_force_fp64_against_oracle():
+    """The FP64 kernels on the whole 1,000,000-atom cutoff force against the
+    oracle (3.6e8 pairs, ~30 s on one host core): energies and forces."""
+    w = workloads.water1m()
+    s = w.system
+    ref = oracle.evaluate(s, [F.parse_definition(w.forces[0])])
+    _, _, f, e = gpu_eval(s, [w.forces[0]], "fp64")
+    rms = np.sqrt((ref["forces"] ** 2).sum(1).mean())
+    print(f"\n1M cutoff force FP64: dLJ {e.lennard_jones - ref['lennard_jones']:+.2e}  "
+          f"dC {e.coulomb - ref['coulomb']:+.2e}  max |dF| / rms {np.abs(f - ref['forces']).max() / rms:.2e}")
+    scale = abs(ref["lennard_jones"]) + abs(ref["coulomb"])
+    assert abs(e.lennard_jones - ref["lennard_jones"]) <= FP64_ENERGY_RTOL * scale
+    assert abs(e.coulomb - ref["coulomb"]) <= FP64_ENERGY_RTOL * scale
+    assert np.abs(f - ref["forces"]).max() <= FP64_FORCE_RTOL * rms
+    assert np.abs(e.virial_tensor - ref["virial"]).max() <= FP64_ENERGY_RTOL * np.abs(ref["virial"]).max()
+
+
 def test_million_atom_box_at_full_size():
     """The 1,000,000-atom configuration (333,333 waters + Na+, 215.4 A, cutoff
     12, PME 216^3) at full size, through size-independent properties: the

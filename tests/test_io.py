@@ -157,3 +157,28 @@ def test_reference_bpti_configuration():
     assert np.abs(a["forces"] - b["forces"]).max() <= 1e-12 * rms
     assert abs(a["lennard_jones"] - b["lennard_jones"]) <= 1e-12 * abs(b["lennard_jones"])
     assert abs(a["coulomb"] - b["coulomb"]) <= 1e-9 * abs(b["coulomb"])
+
+
+@needs_examples
+def test_reference_example_force_lines_parse():
+    """Every nonbonded force line of the reference's example configurations
+    that uses this path's algorithms and switching functions parses (the
+    factory ignores case); Cn switching, FullEwald and MultiGrid are not on
+    this path."""
+    import glob
+    nonbonded = ("lennardjones", "coulomb", "coulombewaldreal", "lennardjonestable", "coulombtable",
+                 "coulombewaldrealtable")
+    other = ("cn", "cmpcncn", "fullewald", "multigrid", "coulombmultigriddirect", "coulombmultigriddirecttable")
+    parsed = 0
+    for conf in sorted(glob.glob(os.path.join(EXAMPLES, "**", "*.conf"), recursive=True)):
+        for d in io.read_conf(conf)["forces"]:
+            toks = [t.lower() for t in d.split()]
+            if toks[0] not in nonbonded or any(t in other for t in toks):
+                continue
+            if "-switchingfunction" in toks and toks.count("-switchingfunction") > \
+                    sum(t in nonbonded and t != "coulombewaldrealtable" for t in toks):
+                continue      # a switching function the registered id does not carry
+            spec = F.parse_definition(d)
+            assert spec["kind"] in ("cut", "full", "pme"), (conf, d)
+            parsed += 1
+    assert parsed >= 40
