@@ -37,8 +37,9 @@ METRIC = "force evals/s (cutoff+PME) mixed vs FP64 on one B200 at ≤1e-5 force 
 UNIT = "evals/s"
 FP32_LANES_PER_SM = 128
 N_SMS = 148
-# DRAM bytes (read + write) of one k_pair_mixed launch on this workload, from
-# the ncu capture summarised in profiles/k_pair_mixed_chain14281.md
+# DRAM bytes (read + write) of one k_pair_mixed launch on this workload:
+# dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of the
+# kernel on this bench command (L2 flushed before the evaluation)
 PAIR_DRAM_BYTES_PER_LAUNCH = 4_994_304
 
 
@@ -93,7 +94,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -274,10 +275,12 @@ def main():
     e_err = abs((em.lennard_jones + em.coulomb) - (ed.lennard_jones + ed.coulomb)) / (
         abs(ed.lennard_jones) + abs(ed.coulomb))
 
-    # FP64 kernels (the comparison point of the metric)
-    ms64, _ = timed(fp64, max(20, args.steps // 10), args.warmup)
-    # mixed precision (the value)
+    # the clocks are sampled from the FP64 loop on, so that a short timed
+    # region still has samples under the same load
     with ClockSampler(local) as clk:
+        # FP64 kernels (the comparison point of the metric)
+        ms64, _ = timed(fp64, max(20, args.steps // 10), args.warmup)
+        # mixed precision (the value)
         ms_mixed, launches = timed(mixed, args.steps, args.warmup)
     # per-kernel profile of the dominant kernel: pair kernel timed alone
     t_local = float(np.mean(ms_mixed))

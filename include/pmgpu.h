@@ -185,7 +185,11 @@ int pmgpu_full_create(pmgpu_system* sys, const pmgpu_cutoff_params* params, pmgp
 
 /* Replaces NonbondedPMEwaldSystemForce::doMake (forces/NonbondedPMEwaldSystemForce.h:1099-1139);
  * rejects the same parameter sets with PMGPU_ERR_ARG (order < 2 or odd,
- * grid < order, cutoff <= 0, accuracy <= 0). */
+ * grid < order, cutoff <= 0, accuracy <= 0).  Term sets that no exemplar
+ * registers (factories/registerForceExemplarsFastElectrostatic.cpp:50-55):
+ * none of real / reciprocal / correction, or real + reciprocal without
+ * correction, return PMGPU_ERR_UNSUPPORTED, as do grid sizes with a prime
+ * factor above 7 and orders above 12. */
 int pmgpu_pme_create(pmgpu_system* sys, const pmgpu_pme_params* params, pmgpu_force** out);
 
 int pmgpu_force_destroy(pmgpu_force* force);
@@ -399,6 +403,8 @@ int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* force, const double* positio
  * All pointers d_* are device memory on `device`.  Limits: N <= 65,536
  * atoms, Kx*Ky*Kz <= 262,144 (64^3), each K <= 1,024, Kx*Ky*(Kz/2+1) <=
  * 196,608 and Ky*(Kz/2+1) <= 8,192; larger sizes return PMGPU_ERR_CAPACITY.
+ * Each K has prime factors 2, 3, 5 and 7 only, as for pmgpu_pme_create;
+ * other grid sizes return PMGPU_ERR_UNSUPPORTED before any launch.
  * Runs on `stream` (NULL: the legacy default stream) and returns when the
  * results are written; PMGPU_ERR_OVERFLOW for non-finite forces.  The first
  * call on a device looks up the scratch address and initialises it (and

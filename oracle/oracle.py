@@ -286,13 +286,29 @@ def reference_available(fast: bool = False) -> bool:
     return os.path.exists(os.path.join(REF_DIR, "pmref_fast" if fast else "pmref"))
 
 
-def build_reference(ref_root: str = "/root/reference") -> bool:
-    """Compile the reference's own sources (only where they are present)."""
+def build_reference(ref_root: str) -> bool:
+    """Compile the reference's own sources (only where they are present) and
+    record where they came from (``reference_root``)."""
     if not os.path.isdir(os.path.join(ref_root, "framework")):
         return reference_available()
     subprocess.check_call(["make", "-C", os.path.join(HERE, "ref"), f"REF={ref_root}",
                            "-j", str(os.cpu_count() or 4), "-s"])
+    with open(os.path.join(REF_DIR, "REFERENCE_ROOT"), "w") as fh:
+        fh.write(os.path.abspath(ref_root) + "\n")
     return True
+
+
+def reference_root():
+    """The ProtoMol source tree: $PROTOMOL_REFERENCE, else the tree the
+    compiled reference was built from; None when neither is known."""
+    env = os.environ.get("PROTOMOL_REFERENCE")
+    if env:
+        return env
+    try:
+        with open(os.path.join(REF_DIR, "REFERENCE_ROOT")) as fh:
+            return fh.read().strip() or None
+    except OSError:
+        return None
 
 
 def _spec_args(spec):

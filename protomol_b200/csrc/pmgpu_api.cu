@@ -1027,6 +1027,10 @@ extern "C" int pmgpu_pme_create(pmgpu_system* sys, const pmgpu_pme_params* p, pm
     if (!(p->accuracy > 0.0)) err += "PMEwald accuracy > 0.";
     if (!err.empty()) return fail(sys, PMGPU_ERR_ARG, " force PMEwald :" + err);
     if (p->order > 12) return fail(sys, PMGPU_ERR_UNSUPPORTED, "PME order > 12");
+    // the (real, reciprocal, correction) sets of the registered exemplars
+    // (factories/registerForceExemplarsFastElectrostatic.cpp:50-55)
+    if (!(p->real || p->reciprocal || p->correction) || (p->real && p->reciprocal && !p->correction))
+        return fail(sys, PMGPU_ERR_UNSUPPORTED, "PMEwald: no registered exemplar with these terms");
     for (int k = 0; k < 3; ++k)
         if (!smooth_ok(p->grid[k]) || p->grid[k] > 4096)
             return fail(sys, PMGPU_ERR_UNSUPPORTED, "PME grid size needs prime factors 2, 3, 5, 7 and <= 4096");
@@ -1817,6 +1821,8 @@ extern "C" int pmgpu_pme_reciprocal_static(int device, int n_atoms, const double
     if (!(alpha > 0.0) || !(box[0] > 0.0) || !(box[1] > 0.0) || !(box[2] > 0.0)) return PMGPU_ERR_ARG;
     const int kx = grid[0], ky = grid[1], kz = grid[2];
     if (kx < order || ky < order || kz < order) return PMGPU_ERR_ARG;
+    // the FFT's radices, as pmgpu_pme_create checks them
+    if (!smooth_ok(kx) || !smooth_ok(ky) || !smooth_ok(kz)) return PMGPU_ERR_UNSUPPORTED;
     const int kzh = kz / 2 + 1;
     // the sizes the static scratch holds
     if (n_atoms > kStaticAtoms || kx > kStaticAxis || ky > kStaticAxis || kz > kStaticAxis ||

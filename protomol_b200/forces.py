@@ -300,6 +300,10 @@ _SWITCHES = ("Universal", "Cutoff", "C1", "C2", "Shift")
 # CoulombTable name it in their id; CoulombEwaldRealTable's is Cutoff and
 # hidden (CoulombEwaldRealTableForce.h:120-124).
 _TABLES = ("LennardJonesTable", "CoulombTable", "CoulombEwaldRealTable")
+# (real, reciprocal, correction) of the registered PMEwald exemplars
+# (factories/registerForceExemplarsFastElectrostatic.cpp:50-55)
+_PME_REGISTERED = ((True, True, True), (True, False, False), (True, False, True),
+                   (False, True, False), (False, True, True), (False, False, True))
 
 
 @dataclass
@@ -467,7 +471,12 @@ def parse_definition(definition: str) -> dict:
             terms.append((s, n, on, rc, alpha))
         return {"kind": "full", "terms": terms}
     if algorithm == "PMEwald":
-        if names != ["Coulomb"] or (interp or "BSpline") != "BSpline":
+        # the registered exemplars (factories/registerForceExemplarsFastElectrostatic.cpp:50-55)
+        # all take the Cutoff switch, which their id leaves unwritten, and
+        # exist for these (real, reciprocal, correction) sets only
+        terms_on = ("real" in flags, "reciprocal" in flags, "correction" in flags)
+        if (names != ["Coulomb"] or (interp or "BSpline") != "BSpline" or sws not in ([], ["Cutoff"])
+                or terms_on not in _PME_REGISTERED):
             raise ValueError(f"Could not find a complete match for '{definition}'")
         params = [_Param("-gridsize"), _Param(""), _Param(""), _Param("-cutoff"),
                   _Param("-order", 4), _Param("-accuracy", 1e-6), _Param("-alpha", -1.0)]

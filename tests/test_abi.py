@@ -86,3 +86,31 @@ def test_parse_reuses_a_keyword_after_wrapping_around():
 def test_parse_rejects_incomplete_definitions(bad):
     with pytest.raises(ValueError):
         F.parse_definition(bad)
+
+
+@pytest.mark.parametrize("bad", [
+    # ProtoMol registers PMEwald with the Cutoff switch only
+    # (registerForceExemplarsFastElectrostatic.cpp:50-55): a Shift or C2 line
+    # finds no exemplar
+    "Coulomb -algorithm PMEwald -real -reciprocal -correction -switchingFunction Shift "
+    "-interpolation BSpline -gridsize 8 8 8 -cutoff 9",
+    "Coulomb -algorithm PMEwald -real -reciprocal -correction -switchingFunction C2 "
+    "-interpolation BSpline -gridsize 8 8 8 -cutoff 9",
+    # no term at all, and -real -reciprocal without -correction: not registered
+    "Coulomb -algorithm PMEwald -interpolation BSpline -gridsize 8 8 8 -cutoff 9",
+    "Coulomb -algorithm PMEwald -real -reciprocal -interpolation BSpline -gridsize 8 8 8 -cutoff 9",
+])
+def test_parse_rejects_unregistered_pme_variants(bad):
+    with pytest.raises(ValueError, match="Could not find a complete match"):
+        F.parse_definition(bad)
+
+
+@pytest.mark.parametrize("flags", ["-real -reciprocal -correction", "-real", "-real -correction",
+                                   "-reciprocal", "-reciprocal -correction", "-correction"])
+def test_parse_accepts_every_registered_pme_variant(flags):
+    d = F.parse_definition(f"Coulomb -algorithm PMEwald {flags} -interpolation BSpline -gridsize 8 8 8 -cutoff 9")
+    assert (d["real"], d["reciprocal"], d["correction"]) == tuple(int(f"-{t}" in flags.split())
+                                                                 for t in ("real", "reciprocal", "correction"))
+    # the Cutoff switch may be written out
+    F.parse_definition(f"Coulomb -algorithm PMEwald {flags} -switchingFunction Cutoff -interpolation BSpline "
+                       "-gridsize 8 8 8 -cutoff 9")

@@ -16,7 +16,9 @@ from protomol_b200 import forces as F
 from protomol_b200 import io, systems
 from protomol_b200.systems import SQRT_COULOMB_CONSTANT
 
-REFERENCE = os.environ.get("PROTOMOL_REFERENCE", "/root/reference")
+from oracle.oracle import reference_root
+
+REFERENCE = reference_root() or ""
 EXAMPLES = os.path.join(REFERENCE, "examples")
 needs_examples = pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference examples not present")
 

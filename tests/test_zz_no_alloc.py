@@ -43,6 +43,10 @@ def test_sizes_beyond_the_static_scratch_are_rejected():
     big = (C.c_int * 3)(128, 128, 128)
     rc = lib.pmgpu_pme_reciprocal_static(0, 10, dummy, dummy, box, big, 4, ALPHA, dummy, dummy, 0, None)
     assert rc == 7
+    # a prime factor above 7 (22 = 2 x 11) is refused before any launch
+    rough = (C.c_int * 3)(22, 24, 24)
+    rc = lib.pmgpu_pme_reciprocal_static(0, 10, dummy, dummy, box, rough, 4, ALPHA, dummy, dummy, 0, None)
+    assert rc == 5        # PMGPU_ERR_UNSUPPORTED
 
 
 @pytest.mark.gpu
