@@ -374,6 +374,16 @@ int pmgpu_impulse_run(pmgpu_system* sys, int n_slow, pmgpu_force* const* slow, i
  * (x, y, z) and the grid dims. */
 int pmgpu_get_cells(pmgpu_system* sys, int* cells, int* dims);
 
+/* No counterpart in the reference (diagnostic).  The cluster layout the
+ * mixed-precision cutoff forces of the last evaluation ran on:
+ * PMGPU_LAYOUT_COLUMNS (fixed-point coordinates in z-sorted columns, boxes
+ * well above twice the cutoff), PMGPU_LAYOUT_CELLS (clusters inside the
+ * reference cells: smaller boxes, the small-grid mode, or a system whose
+ * columns or clusters exceeded the column layout's limits), or 0 (none yet). */
+#define PMGPU_LAYOUT_CELLS 1
+#define PMGPU_LAYOUT_COLUMNS 2
+int pmgpu_pair_layout(pmgpu_system* sys);
+
 /* Evaluates one cutoff force (or a PME force with -real) in pair-recording
  * mode and returns the within-cutoff pair set: every (min, max) atom index
  * pair the force interacted, in no particular order.  *count receives the

@@ -25,7 +25,7 @@ EXPORTS = [
     "pmgpu_system_create", "pmgpu_system_destroy", "pmgpu_set_topology", "pmgpu_set_box",
     "pmgpu_cutoff_create", "pmgpu_pme_create", "pmgpu_force_destroy", "pmgpu_pme_alpha",
     "pmgpu_evaluate", "pmgpu_evaluate_device", "pmgpu_synchronize", "pmgpu_stream",
-    "pmgpu_launch_count", "pmgpu_last_error", "pmgpu_get_cells", "pmgpu_get_pairs",
+    "pmgpu_launch_count", "pmgpu_last_error", "pmgpu_get_cells", "pmgpu_get_pairs", "pmgpu_pair_layout",
     "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
     "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
@@ -99,6 +99,7 @@ def load():
     lib.pmgpu_launch_count.restype = C.c_longlong
     lib.pmgpu_last_error.argtypes = [vp, C.c_char_p, C.c_int]
     lib.pmgpu_get_cells.argtypes = [vp, vp, vp]
+    lib.pmgpu_pair_layout.argtypes = [vp]
     lib.pmgpu_get_pairs.argtypes = [vp, vp, vp, C.POINTER(C.c_longlong), vp, C.c_longlong]
     lib.pmgpu_set_profiling.argtypes = [vp, C.c_int]
     lib.pmgpu_phase_times.argtypes = [vp, vp, C.c_int, C.POINTER(C.c_longlong)]

@@ -230,7 +230,171 @@ __global__ void __launch_bounds__(128) k_bin_cells(BinArgs a)
     }
 }
 
+// ---------------------------------------------------------------- K1c
+// Column clusters of the mixed pair path.  Every atom's position becomes an
+// unsigned 32-bit fixed-point coordinate of the periodic box,
+// round(frac((x - min) / L) 2^32) per axis, so that the wrapped int32
+// difference of two atoms is their minimal-image displacement in units of
+// L / 2^32 with no rounding at all; the atoms are counting-sorted into the
+// columns of an x-y grid and ordered by z inside a column (ties by index).
+// Slot 8 c + k holds atom k of i-cluster c; a column's last cluster is
+// padded (original index -1).  The reference cell of every atom is computed
+// here too (bit-exact, for pmgpu_get_cells).
+
+__device__ __forceinline__ unsigned fix32(double u)
+{
+    const double f = u - floor(u);                        // [0, 1)
+    return (unsigned)(__double2ull_rn(f * 4294967296.0) & 0xffffffffull);
+}
+
+__global__ void __launch_bounds__(kBinThreads) k_col_count(ColBinArgs a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const ColGrid& g = a.g;
+    if (i < a.n) {
+        const double x = a.pos[3 * i], y = a.pos[3 * i + 1], z = a.pos[3 * i + 2];
+        int cx, cy, cz;
+        double vx, vy, vz;
+        bin_cell_of(a.pbc, a.grid, x, y, z, cx, cy, cz, vx, vy, vz);
+        a.cell3[3 * i] = cx;
+        a.cell3[3 * i + 1] = cy;
+        a.cell3[3 * i + 2] = cz;
+        if (cx < 0 || cy < 0 || cz < 0 || cx >= a.grid.nx || cy >= a.grid.ny || cz >= a.grid.nz)
+            atomicOr(a.status, kStatusOutOfGrid);
+        const unsigned qx = fix32((x - g.mnx) / g.lx);
+        const unsigned qy = fix32((y - g.mny) / g.ly);
+        const unsigned qz = fix32((z - g.mnz) / g.lz);
+        a.qfix[3 * i] = qx;
+        a.qfix[3 * i + 1] = qy;
+        a.qfix[3 * i + 2] = qz;
+        const int kx = (int)(((unsigned long long)qx * (unsigned)g.ncx) >> 32);
+        const int ky = (int)(((unsigned long long)qy * (unsigned)g.ncy) >> 32);
+        const int c = kx * g.ncy + ky;
+        a.col[i] = c;
+        atomicAdd(a.counts + c, 1);
+    }
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(a.done, 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    scan_counts(a.counts, a.colstart, a.ccstart, g.ncol);
+}
+
+__global__ void __launch_bounds__(kBinThreads) k_col_scatter(ColBinArgs a)
+{
+    pdl_wait();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int c = a.col[i];
+    a.tmp[a.colstart[c] + atomicSub(a.counts + c, 1) - 1] = i;
+}
+
+constexpr int kColStage = 2048;      // atoms of a column ordered in shared memory
+constexpr int kColThreads = 128;
+
+// one block per column: z order (a bitonic sort of the (z, index) keys in
+// shared memory), slot data, padding, cluster boxes and the clusters' virial
+// origins
+__global__ void __launch_bounds__(kColThreads) k_col_sort(ColBinArgs a)
+{
+    pdl_wait();
+    __shared__ unsigned long long s_key[kColStage];
+    __shared__ int s_ord[kColStage];
+    const int t = threadIdx.x;
+    const ColGrid& g = a.g;
+    const int c = blockIdx.x;
+    const int b = a.colstart[c], m = a.colstart[c + 1] - b;
+    const int cl0 = a.ccstart[c], ncl = (m + 7) / 8;
+    if (m > kColStage || cl0 + ncl > a.ncl_cap) {            // block-uniform: the cell layout takes this system
+        if (t == 0) atomicOr(a.status, kStatusColumns);
+        return;
+    }
+    int n2 = 32;                                            // keys padded to a power of two
+    while (n2 < m) n2 <<= 1;
+    for (int k = t; k < n2; k += kColThreads) {
+        unsigned long long key = ~0ull;
+        if (k < m) {
+            const int i = a.tmp[b + k];
+            key = ((unsigned long long)a.qfix[3 * i + 2] << 32) | (unsigned)i;
+        }
+        s_key[k] = key;
+    }
+    __syncthreads();
+    for (int k = 2; k <= n2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = t; i < n2; i += kColThreads) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long u = s_key[i], v = s_key[ixj];
+                    if (((i & k) == 0) ? (u > v) : (u < v)) { s_key[i] = v; s_key[ixj] = u; }
+                }
+            }
+            __syncthreads();
+        }
+    for (int k = t; k < m; k += kColThreads) s_ord[k] = (int)(s_key[k] & 0xffffffffull);
+    __syncthreads();
+    const size_t slot0 = 8 * (size_t)cl0;
+    for (int r = t; r < 8 * ncl; r += kColThreads) {
+        const bool valid = r < m;
+        const int i = s_ord[valid ? r : (r & ~7)];          // padding: the cluster's first atom's place
+        const double qi = a.q[i];
+        const float qh = valid ? (float)qi : 0.f;
+        const float ql = valid ? (float)(qi - (double)qh) : 0.f;
+        const int4 qv = make_int4((int)a.qfix[3 * i], (int)a.qfix[3 * i + 1], (int)a.qfix[3 * i + 2], __float_as_int(qh));
+        a.cq[slot0 + r] = qv;
+        a.cm[slot0 + r] = valid ? make_int4(i, a.type[i], a.mol[i], __float_as_int(ql)) : make_int4(-1, 0, -2, 0);
+        if (valid) a.slot_of[i] = (int)(slot0 + r);
+        if ((r & 7) == 0) a.corg[cl0 + (r >> 3)] = make_int4(qv.x, qv.y, qv.z, 0);
+    }
+    // boxes of the j-clusters (4 slots each, the halves of the i-clusters)
+    // and of the i-clusters; an empty half gets a box beyond every window
+    const double kx = g.lx * (1.0 / 4294967296.0), ky = g.ly * (1.0 / 4294967296.0), kz = g.lz * (1.0 / 4294967296.0);
+    for (int q = t; q < 2 * ncl; q += kColThreads) {
+        const int r0 = 4 * q, r1 = min(m, r0 + 4);
+        // empty: lo.w = 1, both corners at +3e38 (the z order of the column's
+        // boxes stays monotone, and no window reaches it)
+        float4 lo = make_float4(3e38f, 3e38f, 3e38f, 1.f), hi = make_float4(3e38f, 3e38f, 3e38f, 0.f);
+        if (r0 < r1) { lo.w = 0.f; hi = make_float4(-3e38f, -3e38f, -3e38f, 0.f); }
+        for (int r = r0; r < r1; ++r) {
+            const int i = s_ord[r];
+            const float x = (float)(a.qfix[3 * i] * kx), y = (float)(a.qfix[3 * i + 1] * ky),
+                        z = (float)(a.qfix[3 * i + 2] * kz);
+            lo.x = fminf(lo.x, x); lo.y = fminf(lo.y, y); lo.z = fminf(lo.z, z);
+            hi.x = fmaxf(hi.x, x); hi.y = fmaxf(hi.y, y); hi.z = fmaxf(hi.z, z);
+        }
+        const size_t jc = 2 * (size_t)cl0 + q;
+        a.jbox[2 * jc] = lo;
+        a.jbox[2 * jc + 1] = hi;
+    }
+    __syncthreads();
+    for (int q = t; q < ncl; q += kColThreads) {
+        const size_t j0 = 2 * ((size_t)cl0 + q);
+        const float4 l0 = a.jbox[2 * j0], h0 = a.jbox[2 * j0 + 1];
+        const float4 l1 = a.jbox[2 * j0 + 2], h1 = a.jbox[2 * j0 + 3];
+        const bool e1 = l1.w != 0.f;                        // empty second half
+        a.ibox[2 * (cl0 + q)] = e1 ? l0 : make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
+        a.ibox[2 * (cl0 + q) + 1] = e1 ? h0 : make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
+        a.ccol[cl0 + q] = c;
+    }
+}
+
 }  // namespace
+
+int launch_col_bin(const ColBinArgs& a, cudaStream_t s, long long* launches)
+{
+    const int nb = a.n > 0 ? (a.n + kBinThreads - 1) / kBinThreads : 1;
+    k_col_count<<<nb, kBinThreads, 0, s>>>(a);
+    *launches += 1;
+    if (a.n > 0) {
+        launch_pdl(k_col_scatter, nb, kBinThreads, 0, s, a);
+        launch_pdl(k_col_sort, a.g.ncol, kColThreads, 0, s, a);
+        *launches += 2;
+    }
+    return (int)cudaGetLastError();
+}
 
 int launch_bin(const BinArgs& a, cudaStream_t s, long long* launches)
 {

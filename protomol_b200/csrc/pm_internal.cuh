@@ -29,6 +29,7 @@ constexpr double kFixedLimit = 4.0e18;               // |value * scale| bound be
 constexpr int kStatusOverflow = 1;
 constexpr int kStatusOutOfGrid = 2;
 constexpr int kStatusListFull = 4;     // cluster-pair list or chunk capacity exceeded
+constexpr int kStatusColumns = 8;      // a column or cluster the column path cannot take (use the cell path)
 
 // FP64 constants of PeriodicBoundaryConditions::set
 // (topology/PeriodicBoundaryConditions.cpp:40-77), orthogonal box.

@@ -41,6 +41,54 @@ constexpr int kCluster = 8;     // atoms per cluster (z-sorted slab of a cell)
 // exact FP64, CSR cell offsets, stable (ascending index) order within a cell.
 int launch_bin(const BinArgs& a, cudaStream_t s, long long* launches);
 
+// ---------------------------------------------------------------- column clusters
+// The mixed pair path of boxes well above twice the cutoff: atoms in
+// unsigned 32-bit fixed point of the box (x / L * 2^32, so that the int32
+// difference of two atoms is their minimal-image displacement exactly), in
+// columns of an x-y grid (~4 A side) sorted by z; every run of 8 atoms of a
+// column is an i-cluster, each half of it a 4-atom j-cluster.
+constexpr int kColAtoms = 1024;  // atoms a column may hold (more: the cell-cluster path)
+struct ColGrid {
+    int ncx, ncy, ncol;
+    int rx, ry;                  // column reach of the list
+    double lx, ly, lz;           // box edges
+    double mnx, mny, mnz;        // box minimum corner (origin - L / 2)
+    float sx, sy;                // column side
+    float lxf, lyf, lzf;         // box edges (FP32)
+    float sch[3], scl[3];        // L / 2^32 per axis, FP32 hi + lo
+    float zext;                  // largest z extent of an i-cluster that keeps every tile's image unique
+};
+
+struct ColBinArgs {
+    int n;
+    const double* pos;
+    const double* q;
+    const int* type;
+    const int* mol;
+    Pbc pbc;
+    CellGrid grid;               // reference cells (bit-exact assignment, reported)
+    int* cell3;                  // 3N reference cell of every atom
+    ColGrid g;
+    unsigned* qfix;              // 3N fixed-point position (atom order)
+    int* col;                    // N column of every atom
+    int* counts;                 // ncol; zero on entry, and again on exit
+    int* done;                   // blocks of the count kernel finished (zero on entry)
+    int* colstart;               // ncol + 1: first atom of each column (compact order)
+    int* ccstart;                // ncol + 1: first i-cluster of each column
+    int* tmp;                    // N
+    int4* cq;                    // slot: qx, qy, qz, charge (FP32 hi, as bits)
+    int4* cm;                    // slot: original index (-1: padding), type, molecule, charge (FP32 lo, as bits)
+    int* slot_of;                // N: slot of every atom
+    float4* ibox;                // 2 per i-cluster: lo, hi (A, box frame [0, L))
+    float4* jbox;                // 2 per j-cluster
+    int* ccol;                   // i-cluster -> column
+    int4* corg;                  // i-cluster -> fixed-point position of its first atom (virial origin)
+    int ncl_cap;                 // i-cluster capacity
+    int* status;
+};
+// K1c: fixed point, columns, z order, clusters and their boxes
+int launch_col_bin(const ColBinArgs& a, cudaStream_t s, long long* launches);
+
 // ---------------------------------------------------------------- pair force
 // FP32 constants of one term; the *_lo members are the FP32 remainders of
 // constants that multiply every pair (their rounding would otherwise bias
@@ -153,6 +201,20 @@ struct PairArgs {
     unsigned long long* efix;    // 11 int64 sums (scale 2^32): LJ, Coulomb, virial
     int blocks_per_sm;           // resident blocks of the mixed pair kernel per SM (0: the occupancy limit)
     int chunk;                   // cluster-list entries per chunk of pair work
+    // column-cluster path (K2a' / K2b'): slot data, cluster boxes, grid
+    const int4* cq;
+    const int4* cm;
+    const float4* ibox;
+    const float4* jbox;
+    const int* ccstart;          // ncol + 1
+    const int* ccol;
+    const int4* corg;            // virial origin of every i-cluster
+    int4* clist;                 // column-path entries (the plist buffer): {jc | flags << 25, o.x, o.y, o.z};
+                                 // o = O_c(j) - O_c(i) + t L (FP32 bits), the tile's virial offset
+    int icl_cap;                 // i-clusters the list kernel's grid covers
+    ColGrid cg;
+    const double* qorig;         // charges, types in atom order (FP64 near-pair energies)
+    const int* torig;
 };
 
 // Combination id of the registered OneAtomPair[Two] templates.
@@ -162,6 +224,12 @@ int launch_cluster_list(const PairArgs& a, cudaStream_t s, long long* launches);
 int launch_pair_mixed(const PairArgs& a, int combo, cudaStream_t s, long long* launches);
 // K2c: FP64 energies of the near pairs listed by the mixed pair kernel
 int launch_near_energy(const PairArgs& a, int combo, int n_atoms, cudaStream_t s, long long* launches);
+// K2a' / K2b' / K2c': the column-cluster list, pair kernel and near-pair energies
+int launch_col_list(const PairArgs& a, cudaStream_t s, long long* launches);
+int launch_pair_col(const PairArgs& a, int combo, cudaStream_t s, long long* launches);
+int launch_near_energy_col(const PairArgs& a, int combo, int n_atoms, cudaStream_t s, long long* launches);
+long long col_list_estimate(int n_atoms, const ColGrid& g, double volume, double cutoff);
+long long col_chunk_estimate(long long entries, int n_atoms, const ColGrid& g, int chunk);
 int launch_pair_fp64(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches);
 int pair_blocks(const CellGrid& g, int nd);
 // blocks of the mixed kernel (4 warps, one energy record per warp)
@@ -240,6 +308,7 @@ struct PmeArgs {
     int* status;
     int virial;
     int fft_lines;               // lines per CTA of the strided FFT passes, at most (0: 16)
+    int energy64_apart;          // mixed: the FP64 energy transform is its own stage (kStageEnergy64)
     // mixed precision: the reciprocal energy and virial from an FP64 forward
     // transform of the charge grid (double2 half spectrum, FP64 twiddles),
     // launched after the gather; null: from the FP32 convolution pass
@@ -248,6 +317,7 @@ struct PmeArgs {
 };
 constexpr int kStageSpread = 0, kStageFft = 1, kStageGather = 2;
 constexpr int kStagePotential = 3;   // dE/dq~ = phi at the atoms, into (double*)facc
+constexpr int kStageEnergy64 = 4;    // mixed: the FP64 energy transform alone (energy64_apart)
 // One stage of the reciprocal term: K3 spread, the five FFT passes with the
 // fused convolution (K4/K5, writes energy records), or K6 gather.
 int launch_pme_reciprocal(const PmeArgs& a, int fp64, cudaStream_t s, long long* launches,
@@ -290,6 +360,14 @@ struct FinArgs {
     const float4* spos;
     const float4* slo;
     int pair_virial;
+    // column-cluster pair forces (2^32) per slot, gathered through slot_of;
+    // their virial from the fixed-point positions (cq) times L / 2^32
+    const unsigned long long* c32;
+    const int* c_slot_of;
+    int c_slots;                         // slots of c32 / cq (an out-of-range slot_of adds nothing)
+    const int4* cq;
+    const int4* corg;                    // virial origin of each i-cluster (slot / 8)
+    double cscale[3];
     double* fout;
     double* erec;
     int erec_stride;

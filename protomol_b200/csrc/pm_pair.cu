@@ -380,6 +380,7 @@ __device__ __forceinline__ void sw_f64(const TermD& t, double d2, double& v, dou
 }
 
 #include "pm_pair_mixed.cuh"
+#include "pm_pair_col.cuh"
 
 template <int NT, int P0, int S0, int P1, int S1>
 __global__ void __launch_bounds__(128) k_pair_fp64(PairArgs p)
@@ -625,6 +626,99 @@ int launch_near_energy(const PairArgs& a, int combo, int n_atoms, cudaStream_t s
     long long want = (30LL * n_atoms + 127) / 128;
     const int blocks = (int)std::max(1LL, std::min<long long>(want, 16LL * sms));
     PM_COMBO_SWITCH(k_near_energy)
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- column path
+long long col_list_estimate(int n_atoms, const ColGrid& g, double volume, double cutoff)
+{
+    // half of the 4-atom j-clusters within the cutoff plus 1.5 column sides
+    // of each i-cluster, with 30% slack
+    const double rho = volume > 0.0 ? n_atoms / volume : 0.0;
+    const double r = cutoff + 1.5 * std::max(g.sx, g.sy);
+    const double per = rho * (4.0 / 3.0) * 3.14159265358979 * r * r * r / 8.0;
+    const double icl = (double)n_atoms / kCluster + g.ncol + 1;
+    return (long long)(1.3 * icl * per) + 4096;
+}
+
+long long col_chunk_estimate(long long entries, int n_atoms, const ColGrid& g, int chunk)
+{
+    return entries / std::max(1, chunk) + (long long)n_atoms / kCluster + g.ncol + 1024;
+}
+
+int launch_col_list(const PairArgs& a, cudaStream_t s, long long* launches)
+{
+    const int blocks = std::max(1, (a.icl_cap + 3) / 4);    // one warp per i-cluster
+    launch_pdl(k_col_list, blocks, 128, 0, s, a);
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+template <int NT, int P0, int S0, int P1, int S1>
+static int run_col(const PairArgs& a, cudaStream_t s, long long* launches)
+{
+    static int sms = 0, per_sm = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_col<NT, P0, S0, P1, S1>, 128, 0);
+        if (sms <= 0) sms = 148;
+        if (per_sm <= 0) per_sm = 1;
+    }
+    const int bps = a.blocks_per_sm > 0 ? std::min(per_sm, a.blocks_per_sm) : per_sm;
+    launch_pdl(k_pair_col<NT, P0, S0, P1, S1>, sms * bps, 128, 0, s, a);
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+int launch_pair_col(const PairArgs& a, int combo, cudaStream_t s, long long* launches)
+{
+    switch (combo) {
+#define PM_COL_CASE(ID, ...) case ID: return run_col<__VA_ARGS__>(a, s, launches);
+    PM_COL_CASE(0, 1, CO, SC1, NP, SUN)
+    PM_COL_CASE(1, 1, CO, SC2, NP, SUN)
+    PM_COL_CASE(2, 1, CO, SCUT, NP, SUN)
+    PM_COL_CASE(3, 1, CO, SSH, NP, SUN)
+    PM_COL_CASE(4, 1, EW, SCUT, NP, SUN)
+    PM_COL_CASE(5, 1, LJ, SC1, NP, SUN)
+    PM_COL_CASE(6, 1, LJ, SC2, NP, SUN)
+    PM_COL_CASE(7, 1, LJ, SCUT, NP, SUN)
+    PM_COL_CASE(8, 1, LJ, SSH, NP, SUN)
+    PM_COL_CASE(9, 2, LJ, SC1, EW, SCUT)
+    PM_COL_CASE(10, 2, LJ, SC1, CO, SSH)
+    PM_COL_CASE(11, 2, LJ, SC2, CO, SC1)
+    PM_COL_CASE(12, 2, LJ, SC2, EW, SCUT)
+    PM_COL_CASE(13, 2, LJ, SC2, CO, SCUT)
+    PM_COL_CASE(14, 2, LJ, SC2, CO, SSH)
+    PM_COL_CASE(15, 2, LJ, SCUT, EW, SCUT)
+    PM_COL_CASE(16, 2, LJ, SC2, CO, SC2)
+    PM_COL_CASE(17, 1, LJT, SUN, NP, SUN)
+    PM_COL_CASE(18, 1, COT, SUN, NP, SUN)
+    PM_COL_CASE(19, 1, EWT, SUN, NP, SUN)
+    PM_COL_CASE(20, 2, LJ, SC1, EWT, SUN)
+    PM_COL_CASE(21, 2, LJ, SC2, EWT, SUN)
+    PM_COL_CASE(22, 2, LJ, SCUT, EWT, SUN)
+    PM_COL_CASE(23, 2, LJT, SUN, EWT, SUN)
+    PM_COL_CASE(24, 2, LJT, SUN, COT, SUN)
+#undef PM_COL_CASE
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+int launch_near_energy_col(const PairArgs& a, int combo, int n_atoms, cudaStream_t s, long long* launches)
+{
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    long long want = (30LL * n_atoms + 127) / 128;
+    const int blocks = (int)std::max(1LL, std::min<long long>(want, 16LL * sms));
+    PM_COMBO_SWITCH(k_near_energy_col)
     *launches += 1;
     return (int)cudaGetLastError();
 }

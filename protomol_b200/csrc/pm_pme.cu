@@ -631,12 +631,16 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
             else k_gather<R><<<nb, 128, 0, s>>>(a);
             *launches += 1;
         }
-        if (sizeof(R) == 4 && a.cgrid64) {
+        if (sizeof(R) == 4 && a.cgrid64 && !a.energy64_apart) {
             int e = (int)cudaGetLastError();
             if (e) return e;
             return run_energy64(a, s, launches, erec_used);
         }
         return (int)cudaGetLastError();
+    }
+    if (stage == kStageEnergy64) {
+        if (sizeof(R) == 4 && a.cgrid64) return run_energy64(a, s, launches, erec_used);
+        return 0;
     }
     if (stage == kStagePotential) {   // a.facc holds the double phi[N] output here
         if (a.n > 0) { k_gather_potential<R><<<nb, 128, 0, s>>>(a, (double*)a.facc); *launches += 1; }
@@ -901,7 +905,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
             if (a.a40) f += (double)(long long)a.a40[3 * (size_t)i + c] * (1.0 / kScaleFp64);
             a.fout[3 * (size_t)i + c] += f;
         }
-        if (a.pair_virial) {
+        if (a.pair_virial & 1) {
             // the cell-relative position the FP32 pair vectors were formed from
             const float4 h = a.spos[s], l = a.slo[s];
             const double p[3] = {(double)h.x + (double)l.x, (double)h.y + (double)l.y, (double)h.z + (double)l.z};
@@ -909,6 +913,30 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
             for (int r = 0; r < 3; ++r)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) v[2 + 3 * r + c] = p[r] * fp[c];
+        }
+        if (a.c32) {
+            // column-cluster pair forces, per slot; their virial from the
+            // fixed-point position the pair vectors were formed from
+            // slot_of is whole only when the column binning completed (a
+            // refused system is redone on the cell layout); never read past c32
+            const int sl = min(max(a.c_slot_of[i], 0), a.c_slots - 1);
+            double fc[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                fc[c] = (double)(long long)a.c32[3 * (size_t)sl + c] * (1.0 / kScaleMixed);
+                a.fout[3 * (size_t)i + c] += fc[c];
+            }
+            if (a.pair_virial & 2) {
+                // position relative to its i-cluster's origin (the first atom)
+                const int4 q = a.cq[sl], o = a.corg[sl >> 3];
+                const double p[3] = {(double)(int)((unsigned)q.x - (unsigned)o.x) * a.cscale[0],
+                                     (double)(int)((unsigned)q.y - (unsigned)o.y) * a.cscale[1],
+                                     (double)(int)((unsigned)q.z - (unsigned)o.z) * a.cscale[2]};
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) v[2 + 3 * r + c] += p[r] * fc[c];
+            }
         }
     }
     if (a.pair_virial) block_reduce_store<8>(v, a.erec, a.erec_stride, blockIdx.x);

@@ -23,8 +23,9 @@
 using namespace pm;
 
 static const double kPi = 3.14159265358979323846;   // Constant::M_PI (base/pmconstants.cpp:56)
-// mixed PME grids from this size on take the FP64 energy path (prepare_pme)
-static const size_t kEnergy64Points = (size_t)128 * 128 * 128;
+// mixed PME grids from this size on take the FP64 energy path (prepare_pme):
+// every grid
+static const size_t kEnergy64Points = 0;
 static const double kEpsilon = 1.0e-14;              // Constant::EPSILON (base/pmconstants.cpp:45)
 // status word, list count and need, chunk count and need, work counter, pad,
 // then 11 int64 energy/virial sums
@@ -61,6 +62,10 @@ struct pmgpu_system {
     // PME runs on a second, higher-priority stream beside the pair kernels
     // (forked after binning, joined before finalize)
     cudaStream_t side = nullptr;
+    // two more branches of the PME work: the correction term, and the FP64
+    // energy transform of a mixed force (both beside the FP32 FFT chain)
+    cudaStream_t side2 = nullptr, side3 = nullptr;
+    cudaEvent_t ev_spread = nullptr, ev_e64 = nullptr, ev_corr = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_pair = nullptr, ev_near = nullptr;   // the last near-pair energies on the side stream
     std::string err;
@@ -139,6 +144,33 @@ struct pmgpu_system {
     int ncell_cap = 0;
     double* d_erec = nullptr;
     int erec_cap = 0;
+    // column-cluster path of the mixed pair forces: the grid of the box
+    // (col_set_grid), per-atom and per-slot buffers; disabled for good when a
+    // column or cluster exceeded the path's limits (the cell path takes over)
+    ColGrid cg;
+    bool col_grid = false;
+    bool col_grid_stale = true;        // box or atom count changed since col_set_grid
+    bool col_disabled = false;
+    bool col_just_disabled = false;
+    bool eval_use_col = false;         // the evaluation being enqueued uses the column path
+    int last_layout = 0;               // pmgpu_pair_layout of the last evaluation with mixed cutoff forces
+    ColGrid eval_cg;                   // its grid with the reach of its cutoffs
+    unsigned* d_qfix = nullptr;
+    int* d_colid = nullptr;
+    int* d_ctmp = nullptr;
+    int* d_cslot = nullptr;
+    int* d_ccounts = nullptr;
+    int* d_colstart = nullptr;
+    int* d_ccstart = nullptr;
+    int col_ncol_cap = 0;
+    int4* d_cq = nullptr;
+    int4* d_cm = nullptr;
+    float4* d_ibox = nullptr;
+    float4* d_jbox = nullptr;
+    int* d_ccol = nullptr;
+    int4* d_corg = nullptr;
+    unsigned long long* d_facc32c = nullptr;
+    int col_ncl_cap = 0;
     std::vector<double> h_fbuf;
     bool binned = false;
     std::set<pmgpu_force*> forces;     // live forces made on this system
@@ -176,6 +208,7 @@ struct pmgpu_force {
     // cutoff
     int combo = -1;
     int box_version = -1;
+    int topo_version = -1;           // PME: the self and charged-system terms depend on the charges
     int nd = 0;
     int4* d_deltas = nullptr;
     float4* d_doff = nullptr;
@@ -261,6 +294,11 @@ extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
     int prio_lo = 0, prio_hi = 0;
     cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     if (cudaStreamCreateWithPriority(&sys->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&sys->side2, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&sys->side3, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sys->ev_spread, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sys->ev_e64, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sys->ev_corr, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&sys->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&sys->ev_join, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&sys->ev_pair, cudaEventDisableTiming) != cudaSuccess ||
@@ -296,6 +334,16 @@ static void free_atom_buffers(pmgpu_system* s)
     s->d_facc32p = nullptr;   // second half of d_facc32
     dfree(s->d_cell_lin); dfree(s->d_cell3); dfree(s->d_tmp); dfree(s->d_sorted); dfree(s->d_slot);
     dfree(s->d_spos); dfree(s->d_smeta); dfree(s->d_spos64);
+    dfree(s->d_qfix); dfree(s->d_colid); dfree(s->d_ctmp); dfree(s->d_cslot);
+}
+
+static void free_col_buffers(pmgpu_system* s)
+{
+    dfree(s->d_ccounts); dfree(s->d_colstart); dfree(s->d_ccstart);
+    dfree(s->d_cq); dfree(s->d_cm); dfree(s->d_ibox); dfree(s->d_jbox); dfree(s->d_ccol); dfree(s->d_facc32c);
+    dfree(s->d_corg);
+    s->col_ncol_cap = 0;
+    s->col_ncl_cap = 0;
 }
 
 static void free_force(pmgpu_force* f);
@@ -313,6 +361,7 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     sys->graphs.clear();
     for (cudaEvent_t e : sys->prof_pool) cudaEventDestroy(e);
     free_atom_buffers(sys);
+    free_col_buffers(sys);
     dfree(sys->d_counts); dfree(sys->d_start); dfree(sys->d_erec);
     dfree(sys->d_small); dfree(sys->d_energy);
     dfree(sys->d_cstart); dfree(sys->d_cbox); dfree(sys->d_ccell); dfree(sys->d_plist); dfree(sys->d_chunks);
@@ -322,6 +371,11 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     cudaEventDestroy(sys->ev_join);
     cudaEventDestroy(sys->ev_pair);
     cudaEventDestroy(sys->ev_near);
+    cudaEventDestroy(sys->ev_spread);
+    cudaEventDestroy(sys->ev_e64);
+    cudaEventDestroy(sys->ev_corr);
+    cudaStreamDestroy(sys->side2);
+    cudaStreamDestroy(sys->side3);
     cudaStreamDestroy(sys->side);
     cudaStreamDestroy(sys->stream);
     delete sys;
@@ -381,6 +435,16 @@ extern "C" int pmgpu_synchronize(pmgpu_system* sys)
     CK(cudaMemcpy(&st, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status");
     if (st & kStatusOverflow)
         return fail(sys, PMGPU_ERR_OVERFLOW, "non-finite or out-of-range force (fixed-point range exceeded)");
+    if (st & kStatusColumns) {
+        // a column held more atoms, or an i-cluster spanned more of the box
+        // height, than the column path takes: the cell-cluster path from now on
+        if (!sys->col_disabled) {
+            sys->col_disabled = true;
+            sys->col_just_disabled = true;
+            sys->buf_version++;
+        }
+        return fail(sys, PMGPU_ERR_CAPACITY, "column clusters out of range (the cell-cluster path is used next)");
+    }
     if (st & kStatusListFull) {
         // list need, chunk count, chunk need, work counter, near count, near need
         int need[6] = {0, 0, 0, 0, 0, 0};
@@ -494,12 +558,74 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     CK(dalloc(&sys->d_tmp, n), "alloc"); CK(dalloc(&sys->d_sorted, n), "alloc"); CK(dalloc(&sys->d_slot, n), "alloc");
     CK(dalloc(&sys->d_spos, n), "alloc"); CK(dalloc(&sys->d_smeta, n), "alloc"); CK(dalloc(&sys->d_spos64, n), "alloc");
     CK(dalloc(&sys->d_slo, n), "alloc"); CK(dalloc(&sys->d_skey, n), "alloc");
+    CK(dalloc(&sys->d_qfix, 3 * (size_t)n), "alloc"); CK(dalloc(&sys->d_colid, n), "alloc");
+    CK(dalloc(&sys->d_ctmp, n), "alloc"); CK(dalloc(&sys->d_cslot, n), "alloc");
+    CK(cudaMemset(sys->d_cslot, 0, sizeof(int) * (size_t)std::max(n, 1)), "memset");
+    sys->col_ncl_cap = 0;   // slot arrays depend on N and the column grid: sized at evaluation
+    sys->col_grid_stale = true;
     sys->cbox_cap = 0;   // cluster boxes depend on N and the cell grid: sized at evaluation
     sys->h_fbuf.assign(3 * (size_t)n, 0.0);
     return PMGPU_OK;
 }
 
 // ------------------------------------------------------------------ box
+// Column grid of the column-cluster pair path for the box: columns of ~4 A
+// in x and y (narrower when a column would hold more than ~384 atoms at the
+// box's mean density), fixed point L / 2^32 per axis.  The reach and the
+// eligibility depend on the cutoff (col_reach).
+static int col_set_grid(pmgpu_system* sys)
+{
+    ColGrid& g = sys->cg;
+    memset(&g, 0, sizeof(g));
+    const double lx = sys->box[0], ly = sys->box[4], lz = sys->box[8];
+    g.lx = lx; g.ly = ly; g.lz = lz;
+    g.mnx = sys->box[9] - 0.5 * lx; g.mny = sys->box[10] - 0.5 * ly; g.mnz = sys->box[11] - 0.5 * lz;
+    const double rho = sys->n > 0 ? sys->n / (lx * ly * lz) : 0.0;
+    double side = 4.0;
+    if (rho * side * side * lz > 384.0) side = std::sqrt(384.0 / (rho * lz));
+    g.ncx = std::max(1, (int)std::floor(lx / side));
+    g.ncy = std::max(1, (int)std::floor(ly / side));
+    sys->col_grid = (long long)g.ncx * g.ncy <= (1 << 22);
+    if (!sys->col_grid) return PMGPU_OK;
+    g.ncol = g.ncx * g.ncy;
+    g.sx = (float)(lx / g.ncx); g.sy = (float)(ly / g.ncy);
+    g.lxf = (float)lx; g.lyf = (float)ly; g.lzf = (float)lz;
+    const double L[3] = {lx, ly, lz};
+    for (int a = 0; a < 3; ++a) {
+        const double u = L[a] / 4294967296.0;
+        g.sch[a] = (float)u;
+        g.scl[a] = (float)(u - (double)g.sch[a]);
+    }
+    if (g.ncol > sys->col_ncol_cap) {
+        CK(dalloc(&sys->d_ccounts, g.ncol), "alloc");
+        CK(dalloc(&sys->d_colstart, g.ncol + 1), "alloc");
+        CK(dalloc(&sys->d_ccstart, g.ncol + 1), "alloc");
+        sys->col_ncol_cap = g.ncol;
+    }
+    // the binning returns the counts to zero; they start there
+    CK(cudaMemsetAsync(sys->d_ccounts, 0, sizeof(int) * (size_t)g.ncol, sys->stream), "memset");
+    return PMGPU_OK;
+}
+
+// Reach of the column list for a pair test at cutoff rc, and whether the
+// column path applies: no column may be reached through two offsets, and the
+// z windows (an i-cluster's extent plus twice the list radius) must be
+// shorter than the box, so that every pair inside the cutoff lies in its
+// tile's image
+static bool col_reach(const pmgpu_system* sys, double rc, ColGrid& g)
+{
+    if (!sys->col_grid || sys->col_disabled) return false;
+    g = sys->cg;
+    const double rl = std::sqrt(rc * rc * (1.0 + 8.0 * 2.0e-5) + 1e-3);
+    g.rx = (int)std::ceil(rl / g.sx) + 1;
+    g.ry = (int)std::ceil(rl / g.sy) + 1;
+    if (2 * g.rx + 1 > g.ncx || 2 * g.ry + 1 > g.ncy) return false;
+    const double zext = g.lz - 2.0 * rl - 0.5;
+    if (!(zext > 1.0)) return false;
+    g.zext = (float)zext;
+    return true;
+}
+
 extern "C" int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* e2, const double* e3,
                              const double* origin, double cell_size)
 {
@@ -556,6 +682,7 @@ extern "C" int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* 
     }
     // the binning leaves the counts at zero; they start there
     CK(cudaMemsetAsync(sys->d_counts, 0, sizeof(int) * (size_t)g.ncell, sys->stream), "memset");
+    sys->col_grid_stale = true;
     sys->box_set = true;
     sys->box_version++;
     sys->binned = false;
@@ -1081,7 +1208,7 @@ extern "C" int pmgpu_pme_create(pmgpu_system* sys, const pmgpu_pme_params* p, pm
 static int prepare_pme(pmgpu_force* f)
 {
     pmgpu_system* sys = f->sys;
-    if (f->box_version == sys->box_version) return PMGPU_OK;
+    if (f->box_version == sys->box_version && f->topo_version == sys->topo_version) return PMGPU_OK;
     if (f->real_sub && !(std::fabs(sys->box[0]) > 2.0 * f->pp.cutoff && std::fabs(sys->box[4]) > 2.0 * f->pp.cutoff &&
                          std::fabs(sys->box[8]) > 2.0 * f->pp.cutoff))
         return fail(sys, PMGPU_ERR_UNSUPPORTED, "PMEwald -real needs every box edge > 2 cutoff on the GPU "
@@ -1145,14 +1272,13 @@ static int prepare_pme(pmgpu_force* f)
         CK(dalloc((float2**)&f->d_cgrid, nhalf), "alloc");
         CK(dalloc((float**)&f->d_rgrid, nreal), "alloc");
         CK(dalloc(&f->d_qgrid, nreal), "alloc");
-        // grids of 128^3 points and more: the reciprocal energy and virial
-        // from FP64 B-spline weights and an FP64 forward transform of the
-        // fixed-point charge grid.  With FP32 there the transform's rounding
-        // reaches the total energy of the large boxes, where the real-space,
-        // reciprocal and self terms nearly cancel (1,000,000 atoms at 216^3:
-        // 5.9e-7 of the total with FP32, 1.3e-7 with FP64).  On smaller grids
-        // the FP32 energy meets 1e-7 and the FP64 passes would cost ~8% of
-        // the evaluation (they share the SMs with the pair kernel).
+        // the reciprocal energy and virial from FP64 B-spline weights and an
+        // FP64 forward transform of the fixed-point charge grid; the FP32
+        // chain gives the forces.  With the FP32 weights and transform the
+        // reciprocal energy is off by ~1e-3 kcal/mol per 10^4 atoms, which
+        // reaches the total energy of water boxes (a near cancellation of
+        // the real-space, reciprocal and self terms): 2.5e-7 of the total on
+        // a 9,000-atom box at 45^3, 5.9e-7 on 1,000,000 atoms at 216^3.
         if (nreal >= kEnergy64Points) {
             CK(dalloc((double2**)&f->d_tw64, ntw), "alloc");
             CK(cudaMemcpy(f->d_tw64, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice), "copy");
@@ -1172,6 +1298,7 @@ static int prepare_pme(pmgpu_force* f)
     if (p.correction && std::fabs(q1 * 0.00268283) > 1.0e-5)
         f->charged_energy = -kPi / (2.0 * V * (alpha * alpha)) * q1 * q1;
     f->box_version = sys->box_version;
+    f->topo_version = sys->topo_version;
     return PMGPU_OK;
 }
 
@@ -1224,6 +1351,38 @@ static int bin(pmgpu_system* sys, const double* d_pos)
     if (e) return cuda_fail(sys, (cudaError_t)e, "binning");
     sys->binned = true;
     return PMGPU_OK;
+}
+
+// K1c: the column-cluster layout of the positions (and the reference cell of
+// every atom, as bin() gives it)
+static int col_bin(pmgpu_system* sys, const double* d_pos)
+{
+    ColBinArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = sys->n; a.pos = d_pos; a.q = sys->d_q; a.type = sys->d_type; a.mol = sys->d_mol;
+    a.pbc = sys->pbc; a.grid = sys->grid; a.cell3 = sys->d_cell3;
+    a.g = sys->eval_cg;
+    a.qfix = sys->d_qfix; a.col = sys->d_colid; a.counts = sys->d_ccounts; a.done = sys->d_status + 9;
+    a.colstart = sys->d_colstart; a.ccstart = sys->d_ccstart; a.tmp = sys->d_ctmp;
+    a.cq = sys->d_cq; a.cm = sys->d_cm; a.slot_of = sys->d_cslot;
+    a.ibox = sys->d_ibox; a.jbox = sys->d_jbox; a.ccol = sys->d_ccol; a.ncl_cap = sys->col_ncl_cap;
+    a.corg = sys->d_corg;
+    a.status = sys->d_status;
+    int e = launch_col_bin(a, sys->stream, &sys->launches);
+    if (e) return cuda_fail(sys, (cudaError_t)e, "column binning");
+    sys->binned = true;
+    return PMGPU_OK;
+}
+
+// the column-path members of the pair arguments
+static void fill_col_args(pmgpu_system* sys, PairArgs& a)
+{
+    a.cq = sys->d_cq; a.cm = sys->d_cm; a.ibox = sys->d_ibox; a.jbox = sys->d_jbox;
+    a.ccstart = sys->d_ccstart; a.ccol = sys->d_ccol; a.icl_cap = sys->col_ncl_cap; a.corg = sys->d_corg;
+    a.clist = (int4*)sys->d_plist;          // entries of two int2 places each (plist_cap counts int2)
+    a.cg = sys->eval_cg;
+    a.qorig = sys->d_q; a.torig = sys->d_type;
+    a.facc = sys->d_facc32c;
 }
 
 static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_pos, PairArgs& a)
@@ -1318,12 +1477,58 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
         sys->cbox_cap = ncl;
         sys->buf_version++;
     }
-    long long lneed = 0, cneed = 0;
-    for (int k = 0; k < nf; ++k)
-        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) {
-            lneed = std::max(lneed, plist_estimate(sys->n, sys->grid, forces[k]->nh));
-            cneed = std::max(cneed, chunk_estimate(sys->n, sys->grid, forces[k]->nh, sys->tuning.chunk_entries));
+    // the column-cluster path takes the mixed cutoff forces of the group when
+    // none of them is in the small-grid mode and the box suits the largest
+    // of their cutoffs; otherwise the cell-cluster path takes them all
+    sys->eval_use_col = false;
+    {
+        double rc2 = 0.0;
+        bool any = false, ok = true;
+        for (int k = 0; k < nf; ++k)
+            if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) {
+                any = true;
+                ok = ok && !forces[k]->wrap;
+                rc2 = std::max(rc2, forces[k]->cut2);
+            }
+        if (any && ok) {
+            if (sys->col_grid_stale) {
+                int rg = col_set_grid(sys);
+                if (rg) return rg;
+                sys->col_grid_stale = false;
+            }
+            ColGrid g;
+            if (col_reach(sys, std::sqrt(rc2), g)) {
+                sys->eval_use_col = true;
+                sys->eval_cg = g;
+            }
         }
+    }
+    long long lneed = 0, cneed = 0;
+    if (sys->eval_use_col) {
+        const ColGrid& g = sys->eval_cg;
+        const int icl = sys->n / kCluster + g.ncol + 1;
+        if (icl > sys->col_ncl_cap) {
+            const size_t slots = (size_t)kCluster * icl;
+            CK(dalloc(&sys->d_cq, slots), "alloc"); CK(dalloc(&sys->d_cm, slots), "alloc");
+            CK(dalloc(&sys->d_ibox, 2 * (size_t)icl), "alloc"); CK(dalloc(&sys->d_jbox, 4 * (size_t)icl), "alloc");
+            CK(dalloc(&sys->d_ccol, (size_t)icl), "alloc"); CK(dalloc(&sys->d_facc32c, 3 * slots), "alloc");
+            CK(dalloc(&sys->d_corg, (size_t)icl), "alloc");
+            sys->col_ncl_cap = icl;
+            sys->buf_version++;
+        }
+        double rc2 = 0.0;
+        for (int k = 0; k < nf; ++k)
+            if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) rc2 = std::max(rc2, forces[k]->cut2);
+        const long long entries = col_list_estimate(sys->n, g, g.lx * g.ly * g.lz, std::sqrt(rc2));
+        lneed = 2 * entries;                  // int4 entries in the int2 list buffer
+        cneed = col_chunk_estimate(entries, sys->n, g, sys->tuning.chunk_entries);
+    } else {
+        for (int k = 0; k < nf; ++k)
+            if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) {
+                lneed = std::max(lneed, plist_estimate(sys->n, sys->grid, forces[k]->nh));
+                cneed = std::max(cneed, chunk_estimate(sys->n, sys->grid, forces[k]->nh, sys->tuning.chunk_entries));
+            }
+    }
     if (lneed > 0) {
         lneed = std::max(lneed, sys->plist_need + sys->plist_need / 4);
         cneed = std::max(cneed, sys->chunk_need + sys->chunk_need / 4);
@@ -1403,9 +1608,25 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         any_full |= forces[k]->kind == 2;
     }
     if (any_pme || any_full) CK(cudaMemsetAsync(sys->d_faccA, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
+    const bool use_col = sys->eval_use_col;
+    for (int k = 0; k < nf; ++k)
+        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64)
+            sys->last_layout = use_col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS;
+    if (use_col)
+        CK(cudaMemsetAsync(sys->d_facc32c, 0, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap, s),
+           "memset");
+    // the cell-sorted order: for the FP64 cutoff forces, and for the mixed
+    // ones when the column path does not take them
+    bool cell_sort = false;
+    for (int k = 0; k < nf; ++k)
+        if (forces[k]->kind == 0 && (forces[k]->precision == PMGPU_PRECISION_FP64 || !use_col)) cell_sort = true;
     int used = 0;
-    // PME: reads only positions and charges and accumulates in atom order
-    auto enqueue_pme = [&](cudaStream_t ps) -> int {
+    // PME: reads only positions and charges and accumulates in atom order.
+    // Beside the pair kernels (branches = true) the correction term and the
+    // FP64 energy transform of a mixed force run on branches of their own,
+    // joined back into ps at the end.
+    auto enqueue_pme = [&](cudaStream_t ps, bool branches) -> int {
+        bool corr_branch = false, e64_branch = false;
         for (int k = 0; k < nf; ++k) {
             pmgpu_force* f = forces[k];
             if (f->kind != 1) continue;
@@ -1425,7 +1646,14 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 c.const_virial = f->charged_energy;
                 int b = 0;
                 int m = prof_begin(sys, kPhaseCorrection);
-                int e = launch_pme_correction(c, ps, &sys->launches, &b);
+                cudaStream_t cs = ps;
+                if (branches && !corr_branch) {
+                    CK(cudaEventRecord(sys->ev_corr, ps), "fork");
+                    CK(cudaStreamWaitEvent(sys->side3, sys->ev_corr, 0), "fork");
+                    corr_branch = true;
+                }
+                if (corr_branch) cs = sys->side3;
+                int e = launch_pme_correction(c, cs, &sys->launches, &b);
                 if (e) return cuda_fail(sys, (cudaError_t)e, "PME correction");
                 prof_end(sys, m);
                 used += b;
@@ -1449,6 +1677,8 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 a.wr = 1.0 / LX; a.lr = 1.0 / LY; a.hr = 1.0 / LZ;
                 a.facc = facc; a.scale = scale; a.qscale = kScaleFp64; a.erec_stride = sys->erec_cap;
                 a.status = sys->d_status; a.virial = virial; a.fft_lines = sys->tuning.fft_lines;
+                const bool e64 = branches && a.cgrid64 != nullptr && !e64_branch;
+                a.energy64_apart = e64 ? 1 : 0;
                 const int phases[3] = {kPhaseSpread, kPhaseFft, kPhaseGather};
                 const int stages[3] = {kStageSpread, kStageFft, kStageGather};
                 for (int st = 0; st < 3; ++st) {
@@ -1459,8 +1689,28 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                     if (e) return cuda_fail(sys, (cudaError_t)e, "PME reciprocal");
                     used += u;
                     prof_end(sys, m);
+                    if (st == 0 && e64) {
+                        // the FP64 energy transform reads only the charge grid:
+                        // from the spread on, beside the FP32 transform and gather
+                        CK(cudaEventRecord(sys->ev_spread, ps), "fork");
+                        CK(cudaStreamWaitEvent(sys->side2, sys->ev_spread, 0), "fork");
+                        u = 0;
+                        e = launch_pme_reciprocal(a, 0, sys->side2, &sys->launches, sys->d_erec + used, &u,
+                                                  kStageEnergy64);
+                        if (e) return cuda_fail(sys, (cudaError_t)e, "PME energy transform");
+                        used += u;
+                        e64_branch = true;
+                    }
                 }
             }
+        }
+        if (corr_branch) {
+            CK(cudaEventRecord(sys->ev_corr, sys->side3), "join");
+            CK(cudaStreamWaitEvent(ps, sys->ev_corr, 0), "join");
+        }
+        if (e64_branch) {
+            CK(cudaEventRecord(sys->ev_e64, sys->side2), "join");
+            CK(cudaStreamWaitEvent(ps, sys->ev_e64, 0), "join");
         }
         return PMGPU_OK;
     };
@@ -1471,12 +1721,16 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     if (fork) {
         CK(cudaEventRecord(sys->ev_fork, s), "fork");
         CK(cudaStreamWaitEvent(sys->side, sys->ev_fork, 0), "fork");
-        r = enqueue_pme(sys->side);
+        r = enqueue_pme(sys->side, true);
         if (r) return r;
         CK(cudaEventRecord(sys->ev_join, sys->side), "join");
     }
-    if (any_cut) {   // the cell-sorted order is for the cutoff forces only
+    if (cell_sort) {
         r = bin(sys, d_pos);
+        if (r) return r;
+    }
+    if (use_col) {
+        r = col_bin(sys, d_pos);
         if (r) return r;
     }
     prof_end(sys, mbin);
@@ -1503,39 +1757,46 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) last_mixed = k;
     bool near_on_side = false;
     int lists = 0;
-    int pair_virial = 0;
+    int pair_virial = 0, col_virial = 0;
     for (int k = 0; k < nf; ++k) {
         pmgpu_force* f = forces[k];
         if (f->kind != 0) continue;
         const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
-        if (!fp64 && !f->wrap && virial) pair_virial = 1;
+        const bool col = !fp64 && use_col;
+        if (!fp64 && !col && !f->wrap && virial) pair_virial = 1;
+        if (col && virial) col_virial = 1;
         PairArgs a;
         fill_pair_args(sys, f, d_pos, a);
+        if (col) fill_col_args(sys, a);
         a.virial = virial;
         a.erec = sys->d_erec + used;
         if (!fp64) {
             // list count and need, chunk count and need, work counter
             if (lists++ > 0) CK(cudaMemsetAsync(sys->d_plist_count, 0, 6 * sizeof(int), s), "memset");
             int ml = prof_begin(sys, kPhaseList);
-            int e = launch_cluster_list(a, s, &sys->launches);
+            int e = col ? launch_col_list(a, s, &sys->launches) : launch_cluster_list(a, s, &sys->launches);
             if (e) return cuda_fail(sys, (cudaError_t)e, "cluster-pair list");
             prof_end(sys, ml);
         }
         int m = prof_begin(sys, kPhasePair);
         int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
-                     : launch_pair_mixed(a, f->combo, s, &sys->launches);
+                     : (col ? launch_pair_col(a, f->combo, s, &sys->launches)
+                            : launch_pair_mixed(a, f->combo, s, &sys->launches));
         if (!e && !fp64 && a.near2 > 0.0f) {
             // the last cutoff force's near-pair energies (needed only by the
             // energy reduction) run on the side stream, after PME, beside
             // finalize; earlier forces' before the next list reuses the buffer
+            cudaStream_t ns = s;
             if (fork && k == last_mixed) {
                 CK(cudaEventRecord(sys->ev_pair, s), "event");
                 CK(cudaStreamWaitEvent(sys->side, sys->ev_pair, 0), "event");
-                e = launch_near_energy(a, f->combo, sys->n, sys->side, &sys->launches);
+                ns = sys->side;
+            }
+            e = col ? launch_near_energy_col(a, f->combo, sys->n, ns, &sys->launches)
+                    : launch_near_energy(a, f->combo, sys->n, ns, &sys->launches);
+            if (ns != s) {
                 CK(cudaEventRecord(sys->ev_near, sys->side), "event");
                 near_on_side = true;
-            } else {
-                e = launch_near_energy(a, f->combo, sys->n, s, &sys->launches);
             }
         }
         if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
@@ -1545,7 +1806,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     if (fork) {
         CK(cudaStreamWaitEvent(s, sys->ev_join, 0), "join");
     } else if (any_pme) {
-        r = enqueue_pme(s);
+        r = enqueue_pme(s, false);
         if (r) return r;
     }
     int mfin = prof_begin(sys, kPhaseFinalize);
@@ -1554,16 +1815,24 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         memset(&fa, 0, sizeof(fa));
         fa.n = sys->n;
         // the slot-ordered accumulators exist only with the cell-sorted order
-        fa.f32 = use32 && any_cut ? sys->d_facc32 : nullptr;
-        fa.f32p = use32 && any_cut ? sys->d_facc32p : nullptr;
-        fa.f40 = use40 && any_cut ? sys->d_facc40 : nullptr;
+        fa.f32 = use32 && cell_sort ? sys->d_facc32 : nullptr;
+        fa.f32p = use32 && cell_sort ? sys->d_facc32p : nullptr;
+        fa.f40 = use40 && cell_sort ? sys->d_facc40 : nullptr;
+        if (use_col) {
+            fa.c32 = sys->d_facc32c; fa.c_slot_of = sys->d_cslot; fa.cq = sys->d_cq;
+            fa.c_slots = kCluster * sys->col_ncl_cap;
+            fa.corg = sys->d_corg;
+            fa.cscale[0] = sys->eval_cg.lx / 4294967296.0;
+            fa.cscale[1] = sys->eval_cg.ly / 4294967296.0;
+            fa.cscale[2] = sys->eval_cg.lz / 4294967296.0;
+        }
         for (int k = 0; k < nf; ++k)
             if (forces[k]->kind != 0) {
                 if (forces[k]->precision == PMGPU_PRECISION_FP64) fa.a40 = sys->d_faccA + n3;
                 else fa.a32 = sys->d_faccA;
             }
-        fa.sorted = any_cut ? sys->d_sorted : nullptr; fa.spos = sys->d_spos; fa.slo = sys->d_slo;
-        fa.pair_virial = pair_virial;
+        fa.sorted = cell_sort ? sys->d_sorted : nullptr; fa.spos = sys->d_spos; fa.slo = sys->d_slo;
+        fa.pair_virial = pair_virial | (col_virial << 1);
         fa.fout = d_fout;
         fa.erec = sys->d_erec + used; fa.erec_stride = sys->erec_cap;
         int rec = 0;
@@ -1669,9 +1938,10 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
         if (r) return r;
         CK(cudaMemcpyAsync(sys->h_fbuf.data(), sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
         CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kERec, cudaMemcpyDeviceToHost, s), "D2H energies");
+        sys->col_just_disabled = false;
         r = pmgpu_synchronize(sys);
         if (!(r == PMGPU_ERR_CAPACITY && (sys->plist_need > sys->plist_cap || sys->chunk_need > sys->chunk_cap ||
-                                          sys->near_need > sys->near_cap)))
+                                          sys->near_need > sys->near_cap || sys->col_just_disabled)))
             break;
     }
     if (r) return r;
@@ -1684,6 +1954,8 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
 }
 
 // ------------------------------------------------------------------ diagnostics
+extern "C" int pmgpu_pair_layout(pmgpu_system* sys) { return sys ? sys->last_layout : 0; }
+
 extern "C" int pmgpu_get_cells(pmgpu_system* sys, int* cells, int* dims)
 {
     if (!sys || !cells || !dims) return PMGPU_ERR_ARG;
@@ -1711,9 +1983,17 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
     CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
-    r = bin(sys, sys->d_pos);
-    if (r) return r;
     bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+    const bool col = !fp64 && sys->eval_use_col;          // eval_prepare decided for this force alone
+    if (!fp64) sys->last_layout = col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS;
+    if (col) {
+        CK(cudaMemsetAsync(sys->d_facc32c, 0, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap, s),
+           "memset");
+        r = col_bin(sys, sys->d_pos);
+    } else {
+        r = bin(sys, sys->d_pos);
+    }
+    if (r) return r;
     r = ensure_erec(sys, std::max(1, pair_records(sys, f)));
     if (r) return r;
     int* d_pairs = nullptr;
@@ -1724,15 +2004,27 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     CK(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s), "memset");
     PairArgs a;
     fill_pair_args(sys, f, sys->d_pos, a);
+    if (col) fill_col_args(sys, a);
     a.near2 = 0.0f;                                    // recording only: no near-pair list
     a.erec = sys->d_erec;
     a.rec_pairs = d_pairs; a.rec_count = d_count; a.rec_cap = dcap;
     int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
-                 : launch_cluster_list(a, s, &sys->launches);
-    if (!e && !fp64) e = launch_pair_mixed(a, f->combo, s, &sys->launches);
+                 : (col ? launch_col_list(a, s, &sys->launches) : launch_cluster_list(a, s, &sys->launches));
+    if (!e && !fp64) e = col ? launch_pair_col(a, f->combo, s, &sys->launches)
+                             : launch_pair_mixed(a, f->combo, s, &sys->launches);
     unsigned long long cnt = 0;
+    int st = 0;
     if (!e) e = (int)cudaMemcpyAsync(&cnt, d_count, sizeof(cnt), cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(&st, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
+    if (!e && (st & (kStatusListFull | kStatusColumns))) {
+        // the list did not fit (or the column path refused the system): the
+        // recording is incomplete; the next call runs with the grown buffers
+        cudaFree(d_pairs);
+        cudaFree(d_count);
+        (void)pmgpu_synchronize(sys);                  // records the sizes needed (and its message)
+        return PMGPU_ERR_CAPACITY;
+    }
     if (!e && cnt > 0 && cap > 0)
         e = (int)cudaMemcpy(pairs, d_pairs, sizeof(int) * 2 * (size_t)std::min<long long>(cnt, cap), cudaMemcpyDeviceToHost);
     cudaFree(d_pairs);

@@ -120,6 +120,12 @@ class Topology:
                                  _lib.FLAG_VIRIAL if virial else 0, int(evals), C.byref(t)), self.handle)
         return t.as_dict()
 
+    def pair_layout(self) -> str:
+        """Cluster layout of the last evaluation's mixed cutoff forces:
+        'columns' (fixed-point coordinates in z-sorted columns), 'cells'
+        (clusters inside the reference cells) or '' (none yet)."""
+        return {1: "cells", 2: "columns"}.get(int(_lib.load().pmgpu_pair_layout(self.handle)), "")
+
     def cells(self):
         cells = np.zeros((self.n_atoms, 3), np.int32)
         dims = np.zeros(3, np.int32)
@@ -185,8 +191,14 @@ class SystemForce:
         cap = cap or max(1024, pos.shape[0] * 1200)
         out = np.zeros((cap, 2), np.int32)
         cnt = C.c_longlong(0)
-        check(_lib.load().pmgpu_get_pairs(self.topo.handle, self.handle, pos.ctypes.data_as(_VP), C.byref(cnt),
-                                          out.ctypes.data_as(_VP), cap), self.topo.handle)
+        lib = _lib.load()
+        for attempt in range(3):
+            # a list that outgrew its estimate is grown and the recording rerun
+            rc = lib.pmgpu_get_pairs(self.topo.handle, self.handle, pos.ctypes.data_as(_VP), C.byref(cnt),
+                                     out.ctypes.data_as(_VP), cap)
+            if rc != 7 or cnt.value > cap:
+                break
+        check(rc, self.topo.handle)
         return out[: cnt.value]
 
 

@@ -306,6 +306,7 @@ def test_million_atom_box_at_full_size():
     s = w.system
     assert s.n_atoms == 1_000_000
     topo_m, _, fm, em = gpu_eval(s, w.forces, "mixed")
+    topo_m_layout = topo_m.pair_layout()
     cells, dims = topo_m.cells()
     ocells, odims, _ = oracle.cell_assign(s, s.positions)
     assert dims == odims and np.array_equal(cells, ocells)
@@ -319,11 +320,12 @@ def test_million_atom_box_at_full_size():
           f"LJ rel {abs(em.lennard_jones - ed.lennard_jones) / abs(ed.lennard_jones):.2e}  virial frob rel "
           f"{np.linalg.norm(em.virial_tensor - ed.virial_tensor) / np.linalg.norm(ed.virial_tensor):.2e}")
     # 216^3 takes FP64 B-spline weights and an FP64 forward transform for the
-    # reciprocal energy and virial: the virial within the metric-system bound.
-    # The total energy (-35,145 kcal/mol, a tenfold cancellation of the LJ,
-    # real-space, reciprocal and self terms) keeps the FP32 pair energies
-    # beyond 5 A (measured +3.0e-3 LJ, +1.6e-3 Coulomb: 1.3e-7 of the total)
+    # reciprocal energy and virial.  The total energy (-35,145 kcal/mol, a
+    # tenfold cancellation of the LJ, real-space, reciprocal and self terms)
+    # holds the metric-system bound: the column layout's fixed-point pair
+    # vectors carry no shared rounding into the FP32 pair energies
+    assert topo_m_layout == "columns"
     assert abs(em.lennard_jones - ed.lennard_jones) <= MIXED_METRIC_ENERGY_RTOL * abs(ed.lennard_jones)
-    assert abs(etot - dtot) <= 2 * MIXED_METRIC_ENERGY_RTOL * abs(dtot)
+    assert abs(etot - dtot) <= MIXED_METRIC_ENERGY_RTOL * abs(dtot)
     assert np.linalg.norm(em.virial_tensor - ed.virial_tensor) <= \
         MIXED_METRIC_ENERGY_RTOL * np.linalg.norm(ed.virial_tensor)

@@ -44,3 +44,32 @@ def test_chain14281_split_pme_against_reference():
     assert np.abs(a["forces"] - b["forces"]).max() <= 1e-12 * rms
     assert abs(a["lennard_jones"] - b["lennard_jones"]) <= 1e-12 * abs(b["lennard_jones"])
     assert abs(a["coulomb"] - b["coulomb"]) <= 1e-9 * abs(b["coulomb"])
+
+
+def charged_chain():
+    """The 1,260-atom chain in water with half an elementary charge added to
+    one chain atom: a non-neutral box, where PME adds the charged-system term
+    -pi (sum q~)^2 / (2 V alpha^2) to the energy and the virial diagonal
+    (forces/NonbondedPMEwaldSystemForce.h:604-628)."""
+    s = systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+    s.scaled_charge = s.scaled_charge.copy()
+    s.scaled_charge[5] += 0.5 * systems.SQRT_COULOMB_CONSTANT
+    return s
+
+
+def test_charged_system_pme_against_reference():
+    s = charged_chain()
+    assert abs(s.scaled_charge.sum() * 0.00268283) > 1e-5      # the term is on
+    d = ("Coulomb -algorithm PMEwald -real -reciprocal -correction -interpolation BSpline "
+         "-gridsize 24 24 24 -cutoff 9 -alpha 0.35")
+    specs = [F.parse_definition(d)]
+    a = oracle.evaluate(s, specs)
+    b = oracle.run_reference(s, specs)
+    rms = np.sqrt((b["forces"] ** 2).sum(1).mean())
+    assert np.abs(a["forces"] - b["forces"]).max() <= 1e-11 * rms
+    assert abs(a["coulomb"] - b["coulomb"]) <= 1e-10 * abs(b["coulomb"])
+    assert np.abs(a["virial"] - b["virial"]).max() <= 1e-10 * np.abs(b["virial"]).max()
+    # the same box made neutral again differs by the charged term alone on the diagonal
+    n = systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+    c = oracle.evaluate(n, specs)
+    assert c["coulomb"] != a["coulomb"]
