@@ -313,6 +313,11 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         t_e2e = float(t[0])
 
+    # the ProtoMol drop-in: the same two forces made by ProtoMol's own
+    # ForceFactory and evaluated through SystemForce::evaluate into a
+    # Vector3DBlock (the adapter's group of GPU forces runs as one call)
+    e2e_adapter = measure_adapter(s, w.forces, max(20, min(args.steps, 400)))
+
     # per-phase device times (CUDA events on the library's stream) over a
     # profiled copy of the timed loop, for the rooflines
     phases = profile_phases(lib, topo, mixed, step, flush, stream, torch, max(50, min(args.steps, 400)))
@@ -361,6 +366,7 @@ def main():
             "accuracy_vs_fp64": {"force_rel_rms": force_err, "energy_rel": e_err},
             "e2e": {"value": world * 1000.0 / t_e2e, "unit": UNIT, "ms_per_step": t_e2e,
                     "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 88},
+            "e2e_adapter": e2e_adapter,
             "gpu_launches": int(launches),
             "pair_interactions_per_s": n_pairs * world * 1000.0 / t_local,
             "roofline": roofline,
@@ -376,6 +382,29 @@ def main():
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def measure_adapter(system, defs, repeat):
+    """Evaluations/s through ProtoMol's own ForceFactory and SystemForce::
+    evaluate (protomol_b200/adapter/_build/gpu_force_driver, built where the
+    ProtoMol sources are): Vector3DBlock positions in, forces accumulated
+    into a Vector3DBlock, energies into a ScalarStructure; the driver's wall
+    clock per evaluation over ``repeat`` evaluations after one warm-up."""
+    import tempfile
+    driver = os.path.join(ROOT, "protomol_b200", "adapter", "_build", "gpu_force_driver")
+    if not os.path.exists(driver):
+        return {"unavailable": "the drop-in driver was not built (it links the ProtoMol sources)"}
+    with tempfile.TemporaryDirectory() as td:
+        sp, op = os.path.join(td, "s.bin"), os.path.join(td, "o.bin")
+        system.save(sp)
+        p = subprocess.run([driver, sp, op, str(repeat), *defs], capture_output=True, text=True, timeout=600,
+                           env=dict(os.environ, PMGPU_PRECISION="mixed"))
+        if p.returncode != 0:
+            return {"unavailable": f"driver exit {p.returncode}"}
+        sec = float(np.frombuffer(open(op, "rb").read(104), np.float64)[11])
+    return {"value": 1.0 / sec, "unit": UNIT, "ms_per_step": sec * 1000.0, "evaluations": repeat,
+            "path": "ForceFactory::make -> GpuNonbondedForce::evaluate (one pmgpu_evaluate per group) "
+                    "-> Vector3DBlock / ScalarStructure, wall clock"}
 
 
 def measure_batched(local, rank, world, pg, torch, flush, steps):

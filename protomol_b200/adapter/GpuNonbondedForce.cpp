@@ -4,6 +4,7 @@ using namespace ProtoMol::Report;
 
 #include "GpuNonbondedForce.h"
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -46,13 +47,44 @@ namespace ProtoMol
 		size_t n = 0;
 		double box[12];
 		double cell = 0.0;
-		bool dirty = true;
+		bool dirty = true;            // upload the topology
+		bool recheck = false;         // uncache(): upload it again only if it changed
+		unsigned long long digest = 0;
 	};
+
+	// A digest of the topology members the GPU forces read, so that uncache()
+	// (which the integrators call for box changes, Integrator.cpp:153) does
+	// not re-upload an unchanged topology
+	static unsigned long long topology_digest(const GenericTopology* topo)
+	{
+		unsigned long long h = 1469598103934665603ull;
+		auto mix = [&h](const void* p, size_t n) {
+			const unsigned char* c = (const unsigned char*)p;
+			for (size_t k = 0; k < n; ++k) { h ^= c[k]; h *= 1099511628211ull; }
+		};
+		for (size_t i = 0; i < topo->atoms.size(); ++i) {
+			mix(&topo->atoms[i].scaledCharge, sizeof(Real));
+			mix(&topo->atoms[i].type, sizeof(topo->atoms[i].type));
+			mix(&topo->atoms[i].molecule, sizeof(topo->atoms[i].molecule));
+		}
+		const std::vector<ExclusionPair>& tab = topo->exclusions.getTable();
+		for (size_t k = 0; k < tab.size(); ++k) {
+			mix(&tab[k].a1, sizeof(tab[k].a1)); mix(&tab[k].a2, sizeof(tab[k].a2)); mix(&tab[k].excl, sizeof(tab[k].excl));
+		}
+		int t = topo->lennardJonesParameters.size();
+		for (int a = 0; a < t; ++a)
+			for (int b = 0; b < t; ++b) {
+				const LennardJonesParameters& p = topo->lennardJonesParameters(a, b);
+				mix(&p.A, sizeof(p.A)); mix(&p.B, sizeof(p.B)); mix(&p.A14, sizeof(p.A14)); mix(&p.B14, sizeof(p.B14));
+			}
+		mix(&topo->coulombScalingFactor, sizeof(topo->coulombScalingFactor));
+		return h;
+	}
 
 	static std::map<const GenericTopology*, GpuContext>& contexts()
 	{
-		static std::map<const GenericTopology*, GpuContext> m;
-		return m;
+		static std::map<const GenericTopology*, GpuContext>* m = new std::map<const GenericTopology*, GpuContext>();
+		return *m;
 	}
 
 	static void gpu_fail(pmgpu_system* sys, const std::string& what)
@@ -80,6 +112,10 @@ namespace ProtoMol
 		                        &pt->boundaryConditions.e3(), &pt->boundaryConditions.origin()};
 		for (int k = 0; k < 4; ++k) { box[3 * k] = v[k]->x; box[3 * k + 1] = v[k]->y; box[3 * k + 2] = v[k]->z; }
 		double cell = pt->cellManager.getCellSize();
+		if (c.recheck && !c.dirty && c.n == topo->atoms.size()) {
+			c.dirty = topology_digest(topo) != c.digest;
+			c.recheck = false;
+		}
 		if (c.dirty || c.n != topo->atoms.size()) {
 			size_t n = topo->atoms.size();
 			std::vector<double> q(n);
@@ -110,6 +146,8 @@ namespace ProtoMol
 			c.n = n;
 			c.cell = -1.0;
 			c.dirty = false;
+			c.recheck = false;
+			c.digest = topology_digest(topo);
 		}
 		if (c.cell != cell || memcmp(c.box, box, sizeof(box)) != 0) {
 			if (pmgpu_set_box(c.sys, box, box + 3, box + 6, box + 9, cell) != PMGPU_OK) gpu_fail(c.sys, "set_box");
@@ -117,6 +155,40 @@ namespace ProtoMol
 			c.cell = cell;
 		}
 		return c;
+	}
+
+	// ForceGroup::evaluateSystemForces (forces/ForceGroup.cpp:43-96) calls the
+	// system forces of a group one after another into the same forces and
+	// energies.  The GPU forces of a group run as ONE pmgpu_evaluate (one
+	// upload of the positions, one download of the forces; PME beside the
+	// pair kernels): the first round of calls evaluates each force alone and
+	// records the order in which the group's GPU forces come; from the next
+	// round on, the first of them evaluates the whole group and the others
+	// find their share done.  A group that changes its GPU forces between
+	// rounds is an error (PMGPU_COALESCE=0 evaluates every force alone).
+	struct GroupRun
+	{
+		std::vector<GpuNonbondedForce*> seq;
+		bool learned = false;
+		size_t next = 0;
+	};
+
+	// never destroyed: the factory's exemplars are deleted at exit, after
+	// function-local statics constructed later than the factory
+	static std::map<std::pair<const void*, const void*>, GroupRun>& group_runs()
+	{
+		static std::map<std::pair<const void*, const void*>, GroupRun>* m =
+			new std::map<std::pair<const void*, const void*>, GroupRun>();
+		return *m;
+	}
+
+	static long long g_evaluations = 0;
+	long long GpuNonbondedForce::evaluations() { return g_evaluations; }
+
+	static bool coalescing()
+	{
+		const char* c = getenv("PMGPU_COALESCE");
+		return !(c && strcmp(c, "0") == 0);
 	}
 
 	GpuNonbondedForce::GpuNonbondedForce(SystemForce* reference, int kind, int n_terms, const int* pot,
@@ -134,6 +206,12 @@ namespace ProtoMol
 	{
 		if (myForce && mySystem) pmgpu_force_destroy(myForce);
 		delete myReference;
+		// a group with this force is learned again
+		for (auto it = group_runs().begin(); it != group_runs().end();)
+			if (std::find(it->second.seq.begin(), it->second.seq.end(), this) != it->second.seq.end())
+				it = group_runs().erase(it);
+			else
+				++it;
 	}
 
 	int GpuNonbondedForce::defaultPrecision()
@@ -150,7 +228,9 @@ namespace ProtoMol
 	void GpuNonbondedForce::uncache()
 	{
 		myReference->uncache();
-		for (auto& kv : contexts()) kv.second.dirty = true;
+		// the box is compared at every evaluation; the topology is compared
+		// with its digest at the next one
+		for (auto& kv : contexts()) kv.second.recheck = true;
 	}
 
 	Force* GpuNonbondedForce::doMake(std::string& errMsg, std::vector<Value> values) const
@@ -229,10 +309,39 @@ namespace ProtoMol
 		if (energies->molecularVirial())
 			report << error << "[GpuNonbondedForce] the molecular virial is not computed on the GPU" << endr;
 		if (positions->size() == 0) return;
+		std::vector<pmgpu_force*> run(1, myForce);
+		if (coalescing()) {
+			GroupRun& g = group_runs()[std::make_pair((const void*)forces, (const void*)energies)];
+			if (!g.learned) {
+				if (!g.seq.empty() && g.seq[0] == this) {
+					g.learned = true;                // the group's order repeats: learned
+					g.next = 0;
+				} else {
+					if (std::find(g.seq.begin(), g.seq.end(), this) != g.seq.end())
+						report << error << "[GpuNonbondedForce] a GPU force evaluated twice in one force group" << endr;
+					g.seq.push_back(this);           // still learning: this force alone
+				}
+			}
+			if (g.learned) {
+				if (g.seq[g.next] != this)
+					report << error << "[GpuNonbondedForce] the GPU forces of a force group changed between steps "
+					       << "(set PMGPU_COALESCE=0 to evaluate each force alone)" << endr;
+				const bool first = g.next == 0;
+				g.next = (g.next + 1) % g.seq.size();
+				if (!first) return;                  // included in the group's evaluation
+				run.clear();
+				for (GpuNonbondedForce* f : g.seq) {
+					f->ensureForce(topo);
+					run.push_back(f->myForce);
+				}
+			}
+		}
 		pmgpu_energies e;
 		memset(&e, 0, sizeof(e));
 		unsigned flags = energies->virial() ? PMGPU_FLAG_VIRIAL : 0u;
-		int r = pmgpu_evaluate(mySystem, 1, &myForce, &((*positions)[0].x), &((*forces)[0].x), &e, flags);
+		int r = pmgpu_evaluate(mySystem, (int)run.size(), run.data(), &((*positions)[0].x), &((*forces)[0].x), &e,
+		                       flags);
+		++g_evaluations;
 		if (r != PMGPU_OK) gpu_fail(mySystem, "evaluate");
 		// ScalarStructure slots (base/ScalarStructure.h:25-54)
 		(*energies)[ScalarStructure::LENNARDJONES] += e.lennard_jones;

@@ -60,6 +60,13 @@ namespace ProtoMol
 		// (PMGPU_PRECISION_MIXED unless PMGPU_PRECISION=fp64 is set)
 		static int defaultPrecision();
 
+		// the wrapped reference force (its id, parameters and validation)
+		const SystemForce* reference() const { return myReference; }
+
+		// pmgpu_evaluate calls made by the GPU forces of this process (one
+		// per force group and step once the group is learned)
+		static long long evaluations();
+
 	private:
 		virtual Force* doMake(std::string& errMsg, std::vector<Value> values) const;
 		bool ensureForce(const GenericTopology* topo);

@@ -343,6 +343,31 @@ struct CorrArgs {
     double const_virial;         // charged-system term on the virial diagonal
 };
 int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches, int* blocks_used);
+
+// realTerm with lattice images (boxes with an edge <= 2 rc): every unordered
+// pair and every atom with itself, over the lattice vectors of
+// PeriodicBoundaryConditions::buildLatticeVectors, in FP64
+struct RealLatArgs {
+    int n;
+    const double* pos;
+    const double* q;
+    const int* mol;
+    const uint32_t* xfull;
+    const uint32_t* xmod;
+    const int* xrow;
+    const int2* xent;
+    Pbc pbc;
+    const double4* lattice;      // (0, 0, 0) first, then sorted by norm
+    int n_lattice;
+    double rc2, alpha, two_alpha_pi, csf;
+    unsigned long long* facc;    // atom order
+    double scale;
+    double* erec;
+    int erec_stride;
+    int* status;
+    int virial;
+};
+int launch_pme_real_lattice(const RealLatArgs& a, cudaStream_t s, long long* launches, int* blocks_used);
 int launch_pme_correction_adjoint(const CorrArgs& a, double* dq, cudaStream_t s, long long* launches);
 
 // ---------------------------------------------------------------- finalize

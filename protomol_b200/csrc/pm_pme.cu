@@ -884,6 +884,91 @@ int launch_pme_correction(const CorrArgs& a, cudaStream_t s, long long* launches
     return (int)cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ real space with images
+// realTerm (forces/NonbondedPMEwaldSystemForce.h:658-768) for boxes with an
+// edge <= 2 rc, where the lattice (buildLatticeVectors,
+// topology/PeriodicBoundaryConditions.cpp:80-111) holds images besides
+// (0, 0, 0): for every unordered pair i < j and every atom with itself
+// (whose (0, 0, 0) image is excluded), the minimal difference plus each
+// lattice vector, inside the cutoff (Cutoff switching: no modification).  A
+// FULL exclusion removes the first image only and a MODIFIED one scales the
+// first image only, as the reference's loop resets the class after it.  One
+// warp per atom i, lanes over j >= i; FP64 in the reference's operation
+// order, forces in fixed point.
+__global__ void __launch_bounds__(256) k_pme_real_lattice(RealLatArgs a)
+{
+    double acc[kERec];
+#pragma unroll
+    for (int k = 0; k < kERec; ++k) acc[k] = 0.0;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    const double E1 = 0.254829592, E2 = -0.284496736, E3 = 1.421413741, E4 = -1.453152027, E5 = 1.061405429,
+                 PP = 0.3275911;
+    for (int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < a.n; i += warps) {
+        const double xi = a.pos[3 * (size_t)i], yi = a.pos[3 * (size_t)i + 1], zi = a.pos[3 * (size_t)i + 2];
+        const double qi = a.q[i];
+        const int mi = a.mol[i];
+        double fix = 0.0, fiy = 0.0, fiz = 0.0;
+        for (int j = i + lane; j < a.n; j += 32) {
+            double mx, my, mz;
+            pbc_min_diff(a.pbc, xi, yi, zi, a.pos[3 * (size_t)j], a.pos[3 * (size_t)j + 1], a.pos[3 * (size_t)j + 2],
+                         mx, my, mz);
+            int excl = a.mol[j] == mi ? excl_lookup(a.xfull, a.xmod, a.xrow, a.xent, i, j) : PMGPU_EXCL_NONE;
+            if (i == j) excl = PMGPU_EXCL_FULL;
+            const double qj = a.q[j];
+            double fjx = 0.0, fjy = 0.0, fjz = 0.0;
+            for (int k = 0; k < a.n_lattice; ++k) {
+                if (excl == PMGPU_EXCL_FULL) { excl = PMGPU_EXCL_NONE; continue; }
+                const double4 L = a.lattice[k];
+                const double rx = dadd(mx, L.x), ry = dadd(my, L.y), rz = dadd(mz, L.z);
+                const double r2 = dnorm2(rx, ry, rz);
+                if (r2 > a.rc2) continue;
+                const double r = sqrt(r2);
+                double qq = qi * qj;
+                if (excl == PMGPU_EXCL_MODIFIED) qq *= a.csf;
+                const double rr = 1.0 / r;
+                const double ar = a.alpha * r;
+                const double e = qq * exp(-ar * ar);
+                const double t = 1.0 / (1.0 + PP * ar);
+                const double energy = t * (E1 + t * (E2 + t * (E3 + t * (E4 + t * E5)))) * e * rr;
+                const double force = (energy + a.two_alpha_pi * e) * rr * rr;
+                acc[1] += energy;
+                const double fx = rx * force, fy = ry * force, fz = rz * force;
+                fix -= fx; fiy -= fy; fiz -= fz;
+                fjx += fx; fjy += fy; fjz += fz;
+                if (a.virial) {
+                    const double xy = fx * ry, xz = fx * rz, yz = fy * rz;
+                    acc[2] += fx * rx; acc[3] += xy; acc[4] += xz;
+                    acc[5] += xy; acc[6] += fy * ry; acc[7] += yz;
+                    acc[8] += xz; acc[9] += yz; acc[10] += fz * rz;
+                }
+                excl = PMGPU_EXCL_NONE;
+            }
+            if (fjx != 0.0 || fjy != 0.0 || fjz != 0.0)
+                fixed_add3(a.facc + 3 * (size_t)j, fjx, fjy, fjz, a.scale, a.status);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            fix += __shfl_xor_sync(FULL, fix, o);
+            fiy += __shfl_xor_sync(FULL, fiy, o);
+            fiz += __shfl_xor_sync(FULL, fiz, o);
+        }
+        if (lane == 0) fixed_add3(a.facc + 3 * (size_t)i, fix, fiy, fiz, a.scale, a.status);
+    }
+    block_reduce_store<8>(acc, a.erec, a.erec_stride, blockIdx.x);
+}
+
+int launch_pme_real_lattice(const RealLatArgs& a, cudaStream_t s, long long* launches, int* blocks_used)
+{
+    int blocks = (a.n + 7) / 8;                  // one warp per atom, 8 warps per block
+    if (blocks < 1) blocks = 1;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_pme_real_lattice<<<blocks, 256, 0, s>>>(a);
+    *launches += 1;
+    *blocks_used = blocks;
+    return (int)cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ finalize
 __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
 {

@@ -238,9 +238,22 @@ struct pmgpu_force {
     double self_energy = 0.0, charged_energy = 0.0;
     int twx = 0, twy = 0, twz = 0;
     // -real: the real-space term as an internal CoulombEwaldReal / Cutoff
-    // pair force (owned by this force, evaluated before it)
+    // pair force (owned by this force, evaluated before it) when every box
+    // edge exceeds 2 Rc; otherwise realTerm's lattice images (k_pme_real_lattice)
     pmgpu_force* real_sub = nullptr;
+    double4* d_lattice = nullptr;
+    int n_lattice = 0;
 };
+
+// PMEwald -real in a box with an edge <= 2 Rc: buildLatticeVectors gives
+// images besides (0, 0, 0), so realTerm is the lattice kernel, not the pair force
+static bool pme_needs_lattice(const pmgpu_force* f)
+{
+    if (f->kind != 1 || !f->pp.real || !f->sys->box_set) return false;
+    const double* b = f->sys->box;
+    const double rc2 = 2.0 * f->pp.cutoff;
+    return !(std::fabs(b[0]) > rc2 && std::fabs(b[4]) > rc2 && std::fabs(b[8]) > rc2);
+}
 
 // ------------------------------------------------------------------ helpers
 static int fail(pmgpu_system* s, int code, const std::string& msg)
@@ -1209,11 +1222,31 @@ static int prepare_pme(pmgpu_force* f)
 {
     pmgpu_system* sys = f->sys;
     if (f->box_version == sys->box_version && f->topo_version == sys->topo_version) return PMGPU_OK;
-    if (f->real_sub && !(std::fabs(sys->box[0]) > 2.0 * f->pp.cutoff && std::fabs(sys->box[4]) > 2.0 * f->pp.cutoff &&
-                         std::fabs(sys->box[8]) > 2.0 * f->pp.cutoff))
-        return fail(sys, PMGPU_ERR_UNSUPPORTED, "PMEwald -real needs every box edge > 2 cutoff on the GPU "
-                                                "(no lattice images)");
     const pmgpu_pme_params& p = f->pp;
+    f->n_lattice = 0;
+    if (pme_needs_lattice(f)) {
+        // PeriodicBoundaryConditions::buildLatticeVectors(Rc)
+        // (topology/PeriodicBoundaryConditions.cpp:80-111): k, l, m up to
+        // floor(Rc / L + 1), |v| <= 2 Rc, sorted by norm, (0, 0, 0) first
+        // (NonbondedPMEwaldSystemForce.h:630-631)
+        const double rc = p.cutoff, lx = sys->box[0], ly = sys->box[4], lz = sys->box[8];
+        const int bk = (int)std::floor(rc / std::fabs(lx) + 1.0), bl = (int)std::floor(rc / std::fabs(ly) + 1.0),
+                  bm = (int)std::floor(rc / std::fabs(lz) + 1.0);
+        std::vector<double4> lat;
+        for (int k = -bk; k <= bk; k++)
+            for (int l = -bl; l <= bl; l++)
+                for (int m = -bm; m <= bm; m++)
+                    if (k != 0 || l != 0 || m != 0) {
+                        const double x = lx * k, y = ly * l, z = lz * m;
+                        const double n2 = x * x + y * y + z * z;
+                        if (std::sqrt(n2) <= 2 * rc) lat.push_back(make_double4(x, y, z, n2));
+                    }
+        std::stable_sort(lat.begin(), lat.end(), [](const double4& a, const double4& b) { return a.w < b.w; });
+        lat.insert(lat.begin(), make_double4(0.0, 0.0, 0.0, 0.0));
+        CK(dalloc(&f->d_lattice, lat.size()), "alloc");
+        CK(cudaMemcpy(f->d_lattice, lat.data(), sizeof(double4) * lat.size(), cudaMemcpyHostToDevice), "copy");
+        f->n_lattice = (int)lat.size();
+    }
     int kx = p.grid[0], ky = p.grid[1], kz = p.grid[2];
     f->kzh = kz / 2 + 1;
     double LX = sys->box[0], LY = sys->box[4], LZ = sys->box[8];
@@ -1305,7 +1338,7 @@ static int prepare_pme(pmgpu_force* f)
 static void free_force(pmgpu_force* f)
 {
     if (f->real_sub) free_force(f->real_sub);
-    dfree(f->d_deltas); dfree(f->d_doff); dfree(f->d_qgrid);
+    dfree(f->d_deltas); dfree(f->d_doff); dfree(f->d_qgrid); dfree(f->d_lattice);
     dfree(f->d_hdeltas); dfree(f->d_hoff); dfree(f->d_hoff_lo); dfree(f->d_hoff64);
     if (f->d_cgrid) cudaFree(f->d_cgrid);
     if (f->d_rgrid) cudaFree(f->d_rgrid);
@@ -1464,7 +1497,7 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
         int r = f->kind == 0 ? prepare_cutoff(f) : (f->kind == 1 ? prepare_pme(f) : PMGPU_OK);
         if (r) return r;
         if (f->kind != 1) need += pair_records(sys, f);
-        else need += pme_xblocks(f) + 148 * 4;
+        else need += pme_xblocks(f) + 2 * 148 * 4;    // FFT energy, correction, lattice real space
     }
     need += (sys->n + 255) / 256;   // finalize: pair virial records
     int r = ensure_erec(sys, need);
@@ -1655,6 +1688,23 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 if (corr_branch) cs = sys->side3;
                 int e = launch_pme_correction(c, cs, &sys->launches, &b);
                 if (e) return cuda_fail(sys, (cudaError_t)e, "PME correction");
+                prof_end(sys, m);
+                used += b;
+            }
+            if (p.real && f->n_lattice > 0) {
+                RealLatArgs la;
+                memset(&la, 0, sizeof(la));
+                la.n = sys->n; la.pos = d_pos; la.q = sys->d_q; la.mol = sys->d_mol;
+                la.xfull = sys->d_xfull; la.xmod = sys->d_xmod; la.xrow = sys->d_xrow; la.xent = sys->d_xent;
+                la.pbc = sys->pbc; la.lattice = f->d_lattice; la.n_lattice = f->n_lattice;
+                la.rc2 = f->pp.cutoff * f->pp.cutoff; la.alpha = f->alpha;
+                la.two_alpha_pi = 2.0 * f->alpha / std::sqrt(kPi); la.csf = sys->csf;
+                la.facc = facc; la.scale = scale; la.erec = sys->d_erec + used; la.erec_stride = sys->erec_cap;
+                la.status = sys->d_status; la.virial = virial;
+                int b = 0;
+                int m = prof_begin(sys, kPhasePair);
+                int e = launch_pme_real_lattice(la, ps, &sys->launches, &b);
+                if (e) return cuda_fail(sys, (cudaError_t)e, "PME real space (lattice images)");
                 prof_end(sys, m);
                 used += b;
             }
@@ -1854,11 +1904,12 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
 static int eval_core(pmgpu_system* sys, int nf_in, pmgpu_force* const* forces_in, const double* d_pos,
                      double* d_fout, double* d_energy, unsigned flags)
 {
-    // a PME force with -real brings its real-space pair force along
+    // a PME force with -real brings its real-space pair force along (boxes
+    // whose edges all exceed 2 Rc; in smaller ones its lattice kernel runs)
     std::vector<pmgpu_force*> all;
     for (int k = 0; k < nf_in; ++k) {
         if (!forces_in || !forces_in[k]) return fail(sys, PMGPU_ERR_ARG, "bad force list");
-        if (forces_in[k]->real_sub) all.push_back(forces_in[k]->real_sub);
+        if (forces_in[k]->real_sub && !pme_needs_lattice(forces_in[k])) all.push_back(forces_in[k]->real_sub);
         all.push_back(forces_in[k]);
     }
     const int nf = (int)all.size();
@@ -1971,6 +2022,8 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
                                long long* count, int* pairs, long long cap)
 {
     if (!sys || !f || !positions || !count || (cap > 0 && !pairs)) return PMGPU_ERR_ARG;
+    if (pme_needs_lattice(f))
+        return fail(sys, PMGPU_ERR_UNSUPPORTED, "pair recording of PMEwald -real with lattice images");
     if (f->kind != 0 && f->real_sub) f = f->real_sub;   // PME -real: its real-space pairs
     if (f->kind != 0) return fail(sys, PMGPU_ERR_UNSUPPORTED, "pair recording is for cutoff forces");
     if (!sys->box_set) return fail(sys, PMGPU_ERR_STATE, "box not set");
@@ -2268,7 +2321,7 @@ extern "C" int pmgpu_batch_add(pmgpu_batch* b, pmgpu_system* sys, int n_forces, 
     m.sys = sys; m.pos = d_positions; m.fout = d_forces_accum; m.energy = d_energies; m.flags = flags;
     for (int k = 0; k < n_forces; ++k) {
         if (!forces[k] || forces[k]->sys != sys) return batch_fail(b, PMGPU_ERR_ARG, "force of another system");
-        if (forces[k]->real_sub) m.forces.push_back(forces[k]->real_sub);
+        if (forces[k]->real_sub && !pme_needs_lattice(forces[k])) m.forces.push_back(forces[k]->real_sub);
         m.forces.push_back(forces[k]);
     }
     cudaSetDevice(b->device);
@@ -2548,6 +2601,8 @@ extern "C" int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const
     std::vector<pmgpu_force*> fl;
     for (int k = 0; k < n_forces; ++k) {
         if (!forces_in[k] || forces_in[k]->sys != sys) return fail(sys, PMGPU_ERR_ARG, "bad force list");
+        if (pme_needs_lattice(forces_in[k]))
+            return fail(sys, PMGPU_ERR_UNSUPPORTED, "the Hessian of PMEwald -real with lattice images is not available");
         if (forces_in[k]->real_sub) fl.push_back(forces_in[k]->real_sub);
         if (forces_in[k]->kind == 1 && (forces_in[k]->pp.reciprocal || forces_in[k]->pp.correction))
             return fail(sys, PMGPU_ERR_UNSUPPORTED, "the Hessian of the PME reciprocal / correction terms is not "
@@ -2675,6 +2730,9 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
     std::vector<pmgpu_force*> fl;
     for (int k = 0; k < n_forces; ++k) {
         if (!forces_in[k] || forces_in[k]->sys != sys) return fail(sys, PMGPU_ERR_ARG, "bad force list");
+        if (pme_needs_lattice(forces_in[k]))
+            return fail(sys, PMGPU_ERR_UNSUPPORTED, "the backward pass of PMEwald -real with lattice images is not "
+                                                    "available");
         if (forces_in[k]->real_sub) fl.push_back(forces_in[k]->real_sub);
         fl.push_back(forces_in[k]);
     }

@@ -86,3 +86,51 @@ def test_table_force_keywords_run_on_the_gpu(definition, precision):
     tol_f, tol_e = (1e-9, 1e-10) if precision == "fp64" else (1e-5, 2e-6)
     assert err <= tol_f
     assert abs(r["lennard_jones"] + r["coulomb"] - ref["lennard_jones"] - ref["coulomb"]) <= tol_e * scale
+
+
+LEAPFROG = os.path.join(ROOT, "protomol_b200", "adapter", "_build", "gpu_leapfrog_driver")
+
+
+def run_leapfrog(system, velocities, defs, steps, mode, precision="mixed"):
+    if not os.path.exists(LEAPFROG):
+        pytest.skip("drop-in driver not built (needs the ProtoMol sources at build time)")
+    env = dict(os.environ, PMGPU_PRECISION=precision)
+    with tempfile.TemporaryDirectory() as td:
+        sp, dp, op = (os.path.join(td, f) for f in ("s.bin", "d.bin", "o.bin"))
+        system.save(sp)
+        np.concatenate([system.mass, velocities.ravel()]).astype(np.float64).tofile(dp)
+        p = subprocess.run([LEAPFROG, sp, dp, op, str(steps), "1.0", mode, *defs], env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert p.returncode == 0, p.stderr
+        raw = np.fromfile(op)
+    n = system.n_atoms
+    calls = [int(line.split()[-1]) for line in p.stderr.splitlines() if line.startswith("gpu evaluations:")]
+    return {"epot": raw[0], "ekin": raw[1], "positions": raw[2:2 + 3 * n].reshape(n, 3),
+            "velocities": raw[2 + 3 * n:].reshape(n, 3), "gpu_calls": calls[0] if calls else None}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_reference_leapfrog_integrator_runs_on_the_gpu_forces(precision):
+    """ProtoMol's own LeapfrogIntegrator and ForceGroup, 20 steps of 1 fs on
+    a 216-particle ionic Lennard-Jones fluid with the split Ewald real-space
+    force and PME (two GPU forces in one group), against the same run on the
+    reference forces the GPU ones wrap.  The group's two GPU forces run as
+    one pmgpu_evaluate per step once the group is learned (first step)."""
+    from protomol_b200 import integrate
+    s = systems.ionic_fluid_216()
+    alpha = systems.ewald_alpha(9.0)
+    defs = [workloads.lj_ewald_split(8, 9, alpha), workloads.pme_reciprocal((20, 20, 20), 9, alpha)]
+    v = integrate.maxwell_boltzmann(s.mass, 300.0, seed=7)
+    steps = 20
+    cpu = run_leapfrog(s, v, defs, steps, "cpu")
+    gpu = run_leapfrog(s, v, defs, steps, "gpu", precision)
+    dx = np.abs(gpu["positions"] - cpu["positions"]).max()
+    dv = np.abs(gpu["velocities"] - cpu["velocities"]).max()
+    print(f"\n{precision}: 20 Leapfrog steps, max |dx| {dx:.2e} A, max |dv| {dv:.2e}, "
+          f"E_pot {gpu['epot']:.6f} / {cpu['epot']:.6f}, GPU calls {gpu['gpu_calls']}")
+    tol = 1e-10 if precision == "fp64" else 1e-6
+    assert dx <= tol
+    assert abs(gpu["epot"] - cpu["epot"]) <= (1e-9 if precision == "fp64" else 1e-6) * abs(cpu["epot"])
+    # initializeForces + 20 steps = 21 group evaluations: the first one learns
+    # the group (one call per force), the other 20 make one call each
+    assert gpu["gpu_calls"] == 2 + steps

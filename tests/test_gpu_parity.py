@@ -254,12 +254,31 @@ def test_empty_and_sparse_systems():
         assert rel_rms(f, ref["forces"]) <= MIXED_FORCE_RTOL
 
 
-def test_pme_real_needs_boxes_without_lattice_images():
-    s = systems.water_box(100, seed=7)           # edge < 2 x 9 A: realTerm would add images
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pme_real_with_lattice_images_against_oracle(precision):
+    """A box under twice the cutoff: realTerm sums the lattice images of every
+    pair (and of every atom with itself) besides the minimal one."""
+    s = systems.water_box(100, seed=7)           # edge < 2 x 9 A
     assert min(s.box[k][k] for k in range(3)) < 18.0
-    with pytest.raises(_lib.PmgpuError) as ei:
-        gpu_eval(s, [PME_FULL.replace("-gridsize 24 24 24", "-gridsize 16 16 16")], "mixed")
-    assert ei.value.code == 5
+    d = PME_FULL.replace("-gridsize 24 24 24", "-gridsize 16 16 16")
+    ref = oracle.evaluate(s, [F.parse_definition(d)])
+    _, _, f, e = gpu_eval(s, [d], precision)
+    rms = np.sqrt((ref["forces"] ** 2).sum(1).mean())
+    if precision == "fp64":
+        assert np.abs(f - ref["forces"]).max() <= FP64_FORCE_RTOL * rms
+        assert abs(e.coulomb - ref["coulomb"]) <= FP64_ENERGY_RTOL * abs(ref["coulomb"])
+        assert np.abs(e.virial_tensor - ref["virial"]).max() <= FP64_ENERGY_RTOL * np.abs(ref["virial"]).max()
+    else:
+        # the lattice real space is FP64 in both precisions; the reciprocal
+        # part is the mixed one
+        assert rel_rms(f, ref["forces"]) <= MIXED_FORCE_RTOL
+        assert abs(e.coulomb - ref["coulomb"]) <= MIXED_METRIC_ENERGY_RTOL * abs(ref["coulomb"])
+    # the real-space term alone, where the images matter most
+    dr = "Coulomb -algorithm PMEwald -real -interpolation BSpline -gridsize 16 16 16 -cutoff 9 -alpha 0.35"
+    ref = oracle.evaluate(s, [F.parse_definition(dr)])
+    _, _, f, e = gpu_eval(s, [dr], precision)
+    assert np.abs(f - ref["forces"]).max() <= FP64_FORCE_RTOL * rms
+    assert abs(e.coulomb - ref["coulomb"]) <= FP64_ENERGY_RTOL * abs(ref["coulomb"])
 
 
 def test_pme_rejects_what_the_reference_rejects(small_chain):
