@@ -624,11 +624,50 @@ def measure_1m(local, torch, steps):
                  "pme_gather": 4 * kx ** 3 + 16 * n + 12 * n}
             out["pme_hbm_gbs"] = {k: v / (ph[k] * 1e-3) / 1e9 for k, v in b.items() if ph.get(k)}
             out["phases_ms"] = ph
+            out["trajectory_100"] = measure_1m_trajectory(lib, topo, fs, dpos, dfor, den, stream, torch, npairs)
         for f in fs:
             f.close()
     out["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
     topo.close()
     return out
+
+
+def measure_1m_trajectory(lib, topo, fs, dpos, dfor, den, stream, torch, npairs, evals=100, every=10, skin=1.0):
+    """The large-system configuration as specified: 100 force evaluations of
+    a moving configuration with the pair list rebuilt every 10 (a 1 A skin,
+    the within-cutoff decision exact at every evaluation).  The positions
+    drift along fixed per-atom directions at up to 0.02 A per evaluation
+    (a synthetic trajectory in HBM, updated between the timed events)."""
+    VP = C.c_void_p
+    arr = (VP * len(fs))(*[f.handle for f in fs])
+    g = torch.Generator(device=dpos.device).manual_seed(100)
+    u = torch.randn(dpos.shape, dtype=torch.float64, device=dpos.device, generator=g)
+    u *= 0.02 * torch.rand((dpos.shape[0], 1), dtype=torch.float64, device=dpos.device, generator=g) / u.norm(dim=1,
+                                                                                                       keepdim=True)
+    base = dpos.clone()
+    topo.set_pair_list(skin, every)
+    builds0 = topo.pair_list_builds()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(evals)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k, (a, b) in enumerate(evs):
+            dpos.copy_(base + k * u)                 # between the timed events
+            a.record(stream)
+            lib.pmgpu_evaluate_device(topo.handle, len(fs), arr, VP(dpos.data_ptr()), VP(dfor.data_ptr()),
+                                      VP(den.data_ptr()), 1)
+            b.record(stream)
+    torch.cuda.synchronize()
+    st = lib.pmgpu_synchronize(topo.handle)
+    ms = [a.elapsed_time(b) for a, b in evs]
+    builds = topo.pair_list_builds() - builds0
+    topo.set_pair_list(0.0, 1)
+    dpos.copy_(base)
+    total = float(np.sum(ms))
+    return {"evaluations": evals, "rebuild_every": every, "skin_A": skin, "lists_built": int(builds),
+            "status": int(st), "ms_total": total, "evals_per_s": evals * 1000.0 / total,
+            "ms_build_evaluation_mean": float(np.mean(ms[::every])),
+            "ms_reuse_evaluation_mean": float(np.mean([m for k, m in enumerate(ms) if k % every])),
+            "pair_interactions_per_s": npairs * evals * 1000.0 / total}
 
 
 def _lib_load():

@@ -384,6 +384,21 @@ int pmgpu_get_cells(pmgpu_system* sys, int* cells, int* dims);
 #define PMGPU_LAYOUT_COLUMNS 2
 int pmgpu_pair_layout(pmgpu_system* sys);
 
+/* No counterpart in the reference, whose cutoff force rebuilds its cell lists
+ * at every evaluation (forces/NonbondedCutoffSystemForce.h:63-74).  A reused
+ * pair list for the column layout: the list is built with the cutoff plus
+ * `skin` (A) and kept for `rebuild_every` evaluations of the same forces, the
+ * positions refreshed each time; the within-cutoff decision stays exact per
+ * evaluation, so the interacting pair set is the reference's as long as no
+ * atom moves more than skin / 2 between rebuilds.  One that does makes the
+ * evaluation report PMGPU_ERR_CAPACITY and the list is rebuilt at the next
+ * (pmgpu_evaluate repeats the evaluation by itself).  Applies to force groups
+ * with one mixed-precision cutoff force on the column layout; rebuild_every =
+ * 1 (the default) rebuilds at every evaluation.  pmgpu_pair_list_builds
+ * counts the lists built so far. */
+int pmgpu_set_pair_list(pmgpu_system* sys, double skin, int rebuild_every);
+long long pmgpu_pair_list_builds(pmgpu_system* sys);
+
 /* Evaluates one cutoff force (or a PME force with -real) in pair-recording
  * mode and returns the within-cutoff pair set: every (min, max) atom index
  * pair the force interacted, in no particular order.  *count receives the

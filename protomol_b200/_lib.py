@@ -26,6 +26,7 @@ EXPORTS = [
     "pmgpu_cutoff_create", "pmgpu_pme_create", "pmgpu_force_destroy", "pmgpu_pme_alpha",
     "pmgpu_evaluate", "pmgpu_evaluate_device", "pmgpu_synchronize", "pmgpu_stream",
     "pmgpu_launch_count", "pmgpu_last_error", "pmgpu_get_cells", "pmgpu_get_pairs", "pmgpu_pair_layout",
+    "pmgpu_set_pair_list", "pmgpu_pair_list_builds",
     "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
     "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
@@ -100,6 +101,9 @@ def load():
     lib.pmgpu_last_error.argtypes = [vp, C.c_char_p, C.c_int]
     lib.pmgpu_get_cells.argtypes = [vp, vp, vp]
     lib.pmgpu_pair_layout.argtypes = [vp]
+    lib.pmgpu_set_pair_list.argtypes = [vp, C.c_double, C.c_int]
+    lib.pmgpu_pair_list_builds.argtypes = [vp]
+    lib.pmgpu_pair_list_builds.restype = C.c_longlong
     lib.pmgpu_get_pairs.argtypes = [vp, vp, vp, C.POINTER(C.c_longlong), vp, C.c_longlong]
     lib.pmgpu_set_profiling.argtypes = [vp, C.c_int]
     lib.pmgpu_phase_times.argtypes = [vp, vp, C.c_int, C.POINTER(C.c_longlong)]

@@ -381,7 +381,39 @@ __global__ void __launch_bounds__(kColThreads) k_col_sort(ColBinArgs a)
     }
 }
 
+__global__ void __launch_bounds__(kBinThreads) k_col_refresh(ColBinArgs a, double half_skin2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const ColGrid& g = a.g;
+    const double x = a.pos[3 * i], y = a.pos[3 * i + 1], z = a.pos[3 * i + 2];
+    int cx, cy, cz;
+    double vx, vy, vz;
+    bin_cell_of(a.pbc, a.grid, x, y, z, cx, cy, cz, vx, vy, vz);
+    a.cell3[3 * i] = cx;
+    a.cell3[3 * i + 1] = cy;
+    a.cell3[3 * i + 2] = cz;
+    const unsigned qx = fix32((x - g.mnx) / g.lx), qy = fix32((y - g.mny) / g.ly), qz = fix32((z - g.mnz) / g.lz);
+    // the displacement since the build, from the build-time fixed point
+    const double ux = (double)(int)(qx - a.qfix[3 * i]) * (g.lx * (1.0 / 4294967296.0));
+    const double uy = (double)(int)(qy - a.qfix[3 * i + 1]) * (g.ly * (1.0 / 4294967296.0));
+    const double uz = (double)(int)(qz - a.qfix[3 * i + 2]) * (g.lz * (1.0 / 4294967296.0));
+    if (ux * ux + uy * uy + uz * uz > half_skin2) atomicOr(a.status, kStatusListStale);
+    const int sl = a.slot_of[i];
+    const int4 old = a.cq[sl];
+    a.cq[sl] = make_int4((int)qx, (int)qy, (int)qz, old.w);
+}
+
 }  // namespace
+
+int launch_col_refresh(const ColBinArgs& a, double half_skin, cudaStream_t s, long long* launches)
+{
+    if (a.n <= 0) return 0;
+    const int nb = (a.n + kBinThreads - 1) / kBinThreads;
+    k_col_refresh<<<nb, kBinThreads, 0, s>>>(a, half_skin * half_skin);
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
 
 int launch_col_bin(const ColBinArgs& a, cudaStream_t s, long long* launches)
 {

@@ -30,6 +30,7 @@ constexpr int kStatusOverflow = 1;
 constexpr int kStatusOutOfGrid = 2;
 constexpr int kStatusListFull = 4;     // cluster-pair list or chunk capacity exceeded
 constexpr int kStatusColumns = 8;      // a column or cluster the column path cannot take (use the cell path)
+constexpr int kStatusListStale = 16;   // an atom moved more than half the pair list's skin since it was built
 
 // FP64 constants of PeriodicBoundaryConditions::set
 // (topology/PeriodicBoundaryConditions.cpp:40-77), orthogonal box.

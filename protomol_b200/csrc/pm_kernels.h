@@ -88,6 +88,10 @@ struct ColBinArgs {
 };
 // K1c: fixed point, columns, z order, clusters and their boxes
 int launch_col_bin(const ColBinArgs& a, cudaStream_t s, long long* launches);
+// K1r: between rebuilds of a reused pair list, the current fixed-point
+// positions into the slots (and the reference cells); an atom farther than
+// half the skin from where the list was built sets kStatusListStale
+int launch_col_refresh(const ColBinArgs& a, double half_skin, cudaStream_t s, long long* launches);
 
 // ---------------------------------------------------------------- pair force
 // FP32 constants of one term; the *_lo members are the FP32 remainders of
@@ -215,6 +219,7 @@ struct PairArgs {
     ColGrid cg;
     const double* qorig;         // charges, types in atom order (FP64 near-pair energies)
     const int* torig;
+    float list_skin;             // the column list includes pairs up to the cutoff plus this (reused lists)
 };
 
 // Combination id of the registered OneAtomPair[Two] templates.

@@ -191,17 +191,24 @@ __global__ void __launch_bounds__(128) k_col_list(PairArgs p)
     __shared__ int s_pre[4][33];
     const int ic = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     if (ic >= p.icl_cap) return;                                 // warp-uniform
-    if (*p.status & kStatusColumns) return;
+    // a refused system leaves a mark in the list's need count, which a
+    // reused list keeps (the status word starts at zero every evaluation)
+    if (*p.status & kStatusColumns) {
+        if (ic == 0 && lane == 0) atomicMax(p.plist_need, 1);
+        return;
+    }
     const ColGrid& g = p.cg;
     if (ic >= p.ccstart[g.ncol]) return;
     const int col_i = p.ccol[ic];
     const float4 ilo = p.ibox[2 * ic], ihi = p.ibox[2 * ic + 1];
     if (ihi.z - ilo.z > g.zext) {                                // a tile's image could be ambiguous
-        if (lane == 0) atomicOr(p.status, kStatusColumns);
+        if (lane == 0) { atomicOr(p.status, kStatusColumns); atomicMax(p.plist_need, 1); }
         return;
     }
     const int4 Oi = p.corg[ic];
-    const float lim = p.cut2f * (1.0f + 8.0f * p.guard) + 1e-3f;
+    // a reused list holds the pairs within the cutoff plus the skin
+    const float rl = sqrtf(p.cut2f) + p.list_skin;
+    const float lim = rl * rl * (1.0f + 8.0f * p.guard) + 1e-3f;
     const int ne = col_gather(p, ic, col_i, ilo, ihi, Oi, lim, s_ent[w], kColStageEntries, s_part[w], s_pre[w]);
     if (ne == 0) return;
     const int nch = (ne + p.chunk - 1) / p.chunk;
@@ -299,7 +306,7 @@ __device__ __forceinline__ JAtom col_atom(const int4& P, const int4& M)
 // for 6 values), the fixed-point adds, the virial offsets, the energy sums --
 // is shared by the two.
 template <int NT, int P0, int S0, int P1, int S1>
-__global__ void __launch_bounds__(128, 4) k_pair_col(PairArgs p)
+__global__ void __launch_bounds__(128, 5) k_pair_col(PairArgs p)
 {
     pdl_wait();
     const unsigned FULL = 0xffffffffu;
@@ -312,7 +319,11 @@ __global__ void __launch_bounds__(128, 4) k_pair_col(PairArgs p)
     // virial W[0..2][comp] of the lanes that hold a j-force component
     long long acc[5] = {0, 0, 0, 0, 0};
     bool bad = false;
-    const int nchunks = (*p.status & (kStatusListFull | kStatusColumns)) ? 0 : min(*p.chunk_count, p.chunk_cap);
+    // an incomplete list (capacity exceeded or the system refused, also when
+    // it was built by an earlier evaluation and is reused) runs no pair
+    const bool list_bad = (*p.status & (kStatusListFull | kStatusColumns)) || *p.plist_need != 0 || *p.chunk_need != 0;
+    if (list_bad && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(p.status, kStatusListFull);
+    const int nchunks = list_bad ? 0 : min(*p.chunk_count, p.chunk_cap);
     // after the reduce-scatter lane il (< 6) holds component il % 3 of the
     // j-force of tile A's (il < 3) or tile B's (il >= 3) j-atom jj
     const bool holds = il < 6, onB = il >= 3;

@@ -47,10 +47,12 @@ struct GraphKey {
     const void* energy = nullptr;
     unsigned flags = 0;
     int box_version = -1, topo_version = -1, buf_version = -1;
+    int reuse = 0;                     // the evaluation keeps the pair list of an earlier one
     bool operator==(const GraphKey& o) const
     {
         return ids == o.ids && pos == o.pos && fout == o.fout && energy == o.energy && flags == o.flags &&
-               box_version == o.box_version && topo_version == o.topo_version && buf_version == o.buf_version;
+               box_version == o.box_version && topo_version == o.topo_version && buf_version == o.buf_version &&
+               reuse == o.reuse;
     }
 };
 
@@ -153,6 +155,17 @@ struct pmgpu_system {
     bool col_disabled = false;
     bool col_just_disabled = false;
     bool eval_use_col = false;         // the evaluation being enqueued uses the column path
+    // reused pair lists (pmgpu_set_pair_list): the column list built with the
+    // cutoff plus a skin is kept for rebuild_every evaluations while no atom
+    // moves more than half the skin
+    double list_skin = 0.0;
+    int list_every = 1;
+    bool list_valid = false;
+    bool list_just_invalidated = false;
+    int evals_since_build = 0;
+    std::vector<long long> list_ids;   // the forces the list was built for
+    long long list_builds = 0;
+    bool eval_reuse = false;           // the evaluation being enqueued reuses the list
     int last_layout = 0;               // pmgpu_pair_layout of the last evaluation with mixed cutoff forces
     ColGrid eval_cg;                   // its grid with the reach of its cutoffs
     unsigned* d_qfix = nullptr;
@@ -456,7 +469,14 @@ extern "C" int pmgpu_synchronize(pmgpu_system* sys)
             sys->col_just_disabled = true;
             sys->buf_version++;
         }
+        sys->list_valid = false;
         return fail(sys, PMGPU_ERR_CAPACITY, "column clusters out of range (the cell-cluster path is used next)");
+    }
+    if (st & kStatusListStale) {
+        sys->list_valid = false;
+        sys->list_just_invalidated = true;
+        return fail(sys, PMGPU_ERR_CAPACITY, "an atom moved more than half the pair list's skin since the list was "
+                                             "built (it is rebuilt at the next evaluation)");
     }
     if (st & kStatusListFull) {
         // list need, chunk count, chunk need, work counter, near count, near need
@@ -465,6 +485,7 @@ extern "C" int pmgpu_synchronize(pmgpu_system* sys)
         sys->plist_need = std::max<long long>(sys->plist_need, need[0]);
         sys->chunk_need = std::max<long long>(sys->chunk_need, need[2]);
         sys->near_need = std::max<long long>(sys->near_need, need[5]);
+        sys->list_valid = false;
         return fail(sys, PMGPU_ERR_CAPACITY, "cluster-pair list capacity exceeded (grown for the next evaluation)");
     }
     return PMGPU_OK;
@@ -576,6 +597,7 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     CK(cudaMemset(sys->d_cslot, 0, sizeof(int) * (size_t)std::max(n, 1)), "memset");
     sys->col_ncl_cap = 0;   // slot arrays depend on N and the column grid: sized at evaluation
     sys->col_grid_stale = true;
+    sys->list_valid = false;
     sys->cbox_cap = 0;   // cluster boxes depend on N and the cell grid: sized at evaluation
     sys->h_fbuf.assign(3 * (size_t)n, 0.0);
     return PMGPU_OK;
@@ -696,6 +718,7 @@ extern "C" int pmgpu_set_box(pmgpu_system* sys, const double* e1, const double* 
     // the binning leaves the counts at zero; they start there
     CK(cudaMemsetAsync(sys->d_counts, 0, sizeof(int) * (size_t)g.ncell, sys->stream), "memset");
     sys->col_grid_stale = true;
+    sys->list_valid = false;
     sys->box_set = true;
     sys->box_version++;
     sys->binned = false;
@@ -1407,6 +1430,19 @@ static int col_bin(pmgpu_system* sys, const double* d_pos)
     return PMGPU_OK;
 }
 
+// between rebuilds of a reused list: the current positions into the slots
+static int col_refresh(pmgpu_system* sys, const double* d_pos)
+{
+    ColBinArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = sys->n; a.pos = d_pos; a.pbc = sys->pbc; a.grid = sys->grid; a.cell3 = sys->d_cell3;
+    a.g = sys->eval_cg; a.qfix = sys->d_qfix; a.cq = sys->d_cq; a.slot_of = sys->d_cslot; a.status = sys->d_status;
+    int e = launch_col_refresh(a, 0.5 * sys->list_skin, sys->stream, &sys->launches);
+    if (e) return cuda_fail(sys, (cudaError_t)e, "pair list refresh");
+    sys->binned = true;
+    return PMGPU_OK;
+}
+
 // the column-path members of the pair arguments
 static void fill_col_args(pmgpu_system* sys, PairArgs& a)
 {
@@ -1416,6 +1452,7 @@ static void fill_col_args(pmgpu_system* sys, PairArgs& a)
     a.cg = sys->eval_cg;
     a.qorig = sys->d_q; a.torig = sys->d_type;
     a.facc = sys->d_facc32c;
+    a.list_skin = sys->list_every > 1 ? (float)sys->list_skin : 0.0f;
 }
 
 static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_pos, PairArgs& a)
@@ -1530,7 +1567,7 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
                 sys->col_grid_stale = false;
             }
             ColGrid g;
-            if (col_reach(sys, std::sqrt(rc2), g)) {
+            if (col_reach(sys, std::sqrt(rc2) + sys->list_skin, g)) {
                 sys->eval_use_col = true;
                 sys->eval_cg = g;
             }
@@ -1552,7 +1589,7 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
         double rc2 = 0.0;
         for (int k = 0; k < nf; ++k)
             if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) rc2 = std::max(rc2, forces[k]->cut2);
-        const long long entries = col_list_estimate(sys->n, g, g.lx * g.ly * g.lz, std::sqrt(rc2));
+        const long long entries = col_list_estimate(sys->n, g, g.lx * g.ly * g.lz, std::sqrt(rc2) + sys->list_skin);
         lneed = 2 * entries;                  // int4 entries in the int2 list buffer
         cneed = col_chunk_estimate(entries, sys->n, g, sys->tuning.chunk_entries);
     } else {
@@ -1631,7 +1668,14 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     cudaStream_t s = sys->stream;
     size_t n3 = 3 * (size_t)sys->n;
     int mbin = prof_begin(sys, kPhaseBin);
-    CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
+    if (sys->eval_reuse) {
+        // the list's counts (ints 1-4) stay; the status, the work counter,
+        // the near-pair counts, the binning counters and the sums start at zero
+        CK(cudaMemsetAsync(sys->d_small, 0, sizeof(int), s), "memset");
+        CK(cudaMemsetAsync((char*)sys->d_small + 5 * sizeof(int), 0, kSmallBytes - 5 * sizeof(int), s), "memset");
+    } else {
+        CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
+    }
     if (use32) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
     bool any_cut = false, any_pme = false, any_full = false;
@@ -1780,7 +1824,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         if (r) return r;
     }
     if (use_col) {
-        r = col_bin(sys, d_pos);
+        r = sys->eval_reuse ? col_refresh(sys, d_pos) : col_bin(sys, d_pos);
         if (r) return r;
     }
     prof_end(sys, mbin);
@@ -1820,7 +1864,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         if (col) fill_col_args(sys, a);
         a.virial = virial;
         a.erec = sys->d_erec + used;
-        if (!fp64) {
+        if (!fp64 && !(col && sys->eval_reuse)) {
             // list count and need, chunk count and need, work counter
             if (lists++ > 0) CK(cudaMemsetAsync(sys->d_plist_count, 0, 6 * sizeof(int), s), "memset");
             int ml = prof_begin(sys, kPhaseList);
@@ -1916,9 +1960,36 @@ static int eval_core(pmgpu_system* sys, int nf_in, pmgpu_force* const* forces_in
     pmgpu_force* const* forces = all.data();
     int r = eval_prepare(sys, nf, forces);
     if (r) return r;
-    if (sys->profiling || !sys->use_graphs) return eval_enqueue(sys, nf, forces, d_pos, d_fout, d_energy, flags);
+    // a reused pair list: the column path with one mixed cutoff force (its
+    // list is the system's only one), a rebuild period above one, a list
+    // built for these forces, still valid and younger than the period
+    std::vector<long long> ids;
+    int n_mixed_cut = 0;
+    for (int k = 0; k < nf; ++k) {
+        ids.push_back(forces[k]->id);
+        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) ++n_mixed_cut;
+    }
+    const bool can_reuse = sys->eval_use_col && sys->list_every > 1 && n_mixed_cut == 1;
+    sys->eval_reuse = can_reuse && sys->list_valid && sys->list_ids == ids && sys->evals_since_build < sys->list_every;
+    auto note_list = [&]() {
+        if (!sys->eval_use_col || n_mixed_cut == 0) return;
+        if (sys->eval_reuse) {
+            sys->evals_since_build++;
+        } else {
+            sys->list_builds++;
+            sys->list_valid = can_reuse;
+            sys->list_ids = ids;
+            sys->evals_since_build = 1;
+        }
+    };
+    if (sys->profiling || !sys->use_graphs) {
+        r = eval_enqueue(sys, nf, forces, d_pos, d_fout, d_energy, flags);
+        if (!r) note_list();
+        return r;
+    }
     GraphKey key;
-    for (int k = 0; k < nf; ++k) key.ids.push_back(forces[k]->id);
+    key.ids = ids;
+    key.reuse = sys->eval_reuse ? 1 : 0;
     key.pos = d_pos; key.fout = d_fout; key.energy = d_energy; key.flags = flags;
     key.box_version = sys->box_version; key.topo_version = sys->topo_version; key.buf_version = sys->buf_version;
     cudaStream_t s = sys->stream;
@@ -1956,6 +2027,7 @@ static int eval_core(pmgpu_system* sys, int nf_in, pmgpu_force* const* forces_in
     hit->last_use = ++sys->graph_clock;
     CK(cudaGraphLaunch(hit->exec, s), "graph launch");
     sys->launches += hit->launches;
+    note_list();
     return PMGPU_OK;
 }
 
@@ -1990,9 +2062,11 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
         CK(cudaMemcpyAsync(sys->h_fbuf.data(), sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
         CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kERec, cudaMemcpyDeviceToHost, s), "D2H energies");
         sys->col_just_disabled = false;
+        sys->list_just_invalidated = false;
         r = pmgpu_synchronize(sys);
         if (!(r == PMGPU_ERR_CAPACITY && (sys->plist_need > sys->plist_cap || sys->chunk_need > sys->chunk_cap ||
-                                          sys->near_need > sys->near_cap || sys->col_just_disabled)))
+                                          sys->near_need > sys->near_cap || sys->col_just_disabled ||
+                                          sys->list_just_invalidated)))
             break;
     }
     if (r) return r;
@@ -2006,6 +2080,19 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
 
 // ------------------------------------------------------------------ diagnostics
 extern "C" int pmgpu_pair_layout(pmgpu_system* sys) { return sys ? sys->last_layout : 0; }
+
+extern "C" int pmgpu_set_pair_list(pmgpu_system* sys, double skin, int rebuild_every)
+{
+    if (!sys) return PMGPU_ERR_ARG;
+    if (!(skin >= 0.0 && skin <= 10.0) || rebuild_every < 1) return fail(sys, PMGPU_ERR_ARG, "skin 0..10 A, period >= 1");
+    sys->list_skin = rebuild_every > 1 ? skin : 0.0;
+    sys->list_every = rebuild_every;
+    sys->list_valid = false;
+    sys->buf_version++;                // graphs captured for another list
+    return PMGPU_OK;
+}
+
+extern "C" long long pmgpu_pair_list_builds(pmgpu_system* sys) { return sys ? sys->list_builds : 0; }
 
 extern "C" int pmgpu_get_cells(pmgpu_system* sys, int* cells, int* dims)
 {

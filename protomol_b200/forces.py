@@ -120,6 +120,14 @@ class Topology:
                                  _lib.FLAG_VIRIAL if virial else 0, int(evals), C.byref(t)), self.handle)
         return t.as_dict()
 
+    def set_pair_list(self, skin: float, rebuild_every: int):
+        """pmgpu_set_pair_list: keep the column layout's pair list, built with
+        the cutoff plus ``skin`` A, for ``rebuild_every`` evaluations."""
+        check(_lib.load().pmgpu_set_pair_list(self.handle, float(skin), int(rebuild_every)), self.handle)
+
+    def pair_list_builds(self) -> int:
+        return int(_lib.load().pmgpu_pair_list_builds(self.handle))
+
     def pair_layout(self) -> str:
         """Cluster layout of the last evaluation's mixed cutoff forces:
         'columns' (fixed-point coordinates in z-sorted columns), 'cells'

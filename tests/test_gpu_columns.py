@@ -178,3 +178,59 @@ def test_reference_cells_reported_by_the_column_binning(chain14281):
     cells, dims = topo.cells()
     ocells, odims, _ = oracle.cell_assign(chain14281, chain14281.positions)
     assert dims == odims and np.array_equal(cells, ocells)
+
+
+def _moving(s, steps, seed=21, speed=0.01):
+    """Positions of a synthetic trajectory: every atom moving along its own
+    direction at ``speed`` A per step (a thermal-like drift, no dynamics)."""
+    rng = np.random.default_rng(seed)
+    u = rng.normal(size=s.positions.shape)
+    u *= speed / np.linalg.norm(u, axis=1, keepdims=True) * rng.uniform(0.2, 1.0, size=(s.n_atoms, 1))
+    return [s.positions + k * u for k in range(steps)]
+
+
+def test_reused_pair_list_follows_a_moving_system(medium):
+    """A pair list with a 1 A skin rebuilt every 10 evaluations, over 25
+    evaluations of moving atoms: every evaluation equals a fresh one (list
+    rebuilt) up to the FP32 summation order, three lists are built, and the
+    last one agrees with the oracle."""
+    d = PAIRINGS["lj_c2_ewald"]
+    traj = _moving(medium, 25)
+    topo = F.Topology(medium)
+    fs = [F.ForceFactory.make(topo, d, "mixed")]
+    topo.set_pair_list(1.0, 10)
+    fresh = F.Topology(medium)
+    ff = [F.ForceFactory.make(fresh, d, "mixed")]
+    for k, pos in enumerate(traj):
+        out = np.zeros((medium.n_atoms, 3)); e = F.ScalarStructure()
+        F.evaluate_group(topo, fs, pos, out, e)
+        ref = np.zeros((medium.n_atoms, 3)); er = F.ScalarStructure()
+        F.evaluate_group(fresh, ff, pos, ref, er)
+        assert _rel_rms(out, ref) <= 1e-6, k
+        assert abs((e.lennard_jones + e.coulomb) - (er.lennard_jones + er.coulomb)) <= 1e-9 * (
+            abs(er.lennard_jones) + abs(er.coulomb)), k
+    assert topo.pair_layout() == "columns"
+    assert topo.pair_list_builds() == 3
+    o = oracle.evaluate(medium, [F.parse_definition(d)], positions=traj[-1])
+    assert _rel_rms(out, o["forces"]) <= FORCE_RTOL
+    scale = abs(o["lennard_jones"]) + abs(o["coulomb"])
+    assert abs((e.lennard_jones + e.coulomb) - (o["lennard_jones"] + o["coulomb"])) <= ENERGY_RTOL * scale
+
+
+def test_a_list_older_than_its_skin_is_rebuilt(medium):
+    """One atom jumps 0.8 A (more than half the 1 A skin) between two
+    evaluations of a reused list: the evaluation notices, rebuilds and
+    repeats itself, and its result is the fresh one."""
+    d = PAIRINGS["lj_c2_ewald"]
+    topo = F.Topology(medium)
+    fs = [F.ForceFactory.make(topo, d, "mixed")]
+    topo.set_pair_list(1.0, 10)
+    out = np.zeros((medium.n_atoms, 3))
+    F.evaluate_group(topo, fs, medium.positions, out, F.ScalarStructure())
+    pos = medium.positions.copy()
+    pos[500] += np.array([0.8, 0.0, 0.0])
+    out = np.zeros((medium.n_atoms, 3)); e = F.ScalarStructure()
+    F.evaluate_group(topo, fs, pos, out, e)
+    assert topo.pair_list_builds() == 2
+    o = oracle.evaluate(medium, [F.parse_definition(d)], positions=pos)
+    assert _rel_rms(out, o["forces"]) <= FORCE_RTOL
