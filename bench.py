@@ -636,14 +636,19 @@ def measure_1m_trajectory(lib, topo, fs, dpos, dfor, den, stream, torch, npairs,
     """The large-system configuration as specified: 100 force evaluations of
     a moving configuration with the pair list rebuilt every 10 (a 1 A skin,
     the within-cutoff decision exact at every evaluation).  The positions
-    drift along fixed per-atom directions at up to 0.02 A per evaluation
-    (a synthetic trajectory in HBM, updated between the timed events)."""
+    drift along fixed per-molecule directions at up to 0.005 A per
+    evaluation (a synthetic trajectory in HBM, updated between the timed
+    events): each water moves as a whole, so the molecules keep their
+    shape."""
     VP = C.c_void_p
     arr = (VP * len(fs))(*[f.handle for f in fs])
     g = torch.Generator(device=dpos.device).manual_seed(100)
-    u = torch.randn(dpos.shape, dtype=torch.float64, device=dpos.device, generator=g)
-    u *= 0.02 * torch.rand((dpos.shape[0], 1), dtype=torch.float64, device=dpos.device, generator=g) / u.norm(dim=1,
-                                                                                                       keepdim=True)
+    mol = torch.as_tensor(np.asarray(topo.system.molecule), dtype=torch.long, device=dpos.device)
+    nm = int(mol.max().item()) + 1
+    um = torch.randn((nm, 3), dtype=torch.float64, device=dpos.device, generator=g)
+    um *= 0.005 * torch.rand((nm, 1), dtype=torch.float64, device=dpos.device, generator=g) / um.norm(dim=1,
+                                                                                                  keepdim=True)
+    u = um[mol]
     base = dpos.clone()
     topo.set_pair_list(skin, every)
     builds0 = topo.pair_list_builds()
