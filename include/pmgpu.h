@@ -83,6 +83,14 @@ extern "C" {
 
 /* evaluate flags */
 #define PMGPU_FLAG_VIRIAL 1u          /* ScalarStructure::virial() (base/ScalarStructure.h:135) */
+/* ScalarStructure::molecularVirial() (base/ScalarStructure.h:119): the
+ * energies pointer of pmgpu_evaluate then points to a pmgpu_energies_mol,
+ * d_energies of pmgpu_evaluate_device to 20 doubles; the molecule positions
+ * come from pmgpu_set_molecule_positions.  As in ProtoMol, pairs of atoms of
+ * different molecules then add to the atomic virial even without
+ * PMGPU_FLAG_VIRIAL (OneAtomPair.h:174-185), and the reciprocal term's
+ * scalarSum tensor reaches the molecular virial only with it (Grid.h:341-387). */
+#define PMGPU_FLAG_MOLECULAR_VIRIAL 2u
 
 typedef struct pmgpu_system pmgpu_system;
 typedef struct pmgpu_force pmgpu_force;
@@ -94,6 +102,14 @@ typedef struct {
     double coulomb;
     double virial[9];
 } pmgpu_energies;
+
+/* The same slots plus MOLVIRIALXX..MOLVIRIALZZ (row major). */
+typedef struct {
+    double lennard_jones;
+    double coulomb;
+    double virial[9];
+    double molecular_virial[9];
+} pmgpu_energies_mol;
 
 /* One NonbondedCutoffSystemForce.  n_terms = 1: OneAtomPair<Periodic, sw[0],
  * pot[0]>; n_terms = 2: OneAtomPairTwo<Periodic, sw[0], pot[0], sw[1],
@@ -216,6 +232,16 @@ int pmgpu_evaluate_device(pmgpu_system* sys, int n_forces, pmgpu_force* const* f
                           double* d_energies, unsigned flags);
 
 int pmgpu_synchronize(pmgpu_system* sys);
+
+/* GenericTopology::molecules[m].position for m = 0 .. n_molecules - 1 (3
+ * doubles each, host), the positions the molecular virial measures from
+ * (OneAtomPair.h:178-179, NonbondedPMEwaldSystemForce.h:917-919); ProtoMol
+ * sets them with buildMolecularCenterOfMass (topology/topologyutilities.cpp:
+ * 761-769) or minimalImage.  n_molecules must be the topology's largest
+ * molecule id plus one.  The copy is ordered on the system's stream before
+ * the next evaluation.  The vacuum all-pairs force has no molecular virial
+ * here (PMGPU_ERR_UNSUPPORTED), nor do the resident integrator runs. */
+int pmgpu_set_molecule_positions(pmgpu_system* sys, int n_molecules, const double* positions);
 
 /* The system's CUDA stream (a cudaStream_t). */
 void* pmgpu_stream(pmgpu_system* sys);

@@ -54,7 +54,7 @@ class _System(C.Structure):
         ("type", C.c_void_p), ("mol", C.c_void_p), ("n_types", C.c_int),
         ("lj", C.c_void_p), ("n_excl", C.c_int), ("excl", C.c_void_p),
         ("excl_check", C.c_void_p), ("box", C.c_double * 12), ("csf", C.c_double),
-        ("cell_size", C.c_double),
+        ("cell_size", C.c_double), ("mol_pos", C.c_void_p), ("no_virial", C.c_int),
     ]
 
 
@@ -80,6 +80,7 @@ class _Result(C.Structure):
         ("virial", C.c_double * 9), ("n_pairs", C.c_longlong), ("alpha", C.c_double),
         ("e_real", C.c_double), ("e_recip", C.c_double), ("e_intra", C.c_double),
         ("e_self", C.c_double), ("e_charged", C.c_double), ("out_of_grid", C.c_int),
+        ("mol_virial", C.c_double * 9),
     ]
 
 
@@ -112,7 +113,7 @@ def lookup_table(pot, sw, switchon, cutoff, alpha=0.0) -> np.ndarray:
 class _Keep:
     """Holds the numpy arrays a _System points into."""
 
-    def __init__(self, system, positions=None):
+    def __init__(self, system, positions=None, mol_pos=None, virial=True):
         pos = system.positions if positions is None else positions
         self.pos = np.ascontiguousarray(pos, np.float64)
         self.q = np.ascontiguousarray(system.scaled_charge, np.float64)
@@ -136,6 +137,12 @@ class _Keep:
             s.box[k] = v
         s.csf = system.csf
         s.cell_size = system.cell_size
+        if mol_pos is not None:
+            self.mol_pos = np.ascontiguousarray(mol_pos, np.float64).reshape(-1, 3)
+            if self.mol_pos.shape[0] < int(self.mol.max()) + 1:
+                raise ValueError("one position per molecule is needed")
+            s.mol_pos = self.mol_pos.ctypes.data
+        s.no_virial = 0 if virial else 1
         self.s = s
 
 
@@ -173,13 +180,16 @@ def _result_dict(r: _Result, forces):
         "virial": np.array(list(r.virial)), "n_pairs": int(r.n_pairs), "alpha": r.alpha,
         "e_real": r.e_real, "e_recip": r.e_recip, "e_intra": r.e_intra,
         "e_self": r.e_self, "e_charged": r.e_charged, "out_of_grid": r.out_of_grid,
+        "mol_virial": np.array(list(r.mol_virial)),
     }
 
 
-def evaluate(system, specs, positions=None, want_pairs=False, pair_cap=None):
+def evaluate(system, specs, positions=None, want_pairs=False, pair_cap=None, mol_pos=None, virial=True):
     """Evaluates the force specs in order into one force block (like
-    ForceGroup::evaluateSystemForces).  Returns a dict."""
-    keep = _Keep(system, positions)
+    ForceGroup::evaluateSystemForces).  Returns a dict.  ``mol_pos`` (one
+    position per molecule) turns the molecular virial on; ``virial=False``
+    is ScalarStructure::virial() off."""
+    keep = _Keep(system, positions, mol_pos, virial)
     n = keep.pos.shape[0]
     forces = np.zeros((n, 3), np.float64)
     r = _Result()
@@ -212,6 +222,18 @@ def evaluate(system, specs, positions=None, want_pairs=False, pair_cap=None):
     out = _result_dict(r, forces)
     if want_pairs:
         out["pairs"] = pairs
+    return out
+
+
+def molecular_centers(system, positions=None, mass=None):
+    """buildMolecularCenterOfMass (topology/topologyutilities.cpp:761-769)
+    with unit masses unless ``mass`` is given: (n_molecules, 3)."""
+    keep = _Keep(system, positions)
+    nm = int(keep.mol.max()) + 1 if keep.mol.size else 0
+    out = np.zeros((nm, 3), np.float64)
+    m = None if mass is None else np.ascontiguousarray(mass, np.float64)
+    lib().pmo_molecular_centers(C.byref(keep.s), None if m is None else m.ctypes.data_as(C.c_void_p),
+                                out.ctypes.data_as(C.c_void_p))
     return out
 
 
@@ -328,9 +350,13 @@ def _spec_args(spec):
             repr(float(spec.get("accuracy", 1e-6))), repr(float(spec.get("alpha", -1.0)))]
 
 
-def run_reference(system, specs, repeat: int = 1, fast: bool = False, timeout=None):
+def run_reference(system, specs, repeat: int = 1, fast: bool = False, timeout=None,
+                  molecular_virial=False, virial=True):
     """Runs the compiled reference; returns the same dict as :func:`evaluate`
-    plus ``cells``/``dims`` and ``seconds_per_eval`` (when repeat > 1)."""
+    plus ``cells``/``dims`` and ``seconds_per_eval`` (when repeat > 1).  With
+    ``molecular_virial`` the reference sets the molecule positions itself
+    (buildMolecularCenterOfMass, unit masses) and the dict adds
+    ``mol_pos`` and ``mol_virial``."""
     exe = os.path.join(REF_DIR, "pmref_fast" if fast else "pmref")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
@@ -341,7 +367,9 @@ def run_reference(system, specs, repeat: int = 1, fast: bool = False, timeout=No
         args = [exe, sp, op, str(int(repeat))]
         for spec in specs:
             args += _spec_args(spec)
-        subprocess.run(args, check=True, timeout=timeout, stdout=subprocess.DEVNULL)
+        env = dict(os.environ, PMREF_MOLVIR="1" if molecular_virial else "0",
+                   PMREF_NO_VIRIAL="0" if virial else "1")
+        subprocess.run(args, check=True, timeout=timeout, stdout=subprocess.DEVNULL, env=env)
         raw = open(op, "rb").read()
     n = system.n_atoms
     hdr = np.frombuffer(raw[: 13 * 8], np.float64)
@@ -351,11 +379,19 @@ def run_reference(system, specs, repeat: int = 1, fast: bool = False, timeout=No
     dims = tuple(int(x) for x in np.frombuffer(raw[off: off + 12], np.int32))
     off += 12
     cells = np.frombuffer(raw[off: off + 12 * n], np.int32).reshape(n, 3).copy()
-    return {
+    off += 12 * n
+    out = {
         "forces": forces, "lennard_jones": float(hdr[0]), "coulomb": float(hdr[1]),
         "virial": hdr[2:11].copy(), "seconds_per_eval": float(hdr[11]),
         "cells": cells, "dims": dims,
     }
+    if molecular_virial:
+        nm = int(np.frombuffer(raw[off: off + 4], np.int32)[0])
+        off += 4
+        out["mol_pos"] = np.frombuffer(raw[off: off + 24 * nm], np.float64).reshape(nm, 3).copy()
+        off += 24 * nm
+        out["mol_virial"] = np.frombuffer(raw[off: off + 72], np.float64).copy()
+    return out
 
 
 # ---------------------------------------------------------------- integration

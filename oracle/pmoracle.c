@@ -585,6 +585,16 @@ typedef struct {
     int vacuum;
 } pair_ctx;
 
+/* minimalDifference of the two molecules' positions (OneAtomPair.h:178-179):
+ * minimal image, or the plain difference in vacuum */
+static v3 mol_diff(const pair_ctx* c, int mi, int mj)
+{
+    v3 a = vload(c->s->mol_pos + 3 * (size_t)mi), b = vload(c->s->mol_pos + 3 * (size_t)mj);
+    if (c->vacuum) return vsub(b, a);
+    double d2;
+    return pbc_min_diff(c->b, a, b, &d2);
+}
+
 /* OneAtomPair::doOneAtomPair (forces/OneAtomPair.h:127-188) and
  * OneAtomPairTwo::doOneAtomPair (forces/OneAtomPairTwo.h:131-199). */
 static void one_atom_pair(pair_ctx* c, int i, int j)
@@ -621,7 +631,14 @@ static void one_atom_pair(pair_ctx* c, int i, int j)
     double* fj = c->f + 3 * j;
     fi[0] -= fij.x; fi[1] -= fij.y; fi[2] -= fij.z;
     fj[0] += fij.x; fj[1] += fij.y; fj[2] += fij.z;
-    add_virial(c->r->virial, fij, diff);
+    if (!same && s->mol_pos) {
+        /* ScalarStructure::addVirial(force, diff, comDiff)
+         * (base/ScalarStructure.cpp:90-132): atomic and molecular virial */
+        add_virial(c->r->virial, fij, diff);
+        add_virial(c->r->mol_virial, fij, mol_diff(c, s->mol[i], s->mol[j]));
+    } else if (!s->no_virial) {
+        add_virial(c->r->virial, fij, diff);
+    }
     if (c->pairs && c->r->n_pairs < c->cap) {
         c->pairs[2 * c->r->n_pairs] = i < j ? i : j;
         c->pairs[2 * c->r->n_pairs + 1] = i < j ? j : i;
@@ -649,6 +666,41 @@ static void pair_ctx_init(pair_ctx* c, const pmo_system* s, const pmo_cutoff_par
 static void pair_ctx_free(pair_ctx* c)
 {
     for (int k = 0; k < 2; ++k) { free(c->t[k].tab); c->t[k].tab = NULL; }
+}
+
+int pmo_molecular_centers(const pmo_system* s, const double* mass, double* centers)
+{
+    int nm = 0;
+    for (int i = 0; i < s->n_atoms; ++i)
+        if (s->mol[i] + 1 > nm) nm = s->mol[i] + 1;
+    /* per molecule: center, Kahan compensation, sum of masses, atoms seen */
+    double* acc = (double*)calloc(8 * (size_t)nm, sizeof(double));
+    for (int i = 0; i < s->n_atoms; ++i) {
+        double* a = acc + 8 * (size_t)s->mol[i];
+        double m = mass ? mass[i] : 1.0;
+        v3 x = vmul(vload(s->pos + 3 * i), m);
+        if (a[7] == 0.0) {
+            a[0] = x.x; a[1] = x.y; a[2] = x.z;
+            a[6] = m;
+        } else {
+            v3 center = mk(a[0], a[1], a[2]), tempC = mk(a[3], a[4], a[5]);
+            a[6] += m;
+            v3 tempY = vsub(x, tempC);
+            v3 tempT = vadd(center, tempY);
+            tempC = vsub(vsub(tempT, center), tempY);
+            a[0] = tempT.x; a[1] = tempT.y; a[2] = tempT.z;
+            a[3] = tempC.x; a[4] = tempC.y; a[5] = tempC.z;
+        }
+        a[7] += 1.0;
+    }
+    for (int m = 0; m < nm; ++m) {
+        const double* a = acc + 8 * (size_t)m;
+        if (a[7] == 0.0) { centers[3 * m] = centers[3 * m + 1] = centers[3 * m + 2] = 0.0; continue; }
+        v3 c = vdiv(mk(a[0], a[1], a[2]), a[6]);
+        centers[3 * m] = c.x; centers[3 * m + 1] = c.y; centers[3 * m + 2] = c.z;
+    }
+    free(acc);
+    return nm;
 }
 
 int pmo_cell_assign(const pmo_system* s, int* cells, int* dims)
@@ -878,9 +930,9 @@ int pmo_pme_force(const pmo_system* s, const pmo_pme_params* p, double* forces, 
             double* f1 = forces + 3 * a1; double* f2 = forces + 3 * a2;
             f1[0] -= fij.x; f1[1] -= fij.y; f1[2] -= fij.z;
             f2[0] += fij.x; f2[1] += fij.y; f2[2] += fij.z;
-            add_virial(r->virial, fij, rij);
+            if (!s->no_virial) add_virial(r->virial, fij, rij);
         }
-        r->virial[0] += charged; r->virial[4] += charged; r->virial[8] += charged;
+        if (!s->no_virial) { r->virial[0] += charged; r->virial[4] += charged; r->virial[8] += charged; }
     }
 
     double ereal = 0.0;
@@ -973,7 +1025,16 @@ int pmo_pme_force(const pmo_system* s, const pmo_pme_params* p, double* forces, 
                             fi = vsub(fi, fij);
                             double* fj = forces + 3 * j;
                             fj[0] += fij.x; fj[1] += fij.y; fj[2] += fij.z;
-                            add_virial(r->virial, fij, rij);
+                            if (!same && s->mol_pos) {
+                                /* realTerm (NonbondedPMEwaldSystemForce.h:750-757) */
+                                add_virial(r->virial, fij, rij);
+                                double dd;
+                                add_virial(r->mol_virial, fij,
+                                           pbc_min_diff(&b, vload(s->mol_pos + 3 * (size_t)mi),
+                                                        vload(s->mol_pos + 3 * (size_t)mj), &dd));
+                            } else if (!s->no_virial) {
+                                add_virial(r->virial, fij, rij);
+                            }
                             excl = PMO_EXCL_NONE;
                         }
                     }
@@ -1091,9 +1152,15 @@ int pmo_pme_force(const pmo_system* s, const pmo_pme_params* p, double* forces, 
             }
         }
         Q[0] = 0.0; Q[1] = 0.0;
-        r->virial[0] += vxx * 0.5; r->virial[1] += vxy * 0.5; r->virial[2] += vxz * 0.5;
-        r->virial[3] += vxy * 0.5; r->virial[4] += vyy * 0.5; r->virial[5] += vyz * 0.5;
-        r->virial[6] += vxz * 0.5; r->virial[7] += vyz * 0.5; r->virial[8] += vzz * 0.5;
+        double vrec[9] = {vxx * 0.5, vxy * 0.5, vxz * 0.5, vxy * 0.5, vyy * 0.5, vyz * 0.5,
+                          vxz * 0.5, vyz * 0.5, vzz * 0.5};
+        /* scalarSum's atomic and molecular virial (base/Grid.h:366-387); the
+         * sums themselves are taken only when virial() is on (:341-349), so
+         * without it the molecular virial gets zero here */
+        if (!s->no_virial)
+            for (int k = 0; k < 9; ++k) r->virial[k] += vrec[k];
+        if (s->mol_pos && !s->no_virial)
+            for (int k = 0; k < 9; ++k) r->mol_virial[k] += vrec[k];
         erecip = energy * 0.5;
         pmo_fft3d(Q, NX, NY, NZ, +1);
         /* interpolateForce (base/Grid.h:193-228) */
@@ -1119,9 +1186,19 @@ int pmo_pme_force(const pmo_system* s, const pmo_pme_params* p, double* forces, 
                 }
             }
             double q = s->q[a];
-            forces[3 * a] += fx * HXr * q;
-            forces[3 * a + 1] += fy * HYr * q;
-            forces[3 * a + 2] += fz * HZr * q;
+            v3 fi = mk(fx * HXr * q, fy * HYr * q, fz * HZr * q);
+            forces[3 * a] += fi.x;
+            forces[3 * a + 1] += fi.y;
+            forces[3 * a + 2] += fi.z;
+            if (s->mol_pos) {
+                /* reciprocalTerm (NonbondedPMEwaldSystemForce.h:905-924): the
+                 * atom's reciprocal force against its offset from the
+                 * molecule's position (Darden et al., J. Chem. Phys. 103, 8577) */
+                double dd;
+                v3 ria = pbc_min_pos(&b, vload(s->pos + 3 * a));
+                v3 mri = pbc_min_diff(&b, ria, vload(s->mol_pos + 3 * (size_t)s->mol[a]), &dd);
+                add_virial(r->mol_virial, fi, mri);
+            }
         }
         free(expX); free(expY); free(expZ); free(th0); free(dth0);
         free(modX); free(modY); free(modZ); free(Q); free(ipos); free(th);

@@ -49,6 +49,11 @@ typedef struct {
     double box[12];             /* e1, e2, e3, origin */
     double csf;                 /* coulombScalingFactor */
     double cell_size;           /* CubicCellManager cellsize */
+    /* GenericTopology::molecules[m].position, 3 per molecule: with it the
+     * molecular virial is computed (ScalarStructure::molecularVirial());
+     * NULL: off */
+    const double* mol_pos;
+    int no_virial;              /* ScalarStructure::virial() false */
 } pmo_system;
 
 /* One NonbondedCutoffSystemForce: OneAtomPair (n_terms = 1) or
@@ -82,7 +87,14 @@ typedef struct {
     double alpha;               /* PME: splitting parameter used */
     double e_real, e_recip, e_intra, e_self, e_charged;   /* PME parts */
     int out_of_grid;            /* atoms whose cell fell outside the grid */
+    double mol_virial[9];       /* MOLVIRIALXX..MOLVIRIALZZ (row major) */
 } pmo_result;
+
+/* buildMolecularCenterOfMass (topology/topologyutilities.cpp:761-769): the
+ * centre of mass of every molecule (atoms in index order, Kahan-summed as
+ * molecularCenterOfMass, :729-759), 3 per molecule into centers; mass NULL
+ * = unit masses.  Returns the number of molecules (max molecule id + 1). */
+int pmo_molecular_centers(const pmo_system* s, const double* mass, double* centers);
 
 /* Cell of every atom as buildCellLists computes it, and the grid dims.
  * cells: 3N ints. Returns 0. */

@@ -21,6 +21,11 @@
 //   sw: 0 Universal 1 Cutoff 2 C1 3 C2 4 Shift; pot: 1 LJ 2 Coulomb 3 EwaldReal
 // With repeat > 1 the evaluation is repeated (after one untimed warm-up) and
 // the mean wall time per evaluation is reported (the CPU baseline).
+// PMREF_MOLVIR=1 turns on ScalarStructure::molecularVirial() with the
+// molecule positions set by buildMolecularCenterOfMass (unit masses);
+// the molecule count, their positions and the molecular virial are then
+// appended to the output.  PMREF_NO_VIRIAL=1 turns ScalarStructure::virial()
+// off.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -57,6 +62,7 @@ using namespace ProtoMol::Report;
 #include "BSpline.h"
 #include "ScalarStructure.h"
 #include "Vector3DBlock.h"
+#include "topologyutilities.h"
 
 using namespace ProtoMol;
 
@@ -299,8 +305,12 @@ int main(int argc, char** argv)
     Vector3DBlock pos(b.n), frc(b.n);
     for (int i = 0; i < b.n; ++i) pos[i] = Vector3D(b.pos[3 * i], b.pos[3 * i + 1], b.pos[3 * i + 2]);
     ScalarStructure en;
-    en.molecularVirial(false);
-    en.virial(true);
+    const char* mv_env = getenv("PMREF_MOLVIR");
+    const char* nv_env = getenv("PMREF_NO_VIRIAL");
+    const bool molvir = mv_env && atoi(mv_env) != 0;
+    en.molecularVirial(molvir);
+    en.virial(!(nv_env && atoi(nv_env) != 0));
+    if (molvir) buildMolecularCenterOfMass(&pos, topo);
 
     double t0 = 0.0, t1 = 0.0;
     int reps = repeat > 1 ? repeat + 1 : 1;
@@ -346,6 +356,23 @@ int main(int argc, char** argv)
     }
     fwrite(dims, sizeof(int), 3, out);
     fwrite(cells.data(), sizeof(int), cells.size(), out);
+    if (molvir) {
+        int nm = (int)topo->molecules.size();
+        fwrite(&nm, sizeof(int), 1, out);
+        for (int m = 0; m < nm; ++m) {
+            const Vector3D& c = topo->molecules[m].position;
+            double c3[3] = {c.x, c.y, c.z};
+            fwrite(c3, sizeof(double), 3, out);
+        }
+        const int mslots[9] = {ScalarStructure::MOLVIRIALXX, ScalarStructure::MOLVIRIALXY,
+                               ScalarStructure::MOLVIRIALXZ, ScalarStructure::MOLVIRIALYX,
+                               ScalarStructure::MOLVIRIALYY, ScalarStructure::MOLVIRIALYZ,
+                               ScalarStructure::MOLVIRIALZX, ScalarStructure::MOLVIRIALZY,
+                               ScalarStructure::MOLVIRIALZZ};
+        double mv[9];
+        for (int k = 0; k < 9; ++k) mv[k] = en[(ScalarStructure::Index)mslots[k]];
+        fwrite(mv, sizeof(double), 9, out);
+    }
     fclose(out);
     for (size_t k = 0; k < forces.size(); ++k) delete forces[k];
     delete topo;

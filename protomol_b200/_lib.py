@@ -19,6 +19,7 @@ POT = {"LennardJones": 1, "Coulomb": 2, "CoulombEwaldReal": 3,
 SW = {"Universal": 0, "Cutoff": 1, "C1": 2, "C2": 3, "Shift": 4}
 PRECISION = {"mixed": 0, "fp64": 1}
 FLAG_VIRIAL = 1
+FLAG_MOLECULAR_VIRIAL = 2
 
 # every symbol include/pmgpu.h declares
 EXPORTS = [
@@ -26,7 +27,7 @@ EXPORTS = [
     "pmgpu_cutoff_create", "pmgpu_pme_create", "pmgpu_force_destroy", "pmgpu_pme_alpha",
     "pmgpu_evaluate", "pmgpu_evaluate_device", "pmgpu_synchronize", "pmgpu_stream",
     "pmgpu_launch_count", "pmgpu_last_error", "pmgpu_get_cells", "pmgpu_get_pairs", "pmgpu_pair_layout",
-    "pmgpu_set_pair_list", "pmgpu_pair_list_builds",
+    "pmgpu_set_pair_list", "pmgpu_pair_list_builds", "pmgpu_set_molecule_positions",
     "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
     "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
@@ -64,6 +65,12 @@ class Energies(C.Structure):
     _fields_ = [("lennard_jones", C.c_double), ("coulomb", C.c_double), ("virial", C.c_double * 9)]
 
 
+class EnergiesMol(C.Structure):
+    """pmgpu_energies_mol: the pmgpu_energies slots and the molecular virial."""
+    _fields_ = [("lennard_jones", C.c_double), ("coulomb", C.c_double), ("virial", C.c_double * 9),
+                ("molecular_virial", C.c_double * 9)]
+
+
 class PmgpuError(RuntimeError):
     def __init__(self, code, message):
         super().__init__(f"{ERRORS.get(code, code)}: {message}")
@@ -91,7 +98,8 @@ def load():
     lib.pmgpu_pme_create.argtypes = [vp, C.POINTER(PmeParams), C.POINTER(vp)]
     lib.pmgpu_force_destroy.argtypes = [vp]
     lib.pmgpu_pme_alpha.argtypes = [vp, dp]
-    lib.pmgpu_evaluate.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp, C.POINTER(Energies), C.c_uint]
+    lib.pmgpu_evaluate.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp, vp, C.c_uint]
+    lib.pmgpu_set_molecule_positions.argtypes = [vp, C.c_int, vp]
     lib.pmgpu_evaluate_device.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp, vp, C.c_uint]
     lib.pmgpu_synchronize.argtypes = [vp]
     lib.pmgpu_stream.argtypes = [vp]

@@ -182,6 +182,13 @@ namespace ProtoMol
 		return *m;
 	}
 
+	// host staging of the molecule positions (never destroyed, as above)
+	static std::vector<double>& molecule_positions()
+	{
+		static std::vector<double>* v = new std::vector<double>();
+		return *v;
+	}
+
 	static long long g_evaluations = 0;
 	long long GpuNonbondedForce::evaluations() { return g_evaluations; }
 
@@ -306,8 +313,6 @@ namespace ProtoMol
 	                                 Vector3DBlock* forces, ScalarStructure* energies)
 	{
 		ensureForce(topo);
-		if (energies->molecularVirial())
-			report << error << "[GpuNonbondedForce] the molecular virial is not computed on the GPU" << endr;
 		if (positions->size() == 0) return;
 		std::vector<pmgpu_force*> run(1, myForce);
 		if (coalescing()) {
@@ -336,23 +341,48 @@ namespace ProtoMol
 				}
 			}
 		}
-		pmgpu_energies e;
+		pmgpu_energies_mol e;
 		memset(&e, 0, sizeof(e));
 		unsigned flags = energies->virial() ? PMGPU_FLAG_VIRIAL : 0u;
-		int r = pmgpu_evaluate(mySystem, (int)run.size(), run.data(), &((*positions)[0].x), &((*forces)[0].x), &e,
-		                       flags);
+		const bool molvir = energies->molecularVirial();
+		if (molvir) {
+			// the molecule positions the integrator or front end set
+			// (buildMolecularCenterOfMass / minimalImage), read as the
+			// reference's forces read them
+			std::vector<double>& mp = molecule_positions();
+			mp.resize(3 * topo->molecules.size());
+			for (size_t m = 0; m < topo->molecules.size(); ++m) {
+				const Vector3D& c = topo->molecules[m].position;
+				mp[3 * m] = c.x; mp[3 * m + 1] = c.y; mp[3 * m + 2] = c.z;
+			}
+			if (pmgpu_set_molecule_positions(mySystem, (int)topo->molecules.size(), mp.data()) != PMGPU_OK)
+				gpu_fail(mySystem, "molecule positions");
+			flags |= PMGPU_FLAG_MOLECULAR_VIRIAL;
+		}
+		int r = pmgpu_evaluate(mySystem, (int)run.size(), run.data(), &((*positions)[0].x), &((*forces)[0].x),
+		                       reinterpret_cast<pmgpu_energies*>(&e), flags);
 		++g_evaluations;
 		if (r != PMGPU_OK) gpu_fail(mySystem, "evaluate");
 		// ScalarStructure slots (base/ScalarStructure.h:25-54)
 		(*energies)[ScalarStructure::LENNARDJONES] += e.lennard_jones;
 		(*energies)[ScalarStructure::COULOMB] += e.coulomb;
-		if (energies->virial()) {
+		// with the molecular virial alone the atomic slots hold the pairs of
+		// different molecules, as ScalarStructure::addVirial(f, d, comDiff) adds them
+		if (energies->virial() || molvir) {
 			const ScalarStructure::Index v[9] = {ScalarStructure::VIRIALXX, ScalarStructure::VIRIALXY,
 			                                     ScalarStructure::VIRIALXZ, ScalarStructure::VIRIALYX,
 			                                     ScalarStructure::VIRIALYY, ScalarStructure::VIRIALYZ,
 			                                     ScalarStructure::VIRIALZX, ScalarStructure::VIRIALZY,
 			                                     ScalarStructure::VIRIALZZ};
 			for (int k = 0; k < 9; ++k) (*energies)[v[k]] += e.virial[k];
+		}
+		if (molvir) {
+			const ScalarStructure::Index m[9] = {ScalarStructure::MOLVIRIALXX, ScalarStructure::MOLVIRIALXY,
+			                                     ScalarStructure::MOLVIRIALXZ, ScalarStructure::MOLVIRIALYX,
+			                                     ScalarStructure::MOLVIRIALYY, ScalarStructure::MOLVIRIALYZ,
+			                                     ScalarStructure::MOLVIRIALZX, ScalarStructure::MOLVIRIALZY,
+			                                     ScalarStructure::MOLVIRIALZZ};
+			for (int k = 0; k < 9; ++k) (*energies)[m[k]] += e.molecular_virial[k];
 		}
 	}
 

@@ -10,6 +10,9 @@
 // energies, virial, forces and the per-evaluation wall time.
 //
 // usage: gpu_force_driver <system.bin> <out.bin> <repeat> <definition>...
+// GPU_DRIVER_MOLVIR=1 turns ScalarStructure::molecularVirial() on, with the
+// molecule positions from buildMolecularCenterOfMass (unit masses), and
+// appends the molecular virial to the output.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -28,6 +31,7 @@ using namespace ProtoMol::Report;
 #include "Topology.h"
 #include "Vector3DBlock.h"
 #include "blob_topology.h"
+#include "topologyutilities.h"
 
 using namespace ProtoMol;
 
@@ -56,8 +60,11 @@ int main(int argc, char** argv)
     Vector3DBlock pos(b.n), frc(b.n);
     for (int i = 0; i < b.n; ++i) pos[i] = Vector3D(b.pos[3 * i], b.pos[3 * i + 1], b.pos[3 * i + 2]);
     ScalarStructure en;
-    en.molecularVirial(false);
+    const char* mv_env = getenv("GPU_DRIVER_MOLVIR");
+    const bool molvir = mv_env && atoi(mv_env) != 0;
+    en.molecularVirial(molvir);
     en.virial(true);
+    if (molvir) buildMolecularCenterOfMass(&pos, &topo);
     timespec t0, t1;
     int reps = repeat > 1 ? repeat + 1 : 1;
     for (int r = 0; r < reps; ++r) {
@@ -84,6 +91,15 @@ int main(int argc, char** argv)
     for (int i = 0; i < b.n; ++i) {
         double f3[3] = {frc[i].x, frc[i].y, frc[i].z};
         fwrite(f3, sizeof(double), 3, out);
+    }
+    if (molvir) {
+        const ScalarStructure::Index m[9] = {
+            ScalarStructure::MOLVIRIALXX, ScalarStructure::MOLVIRIALXY, ScalarStructure::MOLVIRIALXZ,
+            ScalarStructure::MOLVIRIALYX, ScalarStructure::MOLVIRIALYY, ScalarStructure::MOLVIRIALYZ,
+            ScalarStructure::MOLVIRIALZX, ScalarStructure::MOLVIRIALZY, ScalarStructure::MOLVIRIALZZ};
+        double mv[9];
+        for (int k = 0; k < 9; ++k) mv[k] = en[m[k]];
+        fwrite(mv, sizeof(double), 9, out);
     }
     for (size_t k = 0; k < forces.size(); ++k) {
         std::string id = forces[k]->getIdNoAlias();

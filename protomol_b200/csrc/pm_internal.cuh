@@ -216,4 +216,38 @@ __device__ __forceinline__ void warp_reduce_store(double (&v)[kERec], double* er
     }
 }
 
+// ---- molecular virial records -------------------------------------------
+// 18 components: MOLVIRIALXX..MOLVIRIALZZ, then the atomic virial of the
+// pairs between different molecules (VIRIALXX..VIRIALZZ), component-major
+// like the energy records
+constexpr int kMRec = 18;
+
+// ScalarStructure::addVirial / addMolVirial (base/ScalarStructure.cpp:41-88):
+// the tensor f (x) d with the upper triangle mirrored
+__device__ __forceinline__ void add_outer(double* v, double fx, double fy, double fz, double dx, double dy,
+                                          double dz)
+{
+    const double xy = fx * dy, xz = fx * dz, yz = fy * dz;
+    v[0] += fx * dx; v[1] += xy; v[2] += xz;
+    v[3] += xy; v[4] += fy * dy; v[5] += yz;
+    v[6] += xz; v[7] += yz; v[8] += fz * dz;
+}
+
+template <int NW, int N>
+__device__ __forceinline__ void block_reduce_store_n(double (&v)[N], double* rec, int stride, int r)
+{
+    for (int k = 0; k < N; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    __shared__ double red[NW][N];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < N; ++k) red[w][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < N) {
+        double s = 0.0;
+        for (int q = 0; q < NW; ++q) s += red[q][threadIdx.x];
+        rec[(size_t)threadIdx.x * stride + r] = s;
+    }
+}
+
 }  // namespace pm

@@ -220,6 +220,10 @@ struct PairArgs {
     const double* qorig;         // charges, types in atom order (FP64 near-pair energies)
     const int* torig;
     float list_skin;             // the column list includes pairs up to the cutoff plus this (reused lists)
+    // molecular virial (launch_pair_molvir): molecule positions, records
+    const double* molpos;        // 3 per molecule
+    double* mrec;
+    int mrec_stride;
 };
 
 // Combination id of the registered OneAtomPair[Two] templates.
@@ -236,6 +240,9 @@ int launch_near_energy_col(const PairArgs& a, int combo, int n_atoms, cudaStream
 long long col_list_estimate(int n_atoms, const ColGrid& g, double volume, double cutoff);
 long long col_chunk_estimate(long long entries, int n_atoms, const ColGrid& g, int chunk);
 int launch_pair_fp64(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches);
+// the molecular virial records (kMRec) of a cutoff force over the cell-sorted
+// order, one per block (blocks as launch_pair_fp64), no forces or energies
+int launch_pair_molvir(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches);
 int pair_blocks(const CellGrid& g, int nd);
 // blocks of the mixed kernel (4 warps, one energy record per warp)
 // estimated cluster-pair list entries and chunks of a system
@@ -319,10 +326,20 @@ struct PmeArgs {
     // launched after the gather; null: from the FP32 convolution pass
     void* cgrid64;
     const void* tw64;
+    // kStageMolvir: the molecular virial records (kMRec) of the reciprocal
+    // forces against each atom's offset from its molecule's position
+    const int* mol;
+    const double* molpos;        // 3 per molecule
+    Pbc pbc;
+    double* mrec;
+    int mrec_stride;
 };
 constexpr int kStageSpread = 0, kStageFft = 1, kStageGather = 2;
 constexpr int kStagePotential = 3;   // dE/dq~ = phi at the atoms, into (double*)facc
 constexpr int kStageEnergy64 = 4;    // mixed: the FP64 energy transform alone (energy64_apart)
+constexpr int kStageMolvir = 5;      // the reciprocal forces' molecular virial (after the gather)
+// molecular virial records one kStageMolvir launch writes
+int pme_molvir_blocks(int n);
 // One stage of the reciprocal term: K3 spread, the five FFT passes with the
 // fused convolution (K4/K5, writes energy records), or K6 gather.
 int launch_pme_reciprocal(const PmeArgs& a, int fp64, cudaStream_t s, long long* launches,
@@ -371,8 +388,13 @@ struct RealLatArgs {
     int erec_stride;
     int* status;
     int virial;
+    const double* molpos;        // molecular virial mode (launch_pme_real_lattice_molvir)
+    double* mrec;
+    int mrec_stride;
 };
 int launch_pme_real_lattice(const RealLatArgs& a, cudaStream_t s, long long* launches, int* blocks_used);
+// the lattice real space's molecular virial records (kMRec), no forces
+int launch_pme_real_lattice_molvir(const RealLatArgs& a, cudaStream_t s, long long* launches, int* blocks_used);
 int launch_pme_correction_adjoint(const CorrArgs& a, double* dq, cudaStream_t s, long long* launches);
 
 // ---------------------------------------------------------------- finalize
@@ -406,6 +428,21 @@ int launch_finalize(const FinArgs& a, cudaStream_t s, long long* launches, int* 
 // sums the FP64 records and adds the int64 fixed-point sums (efix, scale 2^32)
 int launch_energy_reduce(const double* erec, int stride, int nrec, const unsigned long long* efix,
                          double* out, cudaStream_t s, long long* launches);
+// the molecular virial into out[11..19]: the records (kMRec) plus the virial
+// slots of the reciprocal energy records in the given ranges (scalarSum's
+// tensor, which ProtoMol adds to both virials); without the atomic virial
+// (virial = 0) the records' inter-molecular atomic virial into out[2..10]
+struct MolvirFinish {
+    const double* mrec;
+    int mstride, nmrec;
+    const double* erec;
+    int estride;
+    int range_first[4], range_count[4];
+    int nranges;
+    int virial;
+    double* out;
+};
+int launch_molvir_finish(const MolvirFinish& f, cudaStream_t s, long long* launches);
 
 // Leapfrog kick / drift (LeapfrogIntegrator.cpp): the first step's half kick
 // and drift, a middle step's kick and drift, the last half kick

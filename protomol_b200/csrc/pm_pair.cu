@@ -482,6 +482,96 @@ __global__ void __launch_bounds__(128) k_pair_fp64(PairArgs p)
     block_reduce_store<4>(acc, p.erec, p.erec_stride, blockIdx.x);
 }
 
+// Molecular virial of a cutoff force (OneAtomPair.h:174-181,
+// OneAtomPairTwo.h:185-192): every pair of atoms of different molecules inside
+// the cutoff adds its FP64 pair force against the minimal difference of the
+// two molecules' positions (ScalarStructure::addVirial(f, diff, comDiff),
+// base/ScalarStructure.cpp:90-132), and against the pair vector to the
+// inter-molecular atomic virial.  The cell pairs and the arithmetic of
+// k_pair_fp64; a pair of one molecule adds to neither tensor (exclusions act
+// only within a molecule, so none applies here).  No forces, no energies.
+template <int NT, int P0, int S0, int P1, int S1>
+__global__ void __launch_bounds__(128) k_pair_molvir(PairArgs p)
+{
+    constexpr bool kMod = sw_modifies(S0) || (NT > 1 && sw_modifies(S1));
+    constexpr bool kUse = term_cut(P0, S0) || (NT > 1 && term_cut(P1, S1));
+    constexpr bool kR2 = pot_r2(P0) || (NT > 1 && pot_r2(P1));
+    __shared__ double4 sjp[4][32];
+    __shared__ int2 sjm[4][32];       // type, molecule
+    __shared__ double4 sjc[4][32];    // the molecule's position
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int warps_total = gridDim.x * 4;
+    const int n_items = p.grid.ncell * (p.nd + 1);
+    double acc[kMRec];
+    for (int k = 0; k < kMRec; ++k) acc[k] = 0.0;
+
+    for (int item = blockIdx.x * 4 + w; item < n_items; item += warps_total) {
+        ItemGeom g = decode_item(p, item);
+        if (!g.valid) continue;
+        int sa = p.start[g.a], ea = p.start[g.a + 1];
+        int sb = p.start[g.b], eb = p.start[g.b + 1];
+        if (sa == ea || sb == eb) continue;
+        for (int ia = sa; ia < ea; ia += 32) {
+            int i = ia + lane;
+            bool vi = i < ea;
+            double4 pi = vi ? p.spos64[i] : make_double4(0, 0, 0, 0);
+            int4 mi = vi ? p.smeta[i] : make_int4(-1, 0, -2, 0);
+            double cix = 0.0, ciy = 0.0, ciz = 0.0;
+            if (vi) {
+                const double* c = p.molpos + 3 * (size_t)mi.z;
+                cix = c[0]; ciy = c[1]; ciz = c[2];
+            }
+            for (int jb = g.same ? ia : sb; jb < eb; jb += 32) {
+                int j = jb + lane;
+                bool vj = j < eb;
+                sjp[w][lane] = vj ? p.spos64[j] : make_double4(0, 0, 0, 0);
+                int4 mj4 = vj ? p.smeta[j] : make_int4(-1, 0, -3, 0);
+                sjm[w][lane] = make_int2(mj4.y, mj4.z);
+                if (vj) {
+                    const double* c = p.molpos + 3 * (size_t)mj4.z;
+                    sjc[w][lane] = make_double4(c[0], c[1], c[2], 0.0);
+                }
+                __syncwarp();
+                int nj = min(32, eb - jb);
+                bool diag = g.same && jb == ia;
+                for (int t = 0; t < 32; ++t) {
+                    int jl = (lane + t) & 31;
+                    bool ok = vi && jl < nj && (!diag || jb + jl > i);
+                    if (!ok) continue;
+                    const int2 mj = sjm[w][jl];
+                    if (mj.y == mi.z) continue;
+                    double4 pj = sjp[w][jl];
+                    double dx, dy, dz;
+                    double d2 = pbc_min_diff(p.pbc, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+                    if (kUse && d2 > p.cut2d) continue;
+                    double rd2 = kR2 ? 1.0 / d2 : 1.0;
+                    double e0, f0, e1 = 0.0, f1 = 0.0;
+                    pot_f64<P0>(p, p.td[0], d2, rd2, pi.w, pj.w, mi.y, mj.x, PMGPU_EXCL_NONE, e0, f0);
+                    if (NT > 1) pot_f64<P1>(p, p.td[1], d2, rd2, pi.w, pj.w, mi.y, mj.x, PMGPU_EXCL_NONE, e1, f1);
+                    if (kMod) {
+                        double sv, sd;
+                        sw_f64<S0>(p.td[0], d2, sv, sd);
+                        f0 = f0 * sv - e0 * sd;
+                        if (NT > 1) {
+                            sw_f64<S1>(p.td[1], d2, sv, sd);
+                            f1 = f1 * sv - e1 * sd;
+                        }
+                    }
+                    double ft = NT > 1 ? (f0 + f1) : f0;
+                    double fx = dx * ft, fy = dy * ft, fz = dz * ft;
+                    const double4 cj = sjc[w][jl];
+                    double cx, cy, cz;
+                    pbc_min_diff(p.pbc, cix, ciy, ciz, cj.x, cj.y, cj.z, cx, cy, cz);
+                    add_outer(acc, fx, fy, fz, cx, cy, cz);
+                    add_outer(acc + 9, fx, fy, fz, dx, dy, dz);
+                }
+                __syncwarp();
+            }
+        }
+    }
+    block_reduce_store_n<4, kMRec>(acc, p.mrec, p.mrec_stride, blockIdx.x);
+}
+
 // ---------------------------------------------------------------- launch
 long long plist_estimate(int n_atoms, const CellGrid& g, int nh)
 {
@@ -726,6 +816,13 @@ int launch_near_energy_col(const PairArgs& a, int combo, int n_atoms, cudaStream
 int launch_pair_fp64(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches)
 {
     PM_COMBO_SWITCH(k_pair_fp64)
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+int launch_pair_molvir(const PairArgs& a, int combo, int blocks, cudaStream_t s, long long* launches)
+{
+    PM_COMBO_SWITCH(k_pair_molvir)
     *launches += 1;
     return (int)cudaGetLastError();
 }

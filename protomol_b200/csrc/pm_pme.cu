@@ -596,6 +596,55 @@ __global__ void __launch_bounds__(128) k_gather_p(PmeArgs a)
                (double)fz * a.hzr * q, a.scale, a.status);
 }
 
+// The reciprocal term's molecular virial (reciprocalTerm,
+// forces/NonbondedPMEwaldSystemForce.h:903-924): every atom's reciprocal force
+// (interpolateForce, recomputed from the convolved grid as k_gather does)
+// against the minimal difference from the atom's minimal position to its
+// molecule's position (Darden et al., J. Chem. Phys. 103, 8577); one record
+// (kMRec, the atomic part zero) per block of 128 atoms
+template <typename R>
+__global__ void __launch_bounds__(128) k_gather_molvir(PmeArgs a)
+{
+    double acc[kMRec];
+#pragma unroll
+    for (int k = 0; k < kMRec; ++k) acc[k] = 0.0;
+    const int atom = blockIdx.x * blockDim.x + threadIdx.x;
+    if (atom < a.n) {
+        R tx[kMaxOrder], dtx[kMaxOrder], ty[kMaxOrder], dty[kMaxOrder], tz[kMaxOrder], dtz[kMaxOrder];
+        int i0, j0, k0;
+        grid_point<R>(a, atom, i0, j0, k0, tx, dtx, ty, dty, tz, dtz);
+        const R* g = (const R*)a.rgrid;
+        R fx = 0, fy = 0, fz = 0;
+        const int P = a.order;
+        for (int i = 0; i < P; i++) {
+            int i1 = (i + i0) % a.kx;
+            for (int j = 0; j < P; j++) {
+                int j1 = (j + j0) % a.ky;
+                R xij = dtx[i] * ty[j], yij = tx[i] * dty[j], zij = tx[i] * ty[j];
+                size_t row = ((size_t)i1 * a.ky + j1) * a.kz;
+                for (int k = 0; k < P; k++) {
+                    int k1 = (k + k0) % a.kz;
+                    R term = g[row + k1];
+                    fx -= term * xij * tz[k];
+                    fy -= term * yij * tz[k];
+                    fz -= term * zij * dtz[k];
+                }
+            }
+        }
+        const double q = a.q[atom];
+        const double fix = (double)fx * a.hxr * q, fiy = (double)fy * a.hyr * q, fiz = (double)fz * a.hzr * q;
+        double rx, ry, rz, mx, my, mz;
+        pbc_min_pos(a.pbc, a.pos[3 * (size_t)atom], a.pos[3 * (size_t)atom + 1], a.pos[3 * (size_t)atom + 2],
+                    rx, ry, rz);
+        const double* c = a.molpos + 3 * (size_t)a.mol[atom];
+        pbc_min_diff(a.pbc, rx, ry, rz, c[0], c[1], c[2], mx, my, mz);
+        add_outer(acc, fix, fiy, fiz, mx, my, mz);
+    }
+    block_reduce_store_n<4, kMRec>(acc, a.mrec, a.mrec_stride, blockIdx.x);
+}
+
+int pme_molvir_blocks(int n) { return n > 0 ? (n + 127) / 128 : 0; }
+
 static int run_energy64(const PmeArgs& a0, cudaStream_t s, long long* launches, int* erec_used);
 
 template <typename R>
@@ -641,6 +690,10 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     if (stage == kStageEnergy64) {
         if (sizeof(R) == 4 && a.cgrid64) return run_energy64(a, s, launches, erec_used);
         return 0;
+    }
+    if (stage == kStageMolvir) {
+        if (a.n > 0) { k_gather_molvir<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+        return (int)cudaGetLastError();
     }
     if (stage == kStagePotential) {   // a.facc holds the double phi[N] output here
         if (a.n > 0) { k_gather_potential<R><<<nb, 128, 0, s>>>(a, (double*)a.facc); *launches += 1; }
@@ -958,6 +1011,67 @@ __global__ void __launch_bounds__(256) k_pme_real_lattice(RealLatArgs a)
     block_reduce_store<8>(acc, a.erec, a.erec_stride, blockIdx.x);
 }
 
+// realTerm's molecular virial (NonbondedPMEwaldSystemForce.h:750-757): every
+// image of a pair of atoms of different molecules inside the cutoff adds its
+// force against the minimal difference of the molecules' positions, and
+// against the image vector to the inter-molecular atomic virial.  The loop
+// and arithmetic of k_pme_real_lattice (pairs of one molecule skipped: they
+// add to neither tensor); no forces, no energies.
+__global__ void __launch_bounds__(256) k_pme_real_lattice_molvir(RealLatArgs a)
+{
+    double acc[kMRec];
+#pragma unroll
+    for (int k = 0; k < kMRec; ++k) acc[k] = 0.0;
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    const double E1 = 0.254829592, E2 = -0.284496736, E3 = 1.421413741, E4 = -1.453152027, E5 = 1.061405429,
+                 PP = 0.3275911;
+    for (int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < a.n; i += warps) {
+        const double xi = a.pos[3 * (size_t)i], yi = a.pos[3 * (size_t)i + 1], zi = a.pos[3 * (size_t)i + 2];
+        const double qi = a.q[i];
+        const int mi = a.mol[i];
+        const double* ci = a.molpos + 3 * (size_t)mi;
+        for (int j = i + 1 + lane; j < a.n; j += 32) {
+            const int mj = a.mol[j];
+            if (mj == mi) continue;
+            double mx, my, mz, cx, cy, cz;
+            pbc_min_diff(a.pbc, xi, yi, zi, a.pos[3 * (size_t)j], a.pos[3 * (size_t)j + 1], a.pos[3 * (size_t)j + 2],
+                         mx, my, mz);
+            const double* cj = a.molpos + 3 * (size_t)mj;
+            pbc_min_diff(a.pbc, ci[0], ci[1], ci[2], cj[0], cj[1], cj[2], cx, cy, cz);
+            const double qq = qi * a.q[j];
+            for (int k = 0; k < a.n_lattice; ++k) {
+                const double4 L = a.lattice[k];
+                const double rx = dadd(mx, L.x), ry = dadd(my, L.y), rz = dadd(mz, L.z);
+                const double r2 = dnorm2(rx, ry, rz);
+                if (r2 > a.rc2) continue;
+                const double r = sqrt(r2);
+                const double rr = 1.0 / r;
+                const double ar = a.alpha * r;
+                const double e = qq * exp(-ar * ar);
+                const double t = 1.0 / (1.0 + PP * ar);
+                const double energy = t * (E1 + t * (E2 + t * (E3 + t * (E4 + t * E5)))) * e * rr;
+                const double force = (energy + a.two_alpha_pi * e) * rr * rr;
+                const double fx = rx * force, fy = ry * force, fz = rz * force;
+                add_outer(acc, fx, fy, fz, cx, cy, cz);
+                add_outer(acc + 9, fx, fy, fz, rx, ry, rz);
+            }
+        }
+    }
+    block_reduce_store_n<8, kMRec>(acc, a.mrec, a.mrec_stride, blockIdx.x);
+}
+
+int launch_pme_real_lattice_molvir(const RealLatArgs& a, cudaStream_t s, long long* launches, int* blocks_used)
+{
+    int blocks = (a.n + 7) / 8;
+    if (blocks < 1) blocks = 1;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_pme_real_lattice_molvir<<<blocks, 256, 0, s>>>(a);
+    *launches += 1;
+    *blocks_used = blocks;
+    return (int)cudaGetLastError();
+}
+
 int launch_pme_real_lattice(const RealLatArgs& a, cudaStream_t s, long long* launches, int* blocks_used)
 {
     int blocks = (a.n + 7) / 8;                  // one warp per atom, 8 warps per block
@@ -1058,6 +1172,40 @@ __global__ void k_energy_reduce(const double* erec, int stride, int nrec, const 
         if (efix) t += (double)(long long)efix[k] * (1.0 / 4294967296.0);
         out[k] += t;
     }
+}
+
+// block k < 9: molecular virial component k; block 9 + k: the
+// inter-molecular atomic virial component k (only without the atomic virial)
+__global__ void k_molvir_finish(MolvirFinish f)
+{
+    const int k = blockIdx.x;
+    const bool mol = k < 9;
+    if (!mol && f.virial) return;
+    const double* c = f.mrec + (size_t)k * f.mstride;
+    double s = 0.0;
+    for (int r = threadIdx.x; r < f.nmrec; r += blockDim.x) s += c[r];
+    if (mol)
+        for (int g = 0; g < f.nranges; ++g) {
+            const double* e = f.erec + (size_t)(2 + k) * f.estride + f.range_first[g];
+            for (int r = threadIdx.x; r < f.range_count[g]; r += blockDim.x) s += e[r];
+        }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ double part[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) part[w] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += part[q];
+        f.out[mol ? 11 + k : 2 + (k - 9)] += t;
+    }
+}
+
+int launch_molvir_finish(const MolvirFinish& f, cudaStream_t s, long long* launches)
+{
+    k_molvir_finish<<<kMRec, 256, 0, s>>>(f);
+    *launches += 1;
+    return (int)cudaGetLastError();
 }
 
 int launch_energy_reduce(const double* erec, int stride, int nrec, const unsigned long long* efix,

@@ -23,13 +23,13 @@
 using namespace pm;
 
 static const double kPi = 3.14159265358979323846;   // Constant::M_PI (base/pmconstants.cpp:56)
-// mixed PME grids from this size on take the FP64 energy path (prepare_pme):
-// every grid
-static const size_t kEnergy64Points = 0;
 static const double kEpsilon = 1.0e-14;              // Constant::EPSILON (base/pmconstants.cpp:45)
 // status word, list count and need, chunk count and need, work counter, pad,
 // then 11 int64 energy/virial sums
 static const size_t kSmallBytes = 64 + 8 * kERec;
+// the evaluation's output slots: pmgpu_energies_mol (LJ, Coulomb, virial,
+// molecular virial)
+static const int kEOut = 20;
 
 // evaluation phases timed in profiling mode (pmgpu_phase_times)
 enum { kPhaseBin = 0, kPhasePair, kPhaseCorrection, kPhaseSpread, kPhaseFft, kPhaseGather, kPhaseFinalize,
@@ -80,6 +80,13 @@ struct pmgpu_system {
     double* d_q = nullptr;
     int* d_type = nullptr;
     int* d_mol = nullptr;
+    int n_mol = 0;                     // molecule ids 0 .. n_mol - 1
+    // GenericTopology::molecules[m].position (pmgpu_set_molecule_positions),
+    // read by the molecular virial; records of its kernels (kMRec)
+    double* d_molpos = nullptr;
+    bool molpos_set = false;
+    double* d_mrec = nullptr;
+    int mrec_cap = 0;
     float4* d_ljn = nullptr;
     float4* d_ljm = nullptr;
     double4* d_ljd = nullptr;
@@ -99,8 +106,8 @@ struct pmgpu_system {
     // per-evaluation buffers
     double* d_pos = nullptr;
     double* d_fout = nullptr;
-    double* d_energy = nullptr;        // 11
-    double* h_energy = nullptr;        // pinned 11
+    double* d_energy = nullptr;        // kEOut
+    double* h_energy = nullptr;        // pinned kEOut
     unsigned long long* d_facc32 = nullptr;   // mixed (2^32): 3N pair forces + 3N other (d_facc32p)
     unsigned long long* d_facc32p = nullptr;
     unsigned long long* d_facc40 = nullptr;   // FP64 (2^40)
@@ -334,8 +341,8 @@ extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
         return PMGPU_ERR_CUDA;
     }
     if (cudaMalloc(&sys->d_small, kSmallBytes) != cudaSuccess ||
-        cudaMalloc((void**)&sys->d_energy, sizeof(double) * kERec) != cudaSuccess ||
-        cudaMallocHost((void**)&sys->h_energy, sizeof(double) * kERec) != cudaSuccess) {
+        cudaMalloc((void**)&sys->d_energy, sizeof(double) * kEOut) != cudaSuccess ||
+        cudaMallocHost((void**)&sys->h_energy, sizeof(double) * kEOut) != cudaSuccess) {
         delete sys;
         return PMGPU_ERR_NOMEM;
     }
@@ -353,6 +360,7 @@ extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
 static void free_atom_buffers(pmgpu_system* s)
 {
     dfree(s->d_q); dfree(s->d_type); dfree(s->d_mol); dfree(s->d_ljn); dfree(s->d_ljm); dfree(s->d_ljd);
+    dfree(s->d_molpos); s->molpos_set = false;
     dfree(s->d_slo); dfree(s->d_skey);
     dfree(s->d_xfull); dfree(s->d_xmod); dfree(s->d_xrow); dfree(s->d_xent);
     dfree(s->d_epairs); dfree(s->d_ecls);
@@ -388,7 +396,7 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     for (cudaEvent_t e : sys->prof_pool) cudaEventDestroy(e);
     free_atom_buffers(sys);
     free_col_buffers(sys);
-    dfree(sys->d_counts); dfree(sys->d_start); dfree(sys->d_erec);
+    dfree(sys->d_counts); dfree(sys->d_start); dfree(sys->d_erec); dfree(sys->d_mrec);
     dfree(sys->d_small); dfree(sys->d_energy);
     dfree(sys->d_cstart); dfree(sys->d_cbox); dfree(sys->d_ccell); dfree(sys->d_plist); dfree(sys->d_chunks);
     dfree(sys->d_near);
@@ -503,8 +511,12 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     if (n_atoms > 0 && (!scaled_charge || !type || !molecule)) return fail(sys, PMGPU_ERR_ARG, "null atom array");
     if (n_types > 0 && !lj_table) return fail(sys, PMGPU_ERR_ARG, "null Lennard-Jones table");
     if (n_excl > 0 && (!excl_pairs || !excl_class)) return fail(sys, PMGPU_ERR_ARG, "null exclusion array");
-    for (int i = 0; i < n_atoms; ++i)
+    int n_mol = 0;
+    for (int i = 0; i < n_atoms; ++i) {
         if (type[i] < 0 || type[i] >= n_types) return fail(sys, PMGPU_ERR_ARG, "atom type out of range");
+        if (molecule[i] < 0) return fail(sys, PMGPU_ERR_ARG, "negative molecule id");
+        n_mol = std::max(n_mol, molecule[i] + 1);
+    }
     cudaSetDevice(sys->device);
     CK(cudaStreamSynchronize(sys->stream), "set_topology");
     free_atom_buffers(sys);
@@ -512,6 +524,7 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     for (auto& g : sys->graphs) cudaGraphExecDestroy(g.exec);
     sys->graphs.clear();
     sys->n = n_atoms; sys->t = n_types; sys->e = n_excl; sys->csf = coulomb_scaling_factor;
+    sys->n_mol = n_mol;
     sys->q.assign(scaled_charge, scaled_charge + n_atoms);
     sys->binned = false;
     int n = n_atoms;
@@ -1335,14 +1348,9 @@ static int prepare_pme(pmgpu_force* f)
         // reaches the total energy of water boxes (a near cancellation of
         // the real-space, reciprocal and self terms): 2.5e-7 of the total on
         // a 9,000-atom box at 45^3, 5.9e-7 on 1,000,000 atoms at 216^3.
-        if (nreal >= kEnergy64Points) {
-            CK(dalloc((double2**)&f->d_tw64, ntw), "alloc");
-            CK(cudaMemcpy(f->d_tw64, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice), "copy");
-            CK(dalloc((double2**)&f->d_cgrid64, nhalf), "alloc");
-        } else {
-            if (f->d_tw64) { cudaFree(f->d_tw64); f->d_tw64 = nullptr; }
-            if (f->d_cgrid64) { cudaFree(f->d_cgrid64); f->d_cgrid64 = nullptr; }
-        }
+        CK(dalloc((double2**)&f->d_tw64, ntw), "alloc");
+        CK(cudaMemcpy(f->d_tw64, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice), "copy");
+        CK(dalloc((double2**)&f->d_cgrid64, nhalf), "alloc");
     }
     // point self energy and charged-system term (:604-628)
     double V = std::fabs(sys->box[0] * sys->box[4] * sys->box[8]);
@@ -1521,7 +1529,7 @@ static int pme_xblocks(const pmgpu_force* f) { return f->pp.grid[1] * f->kzh; }
 
 // Everything that allocates or copies synchronously: force tables, buffer
 // capacities.  Runs before an evaluation is enqueued (or captured).
-static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
+static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces, unsigned flags)
 {
     if (nf < 0 || (nf > 0 && !forces)) return fail(sys, PMGPU_ERR_ARG, "bad force list");
     bool periodic = false;
@@ -1539,6 +1547,31 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces)
     need += (sys->n + 255) / 256;   // finalize: pair virial records
     int r = ensure_erec(sys, need);
     if (r) return r;
+    if (flags & PMGPU_FLAG_MOLECULAR_VIRIAL) {
+        // the molecule positions come from the caller (GenericTopology::
+        // molecules[m].position, set by the integrator or front end)
+        if (!sys->molpos_set)
+            return fail(sys, PMGPU_ERR_STATE, "molecular virial without molecule positions (pmgpu_set_molecule_positions)");
+        int mneed = 1, n_pme = 0;
+        for (int k = 0; k < nf; ++k) {
+            pmgpu_force* f = forces[k];
+            if (f->kind == 2)
+                return fail(sys, PMGPU_ERR_UNSUPPORTED, "molecular virial of an all-pairs (vacuum) force");
+            if (f->kind == 0) mneed += pair_blocks(sys->grid, f->nd);
+            if (f->kind == 1) {
+                ++n_pme;
+                if (f->pp.real && pme_needs_lattice(f)) mneed += 148 * 4;
+                if (f->pp.reciprocal) mneed += pme_molvir_blocks(sys->n);
+            }
+        }
+        if (n_pme > 4) return fail(sys, PMGPU_ERR_UNSUPPORTED, "molecular virial with more than 4 PME forces");
+        if (mneed > sys->mrec_cap) {
+            int cap = std::max(mneed, 2 * sys->mrec_cap);
+            CK(dalloc(&sys->d_mrec, (size_t)cap * kMRec), "alloc");
+            sys->mrec_cap = cap;
+            sys->buf_version++;
+        }
+    }
     // clusters: at most N / 8 full ones plus one partial per cell
     int ncl = sys->n / kCluster + sys->grid.ncell + 1;
     if (ncl > sys->cbox_cap) {
@@ -1662,6 +1695,10 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                         double* d_fout, double* d_energy, unsigned flags)
 {
     int virial = (flags & PMGPU_FLAG_VIRIAL) ? 1 : 0;
+    const bool molvir = (flags & PMGPU_FLAG_MOLECULAR_VIRIAL) != 0;
+    int mused = 0;                      // molecular virial records
+    MolvirFinish mf;
+    memset(&mf, 0, sizeof(mf));
     bool use32 = false, use40 = false;
     for (int k = 0; k < nf; ++k) (forces[k]->precision == PMGPU_PRECISION_FP64 ? use40 : use32) = true;
     int r;
@@ -1697,6 +1734,9 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     bool cell_sort = false;
     for (int k = 0; k < nf; ++k)
         if (forces[k]->kind == 0 && (forces[k]->precision == PMGPU_PRECISION_FP64 || !use_col)) cell_sort = true;
+    // the molecular virial kernels of the cutoff forces read the cell-sorted
+    // order too (binned for them alone on the column path)
+    const bool mv_bin = molvir && any_cut && !cell_sort;
     int used = 0;
     // PME: reads only positions and charges and accumulates in atom order.
     // Beside the pair kernels (branches = true) the correction term and the
@@ -1751,6 +1791,12 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 if (e) return cuda_fail(sys, (cudaError_t)e, "PME real space (lattice images)");
                 prof_end(sys, m);
                 used += b;
+                if (molvir) {
+                    la.molpos = sys->d_molpos; la.mrec = sys->d_mrec + mused; la.mrec_stride = sys->mrec_cap;
+                    e = launch_pme_real_lattice_molvir(la, ps, &sys->launches, &b);
+                    if (e) return cuda_fail(sys, (cudaError_t)e, "PME real space molecular virial");
+                    mused += b;
+                }
             }
             if (p.reciprocal) {
                 PmeArgs a;
@@ -1771,6 +1817,8 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 a.wr = 1.0 / LX; a.lr = 1.0 / LY; a.hr = 1.0 / LZ;
                 a.facc = facc; a.scale = scale; a.qscale = kScaleFp64; a.erec_stride = sys->erec_cap;
                 a.status = sys->d_status; a.virial = virial; a.fft_lines = sys->tuning.fft_lines;
+                a.mol = sys->d_mol; a.molpos = sys->d_molpos; a.pbc = sys->pbc;
+                a.mrec = sys->d_mrec; a.mrec_stride = sys->mrec_cap;
                 const bool e64 = branches && a.cgrid64 != nullptr && !e64_branch;
                 a.energy64_apart = e64 ? 1 : 0;
                 const int phases[3] = {kPhaseSpread, kPhaseFft, kPhaseGather};
@@ -1781,8 +1829,21 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                     int e = launch_pme_reciprocal(a, fp64 ? 1 : 0, ps, &sys->launches,
                                                   sys->d_erec + used, &u, stages[st]);
                     if (e) return cuda_fail(sys, (cudaError_t)e, "PME reciprocal");
+                    // scalarSum's records: its tensor is the molecular virial's too
+                    if (molvir && u > 0) {
+                        mf.range_first[mf.nranges] = used;
+                        mf.range_count[mf.nranges++] = u;
+                    }
                     used += u;
                     prof_end(sys, m);
+                    if (st == 2 && molvir) {
+                        PmeArgs am = a;
+                        am.mrec = sys->d_mrec + mused;
+                        int um = 0;
+                        e = launch_pme_reciprocal(am, fp64 ? 1 : 0, ps, &sys->launches, nullptr, &um, kStageMolvir);
+                        if (e) return cuda_fail(sys, (cudaError_t)e, "PME reciprocal molecular virial");
+                        mused += pme_molvir_blocks(sys->n);
+                    }
                     if (st == 0 && e64) {
                         // the FP64 energy transform reads only the charge grid:
                         // from the spread on, beside the FP32 transform and gather
@@ -1792,6 +1853,10 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                         e = launch_pme_reciprocal(a, 0, sys->side2, &sys->launches, sys->d_erec + used, &u,
                                                   kStageEnergy64);
                         if (e) return cuda_fail(sys, (cudaError_t)e, "PME energy transform");
+                        if (molvir && u > 0) {
+                            mf.range_first[mf.nranges] = used;
+                            mf.range_count[mf.nranges++] = u;
+                        }
                         used += u;
                         e64_branch = true;
                     }
@@ -1819,7 +1884,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         if (r) return r;
         CK(cudaEventRecord(sys->ev_join, sys->side), "join");
     }
-    if (cell_sort) {
+    if (cell_sort || mv_bin) {
         r = bin(sys, d_pos);
         if (r) return r;
     }
@@ -1897,6 +1962,20 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         prof_end(sys, m);
         used += pair_records(sys, f);
     }
+    if (molvir) {
+        // the cutoff forces' molecular virial over the cell-sorted order
+        for (int k = 0; k < nf; ++k) {
+            pmgpu_force* f = forces[k];
+            if (f->kind != 0) continue;
+            PairArgs a;
+            fill_pair_args(sys, f, d_pos, a);
+            a.molpos = sys->d_molpos; a.mrec = sys->d_mrec + mused; a.mrec_stride = sys->mrec_cap;
+            const int blocks = pair_blocks(sys->grid, f->nd);
+            int e = launch_pair_molvir(a, f->combo, blocks, s, &sys->launches);
+            if (e) return cuda_fail(sys, (cudaError_t)e, "molecular virial");
+            mused += blocks;
+        }
+    }
     if (fork) {
         CK(cudaStreamWaitEvent(s, sys->ev_join, 0), "join");
     } else if (any_pme) {
@@ -1938,6 +2017,13 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         if (near_on_side) CK(cudaStreamWaitEvent(s, sys->ev_near, 0), "join");
         int e = launch_energy_reduce(sys->d_erec, sys->erec_cap, used, sys->d_efix, d_energy, s, &sys->launches);
         if (e) return cuda_fail(sys, (cudaError_t)e, "energy reduce");
+        if (molvir) {
+            mf.mrec = sys->d_mrec; mf.mstride = sys->mrec_cap; mf.nmrec = mused;
+            mf.erec = sys->d_erec; mf.estride = sys->erec_cap;
+            mf.virial = virial; mf.out = d_energy;
+            e = launch_molvir_finish(mf, s, &sys->launches);
+            if (e) return cuda_fail(sys, (cudaError_t)e, "molecular virial");
+        }
     }
     prof_end(sys, mfin);
     return PMGPU_OK;
@@ -1958,7 +2044,7 @@ static int eval_core(pmgpu_system* sys, int nf_in, pmgpu_force* const* forces_in
     }
     const int nf = (int)all.size();
     pmgpu_force* const* forces = all.data();
-    int r = eval_prepare(sys, nf, forces);
+    int r = eval_prepare(sys, nf, forces, flags);
     if (r) return r;
     // a reused pair list: the column path with one mixed cutoff force (its
     // list is the system's only one), a rebuild period above one, a list
@@ -2056,11 +2142,11 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
     // (the first attempt recorded the size it needs)
     for (int attempt = 0; attempt < 2; ++attempt) {
         CK(cudaMemsetAsync(sys->d_fout, 0, sizeof(double) * n3, s), "memset");
-        CK(cudaMemsetAsync(sys->d_energy, 0, sizeof(double) * kERec, s), "memset");
+        CK(cudaMemsetAsync(sys->d_energy, 0, sizeof(double) * kEOut, s), "memset");
         r = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy, flags);
         if (r) return r;
         CK(cudaMemcpyAsync(sys->h_fbuf.data(), sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
-        CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kERec, cudaMemcpyDeviceToHost, s), "D2H energies");
+        CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kEOut, cudaMemcpyDeviceToHost, s), "D2H energies");
         sys->col_just_disabled = false;
         sys->list_just_invalidated = false;
         r = pmgpu_synchronize(sys);
@@ -2073,8 +2159,33 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
     for (size_t k = 0; k < n3; ++k) forces_accum[k] += sys->h_fbuf[k];
     energies->lennard_jones += sys->h_energy[0];
     energies->coulomb += sys->h_energy[1];
-    if (flags & PMGPU_FLAG_VIRIAL)
+    // with the molecular virial alone the atomic slots hold the
+    // inter-molecular pairs' part (ScalarStructure::addVirial(f, d, comDiff))
+    if (flags & (PMGPU_FLAG_VIRIAL | PMGPU_FLAG_MOLECULAR_VIRIAL))
         for (int k = 0; k < 9; ++k) energies->virial[k] += sys->h_energy[2 + k];
+    if (flags & PMGPU_FLAG_MOLECULAR_VIRIAL) {
+        pmgpu_energies_mol* em = reinterpret_cast<pmgpu_energies_mol*>(energies);
+        for (int k = 0; k < 9; ++k) em->molecular_virial[k] += sys->h_energy[11 + k];
+    }
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_set_molecule_positions(pmgpu_system* sys, int n_molecules, const double* positions)
+{
+    if (!sys || !positions) return PMGPU_ERR_ARG;
+    if (sys->n == 0 && sys->q.empty()) return fail(sys, PMGPU_ERR_STATE, "topology not set");
+    if (n_molecules != sys->n_mol)
+        return fail(sys, PMGPU_ERR_ARG, "one position per molecule of the topology is needed");
+    cudaSetDevice(sys->device);
+    if (!sys->d_molpos) {
+        CK(dalloc(&sys->d_molpos, 3 * (size_t)std::max(n_molecules, 1)), "alloc");
+        sys->buf_version++;
+    }
+    // stream-ordered: the next evaluation reads these positions
+    if (n_molecules > 0)
+        CK(cudaMemcpyAsync(sys->d_molpos, positions, sizeof(double) * 3 * (size_t)n_molecules,
+                           cudaMemcpyHostToDevice, sys->stream), "H2D molecule positions");
+    sys->molpos_set = true;
     return PMGPU_OK;
 }
 
@@ -2115,7 +2226,7 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     if (f->kind != 0) return fail(sys, PMGPU_ERR_UNSUPPORTED, "pair recording is for cutoff forces");
     if (!sys->box_set) return fail(sys, PMGPU_ERR_STATE, "box not set");
     cudaSetDevice(sys->device);
-    int r = eval_prepare(sys, 1, &f);
+    int r = eval_prepare(sys, 1, &f, 0);
     if (r) return r;
     cudaStream_t s = sys->stream;
     size_t n3 = 3 * (size_t)sys->n;
@@ -2425,7 +2536,7 @@ extern "C" int pmgpu_batch_evaluate(pmgpu_batch* b)
     std::vector<GraphKey> keys;
     for (auto& m : b->members) {
         if (m.sys->profiling) return batch_fail(b, PMGPU_ERR_STATE, "a member system is in profiling mode");
-        int r = eval_prepare(m.sys, (int)m.forces.size(), m.forces.data());
+        int r = eval_prepare(m.sys, (int)m.forces.size(), m.forces.data(), m.flags);
         if (r) return batch_fail(b, r, m.sys->err);
         GraphKey k;
         for (pmgpu_force* f : m.forces) k.ids.push_back(f->id);
@@ -2583,7 +2694,7 @@ extern "C" int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* cons
     if (!sys || n_forces <= 0 || !forces || !positions || evals < 1 || !best) return PMGPU_ERR_ARG;
     if (sys->profiling) return fail(sys, PMGPU_ERR_STATE, "autotune in profiling mode");
     cudaSetDevice(sys->device);
-    int r = eval_prepare(sys, n_forces, forces);
+    int r = eval_prepare(sys, n_forces, forces, flags);
     if (r) return r;
     cudaStream_t s = sys->stream;
     const size_t n3 = 3 * (size_t)sys->n;
@@ -2697,7 +2808,7 @@ extern "C" int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const
         if (forces_in[k]->kind != 1) fl.push_back(forces_in[k]);
     }
     if (sys->n > kHessianMaxAtoms) return fail(sys, PMGPU_ERR_CAPACITY, "dense Hessian above 8192 atoms");
-    int r = eval_prepare(sys, (int)fl.size(), fl.data());
+    int r = eval_prepare(sys, (int)fl.size(), fl.data(), 0);
     if (r) return r;
     const size_t n3 = 3 * (size_t)sys->n, nh = n3 * n3;
     cudaStream_t s = sys->stream;
@@ -2731,6 +2842,9 @@ extern "C" int pmgpu_leapfrog_run(pmgpu_system* sys, int n_forces, pmgpu_force* 
     if (!sys || n_forces <= 0 || !forces || !d_mass || !d_positions || !d_velocities || !d_forces || !d_energies)
         return PMGPU_ERR_ARG;
     if (!(timestep > 0.0) || n_steps < 0) return fail(sys, PMGPU_ERR_ARG, "timestep must be positive, steps >= 0");
+    // the molecule positions move with the atoms: the caller's per-step evaluation sets them
+    if (flags & PMGPU_FLAG_MOLECULAR_VIRIAL)
+        return fail(sys, PMGPU_ERR_UNSUPPORTED, "molecular virial inside a resident run");
     if (n_steps == 0) return PMGPU_OK;
     cudaSetDevice(sys->device);
     cudaStream_t s = sys->stream;
@@ -2764,6 +2878,8 @@ extern "C" int pmgpu_impulse_run(pmgpu_system* sys, int n_slow, pmgpu_force* con
         return PMGPU_ERR_ARG;
     if (!(timestep > 0.0) || cyclelength < 1 || n_steps < 0)
         return fail(sys, PMGPU_ERR_ARG, "timestep must be positive, cyclelength >= 1, steps >= 0");
+    if (flags & PMGPU_FLAG_MOLECULAR_VIRIAL)
+        return fail(sys, PMGPU_ERR_UNSUPPORTED, "molecular virial inside a resident run");
     cudaSetDevice(sys->device);
     cudaStream_t s = sys->stream;
     const size_t n3 = 3 * (size_t)sys->n;
@@ -2828,7 +2944,7 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
         if (hv && f->kind == 1 && (f->pp.reciprocal || f->pp.correction))
             return fail(sys, PMGPU_ERR_UNSUPPORTED, "Hessian-vector product of the PME reciprocal / correction "
                                                     "terms is not available (the real-space pairs are)");
-    int r = eval_prepare(sys, (int)fl.size(), fl.data());
+    int r = eval_prepare(sys, (int)fl.size(), fl.data(), 0);
     if (r) return r;
     const int n = sys->n, T = sys->t;
     cudaStream_t s = sys->stream;

@@ -33,18 +33,23 @@ _VP = C.c_void_p
 
 class ScalarStructure:
     """The slots of ``ScalarStructure`` (``base/ScalarStructure.h:25-54``)
-    this path writes, with the ``virial()`` switch."""
+    this path writes, with the ``virial()`` and ``molecularVirial()``
+    switches.  The molecular virial needs the molecule positions
+    (:meth:`Topology.set_molecule_positions`)."""
 
-    def __init__(self, virial: bool = True):
+    def __init__(self, virial: bool = True, molecular_virial: bool = False):
         self.lennard_jones = 0.0
         self.coulomb = 0.0
         self.virial_tensor = np.zeros(9)
+        self.molecular_virial_tensor = np.zeros(9)
         self.virial = virial
+        self.molecular_virial = molecular_virial
 
     def clear(self):
         self.lennard_jones = 0.0
         self.coulomb = 0.0
         self.virial_tensor[:] = 0.0
+        self.molecular_virial_tensor[:] = 0.0
 
     def potential_energy(self) -> float:
         return self.lennard_jones + self.coulomb
@@ -119,6 +124,15 @@ class Topology:
         check(lib.pmgpu_autotune(self.handle, len(forces), arr, pos.ctypes.data_as(_VP),
                                  _lib.FLAG_VIRIAL if virial else 0, int(evals), C.byref(t)), self.handle)
         return t.as_dict()
+
+    def set_molecule_positions(self, positions):
+        """pmgpu_set_molecule_positions: ``GenericTopology::molecules[m].
+        position`` for every molecule (n_molecules, 3), the points the
+        molecular virial measures from (ProtoMol sets them with
+        buildMolecularCenterOfMass or minimalImage)."""
+        p = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+        check(_lib.load().pmgpu_set_molecule_positions(self.handle, p.shape[0], p.ctypes.data_as(_VP)),
+              self.handle)
 
     def set_pair_list(self, skin: float, rebuild_every: int):
         """pmgpu_set_pair_list: keep the column layout's pair list, built with
@@ -228,6 +242,45 @@ class NonbondedPMEwaldSystemForce(SystemForce):
         return a.value
 
 
+def molecular_centers(molecule, positions, mass=None) -> np.ndarray:
+    """buildMolecularCenterOfMass (topology/topologyutilities.cpp:761-769):
+    the centre of mass of every molecule, its atoms taken in index order and
+    Kahan-summed as molecularCenterOfMass (:729-759) does, unit masses unless
+    ``mass`` is given.  Returns (max molecule id + 1, 3); the positions for
+    :meth:`Topology.set_molecule_positions`."""
+    mol = np.asarray(molecule, np.int64)
+    pos = np.asarray(positions, np.float64).reshape(-1, 3)
+    m = np.ones(mol.shape[0]) if mass is None else np.asarray(mass, np.float64)
+    nm = int(mol.max()) + 1 if mol.size else 0
+    order = np.argsort(mol, kind="stable")             # each molecule's atoms in index order
+    counts = np.bincount(mol, minlength=nm)
+    first = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    rank = np.empty(mol.shape[0], np.int64)
+    rank[order] = np.arange(mol.shape[0]) - first[mol[order]]
+    center = np.zeros((nm, 3))
+    comp = np.zeros((nm, 3))
+    total = np.zeros(nm)
+    by_rank = np.argsort(rank, kind="stable")
+    bounds = np.searchsorted(rank[by_rank], np.arange(int(counts.max(initial=0)) + 1))
+    for r in range(len(bounds) - 1):
+        sel = by_rank[bounds[r]:bounds[r + 1]]
+        ids = mol[sel]
+        x = pos[sel] * m[sel, None]
+        if r == 0:
+            center[ids] = x
+            total[ids] = m[sel]
+            continue
+        total[ids] += m[sel]
+        y = x - comp[ids]
+        t = center[ids] + y
+        comp[ids] = (t - center[ids]) - y
+        center[ids] = t
+    with np.errstate(invalid="ignore", divide="ignore"):
+        out = center / total[:, None]
+    out[counts == 0] = 0.0
+    return out
+
+
 def evaluate_group(topo: Topology, forces, positions, force_accum, energies: ScalarStructure):
     """ForceGroup::evaluateSystemForces (forces/ForceGroup.cpp:43-96) for GPU
     forces: one host->device copy, all forces, one device->host copy."""
@@ -238,14 +291,19 @@ def evaluate_group(topo: Topology, forces, positions, force_accum, energies: Sca
     if pos.shape != (topo.n_atoms, 3) or force_accum.shape != (topo.n_atoms, 3):
         raise ValueError("positions / forces must have shape (N, 3)")
     arr = (_VP * len(forces))(*[f.handle for f in forces])
-    e = _lib.Energies()
-    flags = _lib.FLAG_VIRIAL if energies.virial else 0
+    mol = getattr(energies, "molecular_virial", False)
+    e = _lib.EnergiesMol() if mol else _lib.Energies()
+    flags = (_lib.FLAG_VIRIAL if energies.virial else 0) | (_lib.FLAG_MOLECULAR_VIRIAL if mol else 0)
     check(lib.pmgpu_evaluate(topo.handle, len(forces), arr, pos.ctypes.data_as(_VP),
                              force_accum.ctypes.data_as(_VP), C.byref(e), flags), topo.handle)
     energies.lennard_jones += e.lennard_jones
     energies.coulomb += e.coulomb
-    if energies.virial:
+    # with the molecular virial alone, the atomic slots still receive the
+    # pairs of different molecules (ScalarStructure::addVirial(f, d, comDiff))
+    if energies.virial or mol:
         energies.virial_tensor += np.array(list(e.virial))
+    if mol:
+        energies.molecular_virial_tensor += np.array(list(e.molecular_virial))
 
 
 def adjoint(topo: Topology, forces, positions, v=None):

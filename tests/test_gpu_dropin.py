@@ -20,10 +20,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DRIVER = os.path.join(ROOT, "protomol_b200", "adapter", "_build", "gpu_force_driver")
 
 
-def run_driver(system, defs, precision="mixed", repeat=1):
+def run_driver(system, defs, precision="mixed", repeat=1, molecular_virial=False):
     if not os.path.exists(DRIVER):
         pytest.skip("drop-in driver not built (needs the ProtoMol sources at build time)")
-    env = dict(os.environ, PMGPU_PRECISION=precision)
+    env = dict(os.environ, PMGPU_PRECISION=precision, GPU_DRIVER_MOLVIR="1" if molecular_virial else "0")
     with tempfile.TemporaryDirectory() as td:
         sp, op = os.path.join(td, "s.bin"), os.path.join(td, "o.bin")
         system.save(sp)
@@ -35,8 +35,11 @@ def run_driver(system, defs, precision="mixed", repeat=1):
     hdr = np.frombuffer(raw[:104], np.float64)
     f = np.frombuffer(raw[104:104 + 24 * n], np.float64).reshape(n, 3)
     made = [line[6:] for line in p.stderr.splitlines() if line.startswith("made: ")]
-    return {"lennard_jones": hdr[0], "coulomb": hdr[1], "virial": hdr[2:11], "forces": f,
-            "seconds": hdr[11], "made": made}
+    out = {"lennard_jones": hdr[0], "coulomb": hdr[1], "virial": hdr[2:11], "forces": f,
+           "seconds": hdr[11], "made": made}
+    if molecular_virial:
+        out["mol_virial"] = np.frombuffer(raw[104 + 24 * n:104 + 24 * n + 72], np.float64)
+    return out
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -60,6 +63,21 @@ def test_force_factory_keywords_run_on_the_gpu(case, precision):
     tol_f, tol_e = (1e-9, 1e-10) if precision == "fp64" else (1e-5, 2e-6)
     assert err <= tol_f
     assert abs(r["lennard_jones"] + r["coulomb"] - ref["lennard_jones"] - ref["coulomb"]) <= tol_e * scale
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_molecular_virial_through_the_adapter(precision):
+    """ScalarStructure::molecularVirial() on, the molecule positions set by
+    ProtoMol's buildMolecularCenterOfMass in the driver: the adapter hands
+    them to the GPU and fills the MOLVIRIAL slots."""
+    system = systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+    defs = ["LennardJones -switchingFunction C2 -algorithm NonbondedCutoff -switchon 8 -cutoff 9 -cutoff 9",
+            "Coulomb -algorithm PMEwald -real -reciprocal -correction -interpolation BSpline "
+            "-gridsize 24 24 24 -cutoff 9 -alpha 0.35"]
+    r = run_driver(system, defs, precision, molecular_virial=True)
+    ref = oracle.evaluate(system, [F.parse_definition(d) for d in defs], mol_pos=oracle.molecular_centers(system))
+    d = np.abs(r["mol_virial"] - ref["mol_virial"]).max() / np.abs(ref["mol_virial"]).max()
+    assert d <= (1e-10 if precision == "fp64" else 1e-6)
 
 
 TABLE_DEFS = [

@@ -73,3 +73,45 @@ def test_charged_system_pme_against_reference():
     n = systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
     c = oracle.evaluate(n, specs)
     assert c["coulomb"] != a["coulomb"]
+
+
+# ---- molecular virial (ScalarStructure::molecularVirial) ----------------------
+PME_CHAIN = ("Coulomb -algorithm PMEwald -real -reciprocal -correction -interpolation BSpline "
+             "-gridsize 24 24 24 -cutoff 9 -alpha 0.35")
+LJ_C2 = "LennardJones -algorithm NonbondedCutoff -switchingFunction C2 -switchon 8 -cutoff 9"
+
+
+def molvir_cases():
+    water = systems.perturbed(systems.water_box_216(), 0.3, 1)
+    chain = systems.chain_in_water(n_chain=60, n_water=400, length=24.0, seed=11)
+    small = systems.water_box(100, seed=7)          # edge < 2 x 9 A: realTerm's lattice images
+    return {
+        "water216_cutoff": (water, workloads.water216().forces),
+        "chain_pme_lj": (chain, [PME_CHAIN, LJ_C2]),
+        "lattice_pme": (small, [PME_CHAIN.replace("-gridsize 24 24 24", "-gridsize 16 16 16")]),
+        "chain_coulomb_c1": (chain, ["Coulomb -algorithm NonbondedCutoff -switchingFunction C1 -cutoff 9"]),
+    }
+
+
+@pytest.mark.parametrize("virial", [True, False])
+@pytest.mark.parametrize("case", ["water216_cutoff", "chain_pme_lj", "lattice_pme", "chain_coulomb_c1"])
+def test_molecular_virial_against_reference(case, virial):
+    """The reference with molecularVirial() on and its molecule positions
+    from buildMolecularCenterOfMass: the oracle's centres bit for bit, its
+    molecular and atomic virial to the FFT's rounding.  With virial() off the
+    atomic slots hold only the pairs of different molecules and the
+    reciprocal tensor is missing from the molecular virial (Grid.h:341-387)."""
+    s, defs = molvir_cases()[case]
+    specs = [F.parse_definition(d) for d in defs]
+    b = oracle.run_reference(s, specs, molecular_virial=True, virial=virial)
+    com = oracle.molecular_centers(s)
+    assert np.array_equal(com, b["mol_pos"])
+    assert np.array_equal(F.molecular_centers(s.molecule, s.positions), com)
+    a = oracle.evaluate(s, specs, mol_pos=com, virial=virial)
+    pme = any(sp["kind"] == "pme" for sp in specs)
+    tol = 1e-12 if pme else 0.0
+    assert np.abs(a["mol_virial"] - b["mol_virial"]).max() <= tol * np.abs(b["mol_virial"]).max()
+    assert np.abs(a["virial"] - b["virial"]).max() <= tol * np.abs(b["virial"]).max()
+    assert np.abs(b["mol_virial"]).max() > 0.0
+    rms = np.sqrt((b["forces"] ** 2).sum(1).mean())
+    assert np.abs(a["forces"] - b["forces"]).max() <= (1e-12 if pme else 0.0) * rms
