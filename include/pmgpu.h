@@ -281,9 +281,15 @@ int pmgpu_last_error(pmgpu_system* sys, char* buf, int len);
  *               {A, B, A14, B14}; each pair's derivative is split evenly
  *               between (t_i, t_j) and (t_j, t_i), so the gradient w.r.t. a
  *               symmetric entry t != t' is G[t][t'] + G[t'][t];
- *   hv      N*3: (H v), the Hessian of the pair energy applied to v (the
- *               negative force Jacobian-vector product); PMGPU_ERR_UNSUPPORTED
- *               when a PME reciprocal or correction term is in the list;
+ *   hv      N*3: (H v), the Hessian of the energy applied to v (the
+ *               negative force Jacobian-vector product): the pair terms, the
+ *               PME reciprocal term (the charges' derivative along v spread
+ *               on a second grid, the same convolution, then a gather of the
+ *               B-splines' second derivatives on the potential and of their
+ *               gradient on the convolved derivative) and the correction
+ *               term's excluded-pair blocks (NonbondedPMEwaldSystemForce.h:
+ *               942-981); PMEwald -real with lattice images is refused
+ *               (PMGPU_ERR_UNSUPPORTED);
  *   energies 2: the pair terms' LJ and Coulomb energies (a check).
  * Any output may be NULL.  Table potentials differentiate their cubic
  * interpolant (exact inside an interval; C1 across intervals). */

@@ -289,6 +289,11 @@ struct AdjArgs {
     int virial;
 };
 int launch_pair_adjoint(const AdjArgs& a, int fp64, cudaStream_t s, long long* launches);
+// the same backward pass for a cutoff force over the cell list (the cell
+// pairs and pair set of launch_pair_fp64; p holds the cell-sorted order):
+// dq, dlj, hv and energy of a (facc, hess and erec are not written)
+int launch_pair_adjoint_cells(const PairArgs& p, const AdjArgs& a, int fp64, int blocks, cudaStream_t s,
+                              long long* launches);
 // records (blocks) of one launch_pair_adjoint
 int adjoint_blocks(int n);
 
@@ -333,11 +338,19 @@ struct PmeArgs {
     Pbc pbc;
     double* mrec;
     int mrec_stride;
+    // Hessian-vector product (kStageSpreadDir, kStageHvpGather): the
+    // displacement v (3N, atom order), the output H v (3N, +=) and the
+    // convolved grid of the directional-derivative charges
+    const double* dir;
+    double* hv;
+    const void* rgrid_d;
 };
 constexpr int kStageSpread = 0, kStageFft = 1, kStageGather = 2;
 constexpr int kStagePotential = 3;   // dE/dq~ = phi at the atoms, into (double*)facc
 constexpr int kStageEnergy64 = 4;    // mixed: the FP64 energy transform alone (energy64_apart)
 constexpr int kStageMolvir = 5;      // the reciprocal forces' molecular virial (after the gather)
+constexpr int kStageSpreadDir = 6;   // H v: the charges' derivative along v spread into qgrid
+constexpr int kStageHvpGather = 7;   // H v: second-derivative gather on rgrid plus gradient gather on rgrid_d
 // molecular virial records one kStageMolvir launch writes
 int pme_molvir_blocks(int n);
 // One stage of the reciprocal term: K3 spread, the five FFT passes with the
@@ -396,6 +409,8 @@ int launch_pme_real_lattice(const RealLatArgs& a, cudaStream_t s, long long* lau
 // the lattice real space's molecular virial records (kMRec), no forces
 int launch_pme_real_lattice_molvir(const RealLatArgs& a, cudaStream_t s, long long* launches, int* blocks_used);
 int launch_pme_correction_adjoint(const CorrArgs& a, double* dq, cudaStream_t s, long long* launches);
+// H v of the correction term's excluded pairs (3N, atom order, +=)
+int launch_pme_correction_hvp(const CorrArgs& a, const double* v, double* hv, cudaStream_t s, long long* launches);
 
 // ---------------------------------------------------------------- finalize
 // forces of the three fixed-point accumulators (any may be null) added into

@@ -41,6 +41,8 @@
 #include "pm_kernels.h"
 #include "../../include/pmgpu.h"
 
+#include "pm_adjoint_math.cuh"
+
 namespace pm {
 
 // ------------------------------------------------------------------ combos
@@ -570,6 +572,145 @@ __global__ void __launch_bounds__(128) k_pair_molvir(PairArgs p)
         }
     }
     block_reduce_store_n<4, kMRec>(acc, p.mrec, p.mrec_stride, blockIdx.x);
+}
+
+// K10 over the cell list: the backward pass of a cutoff force's pair terms
+// (pm_adjoint.cu's per-pair math) over the forward kernels' cell pairs, each
+// unordered pair once (the pair set of k_pair_fp64, exact FP64 minimal image
+// and cutoff decision).  Per pair: dE/dq~ to both atoms, dE/dA, dE/dB split
+// between (t_i, t_j) and (t_j, t_i), (H v)_i += c and (H v)_j -= c with
+// c = F u + 2 F' (d.u) d, u = v_j - v_i, and the energies.  i outputs in
+// registers, j outputs in shared memory per chunk; both added to the
+// atom-order outputs with FP64 atomics.
+constexpr int kAdjSmemTypes = 32;
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_pair_adjoint_cells(PairArgs p, AdjArgs aa)
+{
+    __shared__ double4 sjp[4][32];
+    __shared__ int4 sjm[4][32];
+    __shared__ double sjv[4][32][3];
+    __shared__ double sjdq[4][32];
+    __shared__ double sjhv[4][32][3];
+    __shared__ double s_lj[kAdjSmemTypes * kAdjSmemTypes * 4];
+    const bool lj_smem = aa.dlj && aa.n_types <= kAdjSmemTypes;
+    if (lj_smem)
+        for (int k = threadIdx.x; k < aa.n_types * aa.n_types * 4; k += blockDim.x) s_lj[k] = 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int warps_total = gridDim.x * 4;
+    const int n_items = p.grid.ncell * (p.nd + 1);
+    double el = 0.0, ec = 0.0;
+    for (int item = blockIdx.x * 4 + w; item < n_items; item += warps_total) {
+        ItemGeom g = decode_item(p, item);
+        if (!g.valid) continue;
+        int sa = p.start[g.a], ea = p.start[g.a + 1];
+        int sb = p.start[g.b], eb = p.start[g.b + 1];
+        if (sa == ea || sb == eb) continue;
+        for (int ia = sa; ia < ea; ia += 32) {
+            int i = ia + lane;
+            bool vi = i < ea;
+            double4 pi = vi ? p.spos64[i] : make_double4(0, 0, 0, 0);
+            int4 mi = vi ? p.smeta[i] : make_int4(-1, 0, -2, 0);
+            double vix = 0.0, viy = 0.0, viz = 0.0;
+            if (vi && aa.v) {
+                vix = aa.v[3 * (size_t)mi.x]; viy = aa.v[3 * (size_t)mi.x + 1]; viz = aa.v[3 * (size_t)mi.x + 2];
+            }
+            double dqi = 0.0, hix = 0.0, hiy = 0.0, hiz = 0.0;
+            for (int jb = g.same ? ia : sb; jb < eb; jb += 32) {
+                int j = jb + lane;
+                bool vj = j < eb;
+                sjp[w][lane] = vj ? p.spos64[j] : make_double4(0, 0, 0, 0);
+                int4 mj4 = vj ? p.smeta[j] : make_int4(-1, 0, -3, 0);
+                sjm[w][lane] = mj4;
+                for (int c = 0; c < 3; ++c) {
+                    sjv[w][lane][c] = (vj && aa.v) ? aa.v[3 * (size_t)mj4.x + c] : 0.0;
+                    sjhv[w][lane][c] = 0.0;
+                }
+                sjdq[w][lane] = 0.0;
+                __syncwarp();
+                int nj = min(32, eb - jb);
+                bool diag = g.same && jb == ia;
+                for (int t = 0; t < 32; ++t) {
+                    int jl = (lane + t) & 31;
+                    bool ok = vi && jl < nj && (!diag || jb + jl > i);
+                    if (!ok) continue;
+                    double4 pj = sjp[w][jl];
+                    double dx, dy, dz;
+                    double a = pbc_min_diff(p.pbc, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+                    if (aa.use_cut && a > aa.cut2d) continue;
+                    int4 mj = sjm[w][jl];
+                    int excl = PMGPU_EXCL_NONE;
+                    if (mi.z == mj.z) {
+                        excl = excl_class(p, mi.x, mj.x);
+                        if (excl == PMGPU_EXCL_FULL) continue;
+                    }
+                    const double4 par = aa.ljd[(size_t)mi.y * aa.n_types + mj.y];
+                    R F, F1, pqq, pA, pB;
+                    adj_pair<R>(aa, a, pi.w, pj.w, par, excl, 1.0, F, F1, pqq, pA, pB, el, ec);
+                    dqi += (double)pqq * pj.w;
+                    sjdq[w][jl] += (double)pqq * pi.w;
+                    if (aa.v) {
+                        const double ux = sjv[w][jl][0] - vix, uy = sjv[w][jl][1] - viy, uz = sjv[w][jl][2] - viz;
+                        const double du = dx * ux + dy * uy + dz * uz;
+                        const double fF = (double)F, t2 = 2.0 * (double)F1 * du;
+                        const double cx = fF * ux + t2 * dx, cy = fF * uy + t2 * dy, cz = fF * uz + t2 * dz;
+                        hix += cx; hiy += cy; hiz += cz;
+                        sjhv[w][jl][0] -= cx; sjhv[w][jl][1] -= cy; sjhv[w][jl][2] -= cz;
+                    }
+                    if (aa.dlj && (pA != 0 || pB != 0)) {
+                        const int mo = excl == PMGPU_EXCL_MODIFIED ? 2 : 0;
+                        const size_t k1 = ((size_t)mi.y * aa.n_types + mj.y) * 4 + mo;
+                        const size_t k2 = ((size_t)mj.y * aa.n_types + mi.y) * 4 + mo;
+                        double* tab = lj_smem ? s_lj : aa.dlj;
+                        atomicAdd(tab + k1, 0.5 * (double)pA); atomicAdd(tab + k1 + 1, 0.5 * (double)pB);
+                        atomicAdd(tab + k2, 0.5 * (double)pA); atomicAdd(tab + k2 + 1, 0.5 * (double)pB);
+                    }
+                }
+                __syncwarp();
+                if (vj) {
+                    const int oj = mj4.x;
+                    if (aa.dq && sjdq[w][lane] != 0.0) atomicAdd(aa.dq + oj, sjdq[w][lane]);
+                    if (aa.hv)
+                        for (int c = 0; c < 3; ++c)
+                            if (sjhv[w][lane][c] != 0.0) atomicAdd(aa.hv + 3 * (size_t)oj + c, sjhv[w][lane][c]);
+                }
+                __syncwarp();
+            }
+            if (vi) {
+                if (aa.dq && dqi != 0.0) atomicAdd(aa.dq + mi.x, dqi);
+                if (aa.hv) {
+                    if (hix != 0.0) atomicAdd(aa.hv + 3 * (size_t)mi.x, hix);
+                    if (hiy != 0.0) atomicAdd(aa.hv + 3 * (size_t)mi.x + 1, hiy);
+                    if (hiz != 0.0) atomicAdd(aa.hv + 3 * (size_t)mi.x + 2, hiz);
+                }
+            }
+        }
+    }
+    if (aa.energy) {
+        for (int o = 16; o > 0; o >>= 1) {
+            el += __shfl_xor_sync(0xffffffffu, el, o);
+            ec += __shfl_xor_sync(0xffffffffu, ec, o);
+        }
+        if (lane == 0) {
+            if (el != 0.0) atomicAdd(aa.energy, el);
+            if (ec != 0.0) atomicAdd(aa.energy + 1, ec);
+        }
+    }
+    if (lj_smem) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < aa.n_types * aa.n_types * 4; k += blockDim.x)
+            if (s_lj[k] != 0.0) atomicAdd(aa.dlj + k, s_lj[k]);
+    }
+}
+
+int launch_pair_adjoint_cells(const PairArgs& p, const AdjArgs& a, int fp64, int blocks, cudaStream_t s,
+                              long long* launches)
+{
+    if (fp64) k_pair_adjoint_cells<double><<<blocks, 128, 0, s>>>(p, a);
+    else k_pair_adjoint_cells<float><<<blocks, 128, 0, s>>>(p, a);
+    *launches += 1;
+    return (int)cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- launch

@@ -645,6 +645,118 @@ __global__ void __launch_bounds__(128) k_gather_molvir(PmeArgs a)
 
 int pme_molvir_blocks(int n) { return n > 0 ? (n + 127) / 128 : 0; }
 
+// ---- Hessian-vector product of the reciprocal energy ----------------------
+// E = 1/2 sum_g Q(g) phi(g), phi = G * Q (the convolution of the FFT stage),
+// Q(g) = sum_i q~_i W_i(g), W_i the B-spline weights of atom i.  With
+// dQ(g) = sum_j q~_j grad W_j(g) . v_j and dphi = G * dQ:
+//   (H v)_i = q~_i sum_g [(grad grad W_i(g)) v_i] phi(g) + q~_i sum_g grad W_i(g) dphi(g).
+// The second derivatives of the B-spline along each axis come from the
+// order P - 2 spline (M_P'' = M_{P-2}(u) - 2 M_{P-2}(u - 1) + M_{P-2}(u - 2)).
+template <typename R>
+__device__ __forceinline__ void bspline_second(R w, R (&d2)[kMaxOrder], int order)
+{
+    // u[2 + j] holds the order P - 2 spline value t[j]; two zero pads below
+    // and zeros above make d2[j] = t[j - 2] - 2 t[j - 1] + t[j] a plain stencil
+    R u[kMaxOrder + 2];
+#pragma unroll
+    for (int j = 0; j < kMaxOrder + 2; ++j) u[j] = (R)0;
+    u[2] = (R)1;
+    // raise the order-1 spline to order P - 2 (the recurrence of bspline4)
+    for (int k = 1; k < order - 2; k++) {
+        const R div = (R)1 / (R)k;
+        u[2 + k] = div * w * u[2 + k - 1];
+        for (int j = 1; j < k; j++)
+            u[2 + k - j] = div * ((w + (R)j) * u[2 + k - j - 1] + ((R)(k + 1 - j) - w) * u[2 + k - j]);
+        u[2] = div * ((R)1 - w) * u[2];
+    }
+#pragma unroll
+    for (int j = 0; j < kMaxOrder; ++j) d2[j] = u[j] - (R)2 * u[j + 1] + u[j + 2];
+}
+
+// dQ: every atom's weights differentiated along its displacement v_j
+template <typename R>
+__global__ void __launch_bounds__(128) k_spread_dir(PmeArgs a)
+{
+    const int atom = blockIdx.x * blockDim.x + threadIdx.x;
+    if (atom >= a.n) return;
+    R tx[kMaxOrder], dtx[kMaxOrder], ty[kMaxOrder], dty[kMaxOrder], tz[kMaxOrder], dtz[kMaxOrder];
+    int i0, j0, k0;
+    grid_point<R>(a, atom, i0, j0, k0, tx, dtx, ty, dty, tz, dtz);
+    const double* v = a.dir + 3 * (size_t)atom;
+    const double qs = a.q[atom] * a.qscale;
+    const R vx = (R)(v[0] * a.hxr), vy = (R)(v[1] * a.hyr), vz = (R)(v[2] * a.hzr);
+    const int P = a.order;
+    for (int i = 0; i < P; i++) {
+        const int i1 = (i + i0) % a.kx;
+        for (int j = 0; j < P; j++) {
+            const int j1 = (j + j0) % a.ky;
+            const R cxy = vx * dtx[i] * ty[j] + vy * tx[i] * dty[j];
+            const R txy = tx[i] * ty[j];
+            const size_t row = ((size_t)i1 * a.ky + j1) * a.kz;
+            for (int k = 0; k < P; k++) {
+                const R w = cxy * tz[k] + vz * txy * dtz[k];
+                const long long qv = __double2ll_rn(qs * (double)w);
+                if (qv) atomicAdd((unsigned long long*)(a.qgrid + row + (k + k0) % a.kz), (unsigned long long)qv);
+            }
+        }
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_gather_hvp(PmeArgs a)
+{
+    const int atom = blockIdx.x * blockDim.x + threadIdx.x;
+    if (atom >= a.n) return;
+    R tx[kMaxOrder], dtx[kMaxOrder], ty[kMaxOrder], dty[kMaxOrder], tz[kMaxOrder], dtz[kMaxOrder];
+    R ddx[kMaxOrder], ddy[kMaxOrder], ddz[kMaxOrder];
+    int i0, j0, k0;
+    grid_point<R>(a, atom, i0, j0, k0, tx, dtx, ty, dty, tz, dtz);
+    {
+        const double x = wrap_grid(a.pos[3 * (size_t)atom] * a.hxr, a.kx);
+        const double y = wrap_grid(a.pos[3 * (size_t)atom + 1] * a.hyr, a.ky);
+        const double z = wrap_grid(a.pos[3 * (size_t)atom + 2] * a.hzr, a.kz);
+        bspline_second<R>((R)(x - (int)x), ddx, a.order);
+        bspline_second<R>((R)(y - (int)y), ddy, a.order);
+        bspline_second<R>((R)(z - (int)z), ddz, a.order);
+    }
+    const R* phi = (const R*)a.rgrid;
+    const R* dphi = (const R*)a.rgrid_d;
+    const double* v = a.dir + 3 * (size_t)atom;
+    const R hx = (R)a.hxr, hy = (R)a.hyr, hz = (R)a.hzr;
+    const R vx = (R)v[0], vy = (R)v[1], vz = (R)v[2];
+    // second-derivative sums S_ab = sum phi d2W/dx_a dx_b / (h_a h_b), gradient sums G_a
+    R sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0, gx = 0, gy = 0, gz = 0;
+    const int P = a.order;
+    for (int i = 0; i < P; i++) {
+        const int i1 = (i + i0) % a.kx;
+        for (int j = 0; j < P; j++) {
+            const int j1 = (j + j0) % a.ky;
+            const size_t row = ((size_t)i1 * a.ky + j1) * a.kz;
+            for (int k = 0; k < P; k++) {
+                const size_t g = row + (k + k0) % a.kz;
+                const R p = phi[g], d = dphi[g];
+                sxx += p * ddx[i] * ty[j] * tz[k];
+                syy += p * tx[i] * ddy[j] * tz[k];
+                szz += p * tx[i] * ty[j] * ddz[k];
+                sxy += p * dtx[i] * dty[j] * tz[k];
+                sxz += p * dtx[i] * ty[j] * dtz[k];
+                syz += p * tx[i] * dty[j] * dtz[k];
+                gx += d * dtx[i] * ty[j] * tz[k];
+                gy += d * tx[i] * dty[j] * tz[k];
+                gz += d * tx[i] * ty[j] * dtz[k];
+            }
+        }
+    }
+    const double q = a.q[atom];
+    const double hxx = (double)(hx * hx * sxx), hyy = (double)(hy * hy * syy), hzz = (double)(hz * hz * szz);
+    const double hxy = (double)(hx * hy * sxy), hxz = (double)(hx * hz * sxz), hyz = (double)(hy * hz * syz);
+    const double ox = q * (hxx * vx + hxy * vy + hxz * vz + (double)(hx * gx));
+    const double oy = q * (hxy * vx + hyy * vy + hyz * vz + (double)(hy * gy));
+    const double oz = q * (hxz * vx + hyz * vy + hzz * vz + (double)(hz * gz));
+    double* o = a.hv + 3 * (size_t)atom;
+    o[0] += ox; o[1] += oy; o[2] += oz;
+}
+
 static int run_energy64(const PmeArgs& a0, cudaStream_t s, long long* launches, int* erec_used);
 
 template <typename R>
@@ -693,6 +805,15 @@ static int run_reciprocal(const PmeArgs& a, cudaStream_t s, long long* launches,
     }
     if (stage == kStageMolvir) {
         if (a.n > 0) { k_gather_molvir<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+        return (int)cudaGetLastError();
+    }
+    if (stage == kStageSpreadDir) {
+        cudaMemsetAsync(a.qgrid, 0, sizeof(long long) * nreal, s);
+        if (a.n > 0) { k_spread_dir<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
+        return (int)cudaGetLastError();
+    }
+    if (stage == kStageHvpGather) {
+        if (a.n > 0) { k_gather_hvp<R><<<nb, 128, 0, s>>>(a); *launches += 1; }
         return (int)cudaGetLastError();
     }
     if (stage == kStagePotential) {   // a.facc holds the double phi[N] output here
@@ -914,6 +1035,55 @@ __global__ void k_pme_correction_adjoint(CorrArgs a, double* dq)
         atomicAdd(dq + pr.x, -e * a.q[pr.y]);
         atomicAdd(dq + pr.y, -e * a.q[pr.x]);
     }
+}
+
+// H v of the correction term: each excluded pair's energy
+// U(r) = -kappa q~_a q~_b erf(alpha r) / r (correctionTerm,
+// NonbondedPMEwaldSystemForce.h:942-981) gives the block
+// K = U''(r) u u^T + U'(r) / r (I - u u^T), u = d / r, d = r_b - r_a, added as
+// (H v)_a += K (v_a - v_b), (H v)_b += K (v_b - v_a)
+__global__ void k_pme_correction_hvp(CorrArgs a, const double* v, double* hv)
+{
+    const double sqpi = 1.7724538509055160273;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.n_excl; k += gridDim.x * blockDim.x) {
+        const int2 pr = a.pairs[k];
+        const double* p1 = a.pos + 3 * (size_t)pr.x;
+        const double* p2 = a.pos + 3 * (size_t)pr.y;
+        double dx, dy, dz;
+        const double r2 = pbc_min_diff(a.pbc, p1[0], p1[1], p1[2], p2[0], p2[1], p2[2], dx, dy, dz);
+        const double kappa = a.cls[k] == PMGPU_EXCL_MODIFIED ? 1 - a.csf : 1.0;
+        const double c = -kappa * a.q[pr.x] * a.q[pr.y];
+        const double r = sqrt(r2), ir = 1.0 / r;
+        const double er = erf(a.alpha * r), ex = exp(-a.alpha2 * r2);
+        const double g = 2.0 * a.alpha / sqpi * ex;          // d erf(alpha r) / dr
+        // f = erf(alpha r) / r, f' and f''
+        const double f1 = g * ir - er * ir * ir;
+        const double f2 = -2.0 * a.alpha2 * r * g * ir - 2.0 * g * ir * ir + 2.0 * er * ir * ir * ir;
+        const double U1 = c * f1, U2 = c * f2;
+        const double ux = dx * ir, uy = dy * ir, uz = dz * ir;
+        const double wx = v[3 * (size_t)pr.x] - v[3 * (size_t)pr.y];
+        const double wy = v[3 * (size_t)pr.x + 1] - v[3 * (size_t)pr.y + 1];
+        const double wz = v[3 * (size_t)pr.x + 2] - v[3 * (size_t)pr.y + 2];
+        const double uw = ux * wx + uy * wy + uz * wz;
+        const double t = U1 * ir;
+        const double kx = (U2 - t) * uw * ux + t * wx;
+        const double ky = (U2 - t) * uw * uy + t * wy;
+        const double kz = (U2 - t) * uw * uz + t * wz;
+        atomicAdd(hv + 3 * (size_t)pr.x, kx); atomicAdd(hv + 3 * (size_t)pr.x + 1, ky);
+        atomicAdd(hv + 3 * (size_t)pr.x + 2, kz);
+        atomicAdd(hv + 3 * (size_t)pr.y, -kx); atomicAdd(hv + 3 * (size_t)pr.y + 1, -ky);
+        atomicAdd(hv + 3 * (size_t)pr.y + 2, -kz);
+    }
+}
+
+int launch_pme_correction_hvp(const CorrArgs& a, const double* v, double* hv, cudaStream_t s, long long* launches)
+{
+    if (a.n_excl <= 0) return 0;
+    int blocks = (a.n_excl + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_pme_correction_hvp<<<blocks, 256, 0, s>>>(a, v, hv);
+    *launches += 1;
+    return (int)cudaGetLastError();
 }
 
 int launch_pme_correction_adjoint(const CorrArgs& a, double* dq, cudaStream_t s, long long* launches)

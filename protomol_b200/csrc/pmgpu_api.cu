@@ -251,6 +251,11 @@ struct pmgpu_force {
     void* d_cgrid = nullptr;
     void* d_rgrid = nullptr;
     void* d_tw = nullptr;
+    // Hessian-vector product: the grids of the directional-derivative charges
+    // (allocated by the first pmgpu_adjoint with v)
+    long long* d_hq = nullptr;
+    void* d_hc = nullptr;
+    void* d_hr = nullptr;
     void* d_cgrid64 = nullptr;      // mixed: FP64 half spectrum and twiddles of the energy transform
     void* d_tw64 = nullptr;
     double* d_bfac = nullptr;
@@ -1376,6 +1381,9 @@ static void free_force(pmgpu_force* f)
     if (f->d_tw) cudaFree(f->d_tw);
     if (f->d_cgrid64) cudaFree(f->d_cgrid64);
     if (f->d_tw64) cudaFree(f->d_tw64);
+    dfree(f->d_hq);
+    if (f->d_hc) cudaFree(f->d_hc);
+    if (f->d_hr) cudaFree(f->d_hr);
     dfree(f->d_bfac); dfree(f->d_efac);
     for (int k = 0; k < 2; ++k) { dfree(f->d_tab64[k]); dfree(f->d_tab32[k]); }
     delete f;
@@ -2940,12 +2948,24 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
         fl.push_back(forces_in[k]);
     }
     if (hv && !v) return fail(sys, PMGPU_ERR_ARG, "Hessian-vector product needs v");
-    for (pmgpu_force* f : fl)
-        if (hv && f->kind == 1 && (f->pp.reciprocal || f->pp.correction))
-            return fail(sys, PMGPU_ERR_UNSUPPORTED, "Hessian-vector product of the PME reciprocal / correction "
-                                                    "terms is not available (the real-space pairs are)");
     int r = eval_prepare(sys, (int)fl.size(), fl.data(), 0);
     if (r) return r;
+    if (hv)
+        for (pmgpu_force* f : fl) {
+            if (f->kind != 1 || !f->pp.reciprocal || f->d_hq) continue;
+            // the second set of grids of the reciprocal H v (dQ, its spectrum, dphi)
+            const size_t nreal = (size_t)f->pp.grid[0] * f->pp.grid[1] * f->pp.grid[2];
+            const size_t nhalf = (size_t)f->pp.grid[0] * f->pp.grid[1] * f->kzh;
+            const bool f64 = f->precision == PMGPU_PRECISION_FP64;
+            CK(dalloc(&f->d_hq, nreal), "alloc");
+            if (f64) {
+                CK(dalloc((double2**)&f->d_hc, nhalf), "alloc");
+                CK(dalloc((double**)&f->d_hr, nreal), "alloc");
+            } else {
+                CK(dalloc((float2**)&f->d_hc, nhalf), "alloc");
+                CK(dalloc((float**)&f->d_hr, nreal), "alloc");
+            }
+        }
     const int n = sys->n, T = sys->t;
     cudaStream_t s = sys->stream;
     size_t n3 = 3 * (size_t)n;
@@ -2967,6 +2987,14 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
         }
     }
     if (e != cudaSuccess) { cleanup(); return cuda_fail(sys, e, "adjoint setup"); }
+    // cutoff forces run over the cell list of the positions (the forward
+    // kernels' cell-sorted order)
+    bool any_cut = false;
+    for (pmgpu_force* f : fl) any_cut |= f->kind == 0;
+    if (any_cut) {
+        r = bin(sys, sys->d_pos);
+        if (r) { cleanup(); return r; }
+    }
     std::vector<double> host_dq(n, 0.0);
     for (pmgpu_force* f : fl) {
         const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
@@ -2974,7 +3002,14 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
             AdjArgs a;
             adj_pair_args(sys, f, a);
             a.v = d_v; a.dq = d_dq; a.dlj = d_lj; a.hv = d_hv; a.energy = d_e;
-            ok((cudaError_t)launch_pair_adjoint(a, fp64 ? 1 : 0, s, &sys->launches));
+            if (f->kind == 0) {
+                PairArgs pa;
+                fill_pair_args(sys, f, sys->d_pos, pa);
+                ok((cudaError_t)launch_pair_adjoint_cells(pa, a, fp64 ? 1 : 0, pair_blocks(sys->grid, f->nd), s,
+                                                          &sys->launches));
+            } else {
+                ok((cudaError_t)launch_pair_adjoint(a, fp64 ? 1 : 0, s, &sys->launches));
+            }
         } else {
             const pmgpu_pme_params& p = f->pp;
             if (p.reciprocal) {
@@ -2988,6 +3023,22 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
                     ok((cudaError_t)launch_pme_reciprocal(a, fp64 ? 1 : 0, s, &sys->launches, sys->d_erec, &u,
                                                           stages[st]));
                 }
+                if (hv && e == cudaSuccess) {
+                    // dQ along v, its convolution dphi, then the two gathers (rgrid holds phi)
+                    PmeArgs b = a;
+                    b.qgrid = f->d_hq; b.cgrid = f->d_hc; b.rgrid = f->d_hr; b.dir = d_v;
+                    const int hstages[2] = {kStageSpreadDir, kStageFft};
+                    for (int st = 0; st < 2 && e == cudaSuccess; ++st) {
+                        int u = 0;
+                        ok((cudaError_t)launch_pme_reciprocal(b, fp64 ? 1 : 0, s, &sys->launches, sys->d_erec, &u,
+                                                              hstages[st]));
+                    }
+                    PmeArgs c = a;
+                    c.rgrid_d = f->d_hr; c.dir = d_v; c.hv = d_hv;
+                    int u = 0;
+                    ok((cudaError_t)launch_pme_reciprocal(c, fp64 ? 1 : 0, s, &sys->launches, sys->d_erec, &u,
+                                                          kStageHvpGather));
+                }
             }
             if (p.correction) {
                 CorrArgs c;
@@ -2995,6 +3046,7 @@ extern "C" int pmgpu_adjoint(pmgpu_system* sys, int n_forces, pmgpu_force* const
                 c.n_excl = sys->e; c.pairs = sys->d_epairs; c.cls = sys->d_ecls; c.pos = sys->d_pos; c.q = sys->d_q;
                 c.pbc = sys->pbc; c.alpha = f->alpha; c.alpha2 = f->alpha * f->alpha; c.csf = sys->csf;
                 ok((cudaError_t)launch_pme_correction_adjoint(c, d_dq, s, &sys->launches));
+                if (hv) ok((cudaError_t)launch_pme_correction_hvp(c, d_v, d_hv, s, &sys->launches));
                 // point self energy -alpha/sqrt(pi) sum q~^2 and the charged-system term
                 // -pi/(2 V alpha^2) (sum q~)^2 (initialize, :604-628), differentiated
                 double q1 = 0.0;

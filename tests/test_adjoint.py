@@ -137,9 +137,39 @@ def test_backward_energies_are_the_forward_pair_energies():
     assert abs(b["lennard_jones"] + b["coulomb"] - e_fwd) <= 1e-10 * abs(e_fwd)
 
 
-def test_hessian_vector_product_of_pme_is_refused():
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-6), ("mixed", 1e-4)])
+def test_hessian_vector_product_of_pme_matches_oracle_force_differences(precision, tol):
+    """The reciprocal and correction terms (smooth: no cutoff) against
+    central differences of the oracle's FP64 PME forces, h = 1e-4 A."""
+    from oracle import oracle
     s = small()
-    from protomol_b200 import _lib
-    with pytest.raises(_lib.PmgpuError) as ei:
-        backward(s, [CUT_EWALD, PME], v=np.ones((s.n_atoms, 3)))
-    assert ei.value.code == 5
+    rng = np.random.default_rng(17)
+    v = rng.normal(size=(s.n_atoms, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    hv = backward(s, [PME], precision, v=v)["hv"]
+    h = 1e-4
+    spec = [F.parse_definition(PME)]
+    fp = oracle.evaluate(s, spec, positions=s.positions + h * v)["forces"]
+    fm = oracle.evaluate(s, spec, positions=s.positions - h * v)["forces"]
+    fd = -(fp - fm) / (2 * h)
+    err = np.sqrt(((hv - fd) ** 2).sum() / (fd ** 2).sum())
+    print(f"\nPME H v ({precision}) against oracle differences: {err:.2e}")
+    assert err <= tol, err
+
+
+def test_hessian_vector_product_of_split_pme_matches_force_differences():
+    """Ewald real space as a cutoff force plus PME reciprocal + correction,
+    FP64, against central differences of the GPU forces."""
+    s = small()
+    rng = np.random.default_rng(23)
+    v = rng.normal(size=(s.n_atoms, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    defs = [CUT_EWALD, PME]
+    hv = backward(s, defs, v=v)["hv"]
+    h = 1e-4
+    _, fp = forward(s, defs, positions=s.positions + h * v)
+    _, fm = forward(s, defs, positions=s.positions - h * v)
+    fd = -(fp - fm) / (2 * h)
+    keep = ~near_cutoff_atoms(s, 9.0, 1e-3)
+    err = np.sqrt(((hv - fd)[keep] ** 2).sum() / (fd[keep] ** 2).sum())
+    assert err <= 1e-4, err
