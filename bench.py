@@ -357,6 +357,7 @@ def main():
             extra["scale_1m"] = measure_1m(local, torch, 10)
             extra["leapfrog"] = measure_leapfrog(local, torch)
             extra["table_potentials"] = measure_table(local, torch, flush, 200)
+            extra["adjoint"] = measure_adjoint(local, s, w.forces)
     if rank == 0:
         value = world * 1000.0 / t_local
         line = {
@@ -475,7 +476,41 @@ def measure_batched(local, rank, world, pg, torch, flush, steps):
         t_batch, t_seq = float(t[0]), float(t[1])
     total_atoms = sum(w.system.n_atoms for w in ws)
     batch.close()
+    # like for like: the largest box of the set (same forces, ~9,000 atoms)
+    # evaluated alone as one system, CUDA events, L2 flushed between steps
+    big = ws[int(np.argmax([w.system.n_atoms for w in ws]))]
+    topo = F.Topology(big.system, device=local)
+    fs = [F.ForceFactory.make(topo, d, "mixed") for d in big.forces]
+    nb = big.system.n_atoms
+    dpos = torch.tensor(big.system.positions, dtype=torch.float64, device=f"cuda:{local}")
+    dfor = torch.zeros((nb, 3), dtype=torch.float64, device=f"cuda:{local}")
+    den = torch.zeros(20, dtype=torch.float64, device=f"cuda:{local}")
+    arr = (VP * len(fs))(*[f.handle for f in fs])
+    sstream = torch.cuda.ExternalStream(topo.stream)
+
+    def single():
+        lib.pmgpu_evaluate_device(topo.handle, len(fs), arr, VP(dpos.data_ptr()), VP(dfor.data_ptr()),
+                                  VP(den.data_ptr()), 1)
+    for _ in range(5):
+        single()
+    lib.pmgpu_synchronize(topo.handle)
+    sev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(sstream):
+        for a, b in sev:
+            flush.zero_()
+            a.record(sstream)
+            single()
+            b.record(sstream)
+    torch.cuda.synchronize()
+    lib.pmgpu_synchronize(topo.handle)
+    t_single = float(np.mean([a.elapsed_time(b) for a, b in sev]))
+    topo.close()
+    single_rate = nb * 1000.0 / t_single
     return {"workload": "96 water boxes of 100-3,000 waters, cutoff 9 (C2 8->9), PME ~1 A grid, mixed",
+            "single_box": {"atoms": nb, "ms_per_step": t_single, "atom_evals_per_s": single_rate,
+                           "what": "the set's largest box with the same forces, evaluated alone"},
+            "per_atom_vs_single_box": (total_atoms * 1000.0 / t_batch) / single_rate,
             "systems": len(ws), "atoms": total_atoms, "sharding": f"{world} rank(s), greedy by atom count",
             "ms_per_step": t_batch, "batch_evals_per_s": 1000.0 / t_batch,
             "atom_evals_per_s": total_atoms * 1000.0 / t_batch,
@@ -483,6 +518,28 @@ def measure_batched(local, rank, world, pg, torch, flush, steps):
             "speedup_vs_one_at_a_time": t_seq / t_batch, "tuning": tuning,
             "timing": "CUDA events on the batch stream (batched, L2 flushed between steps); "
                       "wall clock for one at a time (each box synchronized)"}
+
+
+def measure_adjoint(local, system, defs, repeat=10):
+    """The backward pass (pmgpu_adjoint: dE/dq~, dE/d(LJ table) and the
+    Hessian-vector product H v) on the metric system, FP64 and mixed: wall
+    clock per call through the host API (positions and v copied in, the
+    three gradients copied out), after one warm-up call."""
+    from protomol_b200 import forces as F
+    rng = np.random.default_rng(5)
+    v = rng.normal(size=(system.n_atoms, 3))
+    out = {"workload": "chain14281, the metric forces (cutoff pairs over the cell list, PME reciprocal "
+                       "+ correction)", "outputs": "dE/dq, dE/dLJ, H v", "calls": repeat}
+    for prec in ("fp64", "mixed"):
+        topo = F.Topology(system, device=local)
+        fs = [F.ForceFactory.make(topo, d, prec) for d in defs]
+        F.adjoint(topo, fs, system.positions, v)
+        t0 = time.perf_counter()
+        for _ in range(repeat):
+            F.adjoint(topo, fs, system.positions, v)
+        out[prec] = {"ms_per_call": (time.perf_counter() - t0) * 1000.0 / repeat}
+        topo.close()
+    return out
 
 
 def measure_leapfrog(local, torch, steps=1000):

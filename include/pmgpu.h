@@ -368,7 +368,8 @@ int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, c
 /* ---- integration ---------------------------------------------------------
  * LeapfrogIntegrator::run(n_steps) (integrators/LeapfrogIntegrator.cpp:
  * 107-120; doHalfKickdoDrift :47-68, doKickdoDrift :70-101, doHalfKick
- * StandardIntegrator.cpp:83-96) without modifiers, on device buffers that
+ * StandardIntegrator.cpp:83-96), with the SHAKE and RATTLE modifiers of
+ * pmgpu_set_constraints when they are set, on device buffers that
  * stay in HBM: per step one kick/drift kernel and one evaluation of the
  * forces (the captured graph), with no host round trip.  d_forces must hold
  * the forces at d_positions on entry (the integrator's forces after
@@ -383,6 +384,31 @@ int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, c
 int pmgpu_leapfrog_run(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* d_mass,
                        double* d_positions, double* d_velocities, double* d_forces, double* d_energies,
                        double timestep, int n_steps, unsigned flags);
+
+/* Bond constraints of pmgpu_leapfrog_run: SHAKE after every drift
+ * (ModifierShake, integrators/ModifierShake.cpp:21-99, a post-drift
+ * modifier) and RATTLE after every step (ModifierRattle,
+ * ModifierRattle.cpp:19-80, a post-step modifier), as protomol.cpp:553-577
+ * attaches them for shake / rattle in a .conf; an epsilon <= 0 or a
+ * max_iter <= 0 leaves that modifier out.  atoms: 2 per constraint, with
+ * rest_length, in the order buildRattleShakeBondConstraintList gives them
+ * (topology/topologyutilities.cpp:782-860: every bond, then the H-H pair of
+ * every angle between two light atoms).  Each sweep updates the
+ * constraints in that order within every group of constraints that share
+ * atoms (the reference's sequential sweep); the mean error over all
+ * constraints (ModifierMetaShake / ModifierMetaRattle::calcError) decides
+ * the next sweep.  SHAKE's bond vectors start as the positions a run
+ * starts from; RATTLE's virial term enters d_energies with
+ * PMGPU_FLAG_VIRIAL.  One CTA runs the sweeps (sized for molecules of small
+ * systems).  n_constraints = 0 removes them; a pmgpu_set_topology with
+ * another atom count does too.  Masses are the run's d_mass. */
+int pmgpu_set_constraints(pmgpu_system* sys, int n_constraints, const int* atoms, const double* rest_length,
+                          double shake_epsilon, int shake_max_iter, double rattle_epsilon, int rattle_max_iter);
+
+/* Sweeps of SHAKE or RATTLE that stopped at their max_iter since the
+ * constraints were first set (the reference reports each with a warning,
+ * ModifierShake.cpp:85-91).  Synchronizes; -1 on a CUDA error. */
+long long pmgpu_constraint_limit_hits(pmgpu_system* sys);
 
 /* ImpulseIntegrator::run(n_steps) (integrators/ImpulseIntegrator.cpp,
  * MTSIntegrator.cpp, StandardIntegrator.cpp:24-35) over an inner Leapfrog of

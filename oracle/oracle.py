@@ -398,7 +398,32 @@ def run_reference(system, specs, repeat: int = 1, fast: bool = False, timeout=No
 INV_TIMEFACTOR = 0.02045482828087295          # Constant::INV_TIMEFACTOR (base/pmconstants.cpp:49)
 
 
-def leapfrog(system, specs, velocities, timestep, steps, positions=None, forces=None):
+TIMEFACTOR = 48.88821290839616      # Constant::TIMEFACTOR (base/pmconstants.cpp:48)
+
+
+def _shake(c, pos, vel, last, dt):
+    a = np.ascontiguousarray(c["atoms"], np.int32)
+    r = np.ascontiguousarray(c["rest"], np.float64)
+    m = np.ascontiguousarray(c["mass"], np.float64)
+    eps, it = c["shake"]
+    return lib().pmo_shake(len(r), a.ctypes.data_as(C.c_void_p), r.ctypes.data_as(C.c_void_p),
+                           m.ctypes.data_as(C.c_void_p), pos.shape[0], pos.ctypes.data_as(C.c_void_p),
+                           vel.ctypes.data_as(C.c_void_p), last.ctypes.data_as(C.c_void_p), C.c_double(dt),
+                           C.c_double(eps), int(it))
+
+
+def _rattle(c, pos, vel, dt, virial=None):
+    a = np.ascontiguousarray(c["atoms"], np.int32)
+    r = np.ascontiguousarray(c["rest"], np.float64)
+    m = np.ascontiguousarray(c["mass"], np.float64)
+    eps, it = c["rattle"]
+    return lib().pmo_rattle(len(r), a.ctypes.data_as(C.c_void_p), r.ctypes.data_as(C.c_void_p),
+                            m.ctypes.data_as(C.c_void_p), pos.ctypes.data_as(C.c_void_p),
+                            vel.ctypes.data_as(C.c_void_p), C.c_double(dt), C.c_double(eps), int(it),
+                            None if virial is None else virial.ctypes.data_as(C.c_void_p))
+
+
+def leapfrog(system, specs, velocities, timestep, steps, positions=None, forces=None, constraints=None):
     """LeapfrogIntegrator::run(steps) without modifiers
     (integrators/LeapfrogIntegrator.cpp:107-120) on the oracle's forces, in the
     reference's operation order:
@@ -411,24 +436,48 @@ def leapfrog(system, specs, velocities, timestep, steps, positions=None, forces=
 
     numpy multiplies and adds without fusing them, as the reference's build
     without FMA contraction does.  ``forces`` are the forces at the starting
-    positions (evaluated here when not given).  Returns (positions,
-    velocities, forces, result of the last evaluation)."""
+    positions (evaluated here when not given).  ``constraints`` ({"atoms",
+    "rest", "mass", "shake": (eps, max_iter) or None, "rattle": ... or None})
+    adds the SHAKE post-drift and RATTLE post-step modifiers
+    (applications/protomol-app/protomol.cpp:553-577): with RATTLE the later
+    steps are half kick, RATTLE, half kick, drift (:72-83), SHAKE follows
+    every drift, RATTLE the final half kick; its virial then lands in the
+    returned result's "virial" entry.  Returns (positions, velocities,
+    forces, result of the last evaluation)."""
     x = np.array(system.positions if positions is None else positions, np.float64)
     v = np.array(velocities, np.float64)
     m = np.asarray(system.mass, np.float64)[:, None]
     r = None
     f = np.array(forces, np.float64) if forces is not None else evaluate(system, specs, positions=x)["forces"]
     h = timestep * INV_TIMEFACTOR
+    hk = 0.5 * timestep * INV_TIMEFACTOR
+    c = constraints
+    shake = bool(c and c.get("shake"))
+    rattle = bool(c and c.get("rattle"))
+    dt = timestep / TIMEFACTOR
+    last = x.copy() if shake else None
     for step in range(steps):
-        if step == 0:
-            v = v + ((f * h) * 0.5) / m
+        if step > 0 and rattle:
+            v = v + (f * hk) / m
+            _rattle(c, x, v, dt)
+            v = v + (f * hk) / m
+            x = x + v * h
         else:
-            v = v + (f * h) / m
-        x = x + v * h
+            if step == 0:
+                v = v + ((f * h) * 0.5) / m
+            else:
+                v = v + (f * h) / m
+            x = x + v * h
+        if shake:
+            _shake(c, x, v, last, dt)
         r = evaluate(system, specs, positions=x)
         f = r["forces"]
-    hk = 0.5 * timestep * INV_TIMEFACTOR
     v = v + (f * hk) / m
+    if rattle:
+        vir = np.zeros(9)
+        _rattle(c, x, v, dt, vir)
+        if r is not None:
+            r["virial"] = r["virial"] + vir
     return x, v, f, r
 
 

@@ -703,6 +703,99 @@ int pmo_molecular_centers(const pmo_system* s, const double* mass, double* cente
     return nm;
 }
 
+/* ModifierMetaShake::calcError (integrators/ModifierMetaShake.cpp) */
+static double shake_error(int n_cons, const int* atoms, const double* rest, const double* pos)
+{
+    double error = 0;
+    for (int i = 0; i < n_cons; i++) {
+        v3 d = vsub(vload(pos + 3 * atoms[2 * i + 1]), vload(pos + 3 * atoms[2 * i]));
+        double r2 = rest[i] * rest[i];
+        error += fabs(vnorm2(d) - r2) / (2.0 * r2);
+    }
+    return error / n_cons;
+}
+
+int pmo_shake(int n_cons, const int* atoms, const double* rest, const double* mass, int n_atoms,
+              double* pos, double* vel, double* last, double dt, double eps, int max_iter)
+{
+    if (n_cons <= 0) return 0;
+    double error = shake_error(n_cons, atoms, rest, pos);
+    int iter = 0;
+    while (error > eps) {
+        for (int i = 0; i < n_cons; i++) {
+            int a1 = atoms[2 * i], a2 = atoms[2 * i + 1];
+            v3 pab = vsub(vload(pos + 3 * a1), vload(pos + 3 * a2));
+            double pabsq = vnorm2(pab);
+            double rabsq = rest[i] * rest[i];
+            double diffsq = rabsq - pabsq;
+            v3 rab = vsub(vload(last + 3 * a1), vload(last + 3 * a2));
+            double rpab = vdot(rab, pab);
+            double rM1 = 1 / mass[a1];
+            double rM2 = 1 / mass[a2];
+            double gab = diffsq / (2 * (rM1 + rM2) * rpab);
+            v3 dp = vmul(rab, gab);
+            v3 p1 = vadd(vload(pos + 3 * a1), vmul(dp, rM1));
+            v3 p2 = vsub(vload(pos + 3 * a2), vmul(dp, rM2));
+            pos[3 * a1] = p1.x; pos[3 * a1 + 1] = p1.y; pos[3 * a1 + 2] = p1.z;
+            pos[3 * a2] = p2.x; pos[3 * a2 + 1] = p2.y; pos[3 * a2 + 2] = p2.z;
+            dp = vdiv(dp, dt);
+            v3 w1 = vadd(vload(vel + 3 * a1), vmul(dp, rM1));
+            v3 w2 = vsub(vload(vel + 3 * a2), vmul(dp, rM2));
+            vel[3 * a1] = w1.x; vel[3 * a1 + 1] = w1.y; vel[3 * a1 + 2] = w1.z;
+            vel[3 * a2] = w2.x; vel[3 * a2 + 1] = w2.y; vel[3 * a2 + 2] = w2.z;
+        }
+        error = shake_error(n_cons, atoms, rest, pos);
+        iter++;
+        if (iter > max_iter) break;
+    }
+    memcpy(last, pos, sizeof(double) * 3 * (size_t)n_atoms);
+    return iter;
+}
+
+/* ModifierMetaRattle::calcError (integrators/ModifierMetaRattle.cpp) */
+static double rattle_error(int n_cons, const int* atoms, const double* pos, const double* vel)
+{
+    double error = 0;
+    for (int i = 0; i < n_cons; i++) {
+        int a1 = atoms[2 * i], a2 = atoms[2 * i + 1];
+        v3 vab = vsub(vload(vel + 3 * a1), vload(vel + 3 * a2));
+        v3 rab = vsub(vload(pos + 3 * a1), vload(pos + 3 * a2));
+        error += fabs(vdot(rab, vab));
+    }
+    return error / n_cons;
+}
+
+int pmo_rattle(int n_cons, const int* atoms, const double* rest, const double* mass,
+               const double* pos, double* vel, double dt, double eps, int max_iter, double* virial)
+{
+    (void)rest;
+    if (n_cons <= 0) return 0;
+    double error = rattle_error(n_cons, atoms, pos, vel);
+    int iter = 0;
+    while (error > eps) {
+        for (int i = 0; i < n_cons; i++) {
+            int a1 = atoms[2 * i], a2 = atoms[2 * i + 1];
+            double rM1 = 1 / mass[a1];
+            double rM2 = 1 / mass[a2];
+            v3 rab = vsub(vload(pos + 3 * a1), vload(pos + 3 * a2));
+            double rabsq = vnorm2(rab);
+            v3 vab = vsub(vload(vel + 3 * a1), vload(vel + 3 * a2));
+            double rvab = vdot(rab, vab);
+            double gab = -rvab / (dt * (rM1 + rM2) * rabsq);
+            v3 dp = vmul(rab, gab);
+            v3 w1 = vadd(vload(vel + 3 * a1), vmul(vmul(dp, dt), rM1));
+            v3 w2 = vsub(vload(vel + 3 * a2), vmul(vmul(dp, dt), rM2));
+            vel[3 * a1] = w1.x; vel[3 * a1 + 1] = w1.y; vel[3 * a1 + 2] = w1.z;
+            vel[3 * a2] = w2.x; vel[3 * a2 + 1] = w2.y; vel[3 * a2 + 2] = w2.z;
+            if (virial) add_virial(virial, vmul(dp, 2), rab);
+        }
+        error = rattle_error(n_cons, atoms, pos, vel);
+        iter++;
+        if (iter > max_iter) break;
+    }
+    return iter;
+}
+
 int pmo_cell_assign(const pmo_system* s, int* cells, int* dims)
 {
     pbc_t b; pbc_set(&b, s->box);

@@ -96,6 +96,20 @@ typedef struct {
  * = unit masses.  Returns the number of molecules (max molecule id + 1). */
 int pmo_molecular_centers(const pmo_system* s, const double* mass, double* centers);
 
+/* ModifierShake::doExecute (integrators/ModifierShake.cpp:21-99) with
+ * ModifierMetaShake::calcError (ModifierMetaShake.cpp): sweeps over the K
+ * constraints in list order until the mean error is at most eps or max_iter
+ * sweeps are exceeded; pos, vel updated, last (the previous SHAKE's
+ * positions) set to pos at the end.  dt = timestep / TIMEFACTOR.  Returns
+ * the number of sweeps (max_iter + 1 when the limit was hit). */
+int pmo_shake(int n_cons, const int* atoms, const double* rest, const double* mass, int n_atoms,
+              double* pos, double* vel, double* last, double dt, double eps, int max_iter);
+
+/* ModifierRattle::doExecute (integrators/ModifierRattle.cpp:19-80) with
+ * ModifierMetaRattle::calcError; virial (9, +=) or NULL. */
+int pmo_rattle(int n_cons, const int* atoms, const double* rest, const double* mass,
+               const double* pos, double* vel, double dt, double eps, int max_iter, double* virial);
+
 /* Cell of every atom as buildCellLists computes it, and the grid dims.
  * cells: 3N ints. Returns 0. */
 int pmo_cell_assign(const pmo_system* s, int* cells, int* dims);

@@ -32,7 +32,8 @@ EXPORTS = [
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
     "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
     "pmgpu_full_create", "pmgpu_lookup_table", "pmgpu_get_tuning", "pmgpu_set_tuning", "pmgpu_autotune", "pmgpu_batch_autotune",
-    "pmgpu_leapfrog_run", "pmgpu_hessian", "pmgpu_impulse_run",
+    "pmgpu_leapfrog_run", "pmgpu_hessian", "pmgpu_impulse_run", "pmgpu_set_constraints",
+    "pmgpu_constraint_limit_hits",
 ]
 PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
 
@@ -138,6 +139,9 @@ def load():
                                       C.c_double, C.c_int, C.c_int, C.c_uint]
     lib.pmgpu_leapfrog_run.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp, vp, vp, vp, C.c_double, C.c_int,
                                        C.c_uint]
+    lib.pmgpu_set_constraints.argtypes = [vp, C.c_int, vp, vp, C.c_double, C.c_int, C.c_double, C.c_int]
+    lib.pmgpu_constraint_limit_hits.argtypes = [vp]
+    lib.pmgpu_constraint_limit_hits.restype = C.c_longlong
     _lib = lib
     return lib
 

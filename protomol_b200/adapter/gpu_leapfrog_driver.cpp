@@ -9,6 +9,11 @@
 // usage: gpu_leapfrog_driver <system.bin> <dynamics.bin> <out.bin> <steps> <timestep fs> <gpu|cpu> <definition>...
 //   dynamics.bin: N masses, then 3N velocities (doubles, A / fs units of ProtoMol)
 //   out.bin: potential energy, kinetic energy after the run, then 3N positions, 3N velocities
+// LF_CONSTRAINTS=<file> adds the topology's bonds and angles and ProtoMol's
+// SHAKE / RATTLE modifiers as protomol.cpp:553-577 attaches them; the text
+// file holds "n_bonds n_angles shake_eps shake_max_iter rattle_eps
+// rattle_max_iter", then n_bonds lines "a1 a2 rest_length" and n_angles
+// lines "a1 a2 a3 rest_angle_radians".
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -27,6 +32,8 @@ using namespace ProtoMol::Report;
 #include "SystemForce.h"
 #include "Topology.h"
 #include "Vector3DBlock.h"
+#include "Angle.h"
+#include "Bond.h"
 #include "blob_topology.h"
 #include "topologyutilities.h"
 
@@ -88,6 +95,37 @@ int main(int argc, char** argv)
     en.molecularVirial(false);
     en.virial(false);
     LeapfrogIntegrator* lf = new LeapfrogIntegrator(dt, group);
+    const char* cons = getenv("LF_CONSTRAINTS");
+    if (cons && *cons) {
+        FILE* fc = fopen(cons, "r");
+        int nb = 0, na = 0, shake_iter = 0, rattle_iter = 0;
+        double shake_eps = 0.0, rattle_eps = 0.0;
+        if (!fc || fscanf(fc, "%d %d %lf %d %lf %d", &nb, &na, &shake_eps, &shake_iter, &rattle_eps, &rattle_iter) != 6) {
+            fprintf(stderr, "bad constraints file\n");
+            return 2;
+        }
+        for (int k = 0; k < nb; ++k) {
+            int a1, a2;
+            double r;
+            if (fscanf(fc, "%d %d %lf", &a1, &a2, &r) != 3) { fprintf(stderr, "bad bond\n"); return 2; }
+            topo->bonds.push_back(Bond(a1, a2, 0.0, r));
+            topo->atoms[a1].mybonds.push_back((int)topo->bonds.size() - 1);
+            topo->atoms[a2].mybonds.push_back((int)topo->bonds.size() - 1);
+        }
+        for (int k = 0; k < na; ++k) {
+            Angle ang;
+            if (fscanf(fc, "%d %d %d %lf", &ang.atom1, &ang.atom2, &ang.atom3, &ang.restAngle) != 4) {
+                fprintf(stderr, "bad angle\n");
+                return 2;
+            }
+            topo->angles.push_back(ang);
+        }
+        fclose(fc);
+        if (shake_eps > 0.0 && shake_iter > 0)
+            lf->adoptPostDriftOrNextModifier(lf->createShakeModifier(shake_eps, shake_iter));
+        if (rattle_eps > 0.0 && rattle_iter > 0)
+            lf->adoptPostStepModifier(lf->createRattleModifier(rattle_eps, rattle_iter));
+    }
     lf->initialize(topo, &pos, &vel, &en);
     lf->run(steps);
     const double epot = en.potentialEnergy();

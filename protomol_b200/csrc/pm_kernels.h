@@ -461,8 +461,36 @@ int launch_molvir_finish(const MolvirFinish& f, cudaStream_t s, long long* launc
 
 // Leapfrog kick / drift (LeapfrogIntegrator.cpp): the first step's half kick
 // and drift, a middle step's kick and drift, the last half kick
-constexpr int kLeapfrogFirst = 0, kLeapfrogMiddle = 1, kLeapfrogLast = 2;
+// (kLeapfrogLast is also the lone half kick before and after RATTLE; the
+// drift alone follows the second half kick)
+constexpr int kLeapfrogFirst = 0, kLeapfrogMiddle = 1, kLeapfrogLast = 2, kLeapfrogDrift = 3;
 int launch_leapfrog(int n, const double* mass, double* pos, double* vel, const double* force, double h, double hk,
                     int mode, cudaStream_t s, long long* launches);
+
+// Bond constraints of the resident Leapfrog: SHAKE after every drift
+// (ModifierShake, integrators/ModifierShake.cpp:21-99) and RATTLE after every
+// step (ModifierRattle, ModifierRattle.cpp:19-80).  The constraints come
+// grouped in clusters (connected through shared atoms), each cluster's
+// constraints in the caller's list order; one thread sweeps a cluster
+// sequentially, as the reference's Gauss-Seidel sweep treats it, and the
+// mean error over all constraints (ModifierMetaShake::calcError,
+// ModifierMetaRattle::calcError) decides the next sweep.  One CTA.
+struct ConsArgs {
+    int n_cons, n_clusters;
+    const int* cl_start;         // n_clusters + 1
+    const int2* atoms;           // per constraint, cluster order
+    const double* rest;          // rest lengths
+    const double* mass;
+    double* pos;
+    double* vel;
+    const double* last;          // SHAKE: positions after the previous SHAKE
+    double dt;                   // getTimestep() / Constant::TIMEFACTOR
+    double eps;
+    int max_iter;
+    double* virial;              // RATTLE: 9 doubles (+=) or null
+    int* hits;                   // sweeps that ended at max_iter (+1 each)
+};
+int launch_shake(const ConsArgs& a, cudaStream_t s, long long* launches);
+int launch_rattle(const ConsArgs& a, cudaStream_t s, long long* launches);
 
 }  // namespace pm

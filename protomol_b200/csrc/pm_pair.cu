@@ -581,8 +581,35 @@ __global__ void __launch_bounds__(128) k_pair_molvir(PairArgs p)
 // between (t_i, t_j) and (t_j, t_i), (H v)_i += c and (H v)_j -= c with
 // c = F u + 2 F' (d.u) d, u = v_j - v_i, and the energies.  i outputs in
 // registers, j outputs in shared memory per chunk; both added to the
-// atom-order outputs with FP64 atomics.
+// atom-order outputs with FP64 atomics.  The LJ table gradient goes through
+// a small per-thread cache of type-pair sums (a thread's i atom keeps its
+// type, and a few type pairs carry most pairs), flushed to shared or global
+// memory on eviction and at the end: the table's few entries would otherwise
+// take every pair's atomics on the same addresses.
 constexpr int kAdjSmemTypes = 32;
+constexpr int kLjCache = 4;
+
+struct LjCache {
+    long long key[kLjCache];
+    double a[kLjCache], b[kLjCache];
+    int next;
+};
+
+__device__ __forceinline__ void lj_cache_add(LjCache& c, long long key, double pa, double pb, double* tab)
+{
+#pragma unroll
+    for (int s = 0; s < kLjCache; ++s)
+        if (c.key[s] == key) { c.a[s] += pa; c.b[s] += pb; return; }
+    // evict round robin
+    const int v = c.next;
+    c.next = (c.next + 1) % kLjCache;
+#pragma unroll
+    for (int s = 0; s < kLjCache; ++s)
+        if (s == v) {
+            if (c.key[s] >= 0) { atomicAdd(tab + c.key[s], c.a[s]); atomicAdd(tab + c.key[s] + 1, c.b[s]); }
+            c.key[s] = key; c.a[s] = pa; c.b[s] = pb;
+        }
+}
 
 template <typename R>
 __global__ void __launch_bounds__(128) k_pair_adjoint_cells(PairArgs p, AdjArgs aa)
@@ -601,6 +628,11 @@ __global__ void __launch_bounds__(128) k_pair_adjoint_cells(PairArgs p, AdjArgs 
     const int warps_total = gridDim.x * 4;
     const int n_items = p.grid.ncell * (p.nd + 1);
     double el = 0.0, ec = 0.0;
+    double* lj_tab = lj_smem ? s_lj : aa.dlj;
+    LjCache cache;
+#pragma unroll
+    for (int k = 0; k < kLjCache; ++k) { cache.key[k] = -1; cache.a[k] = 0.0; cache.b[k] = 0.0; }
+    cache.next = 0;
     for (int item = blockIdx.x * 4 + w; item < n_items; item += warps_total) {
         ItemGeom g = decode_item(p, item);
         if (!g.valid) continue;
@@ -660,11 +692,10 @@ __global__ void __launch_bounds__(128) k_pair_adjoint_cells(PairArgs p, AdjArgs 
                     }
                     if (aa.dlj && (pA != 0 || pB != 0)) {
                         const int mo = excl == PMGPU_EXCL_MODIFIED ? 2 : 0;
-                        const size_t k1 = ((size_t)mi.y * aa.n_types + mj.y) * 4 + mo;
-                        const size_t k2 = ((size_t)mj.y * aa.n_types + mi.y) * 4 + mo;
-                        double* tab = lj_smem ? s_lj : aa.dlj;
-                        atomicAdd(tab + k1, 0.5 * (double)pA); atomicAdd(tab + k1 + 1, 0.5 * (double)pB);
-                        atomicAdd(tab + k2, 0.5 * (double)pA); atomicAdd(tab + k2 + 1, 0.5 * (double)pB);
+                        const long long k1 = ((long long)mi.y * aa.n_types + mj.y) * 4 + mo;
+                        const long long k2 = ((long long)mj.y * aa.n_types + mi.y) * 4 + mo;
+                        lj_cache_add(cache, k1, 0.5 * (double)pA, 0.5 * (double)pB, lj_tab);
+                        lj_cache_add(cache, k2, 0.5 * (double)pA, 0.5 * (double)pB, lj_tab);
                     }
                 }
                 __syncwarp();
@@ -687,6 +718,12 @@ __global__ void __launch_bounds__(128) k_pair_adjoint_cells(PairArgs p, AdjArgs 
             }
         }
     }
+#pragma unroll
+    for (int k = 0; k < kLjCache; ++k)
+        if (cache.key[k] >= 0) {
+            atomicAdd(lj_tab + cache.key[k], cache.a[k]);
+            atomicAdd(lj_tab + cache.key[k] + 1, cache.b[k]);
+        }
     if (aa.energy) {
         for (int o = 16; o > 0; o >>= 1) {
             el += __shfl_xor_sync(0xffffffffu, el, o);

@@ -87,6 +87,16 @@ struct pmgpu_system {
     bool molpos_set = false;
     double* d_mrec = nullptr;
     int mrec_cap = 0;
+    // bond constraints of the resident Leapfrog (pmgpu_set_constraints):
+    // clusters of constraints sharing atoms, SHAKE's last positions
+    int n_cons = 0, n_ccl = 0;
+    int* d_cl_start = nullptr;
+    int2* d_cons_atoms = nullptr;
+    double* d_cons_rest = nullptr;
+    double* d_cons_last = nullptr;
+    int* d_cons_hits = nullptr;
+    double shake_eps = 0.0, rattle_eps = 0.0;
+    int shake_iter = 0, rattle_iter = 0;
     float4* d_ljn = nullptr;
     float4* d_ljm = nullptr;
     double4* d_ljd = nullptr;
@@ -402,6 +412,8 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     free_atom_buffers(sys);
     free_col_buffers(sys);
     dfree(sys->d_counts); dfree(sys->d_start); dfree(sys->d_erec); dfree(sys->d_mrec);
+    dfree(sys->d_cl_start); dfree(sys->d_cons_atoms); dfree(sys->d_cons_rest); dfree(sys->d_cons_last);
+    dfree(sys->d_cons_hits);
     dfree(sys->d_small); dfree(sys->d_energy);
     dfree(sys->d_cstart); dfree(sys->d_cbox); dfree(sys->d_ccell); dfree(sys->d_plist); dfree(sys->d_chunks);
     dfree(sys->d_near);
@@ -528,6 +540,7 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     sys->topo_version++;
     for (auto& g : sys->graphs) cudaGraphExecDestroy(g.exec);
     sys->graphs.clear();
+    if (n_atoms != sys->n) sys->n_cons = 0;   // constraints name atoms of the previous topology
     sys->n = n_atoms; sys->t = n_types; sys->e = n_excl; sys->csf = coulomb_scaling_factor;
     sys->n_mol = n_mol;
     sys->q.assign(scaled_charge, scaled_charge + n_atoms);
@@ -2842,6 +2855,7 @@ extern "C" int pmgpu_hessian(pmgpu_system* sys, int n_forces, pmgpu_force* const
 
 // ------------------------------------------------------------------ leapfrog
 static const double kInvTimeFactor = 0.02045482828087295;   // Constant::INV_TIMEFACTOR (base/pmconstants.cpp:49)
+static const double kTimeFactor = 48.88821290839616;        // Constant::TIMEFACTOR (base/pmconstants.cpp:48)
 
 extern "C" int pmgpu_leapfrog_run(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* d_mass,
                                   double* d_positions, double* d_velocities, double* d_forces, double* d_energies,
@@ -2859,10 +2873,58 @@ extern "C" int pmgpu_leapfrog_run(pmgpu_system* sys, int n_forces, pmgpu_force* 
     const size_t n3 = 3 * (size_t)sys->n;
     const double h = timestep * kInvTimeFactor;              // getTimestep() * Constant::INV_TIMEFACTOR
     const double hk = 0.5 * timestep * kInvTimeFactor;       // doHalfKick's step
+    // SHAKE as a post-drift modifier, RATTLE as a post-step modifier
+    // (applications/protomol-app/protomol.cpp:553-577)
+    const bool shake = sys->n_cons > 0 && sys->shake_eps > 0.0 && sys->shake_iter > 0;
+    const bool rattle = sys->n_cons > 0 && sys->rattle_eps > 0.0 && sys->rattle_iter > 0;
+    ConsArgs ca;
+    memset(&ca, 0, sizeof(ca));
+    ca.n_cons = sys->n_cons; ca.n_clusters = sys->n_ccl; ca.cl_start = sys->d_cl_start; ca.atoms = sys->d_cons_atoms;
+    ca.rest = sys->d_cons_rest; ca.mass = d_mass; ca.pos = d_positions; ca.vel = d_velocities;
+    ca.last = sys->d_cons_last; ca.dt = timestep / kTimeFactor; ca.hits = sys->d_cons_hits;
+    auto do_shake = [&]() -> int {
+        ConsArgs a = ca;
+        a.eps = sys->shake_eps; a.max_iter = sys->shake_iter;
+        int e = launch_shake(a, s, &sys->launches);
+        if (e) return cuda_fail(sys, (cudaError_t)e, "SHAKE");
+        // ModifierShake stores the positions it leaves for the next sweep's bond vectors
+        CK(cudaMemcpyAsync(sys->d_cons_last, d_positions, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s), "copy");
+        return PMGPU_OK;
+    };
+    auto do_rattle = [&]() -> int {
+        ConsArgs a = ca;
+        a.eps = sys->rattle_eps; a.max_iter = sys->rattle_iter;
+        a.virial = (flags & PMGPU_FLAG_VIRIAL) ? d_energies + 2 : nullptr;
+        int e = launch_rattle(a, s, &sys->launches);
+        return e ? cuda_fail(sys, (cudaError_t)e, "RATTLE") : PMGPU_OK;
+    };
+    // ModifierMetaRattleShake::doInitialize: the last positions start as the positions
+    if (shake)
+        CK(cudaMemcpyAsync(sys->d_cons_last, d_positions, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s), "copy");
     for (int step = 0; step < n_steps; ++step) {
-        int e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_forces, h, h,
-                                step == 0 ? kLeapfrogFirst : kLeapfrogMiddle, s, &sys->launches);
-        if (e) return cuda_fail(sys, (cudaError_t)e, "leapfrog step");
+        if (step > 0 && rattle) {
+            // doKickdoDrift with a post-step modifier: half kick, RATTLE, half
+            // kick, drift (LeapfrogIntegrator.cpp:72-83)
+            int e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_forces, h, hk, kLeapfrogLast, s,
+                                    &sys->launches);
+            if (e) return cuda_fail(sys, (cudaError_t)e, "leapfrog half kick");
+            int r = do_rattle();
+            if (r) return r;
+            e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_forces, h, hk, kLeapfrogLast, s,
+                                &sys->launches);
+            if (e) return cuda_fail(sys, (cudaError_t)e, "leapfrog half kick");
+            e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_forces, h, h, kLeapfrogDrift, s,
+                                &sys->launches);
+            if (e) return cuda_fail(sys, (cudaError_t)e, "leapfrog drift");
+        } else {
+            int e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_forces, h, h,
+                                    step == 0 ? kLeapfrogFirst : kLeapfrogMiddle, s, &sys->launches);
+            if (e) return cuda_fail(sys, (cudaError_t)e, "leapfrog step");
+        }
+        if (shake) {
+            int r = do_shake();
+            if (r) return r;
+        }
         // calculateForces: forces and energies cleared, then evaluated
         CK(cudaMemsetAsync(d_forces, 0, sizeof(double) * n3, s), "memset");
         CK(cudaMemsetAsync(d_energies, 0, sizeof(double) * kERec, s), "memset");
@@ -2872,7 +2934,88 @@ extern "C" int pmgpu_leapfrog_run(pmgpu_system* sys, int n_forces, pmgpu_force* 
     int e = launch_leapfrog(sys->n, d_mass, d_positions, d_velocities, d_forces, h, hk, kLeapfrogLast, s,
                             &sys->launches);
     if (e) return cuda_fail(sys, (cudaError_t)e, "leapfrog half kick");
+    if (rattle) {
+        int r = do_rattle();
+        if (r) return r;
+    }
     return PMGPU_OK;
+}
+
+extern "C" int pmgpu_set_constraints(pmgpu_system* sys, int n_constraints, const int* atoms, const double* rest_length,
+                                     double shake_epsilon, int shake_max_iter, double rattle_epsilon,
+                                     int rattle_max_iter)
+{
+    if (!sys || n_constraints < 0 || (n_constraints > 0 && (!atoms || !rest_length))) return PMGPU_ERR_ARG;
+    const int n = sys->n;
+    for (int k = 0; k < n_constraints; ++k) {
+        const int a = atoms[2 * k], b = atoms[2 * k + 1];
+        if (a < 0 || b < 0 || a >= n || b >= n || a == b) return fail(sys, PMGPU_ERR_ARG, "constraint atom out of range");
+        if (!(rest_length[k] > 0.0)) return fail(sys, PMGPU_ERR_ARG, "constraint rest length must be positive");
+    }
+    cudaSetDevice(sys->device);
+    CK(cudaStreamSynchronize(sys->stream), "set_constraints");
+    // clusters: connected components of the constraint graph, ordered by
+    // their first constraint, each keeping the list order
+    std::vector<int> parent(n);
+    for (int i = 0; i < n; ++i) parent[i] = i;
+    auto find = [&](int x) {
+        while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; }
+        return x;
+    };
+    for (int k = 0; k < n_constraints; ++k) {
+        const int ra = find(atoms[2 * k]), rb = find(atoms[2 * k + 1]);
+        if (ra != rb) parent[std::max(ra, rb)] = std::min(ra, rb);
+    }
+    std::vector<int> cluster_of_root(n, -1), order, start;
+    std::vector<std::vector<int>> members;
+    for (int k = 0; k < n_constraints; ++k) {
+        const int root = find(atoms[2 * k]);
+        if (cluster_of_root[root] < 0) {
+            cluster_of_root[root] = (int)members.size();
+            members.emplace_back();
+        }
+        members[cluster_of_root[root]].push_back(k);
+    }
+    std::vector<int2> ca;
+    std::vector<double> cr;
+    start.push_back(0);
+    for (const auto& m : members) {
+        for (int k : m) {
+            ca.push_back(make_int2(atoms[2 * k], atoms[2 * k + 1]));
+            cr.push_back(rest_length[k]);
+        }
+        start.push_back((int)ca.size());
+    }
+    dfree(sys->d_cl_start); dfree(sys->d_cons_atoms); dfree(sys->d_cons_rest); dfree(sys->d_cons_last);
+    sys->n_cons = 0; sys->n_ccl = 0;
+    if (n_constraints > 0) {
+        CK(dalloc(&sys->d_cl_start, start.size()), "alloc");
+        CK(dalloc(&sys->d_cons_atoms, ca.size()), "alloc");
+        CK(dalloc(&sys->d_cons_rest, cr.size()), "alloc");
+        CK(dalloc(&sys->d_cons_last, 3 * (size_t)n), "alloc");
+        CK(cudaMemcpy(sys->d_cl_start, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice), "copy");
+        CK(cudaMemcpy(sys->d_cons_atoms, ca.data(), sizeof(int2) * ca.size(), cudaMemcpyHostToDevice), "copy");
+        CK(cudaMemcpy(sys->d_cons_rest, cr.data(), sizeof(double) * cr.size(), cudaMemcpyHostToDevice), "copy");
+    }
+    if (!sys->d_cons_hits) {
+        CK(dalloc(&sys->d_cons_hits, 1), "alloc");
+        CK(cudaMemset(sys->d_cons_hits, 0, sizeof(int)), "memset");
+    }
+    sys->n_cons = n_constraints;
+    sys->n_ccl = (int)members.size();
+    sys->shake_eps = shake_epsilon; sys->shake_iter = shake_max_iter;
+    sys->rattle_eps = rattle_epsilon; sys->rattle_iter = rattle_max_iter;
+    return PMGPU_OK;
+}
+
+extern "C" long long pmgpu_constraint_limit_hits(pmgpu_system* sys)
+{
+    if (!sys || !sys->d_cons_hits) return 0;
+    cudaSetDevice(sys->device);
+    if (cudaStreamSynchronize(sys->stream) != cudaSuccess) return -1;
+    int h = 0;
+    if (cudaMemcpy(&h, sys->d_cons_hits, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return h;
 }
 
 extern "C" int pmgpu_impulse_run(pmgpu_system* sys, int n_slow, pmgpu_force* const* slow, int n_fast,

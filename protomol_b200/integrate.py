@@ -36,8 +36,13 @@ def kinetic_energy(masses: np.ndarray, velocities: np.ndarray) -> float:
 
 
 class Leapfrog:
+    """``constraints`` ({"atoms": (K, 2), "rest": (K,), "shake": (epsilon,
+    max_iter) or None, "rattle": (epsilon, max_iter) or None}, the list of
+    systems.rattle_shake_constraints) adds ProtoMol's SHAKE post-drift and
+    RATTLE post-step modifiers (pmgpu_set_constraints)."""
+
     def __init__(self, topo: F.Topology, forces: Sequence[F.SystemForce], positions, velocities, masses,
-                 timestep: float, device: int = 0, virial: bool = False):
+                 timestep: float, device: int = 0, virial: bool = False, constraints=None):
         import torch
         self.topo, self.forces, self.timestep = topo, list(forces), float(timestep)
         self.flags = _lib.FLAG_VIRIAL if virial else 0
@@ -50,6 +55,18 @@ class Leapfrog:
         self.masses = np.asarray(masses, np.float64)
         self._arr = (_VP * len(self.forces))(*[f.handle for f in self.forces])
         self.lib = _lib.load()
+        c = constraints or {}
+        atoms = np.ascontiguousarray(c.get("atoms", np.zeros((0, 2))), np.int32).reshape(-1, 2)
+        rest = np.ascontiguousarray(c.get("rest", np.zeros(0)), np.float64)
+        shake = c.get("shake") or (0.0, 0)
+        rattle = c.get("rattle") or (0.0, 0)
+        F.check(self.lib.pmgpu_set_constraints(self.topo.handle, len(rest), atoms.ctypes.data_as(_VP),
+                                               rest.ctypes.data_as(_VP), float(shake[0]), int(shake[1]),
+                                               float(rattle[0]), int(rattle[1])), self.topo.handle)
+
+    def constraint_limit_hits(self) -> int:
+        """Sweeps that stopped at their max_iter (pmgpu_constraint_limit_hits)."""
+        return int(self.lib.pmgpu_constraint_limit_hits(self.topo.handle))
 
     def initialize(self):
         """initializeForces: the forces (and energies) at the starting positions."""

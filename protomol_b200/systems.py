@@ -478,6 +478,38 @@ def water_box_1m(seed: int = 5) -> System:
                      box_len=length, csf=1.0, cell_size=6.0, scheme="1-3")
 
 
+CHAIN_BOND = 1.53             # the random-walk chains' bond length (A)
+
+
+def rattle_shake_constraints(system: System):
+    """The bond constraints of SHAKE / RATTLE as
+    buildRattleShakeBondConstraintList (topology/topologyutilities.cpp:
+    782-860) builds them: every bond with its rest length (TIP3P O-H 0.9572 A,
+    chain bonds 1.53 A), then for every angle whose two end atoms are light
+    (mass < 5) the end-to-end distance sqrt(b^2 + c^2 - 2 b c cos(theta0))
+    of its two bonds (the water's H-H).  Returns (atoms (K, 2) int32,
+    rest lengths (K,) float64)."""
+    m = np.asarray(system.mass)
+    light = lambda a: m[a] < 5.0
+    rest = {}
+    atoms, lengths = [], []
+    for a, b in system.bonds:
+        r = _OH if (light(a) or light(b)) else CHAIN_BOND
+        rest[(min(a, b), max(a, b))] = r
+        atoms.append((a, b))
+        lengths.append(r)
+    for a1, a2, a3 in system.angles:
+        if not (light(a1) and light(a3)):
+            continue
+        b = rest.get((min(a1, a2), max(a1, a2)))
+        c = rest.get((min(a2, a3), max(a2, a3)))
+        if b is None or c is None:
+            continue
+        atoms.append((a1, a3))
+        lengths.append(math.sqrt(b * b + c * c - 2 * b * c * math.cos(_HOH)))
+    return np.asarray(atoms, np.int32).reshape(-1, 2), np.asarray(lengths, np.float64)
+
+
 def smooth_grid_size(length: float, spacing: float = 1.0) -> int:
     """Smallest 2^a 3^b 5^c >= ceil(length / spacing)."""
     n = max(4, int(math.ceil(length / spacing)))

@@ -5,10 +5,17 @@ seeded 300 K Maxwell-Boltzmann velocities:
 * ten steps of the 648-atom water box of the plain-cutoff configuration
   (LJ + Coulomb, C2 8 -> 9 A, intra-water pairs excluded);
 * one force evaluation plus 1,000 steps of the same box's 216 oxygens as a
-  Lennard-Jones fluid.  The configuration's waters are rigid in the
-  reference, held by the SHAKE/RATTLE modifiers of the integrator; without
-  them (this integrator runs without modifiers) nothing holds a water's
-  hydrogens, so the long runs use the molecule-free fluid."""
+  Lennard-Jones fluid;
+* the configuration as stated: the 216 waters held rigid by ProtoMol's
+  SHAKE (post-drift) and RATTLE (post-step) modifiers, one force evaluation
+  plus 1,000 steps.  The oracle's constrained Leapfrog is pinned bit for
+  bit to ProtoMol's own LeapfrogIntegrator with ModifierShake and
+  ModifierRattle (protomol_b200/adapter's gpu_leapfrog_driver on the
+  reference forces)."""
+import os
+import subprocess
+import tempfile
+
 import numpy as np
 import pytest
 
@@ -16,7 +23,53 @@ from oracle import oracle
 from protomol_b200 import forces as F
 from protomol_b200 import integrate, workloads
 
+from protomol_b200 import systems
+
 DT = 1.0                     # fs
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LEAPFROG = os.path.join(ROOT, "protomol_b200", "adapter", "_build", "gpu_leapfrog_driver")
+# protomol.cpp:137-141 defaults: epsilon 1e-5, 30 sweeps
+RIGID = {"shake": (1e-5, 30), "rattle": (1e-5, 30)}
+
+
+def rigid_constraints(system, shake=(1e-5, 30), rattle=(1e-5, 30)):
+    atoms, rest = systems.rattle_shake_constraints(system)
+    return {"atoms": atoms, "rest": rest, "mass": system.mass, "shake": shake, "rattle": rattle}
+
+
+def reference_constrained_leapfrog(system, defs, v, steps, shake, rattle):
+    """ProtoMol's LeapfrogIntegrator with its SHAKE / RATTLE modifiers on the
+    reference forces (gpu_leapfrog_driver, cpu mode)."""
+    with tempfile.TemporaryDirectory() as td:
+        sp, dp, op, cp = (os.path.join(td, f) for f in ("s.bin", "d.bin", "o.bin", "c.txt"))
+        system.save(sp)
+        np.concatenate([system.mass, v.ravel()]).astype(np.float64).tofile(dp)
+        _, rest = systems.rattle_shake_constraints(system)
+        se, si = shake or (0.0, 0)
+        re_, ri = rattle or (0.0, 0)
+        with open(cp, "w") as fh:
+            fh.write(f"{len(system.bonds)} {len(system.angles)} {float(se)!r} {si} {float(re_)!r} {ri}\n")
+            for (b1, b2), r in zip(system.bonds, rest):
+                fh.write(f"{b1} {b2} {float(r)!r}\n")
+            for a1, a2, a3 in system.angles:
+                fh.write(f"{a1} {a2} {a3} {systems._HOH!r}\n")
+        p = subprocess.run([LEAPFROG, sp, dp, op, str(steps), repr(DT), "cpu", *defs], capture_output=True, text=True,
+                           timeout=600, env=dict(os.environ, LF_CONSTRAINTS=cp))
+        assert p.returncode == 0, p.stderr
+        raw = np.fromfile(op)
+    n = system.n_atoms
+    return raw[2:2 + 3 * n].reshape(n, 3), raw[2 + 3 * n:].reshape(n, 3), raw[0]
+
+
+@pytest.mark.skipif(not os.path.exists(LEAPFROG), reason="the ProtoMol-side driver is not built here")
+@pytest.mark.parametrize("shake,rattle", [((1e-5, 30), None), ((1e-5, 30), (1e-5, 30)), ((1e-8, 100), (1e-8, 100))])
+def test_oracle_constrained_leapfrog_is_the_reference(shake, rattle):
+    w, v = water648()
+    specs = [F.parse_definition(d) for d in w.forces]
+    x, v1, f, r = oracle.leapfrog(w.system, specs, v, DT, 20, constraints=rigid_constraints(w.system, shake, rattle))
+    xr, vr, epot = reference_constrained_leapfrog(w.system, w.forces, v, 20, shake, rattle)
+    assert np.array_equal(x, xr) and np.array_equal(v1, vr)
+    assert epot == r["lennard_jones"] + r["coulomb"]
 
 
 def water648():
@@ -156,3 +209,73 @@ def test_impulse_with_cyclelength_one_is_leapfrog_with_all_forces():
     lf = integrate.Leapfrog(topo, [slow, fast], s.positions, v, s.mass, 1.0).initialize().run(20)
     xl = lf.state()[0]
     assert np.abs(xi - xl).max() <= 1e-9
+
+
+# ---------------------------------------------------------------- rigid water
+def _gpu_rigid(w, v, precision, steps, virial=False):
+    topo = F.Topology(w.system)
+    fs = [F.ForceFactory.make(topo, d, precision) for d in w.forces]
+    lf = integrate.Leapfrog(topo, fs, w.system.positions, v, w.system.mass, DT, virial=virial,
+                            constraints=rigid_constraints(w.system)).initialize()
+    lf.run(steps)
+    return lf.state(), lf.constraint_limit_hits()
+
+
+@pytest.mark.gpu
+def test_rigid_water_ten_steps_match_the_oracle():
+    """SHAKE and RATTLE on the GPU against the oracle (itself the reference's
+    integrator bit for bit), FP64 forces; with the virial, RATTLE's final
+    term included."""
+    w, v = water648()
+    specs = [F.parse_definition(d) for d in w.forces]
+    x, v1, f, r = oracle.leapfrog(w.system, specs, v, DT, 10, constraints=rigid_constraints(w.system))
+    (xg, vg, fg, eg), hits = _gpu_rigid(w, v, "fp64", 10, virial=True)
+    print(f"\nrigid water, 10 steps: |dx| {np.abs(xg - x).max():.2e} A  |dv| {np.abs(vg - v1).max():.2e}")
+    assert hits == 0
+    assert np.abs(xg - x).max() <= 1e-10
+    assert np.abs(vg - v1).max() <= 1e-10 * np.abs(v1).max()
+    assert np.abs(eg.virial_tensor - r["virial"]).max() <= 1e-8 * np.abs(r["virial"]).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_rigid_water_one_evaluation_plus_a_thousand_steps(precision):
+    """The plain-cutoff configuration as stated: 216 rigid TIP3P waters, one
+    evaluation plus 1,000 steps of 1 fs.  The lattice's random orientations
+    heat the box (the kinetic energy grows from ~530 to ~7,800 kcal/mol),
+    after which the total energy creeps up by the 1 fs step's error at that
+    temperature: from step 100 to step 1,000 the oracle's runs gain +38 to
+    +81 kcal/mol (0.5-1% of the kinetic energy) depending on the realization
+    (velocities scaled by 1 + k 1e-12 separate after ~300 steps).  Over four
+    such realizations the GPU's mean gain stays below 2% of the kinetic
+    energy, the bonds stay at their rest lengths within SHAKE's tolerance,
+    and the unscaled FP64 run follows the oracle's over the first 100 steps."""
+    w, v = water648()
+    specs = [F.parse_definition(d) for d in w.forces]
+    c = rigid_constraints(w.system)
+    m = w.system.mass
+    E = lambda e, vel: e.lennard_jones + e.coulomb + integrate.kinetic_energy(m, vel)
+    gains, kes, worst_bond = [], [], 0.0
+    for k in range(4):
+        topo = F.Topology(w.system)
+        fs = [F.ForceFactory.make(topo, d, precision) for d in w.forces]
+        lf = integrate.Leapfrog(topo, fs, w.system.positions, v * (1 + k * 1e-12), m, DT, constraints=c).initialize()
+        lf.run(100)
+        x100, v100, _, e100 = lf.state()
+        if k == 0 and precision == "fp64":
+            r0 = oracle.evaluate(w.system, specs)
+            x, _, _, _ = oracle.leapfrog(w.system, specs, v, DT, 100, forces=r0["forces"], constraints=c)
+            print(f"\nrigid water: |dx| at 100 steps {np.abs(x100 - x).max():.2e} A")
+            assert np.abs(x100 - x).max() <= 1e-6
+        lf.run(900)
+        xg, vg, _, eg = lf.state()
+        assert lf.constraint_limit_hits() == 0
+        gains.append(E(eg, vg) - E(e100, v100))
+        kes.append(integrate.kinetic_energy(m, vg))
+        d = np.linalg.norm(xg[c["atoms"][:, 0]] - xg[c["atoms"][:, 1]], axis=1)
+        worst_bond = max(worst_bond, float(np.abs(d - c["rest"]).max()))
+        topo.close()
+    print(f"rigid water {precision}: E(1000) - E(100) {' '.join(f'{g:+.1f}' for g in gains)} kcal/mol "
+          f"(KE {np.mean(kes):.0f}), bond error {worst_bond:.2e} A")
+    assert worst_bond <= 1e-3
+    assert abs(np.mean(gains)) <= 0.02 * np.mean(kes)
