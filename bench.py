@@ -37,10 +37,10 @@ METRIC = "force evals/s (cutoff+PME) mixed vs FP64 on one B200 at ≤1e-5 force 
 UNIT = "evals/s"
 FP32_LANES_PER_SM = 128
 N_SMS = 148
-# DRAM bytes (read + write) of one k_pair_mixed launch on this workload:
-# dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of the
-# kernel on this bench command (L2 flushed before the evaluation)
-PAIR_DRAM_BYTES_PER_LAUNCH = 4_994_304
+# DRAM bytes (read + write) of one pair-kernel launch on this workload, by
+# layout: dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of
+# the kernel on this bench command (L2 flushed before the evaluation)
+PAIR_DRAM_BYTES_PER_LAUNCH = {"columns": 10_208_512, "cells": 4_994_304}
 
 
 def parse():
@@ -334,9 +334,11 @@ def main():
     fp32_peak = N_SMS * FP32_LANES_PER_SM * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
     pair_ms = phases["pair"]
     achieved = n_pairs * flops_per_pair / (pair_ms * 1e-3) / 1e12
-    roofline = {"bound": "fp32", "kernel": "k_pair_mixed<LJ C2 + EwaldReal Cutoff>",
+    layout = topo.pair_layout() or "cells"
+    kname = "k_pair_col" if layout == "columns" else "k_pair_mixed"
+    roofline = {"bound": "fp32", "kernel": f"{kname}<LJ C2 + EwaldReal Cutoff>", "layout": layout,
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": PAIR_DRAM_BYTES_PER_LAUNCH, "traffic_unit": "B per launch (ncu)",
+                "traffic": PAIR_DRAM_BYTES_PER_LAUNCH[layout], "traffic_unit": "B per launch (ncu)",
                 "launch_ms": pair_ms,
                 "peak_source": f"nominal FP32 CUDA-core rate at sm_max_mhz of MEASURED_PEAKS.json ({peak_src}): "
                                "148 SMs x 128 lanes x 2 flop",
@@ -344,8 +346,7 @@ def main():
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     kx = 64
     kzh = kx // 2 + 1
-    pme_bytes = {"pme_spread": 16 * n + 4 * kx ** 3, "pme_fft": 2 * 2 * 8 * kx * kx * kzh,
-                 "pme_gather": 4 * kx ** 3 + 16 * n + 12 * n}
+    pme_bytes = pme_algorithmic_bytes(n, kx)
     pme_roof = {k: {"achieved_gbs": b / (phases[k] * 1e-3) / 1e9, "peak_gbs": hbm,
                     "frac": b / (phases[k] * 1e-3) / 1e9 / hbm, "bytes": b, "launch_ms": phases[k]}
                 for k, b in pme_bytes.items() if phases.get(k)}
@@ -693,11 +694,11 @@ def measure_1m(local, torch, steps):
             with torch.cuda.stream(stream):
                 for _ in range(3):
                     step()
-            msp = (C.c_double * 8)()
-            cnt = C.c_longlong(0)
-            lib.pmgpu_phase_times(topo.handle, msp, 8, C.byref(cnt))
-            lib.pmgpu_set_profiling(topo.handle, 0)
             from protomol_b200 import _lib
+            msp = (C.c_double * len(_lib.PHASES))()
+            cnt = C.c_longlong(0)
+            lib.pmgpu_phase_times(topo.handle, msp, len(_lib.PHASES), C.byref(cnt))
+            lib.pmgpu_set_profiling(topo.handle, 0)
             ph = {k: msp[i] / max(1, cnt.value) for i, k in enumerate(_lib.PHASES)}
             # count only (capacity 0: the call reports the count it would need)
             cnt = C.c_longlong(0)
@@ -709,8 +710,7 @@ def measure_1m(local, torch, steps):
             out["pair_kernel_ms"] = ph["pair"]
             kx = 216
             kzh = kx // 2 + 1
-            b = {"pme_spread": 16 * n + 4 * kx ** 3, "pme_fft": 2 * 2 * 8 * kx * kx * kzh,
-                 "pme_gather": 4 * kx ** 3 + 16 * n + 12 * n}
+            b = pme_algorithmic_bytes(n, kx)
             out["pme_hbm_gbs"] = {k: v / (ph[k] * 1e-3) / 1e9 for k, v in b.items() if ph.get(k)}
             out["phases_ms"] = ph
             out["trajectory_100"] = measure_1m_trajectory(lib, topo, fs, dpos, dfor, den, stream, torch, npairs)
@@ -769,6 +769,22 @@ def _lib_load():
     return _lib.load()
 
 
+def pme_algorithmic_bytes(n, k):
+    """Bytes each reciprocal phase must move once, for n atoms on a k^3 grid
+    (half spectrum k * k * (k / 2 + 1)): spread reads positions and charges
+    (32 B per atom) and writes the int64 charge grid (8 B per point); the FFT
+    chain reads that grid, writes and reads the FP32 complex half spectrum
+    twice (forward, inverse) and writes the FP32 real grid; the gather reads
+    the real grid and the positions and charges and adds three int64 forces
+    per atom; the FP64 energy transform reads the charge grid and passes the
+    FP64 half spectrum three times."""
+    half = k * k * (k // 2 + 1)
+    return {"pme_spread": 32 * n + 8 * k ** 3,
+            "pme_fft": 8 * k ** 3 + 2 * 2 * 8 * half + 4 * k ** 3,
+            "pme_gather": 4 * k ** 3 + 32 * n + 24 * n,
+            "pme_energy64": 8 * k ** 3 + 3 * 2 * 16 * half}
+
+
 def profile_phases(lib, topo, forces, step, flush, stream, torch, steps):
     """Average device milliseconds per evaluation phase: the library records
     CUDA events around each phase on its own stream (profiling mode)."""
@@ -778,9 +794,9 @@ def profile_phases(lib, topo, forces, step, flush, stream, torch, steps):
         for _ in range(steps):
             flush.zero_()
             step(forces)
-    ms = (C.c_double * 8)()
+    ms = (C.c_double * len(_lib.PHASES))()
     n = C.c_longlong(0)
-    _lib.check(lib.pmgpu_phase_times(topo.handle, ms, 8, C.byref(n)), topo.handle)
+    _lib.check(lib.pmgpu_phase_times(topo.handle, ms, len(_lib.PHASES), C.byref(n)), topo.handle)
     _lib.check(lib.pmgpu_set_profiling(topo.handle, 0), topo.handle)
     evals = max(int(n.value), 1)
     return {name: ms[k] / evals for k, name in enumerate(_lib.PHASES)}

@@ -258,7 +258,8 @@ int pmgpu_set_profiling(pmgpu_system* sys, int enable);
 /* Accumulated device milliseconds per phase since profiling was enabled:
  * ms[0] binning, [1] cutoff pair kernels, [2] PME correction, [3] PME
  * spread, [4] PME FFT + convolution, [5] PME gather, [6] finalize + energy
- * reduction, [7] cluster-pair list of the mixed cutoff kernel; *evals =
+ * reduction, [7] cluster-pair list of the mixed cutoff kernel, [8] the
+ * FP64 reciprocal energy transform of a mixed PME force; *evals =
  * number of profiled evaluations.  Synchronizes. */
 int pmgpu_phase_times(pmgpu_system* sys, double* ms, int n, long long* evals);
 

@@ -35,7 +35,8 @@ EXPORTS = [
     "pmgpu_leapfrog_run", "pmgpu_hessian", "pmgpu_impulse_run", "pmgpu_set_constraints",
     "pmgpu_constraint_limit_hits",
 ]
-PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list"]
+PHASES = ["bin", "pair", "pme_correction", "pme_spread", "pme_fft", "pme_gather", "finalize", "pair_list",
+          "pme_energy64"]
 
 
 class CutoffParams(C.Structure):

@@ -297,12 +297,18 @@ constexpr int kColThreads = 128;
 
 // one block per column: z order (a bitonic sort of the (z, index) keys in
 // shared memory), slot data, padding, cluster boxes and the clusters' virial
-// origins
+// origins.  The sorted atoms' fixed-point coordinates and the j-cluster boxes
+// stay in shared memory for the box passes (no global round trips there).
 __global__ void __launch_bounds__(kColThreads) k_col_sort(ColBinArgs a)
 {
     pdl_wait();
-    __shared__ unsigned long long s_key[kColStage];
-    __shared__ int s_ord[kColStage];
+    // [0, 8K): order; [8K, 32K): sort keys, then the atoms' coordinates;
+    // [32K, 48K): the j-cluster boxes
+    __shared__ __align__(16) unsigned char s_raw[4 * kColStage + 12 * kColStage + 16 * kColStage / 2];
+    int* s_ord = reinterpret_cast<int*>(s_raw);
+    unsigned long long* s_key = reinterpret_cast<unsigned long long*>(s_raw + 4 * kColStage);
+    unsigned* s_qf = reinterpret_cast<unsigned*>(s_raw + 4 * kColStage);
+    float4* s_jb = reinterpret_cast<float4*>(s_raw + 16 * kColStage);
     const int t = threadIdx.x;
     const ColGrid& g = a.g;
     const int c = blockIdx.x;
@@ -335,7 +341,7 @@ __global__ void __launch_bounds__(kColThreads) k_col_sort(ColBinArgs a)
             __syncthreads();
         }
     for (int k = t; k < m; k += kColThreads) s_ord[k] = (int)(s_key[k] & 0xffffffffull);
-    __syncthreads();
+    __syncthreads();                                        // the keys' space becomes the coordinates'
     const size_t slot0 = 8 * (size_t)cl0;
     for (int r = t; r < 8 * ncl; r += kColThreads) {
         const bool valid = r < m;
@@ -343,12 +349,17 @@ __global__ void __launch_bounds__(kColThreads) k_col_sort(ColBinArgs a)
         const double qi = a.q[i];
         const float qh = valid ? (float)qi : 0.f;
         const float ql = valid ? (float)(qi - (double)qh) : 0.f;
-        const int4 qv = make_int4((int)a.qfix[3 * i], (int)a.qfix[3 * i + 1], (int)a.qfix[3 * i + 2], __float_as_int(qh));
+        const unsigned fx = a.qfix[3 * i], fy = a.qfix[3 * i + 1], fz = a.qfix[3 * i + 2];
+        const int4 qv = make_int4((int)fx, (int)fy, (int)fz, __float_as_int(qh));
         a.cq[slot0 + r] = qv;
         a.cm[slot0 + r] = valid ? make_int4(i, a.type[i], a.mol[i], __float_as_int(ql)) : make_int4(-1, 0, -2, 0);
-        if (valid) a.slot_of[i] = (int)(slot0 + r);
+        if (valid) {
+            a.slot_of[i] = (int)(slot0 + r);
+            s_qf[3 * r] = fx; s_qf[3 * r + 1] = fy; s_qf[3 * r + 2] = fz;
+        }
         if ((r & 7) == 0) a.corg[cl0 + (r >> 3)] = make_int4(qv.x, qv.y, qv.z, 0);
     }
+    __syncthreads();
     // boxes of the j-clusters (4 slots each, the halves of the i-clusters)
     // and of the i-clusters; an empty half gets a box beyond every window
     const double kx = g.lx * (1.0 / 4294967296.0), ky = g.ly * (1.0 / 4294967296.0), kz = g.lz * (1.0 / 4294967296.0);
@@ -359,21 +370,21 @@ __global__ void __launch_bounds__(kColThreads) k_col_sort(ColBinArgs a)
         float4 lo = make_float4(3e38f, 3e38f, 3e38f, 1.f), hi = make_float4(3e38f, 3e38f, 3e38f, 0.f);
         if (r0 < r1) { lo.w = 0.f; hi = make_float4(-3e38f, -3e38f, -3e38f, 0.f); }
         for (int r = r0; r < r1; ++r) {
-            const int i = s_ord[r];
-            const float x = (float)(a.qfix[3 * i] * kx), y = (float)(a.qfix[3 * i + 1] * ky),
-                        z = (float)(a.qfix[3 * i + 2] * kz);
+            const float x = (float)(s_qf[3 * r] * kx), y = (float)(s_qf[3 * r + 1] * ky),
+                        z = (float)(s_qf[3 * r + 2] * kz);
             lo.x = fminf(lo.x, x); lo.y = fminf(lo.y, y); lo.z = fminf(lo.z, z);
             hi.x = fmaxf(hi.x, x); hi.y = fmaxf(hi.y, y); hi.z = fmaxf(hi.z, z);
         }
         const size_t jc = 2 * (size_t)cl0 + q;
         a.jbox[2 * jc] = lo;
         a.jbox[2 * jc + 1] = hi;
+        s_jb[2 * q] = lo;
+        s_jb[2 * q + 1] = hi;
     }
     __syncthreads();
     for (int q = t; q < ncl; q += kColThreads) {
-        const size_t j0 = 2 * ((size_t)cl0 + q);
-        const float4 l0 = a.jbox[2 * j0], h0 = a.jbox[2 * j0 + 1];
-        const float4 l1 = a.jbox[2 * j0 + 2], h1 = a.jbox[2 * j0 + 3];
+        const float4 l0 = s_jb[4 * q], h0 = s_jb[4 * q + 1];
+        const float4 l1 = s_jb[4 * q + 2], h1 = s_jb[4 * q + 3];
         const bool e1 = l1.w != 0.f;                        // empty second half
         a.ibox[2 * (cl0 + q)] = e1 ? l0 : make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
         a.ibox[2 * (cl0 + q) + 1] = e1 ? h0 : make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
@@ -417,11 +428,14 @@ int launch_col_refresh(const ColBinArgs& a, double half_skin, cudaStream_t s, lo
 
 int launch_col_bin(const ColBinArgs& a, cudaStream_t s, long long* launches)
 {
-    const int nb = a.n > 0 ? (a.n + kBinThreads - 1) / kBinThreads : 1;
-    k_col_count<<<nb, kBinThreads, 0, s>>>(a);
+    // half-size blocks: the atoms' FP64 conversions are latency-bound, and
+    // twice the blocks spread them over more SMs
+    const int tb = kBinThreads / 2;
+    const int nb = a.n > 0 ? (a.n + tb - 1) / tb : 1;
+    k_col_count<<<nb, tb, 0, s>>>(a);
     *launches += 1;
     if (a.n > 0) {
-        launch_pdl(k_col_scatter, nb, kBinThreads, 0, s, a);
+        launch_pdl(k_col_scatter, nb, tb, 0, s, a);
         launch_pdl(k_col_sort, a.g.ncol, kColThreads, 0, s, a);
         *launches += 2;
     }

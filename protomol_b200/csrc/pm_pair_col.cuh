@@ -72,6 +72,7 @@ __device__ __forceinline__ int2 col_zrange(const PairArgs& p, int jb, int je, fl
 }
 
 constexpr int kColStageEntries = 512;    // entries of one i-cluster staged in shared memory
+constexpr int kEnergyFlush = 8;          // pair-kernel iterations per FP32 energy partial sum
 
 // The list of i-cluster ic (one warp): every candidate column of the half
 // neighbourhood -- the column offsets (ox, oy) with ox > 0 or ox = 0 < oy,
@@ -342,6 +343,10 @@ __global__ void __launch_bounds__(128, 5) k_pair_col(PairArgs p)
         const bool vi = Mi.x >= 0;
         float fix = 0.f, fiy = 0.f, fiz = 0.f;
         double el = 0.0, ec = 0.0;
+        // the far pairs' FP32 energies summed over up to kEnergyFlush
+        // iterations in FP32, then into the FP64 sums
+        float elf = 0.f, ecf = 0.f;
+        int nacc = 0;
         double wv[3] = {0.0, 0.0, 0.0};
         int nq = 0;
         const int e_end = cd.z + cd.w;
@@ -407,8 +412,13 @@ __global__ void __launch_bounds__(128, 5) k_pair_col(PairArgs p)
                     nq += __popc(bb);
                 }
             }
-            el += (double)(ela + elb);
-            ec += (double)(eca + ecb);
+            elf += ela + elb;
+            ecf += eca + ecb;
+            if (++nacc == kEnergyFlush) {
+                el += (double)elf;
+                ec += (double)ecf;
+                elf = 0.f; ecf = 0.f; nacc = 0;
+            }
             // j-forces of both tiles: lane il < 6 ends with one component
             const float v = j_reduce_scatter(xa, ya, za, xb, yb, zb, il);
             if (holds && v != 0.f)
@@ -434,6 +444,8 @@ __global__ void __launch_bounds__(128, 5) k_pair_col(PairArgs p)
                 }
             }
         }
+        el += (double)elf;
+        ec += (double)ecf;
         // chunk end: i-forces (lanes jj = 0, 1, 2 hold component jj of i-atom il)
         const float vi3 = i_reduce_scatter(fix, fiy, fiz, jj);
         if (jj < 3 && vi && vi3 != 0.f) fixed_addf(p.facc + 3 * (size_t)si + jj, vi3, p.status);

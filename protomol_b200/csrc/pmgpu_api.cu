@@ -33,7 +33,7 @@ static const int kEOut = 20;
 
 // evaluation phases timed in profiling mode (pmgpu_phase_times)
 enum { kPhaseBin = 0, kPhasePair, kPhaseCorrection, kPhaseSpread, kPhaseFft, kPhaseGather, kPhaseFinalize,
-       kPhaseList, kNumPhases };
+       kPhaseList, kPhaseEnergy64, kNumPhases };
 
 struct ProfMark {
     int phase;
@@ -1734,16 +1734,25 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     } else {
         CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
     }
-    if (use32) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
-    if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
     bool any_cut = false, any_pme = false, any_full = false;
+    bool atom_mixed = false, atom_fp64 = false;        // PME / all-pairs forces of each precision
     for (int k = 0; k < nf; ++k) {
         any_cut |= forces[k]->kind == 0;
         any_pme |= forces[k]->kind == 1;
         any_full |= forces[k]->kind == 2;
+        if (forces[k]->kind != 0) (forces[k]->precision == PMGPU_PRECISION_FP64 ? atom_fp64 : atom_mixed) = true;
     }
-    if (any_pme || any_full) CK(cudaMemsetAsync(sys->d_faccA, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     const bool use_col = sys->eval_use_col;
+    // the cell-ordered mixed accumulators serve the cell path's mixed cutoff
+    // forces only; the atom-ordered ones (mixed half, FP64 half) PME and the
+    // all-pairs forces of that precision
+    bool mixed_cells = false;
+    for (int k = 0; k < nf; ++k)
+        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64 && !use_col) mixed_cells = true;
+    if (mixed_cells) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
+    if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
+    if (atom_mixed) CK(cudaMemsetAsync(sys->d_faccA, 0, sizeof(unsigned long long) * n3, s), "memset");
+    if (atom_fp64) CK(cudaMemsetAsync(sys->d_faccA + n3, 0, sizeof(unsigned long long) * n3, s), "memset");
     for (int k = 0; k < nf; ++k)
         if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64)
             sys->last_layout = use_col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS;
@@ -1841,7 +1850,9 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                 a.mol = sys->d_mol; a.molpos = sys->d_molpos; a.pbc = sys->pbc;
                 a.mrec = sys->d_mrec; a.mrec_stride = sys->mrec_cap;
                 const bool e64 = branches && a.cgrid64 != nullptr && !e64_branch;
-                a.energy64_apart = e64 ? 1 : 0;
+                // profiling times the FP64 energy transform as a phase of its own
+                const bool e64_timed = sys->profiling && a.cgrid64 != nullptr;
+                a.energy64_apart = (e64 || e64_timed) ? 1 : 0;
                 const int phases[3] = {kPhaseSpread, kPhaseFft, kPhaseGather};
                 const int stages[3] = {kStageSpread, kStageFft, kStageGather};
                 for (int st = 0; st < 3; ++st) {
@@ -1857,6 +1868,18 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
                     }
                     used += u;
                     prof_end(sys, m);
+                    if (st == 2 && e64_timed) {
+                        int me = prof_begin(sys, kPhaseEnergy64);
+                        int ue = 0;
+                        e = launch_pme_reciprocal(a, 0, ps, &sys->launches, sys->d_erec + used, &ue, kStageEnergy64);
+                        if (e) return cuda_fail(sys, (cudaError_t)e, "PME energy transform");
+                        if (molvir && ue > 0) {
+                            mf.range_first[mf.nranges] = used;
+                            mf.range_count[mf.nranges++] = ue;
+                        }
+                        used += ue;
+                        prof_end(sys, me);
+                    }
                     if (st == 2 && molvir) {
                         PmeArgs am = a;
                         am.mrec = sys->d_mrec + mused;
@@ -2009,8 +2032,8 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         memset(&fa, 0, sizeof(fa));
         fa.n = sys->n;
         // the slot-ordered accumulators exist only with the cell-sorted order
-        fa.f32 = use32 && cell_sort ? sys->d_facc32 : nullptr;
-        fa.f32p = use32 && cell_sort ? sys->d_facc32p : nullptr;
+        fa.f32 = mixed_cells ? sys->d_facc32 : nullptr;
+        fa.f32p = mixed_cells ? sys->d_facc32p : nullptr;
         fa.f40 = use40 && cell_sort ? sys->d_facc40 : nullptr;
         if (use_col) {
             fa.c32 = sys->d_facc32c; fa.c_slot_of = sys->d_cslot; fa.cq = sys->d_cq;
