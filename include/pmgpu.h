@@ -327,15 +327,19 @@ void* pmgpu_batch_stream(pmgpu_batch* batch);
  * No counterpart in the reference (its CPU loops have nothing to tune).  The
  * launch shapes of a system's evaluation: the cluster-pair list's work
  * chunks, the mixed pair kernel's resident blocks, the PME FFT's lines per
- * block, and whether PME runs on a second stream beside the pair kernels.
- * Results do not depend on them beyond the last bits of the fixed-point
- * grouping (a chunk's partial sums are rounded together).  Defaults: 16, 0
- * (the occupancy limit), 16, 1. */
+ * block, whether PME runs on a second stream beside the pair kernels, and
+ * whether mixed cutoff forces take the FP64 pair kernels.  Results do not
+ * depend on the first four beyond the last bits of the fixed-point grouping
+ * (a chunk's partial sums are rounded together); fp64_pairs gives the FP64
+ * kernels' results, which hold every mixed-precision bound.  Defaults: 16, 0
+ * (the occupancy limit), 16, 1, 0. */
 typedef struct pmgpu_tuning {
     int chunk_entries;        /* cluster-list entries per chunk of pair work: 4..64 */
     int pair_blocks_per_sm;   /* resident blocks of the mixed pair kernel per SM: 0 (occupancy limit) or 1..8 */
     int fft_lines;            /* lines per block of the strided PME FFT passes, at most: 1..16 (z passes: twice) */
     int pme_concurrent;       /* 1: PME on a second stream beside the pair kernels; 0: after them */
+    int fp64_pairs;           /* 1: mixed cutoff forces run the FP64 pair kernels (no cluster list, no
+                                 near-pair pass: the shorter launch chain, faster on a few hundred atoms) */
     double ms_per_eval;       /* pmgpu_autotune: the measured time of the chosen tuning */
 } pmgpu_tuning;
 int pmgpu_get_tuning(pmgpu_system* sys, pmgpu_tuning* out);
@@ -344,7 +348,7 @@ int pmgpu_set_tuning(pmgpu_system* sys, const pmgpu_tuning* tuning);
 /* Project-written autotuner: times candidate tunings on these forces and
  * these positions (host, N x 3), evals evaluations each after two warm-up
  * ones, with CUDA events on the system's stream; a coordinate search over
- * the four parameters, two sweeps.  Keeps the fastest for the system's later
+ * the five parameters, two sweeps.  Keeps the fastest for the system's later
  * evaluations and returns it (with its time) in *best.  Synchronous; uses
  * the system's own scratch buffers (no caller output is touched). */
 int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,
@@ -438,9 +442,12 @@ int pmgpu_get_cells(pmgpu_system* sys, int* cells, int* dims);
  * PMGPU_LAYOUT_COLUMNS (fixed-point coordinates in z-sorted columns, boxes
  * well above twice the cutoff), PMGPU_LAYOUT_CELLS (clusters inside the
  * reference cells: smaller boxes, the small-grid mode, or a system whose
- * columns or clusters exceeded the column layout's limits), or 0 (none yet). */
+ * columns or clusters exceeded the column layout's limits),
+ * PMGPU_LAYOUT_FP64 (the FP64 pair kernels, tuning fp64_pairs), or 0 (none
+ * yet). */
 #define PMGPU_LAYOUT_CELLS 1
 #define PMGPU_LAYOUT_COLUMNS 2
+#define PMGPU_LAYOUT_FP64 3
 int pmgpu_pair_layout(pmgpu_system* sys);
 
 /* No counterpart in the reference, whose cutoff force rebuilds its cell lists

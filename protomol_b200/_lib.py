@@ -57,7 +57,7 @@ class PmeParams(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("chunk_entries", C.c_int), ("pair_blocks_per_sm", C.c_int), ("fft_lines", C.c_int),
-                ("pme_concurrent", C.c_int), ("ms_per_eval", C.c_double)]
+                ("pme_concurrent", C.c_int), ("fp64_pairs", C.c_int), ("ms_per_eval", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -206,7 +206,7 @@ struct pmgpu_system {
     std::set<pmgpu_force*> forces;     // live forces made on this system
     int topo_version = 0;
     int buf_version = 0;               // bumped when a per-evaluation buffer moves
-    pmgpu_tuning tuning = {16, 0, 16, 1, 0.0};   // launch shapes (pmgpu_set_tuning, pmgpu_autotune)
+    pmgpu_tuning tuning = {16, 0, 16, 1, 0, 0.0};   // launch shapes (pmgpu_set_tuning, pmgpu_autotune)
     // CUDA graphs of the last few distinct evaluations (force groups,
     // buffers, flags), replayed when the key matches; the least recently
     // used is replaced (a multiple-time-step integrator alternates groups)
@@ -1484,6 +1484,15 @@ static void fill_col_args(pmgpu_system* sys, PairArgs& a)
     a.list_skin = sys->list_every > 1 ? (float)sys->list_skin : 0.0f;
 }
 
+// The pair kernels a force runs in this evaluation: the FP64 ones for an
+// FP64 force, and for a mixed cutoff force when the tuning asks for them
+// (fp64_pairs: no cluster list and no near-pair pass, the shorter launch
+// chain that is faster on systems of a few hundred atoms)
+static inline bool pairs64(const pmgpu_system* sys, const pmgpu_force* f)
+{
+    return f->precision == PMGPU_PRECISION_FP64 || (f->kind == 0 && sys->tuning.fp64_pairs);
+}
+
 static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_pos, PairArgs& a)
 {
     memset(&a, 0, sizeof(a));
@@ -1522,7 +1531,7 @@ static void fill_pair_args(pmgpu_system* sys, pmgpu_force* f, const double* d_po
     a.status = sys->d_status;
     // mixed forces on whole-cell shifts go to the pair accumulator (their
     // virial is completed from it at finalize), the small-grid mode to the other
-    if (f->precision == PMGPU_PRECISION_FP64) { a.facc = sys->d_facc40; a.scale = kScaleFp64; }
+    if (pairs64(sys, f)) { a.facc = sys->d_facc40; a.scale = kScaleFp64; }
     else { a.facc = f->wrap ? sys->d_facc32p : sys->d_facc32; a.scale = kScaleMixed; }
 }
 
@@ -1541,7 +1550,7 @@ static int pair_records(pmgpu_system* sys, pmgpu_force* f)
 {
     // the mixed kernel sums energies in fixed point (d_efix), no records
     if (f->kind == 2) return adjoint_blocks(sys->n);
-    return f->precision == PMGPU_PRECISION_FP64 ? pair_blocks(sys->grid, f->nd) : 0;
+    return pairs64(sys, f) ? pair_blocks(sys->grid, f->nd) : 0;
 }
 
 // upper bound of the energy records of the fused x pass (one per CTA, at
@@ -1609,7 +1618,7 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces, u
         double rc2 = 0.0;
         bool any = false, ok = true;
         for (int k = 0; k < nf; ++k)
-            if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) {
+            if (forces[k]->kind == 0 && !pairs64(sys, forces[k])) {
                 any = true;
                 ok = ok && !forces[k]->wrap;
                 rc2 = std::max(rc2, forces[k]->cut2);
@@ -1642,13 +1651,13 @@ static int eval_prepare(pmgpu_system* sys, int nf, pmgpu_force* const* forces, u
         }
         double rc2 = 0.0;
         for (int k = 0; k < nf; ++k)
-            if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) rc2 = std::max(rc2, forces[k]->cut2);
+            if (forces[k]->kind == 0 && !pairs64(sys, forces[k])) rc2 = std::max(rc2, forces[k]->cut2);
         const long long entries = col_list_estimate(sys->n, g, g.lx * g.ly * g.lz, std::sqrt(rc2) + sys->list_skin);
         lneed = 2 * entries;                  // int4 entries in the int2 list buffer
         cneed = col_chunk_estimate(entries, sys->n, g, sys->tuning.chunk_entries);
     } else {
         for (int k = 0; k < nf; ++k)
-            if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) {
+            if (forces[k]->kind == 0 && !pairs64(sys, forces[k])) {
                 lneed = std::max(lneed, plist_estimate(sys->n, sys->grid, forces[k]->nh));
                 cneed = std::max(cneed, chunk_estimate(sys->n, sys->grid, forces[k]->nh, sys->tuning.chunk_entries));
             }
@@ -1721,7 +1730,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     MolvirFinish mf;
     memset(&mf, 0, sizeof(mf));
     bool use32 = false, use40 = false;
-    for (int k = 0; k < nf; ++k) (forces[k]->precision == PMGPU_PRECISION_FP64 ? use40 : use32) = true;
+    for (int k = 0; k < nf; ++k) (pairs64(sys, forces[k]) ? use40 : use32) = true;
     int r;
     cudaStream_t s = sys->stream;
     size_t n3 = 3 * (size_t)sys->n;
@@ -1740,7 +1749,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         any_cut |= forces[k]->kind == 0;
         any_pme |= forces[k]->kind == 1;
         any_full |= forces[k]->kind == 2;
-        if (forces[k]->kind != 0) (forces[k]->precision == PMGPU_PRECISION_FP64 ? atom_fp64 : atom_mixed) = true;
+        if (forces[k]->kind != 0) (pairs64(sys, forces[k]) ? atom_fp64 : atom_mixed) = true;
     }
     const bool use_col = sys->eval_use_col;
     // the cell-ordered mixed accumulators serve the cell path's mixed cutoff
@@ -1748,14 +1757,15 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     // all-pairs forces of that precision
     bool mixed_cells = false;
     for (int k = 0; k < nf; ++k)
-        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64 && !use_col) mixed_cells = true;
+        if (forces[k]->kind == 0 && !pairs64(sys, forces[k]) && !use_col) mixed_cells = true;
     if (mixed_cells) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
     if (atom_mixed) CK(cudaMemsetAsync(sys->d_faccA, 0, sizeof(unsigned long long) * n3, s), "memset");
     if (atom_fp64) CK(cudaMemsetAsync(sys->d_faccA + n3, 0, sizeof(unsigned long long) * n3, s), "memset");
     for (int k = 0; k < nf; ++k)
         if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64)
-            sys->last_layout = use_col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS;
+            sys->last_layout = pairs64(sys, forces[k]) ? PMGPU_LAYOUT_FP64
+                             : (use_col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS);
     if (use_col)
         CK(cudaMemsetAsync(sys->d_facc32c, 0, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap, s),
            "memset");
@@ -1763,7 +1773,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     // ones when the column path does not take them
     bool cell_sort = false;
     for (int k = 0; k < nf; ++k)
-        if (forces[k]->kind == 0 && (forces[k]->precision == PMGPU_PRECISION_FP64 || !use_col)) cell_sort = true;
+        if (forces[k]->kind == 0 && (pairs64(sys, forces[k]) || !use_col)) cell_sort = true;
     // the molecular virial kernels of the cutoff forces read the cell-sorted
     // order too (binned for them alone on the column path)
     const bool mv_bin = molvir && any_cut && !cell_sort;
@@ -1777,7 +1787,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         for (int k = 0; k < nf; ++k) {
             pmgpu_force* f = forces[k];
             if (f->kind != 1) continue;
-            const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+            const bool fp64 = pairs64(sys, f);
             unsigned long long* facc = fp64 ? sys->d_faccA + n3 : sys->d_faccA;
             const double scale = fp64 ? kScaleFp64 : kScaleMixed;
             const pmgpu_pme_params& p = f->pp;
@@ -1942,7 +1952,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     for (int k = 0; k < nf; ++k) {
         pmgpu_force* f = forces[k];
         if (f->kind != 2) continue;
-        const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+        const bool fp64 = pairs64(sys, f);
         AdjArgs a;
         adj_pair_args(sys, f, a);
         a.pos = d_pos;
@@ -1957,14 +1967,14 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     }
     int last_mixed = -1;                // the last mixed cutoff force (its near pairs may go to the side stream)
     for (int k = 0; k < nf; ++k)
-        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) last_mixed = k;
+        if (forces[k]->kind == 0 && !pairs64(sys, forces[k])) last_mixed = k;
     bool near_on_side = false;
     int lists = 0;
     int pair_virial = 0, col_virial = 0;
     for (int k = 0; k < nf; ++k) {
         pmgpu_force* f = forces[k];
         if (f->kind != 0) continue;
-        const bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+        const bool fp64 = pairs64(sys, f);
         const bool col = !fp64 && use_col;
         if (!fp64 && !col && !f->wrap && virial) pair_virial = 1;
         if (col && virial) col_virial = 1;
@@ -2045,7 +2055,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         }
         for (int k = 0; k < nf; ++k)
             if (forces[k]->kind != 0) {
-                if (forces[k]->precision == PMGPU_PRECISION_FP64) fa.a40 = sys->d_faccA + n3;
+                if (pairs64(sys, forces[k])) fa.a40 = sys->d_faccA + n3;
                 else fa.a32 = sys->d_faccA;
             }
         fa.sorted = cell_sort ? sys->d_sorted : nullptr; fa.spos = sys->d_spos; fa.slo = sys->d_slo;
@@ -2097,7 +2107,7 @@ static int eval_core(pmgpu_system* sys, int nf_in, pmgpu_force* const* forces_in
     int n_mixed_cut = 0;
     for (int k = 0; k < nf; ++k) {
         ids.push_back(forces[k]->id);
-        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64) ++n_mixed_cut;
+        if (forces[k]->kind == 0 && !pairs64(sys, forces[k])) ++n_mixed_cut;
     }
     const bool can_reuse = sys->eval_use_col && sys->list_every > 1 && n_mixed_cut == 1;
     sys->eval_reuse = can_reuse && sys->list_valid && sys->list_ids == ids && sys->evals_since_build < sys->list_every;
@@ -2278,9 +2288,10 @@ extern "C" int pmgpu_get_pairs(pmgpu_system* sys, pmgpu_force* f, const double* 
     CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
     CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
     CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
-    bool fp64 = f->precision == PMGPU_PRECISION_FP64;
+    bool fp64 = pairs64(sys, f);
     const bool col = !fp64 && sys->eval_use_col;          // eval_prepare decided for this force alone
-    if (!fp64) sys->last_layout = col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS;
+    if (f->precision != PMGPU_PRECISION_FP64)
+        sys->last_layout = fp64 ? PMGPU_LAYOUT_FP64 : (col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS);
     if (col) {
         CK(cudaMemsetAsync(sys->d_facc32c, 0, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap, s),
            "memset");
@@ -2661,7 +2672,7 @@ static bool tuning_valid(const pmgpu_tuning& t)
 {
     return t.chunk_entries >= 4 && t.chunk_entries <= 64 && t.pair_blocks_per_sm >= 0 &&
            t.pair_blocks_per_sm <= 8 && t.fft_lines >= 1 && t.fft_lines <= 16 &&
-           (t.pme_concurrent == 0 || t.pme_concurrent == 1);
+           (t.pme_concurrent == 0 || t.pme_concurrent == 1) && (t.fp64_pairs == 0 || t.fp64_pairs == 1);
 }
 
 static void apply_tuning(pmgpu_system* sys, const pmgpu_tuning& t)
@@ -2685,7 +2696,7 @@ extern "C" int pmgpu_set_tuning(pmgpu_system* sys, const pmgpu_tuning* t)
     return PMGPU_OK;
 }
 
-// coordinate search over the four launch parameters: each is tried at its
+// coordinate search over the five launch parameters: each is tried at its
 // candidate values with the others at the best so far, two sweeps; time(t)
 // measures one candidate in ms per evaluation
 template <class TimeFn>
@@ -2695,18 +2706,20 @@ static int tune_search(pmgpu_tuning start, bool has_pme, bool has_pairs, TimeFn 
     int r = time(start, &best_ms);
     if (r) return r;
     pmgpu_tuning b = start;
-    const int chunks[3] = {8, 16, 32}, bps[3] = {0, 3, 2}, lines[3] = {16, 8, 4}, conc[2] = {1, 0};
+    const int chunks[3] = {8, 16, 32}, bps[3] = {0, 3, 2}, lines[3] = {16, 8, 4}, conc[2] = {1, 0},
+              f64[2] = {0, 1};
     for (int sweep = 0; sweep < 2; ++sweep) {
-        for (int param = 0; param < 4; ++param) {
-            if ((param == 0 || param == 1) && !has_pairs) continue;
+        for (int param = 0; param < 5; ++param) {
+            if ((param == 0 || param == 1 || param == 4) && !has_pairs) continue;
             if ((param == 2 || param == 3) && !has_pme) continue;
             if (param == 3 && !has_pairs) continue;
-            const int nv = param == 3 ? 2 : 3;
+            const int nv = param >= 3 ? 2 : 3;
             for (int v = 0; v < nv; ++v) {
                 pmgpu_tuning t = b;
                 int* slot = param == 0 ? &t.chunk_entries : param == 1 ? &t.pair_blocks_per_sm
-                          : param == 2 ? &t.fft_lines : &t.pme_concurrent;
-                const int val = param == 0 ? chunks[v] : param == 1 ? bps[v] : param == 2 ? lines[v] : conc[v];
+                          : param == 2 ? &t.fft_lines : param == 3 ? &t.pme_concurrent : &t.fp64_pairs;
+                const int val = param == 0 ? chunks[v] : param == 1 ? bps[v] : param == 2 ? lines[v]
+                              : param == 3 ? conc[v] : f64[v];
                 if (*slot == val) continue;
                 *slot = val;
                 double ms = 0.0;

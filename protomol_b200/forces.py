@@ -145,8 +145,9 @@ class Topology:
     def pair_layout(self) -> str:
         """Cluster layout of the last evaluation's mixed cutoff forces:
         'columns' (fixed-point coordinates in z-sorted columns), 'cells'
-        (clusters inside the reference cells) or '' (none yet)."""
-        return {1: "cells", 2: "columns"}.get(int(_lib.load().pmgpu_pair_layout(self.handle)), "")
+        (clusters inside the reference cells), 'fp64' (the FP64 pair
+        kernels, tuning fp64_pairs) or '' (none yet)."""
+        return {1: "cells", 2: "columns", 3: "fp64"}.get(int(_lib.load().pmgpu_pair_layout(self.handle)), "")
 
     def cells(self):
         cells = np.zeros((self.n_atoms, 3), np.int32)

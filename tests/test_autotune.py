@@ -34,11 +34,12 @@ def test_set_and_get_tuning_round_trip_and_reject_out_of_range():
     s, defs = small_pme_box()
     topo = F.Topology(s)
     t = topo.tuning
-    assert (t["chunk_entries"], t["pair_blocks_per_sm"], t["fft_lines"], t["pme_concurrent"]) == (16, 0, 16, 1)
+    assert (t["chunk_entries"], t["pair_blocks_per_sm"], t["fft_lines"], t["pme_concurrent"],
+            t["fp64_pairs"]) == (16, 0, 16, 1, 0)
     topo.set_tuning(chunk_entries=32, fft_lines=4)
     assert topo.tuning["chunk_entries"] == 32 and topo.tuning["fft_lines"] == 4
     for bad in (dict(chunk_entries=2), dict(chunk_entries=128), dict(pair_blocks_per_sm=-1),
-                dict(fft_lines=0), dict(fft_lines=17), dict(pme_concurrent=2)):
+                dict(fft_lines=0), dict(fft_lines=17), dict(pme_concurrent=2), dict(fp64_pairs=2)):
         with pytest.raises(_lib.PmgpuError):
             topo.set_tuning(**bad)
     assert topo.tuning["chunk_entries"] == 32                  # unchanged by a rejected call
@@ -74,6 +75,46 @@ def test_every_candidate_tuning_gives_the_same_result(precision):
         bad += [(cand, k, v) for k, v in errs.items() if not v <= tol[k]]
     assert not bad, bad
     topo.close()
+
+
+@pytest.mark.parametrize("which", ["water216", "small_pme"])
+def test_fp64_pairs_gives_the_fp64_kernels_results(which):
+    """fp64_pairs = 1 runs a mixed cutoff force on the FP64 pair kernels (the
+    shorter launch chain the autotuner may pick for a few hundred atoms):
+    its forces, energies and virial are the FP64 force's, bit for bit, and
+    the layout reads 'fp64'; back at 0 the mixed kernels run again."""
+    if which == "water216":
+        w = workloads.water216()
+        s, defs = w.system, w.forces
+    else:
+        s, defs = small_pme_box()
+    outs = {}
+    for prec in ("fp64", "mixed"):
+        topo = F.Topology(s)
+        fs = [F.ForceFactory.make(topo, d, prec) for d in defs]
+        if prec == "mixed":
+            fm, em = run(topo, fs, s)
+            assert topo.pair_layout() in ("cells", "columns")
+            topo.set_tuning(fp64_pairs=1)
+        outs[prec] = run(topo, fs, s)
+        if prec == "mixed":
+            assert topo.pair_layout() == "fp64"
+            topo.set_tuning(fp64_pairs=0)
+            f2, e2 = run(topo, fs, s)
+            assert topo.pair_layout() in ("cells", "columns")
+            assert np.array_equal(f2, fm) and e2.lennard_jones == em.lennard_jones
+        topo.close()
+    (fd, ed), (fx, ex) = outs["fp64"], outs["mixed"]
+    if which == "water216":
+        # cutoff forces alone: the same kernels on the same inputs
+        assert np.array_equal(fd, fx)
+        assert ed.lennard_jones == ex.lennard_jones and ed.coulomb == ex.coulomb
+        assert np.array_equal(ed.virial_tensor, ex.virial_tensor)
+    else:
+        # the PME force stays mixed: the pair part is the FP64 one, the sum
+        # within the mixed bounds of the FP64 result
+        assert np.sqrt(((fx - fd) ** 2).sum() / (fd ** 2).sum()) <= 1e-5
+        assert abs(ed.lennard_jones - ex.lennard_jones) <= 1e-12 * abs(ed.lennard_jones)
 
 
 def test_autotuned_system_matches_the_oracle():

@@ -10,11 +10,15 @@ Tolerances (from the reference-parity requirements of this path):
     energy and the virial are within 1e-7 relative of the FP64 oracle: the
     energies of the pairs closer than 5 A, which carry nearly all of the FP32
     rounding there, are evaluated in FP64 (measured: 1e-8 energy, 6e-8
-    virial).  Elsewhere the bound is 2e-6 of |E_LJ| + |E_Coulomb|: plain
-    Coulomb gives every pair inside the cutoff an O(1) kcal/mol energy, so
-    its FP32 rounding (a few ulp per pair, 2^-24) is spread over all pairs
-    (1e-7 to 4e-7 measured), and on small PME-only systems the FP32 FFT
-    leaves ~1e-6.  The FP64 kernels meet 1e-10.
+    virial).  On the small systems here (300 - 1,260 atoms) the total energy
+    is within 1e-7 of |E_LJ| + |E_Coulomb| (measured at most 3.5e-8) and the
+    virial within 1e-6 of its largest entry (at most 4e-7), except for the
+    forces that are Coulomb alone or plain Coulomb: a plain Coulomb term
+    gives every pair inside the cutoff an O(1) kcal/mol energy whose FP32
+    rounding (a few 2^-24 each, unbiased) is not averaged down over a few
+    hundred atoms, and a Coulomb-only total is a cancellation of such terms:
+    2e-6 there (measured 8.3e-7 on water216_c2, 3.7e-7 small_c2_fused,
+    1.3e-7 small_c2lj_c1coul).  The FP64 kernels meet 1e-10.
 """
 import numpy as np
 import pytest
@@ -27,7 +31,9 @@ from protomol_b200 import systems, workloads
 pytestmark = pytest.mark.gpu
 
 MIXED_FORCE_RTOL = 1e-5
-MIXED_ENERGY_RTOL = 2e-6           # relative to |E_LJ| + |E_Coulomb|
+MIXED_ENERGY_RTOL = 1e-7           # relative to |E_LJ| + |E_Coulomb|
+COULOMB_ONLY_ENERGY_RTOL = 2e-6    # plain Coulomb or Coulomb alone, a few hundred atoms
+MIXED_VIRIAL_RTOL = 1e-6           # relative to the largest virial entry, a few hundred atoms
 MIXED_METRIC_ENERGY_RTOL = 1e-7    # the 14,281-atom cutoff + PME system, relative to |E_total|
 FP64_FORCE_RTOL = 1e-9
 FP64_ENERGY_RTOL = 1e-10
@@ -84,6 +90,11 @@ CASES = {
 }
 
 
+# the cases whose forces are plain Coulomb or Coulomb alone
+COULOMB_ONLY = {"water216_c2", "small_c2_fused", "small_c2lj_c1coul", "small_c2lj_shiftcoul",
+                "small_cutoff_coulomb", "small_pme_full"}
+
+
 def energy_scale(r):
     return abs(r["lennard_jones"]) + abs(r["coulomb"])
 
@@ -107,8 +118,9 @@ def test_forces_energies_virial_against_oracle(name, precision):
         assert rel_rms(f, ref["forces"]) <= MIXED_FORCE_RTOL
         etot = e.lennard_jones + e.coulomb
         rtot = ref["lennard_jones"] + ref["coulomb"]
-        assert abs(etot - rtot) <= MIXED_ENERGY_RTOL * scale
-        assert np.abs(e.virial_tensor - ref["virial"]).max() <= MIXED_ENERGY_RTOL * max(vscale, 1.0) * 10
+        etol = COULOMB_ONLY_ENERGY_RTOL if name in COULOMB_ONLY else MIXED_ENERGY_RTOL
+        assert abs(etot - rtot) <= etol * scale
+        assert np.abs(e.virial_tensor - ref["virial"]).max() <= MIXED_VIRIAL_RTOL * vscale
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -333,7 +345,7 @@ def test_million_atom_box_at_full_size():
     _, _, fd, ed = gpu_eval(s, w.forces, "fp64")
     assert np.isfinite(fm).all() and np.abs(fd).max() > 0
     assert rel_rms(fm, fd) <= MIXED_FORCE_RTOL
-    assert np.abs(em.virial_tensor - ed.virial_tensor).max() <= MIXED_ENERGY_RTOL * np.abs(ed.virial_tensor).max() * 10
+    assert np.abs(em.virial_tensor - ed.virial_tensor).max() <= MIXED_VIRIAL_RTOL * np.abs(ed.virial_tensor).max()
     etot, dtot = em.lennard_jones + em.coulomb, ed.lennard_jones + ed.coulomb
     print(f"\n1M: force rel RMS {rel_rms(fm, fd):.2e}  total energy rel {abs(etot - dtot) / abs(dtot):.2e}  "
           f"LJ rel {abs(em.lennard_jones - ed.lennard_jones) / abs(ed.lennard_jones):.2e}  virial frob rel "

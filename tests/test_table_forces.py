@@ -21,7 +21,15 @@ from protomol_b200 import forces as F
 from protomol_b200 import systems, workloads
 
 MIXED_FORCE_RTOL = 1e-5
-MIXED_ENERGY_RTOL = 2e-6           # relative to |E_LJ| + |E_Coulomb|
+# mixed, on the small systems here: the total energy within 1e-7 of
+# |E_LJ| + |E_Coulomb| and the virial within 1e-6 of its largest entry;
+# forces that are plain Coulomb or Coulomb alone 2e-6 on the energy (their
+# per-pair FP32 rounding is not averaged down over a few hundred atoms, and
+# a Coulomb-only total is a cancellation)
+MIXED_ENERGY_RTOL = 1e-7           # relative to |E_LJ| + |E_Coulomb|
+COULOMB_ONLY_ENERGY_RTOL = 2e-6
+MIXED_VIRIAL_RTOL = 1e-6           # relative to the largest virial entry
+COULOMB_ONLY = {"coulomb_shift", "coulomb_cutoff", "ewald", "ljt_coult"}
 MIXED_METRIC_ENERGY_RTOL = 1e-7    # the 14,281-atom system, relative to |E_total|
 FP64_FORCE_RTOL = 1e-9
 FP64_ENERGY_RTOL = 1e-10
@@ -129,7 +137,7 @@ def _gpu(system, defs, precision):
     return out, e
 
 
-def _check(system, defs, precision):
+def _check(system, defs, precision, etol=MIXED_ENERGY_RTOL):
     ref = oracle.evaluate(system, [F.parse_definition(d) for d in defs])
     f, e = _gpu(system, defs, precision)
     rms = np.sqrt((ref["forces"] ** 2).sum(1).mean())
@@ -143,8 +151,8 @@ def _check(system, defs, precision):
     else:
         err = np.sqrt(((f - ref["forces"]) ** 2).sum() / (ref["forces"] ** 2).sum())
         assert err <= MIXED_FORCE_RTOL, err
-        assert abs(e.lennard_jones + e.coulomb - ref["lennard_jones"] - ref["coulomb"]) <= MIXED_ENERGY_RTOL * scale
-        assert np.abs(e.virial_tensor - ref["virial"]).max() <= MIXED_ENERGY_RTOL * vscale * 10
+        assert abs(e.lennard_jones + e.coulomb - ref["lennard_jones"] - ref["coulomb"]) <= etol * scale
+        assert np.abs(e.virial_tensor - ref["virial"]).max() <= MIXED_VIRIAL_RTOL * vscale
     return ref, f, e
 
 
@@ -152,7 +160,8 @@ def _check(system, defs, precision):
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("case", sorted(DEFS))
 def test_table_forces_against_oracle(case, precision):
-    _check(_small_chain(), [DEFS[case]], precision)
+    _check(_small_chain(), [DEFS[case]], precision,
+           COULOMB_ONLY_ENERGY_RTOL if case in COULOMB_ONLY else MIXED_ENERGY_RTOL)
 
 
 @pytest.mark.gpu
