@@ -390,6 +390,27 @@ __global__ void __launch_bounds__(kColThreads) k_col_sort(ColBinArgs a)
         a.ibox[2 * (cl0 + q) + 1] = e1 ? h0 : make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
         a.ccol[cl0 + q] = c;
     }
+    // the column's z index for the list kernel's window searches: per bin
+    // edge z_b = b L_z / kZBins the first j-cluster whose box ends at or
+    // above z_b, and the first whose box starts above it (both corners are
+    // monotone along the column; empty halves sit at +3e38, at the end)
+    const float binw = g.lzf / kZBins;
+    int* zi = a.zidx + (size_t)c * kZIndex;
+    for (int b = t; b <= kZBins; b += kColThreads) {
+        const float zb = b * binw;
+        int lo = 0, hi = 2 * ncl;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (s_jb[2 * mid + 1].z < zb) lo = mid + 1; else hi = mid;
+        }
+        int lo2 = 0, hi2 = 2 * ncl;
+        while (lo2 < hi2) {
+            const int mid = (lo2 + hi2) >> 1;
+            if (s_jb[2 * mid].z > zb) hi2 = mid; else lo2 = mid + 1;
+        }
+        zi[b] = 2 * cl0 + lo;
+        zi[kZBins + 1 + b] = 2 * cl0 + lo2;
+    }
 }
 
 __global__ void __launch_bounds__(kBinThreads) k_col_refresh(ColBinArgs a, double half_skin2)

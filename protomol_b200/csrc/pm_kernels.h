@@ -59,6 +59,12 @@ struct ColGrid {
     float zext;                  // largest z extent of an i-cluster that keeps every tile's image unique
 };
 
+// z index of a column's j-clusters: kZBins bins of L_z / kZBins; per column
+// and bin edge b (0 .. kZBins) the first j-cluster whose box ends at or above
+// b L_z / kZBins, then the first whose box starts above it
+constexpr int kZBins = 64;
+constexpr int kZIndex = 2 * (kZBins + 1);   // ints per column
+
 struct ColBinArgs {
     int n;
     const double* pos;
@@ -83,6 +89,7 @@ struct ColBinArgs {
     float4* jbox;                // 2 per j-cluster
     int* ccol;                   // i-cluster -> column
     int4* corg;                  // i-cluster -> fixed-point position of its first atom (virial origin)
+    int* zidx;                   // kZIndex per column: the z index of its j-clusters
     int ncl_cap;                 // i-cluster capacity
     int* status;
 };
@@ -210,6 +217,7 @@ struct PairArgs {
     const int4* cm;
     const float4* ibox;
     const float4* jbox;
+    const int* zidx;             // kZIndex per column (ColBinArgs::zidx)
     const int* ccstart;          // ncol + 1
     const int* ccol;
     const int4* corg;            // virial origin of every i-cluster

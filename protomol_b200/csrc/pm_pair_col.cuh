@@ -51,23 +51,26 @@ __device__ __forceinline__ int col_entry_y(int tx, int ty, int tz, bool diag)
     return (tx + 1) | ((ty + 1) << 2) | ((tz + 1) << 4) | ((diag ? 1 : 0) << 6);
 }
 
-// the j-cluster range of one candidate column's image tz whose boxes may meet
+// the j-cluster range [jb, je) of column colj's image tz whose boxes may meet
 // the window [zlo, zhi] (in the box frame): j-boxes are sorted by z in a
-// column (both corners monotone), so two binary searches bound it
-__device__ __forceinline__ int2 col_zrange(const PairArgs& p, int jb, int je, float zlo, float zhi, float sz)
+// column (both corners monotone), so the column's z index gives a start at
+// or before each end of the range, and a short forward scan finds it
+__device__ __forceinline__ int2 col_zrange(const PairArgs& p, int colj, int jb, int je, float zlo, float zhi,
+                                           float sz)
 {
     const float plo = zlo - sz, phi = zhi - sz;          // the window in the column's frame [0, L)
     if (phi < 0.f || plo >= p.cg.lzf) return make_int2(jb, 0);
-    int lo = jb, hi = je;                                // first j-cluster ending at or above plo
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (p.jbox[2 * mid + 1].z < plo) lo = mid + 1; else hi = mid;
-    }
-    int lo2 = lo, hi2 = je;                              // first j-cluster starting above phi
-    while (lo2 < hi2) {
-        const int mid = (lo2 + hi2) >> 1;
-        if (p.jbox[2 * mid].z > phi) hi2 = mid; else lo2 = mid + 1;
-    }
+    const int* zi = p.zidx + (size_t)colj * kZIndex;
+    const float inv = kZBins / p.cg.lzf;
+    // first j-cluster ending at or above plo, from the bin edge one below
+    // plo's (the FP32 bin of plo may round up by one)
+    const int b0 = plo <= 0.f ? 0 : max(0, min(kZBins, (int)(plo * inv)) - 1);
+    int lo = max(jb, __ldg(zi + b0));
+    while (lo < je && p.jbox[2 * lo + 1].z < plo) ++lo;
+    // first j-cluster starting above phi, likewise from one bin edge below
+    const int b1 = max(0, min(kZBins, (int)(phi * inv)) - 1);
+    int lo2 = max(lo, __ldg(zi + kZBins + 1 + b1));
+    while (lo2 < je && p.jbox[2 * lo2].z <= phi) ++lo2;
     return make_int2(lo, lo2 - lo);
 }
 
@@ -117,7 +120,7 @@ __device__ int col_gather(const PairArgs& p, int ic, int col_i, const float4& il
 #pragma unroll
                 for (int z = 0; z < 3; ++z) {
                     const int tz = z - 1;
-                    const int2 r = col_zrange(p, jb, je, ilo.z - wz, ihi.z + wz, tz * g.lzf);
+                    const int2 r = col_zrange(p, colj, jb, je, ilo.z - wz, ihi.z + wz, tz * g.lzf);
                     part[z] = make_int4(r.x, r.y, col_entry_y(tx, ty, tz, false) | (own ? 1 << 7 : 0), 0);
                     cnt += r.y;
                 }

@@ -192,6 +192,7 @@ struct pmgpu_system {
     int* d_ccounts = nullptr;
     int* d_colstart = nullptr;
     int* d_ccstart = nullptr;
+    int* d_zidx = nullptr;          // z index of every column's j-clusters (kZIndex ints per column)
     int col_ncol_cap = 0;
     int4* d_cq = nullptr;
     int4* d_cm = nullptr;
@@ -388,7 +389,7 @@ static void free_atom_buffers(pmgpu_system* s)
 
 static void free_col_buffers(pmgpu_system* s)
 {
-    dfree(s->d_ccounts); dfree(s->d_colstart); dfree(s->d_ccstart);
+    dfree(s->d_ccounts); dfree(s->d_colstart); dfree(s->d_ccstart); dfree(s->d_zidx);
     dfree(s->d_cq); dfree(s->d_cm); dfree(s->d_ibox); dfree(s->d_jbox); dfree(s->d_ccol); dfree(s->d_facc32c);
     dfree(s->d_corg);
     s->col_ncol_cap = 0;
@@ -666,6 +667,7 @@ static int col_set_grid(pmgpu_system* sys)
         CK(dalloc(&sys->d_ccounts, g.ncol), "alloc");
         CK(dalloc(&sys->d_colstart, g.ncol + 1), "alloc");
         CK(dalloc(&sys->d_ccstart, g.ncol + 1), "alloc");
+        CK(dalloc(&sys->d_zidx, (size_t)g.ncol * kZIndex), "alloc");
         sys->col_ncol_cap = g.ncol;
     }
     // the binning returns the counts to zero; they start there
@@ -1448,7 +1450,7 @@ static int col_bin(pmgpu_system* sys, const double* d_pos)
     a.pbc = sys->pbc; a.grid = sys->grid; a.cell3 = sys->d_cell3;
     a.g = sys->eval_cg;
     a.qfix = sys->d_qfix; a.col = sys->d_colid; a.counts = sys->d_ccounts; a.done = sys->d_status + 9;
-    a.colstart = sys->d_colstart; a.ccstart = sys->d_ccstart; a.tmp = sys->d_ctmp;
+    a.colstart = sys->d_colstart; a.ccstart = sys->d_ccstart; a.tmp = sys->d_ctmp; a.zidx = sys->d_zidx;
     a.cq = sys->d_cq; a.cm = sys->d_cm; a.slot_of = sys->d_cslot;
     a.ibox = sys->d_ibox; a.jbox = sys->d_jbox; a.ccol = sys->d_ccol; a.ncl_cap = sys->col_ncl_cap;
     a.corg = sys->d_corg;
@@ -1477,6 +1479,7 @@ static void fill_col_args(pmgpu_system* sys, PairArgs& a)
 {
     a.cq = sys->d_cq; a.cm = sys->d_cm; a.ibox = sys->d_ibox; a.jbox = sys->d_jbox;
     a.ccstart = sys->d_ccstart; a.ccol = sys->d_ccol; a.icl_cap = sys->col_ncl_cap; a.corg = sys->d_corg;
+    a.zidx = sys->d_zidx;
     a.clist = (int4*)sys->d_plist;          // entries of two int2 places each (plist_cap counts int2)
     a.cg = sys->eval_cg;
     a.qorig = sys->d_q; a.torig = sys->d_type;
