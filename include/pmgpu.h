@@ -317,6 +317,13 @@ int pmgpu_batch_add(pmgpu_batch* batch, pmgpu_system* sys, int n_forces, pmgpu_f
 /* One graph launch of every member's evaluation, asynchronous on the batch's
  * stream (pmgpu_batch_stream). */
 int pmgpu_batch_evaluate(pmgpu_batch* batch);
+/* one_launch = 1 (the default): the members' column-path mixed cutoff
+ * forces run their pair kernels as ONE persistent launch over every
+ * member's (system, chunk) work items, between the members' own lists and
+ * the rest of their evaluations (members must be distinct systems; up to
+ * 1024); 0: each member's pair kernel on its own stream.  The results are
+ * the same bit for bit; the next evaluation recaptures the graph. */
+int pmgpu_batch_set_pair_launch(pmgpu_batch* batch, int one_launch);
 /* Waits for the batch and reports the first member failure (for
  * PMGPU_ERR_CAPACITY, the member's list has been grown: evaluate again). */
 int pmgpu_batch_synchronize(pmgpu_batch* batch);

@@ -30,7 +30,8 @@ EXPORTS = [
     "pmgpu_set_pair_list", "pmgpu_pair_list_builds", "pmgpu_set_molecule_positions",
     "pmgpu_set_profiling", "pmgpu_phase_times", "pmgpu_pme_reciprocal_static",
     "pmgpu_batch_create", "pmgpu_batch_destroy", "pmgpu_batch_add", "pmgpu_batch_evaluate",
-    "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_adjoint",
+    "pmgpu_batch_synchronize", "pmgpu_batch_last_error", "pmgpu_batch_stream", "pmgpu_batch_set_pair_launch",
+    "pmgpu_adjoint",
     "pmgpu_full_create", "pmgpu_lookup_table", "pmgpu_get_tuning", "pmgpu_set_tuning", "pmgpu_autotune", "pmgpu_batch_autotune",
     "pmgpu_leapfrog_run", "pmgpu_hessian", "pmgpu_impulse_run", "pmgpu_set_constraints",
     "pmgpu_constraint_limit_hits",
@@ -123,6 +124,7 @@ def load():
     lib.pmgpu_batch_destroy.argtypes = [vp]
     lib.pmgpu_batch_add.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp, C.c_uint]
     lib.pmgpu_batch_evaluate.argtypes = [vp]
+    lib.pmgpu_batch_set_pair_launch.argtypes = [vp, C.c_int]
     lib.pmgpu_batch_synchronize.argtypes = [vp]
     lib.pmgpu_batch_last_error.argtypes = [vp, C.c_char_p, C.c_int]
     lib.pmgpu_batch_stream.argtypes = [vp]

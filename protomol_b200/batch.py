@@ -83,6 +83,11 @@ class Batch:
     def evaluate(self):
         self._check(self.lib.pmgpu_batch_evaluate(self.handle))
 
+    def set_pair_launch(self, one_launch: bool):
+        """pmgpu_batch_set_pair_launch: the members' column-path pair kernels
+        as one persistent launch (True, the default) or one per member."""
+        self._check(self.lib.pmgpu_batch_set_pair_launch(self.handle, 1 if one_launch else 0))
+
     def autotune(self, evals: int = 5) -> dict:
         """pmgpu_batch_autotune: one tuning for every member, timed as whole
         batch launches; the members' outputs are zeroed afterwards."""

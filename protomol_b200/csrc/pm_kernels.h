@@ -244,6 +244,15 @@ int launch_near_energy(const PairArgs& a, int combo, int n_atoms, cudaStream_t s
 // K2a' / K2b' / K2c': the column-cluster list, pair kernel and near-pair energies
 int launch_col_list(const PairArgs& a, cudaStream_t s, long long* launches);
 int launch_pair_col(const PairArgs& a, int combo, cudaStream_t s, long long* launches);
+// K11: the column-path pair kernels of up to kBatchPairMax systems (a
+// batch's members, the same combination of terms) as one persistent launch
+constexpr int kBatchPairMax = 1024;
+struct BatchPairArgs {
+    const PairArgs* args;        // device copy of every member's pair arguments
+    int n;
+    int* next;                   // work counter (zero before the launch)
+};
+int launch_pair_col_batch(const BatchPairArgs& b, int combo, cudaStream_t s, long long* launches);
 int launch_near_energy_col(const PairArgs& a, int combo, int n_atoms, cudaStream_t s, long long* launches);
 long long col_list_estimate(int n_atoms, const ColGrid& g, double volume, double cutoff);
 long long col_chunk_estimate(long long entries, int n_atoms, const ColGrid& g, int chunk);

@@ -975,6 +975,58 @@ int launch_pair_col(const PairArgs& a, int combo, cudaStream_t s, long long* lau
     }
 }
 
+template <int NT, int P0, int S0, int P1, int S1>
+static int run_col_batch(const BatchPairArgs& b, cudaStream_t s, long long* launches)
+{
+    static int sms = 0, per_sm = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_col_batch<NT, P0, S0, P1, S1>, 128, 0);
+        if (sms <= 0) sms = 148;
+        if (per_sm <= 0) per_sm = 1;
+    }
+    k_pair_col_batch<NT, P0, S0, P1, S1><<<sms * per_sm, 128, 0, s>>>(b);
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
+
+int launch_pair_col_batch(const BatchPairArgs& b, int combo, cudaStream_t s, long long* launches)
+{
+    if (b.n < 1 || b.n > kBatchPairMax) return (int)cudaErrorInvalidValue;
+    switch (combo) {
+#define PM_COLB_CASE(ID, ...) case ID: return run_col_batch<__VA_ARGS__>(b, s, launches);
+    PM_COLB_CASE(0, 1, CO, SC1, NP, SUN)
+    PM_COLB_CASE(1, 1, CO, SC2, NP, SUN)
+    PM_COLB_CASE(2, 1, CO, SCUT, NP, SUN)
+    PM_COLB_CASE(3, 1, CO, SSH, NP, SUN)
+    PM_COLB_CASE(4, 1, EW, SCUT, NP, SUN)
+    PM_COLB_CASE(5, 1, LJ, SC1, NP, SUN)
+    PM_COLB_CASE(6, 1, LJ, SC2, NP, SUN)
+    PM_COLB_CASE(7, 1, LJ, SCUT, NP, SUN)
+    PM_COLB_CASE(8, 1, LJ, SSH, NP, SUN)
+    PM_COLB_CASE(9, 2, LJ, SC1, EW, SCUT)
+    PM_COLB_CASE(10, 2, LJ, SC1, CO, SSH)
+    PM_COLB_CASE(11, 2, LJ, SC2, CO, SC1)
+    PM_COLB_CASE(12, 2, LJ, SC2, EW, SCUT)
+    PM_COLB_CASE(13, 2, LJ, SC2, CO, SCUT)
+    PM_COLB_CASE(14, 2, LJ, SC2, CO, SSH)
+    PM_COLB_CASE(15, 2, LJ, SCUT, EW, SCUT)
+    PM_COLB_CASE(16, 2, LJ, SC2, CO, SC2)
+    PM_COLB_CASE(17, 1, LJT, SUN, NP, SUN)
+    PM_COLB_CASE(18, 1, COT, SUN, NP, SUN)
+    PM_COLB_CASE(19, 1, EWT, SUN, NP, SUN)
+    PM_COLB_CASE(20, 2, LJ, SC1, EWT, SUN)
+    PM_COLB_CASE(21, 2, LJ, SC2, EWT, SUN)
+    PM_COLB_CASE(22, 2, LJ, SCUT, EWT, SUN)
+    PM_COLB_CASE(23, 2, LJT, SUN, EWT, SUN)
+    PM_COLB_CASE(24, 2, LJT, SUN, COT, SUN)
+#undef PM_COLB_CASE
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
 int launch_near_energy_col(const PairArgs& a, int combo, int n_atoms, cudaStream_t s, long long* launches)
 {
     static int sms = 0;

@@ -290,9 +290,11 @@ __device__ __forceinline__ void col_tile_of(const PairArgs& p, const int4& c, bo
     }
 }
 
-__device__ __forceinline__ int4 col_entry(const PairArgs& p, int e, int e_end)
+template <bool SH>
+__device__ __forceinline__ int4 col_entry(const int4* ents, int e, int e_end)
 {
-    return e < e_end ? __ldg(p.clist + e) : make_int4(0, 0, 0, 0);
+    if (e >= e_end) return make_int4(0, 0, 0, 0);
+    return SH ? ents[e] : __ldg(ents + e);
 }
 
 __device__ __forceinline__ JAtom col_atom(const int4& P, const int4& M)
@@ -302,6 +304,142 @@ __device__ __forceinline__ JAtom col_atom(const int4& P, const int4& M)
     a.l = make_float4(0.f, 0.f, 0.f, __int_as_float(M.w));
     a.m = make_int4(M.x, M.y, M.z, 0);
     return a;
+}
+
+// One i-cluster's run of list entries [e_begin, e_end) of ents (the global
+// list, or entries in shared memory: SH), two tiles per iteration: the tile
+// loop of K2b'.  Adds the j-forces and, at the end, the i-forces; queues the
+// near pairs (flushed at the end) and adds the run's energies and tile virial
+// to the lane's int64 sums acc.
+template <bool SH, int NT, int P0, int S0, int P1, int S1>
+__device__ __forceinline__ void col_run(const PairArgs& p, int ic, const int4* ents, int e_begin, int e_end,
+                                        int2* s_near, long long (&acc)[5], bool& bad)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, il = lane & 7, jj = lane >> 3;
+    // after the reduce-scatter lane il (< 6) holds component il % 3 of the
+    // j-force of tile A's (il < 3) or tile B's (il >= 3) j-atom jj
+    const bool holds = il < 6, onB = il >= 3;
+    const int comp = il < 3 ? il : il - 3;
+    const int si = 8 * ic + il;
+    const int4 Pi = p.cq[si], Mi = p.cm[si];
+    const JAtom ia = col_atom(Pi, Mi);
+    const bool vi = Mi.x >= 0;
+    float fix = 0.f, fiy = 0.f, fiz = 0.f;
+    double el = 0.0, ec = 0.0;
+    // the far pairs' FP32 energies summed over up to kEnergyFlush
+    // iterations in FP32, then into the FP64 sums
+    float elf = 0.f, ecf = 0.f;
+    int nacc = 0;
+    double wv[3] = {0.0, 0.0, 0.0};
+    int nq = 0;
+    // software pipeline: the entries two iterations ahead, the j-atoms of
+    // the next iteration's tiles one ahead
+    ColTile nA, nB;
+    col_tile_of(p, col_entry<SH>(ents, e_begin, e_end), true, jj, nA);
+    col_tile_of(p, col_entry<SH>(ents, e_begin + 1, e_end), e_begin + 1 < e_end, jj, nB);
+    int4 qA = col_entry<SH>(ents, e_begin + 2, e_end), qB = col_entry<SH>(ents, e_begin + 3, e_end);
+    for (int e = e_begin; e < e_end; e += 2) {
+        if (nq > kNearCap - 64) {                  // room for one more pair of tiles
+            append_near(p, s_near, nq, lane);
+            nq = 0;
+        }
+        const ColTile tA = nA, tB = nB;
+        const bool hasB = e + 1 < e_end;           // warp-uniform
+        if (e + 2 < e_end) {
+            col_tile_of(p, qA, true, jj, nA);
+            col_tile_of(p, qB, e + 3 < e_end, jj, nB);
+            qA = col_entry<SH>(ents, e + 4, e_end);
+            qB = col_entry<SH>(ents, e + 5, e_end);
+        }
+        const JAtom ja = col_atom(tA.P, tA.M), jb = col_atom(tB.P, tB.M);
+        const bool va = vi && ja.m.x >= 0 && (!tA.diag || 4 * (tA.jc & 1) + jj > il);
+        const bool vb = hasB && vi && jb.m.x >= 0 && (!tB.diag || 4 * (tB.jc & 1) + jj > il);
+        PairGeo ga = col_geo<NT, S0, S1>(p, Pi, tA.P, va, ia.m.z, ja.m.z);
+        PairGeo gb = col_geo<NT, S0, S1>(p, Pi, tB.P, vb, ia.m.z, jb.m.z);
+        if (__any_sync(FULL, is_rare(ga) || is_rare(gb))) {   // warp-uniform, rare
+            resolve_rare<NT>(p, ga, ia, ja);
+            resolve_rare<NT>(p, gb, ia, jb);
+        }
+        const bool any_a = __any_sync(FULL, ga.act), any_b = __any_sync(FULL, gb.act);
+        if (!(any_a || any_b)) continue;
+        float fta = 0.f, ela = 0.f, eca = 0.f, ftb = 0.f, elb = 0.f, ecb = 0.f;
+        if (any_a && any_b) {
+            pair_math<NT, P0, S0, P1, S1>(p, ga, ia, ja, fta, ela, eca);
+            pair_math<NT, P0, S0, P1, S1>(p, gb, ia, jb, ftb, elb, ecb);
+        } else {
+            float ft, e1, e2;
+            pair_math<NT, P0, S0, P1, S1>(p, any_a ? ga : gb, ia, any_a ? ja : jb, ft, e1, e2);
+            if (any_a) { fta = ft; ela = e1; eca = e2; } else { ftb = ft; elb = e1; ecb = e2; }
+        }
+        const float xa = ga.dx * fta, ya = ga.dy * fta, za = ga.dz * fta;
+        const float xb = gb.dx * ftb, yb = gb.dy * ftb, zb = gb.dz * ftb;
+        fix -= xa + xb; fiy -= ya + yb; fiz -= za + zb;
+        // near pairs: queued (original indices) for FP64 energies in place of the FP32 ones
+        {
+            const bool na = ga.act && ga.r2 < p.near2, nb = gb.act && gb.r2 < p.near2;   // near2 = 0: none
+            if (__any_sync(FULL, na || nb)) {
+                const unsigned ba = __ballot_sync(FULL, na), bb = __ballot_sync(FULL, nb);
+                const unsigned lt = (1u << lane) - 1u;
+                if (na) {
+                    s_near[nq + __popc(ba & lt)] =
+                        make_int2(ia.m.x, ja.m.x | (ga.excl == PMGPU_EXCL_MODIFIED ? 1 << 30 : 0));
+                    ela = 0.f; eca = 0.f;
+                }
+                nq += __popc(ba);
+                if (nb) {
+                    s_near[nq + __popc(bb & lt)] =
+                        make_int2(ia.m.x, jb.m.x | (gb.excl == PMGPU_EXCL_MODIFIED ? 1 << 30 : 0));
+                    elb = 0.f; ecb = 0.f;
+                }
+                nq += __popc(bb);
+            }
+        }
+        elf += ela + elb;
+        ecf += eca + ecb;
+        if (++nacc == kEnergyFlush) {
+            el += (double)elf;
+            ec += (double)ecf;
+            elf = 0.f; ecf = 0.f; nacc = 0;
+        }
+        // j-forces of both tiles: lane il < 6 ends with one component
+        const float v = j_reduce_scatter(xa, ya, za, xb, yb, zb, il);
+        if (holds && v != 0.f)
+            fixed_addf(p.facc + 3 * (4 * (size_t)(onB ? tB.jc : tA.jc) + jj) + comp, v, p.status);
+        if (p.virial && holds) {                       // o (x) F_tile, column comp
+            const float ox = onB ? tB.ox : tA.ox, oy = onB ? tB.oy : tA.oy, oz = onB ? tB.oz : tA.oz;
+            wv[0] += (double)(ox * v);
+            wv[1] += (double)(oy * v);
+            wv[2] += (double)(oz * v);
+        }
+        if (p.rec_pairs) {                             // diagnostic pair recording
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const PairGeo& g = t ? gb : ga;
+                const JAtom& j = t ? jb : ja;
+                if (g.act) {
+                    const unsigned long long r = atomicAdd(p.rec_count, 1ull);
+                    if ((long long)r < p.rec_cap) {
+                        p.rec_pairs[2 * r] = min(ia.m.x, j.m.x);
+                        p.rec_pairs[2 * r + 1] = max(ia.m.x, j.m.x);
+                    }
+                }
+            }
+        }
+    }
+    el += (double)elf;
+    ec += (double)ecf;
+    // chunk end: i-forces (lanes jj = 0, 1, 2 hold component jj of i-atom il)
+    const float vi3 = i_reduce_scatter(fix, fiy, fiz, jj);
+    if (jj < 3 && vi && vi3 != 0.f) fixed_addf(p.facc + 3 * (size_t)si + jj, vi3, p.status);
+    if (nq > 0) append_near(p, s_near, nq, lane);
+    acc[0] += fixed_of(el, bad);
+    acc[1] += fixed_of(ec, bad);
+    if (p.virial) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc[2 + a] += fixed_of(wv[a], bad);
+    }
+    __syncwarp();
 }
 
 // Two 8 x 4 tiles (consecutive entries A and B of the chunk) per iteration:
@@ -328,138 +466,16 @@ __global__ void __launch_bounds__(128, 5) k_pair_col(PairArgs p)
     const bool list_bad = (*p.status & (kStatusListFull | kStatusColumns)) || *p.plist_need != 0 || *p.chunk_need != 0;
     if (list_bad && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(p.status, kStatusListFull);
     const int nchunks = list_bad ? 0 : min(*p.chunk_count, p.chunk_cap);
-    // after the reduce-scatter lane il (< 6) holds component il % 3 of the
-    // j-force of tile A's (il < 3) or tile B's (il >= 3) j-atom jj
-    const bool holds = il < 6, onB = il >= 3;
+    // lane il (< 6) holds component il % 3 of a j-force (col_run)
+    const bool holds = il < 6;
     const int comp = il < 3 ? il : il - 3;
-
     while (true) {
         int ch = 0;
         if (lane == 0) ch = atomicAdd(p.chunk_next, 1);
         ch = __shfl_sync(FULL, ch, 0);
         if (ch >= nchunks) break;
         const int4 cd = p.chunks[ch];
-        const int ic = cd.x;
-        const int si = 8 * ic + il;
-        const int4 Pi = p.cq[si], Mi = p.cm[si];
-        const JAtom ia = col_atom(Pi, Mi);
-        const bool vi = Mi.x >= 0;
-        float fix = 0.f, fiy = 0.f, fiz = 0.f;
-        double el = 0.0, ec = 0.0;
-        // the far pairs' FP32 energies summed over up to kEnergyFlush
-        // iterations in FP32, then into the FP64 sums
-        float elf = 0.f, ecf = 0.f;
-        int nacc = 0;
-        double wv[3] = {0.0, 0.0, 0.0};
-        int nq = 0;
-        const int e_end = cd.z + cd.w;
-        // software pipeline: the entries two iterations ahead, the j-atoms of
-        // the next iteration's tiles one ahead
-        ColTile nA, nB;
-        col_tile_of(p, col_entry(p, cd.z, e_end), true, jj, nA);
-        col_tile_of(p, col_entry(p, cd.z + 1, e_end), cd.z + 1 < e_end, jj, nB);
-        int4 qA = col_entry(p, cd.z + 2, e_end), qB = col_entry(p, cd.z + 3, e_end);
-        for (int e = cd.z; e < e_end; e += 2) {
-            if (nq > kNearCap - 64) {                  // room for one more pair of tiles
-                append_near(p, s_near[w], nq, lane);
-                nq = 0;
-            }
-            const ColTile tA = nA, tB = nB;
-            const bool hasB = e + 1 < e_end;           // warp-uniform
-            if (e + 2 < e_end) {
-                col_tile_of(p, qA, true, jj, nA);
-                col_tile_of(p, qB, e + 3 < e_end, jj, nB);
-                qA = col_entry(p, e + 4, e_end);
-                qB = col_entry(p, e + 5, e_end);
-            }
-            const JAtom ja = col_atom(tA.P, tA.M), jb = col_atom(tB.P, tB.M);
-            const bool va = vi && ja.m.x >= 0 && (!tA.diag || 4 * (tA.jc & 1) + jj > il);
-            const bool vb = hasB && vi && jb.m.x >= 0 && (!tB.diag || 4 * (tB.jc & 1) + jj > il);
-            PairGeo ga = col_geo<NT, S0, S1>(p, Pi, tA.P, va, ia.m.z, ja.m.z);
-            PairGeo gb = col_geo<NT, S0, S1>(p, Pi, tB.P, vb, ia.m.z, jb.m.z);
-            if (__any_sync(FULL, is_rare(ga) || is_rare(gb))) {   // warp-uniform, rare
-                resolve_rare<NT>(p, ga, ia, ja);
-                resolve_rare<NT>(p, gb, ia, jb);
-            }
-            const bool any_a = __any_sync(FULL, ga.act), any_b = __any_sync(FULL, gb.act);
-            if (!(any_a || any_b)) continue;
-            float fta = 0.f, ela = 0.f, eca = 0.f, ftb = 0.f, elb = 0.f, ecb = 0.f;
-            if (any_a && any_b) {
-                pair_math<NT, P0, S0, P1, S1>(p, ga, ia, ja, fta, ela, eca);
-                pair_math<NT, P0, S0, P1, S1>(p, gb, ia, jb, ftb, elb, ecb);
-            } else {
-                float ft, e1, e2;
-                pair_math<NT, P0, S0, P1, S1>(p, any_a ? ga : gb, ia, any_a ? ja : jb, ft, e1, e2);
-                if (any_a) { fta = ft; ela = e1; eca = e2; } else { ftb = ft; elb = e1; ecb = e2; }
-            }
-            const float xa = ga.dx * fta, ya = ga.dy * fta, za = ga.dz * fta;
-            const float xb = gb.dx * ftb, yb = gb.dy * ftb, zb = gb.dz * ftb;
-            fix -= xa + xb; fiy -= ya + yb; fiz -= za + zb;
-            // near pairs: queued (original indices) for FP64 energies in place of the FP32 ones
-            {
-                const bool na = ga.act && ga.r2 < p.near2, nb = gb.act && gb.r2 < p.near2;   // near2 = 0: none
-                if (__any_sync(FULL, na || nb)) {
-                    const unsigned ba = __ballot_sync(FULL, na), bb = __ballot_sync(FULL, nb);
-                    const unsigned lt = (1u << lane) - 1u;
-                    if (na) {
-                        s_near[w][nq + __popc(ba & lt)] =
-                            make_int2(ia.m.x, ja.m.x | (ga.excl == PMGPU_EXCL_MODIFIED ? 1 << 30 : 0));
-                        ela = 0.f; eca = 0.f;
-                    }
-                    nq += __popc(ba);
-                    if (nb) {
-                        s_near[w][nq + __popc(bb & lt)] =
-                            make_int2(ia.m.x, jb.m.x | (gb.excl == PMGPU_EXCL_MODIFIED ? 1 << 30 : 0));
-                        elb = 0.f; ecb = 0.f;
-                    }
-                    nq += __popc(bb);
-                }
-            }
-            elf += ela + elb;
-            ecf += eca + ecb;
-            if (++nacc == kEnergyFlush) {
-                el += (double)elf;
-                ec += (double)ecf;
-                elf = 0.f; ecf = 0.f; nacc = 0;
-            }
-            // j-forces of both tiles: lane il < 6 ends with one component
-            const float v = j_reduce_scatter(xa, ya, za, xb, yb, zb, il);
-            if (holds && v != 0.f)
-                fixed_addf(p.facc + 3 * (4 * (size_t)(onB ? tB.jc : tA.jc) + jj) + comp, v, p.status);
-            if (p.virial && holds) {                       // o (x) F_tile, column comp
-                const float ox = onB ? tB.ox : tA.ox, oy = onB ? tB.oy : tA.oy, oz = onB ? tB.oz : tA.oz;
-                wv[0] += (double)(ox * v);
-                wv[1] += (double)(oy * v);
-                wv[2] += (double)(oz * v);
-            }
-            if (p.rec_pairs) {                             // diagnostic pair recording
-#pragma unroll
-                for (int t = 0; t < 2; ++t) {
-                    const PairGeo& g = t ? gb : ga;
-                    const JAtom& j = t ? jb : ja;
-                    if (g.act) {
-                        const unsigned long long r = atomicAdd(p.rec_count, 1ull);
-                        if ((long long)r < p.rec_cap) {
-                            p.rec_pairs[2 * r] = min(ia.m.x, j.m.x);
-                            p.rec_pairs[2 * r + 1] = max(ia.m.x, j.m.x);
-                        }
-                    }
-                }
-            }
-        }
-        el += (double)elf;
-        ec += (double)ecf;
-        // chunk end: i-forces (lanes jj = 0, 1, 2 hold component jj of i-atom il)
-        const float vi3 = i_reduce_scatter(fix, fiy, fiz, jj);
-        if (jj < 3 && vi && vi3 != 0.f) fixed_addf(p.facc + 3 * (size_t)si + jj, vi3, p.status);
-        if (nq > 0) append_near(p, s_near[w], nq, lane);
-        acc[0] += fixed_of(el, bad);
-        acc[1] += fixed_of(ec, bad);
-        if (p.virial) {
-#pragma unroll
-            for (int a = 0; a < 3; ++a) acc[2 + a] += fixed_of(wv[a], bad);
-        }
-        __syncwarp();
+        col_run<false, NT, P0, S0, P1, S1>(p, cd.x, p.clist, cd.z, cd.z + cd.w, s_near[w], acc, bad);
     }
     if (bad) atomicOr(p.status, kStatusOverflow);
 #pragma unroll
@@ -484,6 +500,98 @@ __global__ void __launch_bounds__(128, 5) k_pair_col(PairArgs p)
     }
     __syncthreads();
     if (threadIdx.x < kERec && s_e[threadIdx.x] != 0ull) atomicAdd(p.efix + threadIdx.x, s_e[threadIdx.x]);
+}
+
+// The lanes' int64 sums (acc) of one system into its energy words, at once
+// (the batch kernel: the warp leaves the system)
+__device__ __forceinline__ void col_warp_sums(const PairArgs& p, long long (&acc)[5], bool& bad)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, il = lane & 7, jj = lane >> 3;
+    const int comp = il < 3 ? il : il - 3;
+    if (bad && lane == 0) atomicOr(p.status, kStatusOverflow);
+    bad = __any_sync(FULL, bad) && false;
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+        for (int o = 16; o > 0; o >>= 1) acc[t] += __shfl_xor_sync(FULL, acc[t], o);
+    if (lane == 0) {
+        if (acc[0] != 0) atomicAdd(p.efix + 0, (unsigned long long)acc[0]);
+        if (acc[1] != 0) atomicAdd(p.efix + 1, (unsigned long long)acc[1]);
+    }
+    if (p.virial) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            acc[2 + a] += __shfl_xor_sync(FULL, acc[2 + a], 8);
+            acc[2 + a] += __shfl_xor_sync(FULL, acc[2 + a], 16);
+        }
+        if (il < 6 && jj == 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                if (acc[2 + a] != 0) atomicAdd(p.efix + 2 + 3 * a + comp, (unsigned long long)acc[2 + a]);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 5; ++t) acc[t] = 0;
+}
+
+// K11: the column-path pair kernels of a batch's members as one persistent
+// launch over (member, chunk) work items.  Every member's list was built by
+// its own K2a' launch before this one.  Each block prefix-sums the members'
+// chunk counts in shared memory (a member whose list is incomplete counts
+// none and is marked as K2b' marks it); a warp takes items from one counter,
+// copies its member's arguments into shared memory when the member changes,
+// runs the chunk (col_run, the K2b' tile loop) and adds its sums to the
+// member's energy words when it leaves the member.  Nothing waits on
+// another launch: the graph orders this one after every member's list.
+template <int NT, int P0, int S0, int P1, int S1>
+__global__ void __launch_bounds__(128, 4) k_pair_col_batch(BatchPairArgs b)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __shared__ int2 s_near[4][kNearCap];
+    __shared__ int s_pre[kBatchPairMax + 1];
+    __shared__ PairArgs s_args[4];
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int m = 0; m < b.n; ++m) {
+            const PairArgs& p = b.args[m];
+            s_pre[m] = t;
+            const bool list_bad = (*p.status & (kStatusListFull | kStatusColumns)) || *p.plist_need != 0 ||
+                                  *p.chunk_need != 0;
+            if (list_bad && blockIdx.x == 0) atomicOr(p.status, kStatusListFull);
+            t += list_bad ? 0 : min(*p.chunk_count, p.chunk_cap);
+        }
+        s_pre[b.n] = t;
+    }
+    __syncthreads();
+    const int total = s_pre[b.n];
+    long long acc[5] = {0, 0, 0, 0, 0};
+    bool bad = false;
+    int cur = -1;
+    const PairArgs& p = s_args[w];
+    while (true) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(b.next, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= total) break;
+        int lo = 0, hi = b.n;                         // the member: s_pre[lo] <= item < s_pre[lo + 1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_pre[mid] <= item) lo = mid; else hi = mid;
+        }
+        if (lo != cur) {
+            if (cur >= 0) col_warp_sums(p, acc, bad);
+            __syncwarp();
+            const int* src = reinterpret_cast<const int*>(b.args + lo);
+            int* dst = reinterpret_cast<int*>(&s_args[w]);
+            for (int i = lane; i < (int)(sizeof(PairArgs) / sizeof(int)); i += 32) dst[i] = src[i];
+            __syncwarp();
+            cur = lo;
+        }
+        const int4 cd = p.chunks[item - s_pre[lo]];
+        col_run<false, NT, P0, S0, P1, S1>(p, cd.x, p.clist, cd.z, cd.z + cd.w, s_near[w], acc, bad);
+    }
+    if (cur >= 0) col_warp_sums(p, acc, bad);
 }
 
 // FP64 energies of one pair of atoms by original index: the FP64 kernel's

@@ -1723,69 +1723,82 @@ static void prof_end(pmgpu_system* sys, int m)
     cudaEventRecord(sys->prof_marks[m].e, sys->stream);
 }
 
-// Only asynchronous work on the system's stream (capturable in a graph).
-static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, const double* d_pos,
-                        double* d_fout, double* d_energy, unsigned flags)
-{
-    int virial = (flags & PMGPU_FLAG_VIRIAL) ? 1 : 0;
-    const bool molvir = (flags & PMGPU_FLAG_MOLECULAR_VIRIAL) != 0;
+// One evaluation's enqueue, in parts, so that a batch can run its members'
+// column-path pair kernels as one launch between them: run_begin (memsets,
+// the PME branch, binning, all-pairs forces), run_cutoffs (the cutoff
+// forces in order; with may_defer, the first column-path mixed force stops
+// after its list, its arguments left in dargs), run_resume (that force's
+// near pairs after the batch's pair kernel, the remaining cutoff forces,
+// run_end) and run_end (molecular virial, PME join, finalize, energy
+// reduction).  Only asynchronous work on the system's stream (capturable
+// in a graph).
+struct EvalRun {
+    pmgpu_system* sys = nullptr;
+    int nf = 0;
+    pmgpu_force* const* forces = nullptr;
+    const double* d_pos = nullptr;
+    double* d_fout = nullptr;
+    double* d_energy = nullptr;
+    unsigned flags = 0;
+    int virial = 0;
+    bool molvir = false;
     int mused = 0;                      // molecular virial records
     MolvirFinish mf;
-    memset(&mf, 0, sizeof(mf));
     bool use32 = false, use40 = false;
-    for (int k = 0; k < nf; ++k) (pairs64(sys, forces[k]) ? use40 : use32) = true;
-    int r;
-    cudaStream_t s = sys->stream;
-    size_t n3 = 3 * (size_t)sys->n;
-    int mbin = prof_begin(sys, kPhaseBin);
-    if (sys->eval_reuse) {
-        // the list's counts (ints 1-4) stay; the status, the work counter,
-        // the near-pair counts, the binning counters and the sums start at zero
-        CK(cudaMemsetAsync(sys->d_small, 0, sizeof(int), s), "memset");
-        CK(cudaMemsetAsync((char*)sys->d_small + 5 * sizeof(int), 0, kSmallBytes - 5 * sizeof(int), s), "memset");
-    } else {
-        CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
-    }
+    size_t n3 = 0;
+    int mbin = -1;
     bool any_cut = false, any_pme = false, any_full = false;
-    bool atom_mixed = false, atom_fp64 = false;        // PME / all-pairs forces of each precision
-    for (int k = 0; k < nf; ++k) {
-        any_cut |= forces[k]->kind == 0;
-        any_pme |= forces[k]->kind == 1;
-        any_full |= forces[k]->kind == 2;
-        if (forces[k]->kind != 0) (pairs64(sys, forces[k]) ? atom_fp64 : atom_mixed) = true;
-    }
-    const bool use_col = sys->eval_use_col;
-    // the cell-ordered mixed accumulators serve the cell path's mixed cutoff
-    // forces only; the atom-ordered ones (mixed half, FP64 half) PME and the
-    // all-pairs forces of that precision
-    bool mixed_cells = false;
-    for (int k = 0; k < nf; ++k)
-        if (forces[k]->kind == 0 && !pairs64(sys, forces[k]) && !use_col) mixed_cells = true;
-    if (mixed_cells) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
-    if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
-    if (atom_mixed) CK(cudaMemsetAsync(sys->d_faccA, 0, sizeof(unsigned long long) * n3, s), "memset");
-    if (atom_fp64) CK(cudaMemsetAsync(sys->d_faccA + n3, 0, sizeof(unsigned long long) * n3, s), "memset");
-    for (int k = 0; k < nf; ++k)
-        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64)
-            sys->last_layout = pairs64(sys, forces[k]) ? PMGPU_LAYOUT_FP64
-                             : (use_col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS);
-    if (use_col)
-        CK(cudaMemsetAsync(sys->d_facc32c, 0, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap, s),
-           "memset");
-    // the cell-sorted order: for the FP64 cutoff forces, and for the mixed
-    // ones when the column path does not take them
-    bool cell_sort = false;
-    for (int k = 0; k < nf; ++k)
-        if (forces[k]->kind == 0 && (pairs64(sys, forces[k]) || !use_col)) cell_sort = true;
-    // the molecular virial kernels of the cutoff forces read the cell-sorted
-    // order too (binned for them alone on the column path)
-    const bool mv_bin = molvir && any_cut && !cell_sort;
-    int used = 0;
-    // PME: reads only positions and charges and accumulates in atom order.
-    // Beside the pair kernels (branches = true) the correction term and the
-    // FP64 energy transform of a mixed force run on branches of their own,
-    // joined back into ps at the end.
-    auto enqueue_pme = [&](cudaStream_t ps, bool branches) -> int {
+    bool use_col = false, mixed_cells = false, cell_sort = false, mv_bin = false;
+    bool fork = false;                  // PME on the side stream beside the pair kernels
+    bool near_on_side = false;
+    int used = 0;                       // energy records
+    int last_mixed = -1;                // the last mixed cutoff force (its near pairs may go to the side stream)
+    int lists = 0;
+    int pair_virial = 0, col_virial = 0;
+    int k_next = 0;                     // the next force run_cutoffs looks at
+    int deferred = -1;                  // the force whose pair kernel a batch runs
+    PairArgs dargs;                     // its arguments
+};
+
+// the names of one evaluation's state (EvalRun) inside its parts
+#define PM_EVAL_RUN_NAMES(R)                                                                              \
+    [[maybe_unused]] pmgpu_system* sys = (R).sys;                                                        \
+    [[maybe_unused]] const int nf = (R).nf;                                                              \
+    [[maybe_unused]] pmgpu_force* const* forces = (R).forces;                                            \
+    [[maybe_unused]] const double* d_pos = (R).d_pos;                                                    \
+    [[maybe_unused]] double* d_fout = (R).d_fout;                                                        \
+    [[maybe_unused]] double* d_energy = (R).d_energy;                                                    \
+    [[maybe_unused]] int& virial = (R).virial;                                                           \
+    [[maybe_unused]] bool& molvir = (R).molvir;                                                          \
+    [[maybe_unused]] int& mused = (R).mused;                                                             \
+    [[maybe_unused]] MolvirFinish& mf = (R).mf;                                                          \
+    [[maybe_unused]] bool& use32 = (R).use32;                                                            \
+    [[maybe_unused]] bool& use40 = (R).use40;                                                            \
+    [[maybe_unused]] size_t& n3 = (R).n3;                                                                \
+    [[maybe_unused]] bool& any_cut = (R).any_cut;                                                        \
+    [[maybe_unused]] bool& any_pme = (R).any_pme;                                                        \
+    [[maybe_unused]] bool& any_full = (R).any_full;                                                      \
+    [[maybe_unused]] bool& use_col = (R).use_col;                                                        \
+    [[maybe_unused]] bool& mixed_cells = (R).mixed_cells;                                                \
+    [[maybe_unused]] bool& cell_sort = (R).cell_sort;                                                    \
+    [[maybe_unused]] bool& mv_bin = (R).mv_bin;                                                          \
+    [[maybe_unused]] bool& fork = (R).fork;                                                              \
+    [[maybe_unused]] bool& near_on_side = (R).near_on_side;                                              \
+    [[maybe_unused]] int& used = (R).used;                                                               \
+    [[maybe_unused]] int& last_mixed = (R).last_mixed;                                                   \
+    [[maybe_unused]] int& lists = (R).lists;                                                             \
+    [[maybe_unused]] int& pair_virial = (R).pair_virial;                                                 \
+    [[maybe_unused]] int& col_virial = (R).col_virial;                                                   \
+    [[maybe_unused]] cudaStream_t s = sys->stream;                                                       \
+    [[maybe_unused]] int r = PMGPU_OK;
+
+// PME: reads only positions and charges and accumulates in atom order.
+// Beside the pair kernels (branches = true) the correction term and the
+// FP64 energy transform of a mixed force run on branches of their own,
+// joined back into ps at the end.
+static int run_pme(EvalRun& R, cudaStream_t ps, bool branches)
+{
+    PM_EVAL_RUN_NAMES(R)
         bool corr_branch = false, e64_branch = false;
         for (int k = 0; k < nf; ++k) {
             pmgpu_force* f = forces[k];
@@ -1929,15 +1942,96 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
             CK(cudaStreamWaitEvent(ps, sys->ev_e64, 0), "join");
         }
         return PMGPU_OK;
-    };
+}
+
+// the near pairs' FP64 energies of cutoff force k after its pair kernel
+static int run_near(EvalRun& R, int k, const PairArgs& a, bool fp64, bool col)
+{
+    PM_EVAL_RUN_NAMES(R)
+    pmgpu_force* f = forces[k];
+    if (fp64 || !(a.near2 > 0.0f)) return PMGPU_OK;
+    // the last cutoff force's near-pair energies (needed only by the energy
+    // reduction) run on the side stream, after PME, beside finalize; earlier
+    // forces' before the next list reuses the buffer
+    cudaStream_t ns = s;
+    if (fork && k == last_mixed) {
+        CK(cudaEventRecord(sys->ev_pair, s), "event");
+        CK(cudaStreamWaitEvent(sys->side, sys->ev_pair, 0), "event");
+        ns = sys->side;
+    }
+    int e = col ? launch_near_energy_col(a, f->combo, sys->n, ns, &sys->launches)
+                : launch_near_energy(a, f->combo, sys->n, ns, &sys->launches);
+    if (e) return cuda_fail(sys, (cudaError_t)e, "near-pair energies");
+    if (ns != s) {
+        CK(cudaEventRecord(sys->ev_near, sys->side), "event");
+        near_on_side = true;
+    }
+    return PMGPU_OK;
+}
+
+static int run_begin(EvalRun& R)
+{
+    PM_EVAL_RUN_NAMES(R)
+    const unsigned flags = R.flags;
+    virial = (flags & PMGPU_FLAG_VIRIAL) ? 1 : 0;
+    molvir = (flags & PMGPU_FLAG_MOLECULAR_VIRIAL) != 0;
+    mused = 0;
+    memset(&mf, 0, sizeof(mf));
+    use32 = use40 = false;
+    for (int k = 0; k < nf; ++k) (pairs64(sys, forces[k]) ? use40 : use32) = true;
+    n3 = 3 * (size_t)sys->n;
+    R.mbin = prof_begin(sys, kPhaseBin);
+    if (sys->eval_reuse) {
+        // the list's counts (ints 1-4) stay; the status, the work counter,
+        // the near-pair counts, the binning counters and the sums start at zero
+        CK(cudaMemsetAsync(sys->d_small, 0, sizeof(int), s), "memset");
+        CK(cudaMemsetAsync((char*)sys->d_small + 5 * sizeof(int), 0, kSmallBytes - 5 * sizeof(int), s), "memset");
+    } else {
+        CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
+    }
+    any_cut = any_pme = any_full = false;
+    bool atom_mixed = false, atom_fp64 = false;        // PME / all-pairs forces of each precision
+    for (int k = 0; k < nf; ++k) {
+        any_cut |= forces[k]->kind == 0;
+        any_pme |= forces[k]->kind == 1;
+        any_full |= forces[k]->kind == 2;
+        if (forces[k]->kind != 0) (pairs64(sys, forces[k]) ? atom_fp64 : atom_mixed) = true;
+    }
+    use_col = sys->eval_use_col;
+    // the cell-ordered mixed accumulators serve the cell path's mixed cutoff
+    // forces only; the atom-ordered ones (mixed half, FP64 half) PME and the
+    // all-pairs forces of that precision
+    mixed_cells = false;
+    for (int k = 0; k < nf; ++k)
+        if (forces[k]->kind == 0 && !pairs64(sys, forces[k]) && !use_col) mixed_cells = true;
+    if (mixed_cells) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
+    if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
+    if (atom_mixed) CK(cudaMemsetAsync(sys->d_faccA, 0, sizeof(unsigned long long) * n3, s), "memset");
+    if (atom_fp64) CK(cudaMemsetAsync(sys->d_faccA + n3, 0, sizeof(unsigned long long) * n3, s), "memset");
+    for (int k = 0; k < nf; ++k)
+        if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64)
+            sys->last_layout = pairs64(sys, forces[k]) ? PMGPU_LAYOUT_FP64
+                             : (use_col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS);
+    if (use_col)
+        CK(cudaMemsetAsync(sys->d_facc32c, 0, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap, s),
+           "memset");
+    // the cell-sorted order: for the FP64 cutoff forces, and for the mixed
+    // ones when the column path does not take them
+    cell_sort = false;
+    for (int k = 0; k < nf; ++k)
+        if (forces[k]->kind == 0 && (pairs64(sys, forces[k]) || !use_col)) cell_sort = true;
+    // the molecular virial kernels of the cutoff forces read the cell-sorted
+    // order too (binned for them alone on the column path)
+    mv_bin = molvir && any_cut && !cell_sort;
+    used = 0;
     // with cutoff forces too, PME runs on the side stream from the start,
     // beside binning, the list and the pair kernels, and is joined before
     // finalize (not while profiling, which times every phase alone)
-    const bool fork = any_cut && any_pme && !sys->profiling && sys->tuning.pme_concurrent;
+    fork = any_cut && any_pme && !sys->profiling && sys->tuning.pme_concurrent;
     if (fork) {
         CK(cudaEventRecord(sys->ev_fork, s), "fork");
         CK(cudaStreamWaitEvent(sys->side, sys->ev_fork, 0), "fork");
-        r = enqueue_pme(sys->side, true);
+        r = run_pme(R, sys->side, true);
         if (r) return r;
         CK(cudaEventRecord(sys->ev_join, sys->side), "join");
     }
@@ -1949,7 +2043,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         r = sys->eval_reuse ? col_refresh(sys, d_pos) : col_bin(sys, d_pos);
         if (r) return r;
     }
-    prof_end(sys, mbin);
+    prof_end(sys, R.mbin);
     // vacuum all-pairs forces: the recompute kernel in forward mode, forces in
     // atom order like PME
     for (int k = 0; k < nf; ++k) {
@@ -1968,13 +2062,22 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
         prof_end(sys, m);
         used += pair_records(sys, f);
     }
-    int last_mixed = -1;                // the last mixed cutoff force (its near pairs may go to the side stream)
+    last_mixed = -1;
     for (int k = 0; k < nf; ++k)
         if (forces[k]->kind == 0 && !pairs64(sys, forces[k])) last_mixed = k;
-    bool near_on_side = false;
-    int lists = 0;
-    int pair_virial = 0, col_virial = 0;
-    for (int k = 0; k < nf; ++k) {
+    near_on_side = false;
+    lists = 0;
+    pair_virial = col_virial = 0;
+    R.k_next = 0;
+    R.deferred = -1;
+    return PMGPU_OK;
+}
+
+static int run_cutoffs(EvalRun& R, bool may_defer)
+{
+    PM_EVAL_RUN_NAMES(R)
+    for (int k = R.k_next; k < nf; ++k) {
+        R.k_next = k + 1;
         pmgpu_force* f = forces[k];
         if (f->kind != 0) continue;
         const bool fp64 = pairs64(sys, f);
@@ -1994,31 +2097,28 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
             if (e) return cuda_fail(sys, (cudaError_t)e, "cluster-pair list");
             prof_end(sys, ml);
         }
+        if (may_defer && col && !sys->eval_reuse) {
+            // a batch runs this pair kernel with its other members' (run_resume)
+            R.deferred = k;
+            R.dargs = a;
+            return PMGPU_OK;
+        }
         int m = prof_begin(sys, kPhasePair);
         int e = fp64 ? launch_pair_fp64(a, f->combo, pair_blocks(sys->grid, f->nd), s, &sys->launches)
                      : (col ? launch_pair_col(a, f->combo, s, &sys->launches)
                             : launch_pair_mixed(a, f->combo, s, &sys->launches));
-        if (!e && !fp64 && a.near2 > 0.0f) {
-            // the last cutoff force's near-pair energies (needed only by the
-            // energy reduction) run on the side stream, after PME, beside
-            // finalize; earlier forces' before the next list reuses the buffer
-            cudaStream_t ns = s;
-            if (fork && k == last_mixed) {
-                CK(cudaEventRecord(sys->ev_pair, s), "event");
-                CK(cudaStreamWaitEvent(sys->side, sys->ev_pair, 0), "event");
-                ns = sys->side;
-            }
-            e = col ? launch_near_energy_col(a, f->combo, sys->n, ns, &sys->launches)
-                    : launch_near_energy(a, f->combo, sys->n, ns, &sys->launches);
-            if (ns != s) {
-                CK(cudaEventRecord(sys->ev_near, sys->side), "event");
-                near_on_side = true;
-            }
-        }
         if (e) return cuda_fail(sys, (cudaError_t)e, "pair kernel");
+        r = run_near(R, k, a, fp64, col);
+        if (r) return r;
         prof_end(sys, m);
         used += pair_records(sys, f);
     }
+    return PMGPU_OK;
+}
+
+static int run_end(EvalRun& R)
+{
+    PM_EVAL_RUN_NAMES(R)
     if (molvir) {
         // the cutoff forces' molecular virial over the cell-sorted order
         for (int k = 0; k < nf; ++k) {
@@ -2036,7 +2136,7 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     if (fork) {
         CK(cudaStreamWaitEvent(s, sys->ev_join, 0), "join");
     } else if (any_pme) {
-        r = enqueue_pme(s, false);
+        r = run_pme(R, s, false);
         if (r) return r;
     }
     int mfin = prof_begin(sys, kPhaseFinalize);
@@ -2084,6 +2184,38 @@ static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, c
     }
     prof_end(sys, mfin);
     return PMGPU_OK;
+}
+
+static int run_resume(EvalRun& R)
+{
+    const int k = R.deferred;
+    R.deferred = -1;
+    int r = run_near(R, k, R.dargs, false, true);
+    if (r) return r;
+    R.used += pair_records(R.sys, R.forces[k]);
+    r = run_cutoffs(R, false);
+    if (r) return r;
+    return run_end(R);
+}
+
+static void run_init(EvalRun& R, pmgpu_system* sys, int nf, pmgpu_force* const* forces, const double* d_pos,
+                     double* d_fout, double* d_energy, unsigned flags)
+{
+    R = EvalRun();
+    R.sys = sys; R.nf = nf; R.forces = forces; R.d_pos = d_pos; R.d_fout = d_fout; R.d_energy = d_energy;
+    R.flags = flags;
+}
+
+static int eval_enqueue(pmgpu_system* sys, int nf, pmgpu_force* const* forces, const double* d_pos,
+                        double* d_fout, double* d_energy, unsigned flags)
+{
+    EvalRun R;
+    run_init(R, sys, nf, forces, d_pos, d_fout, d_energy, flags);
+    int r = run_begin(R);
+    if (r) return r;
+    r = run_cutoffs(R, false);
+    if (r) return r;
+    return run_end(R);
 }
 
 // prepare, then enqueue -- replaying a captured CUDA graph when the same
@@ -2515,6 +2647,11 @@ struct pmgpu_batch {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr;
+    cudaEvent_t ev_pairs = nullptr;           // the members' one pair launch has run
+    int pair_launch = 1;                      // 1: the column-path pair kernels as one launch (K11)
+    PairArgs* d_args = nullptr;               // the members' pair arguments for that launch
+    size_t args_cap = 0;
+    int* d_next = nullptr;                    // its work counters, one per combination of terms
     struct Member {
         pmgpu_system* sys;
         std::vector<pmgpu_force*> forces;    // -real expanded
@@ -2523,6 +2660,7 @@ struct pmgpu_batch {
         double* energy;
         unsigned flags;
         cudaEvent_t done;
+        cudaEvent_t listed;                  // its list is built (before the one pair launch)
     };
     std::vector<Member> members;
     std::vector<GraphKey> keys;               // of the captured graph
@@ -2545,7 +2683,9 @@ extern "C" int pmgpu_batch_create(int device, pmgpu_batch** out)
     pmgpu_batch* b = new pmgpu_batch();
     b->device = device;
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_pairs, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc((void**)&b->d_next, 32 * sizeof(int)) != cudaSuccess) {
         delete b;
         return PMGPU_ERR_CUDA;
     }
@@ -2559,8 +2699,14 @@ extern "C" int pmgpu_batch_destroy(pmgpu_batch* b)
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
-    for (auto& m : b->members) cudaEventDestroy(m.done);
+    for (auto& m : b->members) {
+        cudaEventDestroy(m.done);
+        cudaEventDestroy(m.listed);
+    }
     cudaEventDestroy(b->ev_start);
+    cudaEventDestroy(b->ev_pairs);
+    cudaFree(b->d_args);
+    cudaFree(b->d_next);
     cudaStreamDestroy(b->stream);
     delete b;
     return PMGPU_OK;
@@ -2582,6 +2728,10 @@ extern "C" int pmgpu_batch_add(pmgpu_batch* b, pmgpu_system* sys, int n_forces, 
     }
     cudaSetDevice(b->device);
     if (cudaEventCreateWithFlags(&m.done, cudaEventDisableTiming) != cudaSuccess) return PMGPU_ERR_CUDA;
+    if (cudaEventCreateWithFlags(&m.listed, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventDestroy(m.done);
+        return PMGPU_ERR_CUDA;
+    }
     b->members.push_back(m);
     return PMGPU_OK;
 }
@@ -2607,19 +2757,77 @@ extern "C" int pmgpu_batch_evaluate(pmgpu_batch* b)
         if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
         std::vector<long long> l0;
         for (auto& m : b->members) l0.push_back(m.sys->launches);
+        // the one pair launch (K11) takes the members' column-path mixed
+        // cutoff forces when every member is its own system
+        const size_t nm = b->members.size();
+        bool one_launch = b->pair_launch == 1 && nm <= (size_t)kBatchPairMax;
+        for (size_t i = 0; i < nm && one_launch; ++i)
+            for (size_t j = 0; j < i; ++j)
+                if (b->members[i].sys == b->members[j].sys) one_launch = false;
+        if (one_launch && nm > b->args_cap) {
+            cudaFree(b->d_args);
+            b->d_args = nullptr;
+            b->args_cap = 0;
+            if (cudaMalloc((void**)&b->d_args, nm * sizeof(PairArgs)) != cudaSuccess)
+                return batch_fail(b, PMGPU_ERR_CUDA, "batch pair arguments");
+            b->args_cap = nm;
+        }
+        std::vector<EvalRun> runs(nm);
+        std::vector<size_t> deferred;
+        std::vector<PairArgs> hargs;
         if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             return batch_fail(b, PMGPU_ERR_CUDA, "batch graph capture");
         int r = PMGPU_OK;
         cudaError_t e = cudaEventRecord(b->ev_start, b->stream);
-        for (size_t k = 0; k < b->members.size() && r == PMGPU_OK && e == cudaSuccess; ++k) {
+        for (size_t k = 0; k < nm && r == PMGPU_OK && e == cudaSuccess; ++k) {
             auto& m = b->members[k];
             e = cudaStreamWaitEvent(m.sys->stream, b->ev_start, 0);
             if (e != cudaSuccess) break;
-            r = eval_enqueue(m.sys, (int)m.forces.size(), m.forces.data(), m.pos, m.fout, m.energy, m.flags);
+            run_init(runs[k], m.sys, (int)m.forces.size(), m.forces.data(), m.pos, m.fout, m.energy, m.flags);
+            r = run_begin(runs[k]);
+            if (!r) r = run_cutoffs(runs[k], one_launch);
+            if (!r && runs[k].deferred < 0) r = run_end(runs[k]);
             if (r) { b->err = m.sys->err; break; }
-            e = cudaEventRecord(m.done, m.sys->stream);
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, m.done, 0);
+            if (runs[k].deferred >= 0) {
+                deferred.push_back(k);
+                e = cudaEventRecord(m.listed, m.sys->stream);
+                if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, m.listed, 0);
+            } else {
+                e = cudaEventRecord(m.done, m.sys->stream);
+            }
         }
+        if (r == PMGPU_OK && e == cudaSuccess && !deferred.empty()) {
+            // one persistent launch per combination of terms over the members'
+            // chunks, then every deferred member resumes after it
+            std::vector<int> combos;
+            for (size_t k : deferred) {
+                const int c = runs[k].forces[runs[k].deferred]->combo;
+                if (std::find(combos.begin(), combos.end(), c) == combos.end()) combos.push_back(c);
+            }
+            for (size_t g = 0; g < combos.size() && e == cudaSuccess && r == PMGPU_OK; ++g) {
+                const size_t off = hargs.size();
+                for (size_t k : deferred)
+                    if (runs[k].forces[runs[k].deferred]->combo == combos[g]) hargs.push_back(runs[k].dargs);
+                e = cudaMemsetAsync(b->d_next + g, 0, sizeof(int), b->stream);
+                if (e != cudaSuccess) break;
+                BatchPairArgs ba;
+                ba.args = b->d_args + off;
+                ba.n = (int)(hargs.size() - off);
+                ba.next = b->d_next + g;
+                e = (cudaError_t)launch_pair_col_batch(ba, combos[g], b->stream, &b->members[deferred[0]].sys->launches);
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(b->ev_pairs, b->stream);
+            for (size_t i = 0; i < deferred.size() && e == cudaSuccess && r == PMGPU_OK; ++i) {
+                auto& m = b->members[deferred[i]];
+                e = cudaStreamWaitEvent(m.sys->stream, b->ev_pairs, 0);
+                if (e != cudaSuccess) break;
+                r = run_resume(runs[deferred[i]]);
+                if (r) { b->err = m.sys->err; break; }
+                e = cudaEventRecord(m.done, m.sys->stream);
+            }
+        }
+        for (size_t k = 0; k < nm && r == PMGPU_OK && e == cudaSuccess; ++k)
+            e = cudaStreamWaitEvent(b->stream, b->members[k].done, 0);
         cudaGraph_t graph = nullptr;
         cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
         if (r || e != cudaSuccess || ec != cudaSuccess) {
@@ -2634,6 +2842,15 @@ extern "C" int pmgpu_batch_evaluate(pmgpu_batch* b)
             b->exec = nullptr;
             return batch_fail(b, PMGPU_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(e));
         }
+        // the one pair launch reads the members' arguments from device memory
+        if (!hargs.empty()) {
+            e = cudaMemcpy(b->d_args, hargs.data(), hargs.size() * sizeof(PairArgs), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                cudaGraphExecDestroy(b->exec);
+                b->exec = nullptr;
+                return batch_fail(b, PMGPU_ERR_CUDA, std::string("batch pair arguments: ") + cudaGetErrorString(e));
+            }
+        }
         b->member_launches.clear();
         for (size_t k = 0; k < b->members.size(); ++k) {
             b->member_launches.push_back(b->members[k].sys->launches - l0[k]);
@@ -2644,6 +2861,20 @@ extern "C" int pmgpu_batch_evaluate(pmgpu_batch* b)
     cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
     if (e != cudaSuccess) return batch_fail(b, PMGPU_ERR_CUDA, std::string("batch graph launch: ") + cudaGetErrorString(e));
     for (size_t k = 0; k < b->members.size(); ++k) b->members[k].sys->launches += b->member_launches[k];
+    return PMGPU_OK;
+}
+
+extern "C" int pmgpu_batch_set_pair_launch(pmgpu_batch* b, int one_launch)
+{
+    if (!b || (one_launch != 0 && one_launch != 1)) return PMGPU_ERR_ARG;
+    if (b->pair_launch != one_launch && b->exec) {
+        cudaSetDevice(b->device);
+        cudaStreamSynchronize(b->stream);
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+        b->keys.clear();
+    }
+    b->pair_launch = one_launch;
     return PMGPU_OK;
 }
 

@@ -63,14 +63,22 @@ def test_shards_agree_across_gloo_ranks():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("one_launch", [True, False])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_batch_equals_members_evaluated_alone(precision):
+def test_batch_equals_members_evaluated_alone(precision, one_launch):
+    """The batch's results are its members' own, bit for bit: with the
+    column-path pair kernels of the members as one persistent launch over
+    their (system, chunk) work items (the two largest boxes here take the
+    column path; the others their own cell-path kernels), and with one pair
+    launch per member."""
     from protomol_b200 import forces as F
     from protomol_b200 import workloads
     from protomol_b200.batch import Batch
     ws = [workloads.water_box_workload(n, 50 + k) for k, n in enumerate([100, 260, 640, 1000, 1700, 2400])]
     batch = Batch(0)
+    batch.set_pair_launch(one_launch)
     alone = []
+    layouts = []
     for w in ws:
         topo = F.Topology(w.system)
         fs = [F.ForceFactory.make(topo, d, precision) for d in w.forces]
@@ -78,7 +86,10 @@ def test_batch_equals_members_evaluated_alone(precision):
         e = F.ScalarStructure()
         F.evaluate_group(topo, fs, w.system.positions, out, e)
         alone.append((out, e))
+        layouts.append(topo.pair_layout())
         batch.add(topo, fs, w.system.positions)
+    if precision == "mixed":
+        assert layouts[-2:] == ["columns", "columns"] and "cells" in layouts
     for call in range(2):                       # capture, then replay
         batch.zero()
         batch.evaluate()
