@@ -394,6 +394,29 @@ def run_reference(system, specs, repeat: int = 1, fast: bool = False, timeout=No
     return out
 
 
+def run_reference_hessian(system, specs, timeout=None):
+    """ProtoMol's own Hessian (integrators/Hessian.cpp: ``findForces`` over
+    a ForceGroup of the given forces, then ``evaluate`` without mass
+    re-weighting) on a vacuum system, run by the compiled reference: the
+    dense (3N, 3N) matrix.  Its nonbonded part reads separate LennardJones
+    and Coulomb forces (one term per spec)."""
+    exe = os.path.join(REF_DIR, "pmref")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    with tempfile.TemporaryDirectory() as td:
+        sp = os.path.join(td, "sys.bin")
+        op = os.path.join(td, "out.bin")
+        hp = os.path.join(td, "hess.bin")
+        system.save(sp)
+        args = [exe, sp, op, "1"]
+        for spec in specs:
+            args += _spec_args(spec)
+        env = dict(os.environ, PMREF_HESSIAN=hp)
+        subprocess.run(args, check=True, timeout=timeout, stdout=subprocess.DEVNULL, env=env)
+        n3 = 3 * system.n_atoms
+        return np.frombuffer(open(hp, "rb").read(), np.float64).reshape(n3, n3).copy()
+
+
 # ---------------------------------------------------------------- integration
 INV_TIMEFACTOR = 0.02045482828087295          # Constant::INV_TIMEFACTOR (base/pmconstants.cpp:49)
 

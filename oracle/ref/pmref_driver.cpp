@@ -25,7 +25,11 @@
 // molecule positions set by buildMolecularCenterOfMass (unit masses);
 // the molecule count, their positions and the molecular virial are then
 // appended to the output.  PMREF_NO_VIRIAL=1 turns ScalarStructure::virial()
-// off.
+// off.  PMREF_HESSIAN=<path> (vacuum systems) puts the forces into a
+// ForceGroup, runs ProtoMol's own Hessian (integrators/Hessian.cpp:
+// findForces, then evaluate without mass re-weighting) and writes the dense
+// 3N x 3N matrix to <path> (its nonbonded part reads separate LennardJones
+// and Coulomb forces: give them as two "full 1 ..." specs).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -63,6 +67,8 @@ using namespace ProtoMol::Report;
 #include "ScalarStructure.h"
 #include "Vector3DBlock.h"
 #include "topologyutilities.h"
+#include "ForceGroup.h"
+#include "Hessian.h"
 
 using namespace ProtoMol;
 
@@ -228,8 +234,26 @@ static SystemForce* make_cut(const std::vector<Term>& t, double algo)
     return NULL;
 }
 
+template <class SW, class P>
+static SystemForce* full1(const Term& a)
+{
+    typedef OneAtomPair<VBC, SW, P> OAP;
+    return new NonbondedSimpleFullSystemForce<OAP>(OAP(make_pot<P>(a), make_sw<SW>(a)), 64);
+}
+
 static SystemForce* make_full(const std::vector<Term>& t)
 {
+    // one term (registerForceExemplarsSimpleFull.cpp): LennardJones or
+    // Coulomb under Universal, C1 or C2
+    if (t.size() == 1 && (t[0].pot == 1 || t[0].pot == 2)) {
+        const bool lj = t[0].pot == 1;
+        if (t[0].sw == 0) return lj ? full1<UniversalSwitchingFunction, LennardJonesForce>(t[0])
+                                    : full1<UniversalSwitchingFunction, CoulombForce>(t[0]);
+        if (t[0].sw == 2) return lj ? full1<C1SwitchingFunction, LennardJonesForce>(t[0])
+                                    : full1<C1SwitchingFunction, CoulombForce>(t[0]);
+        if (t[0].sw == 3) return lj ? full1<C2SwitchingFunction, LennardJonesForce>(t[0])
+                                    : full1<C2SwitchingFunction, CoulombForce>(t[0]);
+    }
     if (t.size() == 2 && t[0].pot == 1 && t[1].pot == 2) {
         if (t[0].sw == 0 && t[1].sw == 0)
             return full2<UniversalSwitchingFunction, LennardJonesForce, UniversalSwitchingFunction, CoulombForce>(t[0], t[1]);
@@ -336,6 +360,22 @@ int main(int argc, char** argv)
             cells[3 * i] = c.x; cells[3 * i + 1] = c.y; cells[3 * i + 2] = c.z;
         }
         dims[0] = pt->cellLists.getDimX(); dims[1] = pt->cellLists.getDimY(); dims[2] = pt->cellLists.getDimZ();
+    }
+
+    const char* hess_env = getenv("PMREF_HESSIAN");
+    if (hess_env && !b.periodic) {
+        // the group owns nothing here: it is never destroyed
+        ForceGroup* fg = new ForceGroup();
+        for (size_t k = 0; k < forces.size(); ++k) fg->addSystemForce(forces[k]);
+        const unsigned int sz = 3 * (unsigned int)b.n;
+        Hessian hess(sz);
+        hess.clear();
+        hess.findForces(fg);
+        hess.evaluate(&pos, topo, false);
+        FILE* hf = fopen(hess_env, "wb");
+        if (!hf) return 4;
+        fwrite(hess.hessM, sizeof(double), (size_t)sz * sz, hf);
+        fclose(hf);
     }
 
     FILE* out = fopen(argv[2], "wb");

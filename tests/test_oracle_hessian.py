@@ -1,6 +1,8 @@
 """The oracle's restatement of ProtoMol's analytic pair Hessian
 (integrators/Hessian.cpp:456-623 with ReducedHessLennardJones,
-ReducedHessCoulomb and the C1 / C2 switch Hessians), pinned against central
+ReducedHessCoulomb and the C1 / C2 switch Hessians), pinned to ProtoMol's own
+Hessian (the compiled reference: Hessian::findForces over a ForceGroup of the
+LennardJones and Coulomb forces, then Hessian::evaluate) and against central
 differences of the oracle's own forces on the 104-atom vacuum chain, and the
 LJ parameter chain rule against differences of the energy (CPU only)."""
 import dataclasses
@@ -19,6 +21,23 @@ FULL_SW = ("LennardJones Coulomb -switchingFunction C2 -switchingFunction C1 -al
 
 def forces_of(s, d, pos):
     return oracle.evaluate(s, [F.parse_definition(d)], positions=pos)["forces"]
+
+
+# the same terms as separate forces, the form Hessian::findForces reads
+SEPARATE = {
+    FULL: ["LennardJones -algorithm NonbondedSimpleFull", "Coulomb -algorithm NonbondedSimpleFull"],
+    FULL_SW: ["LennardJones -switchingFunction C2 -algorithm NonbondedSimpleFull -switchon 6 -cutoff 9",
+              "Coulomb -switchingFunction C1 -algorithm NonbondedSimpleFull -cutoff 9"],
+}
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="the compiled reference (oracle/_ref) is not built")
+@pytest.mark.parametrize("d", [FULL, FULL_SW], ids=["universal", "c2_c1"])
+def test_pair_hessian_is_the_reference_hessian(d):
+    s = systems.vacuum_chain_104()
+    H = oracle.pair_hessian(s, F.parse_definition(d))
+    R = oracle.run_reference_hessian(s, [F.parse_definition(x) for x in SEPARATE[d]])
+    assert np.abs(H - R).max() <= 1e-12 * np.abs(R).max()
 
 
 @pytest.mark.parametrize("d", [FULL, FULL_SW], ids=["universal", "c2_c1"])
