@@ -355,7 +355,8 @@ int pmgpu_set_tuning(pmgpu_system* sys, const pmgpu_tuning* tuning);
 /* Project-written autotuner: times candidate tunings on these forces and
  * these positions (host, N x 3), evals evaluations each after two warm-up
  * ones, with CUDA events on the system's stream; a coordinate search over
- * the five parameters, two sweeps.  Keeps the fastest for the system's later
+ * the five parameters, two sweeps (fp64_pairs only on systems of at most
+ * 4,096 atoms; pmgpu_batch_autotune leaves it at 0).  Keeps the fastest for the system's later
  * evaluations and returns it (with its time) in *best.  Synchronous; uses
  * the system's own scratch buffers (no caller output is touched). */
 int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces, const double* positions,

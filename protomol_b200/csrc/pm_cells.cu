@@ -413,6 +413,15 @@ __global__ void __launch_bounds__(kColThreads) k_col_sort(ColBinArgs a)
     }
 }
 
+// K0: range blockIdx.y set to zero, grid-stride
+__global__ void __launch_bounds__(kBinThreads) k_zero(ZeroRanges z)
+{
+    unsigned* p = z.p[blockIdx.y];
+    const long long n = z.words[blockIdx.y];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = 0u;
+}
+
 __global__ void __launch_bounds__(kBinThreads) k_col_refresh(ColBinArgs a, double half_skin2)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -437,6 +446,17 @@ __global__ void __launch_bounds__(kBinThreads) k_col_refresh(ColBinArgs a, doubl
 }
 
 }  // namespace
+
+int launch_zero(const ZeroRanges& z, cudaStream_t s, long long* launches)
+{
+    if (z.count <= 0) return 0;
+    long long most = 0;
+    for (int r = 0; r < z.count; ++r) most = std::max(most, z.words[r]);
+    const int blocks = (int)std::max(1LL, std::min<long long>((most + 4 * kBinThreads - 1) / (4 * kBinThreads), 4 * 148));
+    k_zero<<<dim3(blocks, z.count), kBinThreads, 0, s>>>(z);
+    *launches += 1;
+    return (int)cudaGetLastError();
+}
 
 int launch_col_refresh(const ColBinArgs& a, double half_skin, cudaStream_t s, long long* launches)
 {

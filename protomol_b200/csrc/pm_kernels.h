@@ -93,6 +93,14 @@ struct ColBinArgs {
     int ncl_cap;                 // i-cluster capacity
     int* status;
 };
+// K0: up to kZeroRanges ranges of 4-byte words set to zero in one launch
+constexpr int kZeroRanges = 8;
+struct ZeroRanges {
+    unsigned* p[kZeroRanges];
+    long long words[kZeroRanges];
+    int count;
+};
+int launch_zero(const ZeroRanges& z, cudaStream_t s, long long* launches);
 // K1c: fixed point, columns, z order, clusters and their boxes
 int launch_col_bin(const ColBinArgs& a, cudaStream_t s, long long* launches);
 // K1r: between rebuilds of a reused pair list, the current fixed-point

@@ -202,7 +202,7 @@ struct pmgpu_system {
     int4* d_corg = nullptr;
     unsigned long long* d_facc32c = nullptr;
     int col_ncl_cap = 0;
-    std::vector<double> h_fbuf;
+    double* h_fbuf = nullptr;          // pinned 3N: the forces' device-to-host copy (pmgpu_evaluate)
     bool binned = false;
     std::set<pmgpu_force*> forces;     // live forces made on this system
     int topo_version = 0;
@@ -419,6 +419,7 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     dfree(sys->d_cstart); dfree(sys->d_cbox); dfree(sys->d_ccell); dfree(sys->d_plist); dfree(sys->d_chunks);
     dfree(sys->d_near);
     if (sys->h_energy) cudaFreeHost(sys->h_energy);
+    if (sys->h_fbuf) cudaFreeHost(sys->h_fbuf);
     cudaEventDestroy(sys->ev_fork);
     cudaEventDestroy(sys->ev_join);
     cudaEventDestroy(sys->ev_pair);
@@ -631,7 +632,9 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     sys->col_grid_stale = true;
     sys->list_valid = false;
     sys->cbox_cap = 0;   // cluster boxes depend on N and the cell grid: sized at evaluation
-    sys->h_fbuf.assign(3 * (size_t)n, 0.0);
+    if (sys->h_fbuf) cudaFreeHost(sys->h_fbuf);
+    sys->h_fbuf = nullptr;
+    CK(cudaMallocHost((void**)&sys->h_fbuf, sizeof(double) * 3 * (size_t)std::max(n, 1)), "host alloc");
     return PMGPU_OK;
 }
 
@@ -1981,13 +1984,21 @@ static int run_begin(EvalRun& R)
     for (int k = 0; k < nf; ++k) (pairs64(sys, forces[k]) ? use40 : use32) = true;
     n3 = 3 * (size_t)sys->n;
     R.mbin = prof_begin(sys, kPhaseBin);
+    // the evaluation's counters and accumulators start at zero: one launch
+    // for all of them (k_zero) instead of a memset node each
+    ZeroRanges zr;
+    memset(&zr, 0, sizeof(zr));
+    auto zero = [&zr](void* p, size_t bytes) {
+        zr.p[zr.count] = static_cast<unsigned*>(p);
+        zr.words[zr.count++] = (long long)(bytes / sizeof(unsigned));
+    };
     if (sys->eval_reuse) {
         // the list's counts (ints 1-4) stay; the status, the work counter,
         // the near-pair counts, the binning counters and the sums start at zero
-        CK(cudaMemsetAsync(sys->d_small, 0, sizeof(int), s), "memset");
-        CK(cudaMemsetAsync((char*)sys->d_small + 5 * sizeof(int), 0, kSmallBytes - 5 * sizeof(int), s), "memset");
+        zero(sys->d_small, sizeof(int));
+        zero((char*)sys->d_small + 5 * sizeof(int), kSmallBytes - 5 * sizeof(int));
     } else {
-        CK(cudaMemsetAsync(sys->d_small, 0, kSmallBytes, s), "memset");
+        zero(sys->d_small, kSmallBytes);
     }
     any_cut = any_pme = any_full = false;
     bool atom_mixed = false, atom_fp64 = false;        // PME / all-pairs forces of each precision
@@ -2004,17 +2015,19 @@ static int run_begin(EvalRun& R)
     mixed_cells = false;
     for (int k = 0; k < nf; ++k)
         if (forces[k]->kind == 0 && !pairs64(sys, forces[k]) && !use_col) mixed_cells = true;
-    if (mixed_cells) CK(cudaMemsetAsync(sys->d_facc32, 0, 2 * sizeof(unsigned long long) * n3, s), "memset");
-    if (use40) CK(cudaMemsetAsync(sys->d_facc40, 0, sizeof(unsigned long long) * n3, s), "memset");
-    if (atom_mixed) CK(cudaMemsetAsync(sys->d_faccA, 0, sizeof(unsigned long long) * n3, s), "memset");
-    if (atom_fp64) CK(cudaMemsetAsync(sys->d_faccA + n3, 0, sizeof(unsigned long long) * n3, s), "memset");
+    if (mixed_cells) zero(sys->d_facc32, 2 * sizeof(unsigned long long) * n3);
+    if (use40) zero(sys->d_facc40, sizeof(unsigned long long) * n3);
+    if (atom_mixed) zero(sys->d_faccA, sizeof(unsigned long long) * n3);
+    if (atom_fp64) zero(sys->d_faccA + n3, sizeof(unsigned long long) * n3);
     for (int k = 0; k < nf; ++k)
         if (forces[k]->kind == 0 && forces[k]->precision != PMGPU_PRECISION_FP64)
             sys->last_layout = pairs64(sys, forces[k]) ? PMGPU_LAYOUT_FP64
                              : (use_col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS);
-    if (use_col)
-        CK(cudaMemsetAsync(sys->d_facc32c, 0, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap, s),
-           "memset");
+    if (use_col) zero(sys->d_facc32c, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap);
+    {
+        int e = launch_zero(zr, s, &sys->launches);
+        if (e) return cuda_fail(sys, (cudaError_t)e, "zero");
+    }
     // the cell-sorted order: for the FP64 cutoff forces, and for the mixed
     // ones when the column path does not take them
     cell_sort = false;
@@ -2334,7 +2347,7 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
         CK(cudaMemsetAsync(sys->d_energy, 0, sizeof(double) * kEOut, s), "memset");
         r = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy, flags);
         if (r) return r;
-        CK(cudaMemcpyAsync(sys->h_fbuf.data(), sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
+        CK(cudaMemcpyAsync(sys->h_fbuf, sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
         CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kEOut, cudaMemcpyDeviceToHost, s), "D2H energies");
         sys->col_just_disabled = false;
         sys->list_just_invalidated = false;
@@ -2933,8 +2946,11 @@ extern "C" int pmgpu_set_tuning(pmgpu_system* sys, const pmgpu_tuning* t)
 // coordinate search over the five launch parameters: each is tried at its
 // candidate values with the others at the best so far, two sweeps; time(t)
 // measures one candidate in ms per evaluation
+constexpr int kFp64PairsMaxAtoms = 4096;     // largest system the autotuner offers fp64_pairs
+
 template <class TimeFn>
-static int tune_search(pmgpu_tuning start, bool has_pme, bool has_pairs, TimeFn time, pmgpu_tuning* best)
+static int tune_search(pmgpu_tuning start, bool has_pme, bool has_pairs, bool try_fp64, TimeFn time,
+                       pmgpu_tuning* best)
 {
     double best_ms = 0.0;
     int r = time(start, &best_ms);
@@ -2945,6 +2961,7 @@ static int tune_search(pmgpu_tuning start, bool has_pme, bool has_pairs, TimeFn 
     for (int sweep = 0; sweep < 2; ++sweep) {
         for (int param = 0; param < 5; ++param) {
             if ((param == 0 || param == 1 || param == 4) && !has_pairs) continue;
+            if (param == 4 && !try_fp64) continue;
             if ((param == 2 || param == 3) && !has_pme) continue;
             if (param == 3 && !has_pairs) continue;
             const int nv = param >= 3 ? 2 : 3;
@@ -3022,7 +3039,10 @@ extern "C" int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* cons
     bool has_pme = false, has_pairs = false;
     force_kinds(n_forces, forces, has_pme, has_pairs);
     pmgpu_tuning b;
-    r = tune_search(sys->tuning, has_pme, has_pairs, time, &b);
+    // the FP64 pair kernels can win only on a few thousand atoms or fewer,
+    // where an evaluation is a chain of launch latencies; on larger systems
+    // they are not timed (a disturbed timing could not pick them)
+    r = tune_search(sys->tuning, has_pme, has_pairs, sys->n <= kFp64PairsMaxAtoms, time, &b);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (r) return r;
@@ -3070,7 +3090,8 @@ extern "C" int pmgpu_batch_autotune(pmgpu_batch* b, int evals, pmgpu_tuning* bes
         return PMGPU_OK;
     };
     pmgpu_tuning t;
-    int r = tune_search(b->members[0].sys->tuning, has_pme, has_pairs, time, &t);
+    // one tuning for every member: the FP64 pair kernels are not a candidate
+    int r = tune_search(b->members[0].sys->tuning, has_pme, has_pairs, false, time, &t);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (r) return r;
