@@ -186,7 +186,8 @@ def run_reference_arm(args, rank, world, pg):
         if pg:
             pg.barrier()
         return
-    evals = min(max(1, args.steps), 12)
+    # at least two timed evaluations: the reference driver times repeats only
+    evals = min(max(2, args.steps), 12)
     base = reference_all_cores(w.system, w.forces, evals)
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
             "steps": evals, "warmup": 1, "ms_per_step": 1000.0 / base["value"], "higher_is_better": True,
