@@ -94,7 +94,7 @@ struct ColBinArgs {
     int* status;
 };
 // K0: up to kZeroRanges ranges of 4-byte words set to zero in one launch
-constexpr int kZeroRanges = 8;
+constexpr int kZeroRanges = 10;
 struct ZeroRanges {
     unsigned* p[kZeroRanges];
     long long words[kZeroRanges];

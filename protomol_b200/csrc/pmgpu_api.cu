@@ -118,6 +118,7 @@ struct pmgpu_system {
     double* d_fout = nullptr;
     double* d_energy = nullptr;        // kEOut
     double* h_energy = nullptr;        // pinned kEOut
+    int* h_status = nullptr;           // pinned: the status word, copied back with the results
     unsigned long long* d_facc32 = nullptr;   // mixed (2^32): 3N pair forces + 3N other (d_facc32p)
     unsigned long long* d_facc32p = nullptr;
     unsigned long long* d_facc40 = nullptr;   // FP64 (2^40)
@@ -358,7 +359,8 @@ extern "C" int pmgpu_system_create(int device, pmgpu_system** out)
     }
     if (cudaMalloc(&sys->d_small, kSmallBytes) != cudaSuccess ||
         cudaMalloc((void**)&sys->d_energy, sizeof(double) * kEOut) != cudaSuccess ||
-        cudaMallocHost((void**)&sys->h_energy, sizeof(double) * kEOut) != cudaSuccess) {
+        cudaMallocHost((void**)&sys->h_energy, sizeof(double) * kEOut) != cudaSuccess ||
+        cudaMallocHost((void**)&sys->h_status, sizeof(int)) != cudaSuccess) {
         delete sys;
         return PMGPU_ERR_NOMEM;
     }
@@ -419,6 +421,7 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     dfree(sys->d_cstart); dfree(sys->d_cbox); dfree(sys->d_ccell); dfree(sys->d_plist); dfree(sys->d_chunks);
     dfree(sys->d_near);
     if (sys->h_energy) cudaFreeHost(sys->h_energy);
+    if (sys->h_status) cudaFreeHost(sys->h_status);
     if (sys->h_fbuf) cudaFreeHost(sys->h_fbuf);
     cudaEventDestroy(sys->ev_fork);
     cudaEventDestroy(sys->ev_join);
@@ -479,13 +482,10 @@ extern "C" int pmgpu_phase_times(pmgpu_system* sys, double* ms, int n, long long
 }
 extern "C" long long pmgpu_launch_count(pmgpu_system* sys) { return sys ? sys->launches : 0; }
 
-extern "C" int pmgpu_synchronize(pmgpu_system* sys)
+// the outcome of the evaluations up to now from their status word st (read
+// after the stream has drained)
+static int status_result(pmgpu_system* sys, int st)
 {
-    if (!sys) return PMGPU_ERR_ARG;
-    cudaSetDevice(sys->device);
-    CK(cudaStreamSynchronize(sys->stream), "synchronize");
-    int st = 0;
-    CK(cudaMemcpy(&st, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status");
     if (st & kStatusOverflow)
         return fail(sys, PMGPU_ERR_OVERFLOW, "non-finite or out-of-range force (fixed-point range exceeded)");
     if (st & kStatusColumns) {
@@ -516,6 +516,16 @@ extern "C" int pmgpu_synchronize(pmgpu_system* sys)
         return fail(sys, PMGPU_ERR_CAPACITY, "cluster-pair list capacity exceeded (grown for the next evaluation)");
     }
     return PMGPU_OK;
+}
+
+extern "C" int pmgpu_synchronize(pmgpu_system* sys)
+{
+    if (!sys) return PMGPU_ERR_ARG;
+    cudaSetDevice(sys->device);
+    CK(cudaStreamSynchronize(sys->stream), "synchronize");
+    int st = 0;
+    CK(cudaMemcpy(&st, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status");
+    return status_result(sys, st);
 }
 
 // ------------------------------------------------------------------ topology
@@ -1494,6 +1504,10 @@ static void fill_col_args(pmgpu_system* sys, PairArgs& a)
 // FP64 force, and for a mixed cutoff force when the tuning asks for them
 // (fp64_pairs: no cluster list and no near-pair pass, the shorter launch
 // chain that is faster on systems of a few hundred atoms)
+// internal evaluation flag (never a caller's): the evaluation's outputs start
+// at zero, set by the graph's zero kernel (pmgpu_evaluate's own buffers)
+constexpr unsigned kFlagZeroOut = 1u << 30;
+
 static inline bool pairs64(const pmgpu_system* sys, const pmgpu_force* f)
 {
     return f->precision == PMGPU_PRECISION_FP64 || (f->kind == 0 && sys->tuning.fp64_pairs);
@@ -2024,6 +2038,10 @@ static int run_begin(EvalRun& R)
             sys->last_layout = pairs64(sys, forces[k]) ? PMGPU_LAYOUT_FP64
                              : (use_col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS);
     if (use_col) zero(sys->d_facc32c, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap);
+    if (flags & kFlagZeroOut) {
+        zero(d_fout, sizeof(double) * n3);
+        zero(d_energy, sizeof(double) * kEOut);
+    }
     {
         int e = launch_zero(zr, s, &sys->launches);
         if (e) return cuda_fail(sys, (cudaError_t)e, "zero");
@@ -2326,7 +2344,7 @@ extern "C" int pmgpu_evaluate_device(pmgpu_system* sys, int n_forces, pmgpu_forc
     if (!sys || !d_positions || !d_forces_accum || !d_energies) return PMGPU_ERR_ARG;
     cudaSetDevice(sys->device);
     // without PMGPU_FLAG_VIRIAL every kernel adds zero to the virial slots
-    return eval_core(sys, n_forces, forces, d_positions, d_forces_accum, d_energies, flags);
+    return eval_core(sys, n_forces, forces, d_positions, d_forces_accum, d_energies, flags & ~kFlagZeroOut);
 }
 
 extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces,
@@ -2343,15 +2361,18 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
     // a second attempt only when the cluster-pair list outgrew its estimate
     // (the first attempt recorded the size it needs)
     for (int attempt = 0; attempt < 2; ++attempt) {
-        CK(cudaMemsetAsync(sys->d_fout, 0, sizeof(double) * n3, s), "memset");
-        CK(cudaMemsetAsync(sys->d_energy, 0, sizeof(double) * kEOut, s), "memset");
-        r = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy, flags);
+        // the outputs are zeroed inside the evaluation's graph; the status
+        // word comes back with the results (one wait, no second round trip)
+        r = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy,
+                      (flags & ~kFlagZeroOut) | kFlagZeroOut);
         if (r) return r;
         CK(cudaMemcpyAsync(sys->h_fbuf, sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
         CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kEOut, cudaMemcpyDeviceToHost, s), "D2H energies");
+        CK(cudaMemcpyAsync(sys->h_status, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H status");
         sys->col_just_disabled = false;
         sys->list_just_invalidated = false;
-        r = pmgpu_synchronize(sys);
+        CK(cudaStreamSynchronize(s), "synchronize");
+        r = status_result(sys, *sys->h_status);
         if (!(r == PMGPU_ERR_CAPACITY && (sys->plist_need > sys->plist_cap || sys->chunk_need > sys->chunk_cap ||
                                           sys->near_need > sys->near_cap || sys->col_just_disabled ||
                                           sys->list_just_invalidated)))
@@ -2733,7 +2754,8 @@ extern "C" int pmgpu_batch_add(pmgpu_batch* b, pmgpu_system* sys, int n_forces, 
         return PMGPU_ERR_ARG;
     if (sys->device != b->device) return batch_fail(b, PMGPU_ERR_ARG, "system on another device");
     pmgpu_batch::Member m;
-    m.sys = sys; m.pos = d_positions; m.fout = d_forces_accum; m.energy = d_energies; m.flags = flags;
+    m.sys = sys; m.pos = d_positions; m.fout = d_forces_accum; m.energy = d_energies;
+    m.flags = flags & ~kFlagZeroOut;
     for (int k = 0; k < n_forces; ++k) {
         if (!forces[k] || forces[k]->sys != sys) return batch_fail(b, PMGPU_ERR_ARG, "force of another system");
         if (forces[k]->real_sub && !pme_needs_lattice(forces[k])) m.forces.push_back(forces[k]->real_sub);
@@ -3002,6 +3024,7 @@ extern "C" int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* cons
     if (!sys || n_forces <= 0 || !forces || !positions || evals < 1 || !best) return PMGPU_ERR_ARG;
     if (sys->profiling) return fail(sys, PMGPU_ERR_STATE, "autotune in profiling mode");
     cudaSetDevice(sys->device);
+    flags &= ~kFlagZeroOut;
     int r = eval_prepare(sys, n_forces, forces, flags);
     if (r) return r;
     cudaStream_t s = sys->stream;
