@@ -373,7 +373,9 @@ def main():
             "speedup_vs_fp64": t_fp64 / t_local,
             "accuracy_vs_fp64": {"force_rel_rms": force_err, "energy_rel": e_err},
             "e2e": {"value": world * 1000.0 / t_e2e, "unit": UNIT, "ms_per_step": t_e2e,
-                    "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 88},
+                    # positions, and the page-locked force accumulator the
+                    # library adds to on the device; forces and energies back
+                    "h2d_bytes_per_step": 24 * n + 24 * n, "d2h_bytes_per_step": 24 * n + 88},
             "e2e_adapter": e2e_adapter,
             "gpu_launches": int(launches),
             "pair_interactions_per_s": n_pairs * world * 1000.0 / t_local,

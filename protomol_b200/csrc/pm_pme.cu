@@ -1263,7 +1263,9 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
     for (int k = 0; k < kERec; ++k) v[k] = 0.0;
     if (s < a.n) {
         const int i = a.sorted ? a.sorted[s] : s;   // no cell-sorted order: atom order
-        double fp[3] = {0.0, 0.0, 0.0};
+        // the atom's total force, added to the output once (so that an
+        // output that already holds forces gets one rounding per component)
+        double fp[3] = {0.0, 0.0, 0.0}, ft[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             if (a.f32) fp[c] = (double)(long long)a.f32[3 * (size_t)s + c] * (1.0 / kScaleMixed);
@@ -1272,7 +1274,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
             if (a.f40) f += (double)(long long)a.f40[3 * (size_t)s + c] * (1.0 / kScaleFp64);
             if (a.a32) f += (double)(long long)a.a32[3 * (size_t)i + c] * (1.0 / kScaleMixed);
             if (a.a40) f += (double)(long long)a.a40[3 * (size_t)i + c] * (1.0 / kScaleFp64);
-            a.fout[3 * (size_t)i + c] += f;
+            ft[c] = f;
         }
         if (a.pair_virial & 1) {
             // the cell-relative position the FP32 pair vectors were formed from
@@ -1293,7 +1295,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 fc[c] = (double)(long long)a.c32[3 * (size_t)sl + c] * (1.0 / kScaleMixed);
-                a.fout[3 * (size_t)i + c] += fc[c];
+                ft[c] += fc[c];
             }
             if (a.pair_virial & 2) {
                 // position relative to its i-cluster's origin (the first atom)
@@ -1307,6 +1309,8 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a)
                     for (int c = 0; c < 3; ++c) v[2 + 3 * r + c] += p[r] * fc[c];
             }
         }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a.fout[3 * (size_t)i + c] += ft[c];
     }
     if (a.pair_virial) block_reduce_store<8>(v, a.erec, a.erec_stride, blockIdx.x);
 }

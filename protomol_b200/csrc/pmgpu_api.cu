@@ -203,7 +203,8 @@ struct pmgpu_system {
     int4* d_corg = nullptr;
     unsigned long long* d_facc32c = nullptr;
     int col_ncl_cap = 0;
-    double* h_fbuf = nullptr;          // pinned 3N: the forces' device-to-host copy (pmgpu_evaluate)
+    double* d_acc0 = nullptr;          // 3N: the caller's force accumulator as pmgpu_evaluate received it
+    double* h_fbuf = nullptr;          // pinned 3N: the forces' copy back for a pageable accumulator
     bool binned = false;
     std::set<pmgpu_force*> forces;     // live forces made on this system
     int topo_version = 0;
@@ -422,6 +423,7 @@ extern "C" int pmgpu_system_destroy(pmgpu_system* sys)
     dfree(sys->d_near);
     if (sys->h_energy) cudaFreeHost(sys->h_energy);
     if (sys->h_status) cudaFreeHost(sys->h_status);
+    dfree(sys->d_acc0);
     if (sys->h_fbuf) cudaFreeHost(sys->h_fbuf);
     cudaEventDestroy(sys->ev_fork);
     cudaEventDestroy(sys->ev_join);
@@ -642,6 +644,7 @@ extern "C" int pmgpu_set_topology(pmgpu_system* sys, int n_atoms, const double* 
     sys->col_grid_stale = true;
     sys->list_valid = false;
     sys->cbox_cap = 0;   // cluster boxes depend on N and the cell grid: sized at evaluation
+    CK(dalloc(&sys->d_acc0, 3 * (size_t)std::max(n, 1)), "alloc");
     if (sys->h_fbuf) cudaFreeHost(sys->h_fbuf);
     sys->h_fbuf = nullptr;
     CK(cudaMallocHost((void**)&sys->h_fbuf, sizeof(double) * 3 * (size_t)std::max(n, 1)), "host alloc");
@@ -1504,9 +1507,12 @@ static void fill_col_args(pmgpu_system* sys, PairArgs& a)
 // FP64 force, and for a mixed cutoff force when the tuning asks for them
 // (fp64_pairs: no cluster list and no near-pair pass, the shorter launch
 // chain that is faster on systems of a few hundred atoms)
-// internal evaluation flag (never a caller's): the evaluation's outputs start
-// at zero, set by the graph's zero kernel (pmgpu_evaluate's own buffers)
+// internal evaluation flags (never a caller's): the evaluation's energy
+// output (kFlagZeroOut), and its force output too (kFlagZeroForces), start at
+// zero, set by the graph's zero kernel (pmgpu_evaluate's own buffers)
 constexpr unsigned kFlagZeroOut = 1u << 30;
+constexpr unsigned kFlagZeroForces = 1u << 29;
+constexpr unsigned kFlagsInternal = kFlagZeroOut | kFlagZeroForces;
 
 static inline bool pairs64(const pmgpu_system* sys, const pmgpu_force* f)
 {
@@ -2038,10 +2044,8 @@ static int run_begin(EvalRun& R)
             sys->last_layout = pairs64(sys, forces[k]) ? PMGPU_LAYOUT_FP64
                              : (use_col ? PMGPU_LAYOUT_COLUMNS : PMGPU_LAYOUT_CELLS);
     if (use_col) zero(sys->d_facc32c, sizeof(unsigned long long) * 3 * kCluster * (size_t)sys->col_ncl_cap);
-    if (flags & kFlagZeroOut) {
-        zero(d_fout, sizeof(double) * n3);
-        zero(d_energy, sizeof(double) * kEOut);
-    }
+    if (flags & kFlagZeroOut) zero(d_energy, sizeof(double) * kEOut);
+    if (flags & kFlagZeroForces) zero(d_fout, sizeof(double) * n3);
     {
         int e = launch_zero(zr, s, &sys->launches);
         if (e) return cuda_fail(sys, (cudaError_t)e, "zero");
@@ -2344,7 +2348,7 @@ extern "C" int pmgpu_evaluate_device(pmgpu_system* sys, int n_forces, pmgpu_forc
     if (!sys || !d_positions || !d_forces_accum || !d_energies) return PMGPU_ERR_ARG;
     cudaSetDevice(sys->device);
     // without PMGPU_FLAG_VIRIAL every kernel adds zero to the virial slots
-    return eval_core(sys, n_forces, forces, d_positions, d_forces_accum, d_energies, flags & ~kFlagZeroOut);
+    return eval_core(sys, n_forces, forces, d_positions, d_forces_accum, d_energies, flags & ~kFlagsInternal);
 }
 
 extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* const* forces,
@@ -2356,17 +2360,29 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
     if (sys->n == 0 && sys->q.empty() && sys->d_pos == nullptr) return fail(sys, PMGPU_ERR_STATE, "topology not set");
     size_t n3 = 3 * (size_t)sys->n;
     cudaStream_t s = sys->stream;
-    CK(cudaMemcpyAsync(sys->d_pos, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, s), "H2D positions");
+    const size_t fbytes = sizeof(double) * n3;
+    CK(cudaMemcpyAsync(sys->d_pos, positions, fbytes, cudaMemcpyHostToDevice, s), "H2D positions");
+    // A page-locked accumulator goes to the device, the evaluation adds to it
+    // there and the sum comes back in its place (no pass over it on the
+    // host); a pageable one stays on the host (two pageable copies cost more
+    // than the addition) and receives the forces from a pinned buffer.
+    cudaPointerAttributes pa;
+    const bool pinned = cudaPointerGetAttributes(&pa, forces_accum) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();                          // a pageable pointer may leave an error on older drivers
+    if (pinned) CK(cudaMemcpyAsync(sys->d_acc0, forces_accum, fbytes, cudaMemcpyHostToDevice, s), "H2D forces");
+    const unsigned zflags = pinned ? kFlagZeroOut : (kFlagZeroOut | kFlagZeroForces);
     int r = PMGPU_OK;
     // a second attempt only when the cluster-pair list outgrew its estimate
     // (the first attempt recorded the size it needs)
     for (int attempt = 0; attempt < 2; ++attempt) {
-        // the outputs are zeroed inside the evaluation's graph; the status
+        // the energies are zeroed inside the evaluation's graph; the status
         // word comes back with the results (one wait, no second round trip)
+        if (pinned) CK(cudaMemcpyAsync(sys->d_fout, sys->d_acc0, fbytes, cudaMemcpyDeviceToDevice, s), "copy forces");
         r = eval_core(sys, n_forces, forces, sys->d_pos, sys->d_fout, sys->d_energy,
-                      (flags & ~kFlagZeroOut) | kFlagZeroOut);
-        if (r) return r;
-        CK(cudaMemcpyAsync(sys->h_fbuf, sys->d_fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, s), "D2H forces");
+                      (flags & ~kFlagsInternal) | zflags);
+        if (r) break;
+        CK(cudaMemcpyAsync(pinned ? forces_accum : sys->h_fbuf, sys->d_fout, fbytes, cudaMemcpyDeviceToHost, s),
+           "D2H forces");
         CK(cudaMemcpyAsync(sys->h_energy, sys->d_energy, sizeof(double) * kEOut, cudaMemcpyDeviceToHost, s), "D2H energies");
         CK(cudaMemcpyAsync(sys->h_status, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H status");
         sys->col_just_disabled = false;
@@ -2378,8 +2394,15 @@ extern "C" int pmgpu_evaluate(pmgpu_system* sys, int n_forces, pmgpu_force* cons
                                           sys->list_just_invalidated)))
             break;
     }
-    if (r) return r;
-    for (size_t k = 0; k < n3; ++k) forces_accum[k] += sys->h_fbuf[k];
+    if (r) {
+        // a failed evaluation leaves the caller's accumulator as it was
+        const int r0 = r;
+        if (pinned && cudaMemcpyAsync(forces_accum, sys->d_acc0, fbytes, cudaMemcpyDeviceToHost, s) == cudaSuccess)
+            cudaStreamSynchronize(s);
+        return r0;
+    }
+    if (!pinned)
+        for (size_t k = 0; k < n3; ++k) forces_accum[k] += sys->h_fbuf[k];
     energies->lennard_jones += sys->h_energy[0];
     energies->coulomb += sys->h_energy[1];
     // with the molecular virial alone the atomic slots hold the
@@ -2755,7 +2778,7 @@ extern "C" int pmgpu_batch_add(pmgpu_batch* b, pmgpu_system* sys, int n_forces, 
     if (sys->device != b->device) return batch_fail(b, PMGPU_ERR_ARG, "system on another device");
     pmgpu_batch::Member m;
     m.sys = sys; m.pos = d_positions; m.fout = d_forces_accum; m.energy = d_energies;
-    m.flags = flags & ~kFlagZeroOut;
+    m.flags = flags & ~kFlagsInternal;
     for (int k = 0; k < n_forces; ++k) {
         if (!forces[k] || forces[k]->sys != sys) return batch_fail(b, PMGPU_ERR_ARG, "force of another system");
         if (forces[k]->real_sub && !pme_needs_lattice(forces[k])) m.forces.push_back(forces[k]->real_sub);
@@ -3024,7 +3047,7 @@ extern "C" int pmgpu_autotune(pmgpu_system* sys, int n_forces, pmgpu_force* cons
     if (!sys || n_forces <= 0 || !forces || !positions || evals < 1 || !best) return PMGPU_ERR_ARG;
     if (sys->profiling) return fail(sys, PMGPU_ERR_STATE, "autotune in profiling mode");
     cudaSetDevice(sys->device);
-    flags &= ~kFlagZeroOut;
+    flags &= ~kFlagsInternal;
     int r = eval_prepare(sys, n_forces, forces, flags);
     if (r) return r;
     cudaStream_t s = sys->stream;
